@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""LM iterations/s of the joint Levenberg-Marquardt path (plain FP64 GPU).
+
+Workload (default): the 76-pose indoor loop through a 20 m x 20 m floor plan
+with 6-10 rooms, 360 beams over 360 deg, range noise N(0, 0.02 m), odometry
+noise 0.02 m / 0.01 rad, 100x100 SDF grid at 0.2 m, 6 hallucinated points per
+beam: 191,520 point rows, ~5,000 Eikonal rows, 75 odometry rows, 10,225
+unknowns. Seeded synthetic data (sdf-slam_b200/scenes.py) stands in for the
+reference's datasets.
+
+A step is one LM iteration (residuals and Jacobian, cell sort, J^T J and
+-J^T r, supernodal LDL^T, triangular solves, step, cost). Each timed step is a
+one-iteration solve call; an L2 flush (a write of 2x the 126 MB L2) runs
+between steps outside the timed events. `value` is steps over the device time
+of the steps (CUDA events on the library's stream, max over ranks); `e2e`
+times complete solves through the public API from host buffers (problem
+upload, iterations, state download).
+
+Multi-GPU: replicas only. Every rank solves its own independent problem of
+the same size (a different seed) on its own GPU; no data crosses GPUs; rank 0
+reports the aggregate (weak scaling).
+
+--impl reference times the CPU restatement of the reference's LM (oracle/) on
+the host cores with all threads, on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+
+
+def _load_package():
+    if "sdf_slam_b200" in sys.modules:
+        return sys.modules["sdf_slam_b200"]
+    pkg_dir = os.path.join(ROOT, "sdf-slam_b200")
+    spec = importlib.util.spec_from_file_location("sdf_slam_b200", os.path.join(pkg_dir, "__init__.py"),
+                                                  submodule_search_locations=[pkg_dir])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["sdf_slam_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+METRIC = "LM iters/s plain FP64 vs mixed+batched at equal final cost; served p50/p99 ms"
+WORKLOADS = {
+    "floorplan": "76-pose floor-plan loop, 100x100 grid @0.2 m, 360 beams, 6 hallucinated/beam",
+    "room": "10-pose room loop, 40x40 grid @0.25 m, 180 beams, 4 hallucinated/beam",
+    "office": "910-pose 3-lap office, 200x200 grid @0.15 m, 180 beams/180 deg, 6 hallucinated/beam",
+}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except (OSError, ValueError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() in ("active", "1"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _init_dist(world):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    # replicas only: no data-path collective, the process group carries the
+    # barrier and the max-over-ranks reduction of the timings
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def _reduce_max(dist, value):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _reduce_sum(dist, value):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def _barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def make_scene(workload, seed):
+    import sdf_slam_b200.scenes as scenes
+    if workload == "floorplan":
+        return scenes.floorplan_scene(seed=seed)
+    if workload == "room":
+        return scenes.room_scene(seed=seed)
+    if workload == "office":
+        return scenes.office_scene(seed=seed)
+    raise ValueError(workload)
+
+
+def scene_specs(P, scene):
+    prob = P.Problem.from_scene(scene)
+    return prob.specs(min_corner=scene.min_corner, max_corner=scene.max_corner)
+
+
+def _oracle_problem(specs):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    s = O.Specs(**{k: getattr(specs, k) for k in O.Specs.__dataclass_fields__})
+    return O.OracleProblem.from_specs(s)
+
+
+def cpu_reference_rate(specs, iterations, threads):
+    """The oracle's LM (CPU restatement of the reference) on the same problem:
+    iterations/s with `threads` host threads."""
+    orc = _oracle_problem(specs)
+    t0 = time.perf_counter()
+    res = orc.solve(max_iterations=iterations, step_tolerance=0.0, num_threads=threads)
+    dt = time.perf_counter() - t0
+    return res["iterations"] / dt, res, dt
+
+
+def flush_l2(torch, buf):
+    buf.add_(1.0)
+
+
+def run_reference(args, dist, rank):
+    if rank != 0:
+        return 0
+    P = _load_package()
+    scene = make_scene(args.workload, args.seed)
+    specs = scene_specs(P, scene)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_reference_rate(specs, 1, threads)
+    t0 = time.perf_counter()
+    rate, res, dt = cpu_reference_rate(specs, args.steps, threads)
+    wall = time.perf_counter() - t0
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": "LM iters/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / max(1, res["iterations"]),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded floor plan, scenes.py)",
+        "config": {"workload": WORKLOADS[args.workload], "seed": args.seed, "threads": threads},
+        "cpu_baseline": {"value": rate, "unit": "LM iters/s", "cores": threads, "kind": "port",
+                         "sample": f"{res['iterations']} LM iterations of the workload"},
+        "e2e": {"value": rate, "unit": "LM iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gpu(args, dist, world, rank, local):
+    import numpy as np
+    import torch
+    P = _load_package()
+    scene = make_scene(args.workload, args.seed + rank)
+    specs = scene_specs(P, scene)
+    dev = torch.device("cuda", 0)
+    flush_buf = torch.empty(int(2 * 126e6 // 4), dtype=torch.float32, device=dev)
+    opts1 = P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=args.precision)
+    prob = P.Problem.from_specs(specs)
+    # warm-up: upload, symbolic analysis, first iterations
+    for _ in range(args.warmup):
+        P.solve(prob, opts1)
+    torch.cuda.synchronize()
+    _barrier(dist)
+    sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) \
+        if rank == 0 else None
+    if sampler:
+        sampler.start()
+    torch.cuda.synchronize()
+    _barrier(dist)
+    wall0 = time.perf_counter()
+    device_s = 0.0
+    launches = 0
+    phases = np.zeros(5)
+    for _ in range(args.steps):
+        flush_l2(torch, flush_buf)
+        torch.cuda.synchronize()
+        P.solve(prob, opts1)
+        prof = prob.last_profile()
+        device_s += prof["span"]
+        launches += prof["launches"]
+        phases += [prof["assemble"], prof["normal"], prof["factor"], prof["solve"], prof["update"]]
+    torch.cuda.synchronize()
+    _barrier(dist)
+    wall = time.perf_counter() - wall0
+    clocks = sampler.stop() if sampler else None
+    flops = prob.last_profile()["factor_flops"]
+    device_max = _reduce_max(dist, device_s)
+    wall_max = _reduce_max(dist, wall)
+    total_steps = _reduce_sum(dist, args.steps)
+    # end to end through the public API from host buffers
+    e2e_iters = args.e2e_iterations
+    h2d = specs.host_bytes()
+    e2e_t = 0.0
+    d2h = 0
+    for _ in range(args.e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p2 = P.Problem.from_specs(specs)
+        r = P.solve(p2, P.SolverOptions(max_iterations=e2e_iters, step_tolerance=0.0, precision=args.precision))
+        m, poses = p2.state()
+        e2e_t += time.perf_counter() - t0
+        d2h = m.nbytes + poses.nbytes + 8 * len(r.cost_history)
+        p2.close()
+    e2e_t = _reduce_max(dist, e2e_t)
+    e2e_value = world * args.e2e_steps * e2e_iters / e2e_t if e2e_t > 0 else 0.0
+    if rank != 0:
+        return 0
+    z = prob.sizes()
+    per_step = phases / args.steps
+    names = ["assemble", "normal", "factor", "solve", "update"]
+    dominant = names[int(np.argmax(per_step))]
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    fp64_peak = float(os.environ.get("SDFGPU_FP64_PEAK_TFLOPS", "37.0"))
+    # algorithmic bytes of the assembly phase per iteration (row kernels + sort)
+    P_rows = z["num_points"]
+    assemble_bytes = P_rows * (40 + 64 + 4) + P_rows * 4 * 2 * 2 * 2
+    roofline_factor = {
+        "bound": "tensor", "achieved": flops / per_step[2] / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
+        "frac": flops / per_step[2] / 1e12 / fp64_peak, "traffic": None,
+        "kernel": "multifrontal LDL^T (KPanel + KUpdate + KExtendAdd), FP64",
+        "peak_source": "nominal B200 FP64 (no measured FP64 peak on this pool)"}
+    roofline_assemble = {
+        "bound": "hbm", "achieved": assemble_bytes / per_step[0] / 1e9, "peak": hbm, "unit": "GB/s",
+        "frac": assemble_bytes / per_step[0] / 1e9 / hbm, "traffic": None,
+        "kernel": "point rows + cell sort", "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)"}
+    roofline = roofline_factor if dominant in ("factor",) else roofline_assemble
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, res, dt = cpu_reference_rate(specs, args.cpu_iterations, threads)
+        cpu = {"value": rate, "unit": "LM iters/s", "cores": threads, "kind": "port",
+               "sample": f"{res['iterations']} LM iterations of the same workload ({dt:.1f} s)"}
+    line = {
+        "metric": METRIC, "value": total_steps / device_max, "unit": "LM iters/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * device_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded floor plan, scenes.py)",
+        "config": {"workload": WORKLOADS[args.workload], "seed": args.seed, "precision": args.precision,
+                   "unknowns": z["num_parameters"], "point_rows": z["num_points"],
+                   "l2": "flushed between steps (2x126 MB write)", "parallelism": f"replicas x{world}"},
+        "wall_ms_per_step": 1000.0 * wall_max / args.steps,
+        "phase_ms_per_step": {k: 1000.0 * v for k, v in zip(names, per_step)},
+        "factor_gflop_per_step": flops / 1e9,
+        "gpu_launches": int(launches),
+        "roofline": roofline,
+        "roofline_other": roofline_assemble if roofline is roofline_factor else roofline_factor,
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "LM iters/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "iterations_per_step": e2e_iters},
+        "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="floorplan", choices=list(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-iterations", type=int, default=10)
+    ap.add_argument("--cpu-iterations", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = _dist()
+    if world > 1 and args.impl == "b200":
+        # one GPU per rank
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+    dist = _init_dist(world)
+    try:
+        if args.impl == "reference":
+            rc = run_reference(args, dist, rank)
+        else:
+            rc = run_gpu(args, dist, world, rank, local)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,283 @@
+/*
+ * sdfgpu -- B200 (sm_100a) backend for the joint Levenberg-Marquardt path of
+ * sdf-slam: point / hallucination / Eikonal / odometry residuals and
+ * Jacobians, J^T J and -J^T r accumulation, damping, a supernodal LDL^T
+ * factorization of the normal equations, the step, the state update and the
+ * cost, driven by the reference's LM control logic.
+ *
+ * Plain C ABI: opaque handles, plain pointers and sizes, int status codes.
+ * Every function returns SDFGPU_OK (0) or an SDFGPU_ERR_* code; the message of
+ * the last failure on the calling thread is sdfgpu_last_error_message().
+ * No exception crosses this boundary. Paths in the comments are files of the
+ * reference repository (RobinJehn/sdf-slam) that each entry point replaces.
+ *
+ * Threading: a handle is used by one thread at a time; distinct handles may be
+ * used from distinct threads. Calls are synchronous (they return after the
+ * GPU work they start has finished), except for the serving queue, which has
+ * its own worker thread.
+ */
+#ifndef SDFGPU_H_
+#define SDFGPU_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SDFGPU_OK 0
+#define SDFGPU_ERR_INVALID_ARGUMENT 1 /* std::invalid_argument, problem.cpp:19-24,108-110,118-120 */
+#define SDFGPU_ERR_NUMERICAL 2        /* "sparse Cholesky factorization failed", lm_solver.cpp:354-362 */
+#define SDFGPU_ERR_OUT_OF_MEMORY 3    /* device allocation or admission budget exceeded */
+#define SDFGPU_ERR_TIMEOUT 4          /* a bounded wait ran out */
+#define SDFGPU_ERR_CUDA 5             /* any other CUDA runtime failure */
+#define SDFGPU_ERR_NOT_READY 6        /* serving: the request has not finished yet */
+
+/* Precision of a solve. FP64 runs every step in double precision (the plain
+ * path that matches the reference). MIXED assembles and factors in FP32 and
+ * recovers the FP64 step by iterative refinement against a matrix-free FP64
+ * J^T J product; cost, gain ratio and acceptance stay FP64. */
+#define SDFGPU_PRECISION_FP64 0
+#define SDFGPU_PRECISION_MIXED 1
+
+typedef struct sdfgpu_problem sdfgpu_problem; /* one or more independent problems */
+typedef struct sdfgpu_ldlt sdfgpu_ldlt;       /* factor-only sparse LDL^T */
+typedef struct sdfgpu_server sdfgpu_server;   /* serving queue */
+
+/* Message of the last failure on this thread ("" when none). */
+const char* sdfgpu_last_error_message(void);
+
+/* Library version string. */
+const char* sdfgpu_version(void);
+
+/* Number of CUDA devices visible to the library (0 when none; never fails). */
+int32_t sdfgpu_device_count(void);
+
+/* --------------------------------------------------------------- problem --
+ * Flat arrays of everything the LM path reads from sdf_slam::Problem: the
+ * public getters map(), poses(), point_specs(), eikonal_specs(), odom_specs(),
+ * NodeColumn(), huber_delta(), smooth_gradient(), smooth_gradient_step()
+ * (src/problem/problem.hpp:104-142). The grid follows GridMap
+ * (src/core/grid_map.hpp:13-23): node (w, h) has id h*nx + w, spacing
+ * (max - min) / (n - 1). Arrays are copied; the caller keeps ownership. */
+typedef struct sdfgpu_problem_desc {
+  int32_t nx;
+  int32_t ny;
+  double min_x;
+  double min_y;
+  double max_x;
+  double max_y;
+  const double* map_values;          /* nx*ny */
+  int32_t num_frames;
+  const double* poses;               /* num_frames*3: x, y, theta; frame 0 is fixed */
+  int32_t num_points;                /* PointSpec, problem.hpp:28-33 */
+  const int32_t* point_frame;        /* num_points */
+  const double* point_xy;            /* num_points*2, sensor frame */
+  const double* point_expected;      /* num_points: expected SDF (0 for scan points) */
+  const double* point_sqrt_weight;   /* num_points */
+  int32_t num_eikonal;               /* EikonalSpec, problem.hpp:36-41 */
+  const int32_t* eikonal_wh;         /* num_eikonal*2 */
+  const double* eikonal_normal;      /* num_eikonal*2 */
+  const double* eikonal_sqrt_weight; /* num_eikonal */
+  int32_t num_odom;                  /* OdomSpec, problem.hpp:45-50 (odometry then relations) */
+  const int32_t* odom_ij;            /* num_odom*2: frame_i, frame_j */
+  const double* odom_meas;           /* num_odom*3: x, y, theta */
+  const double* odom_sqrt_weight;    /* num_odom */
+  const int32_t* node_to_active;     /* nx*ny: state column of each node or -1 (NodeColumn) */
+  double huber_delta;                /* 0 disables */
+  int32_t smooth_gradient;
+  double smooth_gradient_step;
+} sdfgpu_problem_desc;
+
+/* ProblemOptions (src/problem/problem.hpp:63-87, with Weights :16-25,
+ * HallucinationOptions src/core/hallucination.hpp:17-23 and NormalOptions
+ * src/core/normals.hpp:44-57). normals_method: 0 pca, 1 hybrid, 2 weighted. */
+typedef struct sdfgpu_problem_options {
+  double weight_scan;
+  double weight_hallucination;
+  double weight_eikonal;
+  double weight_odometry;
+  double weight_relation;
+  int32_t hallucination_points_per_scan_point;
+  double hallucination_step_size;
+  int32_t hallucination_both_directions;
+  int32_t normals_method;
+  int32_t normals_k_neighbors;
+  int32_t normals_per_scan;
+  double normals_corner_threshold;
+  double huber_delta;
+  int32_t smooth_gradient;
+  double smooth_gradient_step;
+  int32_t active_region;
+  int32_t active_margin;
+} sdfgpu_problem_options;
+
+/* Reference defaults of ProblemOptions. */
+void sdfgpu_problem_options_default(sdfgpu_problem_options* options);
+
+/* Problem::Problem (src/problem/problem.cpp:11-115): builds the point specs
+ * (scan points, then hallucinated points, frame by frame), the active-region
+ * index maps, the Eikonal specs from k-NN PCA normals and the odometry and
+ * relation specs, then uploads the problem. scan_offsets has num_frames + 1
+ * entries into scan_xy (2 doubles per point). odometry holds num_odometry
+ * relative poses (0 or num_frames - 1). Relations whose frame_j is not below
+ * num_frames are skipped; frames must satisfy 0 <= i < j. */
+int sdfgpu_problem_build(int32_t nx, int32_t ny, double min_x, double min_y, double max_x,
+                         double max_y, const double* map_values, int32_t num_frames,
+                         const double* poses, const int32_t* scan_offsets, const double* scan_xy,
+                         const double* odometry, int32_t num_odometry, int32_t num_relations,
+                         const int32_t* relation_ij, const double* relation_meas,
+                         const double* relation_sqrt_weight, const sdfgpu_problem_options* options,
+                         sdfgpu_problem** out);
+
+/* Copies a problem given by its spec arrays (the drop-in path: the caller's
+ * own Problem is marshalled into a desc). Validation and spec queries run on
+ * the host; the first call that needs the GPU (cost, step, solve, state,
+ * linearization) uploads the problem to the current CUDA device and fails
+ * with SDFGPU_ERR_CUDA when there is none. */
+int sdfgpu_problem_create(const sdfgpu_problem_desc* desc, sdfgpu_problem** out);
+
+/* Several independent problems solved together: every kernel of an LM
+ * iteration covers all of them in one launch (persistent level schedule of
+ * the factorization, one graph per iteration). */
+int sdfgpu_problem_create_batch(const sdfgpu_problem_desc* descs, int32_t count,
+                                sdfgpu_problem** out);
+
+/* Frees the handle and its device memory. Accepts NULL. */
+int sdfgpu_problem_destroy(sdfgpu_problem* problem);
+
+/* Number of instances in the handle (1 unless created as a batch). */
+int32_t sdfgpu_problem_count(const sdfgpu_problem* problem);
+
+/* sizes[0..8] of instance `index`: num_points, num_eikonal, num_odom,
+ * num_active_nodes, num_parameters, num_residuals, num_frames, nx, ny. */
+int sdfgpu_problem_sizes(const sdfgpu_problem* problem, int32_t index, int32_t* sizes);
+
+/* Copies the spec arrays of instance `index` out (any pointer may be NULL). */
+int sdfgpu_problem_get_specs(const sdfgpu_problem* problem, int32_t index, int32_t* point_frame,
+                             double* point_xy, double* point_expected, double* point_sqrt_weight,
+                             int32_t* eikonal_wh, double* eikonal_normal,
+                             double* eikonal_sqrt_weight, int32_t* odom_ij, double* odom_meas,
+                             double* odom_sqrt_weight, int32_t* node_to_active);
+
+/* problem.map().values() and problem.poses() of instance `index`. */
+int sdfgpu_get_state(sdfgpu_problem* problem, int32_t index, double* map_values, double* poses);
+int sdfgpu_set_state(sdfgpu_problem* problem, int32_t index, const double* map_values,
+                     const double* poses);
+
+/* Problem::Cost (src/problem/problem.cpp:132-156) at the current state. */
+int sdfgpu_cost(sdfgpu_problem* problem, int32_t index, double* cost);
+
+/* Problem::ApplyStep (src/problem/problem.cpp:117-130); step has
+ * num_parameters entries (active node values, then x, y, theta of frames
+ * 1..N-1). */
+int sdfgpu_apply_step(sdfgpu_problem* problem, int32_t index, const double* step);
+
+/* ------------------------------------------------------------------- LM ---
+ * SolverOptions / SolveResult (src/solvers/solver.hpp:29-64). */
+typedef struct sdfgpu_solver_options {
+  int32_t max_iterations;
+  double step_tolerance;
+  double lambda_init;
+  double lambda_factor;
+  int32_t reject_worse_steps;
+  int32_t marquardt_scaling;
+  int32_t trust_region;
+  int32_t num_threads; /* accepted for interface parity; unused on the GPU */
+  int32_t precision;   /* SDFGPU_PRECISION_* */
+} sdfgpu_solver_options;
+
+typedef struct sdfgpu_solve_result {
+  int32_t converged;
+  int32_t iterations;
+  double initial_cost;
+  double final_cost;
+  double duration_seconds;
+  int32_t cost_history_length; /* entries written to cost_history (<= capacity) */
+  int32_t status;              /* SDFGPU_OK or the instance's own error code */
+} sdfgpu_solve_result;
+
+/* Reference defaults of SolverOptions. */
+void sdfgpu_solver_options_default(sdfgpu_solver_options* options);
+
+/* SolveLm (src/solvers/lm_solver.cpp:201-434) behind Solve's dispatch
+ * (:436-444) as SolverBackend::kGpuLm. Mutates the state in place. options,
+ * results and cost_history are per instance: options and results have
+ * sdfgpu_problem_count() entries (options may be NULL for the defaults);
+ * cost_history holds that many rows of `capacity` doubles (NULL to skip).
+ * Returns the first non-OK instance status (SDFGPU_ERR_NUMERICAL when a
+ * factorization failed; that instance stops before applying the step). */
+int sdfgpu_solve(sdfgpu_problem* problem, const sdfgpu_solver_options* options,
+                 sdfgpu_solve_result* results, double* cost_history, int32_t capacity);
+
+/* --------------------------------------------------------- linearization --
+ * One LM iteration's quantities at the current state, without moving it:
+ * residuals and Jacobian (lm_solver.cpp:304-385), J^T J with damping
+ * (:391-402), -J^T r (:403) and the step delta (:423-436). Sizes first, then
+ * the copies; pattern buffers use the reference's layout (CSC of the full
+ * symmetric normal matrix with sorted row indices; Jacobian as CSC). */
+int sdfgpu_linearize(sdfgpu_problem* problem, int32_t index, double lambda, int32_t marquardt,
+                     int32_t compute_step);
+
+/* sizes[0..3]: num_rows, num_parameters, nnz(J), nnz(J^T J + damping). */
+int sdfgpu_linearization_sizes(sdfgpu_problem* problem, int64_t* sizes);
+
+/* Any pointer may be NULL. point_cell: per point row h*(nx)+w of its cell or
+ * -1 outside the domain. */
+int sdfgpu_linearization_get(sdfgpu_problem* problem, double* residuals, int32_t* point_cell,
+                             int32_t* j_outer, int32_t* j_inner, double* j_values,
+                             int32_t* n_outer, int32_t* n_inner, double* n_values, double* rhs,
+                             double* step);
+
+/* Timing breakdown of the last solve on this handle, measured with CUDA
+ * events on the handle's stream, in seconds of GPU time per phase summed over
+ * its iterations: [0] residuals + Jacobian + cell sort, [1] J^T J + J^T r,
+ * [2] factorization, [3] triangular solves, [4] step + cost; [5] iterations;
+ * [6] device time from the first iteration's start to the last one's end;
+ * [7] kernels launched by the iterations; [8] useful FP64 flops of one
+ * factorization. phases must hold 9 doubles. */
+int sdfgpu_last_profile(sdfgpu_problem* problem, double* phases);
+
+/* ------------------------------------------------------------ factor only --
+ * LinearSolver::kGpu: ParallelSimplicialLdlt's interface
+ * (src/solvers/parallel_ldlt.hpp:38-51 and Eigen's solve) for any symmetric
+ * matrix given as a full CSC pattern (both triangles, sorted rows). perm
+ * (new -> old, may be NULL for the natural order) fixes the elimination
+ * order. */
+int sdfgpu_ldlt_create(int32_t n, const int32_t* outer, const int32_t* inner, const int32_t* perm,
+                       sdfgpu_ldlt** out);
+/* Numeric factorization with new values on the same pattern; returns
+ * SDFGPU_ERR_NUMERICAL on a zero pivot (Eigen::NumericalIssue). */
+int sdfgpu_ldlt_factorize(sdfgpu_ldlt* ldlt, const double* values);
+int sdfgpu_ldlt_solve(sdfgpu_ldlt* ldlt, const double* b, double* x);
+int sdfgpu_ldlt_destroy(sdfgpu_ldlt* ldlt);
+
+/* ---------------------------------------------------------------- serving --
+ * A request loop with continuous batching: submitted problems are admitted
+ * while their device footprint (state, symbolic analysis, factors) fits the
+ * budget, run LM iterations together with every other admitted request, and
+ * retire individually. */
+int sdfgpu_server_create(int64_t memory_budget_bytes, int32_t max_batch, sdfgpu_server** out);
+/* Copies the request; returns its id. options as for sdfgpu_solve. Fails with
+ * SDFGPU_ERR_OUT_OF_MEMORY when the request alone exceeds the budget. */
+int sdfgpu_server_submit(sdfgpu_server* server, const sdfgpu_problem_desc* desc,
+                         const sdfgpu_solver_options* options, int64_t* request_id);
+/* SDFGPU_ERR_NOT_READY until the request has finished; then fills result and
+ * copies the final state (pointers may be NULL) and forgets the request. */
+int sdfgpu_server_poll(sdfgpu_server* server, int64_t request_id, sdfgpu_solve_result* result,
+                       double* map_values, double* poses);
+/* Cancels a queued or running request. */
+int sdfgpu_server_cancel(sdfgpu_server* server, int64_t request_id);
+/* stats[0..7]: submitted, completed, queued, running, p50 ms, p99 ms,
+ * throughput requests/s, LM iterations/s since creation. */
+int sdfgpu_server_stats(sdfgpu_server* server, double* stats);
+/* Waits up to timeout_ms for every submitted request to finish;
+ * SDFGPU_ERR_TIMEOUT otherwise. */
+int sdfgpu_server_drain(sdfgpu_server* server, int64_t timeout_ms);
+int sdfgpu_server_destroy(sdfgpu_server* server);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SDFGPU_H_ */

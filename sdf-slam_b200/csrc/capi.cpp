@@ -1,0 +1,466 @@
+// C ABI of the sdfgpu library (declared in include/sdfgpu.h). Every entry
+// point converts exceptions into status codes and records the message for
+// sdfgpu_last_error_message().
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "internal.h"
+#include "ldlt.h"
+#include "server.h"
+
+struct sdfgpu_problem {
+  std::vector<sdfgpu::HostProblem> host;  // specs as given (state lives on the device once uploaded)
+  std::unique_ptr<sdfgpu::Engine> engine;
+  sdfgpu::Engine& Device() {
+    if (!engine) {
+      engine = std::make_unique<sdfgpu::Engine>(host);
+    }
+    return *engine;
+  }
+};
+
+struct sdfgpu_ldlt {
+  std::unique_ptr<sdfgpu::LdltEngine> engine;
+};
+
+struct sdfgpu_server {
+  std::unique_ptr<sdfgpu::Server> server;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <typename Fn>
+int Guard(Fn&& fn) {
+  try {
+    g_last_error.clear();
+    fn();
+    return SDFGPU_OK;
+  } catch (const sdfgpu::Error& e) {
+    g_last_error = e.what();
+    return e.code();
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return SDFGPU_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return SDFGPU_ERR_CUDA;
+  } catch (...) {
+    g_last_error = "unknown error";
+    return SDFGPU_ERR_CUDA;
+  }
+}
+
+void NeedHandle(const void* p, const char* what) {
+  if (p == nullptr) {
+    sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, std::string(what) + " is NULL");
+  }
+}
+
+sdfgpu::Engine& Eng(sdfgpu_problem* p) {
+  NeedHandle(p, "problem");
+  return p->Device();
+}
+
+void CheckIndex(const sdfgpu_problem* p, int32_t index) {
+  NeedHandle(p, "problem");
+  if (index < 0 || index >= static_cast<int32_t>(p->host.size())) {
+    sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "instance index out of range");
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* sdfgpu_last_error_message(void) { return g_last_error.c_str(); }
+
+const char* sdfgpu_version(void) { return "sdfgpu 0.1 (sm_100a)"; }
+
+int32_t sdfgpu_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+void sdfgpu_problem_options_default(sdfgpu_problem_options* o) {
+  if (o == nullptr) {
+    return;
+  }
+  *o = sdfgpu_problem_options{};
+  o->weight_scan = 1.0;
+  o->weight_hallucination = 1.0;
+  o->weight_eikonal = 1.0;
+  o->weight_odometry = 1.0;
+  o->weight_relation = 1.0;
+  o->hallucination_points_per_scan_point = 6;
+  o->hallucination_step_size = 0.1;
+  o->hallucination_both_directions = 1;
+  o->normals_method = 2;
+  o->normals_k_neighbors = 10;
+  o->normals_per_scan = 0;
+  o->normals_corner_threshold = 0.2;
+  o->huber_delta = 0.0;
+  o->smooth_gradient = 1;
+  o->smooth_gradient_step = 0.0;
+  o->active_region = 0;
+  o->active_margin = 2;
+}
+
+void sdfgpu_solver_options_default(sdfgpu_solver_options* o) {
+  if (o == nullptr) {
+    return;
+  }
+  *o = sdfgpu_solver_options{};
+  o->max_iterations = 100;
+  o->step_tolerance = 1e-6;
+  o->lambda_init = 1.0;
+  o->lambda_factor = 1.0;
+  o->reject_worse_steps = 0;
+  o->marquardt_scaling = 0;
+  o->trust_region = 0;
+  o->num_threads = 0;
+  o->precision = SDFGPU_PRECISION_FP64;
+}
+
+int sdfgpu_problem_build(int32_t nx, int32_t ny, double min_x, double min_y, double max_x, double max_y,
+                         const double* map_values, int32_t num_frames, const double* poses,
+                         const int32_t* scan_offsets, const double* scan_xy, const double* odometry,
+                         int32_t num_odometry, int32_t num_relations, const int32_t* relation_ij,
+                         const double* relation_meas, const double* relation_sqrt_weight,
+                         const sdfgpu_problem_options* options, sdfgpu_problem** out) {
+  return Guard([&] {
+    NeedHandle(out, "out");
+    *out = nullptr;
+    sdfgpu_problem_options o;
+    if (options != nullptr) {
+      o = *options;
+    } else {
+      sdfgpu_problem_options_default(&o);
+    }
+    if (num_relations > 0 && (relation_ij == nullptr || relation_meas == nullptr)) {
+      sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "relation arrays missing");
+    }
+    if (num_odometry > 0 && odometry == nullptr) {
+      sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "odometry array missing");
+    }
+    std::vector<sdfgpu::HostProblem> v;
+    v.push_back(sdfgpu::BuildProblem(nx, ny, min_x, min_y, max_x, max_y, map_values, num_frames, poses,
+                                     scan_offsets, scan_xy, odometry, num_odometry, num_relations, relation_ij,
+                                     relation_meas, relation_sqrt_weight, o));
+    auto h = std::make_unique<sdfgpu_problem>();
+    h->host = std::move(v);
+    *out = h.release();
+  });
+}
+
+int sdfgpu_problem_create(const sdfgpu_problem_desc* desc, sdfgpu_problem** out) {
+  return sdfgpu_problem_create_batch(desc, 1, out);
+}
+
+int sdfgpu_problem_create_batch(const sdfgpu_problem_desc* descs, int32_t count, sdfgpu_problem** out) {
+  return Guard([&] {
+    NeedHandle(out, "out");
+    *out = nullptr;
+    NeedHandle(descs, "desc");
+    if (count < 1) {
+      sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "batch count must be >= 1");
+    }
+    std::vector<sdfgpu::HostProblem> v;
+    v.reserve(static_cast<size_t>(count));
+    for (int32_t i = 0; i < count; ++i) {
+      v.push_back(sdfgpu::FromDesc(descs[i]));
+    }
+    auto h = std::make_unique<sdfgpu_problem>();
+    h->host = std::move(v);
+    *out = h.release();
+  });
+}
+
+int sdfgpu_problem_destroy(sdfgpu_problem* problem) {
+  return Guard([&] { delete problem; });
+}
+
+int32_t sdfgpu_problem_count(const sdfgpu_problem* problem) {
+  return problem == nullptr ? 0 : static_cast<int32_t>(problem->host.size());
+}
+
+int sdfgpu_problem_sizes(const sdfgpu_problem* problem, int32_t index, int32_t* sizes) {
+  return Guard([&] {
+    CheckIndex(problem, index);
+    NeedHandle(sizes, "sizes");
+    const sdfgpu::HostProblem& hp = problem->host[static_cast<size_t>(index)];
+    sizes[0] = hp.num_points();
+    sizes[1] = hp.num_eikonal();
+    sizes[2] = hp.num_odom();
+    sizes[3] = hp.num_active();
+    sizes[4] = hp.num_params();
+    sizes[5] = hp.num_rows();
+    sizes[6] = hp.num_frames();
+    sizes[7] = hp.nx;
+    sizes[8] = hp.ny;
+  });
+}
+
+int sdfgpu_problem_get_specs(const sdfgpu_problem* problem, int32_t index, int32_t* point_frame,
+                             double* point_xy, double* point_expected, double* point_sqrt_weight,
+                             int32_t* eikonal_wh, double* eikonal_normal, double* eikonal_sqrt_weight,
+                             int32_t* odom_ij, double* odom_meas, double* odom_sqrt_weight,
+                             int32_t* node_to_active) {
+  return Guard([&] {
+    CheckIndex(problem, index);
+    const sdfgpu::HostProblem& hp = problem->host[static_cast<size_t>(index)];
+    auto cp = [](auto* dst, const auto& v) {
+      if (dst != nullptr && !v.empty()) {
+        std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+      }
+    };
+    cp(point_frame, hp.pt_frame);
+    cp(point_xy, hp.pt_xy);
+    cp(point_expected, hp.pt_expected);
+    cp(point_sqrt_weight, hp.pt_sqrtw);
+    cp(eikonal_wh, hp.eik_wh);
+    cp(eikonal_normal, hp.eik_n);
+    cp(eikonal_sqrt_weight, hp.eik_sqrtw);
+    cp(odom_ij, hp.odom_ij);
+    cp(odom_meas, hp.odom_meas);
+    cp(odom_sqrt_weight, hp.odom_sqrtw);
+    cp(node_to_active, hp.node_to_active);
+  });
+}
+
+int sdfgpu_get_state(sdfgpu_problem* problem, int32_t index, double* map_values, double* poses) {
+  return Guard([&] {
+    CheckIndex(problem, index);
+    if (!problem->engine) {
+      // not uploaded yet: the state is the host copy
+      const sdfgpu::HostProblem& hp = problem->host[static_cast<size_t>(index)];
+      if (map_values != nullptr) {
+        std::memcpy(map_values, hp.map_values.data(), hp.map_values.size() * sizeof(double));
+      }
+      if (poses != nullptr) {
+        std::memcpy(poses, hp.poses.data(), hp.poses.size() * sizeof(double));
+      }
+      return;
+    }
+    Eng(problem).GetState(index, map_values, poses);
+  });
+}
+
+int sdfgpu_set_state(sdfgpu_problem* problem, int32_t index, const double* map_values, const double* poses) {
+  return Guard([&] {
+    CheckIndex(problem, index);
+    if (!problem->engine) {
+      sdfgpu::HostProblem& hp = problem->host[static_cast<size_t>(index)];
+      if (map_values != nullptr) {
+        std::memcpy(hp.map_values.data(), map_values, hp.map_values.size() * sizeof(double));
+      }
+      if (poses != nullptr) {
+        std::memcpy(hp.poses.data(), poses, hp.poses.size() * sizeof(double));
+      }
+      return;
+    }
+    Eng(problem).SetState(index, map_values, poses);
+  });
+}
+
+int sdfgpu_cost(sdfgpu_problem* problem, int32_t index, double* cost) {
+  return Guard([&] {
+    CheckIndex(problem, index);
+    NeedHandle(cost, "cost");
+    *cost = Eng(problem).Cost(index);
+  });
+}
+
+int sdfgpu_apply_step(sdfgpu_problem* problem, int32_t index, const double* step) {
+  return Guard([&] {
+    CheckIndex(problem, index);
+    NeedHandle(step, "step");
+    Eng(problem).ApplyStep(index, step);
+  });
+}
+
+int sdfgpu_solve(sdfgpu_problem* problem, const sdfgpu_solver_options* options, sdfgpu_solve_result* results,
+                 double* cost_history, int32_t capacity) {
+  int first_status = SDFGPU_OK;
+  const int rc = Guard([&] {
+    sdfgpu::Engine& e = Eng(problem);
+    NeedHandle(results, "results");
+    sdfgpu_solver_options def;
+    sdfgpu_solver_options_default(&def);
+    std::vector<sdfgpu_solver_options> opts(static_cast<size_t>(e.count()), def);
+    if (options != nullptr) {
+      opts.assign(options, options + e.count());
+    }
+    for (const auto& o : opts) {
+      if (o.max_iterations < 0 || !(o.lambda_init >= 0.0) || !(o.lambda_factor > 0.0)) {
+        sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "invalid solver options");
+      }
+      if (o.precision != SDFGPU_PRECISION_FP64 && o.precision != SDFGPU_PRECISION_MIXED) {
+        sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "unknown precision");
+      }
+    }
+    e.Solve(opts, results, cost_history, capacity > 0 ? capacity : 0);
+    for (int i = 0; i < e.count(); ++i) {
+      if (results[i].status != SDFGPU_OK && first_status == SDFGPU_OK) {
+        first_status = results[i].status;
+      }
+    }
+  });
+  if (rc != SDFGPU_OK) {
+    return rc;
+  }
+  if (first_status == SDFGPU_ERR_NUMERICAL) {
+    g_last_error = "sparse Cholesky factorization failed";
+  }
+  return first_status;
+}
+
+int sdfgpu_linearize(sdfgpu_problem* problem, int32_t index, double lambda, int32_t marquardt,
+                     int32_t compute_step) {
+  return Guard([&] {
+    CheckIndex(problem, index);
+    Eng(problem).Linearize(index, lambda, marquardt != 0, compute_step != 0);
+  });
+}
+
+int sdfgpu_linearization_sizes(sdfgpu_problem* problem, int64_t* sizes) {
+  return Guard([&] {
+    NeedHandle(sizes, "sizes");
+    Eng(problem).LinearizationSizes(sizes);
+  });
+}
+
+int sdfgpu_linearization_get(sdfgpu_problem* problem, double* residuals, int32_t* point_cell, int32_t* j_outer,
+                             int32_t* j_inner, double* j_values, int32_t* n_outer, int32_t* n_inner,
+                             double* n_values, double* rhs, double* step) {
+  return Guard([&] {
+    Eng(problem).LinearizationGet(residuals, point_cell, j_outer, j_inner, j_values, n_outer, n_inner, n_values,
+                                  rhs, step);
+  });
+}
+
+int sdfgpu_last_profile(sdfgpu_problem* problem, double* phases) {
+  return Guard([&] {
+    NeedHandle(phases, "phases");
+    const sdfgpu::IterTimes& t = Eng(problem).times();
+    phases[0] = t.assemble;
+    phases[1] = t.normal;
+    phases[2] = t.factor;
+    phases[3] = t.solve;
+    phases[4] = t.update;
+    phases[5] = t.iterations;
+    phases[6] = t.span;
+    phases[7] = static_cast<double>(t.launches);
+    phases[8] = static_cast<double>(Eng(problem).factor_flops()) * 2.0;
+  });
+}
+
+int sdfgpu_ldlt_create(int32_t n, const int32_t* outer, const int32_t* inner, const int32_t* perm,
+                       sdfgpu_ldlt** out) {
+  return Guard([&] {
+    NeedHandle(out, "out");
+    *out = nullptr;
+    if (n < 1 || outer == nullptr || inner == nullptr) {
+      sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "ldlt needs n >= 1 and a CSC pattern");
+    }
+    auto h = std::make_unique<sdfgpu_ldlt>();
+    h->engine = std::make_unique<sdfgpu::LdltEngine>(n, outer, inner, perm);
+    *out = h.release();
+  });
+}
+
+int sdfgpu_ldlt_factorize(sdfgpu_ldlt* ldlt, const double* values) {
+  return Guard([&] {
+    NeedHandle(ldlt, "ldlt");
+    NeedHandle(values, "values");
+    ldlt->engine->Factorize(values);
+  });
+}
+
+int sdfgpu_ldlt_solve(sdfgpu_ldlt* ldlt, const double* b, double* x) {
+  return Guard([&] {
+    NeedHandle(ldlt, "ldlt");
+    NeedHandle(b, "b");
+    NeedHandle(x, "x");
+    ldlt->engine->Solve(b, x);
+  });
+}
+
+int sdfgpu_ldlt_destroy(sdfgpu_ldlt* ldlt) {
+  return Guard([&] { delete ldlt; });
+}
+
+int sdfgpu_server_create(int64_t memory_budget_bytes, int32_t max_batch, sdfgpu_server** out) {
+  return Guard([&] {
+    NeedHandle(out, "out");
+    *out = nullptr;
+    if (memory_budget_bytes <= 0 || max_batch < 1) {
+      sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "server needs a positive budget and batch size");
+    }
+    auto h = std::make_unique<sdfgpu_server>();
+    h->server = std::make_unique<sdfgpu::Server>(memory_budget_bytes, max_batch);
+    *out = h.release();
+  });
+}
+
+int sdfgpu_server_submit(sdfgpu_server* server, const sdfgpu_problem_desc* desc,
+                         const sdfgpu_solver_options* options, int64_t* request_id) {
+  return Guard([&] {
+    NeedHandle(server, "server");
+    NeedHandle(desc, "desc");
+    NeedHandle(request_id, "request_id");
+    sdfgpu_solver_options o;
+    sdfgpu_solver_options_default(&o);
+    if (options != nullptr) {
+      o = *options;
+    }
+    *request_id = server->server->Submit(sdfgpu::FromDesc(*desc), o);
+  });
+}
+
+int sdfgpu_server_poll(sdfgpu_server* server, int64_t request_id, sdfgpu_solve_result* result,
+                       double* map_values, double* poses) {
+  return Guard([&] {
+    NeedHandle(server, "server");
+    server->server->Poll(request_id, result, map_values, poses);
+  });
+}
+
+int sdfgpu_server_cancel(sdfgpu_server* server, int64_t request_id) {
+  return Guard([&] {
+    NeedHandle(server, "server");
+    server->server->Cancel(request_id);
+  });
+}
+
+int sdfgpu_server_stats(sdfgpu_server* server, double* stats) {
+  return Guard([&] {
+    NeedHandle(server, "server");
+    NeedHandle(stats, "stats");
+    server->server->Stats(stats);
+  });
+}
+
+int sdfgpu_server_drain(sdfgpu_server* server, int64_t timeout_ms) {
+  return Guard([&] {
+    NeedHandle(server, "server");
+    server->server->Drain(timeout_ms);
+  });
+}
+
+int sdfgpu_server_destroy(sdfgpu_server* server) {
+  return Guard([&] { delete server; });
+}
+
+}  // extern "C"

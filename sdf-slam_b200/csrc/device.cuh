@@ -1,0 +1,121 @@
+// Device-side data view shared by the assembly, factorization and solve
+// kernels of the sdfgpu library.
+#pragma once
+
+#include <cstdint>
+
+#include "internal.h"
+
+namespace sdfgpu {
+
+/// Per-instance constants (device copy of InstanceLayout plus schedule data).
+struct InstDev {
+  int32_t nx, ny;
+  double min_x, min_y, dx, dy;
+  int64_t node_off;
+  int64_t cell_off;
+  int32_t col_off;
+  int32_t num_active;
+  int32_t num_frames;
+  int32_t frame_off;
+  int64_t pt_off;
+  int32_t num_points;
+  int64_t eik_off;
+  int32_t num_eik;
+  int64_t odom_off;
+  int32_t num_odom;
+  int32_t smooth_gradient;
+  double smooth_gradient_step;
+  double huber_delta;
+  int64_t allow_off;
+  int32_t allow_words;
+  int32_t pp_ld;
+  int64_t pp_base;
+  int32_t pp_first;
+  int32_t num_params;
+};
+
+/// Status bits per instance.
+constexpr int kStatusZeroPivot = 1;
+constexpr int kStatusPatternOverflow = 2;
+
+/// Per point row record: 4 node Jacobian entries, 3 pose entries, residual.
+constexpr int kPointRec = 8;
+/// Per Eikonal row record: 3 node entries, residual.
+constexpr int kEikRec = 4;
+/// Per odometry spec: residual[3], d_pose_i[3][3], d_pose_j[3][3] (scaled).
+constexpr int kOdomRec = 24;
+
+struct DeviceView {
+  // problem (static between uploads)
+  const InstDev* inst;
+  int32_t num_inst;
+  int64_t total_nodes;
+  int64_t total_cells;
+  int32_t total_frames;
+  int64_t total_points;
+  int64_t total_eik;
+  int64_t total_odom;
+  int32_t n;  // total columns
+  const int32_t* node_col;       // global node -> global natural column or -1
+  const int32_t* col_node;       // global natural column -> global node, or -1 for poses
+  const int32_t* col_inst;       // global natural column -> instance
+  const int32_t* frame_inst;     // global frame -> instance
+  const int32_t* frame_col;      // global frame -> global natural column of x (or -1, frame 0)
+  const int32_t* pt_frame;       // global frame id
+  const double2* pt_xy;
+  const double* pt_exp;
+  const double* pt_sw;
+  const int32_t* eik_node;       // global node of (w, h)
+  const double2* eik_n;
+  const double* eik_sw;
+  const int32_t* eik_index;      // global node -> Eikonal spec whose (w,h) it is, or -1
+  const int32_t* odom_fi;        // global frames
+  const int32_t* odom_fj;
+  const double* odom_meas;       // 3 per spec
+  const double* odom_sw;
+  const int64_t* frame_rows_ptr; // per global frame + 1
+  const int32_t* frame_rows;     // point rows of each frame, ascending
+  const int64_t* frame_odom_ptr; // per global frame + 1
+  const int32_t* frame_odom;     // 2*spec + role (0: frame is i, 1: frame is j)
+  int32_t num_pairs;
+  const int32_t* pair_f;         // smaller frame (global)
+  const int32_t* pair_g;         // larger frame (global)
+  const int64_t* pair_ptr;
+  const int32_t* pair_spec;      // 2*spec + (1 if frame_i of the spec is the larger frame)
+  // state
+  double* map;
+  double* poses;
+  double* map_backup;
+  double* poses_backup;
+  // per iteration
+  double* pt_rec;                // kPointRec per point row
+  int32_t* pt_cell;              // global cell or -1
+  double* eik_rec;
+  double* odom_rec;
+  int32_t* cell_start;           // total_cells + 1
+  int32_t* cell_rows;            // point rows sorted by cell
+  double* rhs;                   // natural order, -J^T r
+  double* step;                  // natural order
+  double* xs;                    // permuted solve vector
+  double* lam;                   // per instance
+  int32_t* marquardt;            // per instance
+  int32_t* status;               // per instance
+  int32_t* active;               // per instance: 1 while the instance is iterating
+  // symbolic
+  const int32_t* perm;
+  const int32_t* pinv;
+  const SupernodeRec* sn;
+  const int32_t* sn_rows;
+  const int32_t* sn_rel;
+  const int32_t* child_list;
+  const int64_t* mm_off;
+  const int64_t* mp_ptr;
+  const int32_t* mp_frame;
+  const int64_t* mp_off;
+  const uint32_t* allow_bits;
+  double* fronts;
+  double* upd;
+};
+
+}  // namespace sdfgpu

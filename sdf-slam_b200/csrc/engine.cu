@@ -1,0 +1,1125 @@
+// Engine: uploads problems, runs the symbolic analysis, and drives the LM
+// iterations of SolveLm (src/solvers/lm_solver.cpp:201-434) on the device.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <utility>
+
+#include "engine.h"
+
+namespace sdfgpu {
+
+__global__ void KPointRows(DeviceView V);
+__global__ void KEikonalRows(DeviceView V);
+__global__ void KOdomRows(DeviceView V);
+__global__ void KCellStart(const int32_t* keys, int64_t n, int64_t num_cells, int32_t* cell_start);
+__global__ void KNodeColumns(DeviceView V);
+__global__ void KPoseBlocks(DeviceView V);
+__global__ void KPosePairs(DeviceView V);
+__global__ void KBackup(DeviceView V, int dir, const int32_t* revert_mask);
+__global__ void KApplyStep(DeviceView V);
+__global__ void KCostTerms(DeviceView V, double* terms);
+__global__ void KStepTerms(DeviceView V, double* sq, double* pred);
+__global__ void KSegmentSum(const double* x, const int64_t* seg_begin, const int64_t* seg_end, double* out);
+void LaunchCellSort(const int32_t* pt_cell, int64_t n, int64_t num_cells, int32_t* keys_a, int32_t* vals_a,
+                    int32_t* keys_b, int32_t* vals_b, int32_t* hist, cudaStream_t stream, bool* result_in_a);
+
+void ThrowCuda(cudaError_t e, const char* what) {
+  const int code = (e == cudaErrorMemoryAllocation) ? SDFGPU_ERR_OUT_OF_MEMORY : SDFGPU_ERR_CUDA;
+  Fail(code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+namespace {
+
+inline unsigned Blocks(int64_t n, int threads) {
+  return static_cast<unsigned>((n + threads - 1) / threads);
+}
+
+/// Position of permuted row r in the front index list of supernode s.
+int FrontIndex(const Symbolic& S, const SupernodeRec& s, int r) {
+  if (r < s.first_col + s.ncols) {
+    return r - s.first_col;
+  }
+  const int32_t* rows = S.sn_rows.data() + s.rows_off;
+  const int32_t* it = std::lower_bound(rows, rows + s.nrows, r);
+  if (it == rows + s.nrows || *it != r) {
+    return -1;
+  }
+  return s.ncols + static_cast<int>(it - rows);
+}
+
+}  // namespace
+
+Engine::Engine(std::vector<HostProblem> problems) : host_(std::move(problems)) {
+  if (host_.empty()) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT, "no problems");
+  }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    Fail(SDFGPU_ERR_CUDA, "no CUDA device available (the GPU backend has no CPU fallback)");
+  }
+  CudaCheck(cudaGetDevice(&device_), "cudaGetDevice");
+  CudaCheck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  for (auto& e : ev_) {
+    CudaCheck(cudaEventCreate(&e), "cudaEventCreate");
+  }
+  for (auto& e : span_) {
+    CudaCheck(cudaEventCreate(&e), "cudaEventCreate");
+  }
+  BuildLayout();
+  UploadProblem();
+  Analyze();
+}
+
+Engine::~Engine() {
+  if (stream_ != nullptr) {
+    cudaStreamSynchronize(stream_);
+    cudaStreamDestroy(stream_);
+  }
+  for (auto& e : ev_) {
+    if (e != nullptr) {
+      cudaEventDestroy(e);
+    }
+  }
+  for (auto& e : span_) {
+    if (e != nullptr) {
+      cudaEventDestroy(e);
+    }
+  }
+}
+
+void Engine::BuildLayout() {
+  layout_.clear();
+  int64_t node = 0;
+  int64_t cell = 0;
+  int col = 0;
+  int frame = 0;
+  int64_t pt = 0;
+  int64_t eik = 0;
+  int64_t odom = 0;
+  for (const HostProblem& hp : host_) {
+    InstanceLayout L{};
+    L.nx = hp.nx;
+    L.ny = hp.ny;
+    L.min_x = hp.min_x;
+    L.min_y = hp.min_y;
+    L.dx = hp.dx();
+    L.dy = hp.dy();
+    L.node_off = node;
+    L.cell_off = cell;
+    L.col_off = col;
+    L.num_active = hp.num_active();
+    L.num_frames = hp.num_frames();
+    L.frame_off = frame;
+    L.pt_off = pt;
+    L.num_points = hp.num_points();
+    L.eik_off = eik;
+    L.num_eik = hp.num_eikonal();
+    L.odom_off = odom;
+    L.num_odom = hp.num_odom();
+    L.huber_delta = hp.huber_delta;
+    L.smooth_gradient = hp.smooth_gradient ? 1 : 0;
+    L.smooth_gradient_step = hp.smooth_gradient_step;
+    layout_.push_back(L);
+    node += static_cast<int64_t>(hp.nx) * hp.ny;
+    cell += static_cast<int64_t>(hp.nx - 1) * (hp.ny - 1);
+    col += hp.num_params();
+    frame += hp.num_frames();
+    pt += hp.num_points();
+    eik += hp.num_eikonal();
+    odom += hp.num_odom();
+  }
+  if (pt > (int64_t{1} << 31) - 1 || col > (1 << 30)) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT, "problem too large for 32-bit row / column indices");
+  }
+  total_nodes_ = node;
+  total_cells_ = cell;
+  n_ = col;
+  total_frames_ = frame;
+  total_points_ = pt;
+  total_eik_ = eik;
+  total_odom_ = odom;
+}
+
+void Engine::UploadProblem() {
+  const size_t I = host_.size();
+  std::vector<int32_t> node_col(static_cast<size_t>(total_nodes_), -1);
+  std::vector<int32_t> col_node(static_cast<size_t>(n_), -1);
+  std::vector<int32_t> col_inst(static_cast<size_t>(n_), 0);
+  std::vector<int32_t> frame_inst(static_cast<size_t>(total_frames_), 0);
+  std::vector<int32_t> frame_col(static_cast<size_t>(total_frames_), -1);
+  std::vector<int32_t> pt_frame(static_cast<size_t>(total_points_));
+  std::vector<double2> pt_xy(static_cast<size_t>(total_points_));
+  std::vector<double> pt_exp(static_cast<size_t>(total_points_));
+  std::vector<double> pt_sw(static_cast<size_t>(total_points_));
+  std::vector<int32_t> eik_node(static_cast<size_t>(total_eik_));
+  std::vector<int32_t> eik_index(static_cast<size_t>(total_nodes_), -1);
+  std::vector<double2> eik_n(static_cast<size_t>(total_eik_));
+  std::vector<double> eik_sw(static_cast<size_t>(total_eik_));
+  std::vector<int32_t> odom_fi(static_cast<size_t>(total_odom_));
+  std::vector<int32_t> odom_fj(static_cast<size_t>(total_odom_));
+  std::vector<double> odom_meas(3 * static_cast<size_t>(total_odom_));
+  std::vector<double> odom_sw(static_cast<size_t>(total_odom_));
+  std::vector<int64_t> frame_rows_ptr(static_cast<size_t>(total_frames_) + 1, 0);
+  std::vector<int32_t> frame_rows(static_cast<size_t>(total_points_));
+  std::vector<int64_t> frame_odom_ptr(static_cast<size_t>(total_frames_) + 1, 0);
+  std::vector<int32_t> frame_odom(2 * static_cast<size_t>(total_odom_));
+  std::vector<int32_t> pair_f;
+  std::vector<int32_t> pair_g;
+  std::vector<int64_t> pair_ptr{0};
+  std::vector<int32_t> pair_spec;
+  std::vector<double> map;
+  std::vector<double> poses;
+  for (size_t i = 0; i < I; ++i) {
+    const HostProblem& hp = host_[i];
+    const InstanceLayout& L = layout_[i];
+    map.insert(map.end(), hp.map_values.begin(), hp.map_values.end());
+    poses.insert(poses.end(), hp.poses.begin(), hp.poses.end());
+    for (int a = 0; a < hp.num_active(); ++a) {
+      const int64_t node = L.node_off + hp.active_to_node[static_cast<size_t>(a)];
+      node_col[static_cast<size_t>(node)] = L.col_off + a;
+      col_node[static_cast<size_t>(L.col_off + a)] = static_cast<int32_t>(node);
+    }
+    for (int c = 0; c < hp.num_params(); ++c) {
+      col_inst[static_cast<size_t>(L.col_off + c)] = static_cast<int32_t>(i);
+    }
+    for (int f = 0; f < hp.num_frames(); ++f) {
+      frame_inst[static_cast<size_t>(L.frame_off + f)] = static_cast<int32_t>(i);
+      frame_col[static_cast<size_t>(L.frame_off + f)] = f >= 1 ? L.col_off + hp.num_active() + 3 * (f - 1) : -1;
+    }
+    for (int k = 0; k < hp.num_points(); ++k) {
+      const size_t g = static_cast<size_t>(L.pt_off + k);
+      pt_frame[g] = L.frame_off + hp.pt_frame[static_cast<size_t>(k)];
+      pt_xy[g] = make_double2(hp.pt_xy[2 * static_cast<size_t>(k)], hp.pt_xy[2 * static_cast<size_t>(k) + 1]);
+      pt_exp[g] = hp.pt_expected[static_cast<size_t>(k)];
+      pt_sw[g] = hp.pt_sqrtw[static_cast<size_t>(k)];
+      ++frame_rows_ptr[static_cast<size_t>(pt_frame[g]) + 1];
+    }
+    for (int e = 0; e < hp.num_eikonal(); ++e) {
+      const size_t g = static_cast<size_t>(L.eik_off + e);
+      const int64_t node = L.node_off + static_cast<int64_t>(hp.eik_wh[2 * static_cast<size_t>(e) + 1]) * hp.nx +
+                           hp.eik_wh[2 * static_cast<size_t>(e)];
+      eik_node[g] = static_cast<int32_t>(node);
+      eik_index[static_cast<size_t>(node)] = static_cast<int32_t>(g);
+      eik_n[g] = make_double2(hp.eik_n[2 * static_cast<size_t>(e)], hp.eik_n[2 * static_cast<size_t>(e) + 1]);
+      eik_sw[g] = hp.eik_sqrtw[static_cast<size_t>(e)];
+    }
+    std::map<std::pair<int, int>, std::vector<int32_t>> pairs;
+    for (int o = 0; o < hp.num_odom(); ++o) {
+      const size_t g = static_cast<size_t>(L.odom_off + o);
+      const int fi = hp.odom_ij[2 * static_cast<size_t>(o)];
+      const int fj = hp.odom_ij[2 * static_cast<size_t>(o) + 1];
+      odom_fi[g] = L.frame_off + fi;
+      odom_fj[g] = L.frame_off + fj;
+      for (int q = 0; q < 3; ++q) {
+        odom_meas[3 * g + static_cast<size_t>(q)] = hp.odom_meas[3 * static_cast<size_t>(o) + static_cast<size_t>(q)];
+      }
+      odom_sw[g] = hp.odom_sqrtw[static_cast<size_t>(o)];
+      ++frame_odom_ptr[static_cast<size_t>(odom_fi[g]) + 1];
+      ++frame_odom_ptr[static_cast<size_t>(odom_fj[g]) + 1];
+      if (fi >= 1 && fj >= 1) {
+        const int lo = std::min(fi, fj);
+        const int hi = std::max(fi, fj);
+        pairs[{lo, hi}].push_back(static_cast<int32_t>(2 * g + (fi > fj ? 1 : 0)));
+      }
+    }
+    for (const auto& kv : pairs) {
+      pair_f.push_back(L.frame_off + kv.first.first);
+      pair_g.push_back(L.frame_off + kv.first.second);
+      pair_spec.insert(pair_spec.end(), kv.second.begin(), kv.second.end());
+      pair_ptr.push_back(static_cast<int64_t>(pair_spec.size()));
+    }
+  }
+  for (int f = 0; f < total_frames_; ++f) {
+    frame_rows_ptr[static_cast<size_t>(f) + 1] += frame_rows_ptr[static_cast<size_t>(f)];
+    frame_odom_ptr[static_cast<size_t>(f) + 1] += frame_odom_ptr[static_cast<size_t>(f)];
+  }
+  {
+    std::vector<int64_t> fill(frame_rows_ptr.begin(), frame_rows_ptr.end() - 1);
+    for (int64_t k = 0; k < total_points_; ++k) {
+      frame_rows[static_cast<size_t>(fill[static_cast<size_t>(pt_frame[static_cast<size_t>(k)])]++)] =
+          static_cast<int32_t>(k);
+    }
+    std::vector<int64_t> ofill(frame_odom_ptr.begin(), frame_odom_ptr.end() - 1);
+    for (int64_t o = 0; o < total_odom_; ++o) {
+      frame_odom[static_cast<size_t>(ofill[static_cast<size_t>(odom_fi[static_cast<size_t>(o)])]++)] =
+          static_cast<int32_t>(2 * o);
+      frame_odom[static_cast<size_t>(ofill[static_cast<size_t>(odom_fj[static_cast<size_t>(o)])]++)] =
+          static_cast<int32_t>(2 * o + 1);
+    }
+  }
+  num_pairs_ = static_cast<int>(pair_f.size());
+  cudaStream_t s = stream_;
+  node_col_.Upload(node_col, s);
+  col_node_.Upload(col_node, s);
+  col_inst_.Upload(col_inst, s);
+  frame_inst_.Upload(frame_inst, s);
+  frame_col_.Upload(frame_col, s);
+  pt_frame_.Upload(pt_frame, s);
+  pt_xy_.Upload(pt_xy, s);
+  pt_exp_.Upload(pt_exp, s);
+  pt_sw_.Upload(pt_sw, s);
+  eik_node_.Upload(eik_node, s);
+  eik_index_.Upload(eik_index, s);
+  eik_n_.Upload(eik_n, s);
+  eik_sw_.Upload(eik_sw, s);
+  odom_fi_.Upload(odom_fi, s);
+  odom_fj_.Upload(odom_fj, s);
+  odom_meas_.Upload(odom_meas, s);
+  odom_sw_.Upload(odom_sw, s);
+  frame_rows_ptr_.Upload(frame_rows_ptr, s);
+  frame_rows_.Upload(frame_rows, s);
+  frame_odom_ptr_.Upload(frame_odom_ptr, s);
+  frame_odom_.Upload(frame_odom, s);
+  pair_f_.Upload(pair_f, s);
+  pair_g_.Upload(pair_g, s);
+  pair_ptr_.Upload(pair_ptr, s);
+  pair_spec_.Upload(pair_spec, s);
+  map_.Upload(map, s);
+  poses_.Upload(poses, s);
+  map_backup_.Alloc(map.size());
+  poses_backup_.Alloc(poses.size());
+  pt_rec_.Alloc(static_cast<size_t>(total_points_) * kPointRec);
+  pt_cell_.Alloc(static_cast<size_t>(total_points_));
+  eik_rec_.Alloc(static_cast<size_t>(total_eik_) * kEikRec);
+  odom_rec_.Alloc(static_cast<size_t>(total_odom_) * kOdomRec);
+  cell_start_.Alloc(static_cast<size_t>(total_cells_) + 2);
+  sort_keys_a_.Alloc(static_cast<size_t>(total_points_));
+  sort_vals_a_.Alloc(static_cast<size_t>(total_points_));
+  sort_keys_b_.Alloc(static_cast<size_t>(total_points_));
+  sort_vals_b_.Alloc(static_cast<size_t>(total_points_));
+  sort_hist_.Alloc(256 * static_cast<size_t>((total_points_ + 2047) / 2048 + 1));
+  rhs_.Alloc(static_cast<size_t>(n_));
+  step_.Alloc(static_cast<size_t>(n_));
+  xs_.Alloc(static_cast<size_t>(n_));
+  dvec_.Alloc(static_cast<size_t>(n_));
+  lam_.Alloc(I);
+  marq_.Alloc(I);
+  status_.Alloc(I);
+  active_.Alloc(I);
+  revert_.Alloc(I);
+  terms_.Alloc(static_cast<size_t>(total_points_ + total_eik_ + total_odom_));
+  sq_terms_.Alloc(static_cast<size_t>(n_));
+  pred_terms_.Alloc(static_cast<size_t>(n_));
+  seg_out_.Alloc(5 * I);
+  std::vector<int64_t> sb;
+  std::vector<int64_t> se;
+  for (size_t i = 0; i < I; ++i) {
+    const InstanceLayout& L = layout_[i];
+    sb.push_back(L.pt_off);
+    se.push_back(L.pt_off + L.num_points);
+    sb.push_back(total_points_ + L.eik_off);
+    se.push_back(total_points_ + L.eik_off + L.num_eik);
+    sb.push_back(total_points_ + total_eik_ + L.odom_off);
+    se.push_back(total_points_ + total_eik_ + L.odom_off + L.num_odom);
+  }
+  seg_begin_.Upload(sb, s);
+  seg_end_.Upload(se, s);
+  std::vector<int64_t> ssb;
+  std::vector<int64_t> sse;
+  for (size_t i = 0; i < I; ++i) {
+    ssb.push_back(layout_[i].col_off);
+    sse.push_back(layout_[i].col_off + host_[i].num_params());
+  }
+  step_seg_begin_.Upload(ssb, s);
+  step_seg_end_.Upload(sse, s);
+  std::vector<int32_t> ones(I, 1);
+  active_.Upload(ones, s);
+  std::vector<int32_t> zeros(I, 0);
+  status_.Upload(zeros, s);
+  marq_.Upload(zeros, s);
+  std::vector<double> lam(I, 1.0);
+  lam_.Upload(lam, s);
+  CudaCheck(cudaStreamSynchronize(s), "upload");
+}
+
+void Engine::Analyze() {
+  sym_ = sdfgpu::Analyze(host_, layout_, 32, 64);
+  cudaStream_t s = stream_;
+  perm_.Upload(sym_.perm, s);
+  pinv_.Upload(sym_.pinv, s);
+  sn_.Upload(sym_.sn, s);
+  sn_rows_.Upload(sym_.sn_rows, s);
+  sn_rel_.Upload(sym_.sn_rel, s);
+  child_list_.Upload(sym_.child_list, s);
+  level_sn_.Upload(sym_.level_sn, s);
+  mm_off_.Upload(sym_.mm_off, s);
+  mp_ptr_.Upload(sym_.mp_ptr, s);
+  mp_off_.Upload(sym_.mp_off, s);
+  mp_frame_.Upload(sym_.mp_frame, s);
+  allow_bits_.Upload(sym_.allow_bits, s);
+  ea_tasks_.Upload(sym_.ea_tasks, s);
+  panel_tasks_.Upload(sym_.panel_tasks, s);
+  update_tasks_.Upload(sym_.update_tasks, s);
+  fronts_.Alloc(static_cast<size_t>(sym_.front_doubles));
+  upd_.Alloc(static_cast<size_t>(std::max<int64_t>(1, sym_.update_doubles)));
+  max_front_ = 1;
+  for (const SupernodeRec& r : sym_.sn) {
+    max_front_ = std::max(max_front_, r.F);
+  }
+  ConfigureSolveKernels(max_front_);
+  std::vector<InstDev> inst(host_.size());
+  for (size_t i = 0; i < host_.size(); ++i) {
+    const InstanceLayout& L = layout_[i];
+    InstDev& d = inst[i];
+    d.nx = L.nx;
+    d.ny = L.ny;
+    d.min_x = L.min_x;
+    d.min_y = L.min_y;
+    d.dx = L.dx;
+    d.dy = L.dy;
+    d.node_off = L.node_off;
+    d.cell_off = L.cell_off;
+    d.col_off = L.col_off;
+    d.num_active = L.num_active;
+    d.num_frames = L.num_frames;
+    d.frame_off = L.frame_off;
+    d.pt_off = L.pt_off;
+    d.num_points = L.num_points;
+    d.eik_off = L.eik_off;
+    d.num_eik = L.num_eik;
+    d.odom_off = L.odom_off;
+    d.num_odom = L.num_odom;
+    d.smooth_gradient = L.smooth_gradient;
+    d.smooth_gradient_step = L.smooth_gradient_step;
+    d.huber_delta = L.huber_delta;
+    d.allow_off = sym_.allow_off[i];
+    d.allow_words = sym_.allow_words[i];
+    d.pp_base = sym_.pp_base[i];
+    d.pp_ld = sym_.pp_ld[i];
+    d.pp_first = sym_.pp_first[i];
+    d.num_params = host_[i].num_params();
+  }
+  inst_.Upload(inst, s);
+  device_bytes_ = 0;
+  device_bytes_ += static_cast<int64_t>(fronts_.size()) * 8 + static_cast<int64_t>(pt_rec_.size()) * 8 +
+                   static_cast<int64_t>(mp_off_.size()) * 12 + static_cast<int64_t>(mm_off_.size()) * 8 +
+                   static_cast<int64_t>(total_points_) * 48;
+  RefreshView();
+  CudaCheck(cudaStreamSynchronize(s), "analyze upload");
+}
+
+void Engine::RefreshView() {
+  DeviceView& V = V_;
+  V.inst = inst_.get();
+  V.num_inst = count();
+  V.total_nodes = total_nodes_;
+  V.total_cells = total_cells_;
+  V.total_frames = total_frames_;
+  V.total_points = total_points_;
+  V.total_eik = total_eik_;
+  V.total_odom = total_odom_;
+  V.n = n_;
+  V.node_col = node_col_.get();
+  V.col_node = col_node_.get();
+  V.col_inst = col_inst_.get();
+  V.frame_inst = frame_inst_.get();
+  V.frame_col = frame_col_.get();
+  V.pt_frame = pt_frame_.get();
+  V.pt_xy = pt_xy_.get();
+  V.pt_exp = pt_exp_.get();
+  V.pt_sw = pt_sw_.get();
+  V.eik_node = eik_node_.get();
+  V.eik_n = eik_n_.get();
+  V.eik_sw = eik_sw_.get();
+  V.eik_index = eik_index_.get();
+  V.odom_fi = odom_fi_.get();
+  V.odom_fj = odom_fj_.get();
+  V.odom_meas = odom_meas_.get();
+  V.odom_sw = odom_sw_.get();
+  V.frame_rows_ptr = frame_rows_ptr_.get();
+  V.frame_rows = frame_rows_.get();
+  V.frame_odom_ptr = frame_odom_ptr_.get();
+  V.frame_odom = frame_odom_.get();
+  V.num_pairs = num_pairs_;
+  V.pair_f = pair_f_.get();
+  V.pair_g = pair_g_.get();
+  V.pair_ptr = pair_ptr_.get();
+  V.pair_spec = pair_spec_.get();
+  V.map = map_.get();
+  V.poses = poses_.get();
+  V.map_backup = map_backup_.get();
+  V.poses_backup = poses_backup_.get();
+  V.pt_rec = pt_rec_.get();
+  V.pt_cell = pt_cell_.get();
+  V.eik_rec = eik_rec_.get();
+  V.odom_rec = odom_rec_.get();
+  V.cell_start = cell_start_.get();
+  V.cell_rows = cell_rows_ptr_;
+  V.rhs = rhs_.get();
+  V.step = step_.get();
+  V.xs = xs_.get();
+  V.lam = lam_.get();
+  V.marquardt = marq_.get();
+  V.status = status_.get();
+  V.active = active_.get();
+  V.perm = perm_.get();
+  V.pinv = pinv_.get();
+  V.sn = sn_.get();
+  V.sn_rows = sn_rows_.get();
+  V.sn_rel = sn_rel_.get();
+  V.child_list = child_list_.get();
+  V.mm_off = mm_off_.get();
+  V.mp_ptr = mp_ptr_.get();
+  V.mp_frame = mp_frame_.get();
+  V.mp_off = mp_off_.get();
+  V.allow_bits = allow_bits_.get();
+  V.fronts = fronts_.get();
+  V.upd = upd_.get();
+}
+
+void Engine::SetActive(const std::vector<int32_t>& active) {
+  CudaCheck(cudaMemcpyAsync(active_.get(), active.data(), active.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                            stream_),
+            "active");
+}
+
+void Engine::SetLambda(const std::vector<double>& lam, const std::vector<int32_t>& marquardt) {
+  CudaCheck(cudaMemcpyAsync(lam_.get(), lam.data(), lam.size() * sizeof(double), cudaMemcpyHostToDevice, stream_),
+            "lambda");
+  CudaCheck(cudaMemcpyAsync(marq_.get(), marquardt.data(), marquardt.size() * sizeof(int32_t),
+                            cudaMemcpyHostToDevice, stream_),
+            "marquardt");
+}
+
+void Engine::ClearStatus() {
+  CudaCheck(cudaMemsetAsync(status_.get(), 0, sizeof(int32_t) * host_.size(), stream_), "status");
+}
+
+std::vector<int32_t> Engine::DownloadStatus() {
+  std::vector<int32_t> st(host_.size());
+  CudaCheck(cudaMemcpyAsync(st.data(), status_.get(), st.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_),
+            "status");
+  CudaCheck(cudaStreamSynchronize(stream_), "status sync");
+  return st;
+}
+
+void Engine::LaunchRows() {
+  if (total_points_ > 0) {
+    KPointRows<<<Blocks(total_points_, 256), 256, 0, stream_>>>(V_);
+  }
+  if (total_eik_ > 0) {
+    KEikonalRows<<<Blocks(total_eik_, 256), 256, 0, stream_>>>(V_);
+  }
+  if (total_odom_ > 0) {
+    KOdomRows<<<Blocks(total_odom_, 128), 128, 0, stream_>>>(V_);
+  }
+  bool in_a = true;
+  if (total_points_ > 0) {
+    LaunchCellSort(pt_cell_.get(), total_points_, total_cells_, sort_keys_a_.get(), sort_vals_a_.get(),
+                   sort_keys_b_.get(), sort_vals_b_.get(), sort_hist_.get(), stream_, &in_a);
+  }
+  const int32_t* keys = in_a ? sort_keys_a_.get() : sort_keys_b_.get();
+  cell_rows_ptr_ = in_a ? sort_vals_a_.get() : sort_vals_b_.get();
+  V_.cell_rows = cell_rows_ptr_;
+  KCellStart<<<Blocks(total_cells_ + 1, 256), 256, 0, stream_>>>(keys, total_points_, total_cells_,
+                                                                   cell_start_.get());
+  CudaCheck(cudaGetLastError(), "row kernels");
+  int bits = 1;
+  while ((int64_t{1} << bits) <= total_cells_) {
+    ++bits;
+  }
+  times_.launches += (total_points_ > 0 ? 1 + 1 + 3 * ((bits + 7) / 8) : 0) + (total_eik_ > 0 ? 1 : 0) +
+                     (total_odom_ > 0 ? 1 : 0) + 1;
+}
+
+void Engine::LaunchNormal() {
+  CudaCheck(cudaMemsetAsync(fronts_.get(), 0, static_cast<size_t>(sym_.front_doubles) * sizeof(double), stream_),
+            "front memset");
+  if (n_ > 0) {
+    KNodeColumns<<<Blocks(n_, 128), 128, 0, stream_>>>(V_);
+  }
+  KPoseBlocks<<<Blocks(static_cast<int64_t>(total_frames_) * 9, 128), 128, 0, stream_>>>(V_);
+  if (num_pairs_ > 0) {
+    KPosePairs<<<Blocks(static_cast<int64_t>(num_pairs_) * 9, 128), 128, 0, stream_>>>(V_);
+  }
+  CudaCheck(cudaGetLastError(), "normal kernels");
+  times_.launches += 2 + (num_pairs_ > 0 ? 1 : 0);
+}
+
+FactorPlan Engine::Plan() {
+  FactorPlan P;
+  P.ea_tasks = ea_tasks_.get();
+  P.panel_tasks = panel_tasks_.get();
+  P.update_tasks = update_tasks_.get();
+  P.level_sn = level_sn_.get();
+  P.dvec = dvec_.get();
+  P.max_front = max_front_;
+  return P;
+}
+
+void Engine::LaunchFactor() { times_.launches += LaunchFactorLevels(sym_, V_, Plan(), stream_); }
+
+void Engine::LaunchSolve() { times_.launches += LaunchSolveLevels(sym_, V_, Plan(), stream_); }
+
+void Engine::LaunchCost(std::vector<double>& cost) {
+  const int64_t terms = total_points_ + total_eik_ + total_odom_;
+  if (terms > 0) {
+    KCostTerms<<<Blocks(terms, 128), 128, 0, stream_>>>(V_, terms_.get());
+  }
+  const size_t I = host_.size();
+  KSegmentSum<<<static_cast<unsigned>(3 * I), 256, 0, stream_>>>(terms_.get(), seg_begin_.get(), seg_end_.get(),
+                                                                   seg_out_.get());
+  std::vector<double> out(3 * I);
+  CudaCheck(cudaMemcpyAsync(out.data(), seg_out_.get(), out.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+            "cost");
+  CudaCheck(cudaStreamSynchronize(stream_), "cost sync");
+  cost.resize(I);
+  for (size_t i = 0; i < I; ++i) {
+    cost[i] = (out[3 * i] + out[3 * i + 1]) + out[3 * i + 2];
+  }
+}
+
+void Engine::LaunchStepAndCost(bool backup) {
+  const int64_t big = std::max<int64_t>(total_nodes_, 3 * static_cast<int64_t>(total_frames_));
+  if (backup) {
+    KBackup<<<Blocks(big, 256), 256, 0, stream_>>>(V_, 0, revert_.get());
+  }
+  if (n_ > 0) {
+    KApplyStep<<<Blocks(n_, 256), 256, 0, stream_>>>(V_);
+    KStepTerms<<<Blocks(n_, 256), 256, 0, stream_>>>(V_, sq_terms_.get(), pred_terms_.get());
+  }
+  const size_t I = host_.size();
+  KSegmentSum<<<static_cast<unsigned>(I), 256, 0, stream_>>>(sq_terms_.get(), step_seg_begin_.get(),
+                                                              step_seg_end_.get(), seg_out_.get() + 3 * I);
+  KSegmentSum<<<static_cast<unsigned>(I), 256, 0, stream_>>>(pred_terms_.get(), step_seg_begin_.get(),
+                                                              step_seg_end_.get(), seg_out_.get() + 4 * I);
+  const int64_t terms = total_points_ + total_eik_ + total_odom_;
+  if (terms > 0) {
+    KCostTerms<<<Blocks(terms, 128), 128, 0, stream_>>>(V_, terms_.get());
+  }
+  KSegmentSum<<<static_cast<unsigned>(3 * I), 256, 0, stream_>>>(terms_.get(), seg_begin_.get(), seg_end_.get(),
+                                                                   seg_out_.get());
+  times_.launches += (backup ? 1 : 0) + 5 + (terms > 0 ? 1 : 0);
+  CudaCheck(cudaMemcpyAsync(h_seg_.get(), seg_out_.get(), 5 * I * sizeof(double), cudaMemcpyDeviceToHost, stream_),
+            "step terms");
+  CudaCheck(cudaMemcpyAsync(h_status_.get(), status_.get(), I * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_),
+            "status");
+  CudaCheck(cudaGetLastError(), "step kernels");
+}
+
+void Engine::Reanalyze() {
+  std::vector<double> poses(3 * static_cast<size_t>(total_frames_));
+  CudaCheck(cudaMemcpyAsync(poses.data(), poses_.get(), poses.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                            stream_),
+            "poses");
+  CudaCheck(cudaStreamSynchronize(stream_), "reanalyze sync");
+  for (size_t i = 0; i < host_.size(); ++i) {
+    std::copy(poses.begin() + 3 * layout_[i].frame_off,
+              poses.begin() + 3 * (layout_[i].frame_off + layout_[i].num_frames), host_[i].poses.begin());
+  }
+  Analyze();
+}
+
+/// Rows + normal equations; re-runs the symbolic analysis (once) when a point
+/// left its pose's analysed cell set. Returns the per-instance status OR.
+int Engine::AssembleWithPattern() {
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    ClearStatus();
+    CudaCheck(cudaEventRecord(ev_[0], stream_), "event");
+    LaunchRows();
+    CudaCheck(cudaEventRecord(ev_[1], stream_), "event");
+    LaunchNormal();
+    CudaCheck(cudaEventRecord(ev_[2], stream_), "event");
+    const std::vector<int32_t> st = DownloadStatus();
+    bool overflow = false;
+    for (const int32_t v : st) {
+      overflow = overflow || (v & kStatusPatternOverflow) != 0;
+    }
+    if (!overflow) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+      times_.assemble += ms * 1e-3;
+      cudaEventElapsedTime(&ms, ev_[1], ev_[2]);
+      times_.normal += ms * 1e-3;
+      return 0;
+    }
+    Reanalyze();
+  }
+  Fail(SDFGPU_ERR_CUDA, "sparsity pattern still overflows after re-analysis");
+}
+
+void Engine::GetState(int i, double* map_values, double* poses) {
+  const InstanceLayout& L = layout_[static_cast<size_t>(i)];
+  if (map_values != nullptr) {
+    CudaCheck(cudaMemcpyAsync(map_values, map_.get() + L.node_off,
+                              sizeof(double) * static_cast<size_t>(L.nx) * L.ny, cudaMemcpyDeviceToHost, stream_),
+              "get map");
+  }
+  if (poses != nullptr) {
+    CudaCheck(cudaMemcpyAsync(poses, poses_.get() + 3 * L.frame_off, sizeof(double) * 3 * L.num_frames,
+                              cudaMemcpyDeviceToHost, stream_),
+              "get poses");
+  }
+  CudaCheck(cudaStreamSynchronize(stream_), "get state");
+}
+
+void Engine::SetState(int i, const double* map_values, const double* poses) {
+  const InstanceLayout& L = layout_[static_cast<size_t>(i)];
+  if (map_values != nullptr) {
+    CudaCheck(cudaMemcpyAsync(map_.get() + L.node_off, map_values,
+                              sizeof(double) * static_cast<size_t>(L.nx) * L.ny, cudaMemcpyHostToDevice, stream_),
+              "set map");
+  }
+  if (poses != nullptr) {
+    CudaCheck(cudaMemcpyAsync(poses_.get() + 3 * L.frame_off, poses, sizeof(double) * 3 * L.num_frames,
+                              cudaMemcpyHostToDevice, stream_),
+              "set poses");
+  }
+  CudaCheck(cudaStreamSynchronize(stream_), "set state");
+}
+
+double Engine::Cost(int i) {
+  std::vector<double> cost;
+  LaunchCost(cost);
+  return cost[static_cast<size_t>(i)];
+}
+
+void Engine::ApplyStep(int i, const double* step) {
+  const InstanceLayout& L = layout_[static_cast<size_t>(i)];
+  std::vector<int32_t> active(host_.size(), 0);
+  active[static_cast<size_t>(i)] = 1;
+  SetActive(active);
+  ClearStatus();
+  CudaCheck(cudaMemcpyAsync(step_.get() + L.col_off, step, sizeof(double) * host_[static_cast<size_t>(i)].num_params(),
+                            cudaMemcpyHostToDevice, stream_),
+            "step");
+  if (n_ > 0) {
+    KApplyStep<<<Blocks(n_, 256), 256, 0, stream_>>>(V_);
+  }
+  CudaCheck(cudaGetLastError(), "apply step");
+  std::vector<int32_t> ones(host_.size(), 1);
+  SetActive(ones);
+  CudaCheck(cudaStreamSynchronize(stream_), "apply step sync");
+}
+
+void Engine::Linearize(int i, double lambda, bool marquardt, bool compute_step) {
+  const size_t I = host_.size();
+  const HostProblem& hp = host_[static_cast<size_t>(i)];
+  const InstanceLayout& L = layout_[static_cast<size_t>(i)];
+  std::vector<int32_t> active(I, 0);
+  active[static_cast<size_t>(i)] = 1;
+  SetActive(active);
+  std::vector<double> lam(I, lambda);
+  std::vector<int32_t> marq(I, marquardt ? 1 : 0);
+  SetLambda(lam, marq);
+  AssembleWithPattern();
+  const int P = hp.num_points();
+  const int E = hp.num_eikonal();
+  const int O = hp.num_odom();
+  std::vector<double> prec(static_cast<size_t>(P) * kPointRec);
+  std::vector<double> erec(static_cast<size_t>(E) * kEikRec);
+  std::vector<double> orec(static_cast<size_t>(O) * kOdomRec);
+  std::vector<int32_t> cells(static_cast<size_t>(P));
+  std::vector<double> rhs(static_cast<size_t>(hp.num_params()));
+  std::vector<double> fronts(static_cast<size_t>(sym_.front_doubles));
+  cudaStream_t s = stream_;
+  CudaCheck(cudaMemcpyAsync(prec.data(), pt_rec_.get() + L.pt_off * kPointRec, prec.size() * 8, cudaMemcpyDeviceToHost, s), "lin");
+  CudaCheck(cudaMemcpyAsync(erec.data(), eik_rec_.get() + L.eik_off * kEikRec, erec.size() * 8, cudaMemcpyDeviceToHost, s), "lin");
+  CudaCheck(cudaMemcpyAsync(orec.data(), odom_rec_.get() + L.odom_off * kOdomRec, orec.size() * 8, cudaMemcpyDeviceToHost, s), "lin");
+  CudaCheck(cudaMemcpyAsync(cells.data(), pt_cell_.get() + L.pt_off, cells.size() * 4, cudaMemcpyDeviceToHost, s), "lin");
+  CudaCheck(cudaMemcpyAsync(rhs.data(), rhs_.get() + L.col_off, rhs.size() * 8, cudaMemcpyDeviceToHost, s), "lin");
+  CudaCheck(cudaMemcpyAsync(fronts.data(), fronts_.get(), fronts.size() * 8, cudaMemcpyDeviceToHost, s), "lin");
+  CudaCheck(cudaStreamSynchronize(s), "lin sync");
+  Lin out;
+  out.instance = i;
+  const int nrows = hp.num_rows();
+  const int np = hp.num_params();
+  out.residuals.resize(static_cast<size_t>(nrows));
+  out.point_cell.resize(static_cast<size_t>(P));
+  // rows in the reference's order with their (column, value) entries
+  std::vector<int32_t> row_ptr(static_cast<size_t>(nrows) + 1, 0);
+  std::vector<int32_t> rcols;
+  std::vector<double> rvals;
+  const int A = hp.num_active();
+  const int cw = hp.nx - 1;
+  for (int k = 0; k < P; ++k) {
+    const double* rec = prec.data() + static_cast<size_t>(k) * kPointRec;
+    out.residuals[static_cast<size_t>(k)] = rec[7];
+    const int cell = cells[static_cast<size_t>(k)];
+    if (cell >= 0) {
+      const int local_cell = static_cast<int>(cell - L.cell_off);
+      const int w = local_cell % cw;
+      const int h = local_cell / cw;
+      out.point_cell[static_cast<size_t>(k)] = h * hp.nx + w;
+      for (int q = 0; q < 4; ++q) {
+        const int node = (h + (q >> 1)) * hp.nx + w + (q & 1);
+        const int col = hp.node_to_active[static_cast<size_t>(node)];
+        if (col >= 0) {
+          rcols.push_back(col);
+          rvals.push_back(rec[q]);
+        }
+      }
+      const int f = hp.pt_frame[static_cast<size_t>(k)];
+      if (f >= 1) {
+        for (int c = 0; c < 3; ++c) {
+          rcols.push_back(A + 3 * (f - 1) + c);
+          rvals.push_back(rec[4 + c]);
+        }
+      }
+    } else {
+      out.point_cell[static_cast<size_t>(k)] = -1;
+    }
+    row_ptr[static_cast<size_t>(k) + 1] = static_cast<int32_t>(rcols.size());
+  }
+  for (int e = 0; e < E; ++e) {
+    const double* rec = erec.data() + static_cast<size_t>(e) * kEikRec;
+    out.residuals[static_cast<size_t>(P + e)] = rec[3];
+    const int w = hp.eik_wh[2 * static_cast<size_t>(e)];
+    const int h = hp.eik_wh[2 * static_cast<size_t>(e) + 1];
+    const int nodes[3] = {h * hp.nx + w, h * hp.nx + w + 1, (h + 1) * hp.nx + w};
+    for (int q = 0; q < 3; ++q) {
+      rcols.push_back(hp.node_to_active[static_cast<size_t>(nodes[q])]);
+      rvals.push_back(rec[q]);
+    }
+    row_ptr[static_cast<size_t>(P + e) + 1] = static_cast<int32_t>(rcols.size());
+  }
+  for (int o = 0; o < O; ++o) {
+    const double* rec = orec.data() + static_cast<size_t>(o) * kOdomRec;
+    const int fi = hp.odom_ij[2 * static_cast<size_t>(o)];
+    const int fj = hp.odom_ij[2 * static_cast<size_t>(o) + 1];
+    for (int r = 0; r < 3; ++r) {
+      const int row = P + E + 3 * o + r;
+      out.residuals[static_cast<size_t>(row)] = rec[r];
+      std::vector<std::pair<int, double>> ent;
+      if (fi >= 1) {
+        for (int c = 0; c < 3; ++c) {
+          ent.emplace_back(A + 3 * (fi - 1) + c, rec[3 + 3 * r + c]);
+        }
+      }
+      for (int c = 0; c < 3; ++c) {
+        ent.emplace_back(A + 3 * (fj - 1) + c, rec[12 + 3 * r + c]);
+      }
+      std::sort(ent.begin(), ent.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+      for (const auto& pr : ent) {
+        rcols.push_back(pr.first);
+        rvals.push_back(pr.second);
+      }
+      row_ptr[static_cast<size_t>(row) + 1] = static_cast<int32_t>(rcols.size());
+    }
+  }
+  // J as CSC (rows ascending per column)
+  out.j_outer.assign(static_cast<size_t>(np) + 1, 0);
+  for (const int c : rcols) {
+    ++out.j_outer[static_cast<size_t>(c) + 1];
+  }
+  for (int c = 0; c < np; ++c) {
+    out.j_outer[static_cast<size_t>(c) + 1] += out.j_outer[static_cast<size_t>(c)];
+  }
+  out.j_inner.resize(rcols.size());
+  out.j_values.resize(rcols.size());
+  {
+    std::vector<int32_t> fill(out.j_outer.begin(), out.j_outer.end() - 1);
+    for (int r = 0; r < nrows; ++r) {
+      for (int p = row_ptr[static_cast<size_t>(r)]; p < row_ptr[static_cast<size_t>(r) + 1]; ++p) {
+        const int c = rcols[static_cast<size_t>(p)];
+        const int dst = fill[static_cast<size_t>(c)]++;
+        out.j_inner[static_cast<size_t>(dst)] = r;
+        out.j_values[static_cast<size_t>(dst)] = rvals[static_cast<size_t>(p)];
+      }
+    }
+  }
+  // structural J^T J (+ inserted diagonal) with values read from the fronts
+  out.n_outer.assign(static_cast<size_t>(np) + 1, 0);
+  std::vector<char> mark(static_cast<size_t>(np), 0);
+  std::vector<int32_t> idx;
+  for (int j = 0; j < np; ++j) {
+    idx.clear();
+    for (int q = out.j_outer[static_cast<size_t>(j)]; q < out.j_outer[static_cast<size_t>(j) + 1]; ++q) {
+      const int r = out.j_inner[static_cast<size_t>(q)];
+      for (int p = row_ptr[static_cast<size_t>(r)]; p < row_ptr[static_cast<size_t>(r) + 1]; ++p) {
+        const int c = rcols[static_cast<size_t>(p)];
+        if (mark[static_cast<size_t>(c)] == 0) {
+          mark[static_cast<size_t>(c)] = 1;
+          idx.push_back(c);
+        }
+      }
+    }
+    if (mark[static_cast<size_t>(j)] == 0) {
+      mark[static_cast<size_t>(j)] = 1;
+      idx.push_back(j);
+    }
+    std::sort(idx.begin(), idx.end());
+    for (const int c : idx) {
+      mark[static_cast<size_t>(c)] = 0;
+      const int pa = sym_.pinv[static_cast<size_t>(L.col_off + c)];
+      const int pb = sym_.pinv[static_cast<size_t>(L.col_off + j)];
+      const int hi = std::max(pa, pb);
+      const int lo = std::min(pa, pb);
+      const SupernodeRec& rec = sym_.sn[static_cast<size_t>(sym_.col_owner[static_cast<size_t>(lo)])];
+      const int li = FrontIndex(sym_, rec, hi);
+      double v = 0.0;
+      if (li >= 0) {
+        v = fronts[static_cast<size_t>(rec.front_off + static_cast<int64_t>(lo - rec.first_col) * rec.F + li)];
+      }
+      out.n_inner.push_back(c);
+      out.n_values.push_back(v);
+    }
+    out.n_outer[static_cast<size_t>(j) + 1] = static_cast<int32_t>(out.n_inner.size());
+  }
+  out.rhs = rhs;
+  if (compute_step) {
+    LaunchFactor();
+    LaunchSolve();
+    const std::vector<int32_t> st = DownloadStatus();
+    if ((st[static_cast<size_t>(i)] & kStatusZeroPivot) != 0) {
+      std::vector<int32_t> ones(I, 1);
+      SetActive(ones);
+      Fail(SDFGPU_ERR_NUMERICAL, "sparse Cholesky factorization failed");
+    }
+    out.step.resize(static_cast<size_t>(np));
+    CudaCheck(cudaMemcpyAsync(out.step.data(), step_.get() + L.col_off, out.step.size() * 8, cudaMemcpyDeviceToHost, s),
+              "step");
+    CudaCheck(cudaStreamSynchronize(s), "step sync");
+  }
+  std::vector<int32_t> ones(I, 1);
+  SetActive(ones);
+  CudaCheck(cudaStreamSynchronize(s), "lin done");
+  lin_ = std::move(out);
+}
+
+void Engine::LinearizationSizes(int64_t* sizes) const {
+  if (lin_.instance < 0) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT, "no linearization computed");
+  }
+  sizes[0] = static_cast<int64_t>(lin_.residuals.size());
+  sizes[1] = static_cast<int64_t>(lin_.rhs.size());
+  sizes[2] = static_cast<int64_t>(lin_.j_inner.size());
+  sizes[3] = static_cast<int64_t>(lin_.n_inner.size());
+}
+
+void Engine::LinearizationGet(double* residuals, int32_t* point_cell, int32_t* j_outer, int32_t* j_inner,
+                              double* j_values, int32_t* n_outer, int32_t* n_inner, double* n_values,
+                              double* rhs, double* step) const {
+  if (lin_.instance < 0) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT, "no linearization computed");
+  }
+  auto cp = [](auto* dst, const auto& v) {
+    if (dst != nullptr && !v.empty()) {
+      std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    }
+  };
+  cp(residuals, lin_.residuals);
+  cp(point_cell, lin_.point_cell);
+  cp(j_outer, lin_.j_outer);
+  cp(j_inner, lin_.j_inner);
+  cp(j_values, lin_.j_values);
+  cp(n_outer, lin_.n_outer);
+  cp(n_inner, lin_.n_inner);
+  cp(n_values, lin_.n_values);
+  cp(rhs, lin_.rhs);
+  if (step != nullptr && lin_.step.empty()) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT, "step was not computed");
+  }
+  cp(step, lin_.step);
+}
+
+void Engine::BeginSolve(const std::vector<sdfgpu_solver_options>& options) {
+  const size_t I = host_.size();
+  t_start_ = std::chrono::steady_clock::now();
+  times_ = IterTimes{};
+  lm_.assign(I, LmInst{});
+  span_started_ = false;
+  need_backup_ = false;
+  iter_ = 0;
+  h_seg_.Alloc(5 * I);
+  h_status_.Alloc(I);
+  SetActive(std::vector<int32_t>(I, 1));
+  std::vector<double> cost0;
+  LaunchCost(cost0);
+  for (size_t i = 0; i < I; ++i) {
+    LmInst& L = lm_[i];
+    L.opt = options[i];
+    L.lam = L.opt.lambda_init;
+    L.prev = cost0[i];
+    L.nu = 2.0;
+    L.active = L.opt.max_iterations > 0 ? 1 : 0;
+    L.res = sdfgpu_solve_result{};
+    L.res.initial_cost = cost0[i];
+    L.hist.assign(1, cost0[i]);
+    need_backup_ = need_backup_ || L.opt.reject_worse_steps != 0 || L.opt.trust_region != 0;
+  }
+}
+
+bool Engine::SolveDone() const {
+  for (const LmInst& L : lm_) {
+    if (L.active != 0 && iter_ < L.opt.max_iterations) {
+      return false;
+    }
+  }
+  return true;
+}
+
+void Engine::LaunchIteration() {
+  const size_t I = host_.size();
+  std::vector<int32_t> active(I);
+  std::vector<double> lam(I);
+  std::vector<int32_t> marq(I);
+  for (size_t i = 0; i < I; ++i) {
+    LmInst& L = lm_[i];
+    if (L.active != 0 && iter_ >= L.opt.max_iterations) {
+      L.active = 0;
+    }
+    active[i] = L.active;
+    lam[i] = L.lam;
+    marq[i] = L.opt.marquardt_scaling != 0 ? 1 : 0;
+  }
+  SetActive(active);
+  SetLambda(lam, marq);
+  ClearStatus();
+  if (!span_started_) {
+    CudaCheck(cudaEventRecord(span_[0], stream_), "event");
+    span_started_ = true;
+  }
+  CudaCheck(cudaEventRecord(ev_[0], stream_), "event");
+  LaunchRows();
+  CudaCheck(cudaEventRecord(ev_[1], stream_), "event");
+  LaunchNormal();
+  CudaCheck(cudaEventRecord(ev_[2], stream_), "event");
+  LaunchFactor();
+  CudaCheck(cudaEventRecord(ev_[3], stream_), "event");
+  LaunchSolve();
+  CudaCheck(cudaEventRecord(ev_[4], stream_), "event");
+  LaunchStepAndCost(need_backup_);
+  CudaCheck(cudaEventRecord(ev_[5], stream_), "event");
+}
+
+void Engine::FinishIteration() {
+  const size_t I = host_.size();
+  for (int attempt = 0;; ++attempt) {
+    CudaCheck(cudaStreamSynchronize(stream_), "iteration");
+    bool overflow = false;
+    for (size_t i = 0; i < I; ++i) {
+      overflow = overflow || (lm_[i].active != 0 && (h_status_[i] & kStatusPatternOverflow) != 0);
+    }
+    if (!overflow) {
+      break;
+    }
+    if (attempt >= 1) {
+      Fail(SDFGPU_ERR_CUDA, "sparsity pattern still overflows after re-analysis");
+    }
+    // a point left its pose's analysed cell set: the step kernel skipped the
+    // update, so re-analyse at the current state and run the iteration again
+    Reanalyze();
+    LaunchIteration();
+  }
+  float ms = 0.0f;
+  double* acc[5] = {&times_.assemble, &times_.normal, &times_.factor, &times_.solve, &times_.update};
+  for (int q = 0; q < 5; ++q) {
+    cudaEventElapsedTime(&ms, ev_[q], ev_[q + 1]);
+    *acc[q] += ms * 1e-3;
+  }
+  ++times_.iterations;
+  bool any_revert = false;
+  std::vector<int32_t> revert(I, 0);
+  for (size_t i = 0; i < I; ++i) {
+    LmInst& L = lm_[i];
+    if (L.active == 0) {
+      continue;
+    }
+    const double cost = (h_seg_[3 * i] + h_seg_[3 * i + 1]) + h_seg_[3 * i + 2];
+    const double sq = h_seg_[3 * I + i];
+    const double pred = h_seg_[4 * I + i];
+    if ((h_status_[i] & kStatusZeroPivot) != 0) {
+      // lm_solver.cpp:354-362: the factorization failure ends the solve
+      // before ApplyStep (the step kernel skipped this instance).
+      L.res.status = SDFGPU_ERR_NUMERICAL;
+      L.active = 0;
+      continue;
+    }
+    L.res.iterations = iter_ + 1;
+    if (std::sqrt(sq) < L.opt.step_tolerance) {
+      L.hist.push_back(cost);
+      L.res.final_cost = cost;
+      L.res.converged = 1;
+      L.active = 0;
+      continue;
+    }
+    double current = cost;
+    if (L.opt.trust_region != 0) {
+      const double rho = pred > 0.0 ? (L.prev - cost) / pred : -1.0;
+      if (rho > 0.0) {
+        L.prev = cost;
+        const double shrink = 1.0 - std::pow(2.0 * rho - 1.0, 3);
+        L.lam = std::max(L.lam * std::max(1.0 / 3.0, shrink), 1e-7);
+        L.nu = 2.0;
+      } else {
+        revert[i] = 1;
+        any_revert = true;
+        current = L.prev;
+        L.lam *= L.nu;
+        L.nu *= 2.0;
+      }
+    } else if (cost < L.prev) {
+      L.lam /= L.opt.lambda_factor;
+      L.prev = cost;
+    } else {
+      L.lam *= L.opt.lambda_factor;
+      if (L.opt.reject_worse_steps != 0) {
+        revert[i] = 1;
+        any_revert = true;
+        current = L.prev;
+      } else {
+        L.prev = cost;
+      }
+    }
+    L.hist.push_back(current);
+    L.res.final_cost = current;
+  }
+  if (any_revert) {
+    CudaCheck(cudaMemcpyAsync(revert_.get(), revert.data(), revert.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                              stream_),
+              "revert mask");
+    const int64_t big = std::max<int64_t>(total_nodes_, 3 * static_cast<int64_t>(total_frames_));
+    KBackup<<<Blocks(big, 256), 256, 0, stream_>>>(V_, 1, revert_.get());
+    CudaCheck(cudaGetLastError(), "restore");
+    // the revert mask is read by the kernel; keep the host copy alive
+    CudaCheck(cudaStreamSynchronize(stream_), "restore");
+  }
+  ++iter_;
+}
+
+void Engine::EndSolve(sdfgpu_solve_result* results, double* cost_history, int capacity) {
+  const size_t I = host_.size();
+  if (span_started_) {
+    CudaCheck(cudaEventRecord(span_[1], stream_), "event");
+  }
+  SetActive(std::vector<int32_t>(I, 1));
+  CudaCheck(cudaStreamSynchronize(stream_), "solve done");
+  if (span_started_) {
+    float ms = 0.0f;
+    CudaCheck(cudaEventElapsedTime(&ms, span_[0], span_[1]), "span");
+    times_.span = ms * 1e-3;
+  }
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start_).count();
+  for (size_t i = 0; i < I; ++i) {
+    LmInst& L = lm_[i];
+    if (L.res.iterations == 0) {
+      L.res.final_cost = L.res.initial_cost;
+    }
+    L.res.duration_seconds = secs;
+    const int len = static_cast<int>(L.hist.size());
+    L.res.cost_history_length = std::min(len, capacity);
+    if (cost_history != nullptr) {
+      for (int q = 0; q < L.res.cost_history_length; ++q) {
+        cost_history[i * static_cast<size_t>(capacity) + static_cast<size_t>(q)] = L.hist[static_cast<size_t>(q)];
+      }
+    }
+    results[i] = L.res;
+  }
+}
+
+void Engine::Solve(const std::vector<sdfgpu_solver_options>& options, sdfgpu_solve_result* results,
+                   double* cost_history, int capacity) {
+  BeginSolve(options);
+  while (!SolveDone()) {
+    LaunchIteration();
+    FinishIteration();
+  }
+  EndSolve(results, cost_history, capacity);
+}
+
+}  // namespace sdfgpu

@@ -1,0 +1,273 @@
+// Engine: device-resident state, symbolic structure and LM driver of one
+// sdfgpu handle (one or several independent problems).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "device.cuh"
+#include "internal.h"
+
+namespace sdfgpu {
+
+[[noreturn]] void ThrowCuda(cudaError_t e, const char* what);
+
+inline void CudaCheck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    ThrowCuda(e, what);
+  }
+}
+
+/// Owning device buffer.
+template <typename T>
+class DevBuf {
+ public:
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { Free(); }
+  void Free() {
+    if (ptr_ != nullptr) {
+      cudaFree(ptr_);
+      ptr_ = nullptr;
+      count_ = 0;
+    }
+  }
+  void Alloc(size_t count) {
+    if (count <= count_ && ptr_ != nullptr) {
+      return;
+    }
+    Free();
+    const size_t bytes = std::max<size_t>(1, count) * sizeof(T);
+    const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&ptr_), bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      ptr_ = nullptr;
+      Fail(SDFGPU_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    count_ = count;
+  }
+  void Upload(const std::vector<T>& v, cudaStream_t s) {
+    Alloc(v.size());
+    if (!v.empty()) {
+      CudaCheck(cudaMemcpyAsync(ptr_, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
+    }
+  }
+  T* get() const { return ptr_; }
+  [[nodiscard]] size_t size() const { return count_; }
+
+ private:
+  T* ptr_{nullptr};
+  size_t count_{0};
+};
+
+/// Device task lists of a symbolic analysis plus the launch parameters of
+/// the factorization and solve kernels.
+struct FactorPlan {
+  const int32_t* ea_tasks{nullptr};
+  const int32_t* panel_tasks{nullptr};
+  const int32_t* update_tasks{nullptr};
+  const int32_t* level_sn{nullptr};
+  double* dvec{nullptr};
+  int max_front{1};
+};
+
+/// Level-scheduled multifrontal LDL^T of the assembled fronts.
+/// Returns the number of kernels launched.
+int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan& P, cudaStream_t stream);
+/// Forward sweep, diagonal, backward sweep: V.step = A^-1 V.rhs (natural order).
+int LaunchSolveLevels(const Symbolic& S, const DeviceView& V, const FactorPlan& P, cudaStream_t stream);
+/// Raises the dynamic shared memory limit of the solve kernels.
+void ConfigureSolveKernels(int max_front);
+
+/// Pinned host buffer.
+template <typename T>
+class HostBuf {
+ public:
+  HostBuf() = default;
+  HostBuf(const HostBuf&) = delete;
+  HostBuf& operator=(const HostBuf&) = delete;
+  ~HostBuf() {
+    if (ptr_ != nullptr) {
+      cudaFreeHost(ptr_);
+    }
+  }
+  void Alloc(size_t count) {
+    if (count <= count_ && ptr_ != nullptr) {
+      return;
+    }
+    if (ptr_ != nullptr) {
+      cudaFreeHost(ptr_);
+      ptr_ = nullptr;
+    }
+    CudaCheck(cudaMallocHost(reinterpret_cast<void**>(&ptr_), std::max<size_t>(1, count) * sizeof(T)),
+              "cudaMallocHost");
+    count_ = count;
+  }
+  T* get() const { return ptr_; }
+  T& operator[](size_t i) const { return ptr_[i]; }
+
+ private:
+  T* ptr_{nullptr};
+  size_t count_{0};
+};
+
+struct IterTimes {
+  double assemble{0};
+  double normal{0};
+  double factor{0};
+  double solve{0};
+  double update{0};
+  int iterations{0};
+  double span{0};        // device time from the first iteration's start to the last one's end
+  int64_t launches{0};   // kernels launched by the iterations
+};
+
+class Engine {
+ public:
+  explicit Engine(std::vector<HostProblem> problems);
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  [[nodiscard]] int count() const { return static_cast<int>(host_.size()); }
+  [[nodiscard]] const HostProblem& host(int i) const { return host_[static_cast<size_t>(i)]; }
+  [[nodiscard]] int64_t DeviceBytes() const { return device_bytes_; }
+
+  void GetState(int i, double* map_values, double* poses);
+  void SetState(int i, const double* map_values, const double* poses);
+  double Cost(int i);
+  void ApplyStep(int i, const double* step);
+
+  void Linearize(int i, double lambda, bool marquardt, bool compute_step);
+  void LinearizationSizes(int64_t* sizes) const;
+  void LinearizationGet(double* residuals, int32_t* point_cell, int32_t* j_outer, int32_t* j_inner,
+                        double* j_values, int32_t* n_outer, int32_t* n_inner, double* n_values, double* rhs,
+                        double* step) const;
+
+  void Solve(const std::vector<sdfgpu_solver_options>& options, sdfgpu_solve_result* results,
+             double* cost_history, int capacity);
+
+  // Split LM driver (used by Solve and by the serving loop, which interleaves
+  // the iterations of several engines on the device):
+  /// Starts a solve: options per instance, initial cost (synchronous).
+  void BeginSolve(const std::vector<sdfgpu_solver_options>& options);
+  /// True when every instance has finished.
+  [[nodiscard]] bool SolveDone() const;
+  /// Enqueues one LM iteration of every running instance (asynchronous).
+  void LaunchIteration();
+  /// Waits for the iteration, re-runs it after a pattern re-analysis if a
+  /// point left its pose's analysed cells, and applies the LM control logic.
+  void FinishIteration();
+  /// Copies results and cost histories (rows of `capacity`).
+  void EndSolve(sdfgpu_solve_result* results, double* cost_history, int capacity);
+  [[nodiscard]] cudaStream_t stream() const { return stream_; }
+  [[nodiscard]] const IterTimes& times() const { return times_; }
+  [[nodiscard]] int64_t factor_flops() const { return sym_.total_flops; }
+  [[nodiscard]] const Symbolic& symbolic() const { return sym_; }
+
+ private:
+  void BuildLayout();
+  void UploadProblem();
+  void Analyze();
+  void RefreshView();
+  void SetActive(const std::vector<int32_t>& active);
+  void SetLambda(const std::vector<double>& lam, const std::vector<int32_t>& marquardt);
+  void ClearStatus();
+  std::vector<int32_t> DownloadStatus();
+  void LaunchRows();
+  void LaunchNormal();
+  void LaunchFactor();
+  void LaunchSolve();
+  void LaunchStepAndCost(bool backup);
+  void LaunchCost(std::vector<double>& cost);
+  void Reanalyze();
+  int AssembleWithPattern();
+  [[nodiscard]] FactorPlan Plan();
+
+  std::vector<HostProblem> host_;
+  std::vector<InstanceLayout> layout_;
+  Symbolic sym_;
+  cudaStream_t stream_{nullptr};
+  cudaEvent_t ev_[6]{};
+  cudaEvent_t span_[2]{};
+  bool span_started_{false};
+  int device_{0};
+  int64_t device_bytes_{0};
+  DeviceView V_{};
+  IterTimes times_;
+  int64_t total_cells_{0};
+  int64_t total_points_{0};
+  int64_t total_eik_{0};
+  int64_t total_odom_{0};
+  int64_t total_nodes_{0};
+  int total_frames_{0};
+  int n_{0};
+  int max_front_{0};
+
+  // problem buffers
+  DevBuf<InstDev> inst_;
+  DevBuf<int32_t> node_col_, col_node_, col_inst_, frame_inst_, frame_col_;
+  DevBuf<int32_t> pt_frame_;
+  DevBuf<double2> pt_xy_;
+  DevBuf<double> pt_exp_, pt_sw_;
+  DevBuf<int32_t> eik_node_, eik_index_;
+  DevBuf<double2> eik_n_;
+  DevBuf<double> eik_sw_;
+  DevBuf<int32_t> odom_fi_, odom_fj_;
+  DevBuf<double> odom_meas_, odom_sw_;
+  DevBuf<int64_t> frame_rows_ptr_, frame_odom_ptr_, pair_ptr_;
+  DevBuf<int32_t> frame_rows_, frame_odom_, pair_f_, pair_g_, pair_spec_;
+  int num_pairs_{0};
+  // state and per-iteration buffers
+  DevBuf<double> map_, poses_, map_backup_, poses_backup_;
+  DevBuf<double> pt_rec_, eik_rec_, odom_rec_;
+  DevBuf<int32_t> pt_cell_, cell_start_, sort_keys_a_, sort_vals_a_, sort_keys_b_, sort_vals_b_, sort_hist_;
+  DevBuf<double> rhs_, step_, xs_, lam_, dvec_;
+  DevBuf<int32_t> marq_, status_, active_, revert_;
+  DevBuf<double> terms_, sq_terms_, pred_terms_, seg_out_;
+  DevBuf<int64_t> seg_begin_, seg_end_, step_seg_begin_, step_seg_end_;
+  // symbolic buffers
+  DevBuf<int32_t> perm_, pinv_, sn_rows_, sn_rel_, child_list_, level_sn_;
+  DevBuf<SupernodeRec> sn_;
+  DevBuf<int64_t> mm_off_, mp_ptr_, mp_off_;
+  DevBuf<int32_t> mp_frame_;
+  DevBuf<uint32_t> allow_bits_;
+  DevBuf<int32_t> ea_tasks_, panel_tasks_, update_tasks_;
+  DevBuf<double> fronts_, upd_;
+  int32_t* cell_rows_ptr_{nullptr};
+  HostBuf<double> h_seg_;      // 5 per instance: cost parts x3, |delta|^2, prediction
+  HostBuf<int32_t> h_status_;
+
+  // LM control state of the current solve (lm_solver.cpp:201-434)
+  struct LmInst {
+    sdfgpu_solver_options opt{};
+    double lam{1.0};
+    double prev{0.0};
+    double nu{2.0};
+    int32_t active{0};
+    int32_t revert{0};
+    sdfgpu_solve_result res{};
+    std::vector<double> hist;
+  };
+  std::vector<LmInst> lm_;
+  int iter_{0};
+  bool need_backup_{false};
+  std::chrono::steady_clock::time_point t_start_;
+
+  // linearization snapshot (host)
+  struct Lin {
+    int instance{-1};
+    std::vector<double> residuals;
+    std::vector<int32_t> point_cell;
+    std::vector<int32_t> j_outer, j_inner, n_outer, n_inner;
+    std::vector<double> j_values, n_values, rhs, step;
+  } lin_;
+};
+
+}  // namespace sdfgpu

@@ -1,0 +1,453 @@
+// Multifrontal supernodal LDL^T of the damped normal equations and its
+// triangular solves (FP64), level by level over the assembly tree.
+//
+// Replaces ParallelSimplicialLdlt::FactorizeParallel / Eigen's solve
+// (src/solvers/parallel_ldlt.hpp:44-51,150-244; src/solvers/lm_solver.cpp:
+// 352-364) with dense frontal work: every supernode's front is assembled from
+// J^T J (written in place by the column kernels) plus its children's update
+// matrices, its pivot columns are factored in panels of kPanel columns, and
+// the Schur complement of the remaining rows is one rank-k update.
+//
+// Storage of a front (column major, leading dimension F = k + m): the lower
+// triangle holds the assembled values, then L below each panel's diagonal
+// block. The strictly lower part of each kPanel x kPanel diagonal block of L
+// is stored transposed in the block's upper triangle, and D in `dvec`
+// (permuted order), so the lower triangle of a diagonal block is never
+// written while other blocks of the same panel still read it.
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace sdfgpu {
+
+constexpr int kPanel = 32;
+constexpr int kTile = 64;
+constexpr int kPanelRowsPerBlock = 128;
+
+/// L(i, j), i > j, of front s (local indices), honouring the transposed
+/// storage of diagonal panel blocks.
+__device__ __forceinline__ double LoadL(const double* Fs, int F, int i, int j) {
+  return (i / kPanel == j / kPanel) ? Fs[static_cast<int64_t>(i) * F + j] : Fs[static_cast<int64_t>(j) * F + i];
+}
+
+/// Adds the children's update matrices into each parent front. A task owns a
+/// range of parent columns, so no two blocks write the same entry; children
+/// are added in their fixed order.
+__global__ void KExtendAdd(DeviceView V, const int32_t* tasks) {
+  const int32_t* t = tasks + 3 * static_cast<int64_t>(blockIdx.x);
+  const int p = t[0];
+  const int clo = t[1];
+  const int chi = t[2];
+  const SupernodeRec P = V.sn[p];
+  if (V.active[P.instance] == 0) {
+    return;
+  }
+  double* Fp = V.fronts + P.front_off;
+  for (int ci = 0; ci < P.child_count; ++ci) {
+    const SupernodeRec C = V.sn[V.child_list[P.child_begin + ci]];
+    const int32_t* rel = V.sn_rel + C.rows_off;
+    const int m = C.nrows;
+    int lo = 0;
+    int hi = m;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (rel[mid] < clo) {
+        lo = mid + 1;
+      } else {
+        hi = mid;
+      }
+    }
+    const int cbeg = lo;
+    hi = m;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (rel[mid] < chi) {
+        lo = mid + 1;
+      } else {
+        hi = mid;
+      }
+    }
+    const int cend = lo;
+    const double* U = V.fronts + C.front_off + static_cast<int64_t>(C.ncols) * C.F + C.ncols;
+    for (int cc = cbeg; cc < cend; ++cc) {
+      double* dst = Fp + static_cast<int64_t>(rel[cc]) * P.F;
+      const double* src = U + static_cast<int64_t>(cc) * C.F;
+      for (int r = cc + threadIdx.x; r < m; r += blockDim.x) {
+        dst[rel[r]] += src[r];
+      }
+    }
+    __syncthreads();
+  }
+}
+
+/// Panel factorization: LDL^T of the panel's diagonal block (redundantly in
+/// every block of the panel, written back by the first), then
+/// L(r, panel) = A(r, panel) L11^-T D^-1 for a chunk of rows below it.
+__global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const int32_t* tasks, double* dvec) {
+  const int32_t* t = tasks + 3 * static_cast<int64_t>(blockIdx.x);
+  const int s = t[0];
+  const int panel = t[1];
+  const int row_begin = t[2];
+  const SupernodeRec S = V.sn[s];
+  if (V.active[S.instance] == 0) {
+    return;
+  }
+  const int F = S.F;
+  const int c0 = panel * kPanel;
+  const int w = min(kPanel, S.ncols - c0);
+  const int c1 = c0 + w;
+  double* Fs = V.fronts + S.front_off;
+  __shared__ double D[kPanel][kPanel + 1];
+  __shared__ double lcol[kPanel];
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < kPanel * kPanel; idx += blockDim.x) {
+    const int i = idx % kPanel;
+    const int j = idx / kPanel;
+    double v;
+    if (i < w && j < w) {
+      v = i >= j ? Fs[static_cast<int64_t>(c0 + j) * F + (c0 + i)] : 0.0;
+    } else {
+      v = (i == j) ? 1.0 : 0.0;
+    }
+    D[i][j] = v;
+  }
+  __syncthreads();
+  bool zero_pivot = false;
+  for (int j = 0; j < w; ++j) {
+    const double dj = D[j][j];
+    zero_pivot = zero_pivot || (dj == 0.0);
+    if (tid > j && tid < w) {
+      lcol[tid] = D[tid][j] / dj;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < kPanel * kPanel; idx += blockDim.x) {
+      const int i = idx % kPanel;
+      const int l = idx / kPanel;
+      if (l > j && i >= l && i < w) {
+        D[i][l] -= D[i][j] * lcol[l];
+      }
+    }
+    __syncthreads();
+    if (tid > j && tid < w) {
+      D[tid][j] = lcol[tid];
+    }
+    __syncthreads();
+  }
+  if (row_begin == c1) {
+    // first block of the panel: D into dvec, L11 transposed into the upper
+    // triangle of the diagonal block
+    if (tid < w) {
+      dvec[S.first_col + c0 + tid] = D[tid][tid];
+    }
+    for (int idx = tid; idx < kPanel * kPanel; idx += blockDim.x) {
+      const int i = idx % kPanel;
+      const int j = idx / kPanel;
+      if (i > j && i < w) {
+        Fs[static_cast<int64_t>(c0 + i) * F + (c0 + j)] = D[i][j];
+      }
+    }
+    if (tid == 0 && zero_pivot) {
+      atomicOr(V.status + S.instance, kStatusZeroPivot);
+    }
+  }
+  const int r = row_begin + tid;
+  if (r < F && r >= c1) {
+    double y[kPanel];
+#pragma unroll
+    for (int j = 0; j < kPanel; ++j) {
+      y[j] = j < w ? Fs[static_cast<int64_t>(c0 + j) * F + r] : 0.0;
+    }
+#pragma unroll
+    for (int j = 1; j < kPanel; ++j) {
+#pragma unroll
+      for (int l = 0; l < j; ++l) {
+        y[j] -= y[l] * D[j][l];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kPanel; ++j) {
+      if (j < w) {
+        Fs[static_cast<int64_t>(c0 + j) * F + r] = y[j] / D[j][j];
+      }
+    }
+  }
+}
+
+/// Tiled rank-k update C -= L_I D L_J^T (lower part only). panel >= 0:
+/// update of the remaining pivot columns by one panel; panel == -1: Schur
+/// complement of the trailing m x m block by all k pivots.
+__global__ void __launch_bounds__(256) KUpdate(DeviceView V, const int32_t* tasks, const double* dvec) {
+  const int32_t* t = tasks + 4 * static_cast<int64_t>(blockIdx.x);
+  const int s = t[0];
+  const int panel = t[1];
+  const int ti = t[2];
+  const int tj = t[3];
+  const SupernodeRec S = V.sn[s];
+  if (V.active[S.instance] == 0) {
+    return;
+  }
+  const int F = S.F;
+  int kb;
+  int ke;
+  int r0;
+  int cc0;
+  int clim;
+  if (panel >= 0) {
+    kb = panel * kPanel;
+    ke = min(S.ncols, kb + kPanel);
+    r0 = ke + ti * kTile;
+    cc0 = ke + tj * kTile;
+    clim = S.ncols;
+  } else {
+    kb = 0;
+    ke = S.ncols;
+    r0 = S.ncols + ti * kTile;
+    cc0 = S.ncols + tj * kTile;
+    clim = F;
+  }
+  double* Fs = V.fronts + S.front_off;
+  const double* d = dvec + S.first_col;
+  __shared__ double As[kPanel][kTile];
+  __shared__ double Bs[kPanel][kTile];
+  const int tid = threadIdx.x;
+  const int tx = tid % 16;
+  const int ty = tid / 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      acc[a][b] = 0.0;
+    }
+  }
+  for (int kk = kb; kk < ke; kk += kPanel) {
+    const int kw = min(kPanel, ke - kk);
+#pragma unroll
+    for (int q = 0; q < (kPanel * kTile) / 256; ++q) {
+      const int idx = tid + 256 * q;
+      const int rr = idx % kTile;
+      const int l = idx / kTile;
+      double av = 0.0;
+      double bv = 0.0;
+      if (l < kw) {
+        const int64_t colbase = static_cast<int64_t>(kk + l) * F;
+        if (r0 + rr < F) {
+          av = Fs[colbase + r0 + rr] * d[kk + l];
+        }
+        if (cc0 + rr < clim) {
+          bv = Fs[colbase + cc0 + rr];
+        }
+      }
+      As[l][rr] = av;
+      Bs[l][rr] = bv;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int l = 0; l < kPanel; ++l) {
+      double av[4];
+      double bv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        av[a] = As[l][tx + 16 * a];
+        bv[a] = Bs[l][ty + 16 * a];
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int c = cc0 + ty + 16 * b;
+    if (c >= clim) {
+      continue;
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int r = r0 + tx + 16 * a;
+      if (r < F && r >= c) {
+        Fs[static_cast<int64_t>(c) * F + r] -= acc[a][b];
+      }
+    }
+  }
+}
+
+/// Forward solve of one level: gathers the children's update vectors,
+/// solves L11 y = v, forms the update u = v_m - L21 y for the parent and
+/// stores D^-1 y (Eigen's solve applies the inverse diagonal between the two
+/// triangular sweeps).
+__global__ void KForward(DeviceView V, const int32_t* level_sn, const double* dvec) {
+  extern __shared__ double v[];
+  const int s = level_sn[blockIdx.x];
+  const SupernodeRec S = V.sn[s];
+  if (V.active[S.instance] == 0) {
+    return;
+  }
+  const int k = S.ncols;
+  const int m = S.nrows;
+  const int F = S.F;
+  const double* Fs = V.fronts + S.front_off;
+  for (int j = threadIdx.x; j < F; j += blockDim.x) {
+    v[j] = j < k ? V.rhs[V.perm[S.first_col + j]] : 0.0;
+  }
+  __syncthreads();
+  for (int ci = 0; ci < S.child_count; ++ci) {
+    const SupernodeRec C = V.sn[V.child_list[S.child_begin + ci]];
+    const int32_t* rel = V.sn_rel + C.rows_off;
+    const double* u = V.upd + C.upd_off;
+    for (int r = threadIdx.x; r < C.nrows; r += blockDim.x) {
+      v[rel[r]] += u[r];
+    }
+    __syncthreads();
+  }
+  for (int j = 0; j < k; ++j) {
+    const double yj = v[j];
+    for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) {
+      v[i] -= LoadL(Fs, F, i, j) * yj;
+    }
+    __syncthreads();
+  }
+  for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    double acc = v[k + r];
+    for (int j = 0; j < k; ++j) {
+      acc -= Fs[static_cast<int64_t>(j) * F + k + r] * v[j];
+    }
+    V.upd[S.upd_off + r] = acc;
+  }
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    V.xs[S.first_col + j] = (1.0 / dvec[S.first_col + j]) * v[j];
+  }
+}
+
+/// Backward solve of one level (root first): z = x_k - L21^T x_R, then
+/// L11^T x = z; writes the step in natural order.
+__global__ void KBackward(DeviceView V, const int32_t* level_sn) {
+  extern __shared__ double z[];
+  const int s = level_sn[blockIdx.x];
+  const SupernodeRec S = V.sn[s];
+  if (V.active[S.instance] == 0) {
+    return;
+  }
+  const int k = S.ncols;
+  const int m = S.nrows;
+  const int F = S.F;
+  const double* Fs = V.fronts + S.front_off;
+  const int32_t* rows = V.sn_rows + S.rows_off;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  for (int j = warp; j < k; j += nwarps) {
+    double acc = 0.0;
+    const double* col = Fs + static_cast<int64_t>(j) * F + k;
+    for (int r = lane; r < m; r += 32) {
+      acc += col[r] * V.xs[rows[r]];
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      acc += __shfl_down_sync(0xffffffffu, acc, off);
+    }
+    if (lane == 0) {
+      z[j] = V.xs[S.first_col + j] - acc;
+    }
+  }
+  __syncthreads();
+  for (int j = k - 1; j >= 0; --j) {
+    const double xj = z[j];
+    for (int i = threadIdx.x; i < j; i += blockDim.x) {
+      z[i] -= LoadL(Fs, F, j, i) * xj;
+    }
+    __syncthreads();
+  }
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    V.xs[S.first_col + j] = z[j];
+    V.step[V.perm[S.first_col + j]] = z[j];
+  }
+}
+
+}  // namespace sdfgpu
+
+// ------------------------------------------------------------ launchers --
+
+#include <mutex>
+
+#include "engine.h"
+
+namespace sdfgpu {
+
+void ConfigureSolveKernels(int max_front) {
+  // The attribute belongs to the kernel, not to an engine: it only grows, so
+  // an engine with smaller fronts never lowers another engine's limit.
+  static std::mutex mu;
+  static int configured = 48 * 1024;
+  const int smem = max_front * static_cast<int>(sizeof(double));
+  if (smem > 227 * 1024) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT, "front too large for the solve kernels");
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (smem > configured) {
+    CudaCheck(cudaFuncSetAttribute(KForward, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
+    CudaCheck(cudaFuncSetAttribute(KBackward, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
+    configured = smem;
+  }
+}
+
+int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan& P, cudaStream_t stream) {
+  int launches = 0;
+  for (int l = 0; l < S.num_levels; ++l) {
+    const TaskRange ea = S.ea_range[static_cast<size_t>(l)];
+    if (ea.count > 0) {
+      KExtendAdd<<<static_cast<unsigned>(ea.count), 128, 0, stream>>>(V, P.ea_tasks + 3 * ea.begin);
+      ++launches;
+    }
+    for (int t = 0; t < S.level_panels[static_cast<size_t>(l)]; ++t) {
+      const size_t slot = static_cast<size_t>(S.panel_index_base[static_cast<size_t>(l)] + t);
+      const TaskRange pr = S.panel_range[slot];
+      if (pr.count > 0) {
+        KPanel<<<static_cast<unsigned>(pr.count), kPanelRowsPerBlock, 0, stream>>>(V, P.panel_tasks + 3 * pr.begin,
+                                                                                   P.dvec);
+        ++launches;
+      }
+      const TaskRange ur = S.update_range[slot];
+      if (ur.count > 0) {
+        KUpdate<<<static_cast<unsigned>(ur.count), 256, 0, stream>>>(V, P.update_tasks + 4 * ur.begin, P.dvec);
+        ++launches;
+      }
+    }
+    const TaskRange sr = S.update_range[static_cast<size_t>(S.panel_index_base.back() + l)];
+    if (sr.count > 0) {
+      KUpdate<<<static_cast<unsigned>(sr.count), 256, 0, stream>>>(V, P.update_tasks + 4 * sr.begin, P.dvec);
+      ++launches;
+    }
+  }
+  CudaCheck(cudaGetLastError(), "factor kernels");
+  return launches;
+}
+
+int LaunchSolveLevels(const Symbolic& S, const DeviceView& V, const FactorPlan& P, cudaStream_t stream) {
+  int launches = 0;
+  const size_t smem = static_cast<size_t>(P.max_front) * sizeof(double);
+  for (int l = 0; l < S.num_levels; ++l) {
+    const int b = S.level_begin[static_cast<size_t>(l)];
+    const int e = S.level_begin[static_cast<size_t>(l) + 1];
+    if (e > b) {
+      KForward<<<static_cast<unsigned>(e - b), 256, smem, stream>>>(V, P.level_sn + b, P.dvec);
+      ++launches;
+    }
+  }
+  for (int l = S.num_levels - 1; l >= 0; --l) {
+    const int b = S.level_begin[static_cast<size_t>(l)];
+    const int e = S.level_begin[static_cast<size_t>(l) + 1];
+    if (e > b) {
+      KBackward<<<static_cast<unsigned>(e - b), 256, smem, stream>>>(V, P.level_sn + b);
+      ++launches;
+    }
+  }
+  CudaCheck(cudaGetLastError(), "solve kernels");
+  return launches;
+}
+
+}  // namespace sdfgpu

@@ -1,0 +1,177 @@
+// Internal host-side types of the sdfgpu library (not part of the C ABI).
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sdfgpu.h"
+
+namespace sdfgpu {
+
+/// Exception carrying a C-ABI status code; converted at the boundary.
+class Error : public std::runtime_error {
+ public:
+  Error(int code, const std::string& msg) : std::runtime_error(msg), code_(code) {}
+  [[nodiscard]] int code() const { return code_; }
+
+ private:
+  int code_;
+};
+
+[[noreturn]] inline void Fail(int code, const std::string& msg) { throw Error(code, msg); }
+
+/// One problem's spec arrays in host memory: the fields of sdf_slam::Problem
+/// the LM path reads (src/problem/problem.hpp:104-142), flattened.
+struct HostProblem {
+  int nx{2};
+  int ny{2};
+  double min_x{0.0};
+  double min_y{0.0};
+  double max_x{1.0};
+  double max_y{1.0};
+  std::vector<double> map_values;
+  std::vector<double> poses;  // 3 per frame
+  std::vector<int32_t> pt_frame;
+  std::vector<double> pt_xy;
+  std::vector<double> pt_expected;
+  std::vector<double> pt_sqrtw;
+  std::vector<int32_t> eik_wh;
+  std::vector<double> eik_n;
+  std::vector<double> eik_sqrtw;
+  std::vector<int32_t> odom_ij;
+  std::vector<double> odom_meas;
+  std::vector<double> odom_sqrtw;
+  std::vector<int32_t> node_to_active;
+  std::vector<int32_t> active_to_node;
+  double huber_delta{0.0};
+  bool smooth_gradient{true};
+  double smooth_gradient_step{0.0};
+
+  [[nodiscard]] int num_frames() const { return static_cast<int>(poses.size() / 3); }
+  [[nodiscard]] int num_points() const { return static_cast<int>(pt_frame.size()); }
+  [[nodiscard]] int num_eikonal() const { return static_cast<int>(eik_sqrtw.size()); }
+  [[nodiscard]] int num_odom() const { return static_cast<int>(odom_sqrtw.size()); }
+  [[nodiscard]] int num_active() const { return static_cast<int>(active_to_node.size()); }
+  [[nodiscard]] int num_pose_params() const { return 3 * (num_frames() - 1); }
+  [[nodiscard]] int num_params() const { return num_active() + num_pose_params(); }
+  [[nodiscard]] int num_rows() const { return num_points() + num_eikonal() + 3 * num_odom(); }
+  [[nodiscard]] double dx() const { return (max_x - min_x) / (nx - 1); }
+  [[nodiscard]] double dy() const { return (max_y - min_y) / (ny - 1); }
+};
+
+/// Validates a C-ABI problem description and copies it (throws Error with
+/// SDFGPU_ERR_INVALID_ARGUMENT).
+HostProblem FromDesc(const sdfgpu_problem_desc& desc);
+
+/// Problem::Problem (src/problem/problem.cpp:11-115) on the host.
+HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_x, double max_y,
+                         const double* map_values, int num_frames, const double* poses,
+                         const int32_t* scan_offsets, const double* scan_xy,
+                         const double* odometry, int num_odometry, int num_relations,
+                         const int32_t* relation_ij, const double* relation_meas,
+                         const double* relation_sqrt_weight, const sdfgpu_problem_options& options);
+
+// ------------------------------------------------------------- symbolic --
+
+/// Per-supernode record uploaded to the device.
+struct SupernodeRec {
+  int64_t front_off;  // first double of the dense front (column major, ld = F)
+  int64_t rows_off;   // first entry in the row / relative-index arrays
+  int64_t upd_off;    // first entry of the forward-solve update vector
+  int32_t first_col;  // global permuted column of the first pivot
+  int32_t ncols;      // k: pivots
+  int32_t nrows;      // m: rows below the pivot block
+  int32_t F;          // k + m
+  int32_t child_begin;
+  int32_t child_count;
+  int32_t parent;     // -1 for a root
+  int32_t instance;
+};
+
+/// A contiguous block of work items of one kernel launch in the level
+/// schedule.
+struct TaskRange {
+  int64_t begin{0};
+  int64_t count{0};
+};
+
+/// Supernodal multifrontal structure of the normal equations of all
+/// instances of a handle (nested dissection of each grid, pose block last).
+struct Symbolic {
+  int n{0};                                  // total columns, all instances
+  std::vector<int32_t> perm;                 // permuted -> natural (global)
+  std::vector<int32_t> pinv;                 // natural -> permuted (global)
+  std::vector<SupernodeRec> sn;
+  std::vector<int32_t> sn_rows;              // concatenated R_s (global permuted rows)
+  std::vector<int32_t> sn_rel;               // position of each R_s row in the parent front
+  std::vector<int32_t> child_list;
+  std::vector<int32_t> col_owner;            // permuted column -> supernode
+  int64_t front_doubles{0};
+  int64_t update_doubles{0};
+  int num_levels{0};
+  int panel_width{32};
+  int tile{64};
+  // Level schedule. For level L: supernodes level_sn[level_begin[L]..]. For
+  // each (level, panel t) a range of panel tasks (supernode, row chunk) and of
+  // update tasks (supernode, tile i, tile j); extend-add tasks per level.
+  std::vector<int32_t> level_begin;
+  std::vector<int32_t> level_sn;
+  std::vector<int32_t> level_panels;         // max panel count per level
+  std::vector<int32_t> ea_tasks;             // (sn, col_lo, col_hi) triples
+  std::vector<TaskRange> ea_range;           // per level
+  std::vector<int32_t> panel_tasks;          // (sn, panel, row_begin) triples
+  std::vector<TaskRange> panel_range;        // per (level, panel) flattened
+  std::vector<int32_t> update_tasks;         // (sn, panel, ti, tj) quads
+  std::vector<TaskRange> update_range;       // per (level, panel) flattened
+  std::vector<int32_t> panel_index_base;     // level -> first (level,panel) slot
+  // Assembly offsets of J^T J entries into the front buffer, indexed by the
+  // global natural column of a node.
+  std::vector<int64_t> mm_off;               // 9 stencil slots per column (-1: stored elsewhere)
+  std::vector<int64_t> mp_ptr;               // per column + 1: range in mp_frame / mp_off
+  std::vector<int32_t> mp_frame;             // coupled frame (instance-local, >= 1), ascending
+  std::vector<int64_t> mp_off;               // offset of (pose var (frame, x), node column)
+  // Cells each frame's points may occupy without leaving the pattern:
+  // bitmap over the instance's cells, one row of words per frame.
+  std::vector<uint32_t> allow_bits;
+  std::vector<int64_t> allow_off;            // per instance: first word
+  std::vector<int32_t> allow_words;          // per instance: words per frame
+  std::vector<int64_t> pp_base;              // per instance: root front offset (pose block)
+  std::vector<int32_t> pp_ld;                // per instance: root front leading dimension
+  std::vector<int32_t> pp_first;             // per instance: local index of pose var 0 in the root front
+  int64_t total_flops{0};                    // dense front flops (useful)
+};
+
+/// Per-instance layout inside a handle's concatenated arrays.
+struct InstanceLayout {
+  int nx, ny;
+  double min_x, min_y, dx, dy;
+  int64_t node_off;   // first global node
+  int64_t cell_off;   // first global cell ((nx-1)*(ny-1) per instance)
+  int32_t col_off;    // first global (natural and permuted) column
+  int32_t num_active;
+  int32_t num_frames;
+  int32_t frame_off;
+  int64_t pt_off;
+  int32_t num_points;
+  int64_t eik_off;
+  int32_t num_eik;
+  int64_t odom_off;
+  int32_t num_odom;
+  double huber_delta;
+  int32_t smooth_gradient;
+  double smooth_gradient_step;
+};
+
+/// Builds the supernodal symbolic factorization for a set of instances.
+Symbolic Analyze(const std::vector<HostProblem>& problems, const std::vector<InstanceLayout>& layout,
+                 int panel_width, int tile);
+
+/// Symbolic analysis of a general symmetric pattern (factor-only API): full
+/// CSC pattern, perm new->old (empty: natural order).
+Symbolic AnalyzeGeneral(int n, const int32_t* outer, const int32_t* inner,
+                        const std::vector<int32_t>& perm, int panel_width, int tile,
+                        std::vector<int64_t>& value_offsets);
+
+}  // namespace sdfgpu

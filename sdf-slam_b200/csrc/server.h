@@ -1,0 +1,75 @@
+// Serving loop with continuous batching. Each admitted request keeps its
+// state, symbolic analysis and factors resident on the device in its own
+// engine (own CUDA stream); every round enqueues one LM iteration of every
+// running request before waiting for any of them, so their kernels overlap
+// on the GPU. Requests are admitted while their estimated device footprint
+// fits the budget and retire as soon as their solve ends.
+#pragma once
+
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "engine.h"
+
+namespace sdfgpu {
+
+/// Device bytes an engine for `hp` will hold (state, specs, symbolic
+/// structure, fronts), from a host-side symbolic analysis.
+int64_t EstimateDeviceBytes(const HostProblem& hp);
+
+class Server {
+ public:
+  Server(int64_t budget_bytes, int max_batch);
+  ~Server();
+  Server(const Server&) = delete;
+  Server& operator=(const Server&) = delete;
+
+  int64_t Submit(HostProblem hp, const sdfgpu_solver_options& options);
+  void Poll(int64_t id, sdfgpu_solve_result* result, double* map_values, double* poses);
+  void Cancel(int64_t id);
+  void Stats(double* stats);
+  void Drain(int64_t timeout_ms);
+
+ private:
+  enum class State { kQueued, kRunning, kDone, kCancelled };
+  struct Request {
+    int64_t id{0};
+    HostProblem hp;
+    sdfgpu_solver_options options{};
+    int64_t bytes{0};
+    State state{State::kQueued};
+    std::chrono::steady_clock::time_point submitted;
+    std::unique_ptr<Engine> engine;
+    sdfgpu_solve_result result{};
+    std::vector<double> map_values;
+    std::vector<double> poses;
+  };
+  void Loop();
+  void Retire(Request& r);
+
+  int64_t budget_;
+  int max_batch_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::condition_variable done_cv_;
+  bool stop_{false};
+  std::deque<int64_t> queue_;
+  std::map<int64_t, std::unique_ptr<Request>> requests_;
+  std::vector<Request*> running_;
+  int64_t used_bytes_{0};
+  int64_t next_id_{1};
+  int64_t submitted_{0};
+  int64_t completed_{0};
+  int64_t iterations_{0};
+  std::vector<double> latencies_ms_;
+  std::chrono::steady_clock::time_point created_;
+  std::thread worker_;
+};
+
+}  // namespace sdfgpu

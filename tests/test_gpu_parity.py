@@ -1,0 +1,247 @@
+"""GPU parity tests: the CUDA LM path through the C ABI against the CPU oracle
+on the same input state.
+
+Tolerances (the contract of the FP64 path):
+* point-to-cell assignment, the Jacobian's and the normal matrix's sparsity
+  patterns: bit-exact;
+* Jacobian entries, residuals, J^T J, -J^T r: <= 1e-12 relative (the kernels
+  evaluate the reference's expressions unfused in its association order;
+  only the device cos/sin/atan2 may differ from glibc by an ulp);
+* the LM step delta: <= 1e-10 norm-wise relative (an independent FP64
+  factorization with a different elimination order);
+* full solves: cost history <= 1e-8 relative, poses <= 1e-4 m.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import oracle as O
+import sdf_slam_b200 as P
+import sdf_slam_b200.scenes as scenes
+from helpers import corner_setup, expect_recovered, oracle_from_specs, rel_err, scene_specs
+
+pytestmark = pytest.mark.gpu
+
+TOL_EVAL = 1e-12
+TOL_STEP = 1e-10
+
+
+def _warm_state(specs, iterations=3):
+    """A nontrivial identical input state: the oracle's state after a few
+    iterations from the scene's start."""
+    o = oracle_from_specs(specs)
+    o.solve(max_iterations=iterations, num_threads=4)
+    return o.state()
+
+
+def _compare_linearization(g, o):
+    assert np.array_equal(g["point_cell"], o["point_cell"]), "point-to-cell assignment"
+    assert np.array_equal(g["j_outer"], o["j_outer"]) and np.array_equal(g["j_inner"], o["j_inner"])
+    assert np.array_equal(g["n_outer"], o["n_outer"]) and np.array_equal(g["n_inner"], o["n_inner"])
+    assert rel_err(g["residuals"], o["residuals"]) <= TOL_EVAL
+    assert rel_err(g["j_values"], o["j_values"]) <= TOL_EVAL
+    assert rel_err(g["n_values"], o["n_values"]) <= TOL_EVAL
+    assert rel_err(g["rhs"], o["rhs"]) <= TOL_EVAL
+    assert rel_err(g["step"], o["step"]) <= TOL_STEP
+
+
+VARIANTS = {
+    "smooth_node": dict(),
+    "exact_gradient": dict(smooth_gradient=False),
+    "smooth_meters": dict(smooth_gradient_step=0.3),
+    "huber": dict(huber_delta=0.05),
+    "active_region": dict(active_region=True),
+}
+
+
+@pytest.mark.parametrize("variant", list(VARIANTS))
+def test_linearization_parity_room(variant):
+    sc = scenes.room_scene(seed=0)
+    opts = P.ProblemOptions(hallucination_points=4, **VARIANTS[variant])
+    specs, _ = scene_specs(sc, opts)
+    m, p = _warm_state(specs)
+    gpu = P.Problem.from_specs(specs)
+    gpu.set_state(m, p)
+    orc = oracle_from_specs(specs)
+    orc.set_state(m, p)
+    for lam, marq in [(1.0, False), (0.5, True)]:
+        g = gpu.linearize(lam, marq)
+        o = orc.linearize(lam, marq, 4, True)
+        _compare_linearization(g, o)
+
+
+def test_cost_and_apply_step_parity():
+    sc = scenes.room_scene(seed=3)
+    specs, _ = scene_specs(sc, P.ProblemOptions(hallucination_points=4))
+    m, p = _warm_state(specs, 2)
+    gpu = P.Problem.from_specs(specs)
+    orc = oracle_from_specs(specs)
+    gpu.set_state(m, p)
+    orc.set_state(m, p)
+    assert abs(gpu.cost() - orc.cost()) <= 1e-12 * orc.cost()
+    step = np.random.default_rng(0).normal(0, 1e-2, gpu.num_parameters())
+    gpu.apply_step(step)
+    orc.apply_step(step)
+    gm, gp = gpu.state()
+    om, op = orc.state()
+    assert np.array_equal(gm, om)
+    assert np.max(np.abs(gp - op)) <= 1e-15
+
+
+@pytest.mark.parametrize("options", [
+    dict(),
+    dict(trust_region=True),
+    dict(lambda_factor=2.0, reject_worse_steps=True),
+    dict(marquardt_scaling=True, lambda_init=0.1),
+])
+def test_solve_parity_room(options):
+    sc = scenes.room_scene(seed=0)
+    specs, _ = scene_specs(sc, P.ProblemOptions(hallucination_points=4))
+    gpu = P.Problem.from_specs(specs)
+    orc = oracle_from_specs(specs)
+    rg = P.solve(gpu, P.SolverOptions(max_iterations=10, **options))
+    ro = orc.solve(max_iterations=10, num_threads=4, **options)
+    assert rg.iterations == ro["iterations"]
+    assert rg.converged == ro["converged"]
+    hg = np.array(rg.cost_history)
+    ho = np.array(ro["cost_history"])
+    assert hg.shape == ho.shape
+    assert np.max(np.abs(hg - ho) / np.abs(ho)) <= 1e-8
+    gm, gp = gpu.state()
+    om, op = orc.state()
+    assert np.max(np.abs(gp[:, :2] - op[:, :2])) <= 1e-4
+    assert np.max(np.abs(gm - om)) <= 1e-4
+
+
+def test_solve_is_deterministic():
+    sc = scenes.room_scene(seed=2)
+    specs, _ = scene_specs(sc, P.ProblemOptions(hallucination_points=4))
+    outs = []
+    for _ in range(2):
+        gpu = P.Problem.from_specs(specs)
+        r = P.solve(gpu, P.SolverOptions(max_iterations=5))
+        outs.append((np.array(r.cost_history), *gpu.state()))
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("variant", ["lm", "relation", "trust_region", "huber", "active_region"])
+def test_e2e_corner_scan_gpu(variant):
+    """tests/test_e2e.cpp:90-218 with the GPU backend."""
+    s = corner_setup()
+    o = s["opts"]
+    if variant == "huber":
+        o.huber_delta = 0.5
+    if variant == "active_region":
+        o.active_region = True
+    rel, odo = [], [s["odo"]]
+    if variant == "relation":
+        rel, odo = [(0, 1, s["odo"], 1.0)], []
+    nx, ny, mn, mx = s["grid"]
+    prob = P.Problem(nx, ny, mn, mx, s["init"], s["scans"], odo, o, rel)
+    r = P.solve(prob, P.SolverOptions(max_iterations=40, trust_region=(variant == "trust_region")))
+    m, poses = prob.state()
+    expect_recovered(m, poses, s, r.initial_cost, r.final_cost, s["grid"])
+    if variant == "trust_region":
+        h = r.cost_history
+        assert all(h[i] <= h[i - 1] + 1e-9 for i in range(1, len(h)))
+
+
+def test_zero_pivot_raises_and_keeps_state():
+    """lambda = 0 leaves map nodes without residual rows with a zero pivot:
+    the reference throws "sparse Cholesky factorization failed" before it
+    applies the step (lm_solver.cpp:354-362)."""
+    sc = scenes.room_scene(seed=0)
+    specs, _ = scene_specs(sc, P.ProblemOptions(hallucination_points=4, weights_eikonal=0.0))
+    gpu = P.Problem.from_specs(specs)
+    before = gpu.state()
+    with pytest.raises(RuntimeError, match="sparse Cholesky factorization failed"):
+        P.solve(gpu, P.SolverOptions(max_iterations=3, lambda_init=0.0))
+    after = gpu.state()
+    assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
+
+
+def test_floorplan_full_size_linearization():
+    """The 76-pose / 100x100 workload at full size: bit-exact cells and
+    patterns, values and step within tolerance."""
+    sc = scenes.floorplan_scene(seed=1)
+    specs, _ = scene_specs(sc)
+    m, p = _warm_state(specs, 2)
+    gpu = P.Problem.from_specs(specs)
+    gpu.set_state(m, p)
+    orc = oracle_from_specs(specs)
+    orc.set_state(m, p)
+    _compare_linearization(gpu.linearize(1.0, False), orc.linearize(1.0, False, 0, True))
+
+
+def test_batch_matches_individual_solves():
+    scs = [scenes.room_scene(seed=s, grid=g, frames=f, beams=b, active_region=a)
+           for s, g, f, b, a in [(10, 40, 10, 180, False), (11, 56, 14, 120, True), (12, 48, 7, 90, False)]]
+    specs = [scene_specs(sc, P.ProblemOptions(hallucination_points=4, active_region=sc.options["active_region"]))[0]
+             for sc in scs]
+    batch = P.Problem.batch(specs)
+    opts = [P.SolverOptions(max_iterations=6), P.SolverOptions(max_iterations=4, trust_region=True),
+            P.SolverOptions(max_iterations=5)]
+    rb = P.solve(batch, opts)
+    for i, s in enumerate(specs):
+        single = P.Problem.from_specs(s)
+        r1 = P.solve(single, opts[i])
+        assert rb[i].cost_history == r1.cost_history
+        bm, bp = batch.state(i)
+        sm, sp = single.state()
+        assert np.array_equal(bm, sm) and np.array_equal(bp, sp)
+
+
+def test_server_results_equal_alone_and_in_mix():
+    scs = [scenes.request_scene(seed=100 + i, grid_range=(40, 70), pose_range=(8, 24), iterations=6)
+           for i in range(5)]
+    specs = [scene_specs(sc, P.ProblemOptions(hallucination_points=4))[0] for sc in scs]
+    server = P.Server(memory_budget_bytes=8 << 30, max_batch=3)
+    ids = [server.submit(s, P.SolverOptions(max_iterations=6)) for s in specs]
+    server.drain(300000)
+    for s, rid in zip(specs, ids):
+        res, m, p = server.poll(rid, nx_ny=s.nx * s.ny, num_frames=len(s.poses))
+        alone = P.Problem.from_specs(s)
+        ra = P.solve(alone, P.SolverOptions(max_iterations=6))
+        am, ap = alone.state()
+        assert res.status == 0
+        assert res.final_cost == ra.final_cost and res.iterations == ra.iterations
+        assert np.array_equal(m, am) and np.array_equal(p, ap)
+    st = server.stats()
+    assert st["completed"] == 5 and st["p99_ms"] >= st["p50_ms"] > 0
+    server.close()
+
+
+def _random_spd(n, width, seed):
+    from test_oracle_known_answers import random_spd
+    return random_spd(n, width, seed)
+
+
+@pytest.mark.parametrize("seed", [11, 12, 13])
+def test_ldlt_factor_only_matches_oracle(seed):
+    n = 3000 + 500 * seed // 11
+    outer, inner, vals = _random_spd(n, 57, seed)
+    b = np.random.default_rng(seed).uniform(-1, 1, n)
+    solver = P.LdltSolver(n, outer, inner)
+    solver.factorize(vals)
+    x = solver.solve(b)
+    xo, _ = O.ldlt_solve(n, outer, inner, vals, b, num_threads=4)
+    assert rel_err(x, xo) <= 1e-13
+    # refactorization with new values on the same pattern
+    diag = np.array([inner[p] == j for j in range(n) for p in range(outer[j], outer[j + 1])])
+    vals2 = vals + 2.5 * diag
+    solver.factorize(vals2)
+    x2 = solver.solve(b)
+    xo2, _ = O.ldlt_solve(n, outer, inner, vals2, b, num_threads=4)
+    assert rel_err(x2, xo2) <= 1e-13
+
+
+def test_ldlt_factor_only_singular():
+    n = 600
+    outer = np.arange(n + 1, dtype=np.int32)
+    inner = np.arange(n, dtype=np.int32)
+    vals = np.where(np.arange(n) == n // 2, 0.0, 2.0)
+    solver = P.LdltSolver(n, outer, inner)
+    with pytest.raises(RuntimeError, match="factorization failed"):
+        solver.factorize(vals)
