@@ -276,6 +276,24 @@ int sdfgpu_server_stats(sdfgpu_server* server, double* stats);
 int sdfgpu_server_drain(sdfgpu_server* server, int64_t timeout_ms);
 int sdfgpu_server_destroy(sdfgpu_server* server);
 
+/* ------------------------------------------------- allocation-free solve --
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory when they need a solve -- a host framework whose caching allocator
+ * already holds the device's free memory, or a real-time loop that allows no
+ * allocation after start-up: solves A x = b for a dense symmetric n x n
+ * matrix A (host arrays; A column major, only its lower triangle is read)
+ * with the library's LDL^T panel, update and triangular-solve kernels,
+ * keeping every intermediate in one file-scope device array of about 8.6 MB
+ * that each GPU loading the library holds until the process exits. Calls no
+ * cudaMalloc / cudaFree and creates no stream. n above SDFGPU_NOALLOC_MAX_N
+ * gives SDFGPU_ERR_INVALID_ARGUMENT; a zero pivot SDFGPU_ERR_NUMERICAL. The
+ * first call on a device looks the array's address up with that device
+ * current: make it before any stream capture. All calls share the array and
+ * it keeps the last call's contents; calls whose GPU work overlaps (from
+ * several host threads, for example) race and must be serialised. */
+#define SDFGPU_NOALLOC_MAX_N 1024
+int sdfgpu_dense_ldlt_solve_noalloc(int32_t n, const double* a, const double* b, double* x);
+
 #ifdef __cplusplus
 }
 #endif

@@ -122,6 +122,7 @@ SIGNATURES = {
     "sdfgpu_server_stats": (ctypes.c_int, [vp, c_dbl_p]),
     "sdfgpu_server_drain": (ctypes.c_int, [vp, ctypes.c_int64]),
     "sdfgpu_server_destroy": (ctypes.c_int, [vp]),
+    "sdfgpu_dense_ldlt_solve_noalloc": (ctypes.c_int, [ctypes.c_int32, c_dbl_p, c_dbl_p, c_dbl_p]),
 }
 
 _lib = None

@@ -28,6 +28,7 @@ SOURCES = {
     "factor.cu": [],
     "engine.cu": [],
     "ldlt.cu": [],
+    "noalloc.cu": [],
     "problem_build.cpp": ["-x", "cu"],
     "symbolic.cpp": ["-x", "cu"],
     "capi.cpp": ["-x", "cu"],

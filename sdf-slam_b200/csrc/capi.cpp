@@ -14,6 +14,10 @@
 #include "ldlt.h"
 #include "server.h"
 
+namespace sdfgpu {
+void DenseLdltSolveNoAlloc(int n, const double* a, const double* b, double* x);
+}  // namespace sdfgpu
+
 struct sdfgpu_problem {
   std::vector<sdfgpu::HostProblem> host;  // specs as given (state lives on the device once uploaded)
   std::unique_ptr<sdfgpu::Engine> engine;
@@ -461,6 +465,10 @@ int sdfgpu_server_drain(sdfgpu_server* server, int64_t timeout_ms) {
 
 int sdfgpu_server_destroy(sdfgpu_server* server) {
   return Guard([&] { delete server; });
+}
+
+int sdfgpu_dense_ldlt_solve_noalloc(int32_t n, const double* a, const double* b, double* x) {
+  return Guard([&] { sdfgpu::DenseLdltSolveNoAlloc(n, a, b, x); });
 }
 
 }  // extern "C"
