@@ -187,8 +187,30 @@ def cpu_reference_rate(specs, iterations, threads):
     return res["iterations"] / dt, res, dt
 
 
-def flush_l2(torch, buf):
-    buf.add_(1.0)
+class L2Flusher:
+    """Writes 2x the 126 MB L2 between timed steps (cuda-python runtime; no
+    torch in the process, so that ncu sees the library's kernels)."""
+
+    BYTES = 2 * 126 * 1000 * 1000
+
+    def __init__(self):
+        from cuda.bindings import runtime as rt
+        self.rt = rt
+        err, self.ptr = rt.cudaMalloc(self.BYTES)
+        if err != rt.cudaError_t.cudaSuccess:
+            raise RuntimeError(f"cudaMalloc for the L2 flush failed: {err}")
+        self.value = 0
+
+    def flush(self):
+        self.value = (self.value + 1) & 0xFF
+        self.rt.cudaMemset(self.ptr, self.value, self.BYTES)
+        self.sync()
+
+    def sync(self):
+        self.rt.cudaDeviceSynchronize()
+
+    def close(self):
+        self.rt.cudaFree(self.ptr)
 
 
 def run_reference(args, dist, rank):
@@ -217,40 +239,102 @@ def run_reference(args, dist, rank):
     return 0
 
 
+def run_batch(P, args, flusher):
+    """Uneven independent instances solved together in one engine (every
+    kernel of an iteration covers all of them): aggregate LM iterations/s."""
+    import sdf_slam_b200.scenes as scenes
+    scs = scenes.batch_scenes(seed=3, count=args.batch_count)
+    specs = []
+    for sc in scs:
+        opts = P.ProblemOptions(hallucination_points=4, active_region=sc.options["active_region"])
+        prob = P.Problem.from_scene(sc, opts)
+        specs.append(prob.specs(min_corner=sc.min_corner, max_corner=sc.max_corner))
+    batch = P.Problem.batch(specs)
+    count = len(specs)
+    opts1 = [P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=args.precision)] * count
+    for _ in range(2):
+        P.solve(batch, opts1)
+    device = 0.0
+    steps = max(3, args.steps // 2)
+    for _ in range(steps):
+        flusher.flush()
+        P.solve(batch, opts1)
+        device += batch.last_profile()["span"]
+    rows = sum(len(s.pt_frame) for s in specs)
+    return {"instances": count, "value": count * steps / device, "unit": "LM iters/s (all instances)",
+            "ms_per_batched_iteration": 1000.0 * device / steps, "point_rows": rows,
+            "workload": "uneven room-style instances, grid 40-150 @0.25 m, 10-200 poses, 90-360 beams, "
+                        "every other one active-region"}
+
+
+def run_serve(P, args):
+    """Poisson stream of solve requests through the serving loop: p50/p99
+    latency and throughput."""
+    import numpy as np
+    import sdf_slam_b200.scenes as scenes
+    rng = np.random.default_rng(7)
+    reqs = []
+    for i in range(args.serve_requests):
+        sc = scenes.request_scene(seed=500 + i, iterations=args.serve_iterations)
+        prob = P.Problem.from_scene(sc, P.ProblemOptions(hallucination_points=4))
+        reqs.append(prob.specs(min_corner=sc.min_corner, max_corner=sc.max_corner))
+    gaps = rng.exponential(1.0 / args.serve_rate, size=len(reqs))
+    server = P.Server(memory_budget_bytes=int(args.serve_budget_gb * (1 << 30)), max_batch=args.serve_batch)
+    opts = P.SolverOptions(max_iterations=args.serve_iterations, step_tolerance=0.0, precision=args.precision)
+    t0 = time.perf_counter()
+    ids = []
+    due = t0
+    for spec, gap in zip(reqs, gaps):
+        due += gap
+        now = time.perf_counter()
+        if due > now:
+            time.sleep(due - now)
+        ids.append(server.submit(spec, opts))
+    server.drain(600000)
+    wall = time.perf_counter() - t0
+    st = server.stats()
+    ok = 0
+    for spec, rid in zip(reqs, ids):
+        res, _, _ = server.poll(rid)
+        ok += int(res.status == 0)
+    server.close()
+    return {"requests": len(reqs), "completed_ok": ok, "rate_req_s": args.serve_rate,
+            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "throughput_req_s": len(reqs) / wall,
+            "lm_iters_s": st["iterations_per_s"], "iterations_per_request": args.serve_iterations,
+            "workload": "room-style requests, grid log-U[40,200] @0.25 m, 10-400 poses, 180 beams"}
+
+
 def run_gpu(args, dist, world, rank, local):
     import numpy as np
-    import torch
     P = _load_package()
     scene = make_scene(args.workload, args.seed + rank)
     specs = scene_specs(P, scene)
-    dev = torch.device("cuda", 0)
-    flush_buf = torch.empty(int(2 * 126e6 // 4), dtype=torch.float32, device=dev)
+    flusher = L2Flusher()
     opts1 = P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=args.precision)
     prob = P.Problem.from_specs(specs)
     # warm-up: upload, symbolic analysis, first iterations
     for _ in range(args.warmup):
         P.solve(prob, opts1)
-    torch.cuda.synchronize()
+    flusher.sync()
     _barrier(dist)
     sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) \
         if rank == 0 else None
     if sampler:
         sampler.start()
-    torch.cuda.synchronize()
+    flusher.sync()
     _barrier(dist)
     wall0 = time.perf_counter()
     device_s = 0.0
     launches = 0
     phases = np.zeros(5)
     for _ in range(args.steps):
-        flush_l2(torch, flush_buf)
-        torch.cuda.synchronize()
+        flusher.flush()
         P.solve(prob, opts1)
         prof = prob.last_profile()
         device_s += prof["span"]
         launches += prof["launches"]
         phases += [prof["assemble"], prof["normal"], prof["factor"], prof["solve"], prof["update"]]
-    torch.cuda.synchronize()
+    flusher.sync()
     _barrier(dist)
     wall = time.perf_counter() - wall0
     clocks = sampler.stop() if sampler else None
@@ -264,7 +348,7 @@ def run_gpu(args, dist, world, rank, local):
     e2e_t = 0.0
     d2h = 0
     for _ in range(args.e2e_steps):
-        torch.cuda.synchronize()
+        flusher.sync()
         t0 = time.perf_counter()
         p2 = P.Problem.from_specs(specs)
         r = P.solve(p2, P.SolverOptions(max_iterations=e2e_iters, step_tolerance=0.0, precision=args.precision))
@@ -272,6 +356,9 @@ def run_gpu(args, dist, world, rank, local):
         e2e_t += time.perf_counter() - t0
         d2h = m.nbytes + poses.nbytes + 8 * len(r.cost_history)
         p2.close()
+    batched = run_batch(P, args, flusher) if (args.batch_count > 0 and world == 1) else None
+    flusher.close()
+    served = run_serve(P, args) if (args.serve_requests > 0 and world == 1) else None
     e2e_t = _reduce_max(dist, e2e_t)
     e2e_value = world * args.e2e_steps * e2e_iters / e2e_t if e2e_t > 0 else 0.0
     if rank != 0:
@@ -324,6 +411,8 @@ def run_gpu(args, dist, world, rank, local):
         "e2e": {"value": e2e_value, "unit": "LM iters/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "iterations_per_step": e2e_iters},
         "clocks": clocks,
+        "batched": batched,
+        "served": served,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -342,6 +431,12 @@ def main():
     ap.add_argument("--e2e-iterations", type=int, default=10)
     ap.add_argument("--cpu-iterations", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-count", type=int, default=64)
+    ap.add_argument("--serve-requests", type=int, default=32)
+    ap.add_argument("--serve-rate", type=float, default=100.0)
+    ap.add_argument("--serve-iterations", type=int, default=20)
+    ap.add_argument("--serve-batch", type=int, default=16)
+    ap.add_argument("--serve-budget-gb", type=float, default=32.0)
     args = ap.parse_args()
     world, rank, local = _dist()
     if world > 1 and args.impl == "b200":

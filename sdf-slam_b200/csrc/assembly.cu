@@ -292,296 +292,360 @@ __global__ void KCellStart(const int32_t* keys, int64_t n, int64_t num_cells, in
 
 namespace {
 
-/// Adds rec[q'] * x into the stencil accumulators for the three other
-/// corners (and the node itself) of a point row whose cell sits at offset C
-/// (0: cell (w-1,h-1), 1: (w,h-1), 2: (w-1,h), 3: (w,h)) from node (w, h).
-template <int C>
-__device__ __forceinline__ void AccumulateCell(double* acc, const double* rec, double x, unsigned act) {
-  constexpr int q = 3 - C;
-  constexpr int jx = q & 1;
-  constexpr int jy = q >> 1;
+__device__ __forceinline__ double WarpSum(double v) {
+  // xor butterfly: every lane ends with the same, fixed-order sum
 #pragma unroll
-  for (int qq = 0; qq < 4; ++qq) {
-    const int dw = (qq & 1) - jx;
-    const int dh = (qq >> 1) - jy;
-    const int slot = (dh + 1) * 3 + (dw + 1);
-    if (act & (1u << slot)) {
-      acc[slot] = acc[slot] + rec[qq] * x;
+  for (int m = 16; m > 0; m >>= 1) {
+    v += __shfl_xor_sync(0xffffffffu, v, m);
+  }
+  return v;
+}
+
+/// Front offset of the J^T J entry between the cell corners a and b of a cell
+/// whose corner columns are col[], or -1 when one corner is constant.
+__device__ __forceinline__ int64_t PairOffset(const DeviceView& V, const int* col, int a, int b) {
+  if (col[a] < 0 || col[b] < 0) {
+    return -1;
+  }
+  const int dw = (b & 1) - (a & 1);
+  const int dh = (b >> 1) - (a >> 1);
+  const int64_t off = V.mm_off[static_cast<int64_t>(col[a]) * 9 + (dh + 1) * 3 + (dw + 1)];
+  if (off >= 0) {
+    return off;
+  }
+  return V.mm_off[static_cast<int64_t>(col[b]) * 9 + (1 - dh) * 3 + (1 - dw)];
+}
+
+/// Offset of (pose var (frame, 0), node column) in the front, or -1 when the
+/// frame is not in the node's analysed coupling set.
+__device__ __forceinline__ int64_t PoseOffset(const DeviceView& V, int col, int frame_local) {
+  int64_t lo = V.mp_ptr[col];
+  int64_t hi = V.mp_ptr[col + 1];
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (V.mp_frame[mid] < frame_local) {
+      lo = mid + 1;
+    } else {
+      hi = mid;
     }
   }
+  return (lo < V.mp_ptr[col + 1] && V.mp_frame[lo] == frame_local) ? V.mp_off[lo] : -1;
+}
+
+__device__ __forceinline__ int FindInstanceByCell(const DeviceView& V, int64_t cell) {
+  int lo = 0;
+  int hi = V.num_inst - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (V.inst[mid].cell_off <= cell) {
+      lo = mid;
+    } else {
+      hi = mid - 1;
+    }
+  }
+  return lo;
 }
 
 }  // namespace
 
-/// Column gather for every active map node j: J^T J entries (i, j) of the 9
-/// stencil neighbours and of the pose parameters of every frame whose points
-/// touch j, plus -J^T r at j, all summed in ascending row order. Point rows
-/// of the 4 cells around j are merged by row index; Eikonal rows follow
-/// (specs at (w,h-1), (w-1,h), (w,h) in spec order). Damping
-/// (lm_solver.cpp:321-330) is applied to the diagonal entry.
-__global__ void KNodeColumns(DeviceView V) {
-  const int col = blockIdx.x * blockDim.x + threadIdx.x;
-  if (col >= V.n) {
+/// One colour class of cells (cx % 2, cy % 2) = (pass & 1, pass >> 1): cells
+/// of one class share no node, so each adds its contributions to J^T J and
+/// J^T r with plain read-modify-writes. One warp per cell: the 4x4 map block
+/// and the corner gradients are lane-strided sums over the cell's point rows
+/// reduced by a fixed butterfly; the map-pose blocks are segmented sums over
+/// runs of rows of one frame (rows of a cell are sorted, so frames are
+/// contiguous); the cell's Eikonal row (spec at its lower-left node) follows.
+/// Passes run in a fixed order, so every entry is a deterministic sum.
+__global__ void KCellPass(DeviceView V, int pass) {
+  const int64_t cell = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (cell >= V.total_cells) {
     return;
   }
-  const int node = V.col_node[col];
-  if (node < 0) {
+  const int i = FindInstanceByCell(V, cell);
+  const InstDev& I = V.inst[i];
+  if (V.active[i] == 0) {
+    return;
+  }
+  const int cw = I.nx - 1;
+  const int local = static_cast<int>(cell - I.cell_off);
+  const int cx = local % cw;
+  const int cy = local / cw;
+  if ((cx & 1) != (pass & 1) || (cy & 1) != (pass >> 1)) {
+    return;
+  }
+  const int64_t n0 = I.node_off + static_cast<int64_t>(cy) * I.nx + cx;
+  int col[4];
+  col[0] = V.node_col[n0];
+  col[1] = V.node_col[n0 + 1];
+  col[2] = V.node_col[n0 + I.nx];
+  col[3] = V.node_col[n0 + I.nx + 1];
+  const int rb = V.cell_start[cell];
+  const int re = V.cell_start[cell + 1];
+  const int eik = V.eik_index[n0];
+  if (rb == re && eik < 0) {
+    return;
+  }
+  // One pass over the cell's rows in chunks of 32 (lane l takes rows
+  // rb + l + 32 t): the 4x4 map block and corner gradients accumulate per
+  // lane and are reduced by a fixed butterfly at the end; the map-pose
+  // blocks are segmented sums over runs of one frame inside each chunk. The
+  // next chunk's row indices are loaded ahead.
+  double mm[10];
+  double g[4];
+#pragma unroll
+  for (int q = 0; q < 10; ++q) {
+    mm[q] = 0.0;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    g[q] = 0.0;
+  }
+  bool overflow = false;
+  int k_next = (rb + lane < re) ? V.cell_rows[rb + lane] : -1;
+  for (int base = rb; base < re; base += 32) {
+    const int k = k_next;
+    const bool in = k >= 0;
+    k_next = (base + 32 + lane < re) ? V.cell_rows[base + 32 + lane] : -1;
+    int f = -1;
+    double J[4] = {0.0, 0.0, 0.0, 0.0};
+    double jp[3] = {0.0, 0.0, 0.0};
+    double r = 0.0;
+    if (in) {
+      const double2* r2 = reinterpret_cast<const double2*>(V.pt_rec + static_cast<int64_t>(k) * kPointRec);
+      const double2 a01 = r2[0];
+      const double2 a23 = r2[1];
+      const double2 p01 = r2[2];
+      const double2 p2r = r2[3];
+      J[0] = a01.x;
+      J[1] = a01.y;
+      J[2] = a23.x;
+      J[3] = a23.y;
+      jp[0] = p01.x;
+      jp[1] = p01.y;
+      jp[2] = p2r.x;
+      r = p2r.y;
+      f = V.pt_frame[k];
+      int q = 0;
+#pragma unroll
+      for (int aa = 0; aa < 4; ++aa) {
+#pragma unroll
+        for (int bb = aa; bb < 4; ++bb) {
+          mm[q] = mm[q] + J[aa] * J[bb];
+          ++q;
+        }
+        g[aa] = g[aa] + J[aa] * r;
+      }
+    }
+    double v[12];
+    const bool posed = in && (f - I.frame_off >= 1);
+#pragma unroll
+    for (int aa = 0; aa < 4; ++aa) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        v[3 * aa + c] = posed ? J[aa] * jp[c] : 0.0;
+      }
+    }
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int fu = __shfl_up_sync(0xffffffffu, f, d);
+#pragma unroll
+      for (int q = 0; q < 12; ++q) {
+        const double vu = __shfl_up_sync(0xffffffffu, v[q], d);
+        if (lane >= d && fu == f) {
+          v[q] = vu + v[q];
+        }
+      }
+    }
+    const int fn = __shfl_down_sync(0xffffffffu, f, 1);
+    const int p = base + lane;
+    const bool tail = in && (lane == 31 || p + 1 >= re || fn != f);
+    const int fl = f - I.frame_off;
+    if (tail && fl >= 1) {
+#pragma unroll
+      for (int aa = 0; aa < 4; ++aa) {
+        if (col[aa] >= 0) {
+          const int64_t off = PoseOffset(V, col[aa], fl);
+          if (off >= 0) {
+            V.fronts[off] += v[3 * aa];
+            V.fronts[off + 1] += v[3 * aa + 1];
+            V.fronts[off + 2] += v[3 * aa + 2];
+          } else {
+            overflow = true;
+          }
+        }
+      }
+    }
+    __syncwarp();
+  }
+#pragma unroll
+  for (int q = 0; q < 10; ++q) {
+    mm[q] = WarpSum(mm[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    g[q] = WarpSum(g[q]);
+  }
+  if (rb < re) {
+    // lanes 0..9 write the pairs, 10..13 the gradients
+    int q = 0;
+#pragma unroll
+    for (int aa = 0; aa < 4; ++aa) {
+#pragma unroll
+      for (int bb = aa; bb < 4; ++bb) {
+        if (lane == q) {
+          const int64_t off = PairOffset(V, col, aa, bb);
+          if (off >= 0) {
+            V.fronts[off] += mm[q];
+          }
+        }
+        ++q;
+      }
+    }
+#pragma unroll
+    for (int aa = 0; aa < 4; ++aa) {
+      if (lane == 10 + aa && col[aa] >= 0) {
+        V.rhs[col[aa]] += g[aa];
+      }
+    }
+  }
+  __syncwarp();
+  // the cell's Eikonal row: nodes (cx,cy), (cx+1,cy), (cx,cy+1) = corners 0, 1, 2
+  if (lane == 0 && eik >= 0) {
+    const double* r = V.eik_rec + static_cast<int64_t>(eik) * kEikRec;
+    const int corner[3] = {0, 1, 2};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+      for (int b = a; b < 3; ++b) {
+        const int64_t off = PairOffset(V, col, corner[a], corner[b]);
+        if (off >= 0) {
+          V.fronts[off] += r[a] * r[b];
+        }
+      }
+      V.rhs[col[corner[a]]] += r[a] * r[3];
+    }
+  }
+  if (overflow) {
+    atomicOr(V.status + i, kStatusPatternOverflow);
+  }
+}
+
+/// Same-frame pose blocks and the pose columns of J^T r: one block of 256
+/// threads per frame, thread-strided over the frame's point rows, a fixed
+/// butterfly per warp and a fixed order over warps, then the frame's odometry
+/// / relation rows in spec order.
+__global__ void __launch_bounds__(256) KPoseFrames(DeviceView V) {
+  __shared__ double part[8][9];
+  const int64_t f = blockIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int i = V.frame_inst[f];
+  const InstDev& I = V.inst[i];
+  const int fl = static_cast<int>(f) - I.frame_off;
+  if (fl < 1 || V.active[i] == 0) {
+    return;
+  }
+  double acc[9];
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    acc[q] = 0.0;
+  }
+  const int64_t rb = V.frame_rows_ptr[f];
+  const int64_t re = V.frame_rows_ptr[f + 1];
+#pragma unroll 2
+  for (int64_t q = rb + threadIdx.x; q < re; q += blockDim.x) {
+    const int k = V.frame_rows[q];
+    if (V.pt_cell[k] < 0) {
+      continue;
+    }
+    const double2* r2 = reinterpret_cast<const double2*>(V.pt_rec + static_cast<int64_t>(k) * kPointRec);
+    const double2 j01 = r2[2];
+    const double2 j2r = r2[3];
+    const double j0 = j01.x;
+    const double j1 = j01.y;
+    const double j2 = j2r.x;
+    const double r = j2r.y;
+    acc[0] = acc[0] + j0 * j0;
+    acc[1] = acc[1] + j1 * j0;
+    acc[2] = acc[2] + j2 * j0;
+    acc[3] = acc[3] + j1 * j1;
+    acc[4] = acc[4] + j2 * j1;
+    acc[5] = acc[5] + j2 * j2;
+    acc[6] = acc[6] + j0 * r;
+    acc[7] = acc[7] + j1 * r;
+    acc[8] = acc[8] + j2 * r;
+  }
+#pragma unroll
+  for (int q = 0; q < 9; ++q) {
+    acc[q] = WarpSum(acc[q]);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      part[warp][q] = acc[q];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) {
+    return;
+  }
+  for (int q = 0; q < 9; ++q) {
+    double v = part[0][q];
+    for (int w = 1; w < 8; ++w) {
+      v = v + part[w][q];
+    }
+    acc[q] = v;
+  }
+  const int aa[6] = {0, 1, 2, 1, 2, 2};
+  const int bb[6] = {0, 0, 0, 1, 1, 2};
+  for (int64_t q = V.frame_odom_ptr[f]; q < V.frame_odom_ptr[f + 1]; ++q) {
+    const int code = V.frame_odom[q];
+    const double* rec = V.odom_rec + static_cast<int64_t>(code >> 1) * kOdomRec;
+    const double* blk = rec + ((code & 1) ? 12 : 3);
+    for (int r = 0; r < 3; ++r) {
+      for (int e = 0; e < 6; ++e) {
+        acc[e] = acc[e] + blk[3 * r + aa[e]] * blk[3 * r + bb[e]];
+      }
+      for (int a = 0; a < 3; ++a) {
+        acc[6 + a] = acc[6 + a] + blk[3 * r + a] * rec[r];
+      }
+    }
+  }
+  const int base = I.pp_first + 3 * (fl - 1);
+  for (int e = 0; e < 6; ++e) {
+    V.fronts[I.pp_base + static_cast<int64_t>(base + bb[e]) * I.pp_ld + (base + aa[e])] = acc[e];
+  }
+  const int c0 = V.frame_col[f];
+  V.rhs[c0] = acc[6];
+  V.rhs[c0 + 1] = acc[7];
+  V.rhs[c0 + 2] = acc[8];
+}
+
+/// Turns the accumulated J^T r into -J^T r and applies the damping of
+/// lm_solver.cpp:321-330 to every diagonal entry (lambda, or lambda times
+/// max(diag, 1e-12) under Marquardt scaling).
+__global__ void KFinalizeNormal(DeviceView V) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= V.n) {
     return;
   }
   const int i = V.col_inst[col];
   if (V.active[i] == 0) {
     return;
   }
-  const InstDev& I = V.inst[i];
-  const int local = node - static_cast<int>(I.node_off);
-  const int w = local % I.nx;
-  const int h = local / I.nx;
-  unsigned act = 0;
-#pragma unroll
-  for (int slot = 0; slot < 9; ++slot) {
-    const int ww = w + slot % 3 - 1;
-    const int hh = h + slot / 3 - 1;
-    if (ww >= 0 && hh >= 0 && ww < I.nx && hh < I.ny && V.node_col[node + (slot / 3 - 1) * I.nx + (slot % 3 - 1)] >= 0) {
-      act |= 1u << slot;
-    }
-  }
-  const int cw = I.nx - 1;
-  const int ch = I.ny - 1;
-  int pos[4];
-  int end[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    const int cx = w - 1 + (c & 1);
-    const int cy = h - 1 + (c >> 1);
-    if (cx >= 0 && cy >= 0 && cx < cw && cy < ch) {
-      const int64_t cell = I.cell_off + static_cast<int64_t>(cy) * cw + cx;
-      pos[c] = V.cell_start[cell];
-      end[c] = V.cell_start[cell + 1];
-    } else {
-      pos[c] = 0;
-      end[c] = 0;
-    }
-  }
-  double acc[9];
-#pragma unroll
-  for (int q = 0; q < 9; ++q) {
-    acc[q] = -0.0;
-  }
-  double pacc[3] = {-0.0, -0.0, -0.0};
-  int cur_f = -1;
-  double tmp_a = 0.0;
-  double tmp_b = 0.0;
-  int parity = 0;
-  int64_t mpc = V.mp_ptr[col];
-  const int64_t mpe = V.mp_ptr[col + 1];
-  bool overflow = false;
-  auto flush = [&]() {
-    if (cur_f < 0) {
-      return;
-    }
-    const int fl = cur_f - I.frame_off;
-    while (mpc < mpe && V.mp_frame[mpc] < fl) {
-      ++mpc;
-    }
-    if (mpc < mpe && V.mp_frame[mpc] == fl) {
-      double* dst = V.fronts + V.mp_off[mpc];
-      dst[0] = pacc[0];
-      dst[1] = pacc[1];
-      dst[2] = pacc[2];
-    } else {
-      overflow = true;
-    }
-  };
-  int head[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    head[c] = pos[c] < end[c] ? V.cell_rows[pos[c]] : INT_MAX;
-  }
-  while (true) {
-    int best = 0;
-#pragma unroll
-    for (int c = 1; c < 4; ++c) {
-      if (head[c] < head[best]) {
-        best = c;
-      }
-    }
-    const int k = head[best];
-    if (k == INT_MAX) {
-      break;
-    }
-    ++pos[best];
-    head[best] = pos[best] < end[best] ? V.cell_rows[pos[best]] : INT_MAX;
-    const double* rec = V.pt_rec + static_cast<int64_t>(k) * kPointRec;
-    double rv[8];
-    const double2* r2 = reinterpret_cast<const double2*>(rec);
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const double2 t = r2[q];
-      rv[2 * q] = t.x;
-      rv[2 * q + 1] = t.y;
-    }
-    const double x = rv[3 - best];
-    switch (best) {
-      case 0:
-        AccumulateCell<0>(acc, rv, x, act);
-        break;
-      case 1:
-        AccumulateCell<1>(acc, rv, x, act);
-        break;
-      case 2:
-        AccumulateCell<2>(acc, rv, x, act);
-        break;
-      default:
-        AccumulateCell<3>(acc, rv, x, act);
-        break;
-    }
-    if (parity == 0) {
-      tmp_a += x * rv[7];
-    } else {
-      tmp_b += x * rv[7];
-    }
-    parity ^= 1;
-    const int f = V.pt_frame[k];
-    if (f - I.frame_off >= 1) {
-      if (f != cur_f) {
-        flush();
-        cur_f = f;
-        pacc[0] = -0.0;
-        pacc[1] = -0.0;
-        pacc[2] = -0.0;
-      }
-      pacc[0] = pacc[0] + rv[4] * x;
-      pacc[1] = pacc[1] + rv[5] * x;
-      pacc[2] = pacc[2] + rv[6] * x;
-    }
-  }
-  flush();
-  // Eikonal rows touching j: spec at (w,h-1) [j is its node 2], (w-1,h)
-  // [node 1], (w,h) [node 0]; slots of the spec's other nodes relative to j.
-  {
-    const int e0 = h >= 1 ? V.eik_index[node - I.nx] : -1;
-    const int e1 = w >= 1 ? V.eik_index[node - 1] : -1;
-    const int e2 = V.eik_index[node];
-    if (e0 >= 0) {
-      const double* r = V.eik_rec + static_cast<int64_t>(e0) * kEikRec;
-      const double x = r[2];
-      acc[1] = acc[1] + r[0] * x;
-      acc[2] = acc[2] + r[1] * x;
-      acc[4] = acc[4] + r[2] * x;
-      if (parity == 0) { tmp_a += x * r[3]; } else { tmp_b += x * r[3]; }
-      parity ^= 1;
-    }
-    if (e1 >= 0) {
-      const double* r = V.eik_rec + static_cast<int64_t>(e1) * kEikRec;
-      const double x = r[1];
-      acc[3] = acc[3] + r[0] * x;
-      acc[4] = acc[4] + r[1] * x;
-      acc[6] = acc[6] + r[2] * x;
-      if (parity == 0) { tmp_a += x * r[3]; } else { tmp_b += x * r[3]; }
-      parity ^= 1;
-    }
-    if (e2 >= 0) {
-      const double* r = V.eik_rec + static_cast<int64_t>(e2) * kEikRec;
-      const double x = r[0];
-      acc[4] = acc[4] + r[0] * x;
-      acc[5] = acc[5] + r[1] * x;
-      acc[7] = acc[7] + r[2] * x;
-      if (parity == 0) { tmp_a += x * r[3]; } else { tmp_b += x * r[3]; }
-      parity ^= 1;
-    }
-  }
-  const double lam = V.lam[i];
-  {
-    const double v = acc[4];
-    acc[4] = V.marquardt[i] != 0 ? v + lam * fmax(v, 1e-12) : v + lam;
-  }
-  const int64_t* mo = V.mm_off + static_cast<int64_t>(col) * 9;
-#pragma unroll
-  for (int slot = 0; slot < 9; ++slot) {
-    const int64_t off = mo[slot];
-    if (off >= 0) {
-      V.fronts[off] = acc[slot];
-    }
-  }
-  V.rhs[col] = -(tmp_a + tmp_b);
-  if (overflow) {
-    atomicOr(V.status + i, kStatusPatternOverflow);
-  }
-}
-
-/// Same-frame pose blocks (6 entries per frame) and -J^T r of the pose
-/// columns: point rows of the frame in ascending order, then its odometry /
-/// relation rows.
-__global__ void KPoseBlocks(DeviceView V) {
-  const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int f = static_cast<int>(t / 9);
-  const int e = static_cast<int>(t % 9);
-  if (f >= V.total_frames) {
-    return;
-  }
-  const int i = V.frame_inst[f];
-  const InstDev& I = V.inst[i];
-  const int fl = f - I.frame_off;
-  if (fl < 1 || V.active[i] == 0) {
-    return;
-  }
-  const int64_t rb = V.frame_rows_ptr[f];
-  const int64_t re = V.frame_rows_ptr[f + 1];
-  const int64_t ob = V.frame_odom_ptr[f];
-  const int64_t oe = V.frame_odom_ptr[f + 1];
-  if (e < 6) {
-    const int aa[6] = {0, 1, 2, 1, 2, 2};
-    const int bb[6] = {0, 0, 0, 1, 1, 2};
-    const int a = aa[e];
-    const int b = bb[e];
-    double acc = -0.0;
-    for (int64_t q = rb; q < re; ++q) {
-      const int k = V.frame_rows[q];
-      if (V.pt_cell[k] < 0) {
-        continue;
-      }
-      const double* rec = V.pt_rec + static_cast<int64_t>(k) * kPointRec;
-      acc = acc + rec[4 + a] * rec[4 + b];
-    }
-    for (int64_t q = ob; q < oe; ++q) {
-      const int code = V.frame_odom[q];
-      const double* rec = V.odom_rec + static_cast<int64_t>(code >> 1) * kOdomRec;
-      const double* blk = rec + ((code & 1) ? 12 : 3);
-      for (int r = 0; r < 3; ++r) {
-        acc = acc + blk[3 * r + a] * blk[3 * r + b];
-      }
-    }
-    if (a == b) {
-      const double lam = V.lam[i];
-      acc = V.marquardt[i] != 0 ? acc + lam * fmax(acc, 1e-12) : acc + lam;
-    }
-    const int base = I.pp_first + 3 * (fl - 1);
-    V.fronts[I.pp_base + static_cast<int64_t>(base + b) * I.pp_ld + (base + a)] = acc;
+  V.rhs[col] = -V.rhs[col];
+  int64_t off;
+  if (V.col_node[col] >= 0) {
+    off = V.mm_off[static_cast<int64_t>(col) * 9 + 4];
   } else {
-    const int a = e - 6;
-    double tmp_a = 0.0;
-    double tmp_b = 0.0;
-    int parity = 0;
-    for (int64_t q = rb; q < re; ++q) {
-      const int k = V.frame_rows[q];
-      if (V.pt_cell[k] < 0) {
-        continue;
-      }
-      const double* rec = V.pt_rec + static_cast<int64_t>(k) * kPointRec;
-      if (parity == 0) { tmp_a += rec[4 + a] * rec[7]; } else { tmp_b += rec[4 + a] * rec[7]; }
-      parity ^= 1;
-    }
-    for (int64_t q = ob; q < oe; ++q) {
-      const int code = V.frame_odom[q];
-      const double* rec = V.odom_rec + static_cast<int64_t>(code >> 1) * kOdomRec;
-      const double* blk = rec + ((code & 1) ? 12 : 3);
-      for (int r = 0; r < 3; ++r) {
-        if (parity == 0) { tmp_a += blk[3 * r + a] * rec[r]; } else { tmp_b += blk[3 * r + a] * rec[r]; }
-        parity ^= 1;
-      }
-    }
-    V.rhs[V.frame_col[f] + a] = -(tmp_a + tmp_b);
+    const InstDev& I = V.inst[i];
+    const int rel = I.pp_first + (col - I.col_off - I.num_active);
+    off = I.pp_base + static_cast<int64_t>(rel) * I.pp_ld + rel;
   }
+  const double d = V.fronts[off];
+  const double lam = V.lam[i];
+  V.fronts[off] = V.marquardt[i] != 0 ? d + lam * fmax(d, 1e-12) : d + lam;
 }
 
 /// Cross-frame pose blocks of frame pairs linked by odometry / relation rows.
@@ -749,14 +813,23 @@ __global__ void KStepTerms(DeviceView V, double* sq, double* pred) {
   pred[col] = d * (V.lam[V.col_inst[col]] * d + V.rhs[col]);
 }
 
-/// Deterministic segmented sum: block b sums seg_begin[b]..seg_end[b] with a
-/// fixed per-thread stride and a fixed tree.
-__global__ void KSegmentSum(const double* x, const int64_t* seg_begin, const int64_t* seg_end, double* out) {
+/// Deterministic segmented sum, first level: block (seg, part) sums the
+/// part-th of kSegParts equal slices of segment seg with a fixed per-thread
+/// stride and a fixed tree.
+constexpr int kSegParts = 32;
+
+__global__ void __launch_bounds__(256) KSegmentPartial(const double* x, const int64_t* seg_begin,
+                                                       const int64_t* seg_end, double* partial) {
   __shared__ double red[256];
-  const int64_t b = seg_begin[blockIdx.x];
-  const int64_t e = seg_end[blockIdx.x];
+  const int seg = blockIdx.x / kSegParts;
+  const int part = blockIdx.x % kSegParts;
+  const int64_t b = seg_begin[seg];
+  const int64_t e = seg_end[seg];
+  const int64_t len = (e - b + kSegParts - 1) / kSegParts;
+  const int64_t pb = b + part * len;
+  const int64_t pe = min(e, pb + len);
   double s = 0.0;
-  for (int64_t q = b + threadIdx.x; q < e; q += blockDim.x) {
+  for (int64_t q = pb + threadIdx.x; q < pe; q += blockDim.x) {
     s += x[q];
   }
   red[threadIdx.x] = s;
@@ -768,7 +841,21 @@ __global__ void KSegmentSum(const double* x, const int64_t* seg_begin, const int
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    out[blockIdx.x] = red[0];
+    partial[blockIdx.x] = red[0];
+  }
+}
+
+/// Second level: one warp per segment adds its kSegParts partials with a
+/// fixed butterfly.
+__global__ void KSegmentFinal(const double* partial, int num_segments, double* out) {
+  const int seg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (seg >= num_segments) {
+    return;
+  }
+  const double v = WarpSum(partial[static_cast<int64_t>(seg) * kSegParts + lane]);
+  if (lane == 0) {
+    out[seg] = v;
   }
 }
 

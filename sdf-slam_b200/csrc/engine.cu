@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <utility>
@@ -15,14 +16,16 @@ __global__ void KPointRows(DeviceView V);
 __global__ void KEikonalRows(DeviceView V);
 __global__ void KOdomRows(DeviceView V);
 __global__ void KCellStart(const int32_t* keys, int64_t n, int64_t num_cells, int32_t* cell_start);
-__global__ void KNodeColumns(DeviceView V);
-__global__ void KPoseBlocks(DeviceView V);
+__global__ void KCellPass(DeviceView V, int pass);
+__global__ void KPoseFrames(DeviceView V);
+__global__ void KFinalizeNormal(DeviceView V);
 __global__ void KPosePairs(DeviceView V);
 __global__ void KBackup(DeviceView V, int dir, const int32_t* revert_mask);
 __global__ void KApplyStep(DeviceView V);
 __global__ void KCostTerms(DeviceView V, double* terms);
 __global__ void KStepTerms(DeviceView V, double* sq, double* pred);
-__global__ void KSegmentSum(const double* x, const int64_t* seg_begin, const int64_t* seg_end, double* out);
+__global__ void KSegmentPartial(const double* x, const int64_t* seg_begin, const int64_t* seg_end, double* partial);
+__global__ void KSegmentFinal(const double* partial, int num_segments, double* out);
 void LaunchCellSort(const int32_t* pt_cell, int64_t n, int64_t num_cells, int32_t* keys_a, int32_t* vals_a,
                     int32_t* keys_b, int32_t* vals_b, int32_t* hist, cudaStream_t stream, bool* result_in_a);
 
@@ -69,12 +72,29 @@ Engine::Engine(std::vector<HostProblem> problems) : host_(std::move(problems)) {
   for (auto& e : span_) {
     CudaCheck(cudaEventCreate(&e), "cudaEventCreate");
   }
+  const char* ng = std::getenv("SDFGPU_NO_GRAPH");
+  use_graph_ = !(ng != nullptr && ng[0] == '1');
   BuildLayout();
+  h_active_.Alloc(host_.size());
+  h_marq_.Alloc(host_.size());
+  h_lam_.Alloc(host_.size());
+  h_seg_.Alloc(5 * host_.size());
+  h_status_.Alloc(host_.size());
   UploadProblem();
   Analyze();
 }
 
+void Engine::DropGraph() {
+  for (auto& g : graph_exec_) {
+    if (g != nullptr) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  }
+}
+
 Engine::~Engine() {
+  DropGraph();
   if (stream_ != nullptr) {
     cudaStreamSynchronize(stream_);
     cudaStreamDestroy(stream_);
@@ -305,6 +325,7 @@ void Engine::UploadProblem() {
   sq_terms_.Alloc(static_cast<size_t>(n_));
   pred_terms_.Alloc(static_cast<size_t>(n_));
   seg_out_.Alloc(5 * I);
+  seg_partial_.Alloc(32 * 3 * I);
   std::vector<int64_t> sb;
   std::vector<int64_t> se;
   for (size_t i = 0; i < I; ++i) {
@@ -337,6 +358,7 @@ void Engine::UploadProblem() {
 }
 
 void Engine::Analyze() {
+  DropGraph();
   sym_ = sdfgpu::Analyze(host_, layout_, 32, 64);
   cudaStream_t s = stream_;
   perm_.Upload(sym_.perm, s);
@@ -354,6 +376,7 @@ void Engine::Analyze() {
   ea_tasks_.Upload(sym_.ea_tasks, s);
   panel_tasks_.Upload(sym_.panel_tasks, s);
   update_tasks_.Upload(sym_.update_tasks, s);
+  small_tasks_.Upload(sym_.small_tasks, s);
   fronts_.Alloc(static_cast<size_t>(sym_.front_doubles));
   upd_.Alloc(static_cast<size_t>(std::max<int64_t>(1, sym_.update_doubles)));
   max_front_ = 1;
@@ -472,16 +495,22 @@ void Engine::RefreshView() {
 }
 
 void Engine::SetActive(const std::vector<int32_t>& active) {
-  CudaCheck(cudaMemcpyAsync(active_.get(), active.data(), active.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+  // the pinned buffer may still feed an enqueued copy
+  CudaCheck(cudaStreamSynchronize(stream_), "active sync");
+  std::copy(active.begin(), active.end(), h_active_.get());
+  CudaCheck(cudaMemcpyAsync(active_.get(), h_active_.get(), active.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
                             stream_),
             "active");
 }
 
 void Engine::SetLambda(const std::vector<double>& lam, const std::vector<int32_t>& marquardt) {
-  CudaCheck(cudaMemcpyAsync(lam_.get(), lam.data(), lam.size() * sizeof(double), cudaMemcpyHostToDevice, stream_),
+  CudaCheck(cudaStreamSynchronize(stream_), "lambda sync");
+  std::copy(lam.begin(), lam.end(), h_lam_.get());
+  std::copy(marquardt.begin(), marquardt.end(), h_marq_.get());
+  CudaCheck(cudaMemcpyAsync(lam_.get(), h_lam_.get(), lam.size() * sizeof(double), cudaMemcpyHostToDevice, stream_),
             "lambda");
-  CudaCheck(cudaMemcpyAsync(marq_.get(), marquardt.data(), marquardt.size() * sizeof(int32_t),
-                            cudaMemcpyHostToDevice, stream_),
+  CudaCheck(cudaMemcpyAsync(marq_.get(), h_marq_.get(), marquardt.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                            stream_),
             "marquardt");
 }
 
@@ -529,19 +558,35 @@ void Engine::LaunchRows() {
 void Engine::LaunchNormal() {
   CudaCheck(cudaMemsetAsync(fronts_.get(), 0, static_cast<size_t>(sym_.front_doubles) * sizeof(double), stream_),
             "front memset");
-  if (n_ > 0) {
-    KNodeColumns<<<Blocks(n_, 128), 128, 0, stream_>>>(V_);
+  CudaCheck(cudaMemsetAsync(rhs_.get(), 0, static_cast<size_t>(n_) * sizeof(double), stream_), "rhs memset");
+  if (total_cells_ > 0) {
+    for (int pass = 0; pass < 4; ++pass) {
+      KCellPass<<<Blocks(total_cells_ * 32, 256), 256, 0, stream_>>>(V_, pass);
+    }
   }
-  KPoseBlocks<<<Blocks(static_cast<int64_t>(total_frames_) * 9, 128), 128, 0, stream_>>>(V_);
+  KPoseFrames<<<static_cast<unsigned>(total_frames_), 256, 0, stream_>>>(V_);
   if (num_pairs_ > 0) {
     KPosePairs<<<Blocks(static_cast<int64_t>(num_pairs_) * 9, 128), 128, 0, stream_>>>(V_);
   }
+  if (n_ > 0) {
+    KFinalizeNormal<<<Blocks(n_, 256), 256, 0, stream_>>>(V_);
+  }
   CudaCheck(cudaGetLastError(), "normal kernels");
-  times_.launches += 2 + (num_pairs_ > 0 ? 1 : 0);
+  times_.launches += (total_cells_ > 0 ? 4 : 0) + 1 + (num_pairs_ > 0 ? 1 : 0) + (n_ > 0 ? 1 : 0);
+}
+
+void Engine::SegmentSum(const double* x, const int64_t* seg_begin, const int64_t* seg_end, int segments,
+                        double* out) {
+  KSegmentPartial<<<static_cast<unsigned>(segments * 32), 256, 0, stream_>>>(x, seg_begin, seg_end,
+                                                                            seg_partial_.get());
+  KSegmentFinal<<<Blocks(static_cast<int64_t>(segments) * 32, 128), 128, 0, stream_>>>(seg_partial_.get(), segments,
+                                                                                      out);
+  times_.launches += 2;
 }
 
 FactorPlan Engine::Plan() {
   FactorPlan P;
+  P.small_tasks = small_tasks_.get();
   P.ea_tasks = ea_tasks_.get();
   P.panel_tasks = panel_tasks_.get();
   P.update_tasks = update_tasks_.get();
@@ -561,8 +606,7 @@ void Engine::LaunchCost(std::vector<double>& cost) {
     KCostTerms<<<Blocks(terms, 128), 128, 0, stream_>>>(V_, terms_.get());
   }
   const size_t I = host_.size();
-  KSegmentSum<<<static_cast<unsigned>(3 * I), 256, 0, stream_>>>(terms_.get(), seg_begin_.get(), seg_end_.get(),
-                                                                   seg_out_.get());
+  SegmentSum(terms_.get(), seg_begin_.get(), seg_end_.get(), static_cast<int>(3 * I), seg_out_.get());
   std::vector<double> out(3 * I);
   CudaCheck(cudaMemcpyAsync(out.data(), seg_out_.get(), out.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_),
             "cost");
@@ -583,17 +627,15 @@ void Engine::LaunchStepAndCost(bool backup) {
     KStepTerms<<<Blocks(n_, 256), 256, 0, stream_>>>(V_, sq_terms_.get(), pred_terms_.get());
   }
   const size_t I = host_.size();
-  KSegmentSum<<<static_cast<unsigned>(I), 256, 0, stream_>>>(sq_terms_.get(), step_seg_begin_.get(),
-                                                              step_seg_end_.get(), seg_out_.get() + 3 * I);
-  KSegmentSum<<<static_cast<unsigned>(I), 256, 0, stream_>>>(pred_terms_.get(), step_seg_begin_.get(),
-                                                              step_seg_end_.get(), seg_out_.get() + 4 * I);
+  SegmentSum(sq_terms_.get(), step_seg_begin_.get(), step_seg_end_.get(), static_cast<int>(I), seg_out_.get() + 3 * I);
+  SegmentSum(pred_terms_.get(), step_seg_begin_.get(), step_seg_end_.get(), static_cast<int>(I),
+             seg_out_.get() + 4 * I);
   const int64_t terms = total_points_ + total_eik_ + total_odom_;
   if (terms > 0) {
     KCostTerms<<<Blocks(terms, 128), 128, 0, stream_>>>(V_, terms_.get());
   }
-  KSegmentSum<<<static_cast<unsigned>(3 * I), 256, 0, stream_>>>(terms_.get(), seg_begin_.get(), seg_end_.get(),
-                                                                   seg_out_.get());
-  times_.launches += (backup ? 1 : 0) + 5 + (terms > 0 ? 1 : 0);
+  SegmentSum(terms_.get(), seg_begin_.get(), seg_end_.get(), static_cast<int>(3 * I), seg_out_.get());
+  times_.launches += (backup ? 1 : 0) + (n_ > 0 ? 2 : 0) + (terms > 0 ? 1 : 0);
   CudaCheck(cudaMemcpyAsync(h_seg_.get(), seg_out_.get(), 5 * I * sizeof(double), cudaMemcpyDeviceToHost, stream_),
             "step terms");
   CudaCheck(cudaMemcpyAsync(h_status_.get(), status_.get(), I * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_),
@@ -631,9 +673,9 @@ int Engine::AssembleWithPattern() {
     }
     if (!overflow) {
       float ms = 0.0f;
-      cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+      CudaCheck(cudaEventElapsedTime(&ms, ev_[0], ev_[1]), "phase timing");
       times_.assemble += ms * 1e-3;
-      cudaEventElapsedTime(&ms, ev_[1], ev_[2]);
+      CudaCheck(cudaEventElapsedTime(&ms, ev_[1], ev_[2]), "phase timing");
       times_.normal += ms * 1e-3;
       return 0;
     }
@@ -953,38 +995,89 @@ bool Engine::SolveDone() const {
   return true;
 }
 
+void Engine::EnqueuePhase(int phase) {
+  switch (phase) {
+    case 0: {
+      const size_t I = host_.size();
+      CudaCheck(cudaMemcpyAsync(active_.get(), h_active_.get(), I * sizeof(int32_t), cudaMemcpyHostToDevice, stream_),
+                "active");
+      CudaCheck(cudaMemcpyAsync(lam_.get(), h_lam_.get(), I * sizeof(double), cudaMemcpyHostToDevice, stream_),
+                "lambda");
+      CudaCheck(cudaMemcpyAsync(marq_.get(), h_marq_.get(), I * sizeof(int32_t), cudaMemcpyHostToDevice, stream_),
+                "marquardt");
+      ClearStatus();
+      LaunchRows();
+      break;
+    }
+    case 1:
+      LaunchNormal();
+      break;
+    case 2:
+      LaunchFactor();
+      break;
+    case 3:
+      LaunchSolve();
+      break;
+    default:
+      LaunchStepAndCost(need_backup_);
+      break;
+  }
+}
+
 void Engine::LaunchIteration() {
   const size_t I = host_.size();
-  std::vector<int32_t> active(I);
-  std::vector<double> lam(I);
-  std::vector<int32_t> marq(I);
+  // the previous iteration (and any copy reading the pinned parameters) has
+  // finished: FinishIteration synchronised the stream
   for (size_t i = 0; i < I; ++i) {
     LmInst& L = lm_[i];
     if (L.active != 0 && iter_ >= L.opt.max_iterations) {
       L.active = 0;
     }
-    active[i] = L.active;
-    lam[i] = L.lam;
-    marq[i] = L.opt.marquardt_scaling != 0 ? 1 : 0;
+    h_active_[i] = L.active;
+    h_lam_[i] = L.lam;
+    h_marq_[i] = L.opt.marquardt_scaling != 0 ? 1 : 0;
   }
-  SetActive(active);
-  SetLambda(lam, marq);
-  ClearStatus();
   if (!span_started_) {
     CudaCheck(cudaEventRecord(span_[0], stream_), "event");
     span_started_ = true;
   }
-  CudaCheck(cudaEventRecord(ev_[0], stream_), "event");
-  LaunchRows();
-  CudaCheck(cudaEventRecord(ev_[1], stream_), "event");
-  LaunchNormal();
-  CudaCheck(cudaEventRecord(ev_[2], stream_), "event");
-  LaunchFactor();
-  CudaCheck(cudaEventRecord(ev_[3], stream_), "event");
-  LaunchSolve();
-  CudaCheck(cudaEventRecord(ev_[4], stream_), "event");
-  LaunchStepAndCost(need_backup_);
+  if (use_graph_ && (graph_exec_[0] == nullptr || graph_backup_ != need_backup_)) {
+    DropGraph();
+    const int64_t before = times_.launches;
+    for (int phase = 0; phase < 5; ++phase) {
+      cudaGraph_t graph = nullptr;
+      CudaCheck(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+      try {
+        EnqueuePhase(phase);
+      } catch (...) {
+        cudaStreamEndCapture(stream_, &graph);
+        if (graph != nullptr) {
+          cudaGraphDestroy(graph);
+        }
+        DropGraph();
+        throw;
+      }
+      CudaCheck(cudaStreamEndCapture(stream_, &graph), "end capture");
+      const cudaError_t e = cudaGraphInstantiate(&graph_exec_[phase], graph, 0);
+      cudaGraphDestroy(graph);
+      CudaCheck(e, "graph instantiate");
+    }
+    graph_launches_ = times_.launches - before;
+    times_.launches = before;
+    graph_backup_ = need_backup_;
+  }
+  for (int phase = 0; phase < 5; ++phase) {
+    CudaCheck(cudaEventRecord(ev_[phase], stream_), "event");
+    if (use_graph_) {
+      CudaCheck(cudaGraphLaunch(graph_exec_[phase], stream_), "graph launch");
+    } else {
+      EnqueuePhase(phase);
+    }
+  }
   CudaCheck(cudaEventRecord(ev_[5], stream_), "event");
+  if (use_graph_) {
+    times_.launches += graph_launches_;
+  }
 }
 
 void Engine::FinishIteration() {
@@ -1009,7 +1102,7 @@ void Engine::FinishIteration() {
   float ms = 0.0f;
   double* acc[5] = {&times_.assemble, &times_.normal, &times_.factor, &times_.solve, &times_.update};
   for (int q = 0; q < 5; ++q) {
-    cudaEventElapsedTime(&ms, ev_[q], ev_[q + 1]);
+    CudaCheck(cudaEventElapsedTime(&ms, ev_[q], ev_[q + 1]), "phase timing");
     *acc[q] += ms * 1e-3;
   }
   ++times_.iterations;

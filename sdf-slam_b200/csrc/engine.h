@@ -69,6 +69,7 @@ class DevBuf {
 /// Device task lists of a symbolic analysis plus the launch parameters of
 /// the factorization and solve kernels.
 struct FactorPlan {
+  const int32_t* small_tasks{nullptr};
   const int32_t* ea_tasks{nullptr};
   const int32_t* panel_tasks{nullptr};
   const int32_t* update_tasks{nullptr};
@@ -189,6 +190,7 @@ class Engine {
   void Reanalyze();
   int AssembleWithPattern();
   [[nodiscard]] FactorPlan Plan();
+  void SegmentSum(const double* x, const int64_t* seg_begin, const int64_t* seg_end, int segments, double* out);
 
   std::vector<HostProblem> host_;
   std::vector<InstanceLayout> layout_;
@@ -230,7 +232,7 @@ class Engine {
   DevBuf<int32_t> pt_cell_, cell_start_, sort_keys_a_, sort_vals_a_, sort_keys_b_, sort_vals_b_, sort_hist_;
   DevBuf<double> rhs_, step_, xs_, lam_, dvec_;
   DevBuf<int32_t> marq_, status_, active_, revert_;
-  DevBuf<double> terms_, sq_terms_, pred_terms_, seg_out_;
+  DevBuf<double> terms_, sq_terms_, pred_terms_, seg_out_, seg_partial_;
   DevBuf<int64_t> seg_begin_, seg_end_, step_seg_begin_, step_seg_end_;
   // symbolic buffers
   DevBuf<int32_t> perm_, pinv_, sn_rows_, sn_rel_, child_list_, level_sn_;
@@ -238,11 +240,22 @@ class Engine {
   DevBuf<int64_t> mm_off_, mp_ptr_, mp_off_;
   DevBuf<int32_t> mp_frame_;
   DevBuf<uint32_t> allow_bits_;
-  DevBuf<int32_t> ea_tasks_, panel_tasks_, update_tasks_;
+  DevBuf<int32_t> ea_tasks_, panel_tasks_, update_tasks_, small_tasks_;
   DevBuf<double> fronts_, upd_;
   int32_t* cell_rows_ptr_{nullptr};
   HostBuf<double> h_seg_;      // 5 per instance: cost parts x3, |delta|^2, prediction
   HostBuf<int32_t> h_status_;
+  HostBuf<int32_t> h_active_;  // per-iteration parameters read by the graph's copies
+  HostBuf<int32_t> h_marq_;
+  HostBuf<double> h_lam_;
+  // CUDA graphs of one LM iteration, one per phase (fixed per symbolic
+  // analysis); the phase events are recorded between the graph launches
+  cudaGraphExec_t graph_exec_[5]{};
+  bool graph_backup_{false};
+  bool use_graph_{true};
+  int64_t graph_launches_{0};
+  void EnqueuePhase(int phase);
+  void DropGraph();
 
   // LM control state of the current solve (lm_solver.cpp:201-434)
   struct LmInst {

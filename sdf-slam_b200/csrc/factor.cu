@@ -69,10 +69,13 @@ __global__ void KExtendAdd(DeviceView V, const int32_t* tasks) {
     }
     const int cend = lo;
     const double* U = V.fronts + C.front_off + static_cast<int64_t>(C.ncols) * C.F + C.ncols;
-    for (int cc = cbeg; cc < cend; ++cc) {
-      double* dst = Fp + static_cast<int64_t>(rel[cc]) * P.F;
-      const double* src = U + static_cast<int64_t>(cc) * C.F;
-      for (int r = cc + threadIdx.x; r < m; r += blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = blockDim.x >> 5;
+    for (int cc = cbeg + (threadIdx.x >> 5); cc < cend; cc += nwarps) {
+      double* __restrict__ dst = Fp + static_cast<int64_t>(rel[cc]) * P.F;
+      const double* __restrict__ src = U + static_cast<int64_t>(cc) * C.F;
+#pragma unroll 4
+      for (int r = cc + lane; r < m; r += 32) {
         dst[rel[r]] += src[r];
       }
     }
@@ -168,6 +171,171 @@ __global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const
     for (int j = 0; j < kPanel; ++j) {
       if (j < w) {
         Fs[static_cast<int64_t>(c0 + j) * F + r] = y[j] / D[j][j];
+      }
+    }
+  }
+}
+
+/// Pivot block of a front with at most kSmallPivots columns, factored in
+/// one block: blocked LDL^T of the k x k pivot block in shared memory (warp 0
+/// factors each 32-wide diagonal block, all threads solve the rows below it
+/// inside the pivot block and apply the rank-32 update), then the rows below
+/// the pivot block, `row_begin` onwards, get L(r, :) = A(r, :) L11^-T D^-1,
+/// panel by panel, in registers. Every block of a front repeats the pivot
+/// factorization; the one with row_begin == k writes L11 (the transposed
+/// storage of LoadL) and D.
+constexpr int kSmallPivots = 128;
+constexpr int kFrontRows = 256;
+
+__global__ void __launch_bounds__(256) KFactorFront(DeviceView V, const int32_t* tasks, double* dvec) {
+  extern __shared__ double sm[];
+  const int32_t* t = tasks + 2 * static_cast<int64_t>(blockIdx.x);
+  const int s = t[0];
+  const int row_begin = t[1];
+  const SupernodeRec S = V.sn[s];
+  if (V.active[S.instance] == 0) {
+    return;
+  }
+  const int k = S.ncols;
+  const int F = S.F;
+  const int ld = k + 1;
+  double* D = sm;  // D[r * ld + c], lower triangle of the pivot block
+  double* Fs = V.fronts + S.front_off;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  for (int idx = tid; idx < k * k; idx += blockDim.x) {
+    const int r = idx % k;
+    const int c = idx / k;
+    if (r >= c) {
+      D[r * ld + c] = Fs[static_cast<int64_t>(c) * F + r];
+    }
+  }
+  __syncthreads();
+  bool zero_pivot = false;
+  for (int p0 = 0; p0 < k; p0 += kPanel) {
+    const int w = min(kPanel, k - p0);
+    if (warp == 0) {
+      // 32 x 32 diagonal block: lane i owns row p0 + i
+      for (int j = 0; j < w; ++j) {
+        const double dj = D[(p0 + j) * ld + p0 + j];
+        zero_pivot = zero_pivot || (dj == 0.0);
+        double wij = 0.0;
+        if (lane > j && lane < w) {
+          wij = D[(p0 + lane) * ld + p0 + j];
+        }
+        __syncwarp();
+        if (lane > j && lane < w) {
+          D[(p0 + lane) * ld + p0 + j] = wij / dj;
+        }
+        __syncwarp();
+        if (lane > j && lane < w) {
+          for (int c = j + 1; c <= lane; ++c) {
+            D[(p0 + lane) * ld + p0 + c] -= wij * D[(p0 + c) * ld + p0 + j];
+          }
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+    // rows of the pivot block below this diagonal block (registers; the
+    // panel is full width here because a later row exists)
+    for (int r = p0 + w + tid; r < k; r += blockDim.x) {
+      double* row = D + r * ld + p0;
+      double y[kPanel];
+#pragma unroll
+      for (int j = 0; j < kPanel; ++j) {
+        y[j] = row[j];
+      }
+#pragma unroll
+      for (int j = 1; j < kPanel; ++j) {
+#pragma unroll
+        for (int l = 0; l < j; ++l) {
+          y[j] -= y[l] * D[(p0 + j) * ld + p0 + l];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < kPanel; ++j) {
+        row[j] = y[j] / D[(p0 + j) * ld + p0 + j];
+      }
+    }
+    __syncthreads();
+    // rank-w update of the trailing pivot block
+    const int rest = k - p0 - w;
+    for (int idx = tid; idx < rest * rest; idx += blockDim.x) {
+      const int r = p0 + w + idx % rest;
+      const int c = p0 + w + idx / rest;
+      if (r >= c) {
+        double acc = 0.0;
+        for (int l = 0; l < w; ++l) {
+          acc += (D[r * ld + p0 + l] * D[(p0 + l) * ld + p0 + l]) * D[c * ld + p0 + l];
+        }
+        D[r * ld + c] -= acc;
+      }
+    }
+    __syncthreads();
+  }
+  if (row_begin == k) {
+    for (int idx = tid; idx < k * k; idx += blockDim.x) {
+      const int r = idx % k;
+      const int c = idx / k;
+      if (r > c) {
+        const bool same = (r / kPanel) == (c / kPanel);
+        Fs[same ? static_cast<int64_t>(r) * F + c : static_cast<int64_t>(c) * F + r] = D[r * ld + c];
+      }
+    }
+    for (int j = tid; j < k; j += blockDim.x) {
+      dvec[S.first_col + j] = D[j * ld + j];
+    }
+    if (tid == 0 && zero_pivot) {
+      atomicOr(V.status + S.instance, kStatusZeroPivot);
+    }
+  }
+  // rows below the pivot block: thread per row, panel by panel
+  const int r = row_begin + tid;
+  if (r >= F || r >= row_begin + kFrontRows) {
+    return;
+  }
+  for (int p0 = 0; p0 < k; p0 += kPanel) {
+    const int w = min(kPanel, k - p0);
+    double y[kPanel];
+#pragma unroll
+    for (int j = 0; j < kPanel; ++j) {
+      y[j] = j < w ? Fs[static_cast<int64_t>(p0 + j) * F + r] : 0.0;
+    }
+    // contributions of the earlier panels (each panel's 32 values of this
+    // row loaded together, then 32 x 32 multiply-adds)
+    for (int q0 = 0; q0 < p0; q0 += kPanel) {
+      double yq[kPanel];
+#pragma unroll
+      for (int l = 0; l < kPanel; ++l) {
+        yq[l] = Fs[static_cast<int64_t>(q0 + l) * F + r];
+      }
+#pragma unroll
+      for (int l = 0; l < kPanel; ++l) {
+        const double yl = yq[l] * D[(q0 + l) * ld + q0 + l];
+#pragma unroll
+        for (int j = 0; j < kPanel; ++j) {
+          // rows p0 + j >= k (a narrow last panel) lie outside the pivot block
+          const double ljl = j < w ? D[(p0 + j) * ld + q0 + l] : 0.0;
+          y[j] -= yl * ljl;
+        }
+      }
+    }
+    // this panel's triangle
+#pragma unroll
+    for (int j = 1; j < kPanel; ++j) {
+#pragma unroll
+      for (int l = 0; l < j; ++l) {
+        if (j < w) {
+          y[j] -= y[l] * D[(p0 + j) * ld + p0 + l];
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kPanel; ++j) {
+      if (j < w) {
+        Fs[static_cast<int64_t>(p0 + j) * F + r] = y[j] / D[(p0 + j) * ld + p0 + j];
       }
     }
   }
@@ -278,10 +446,12 @@ __global__ void __launch_bounds__(256) KUpdate(DeviceView V, const int32_t* task
 }
 
 /// Forward solve of one level: gathers the children's update vectors,
-/// solves L11 y = v, forms the update u = v_m - L21 y for the parent and
-/// stores D^-1 y (Eigen's solve applies the inverse diagonal between the two
-/// triangular sweeps).
-__global__ void KForward(DeviceView V, const int32_t* level_sn, const double* dvec) {
+/// solves L11 y = v in 32-wide panels (warp 0 solves each panel's unit
+/// triangle with shuffles, then all threads update every row below it,
+/// including the front's m rows), stores the parent's update vector
+/// u = v_m - L21 y and D^-1 y (Eigen's solve applies the inverse diagonal
+/// between the two triangular sweeps).
+__global__ void __launch_bounds__(256) KForward(DeviceView V, const int32_t* level_sn, const double* dvec) {
   extern __shared__ double v[];
   const int s = level_sn[blockIdx.x];
   const SupernodeRec S = V.sn[s];
@@ -289,9 +459,10 @@ __global__ void KForward(DeviceView V, const int32_t* level_sn, const double* dv
     return;
   }
   const int k = S.ncols;
-  const int m = S.nrows;
   const int F = S.F;
   const double* Fs = V.fronts + S.front_off;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
   for (int j = threadIdx.x; j < F; j += blockDim.x) {
     v[j] = j < k ? V.rhs[V.perm[S.first_col + j]] : 0.0;
   }
@@ -305,28 +476,50 @@ __global__ void KForward(DeviceView V, const int32_t* level_sn, const double* dv
     }
     __syncthreads();
   }
-  for (int j = 0; j < k; ++j) {
-    const double yj = v[j];
-    for (int i = j + 1 + threadIdx.x; i < k; i += blockDim.x) {
-      v[i] -= LoadL(Fs, F, i, j) * yj;
+  for (int p0 = 0; p0 < k; p0 += kPanel) {
+    const int w = min(kPanel, k - p0);
+    if (warp == 0) {
+      // lane i preloads row i of the panel's unit triangle (same panel:
+      // transposed storage), then the sequential sweep runs on registers
+      double lrow[kPanel];
+#pragma unroll
+      for (int j = 0; j < kPanel; ++j) {
+        lrow[j] = (j < lane && lane < w) ? Fs[static_cast<int64_t>(p0 + lane) * F + (p0 + j)] : 0.0;
+      }
+      double y = lane < w ? v[p0 + lane] : 0.0;
+#pragma unroll
+      for (int j = 0; j < kPanel; ++j) {
+        const double yj = __shfl_sync(0xffffffffu, y, j);
+        y -= lrow[j] * yj;
+      }
+      if (lane < w) {
+        v[p0 + lane] = y;
+      }
+    }
+    __syncthreads();
+    for (int r = p0 + w + threadIdx.x; r < F; r += blockDim.x) {
+      double acc = v[r];
+      for (int j = 0; j < w; ++j) {
+        acc -= Fs[static_cast<int64_t>(p0 + j) * F + r] * v[p0 + j];
+      }
+      v[r] = acc;
     }
     __syncthreads();
   }
-  for (int r = threadIdx.x; r < m; r += blockDim.x) {
-    double acc = v[k + r];
-    for (int j = 0; j < k; ++j) {
-      acc -= Fs[static_cast<int64_t>(j) * F + k + r] * v[j];
-    }
-    V.upd[S.upd_off + r] = acc;
+  for (int r = threadIdx.x; r < F - k; r += blockDim.x) {
+    V.upd[S.upd_off + r] = v[k + r];
   }
   for (int j = threadIdx.x; j < k; j += blockDim.x) {
     V.xs[S.first_col + j] = (1.0 / dvec[S.first_col + j]) * v[j];
   }
 }
 
-/// Backward solve of one level (root first): z = x_k - L21^T x_R, then
-/// L11^T x = z; writes the step in natural order.
-__global__ void KBackward(DeviceView V, const int32_t* level_sn) {
+/// Backward solve of one level (root first): z = x_k - L21^T x_R with one
+/// warp per column, then L11^T x = z in 32-wide panels from the last (all
+/// threads subtract the later pivots' contribution, warp 0 solves the
+/// panel's unit upper triangle with shuffles); writes the step in natural
+/// order.
+__global__ void __launch_bounds__(256) KBackward(DeviceView V, const int32_t* level_sn) {
   extern __shared__ double z[];
   const int s = level_sn[blockIdx.x];
   const SupernodeRec S = V.sn[s];
@@ -347,6 +540,7 @@ __global__ void KBackward(DeviceView V, const int32_t* level_sn) {
     for (int r = lane; r < m; r += 32) {
       acc += col[r] * V.xs[rows[r]];
     }
+#pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
       acc += __shfl_down_sync(0xffffffffu, acc, off);
     }
@@ -355,10 +549,42 @@ __global__ void KBackward(DeviceView V, const int32_t* level_sn) {
     }
   }
   __syncthreads();
-  for (int j = k - 1; j >= 0; --j) {
-    const double xj = z[j];
-    for (int i = threadIdx.x; i < j; i += blockDim.x) {
-      z[i] -= LoadL(Fs, F, j, i) * xj;
+  const int last = ((k - 1) / kPanel) * kPanel;
+  for (int p0 = last; p0 >= 0; p0 -= kPanel) {
+    const int w = min(kPanel, k - p0);
+    // later pivots of this front: z[p0 + j] -= sum_{i >= p0 + w} L(i, p0 + j) x_i
+    for (int j = warp; j < w; j += nwarps) {
+      double acc = 0.0;
+      const double* col = Fs + static_cast<int64_t>(p0 + j) * F;
+      for (int i = p0 + w + lane; i < k; i += 32) {
+        acc += col[i] * z[i];
+      }
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        acc += __shfl_down_sync(0xffffffffu, acc, off);
+      }
+      if (lane == 0) {
+        z[p0 + j] -= acc;
+      }
+    }
+    __syncthreads();
+    if (warp == 0) {
+      // lane i preloads column i of the panel's unit triangle: L(j, i) for
+      // j > i (same panel: transposed storage)
+      double lcolv[kPanel];
+#pragma unroll
+      for (int j = 0; j < kPanel; ++j) {
+        lcolv[j] = (lane < j && j < w) ? Fs[static_cast<int64_t>(p0 + j) * F + (p0 + lane)] : 0.0;
+      }
+      double x = lane < w ? z[p0 + lane] : 0.0;
+#pragma unroll
+      for (int j = kPanel - 1; j >= 0; --j) {
+        const double xj = __shfl_sync(0xffffffffu, x, j);
+        x -= lcolv[j] * xj;
+      }
+      if (lane < w) {
+        z[p0 + lane] = x;
+      }
     }
     __syncthreads();
   }
@@ -383,6 +609,15 @@ void ConfigureSolveKernels(int max_front) {
   // an engine with smaller fronts never lowers another engine's limit.
   static std::mutex mu;
   static int configured = 48 * 1024;
+  static bool front_configured = false;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!front_configured) {
+      const int bytes = kSmallPivots * (kSmallPivots + 1) * static_cast<int>(sizeof(double));
+      CudaCheck(cudaFuncSetAttribute(KFactorFront, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "smem attr");
+      front_configured = true;
+    }
+  }
   const int smem = max_front * static_cast<int>(sizeof(double));
   if (smem > 227 * 1024) {
     Fail(SDFGPU_ERR_INVALID_ARGUMENT, "front too large for the solve kernels");
@@ -400,7 +635,15 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
   for (int l = 0; l < S.num_levels; ++l) {
     const TaskRange ea = S.ea_range[static_cast<size_t>(l)];
     if (ea.count > 0) {
-      KExtendAdd<<<static_cast<unsigned>(ea.count), 128, 0, stream>>>(V, P.ea_tasks + 3 * ea.begin);
+      KExtendAdd<<<static_cast<unsigned>(ea.count), 256, 0, stream>>>(V, P.ea_tasks + 3 * ea.begin);
+      ++launches;
+    }
+    const TaskRange sm = S.small_range[static_cast<size_t>(l)];
+    if (sm.count > 0) {
+      const int kmax = S.small_max_k[static_cast<size_t>(l)];
+      const size_t bytes = static_cast<size_t>(kmax) * (kmax + 1) * sizeof(double);
+      KFactorFront<<<static_cast<unsigned>(sm.count), kFrontRows, bytes, stream>>>(V, P.small_tasks + 2 * sm.begin,
+                                                                                  P.dvec);
       ++launches;
     }
     for (int t = 0; t < S.level_panels[static_cast<size_t>(l)]; ++t) {

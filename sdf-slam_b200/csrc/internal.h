@@ -126,6 +126,12 @@ struct Symbolic {
   std::vector<int32_t> update_tasks;         // (sn, panel, ti, tj) quads
   std::vector<TaskRange> update_range;       // per (level, panel) flattened
   std::vector<int32_t> panel_index_base;     // level -> first (level,panel) slot
+  // fronts with at most small_pivots pivots: one factorization kernel per
+  // level, tasks (sn, first row of the chunk below the pivot block)
+  int small_pivots{128};
+  std::vector<int32_t> small_tasks;
+  std::vector<TaskRange> small_range;        // per level
+  std::vector<int32_t> small_max_k;          // per level
   // Assembly offsets of J^T J entries into the front buffer, indexed by the
   // global natural column of a node.
   std::vector<int64_t> mm_off;               // 9 stencil slots per column (-1: stored elsewhere)

@@ -53,6 +53,7 @@ LdltEngine::LdltEngine(int n, const int32_t* outer, const int32_t* inner, const 
   ea_tasks_.Upload(sym_.ea_tasks, s);
   panel_tasks_.Upload(sym_.panel_tasks, s);
   update_tasks_.Upload(sym_.update_tasks, s);
+  small_tasks_.Upload(sym_.small_tasks, s);
   value_off_.Upload(offs, s);
   values_.Alloc(static_cast<size_t>(nnz_));
   fronts_.Alloc(static_cast<size_t>(sym_.front_doubles));
@@ -82,6 +83,7 @@ LdltEngine::LdltEngine(int n, const int32_t* outer, const int32_t* inner, const 
   V_.xs = xs_.get();
   V_.status = status_.get();
   V_.active = active_.get();
+  plan_.small_tasks = small_tasks_.get();
   plan_.ea_tasks = ea_tasks_.get();
   plan_.panel_tasks = panel_tasks_.get();
   plan_.update_tasks = update_tasks_.get();

@@ -240,14 +240,32 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   const int T = tile;
   constexpr int kPanelRows = 128;
   constexpr int kEaCols = 16;
+  constexpr int kFrontRows = 256;
+  const int small = S.small_pivots;
   S.level_panels.assign(static_cast<size_t>(levels), 0);
   S.panel_index_base.assign(static_cast<size_t>(levels) + 1, 0);
+  S.small_range.assign(static_cast<size_t>(levels), {});
+  S.small_max_k.assign(static_cast<size_t>(levels), 0);
+  S.small_tasks.clear();
   for (int l = 0; l < levels; ++l) {
     int maxp = 0;
+    S.small_range[static_cast<size_t>(l)].begin = static_cast<int64_t>(S.small_tasks.size() / 2);
     for (int q = S.level_begin[static_cast<size_t>(l)]; q < S.level_begin[static_cast<size_t>(l) + 1]; ++q) {
-      const SupernodeRec& r = S.sn[static_cast<size_t>(S.level_sn[static_cast<size_t>(q)])];
+      const int sid = S.level_sn[static_cast<size_t>(q)];
+      const SupernodeRec& r = S.sn[static_cast<size_t>(sid)];
+      if (r.ncols <= small) {
+        const int chunks = std::max(1, (r.nrows + kFrontRows - 1) / kFrontRows);
+        for (int ch = 0; ch < chunks; ++ch) {
+          S.small_tasks.push_back(sid);
+          S.small_tasks.push_back(r.ncols + ch * kFrontRows);
+        }
+        S.small_max_k[static_cast<size_t>(l)] = std::max(S.small_max_k[static_cast<size_t>(l)], r.ncols);
+        continue;
+      }
       maxp = std::max(maxp, (r.ncols + B - 1) / B);
     }
+    S.small_range[static_cast<size_t>(l)].count =
+        static_cast<int64_t>(S.small_tasks.size() / 2) - S.small_range[static_cast<size_t>(l)].begin;
     S.level_panels[static_cast<size_t>(l)] = maxp;
     S.panel_index_base[static_cast<size_t>(l) + 1] = S.panel_index_base[static_cast<size_t>(l)] + maxp;
   }
@@ -286,7 +304,7 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
         const int s = S.level_sn[static_cast<size_t>(q)];
         const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
         const int c0 = t * B;
-        if (c0 >= r.ncols) {
+        if (c0 >= r.ncols || r.ncols <= small) {
           continue;
         }
         const int c1 = std::min(r.ncols, c0 + B);
