@@ -69,16 +69,28 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.lines = []
+        self.first = 0
 
     def start(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.reader = threading.Thread(target=self._read, daemon=True)
             self.reader.start()
         except (OSError, ValueError):
             self.proc = None
+            return
+        # nvidia-smi needs a moment before its first sample: wait for it so
+        # that the samples cover the timed region
+        deadline = time.perf_counter() + 5.0
+        while not self.lines and time.perf_counter() < deadline and self.proc.poll() is None:
+            time.sleep(0.01)
+
+    def mark(self):
+        """Start of the timed region: earlier samples are dropped (the last
+        one before it is kept, as the clock the region started at)."""
+        self.first = max(0, len(self.lines) - 1)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -94,7 +106,7 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for line in self.lines[self.first:]:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -323,6 +335,8 @@ def run_gpu(args, dist, world, rank, local):
         sampler.start()
     flusher.sync()
     _barrier(dist)
+    if sampler:
+        sampler.mark()
     wall0 = time.perf_counter()
     device_s = 0.0
     launches = 0
@@ -421,7 +435,7 @@ def run_gpu(args, dist, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="floorplan", choices=list(WORKLOADS))

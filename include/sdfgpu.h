@@ -235,7 +235,10 @@ int sdfgpu_linearization_get(sdfgpu_problem* problem, double* residuals, int32_t
  * [2] factorization, [3] triangular solves, [4] step + cost; [5] iterations;
  * [6] device time from the first iteration's start to the last one's end;
  * [7] kernels launched by the iterations; [8] useful FP64 flops of one
- * factorization. phases must hold 9 doubles. */
+ * factorization; [9] symbolic re-analyses during the solve (a state left
+ * the analysed sparsity pattern); [10] host seconds spent in those
+ * re-analyses; [11] host seconds capturing the iteration's CUDA graphs.
+ * phases must hold 12 doubles. */
 int sdfgpu_last_profile(sdfgpu_problem* problem, double* phases);
 
 /* ------------------------------------------------------------ factor only --

@@ -368,10 +368,11 @@ class Problem:
         return out
 
     def last_profile(self) -> dict:
-        ph = np.zeros(9)
+        ph = np.zeros(12)
         _check(lib().sdfgpu_last_profile(self._h, _d(ph)))
         return dict(assemble=ph[0], normal=ph[1], factor=ph[2], solve=ph[3], update=ph[4],
-                    iterations=int(ph[5]), span=ph[6], launches=int(ph[7]), factor_flops=ph[8])
+                    iterations=int(ph[5]), span=ph[6], launches=int(ph[7]), factor_flops=ph[8],
+                    reanalyses=int(ph[9]), reanalysis_host=ph[10], capture_host=ph[11])
 
 
 def solve(problem: Problem, options: SolverOptions | list | None = None):

@@ -141,6 +141,22 @@ __device__ __forceinline__ double WrapAngle(double a) {
 
 }  // namespace
 
+/// Offset of (pose var (frame, 0), node column) in the front, or -1 when the
+/// frame is not in the node's analysed coupling set.
+__device__ __forceinline__ int64_t PoseOffset(const DeviceView& V, int col, int frame_local) {
+  int64_t lo = V.mp_ptr[col];
+  int64_t hi = V.mp_ptr[col + 1];
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (V.mp_frame[mid] < frame_local) {
+      lo = mid + 1;
+    } else {
+      hi = mid;
+    }
+  }
+  return (lo < V.mp_ptr[col + 1] && V.mp_frame[lo] == frame_local) ? V.mp_off[lo] : -1;
+}
+
 /// Point rows: AssemblePointRows (lm_solver.cpp:30-61) with HuberWeight
 /// (problem.hpp:115-121). Writes the row record and the row's cell, and flags
 /// a point whose cell lies outside its pose's analysed coupling set.
@@ -191,6 +207,19 @@ __global__ void KPointRows(DeviceView V) {
     if (((word >> (cell & 31)) & 1u) == 0u) {
       atomicOr(V.status + i, kStatusPatternOverflow);
     }
+    // front offsets of the (pose, corner node) blocks this row adds to; the
+    // lookups run here, one thread per row, so that the cell passes read them
+    // instead of searching
+    const int64_t n0 = I.node_off + static_cast<int64_t>(ev.h) * I.nx + ev.w;
+    int64_t off[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int col = V.node_col[n0 + (q >> 1) * I.nx + (q & 1)];
+      off[q] = col >= 0 ? PoseOffset(V, col, local) : -1;
+    }
+    longlong2* po = reinterpret_cast<longlong2*>(V.pt_poff + 4 * k);
+    po[0] = make_longlong2(off[0], off[1]);
+    po[1] = make_longlong2(off[2], off[3]);
   }
 }
 
@@ -314,22 +343,6 @@ __device__ __forceinline__ int64_t PairOffset(const DeviceView& V, const int* co
     return off;
   }
   return V.mm_off[static_cast<int64_t>(col[b]) * 9 + (1 - dh) * 3 + (1 - dw)];
-}
-
-/// Offset of (pose var (frame, 0), node column) in the front, or -1 when the
-/// frame is not in the node's analysed coupling set.
-__device__ __forceinline__ int64_t PoseOffset(const DeviceView& V, int col, int frame_local) {
-  int64_t lo = V.mp_ptr[col];
-  int64_t hi = V.mp_ptr[col + 1];
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (V.mp_frame[mid] < frame_local) {
-      lo = mid + 1;
-    } else {
-      hi = mid;
-    }
-  }
-  return (lo < V.mp_ptr[col + 1] && V.mp_frame[lo] == frame_local) ? V.mp_off[lo] : -1;
 }
 
 __device__ __forceinline__ int FindInstanceByCell(const DeviceView& V, int64_t cell) {
@@ -462,10 +475,14 @@ __global__ void KCellPass(DeviceView V, int pass) {
     const bool tail = in && (lane == 31 || p + 1 >= re || fn != f);
     const int fl = f - I.frame_off;
     if (tail && fl >= 1) {
+      const longlong2* po = reinterpret_cast<const longlong2*>(V.pt_poff + 4 * static_cast<int64_t>(k));
+      const longlong2 o01 = po[0];
+      const longlong2 o23 = po[1];
+      const int64_t offs[4] = {o01.x, o01.y, o23.x, o23.y};
 #pragma unroll
       for (int aa = 0; aa < 4; ++aa) {
         if (col[aa] >= 0) {
-          const int64_t off = PoseOffset(V, col[aa], fl);
+          const int64_t off = offs[aa];
           if (off >= 0) {
             V.fronts[off] += v[3 * aa];
             V.fronts[off + 1] += v[3 * aa + 1];
@@ -758,6 +775,14 @@ __global__ void KCostTerms(DeviceView V, double* terms) {
     const double2 p = V.pt_xy[t];
     PointEval ev;
     EvalPoint(V, I, c, s, pose, p.x, p.y, V.pt_exp[t], 0, false, ev);
+    const int local = f - I.frame_off;
+    if (ev.valid && local >= 1) {
+      const int cell = ev.h * (I.nx - 1) + ev.w;
+      const uint32_t word = V.allow_bits[I.allow_off + static_cast<int64_t>(local) * I.allow_words + (cell >> 5)];
+      if (((word >> (cell & 31)) & 1u) == 0u) {
+        atomicOr(V.status + i, kStatusNextOverflow);
+      }
+    }
     const double r = V.pt_sw[t] * ev.residual;
     double term;
     if (I.huber_delta > 0.0 && fabs(r) > I.huber_delta) {

@@ -367,6 +367,9 @@ int sdfgpu_last_profile(sdfgpu_problem* problem, double* phases) {
     phases[6] = t.span;
     phases[7] = static_cast<double>(t.launches);
     phases[8] = static_cast<double>(Eng(problem).factor_flops()) * 2.0;
+    phases[9] = static_cast<double>(t.reanalyses);
+    phases[10] = t.reanalysis_host;
+    phases[11] = t.capture_host;
   });
 }
 

@@ -33,50 +33,47 @@ __global__ void KRadixHist(const int32_t* keys, int64_t n, int shift, int32_t* h
 }
 
 /// Exclusive scan of `count` int32 values in place by one block of 1024
-/// threads (counts here are at most 256 * tiles).
+/// threads (counts here are at most 256 * tiles): thread t owns a contiguous
+/// segment, whose loads are all in flight together; one block scan of the
+/// segment sums gives each segment's start.
 __global__ void KExclusiveScan(int32_t* data, int64_t count) {
   __shared__ int32_t warp_sums[32];
-  __shared__ int32_t carry;
-  if (threadIdx.x == 0) {
-    carry = 0;
-  }
-  __syncthreads();
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  for (int64_t base = 0; base < count; base += blockDim.x) {
-    const int64_t idx = base + threadIdx.x;
-    const int32_t v = idx < count ? data[idx] : 0;
-    int32_t x = v;
+  const int64_t per = (count + blockDim.x - 1) / blockDim.x;
+  const int64_t b = min(count, static_cast<int64_t>(threadIdx.x) * per);
+  const int64_t e = min(count, b + per);
+  int32_t local = 0;
+  for (int64_t q = b; q < e; ++q) {
+    local += data[q];
+  }
+  int32_t x = local;
+  for (int d = 1; d < 32; d <<= 1) {
+    const int32_t y = __shfl_up_sync(0xffffffffu, x, d);
+    if (lane >= d) {
+      x += y;
+    }
+  }
+  if (lane == 31) {
+    warp_sums[warp] = x;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    int32_t s = lane < static_cast<int>(blockDim.x >> 5) ? warp_sums[lane] : 0;
     for (int d = 1; d < 32; d <<= 1) {
-      const int32_t y = __shfl_up_sync(0xffffffffu, x, d);
+      const int32_t y = __shfl_up_sync(0xffffffffu, s, d);
       if (lane >= d) {
-        x += y;
+        s += y;
       }
     }
-    if (lane == 31) {
-      warp_sums[warp] = x;
-    }
-    __syncthreads();
-    if (warp == 0) {
-      int32_t s = lane < static_cast<int>(blockDim.x >> 5) ? warp_sums[lane] : 0;
-      for (int d = 1; d < 32; d <<= 1) {
-        const int32_t y = __shfl_up_sync(0xffffffffu, s, d);
-        if (lane >= d) {
-          s += y;
-        }
-      }
-      warp_sums[lane] = s;
-    }
-    __syncthreads();
-    const int32_t warp_prefix = warp > 0 ? warp_sums[warp - 1] : 0;
-    if (idx < count) {
-      data[idx] = carry + warp_prefix + x - v;
-    }
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) {
-      carry += warp_prefix + x;
-    }
-    __syncthreads();
+    warp_sums[lane] = s;
+  }
+  __syncthreads();
+  int32_t run = (warp > 0 ? warp_sums[warp - 1] : 0) + x - local;
+  for (int64_t q = b; q < e; ++q) {
+    const int32_t v = data[q];
+    data[q] = run;
+    run += v;
   }
 }
 

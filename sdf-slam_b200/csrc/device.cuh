@@ -38,6 +38,9 @@ struct InstDev {
 /// Status bits per instance.
 constexpr int kStatusZeroPivot = 1;
 constexpr int kStatusPatternOverflow = 2;
+// set by the cost kernel: at the state it evaluated, a point lies outside its
+// pose's analysed cell set (the next linearization would overflow)
+constexpr int kStatusNextOverflow = 4;
 
 /// Per point row record: 4 node Jacobian entries, 3 pose entries, residual.
 constexpr int kPointRec = 8;
@@ -90,6 +93,7 @@ struct DeviceView {
   double* poses_backup;
   // per iteration
   double* pt_rec;                // kPointRec per point row
+  int64_t* pt_poff;              // 4 per point row: front offsets of its (pose, corner node) blocks
   int32_t* pt_cell;              // global cell or -1
   double* eik_rec;
   double* odom_rec;

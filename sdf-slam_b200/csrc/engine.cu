@@ -303,6 +303,7 @@ void Engine::UploadProblem() {
   map_backup_.Alloc(map.size());
   poses_backup_.Alloc(poses.size());
   pt_rec_.Alloc(static_cast<size_t>(total_points_) * kPointRec);
+  pt_poff_.Alloc(static_cast<size_t>(total_points_) * 4);
   pt_cell_.Alloc(static_cast<size_t>(total_points_));
   eik_rec_.Alloc(static_cast<size_t>(total_eik_) * kEikRec);
   odom_rec_.Alloc(static_cast<size_t>(total_odom_) * kOdomRec);
@@ -358,8 +359,18 @@ void Engine::UploadProblem() {
 }
 
 void Engine::Analyze() {
+  margin_.assign(host_.size(), kDefaultMargin);
+  pieces_.assign(host_.size(), SymPiece{});
+  pending_.clear();
+  AnalyzeInstances(host_, margin_, pieces_, nullptr);
+  sym_ = Concatenate(pieces_, layout_, 32, 64);
+  UploadSymbolic();
+}
+
+void Engine::UploadSymbolic() {
   DropGraph();
-  sym_ = sdfgpu::Analyze(host_, layout_, 32, 64);
+  // the previous structure may still be read by enqueued work
+  CudaCheck(cudaStreamSynchronize(stream_), "analysis sync");
   cudaStream_t s = stream_;
   perm_.Upload(sym_.perm, s);
   pinv_.Upload(sym_.pinv, s);
@@ -374,6 +385,7 @@ void Engine::Analyze() {
   mp_frame_.Upload(sym_.mp_frame, s);
   allow_bits_.Upload(sym_.allow_bits, s);
   ea_tasks_.Upload(sym_.ea_tasks, s);
+  ea_child_.Upload(sym_.ea_child, s);
   panel_tasks_.Upload(sym_.panel_tasks, s);
   update_tasks_.Upload(sym_.update_tasks, s);
   small_tasks_.Upload(sym_.small_tasks, s);
@@ -420,7 +432,7 @@ void Engine::Analyze() {
   device_bytes_ = 0;
   device_bytes_ += static_cast<int64_t>(fronts_.size()) * 8 + static_cast<int64_t>(pt_rec_.size()) * 8 +
                    static_cast<int64_t>(mp_off_.size()) * 12 + static_cast<int64_t>(mm_off_.size()) * 8 +
-                   static_cast<int64_t>(total_points_) * 48;
+                   static_cast<int64_t>(total_points_) * 80;
   RefreshView();
   CudaCheck(cudaStreamSynchronize(s), "analyze upload");
 }
@@ -467,6 +479,7 @@ void Engine::RefreshView() {
   V.map_backup = map_backup_.get();
   V.poses_backup = poses_backup_.get();
   V.pt_rec = pt_rec_.get();
+  V.pt_poff = pt_poff_.get();
   V.pt_cell = pt_cell_.get();
   V.eik_rec = eik_rec_.get();
   V.odom_rec = odom_rec_.get();
@@ -588,6 +601,7 @@ FactorPlan Engine::Plan() {
   FactorPlan P;
   P.small_tasks = small_tasks_.get();
   P.ea_tasks = ea_tasks_.get();
+  P.ea_child = ea_child_.get();
   P.panel_tasks = panel_tasks_.get();
   P.update_tasks = update_tasks_.get();
   P.level_sn = level_sn_.get();
@@ -602,6 +616,7 @@ void Engine::LaunchSolve() { times_.launches += LaunchSolveLevels(sym_, V_, Plan
 
 void Engine::LaunchCost(std::vector<double>& cost) {
   const int64_t terms = total_points_ + total_eik_ + total_odom_;
+  ClearStatus();
   if (terms > 0) {
     KCostTerms<<<Blocks(terms, 128), 128, 0, stream_>>>(V_, terms_.get());
   }
@@ -610,10 +625,16 @@ void Engine::LaunchCost(std::vector<double>& cost) {
   std::vector<double> out(3 * I);
   CudaCheck(cudaMemcpyAsync(out.data(), seg_out_.get(), out.size() * sizeof(double), cudaMemcpyDeviceToHost, stream_),
             "cost");
+  std::vector<int32_t> st(I);
+  CudaCheck(cudaMemcpyAsync(st.data(), status_.get(), I * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_),
+            "status");
   CudaCheck(cudaStreamSynchronize(stream_), "cost sync");
   cost.resize(I);
   for (size_t i = 0; i < I; ++i) {
     cost[i] = (out[3 * i] + out[3 * i + 1]) + out[3 * i + 2];
+    if ((st[i] & kStatusNextOverflow) != 0) {
+      pending_.push_back(static_cast<int>(i));
+    }
   }
 }
 
@@ -643,17 +664,36 @@ void Engine::LaunchStepAndCost(bool backup) {
   CudaCheck(cudaGetLastError(), "step kernels");
 }
 
-void Engine::Reanalyze() {
+void Engine::Reanalyze(const std::vector<int>& which) {
+  const auto t0 = std::chrono::steady_clock::now();
   std::vector<double> poses(3 * static_cast<size_t>(total_frames_));
   CudaCheck(cudaMemcpyAsync(poses.data(), poses_.get(), poses.size() * sizeof(double), cudaMemcpyDeviceToHost,
                             stream_),
             "poses");
   CudaCheck(cudaStreamSynchronize(stream_), "reanalyze sync");
-  for (size_t i = 0; i < host_.size(); ++i) {
-    std::copy(poses.begin() + 3 * layout_[i].frame_off,
-              poses.begin() + 3 * (layout_[i].frame_off + layout_[i].num_frames), host_[i].poses.begin());
+  for (const int i : which) {
+    const InstanceLayout& L = layout_[static_cast<size_t>(i)];
+    std::copy(poses.begin() + 3 * L.frame_off, poses.begin() + 3 * (L.frame_off + L.num_frames),
+              host_[static_cast<size_t>(i)].poses.begin());
+    // a pattern that was left once is widened so that it is left less often
+    margin_[static_cast<size_t>(i)] = std::min(margin_[static_cast<size_t>(i)] + 1, kMaxMargin);
   }
-  Analyze();
+  AnalyzeInstances(host_, margin_, pieces_, &which);
+  sym_ = Concatenate(pieces_, layout_, 32, 64);
+  UploadSymbolic();
+  ++times_.reanalyses;
+  times_.reanalysis_host += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void Engine::ReanalyzePending() {
+  if (pending_.empty()) {
+    return;
+  }
+  std::sort(pending_.begin(), pending_.end());
+  pending_.erase(std::unique(pending_.begin(), pending_.end()), pending_.end());
+  const std::vector<int> which = std::move(pending_);
+  pending_.clear();
+  Reanalyze(which);
 }
 
 /// Rows + normal equations; re-runs the symbolic analysis (once) when a point
@@ -667,11 +707,13 @@ int Engine::AssembleWithPattern() {
     LaunchNormal();
     CudaCheck(cudaEventRecord(ev_[2], stream_), "event");
     const std::vector<int32_t> st = DownloadStatus();
-    bool overflow = false;
-    for (const int32_t v : st) {
-      overflow = overflow || (v & kStatusPatternOverflow) != 0;
+    std::vector<int> overflow;
+    for (size_t i = 0; i < st.size(); ++i) {
+      if ((st[i] & kStatusPatternOverflow) != 0) {
+        overflow.push_back(static_cast<int>(i));
+      }
     }
-    if (!overflow) {
+    if (overflow.empty()) {
       float ms = 0.0f;
       CudaCheck(cudaEventElapsedTime(&ms, ev_[0], ev_[1]), "phase timing");
       times_.assemble += ms * 1e-3;
@@ -679,7 +721,7 @@ int Engine::AssembleWithPattern() {
       times_.normal += ms * 1e-3;
       return 0;
     }
-    Reanalyze();
+    Reanalyze(overflow);
   }
   Fail(SDFGPU_ERR_CUDA, "sparsity pattern still overflows after re-analysis");
 }
@@ -1041,7 +1083,14 @@ void Engine::LaunchIteration() {
     CudaCheck(cudaEventRecord(span_[0], stream_), "event");
     span_started_ = true;
   }
+  // a state that left its pattern is re-analysed before it is linearized
+  ReanalyzePending();
+  EnqueueIteration();
+}
+
+void Engine::EnqueueIteration() {
   if (use_graph_ && (graph_exec_[0] == nullptr || graph_backup_ != need_backup_)) {
+    const auto t0 = std::chrono::steady_clock::now();
     DropGraph();
     const int64_t before = times_.launches;
     for (int phase = 0; phase < 5; ++phase) {
@@ -1065,6 +1114,7 @@ void Engine::LaunchIteration() {
     graph_launches_ = times_.launches - before;
     times_.launches = before;
     graph_backup_ = need_backup_;
+    times_.capture_host += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
   for (int phase = 0; phase < 5; ++phase) {
     CudaCheck(cudaEventRecord(ev_[phase], stream_), "event");
@@ -1082,22 +1132,45 @@ void Engine::LaunchIteration() {
 
 void Engine::FinishIteration() {
   const size_t I = host_.size();
-  for (int attempt = 0;; ++attempt) {
+  CudaCheck(cudaStreamSynchronize(stream_), "iteration");
+  std::vector<int> overflow;
+  for (size_t i = 0; i < I; ++i) {
+    if (lm_[i].active != 0 && (h_status_[i] & kStatusPatternOverflow) != 0) {
+      overflow.push_back(static_cast<int>(i));
+    }
+  }
+  if (!overflow.empty()) {
+    // A point left its pose's analysed cell set (a state the look-ahead of
+    // the cost kernel did not see, e.g. one set by the caller): the step
+    // kernel skipped these instances. Re-analyse them at the current state
+    // and run the iteration again for them alone; the other instances keep
+    // the results (and the applied steps) of the first run.
+    std::vector<double> seg(h_seg_.get(), h_seg_.get() + 5 * I);
+    std::vector<int32_t> st(h_status_.get(), h_status_.get() + I);
+    Reanalyze(overflow);
+    std::fill(h_active_.get(), h_active_.get() + I, 0);
+    for (const int i : overflow) {
+      h_active_[i] = 1;
+    }
+    EnqueueIteration();
     CudaCheck(cudaStreamSynchronize(stream_), "iteration");
-    bool overflow = false;
+    std::vector<char> rerun(I, 0);
+    for (const int i : overflow) {
+      rerun[static_cast<size_t>(i)] = 1;
+      if ((h_status_[i] & kStatusPatternOverflow) != 0) {
+        Fail(SDFGPU_ERR_CUDA, "sparsity pattern still overflows after re-analysis");
+      }
+    }
     for (size_t i = 0; i < I; ++i) {
-      overflow = overflow || (lm_[i].active != 0 && (h_status_[i] & kStatusPatternOverflow) != 0);
+      if (rerun[i] == 0) {
+        h_seg_[3 * i] = seg[3 * i];
+        h_seg_[3 * i + 1] = seg[3 * i + 1];
+        h_seg_[3 * i + 2] = seg[3 * i + 2];
+        h_seg_[3 * I + i] = seg[3 * I + i];
+        h_seg_[4 * I + i] = seg[4 * I + i];
+        h_status_[i] = st[i];
+      }
     }
-    if (!overflow) {
-      break;
-    }
-    if (attempt >= 1) {
-      Fail(SDFGPU_ERR_CUDA, "sparsity pattern still overflows after re-analysis");
-    }
-    // a point left its pose's analysed cell set: the step kernel skipped the
-    // update, so re-analyse at the current state and run the iteration again
-    Reanalyze();
-    LaunchIteration();
   }
   float ms = 0.0f;
   double* acc[5] = {&times_.assemble, &times_.normal, &times_.factor, &times_.solve, &times_.update};
@@ -1161,6 +1234,14 @@ void Engine::FinishIteration() {
     }
     L.hist.push_back(current);
     L.res.final_cost = current;
+  }
+  for (size_t i = 0; i < I; ++i) {
+    // the accepted state lies outside the pattern: analyse before the next
+    // linearization (a reverted state is the one just linearized)
+    if (h_active_[i] != 0 && (h_status_[i] & kStatusNextOverflow) != 0 && revert[i] == 0 &&
+        (h_status_[i] & kStatusZeroPivot) == 0) {
+      pending_.push_back(static_cast<int>(i));
+    }
   }
   if (any_revert) {
     CudaCheck(cudaMemcpyAsync(revert_.get(), revert.data(), revert.size() * sizeof(int32_t), cudaMemcpyHostToDevice,

@@ -71,6 +71,7 @@ class DevBuf {
 struct FactorPlan {
   const int32_t* small_tasks{nullptr};
   const int32_t* ea_tasks{nullptr};
+  const int32_t* ea_child{nullptr};
   const int32_t* panel_tasks{nullptr};
   const int32_t* update_tasks{nullptr};
   const int32_t* level_sn{nullptr};
@@ -127,6 +128,9 @@ struct IterTimes {
   int iterations{0};
   double span{0};        // device time from the first iteration's start to the last one's end
   int64_t launches{0};   // kernels launched by the iterations
+  int reanalyses{0};     // symbolic re-analyses (a state left its pattern)
+  double reanalysis_host{0};  // host seconds in re-analyses (analysis, upload)
+  double capture_host{0};     // host seconds capturing and instantiating graphs
 };
 
 class Engine {
@@ -176,6 +180,7 @@ class Engine {
   void BuildLayout();
   void UploadProblem();
   void Analyze();
+  void UploadSymbolic();
   void RefreshView();
   void SetActive(const std::vector<int32_t>& active);
   void SetLambda(const std::vector<double>& lam, const std::vector<int32_t>& marquardt);
@@ -187,13 +192,21 @@ class Engine {
   void LaunchSolve();
   void LaunchStepAndCost(bool backup);
   void LaunchCost(std::vector<double>& cost);
-  void Reanalyze();
+  /// Re-analyses the listed instances at the current state (with a wider
+  /// coupling margin) and rebuilds the global structure.
+  void Reanalyze(const std::vector<int>& which);
+  /// Re-analyses the instances whose state left their pattern (pending_).
+  void ReanalyzePending();
+  void EnqueueIteration();
   int AssembleWithPattern();
   [[nodiscard]] FactorPlan Plan();
   void SegmentSum(const double* x, const int64_t* seg_begin, const int64_t* seg_end, int segments, double* out);
 
   std::vector<HostProblem> host_;
   std::vector<InstanceLayout> layout_;
+  std::vector<SymPiece> pieces_;   // per-instance analyses (local numbering)
+  std::vector<int> margin_;        // per instance: coupling margin of its piece
+  std::vector<int> pending_;       // instances whose current state overflows their pattern
   Symbolic sym_;
   cudaStream_t stream_{nullptr};
   cudaEvent_t ev_[6]{};
@@ -229,6 +242,7 @@ class Engine {
   // state and per-iteration buffers
   DevBuf<double> map_, poses_, map_backup_, poses_backup_;
   DevBuf<double> pt_rec_, eik_rec_, odom_rec_;
+  DevBuf<int64_t> pt_poff_;
   DevBuf<int32_t> pt_cell_, cell_start_, sort_keys_a_, sort_vals_a_, sort_keys_b_, sort_vals_b_, sort_hist_;
   DevBuf<double> rhs_, step_, xs_, lam_, dvec_;
   DevBuf<int32_t> marq_, status_, active_, revert_;
@@ -240,7 +254,7 @@ class Engine {
   DevBuf<int64_t> mm_off_, mp_ptr_, mp_off_;
   DevBuf<int32_t> mp_frame_;
   DevBuf<uint32_t> allow_bits_;
-  DevBuf<int32_t> ea_tasks_, panel_tasks_, update_tasks_, small_tasks_;
+  DevBuf<int32_t> ea_tasks_, ea_child_, panel_tasks_, update_tasks_, small_tasks_;
   DevBuf<double> fronts_, upd_;
   int32_t* cell_rows_ptr_{nullptr};
   HostBuf<double> h_seg_;      // 5 per instance: cost parts x3, |delta|^2, prediction

@@ -30,44 +30,63 @@ __device__ __forceinline__ double LoadL(const double* Fs, int F, int i, int j) {
   return (i / kPanel == j / kPanel) ? Fs[static_cast<int64_t>(i) * F + j] : Fs[static_cast<int64_t>(j) * F + i];
 }
 
+/// LDL^T of the w x w diagonal block at B (row r, column c at B[r * ld + c],
+/// lower triangle) by one warp in registers: lane i owns row i; at step j
+/// its registers hold columns j.., so every register index is static while
+/// the step loop stays rolled (a small code footprint). Writes L below the
+/// diagonal and D on it; returns true when a pivot is exactly zero.
+__device__ __noinline__ bool DiagonalBlockLdlt(double* B, int ld, int w) {
+  const int lane = threadIdx.x & 31;
+  double row[kPanel];
+#pragma unroll
+  for (int c = 0; c < kPanel; ++c) {
+    row[c] = (lane < w && c <= lane) ? B[lane * ld + c] : (c == lane ? 1.0 : 0.0);
+  }
+  bool zero = false;
+  for (int j = 0; j < w; ++j) {
+    const double dj = __shfl_sync(0xffffffffu, row[0], j);
+    zero = zero || (dj == 0.0);
+    const double wij = row[0];
+    const double lij = wij / dj;
+    if (lane < w && lane >= j) {
+      B[lane * ld + j] = lane == j ? dj : lij;
+    }
+#pragma unroll
+    for (int c = 1; c < kPanel; ++c) {
+      // column j + c: A(i, j + c) -= W(i, j) L(j + c, j) for j < i, j + c <= i
+      const double lcj = __shfl_sync(0xffffffffu, lij, (j + c) & 31);
+      if (lane > j && j + c <= lane) {
+        row[c] -= wij * lcj;
+      }
+    }
+#pragma unroll
+    for (int c = 0; c + 1 < kPanel; ++c) {
+      row[c] = row[c + 1];
+    }
+    row[kPanel - 1] = 0.0;
+  }
+  return zero;
+}
+
 /// Adds the children's update matrices into each parent front. A task owns a
 /// range of parent columns, so no two blocks write the same entry; children
 /// are added in their fixed order.
-__global__ void KExtendAdd(DeviceView V, const int32_t* tasks) {
-  const int32_t* t = tasks + 3 * static_cast<int64_t>(blockIdx.x);
+__global__ void KExtendAdd(DeviceView V, const int32_t* tasks, const int32_t* child_ranges) {
+  const int32_t* t = tasks + 4 * static_cast<int64_t>(blockIdx.x);
   const int p = t[0];
-  const int clo = t[1];
-  const int chi = t[2];
   const SupernodeRec P = V.sn[p];
   if (V.active[P.instance] == 0) {
     return;
   }
+  const int32_t* ranges = child_ranges + t[3];
   double* Fp = V.fronts + P.front_off;
   for (int ci = 0; ci < P.child_count; ++ci) {
     const SupernodeRec C = V.sn[V.child_list[P.child_begin + ci]];
     const int32_t* rel = V.sn_rel + C.rows_off;
     const int m = C.nrows;
-    int lo = 0;
-    int hi = m;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if (rel[mid] < clo) {
-        lo = mid + 1;
-      } else {
-        hi = mid;
-      }
-    }
-    const int cbeg = lo;
-    hi = m;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if (rel[mid] < chi) {
-        lo = mid + 1;
-      } else {
-        hi = mid;
-      }
-    }
-    const int cend = lo;
+    // update columns of this child that land in the task's parent columns
+    const int cbeg = ranges[2 * ci];
+    const int cend = ranges[2 * ci + 1];
     const double* U = V.fronts + C.front_off + static_cast<int64_t>(C.ncols) * C.F + C.ncols;
     const int lane = threadIdx.x & 31;
     const int nwarps = blockDim.x >> 5;
@@ -101,7 +120,6 @@ __global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const
   const int c1 = c0 + w;
   double* Fs = V.fronts + S.front_off;
   __shared__ double D[kPanel][kPanel + 1];
-  __shared__ double lcol[kPanel];
   const int tid = threadIdx.x;
   for (int idx = tid; idx < kPanel * kPanel; idx += blockDim.x) {
     const int i = idx % kPanel;
@@ -116,26 +134,10 @@ __global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const
   }
   __syncthreads();
   bool zero_pivot = false;
-  for (int j = 0; j < w; ++j) {
-    const double dj = D[j][j];
-    zero_pivot = zero_pivot || (dj == 0.0);
-    if (tid > j && tid < w) {
-      lcol[tid] = D[tid][j] / dj;
-    }
-    __syncthreads();
-    for (int idx = tid; idx < kPanel * kPanel; idx += blockDim.x) {
-      const int i = idx % kPanel;
-      const int l = idx / kPanel;
-      if (l > j && i >= l && i < w) {
-        D[i][l] -= D[i][j] * lcol[l];
-      }
-    }
-    __syncthreads();
-    if (tid > j && tid < w) {
-      D[tid][j] = lcol[tid];
-    }
-    __syncthreads();
+  if ((tid >> 5) == 0) {
+    zero_pivot = DiagonalBlockLdlt(&D[0][0], kPanel + 1, w);
   }
+  __syncthreads();
   if (row_begin == c1) {
     // first block of the panel: D into dvec, L11 transposed into the upper
     // triangle of the diagonal block
@@ -216,26 +218,7 @@ __global__ void __launch_bounds__(256) KFactorFront(DeviceView V, const int32_t*
   for (int p0 = 0; p0 < k; p0 += kPanel) {
     const int w = min(kPanel, k - p0);
     if (warp == 0) {
-      // 32 x 32 diagonal block: lane i owns row p0 + i
-      for (int j = 0; j < w; ++j) {
-        const double dj = D[(p0 + j) * ld + p0 + j];
-        zero_pivot = zero_pivot || (dj == 0.0);
-        double wij = 0.0;
-        if (lane > j && lane < w) {
-          wij = D[(p0 + lane) * ld + p0 + j];
-        }
-        __syncwarp();
-        if (lane > j && lane < w) {
-          D[(p0 + lane) * ld + p0 + j] = wij / dj;
-        }
-        __syncwarp();
-        if (lane > j && lane < w) {
-          for (int c = j + 1; c <= lane; ++c) {
-            D[(p0 + lane) * ld + p0 + c] -= wij * D[(p0 + c) * ld + p0 + j];
-          }
-        }
-        __syncwarp();
-      }
+      zero_pivot = DiagonalBlockLdlt(D + p0 * ld + p0, ld, w) || zero_pivot;
     }
     __syncthreads();
     // rows of the pivot block below this diagonal block (registers; the
@@ -635,7 +618,7 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
   for (int l = 0; l < S.num_levels; ++l) {
     const TaskRange ea = S.ea_range[static_cast<size_t>(l)];
     if (ea.count > 0) {
-      KExtendAdd<<<static_cast<unsigned>(ea.count), 256, 0, stream>>>(V, P.ea_tasks + 3 * ea.begin);
+      KExtendAdd<<<static_cast<unsigned>(ea.count), 256, 0, stream>>>(V, P.ea_tasks + 4 * ea.begin, P.ea_child);
       ++launches;
     }
     const TaskRange sm = S.small_range[static_cast<size_t>(l)];

@@ -119,7 +119,8 @@ struct Symbolic {
   std::vector<int32_t> level_begin;
   std::vector<int32_t> level_sn;
   std::vector<int32_t> level_panels;         // max panel count per level
-  std::vector<int32_t> ea_tasks;             // (sn, col_lo, col_hi) triples
+  std::vector<int32_t> ea_tasks;             // (sn, col_lo, col_hi, ea_child offset) quads
+  std::vector<int32_t> ea_child;             // per task and child: update column range [begin, end)
   std::vector<TaskRange> ea_range;           // per level
   std::vector<int32_t> panel_tasks;          // (sn, panel, row_begin) triples
   std::vector<TaskRange> panel_range;        // per (level, panel) flattened
@@ -169,6 +170,33 @@ struct InstanceLayout {
   int32_t smooth_gradient;
   double smooth_gradient_step;
 };
+
+/// Symbolic analysis of one grid instance in instance-local numbering
+/// (columns, supernodes, rows and front offsets start at 0; relative
+/// extend-add indices filled); Concatenate places pieces one after another.
+struct SymPiece {
+  Symbolic s;
+  std::vector<int> height;  // per supernode: height in the assembly tree
+  int margin{0};            // coupling dilation (cells) the piece was built with
+};
+
+/// Coupling dilation (cells) of a first analysis.
+constexpr int kDefaultMargin = 2;
+/// Largest dilation re-analysis grows a pattern to.
+constexpr int kMaxMargin = 5;
+
+/// Analyses one instance at its current state.
+SymPiece AnalyzeInstance(const HostProblem& hp, int margin);
+
+/// Analyses the instances listed in `which` (all when null) into
+/// pieces[i], on up to hardware_concurrency threads.
+void AnalyzeInstances(const std::vector<HostProblem>& problems, const std::vector<int>& margin,
+                      std::vector<SymPiece>& pieces, const std::vector<int>* which);
+
+/// Global structure (task lists, level schedule) of pieces laid out by
+/// `layout`.
+Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<InstanceLayout>& layout,
+                     int panel_width, int tile);
 
 /// Builds the supernodal symbolic factorization for a set of instances.
 Symbolic Analyze(const std::vector<HostProblem>& problems, const std::vector<InstanceLayout>& layout,

@@ -51,6 +51,7 @@ LdltEngine::LdltEngine(int n, const int32_t* outer, const int32_t* inner, const 
   child_list_.Upload(sym_.child_list, s);
   level_sn_.Upload(sym_.level_sn, s);
   ea_tasks_.Upload(sym_.ea_tasks, s);
+  ea_child_.Upload(sym_.ea_child, s);
   panel_tasks_.Upload(sym_.panel_tasks, s);
   update_tasks_.Upload(sym_.update_tasks, s);
   small_tasks_.Upload(sym_.small_tasks, s);
@@ -85,6 +86,7 @@ LdltEngine::LdltEngine(int n, const int32_t* outer, const int32_t* inner, const 
   V_.active = active_.get();
   plan_.small_tasks = small_tasks_.get();
   plan_.ea_tasks = ea_tasks_.get();
+  plan_.ea_child = ea_child_.get();
   plan_.panel_tasks = panel_tasks_.get();
   plan_.update_tasks = update_tasks_.get();
   plan_.level_sn = level_sn_.get();

@@ -30,7 +30,7 @@ class LdltEngine {
   cudaStream_t stream_{nullptr};
   DeviceView V_{};
   FactorPlan plan_{};
-  DevBuf<int32_t> perm_, sn_rows_, sn_rel_, child_list_, level_sn_, ea_tasks_, panel_tasks_, update_tasks_,
+  DevBuf<int32_t> perm_, sn_rows_, sn_rel_, child_list_, level_sn_, ea_tasks_, ea_child_, panel_tasks_, update_tasks_,
       small_tasks_;
   DevBuf<SupernodeRec> sn_;
   DevBuf<int64_t> value_off_;

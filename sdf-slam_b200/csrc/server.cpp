@@ -13,8 +13,9 @@ int64_t EstimateDeviceBytes(const HostProblem& hp) {
   const Symbolic S = Analyze(v, {L}, 32, 64);
   const int64_t P = hp.num_points();
   const int64_t nodes = static_cast<int64_t>(hp.nx) * hp.ny;
-  int64_t bytes = S.front_doubles * 8;
-  bytes += P * (8 * 8 + 4 * 8 + 48);               // row records, cells, sort buffers, specs
+  // fronts grow when a re-analysis widens the coupling margin
+  int64_t bytes = S.front_doubles * 8 * 3 / 2;
+  bytes += P * (8 * 8 + 4 * 8 + 4 * 8 + 48);       // row records, pose offsets, cells, sort buffers, specs
   bytes += nodes * (8 * 3 + 4 * 4);                 // map, backup, index maps
   bytes += static_cast<int64_t>(S.mm_off.size()) * 8 + static_cast<int64_t>(S.mp_off.size()) * 12;
   bytes += static_cast<int64_t>(S.sn_rows.size()) * 8 + static_cast<int64_t>(S.update_tasks.size()) * 4;

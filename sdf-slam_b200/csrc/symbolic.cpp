@@ -22,9 +22,13 @@
 // that structure. Any contiguous partition gives a valid assembly tree this
 // way.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <exception>
 #include <functional>
+#include <mutex>
 #include <numeric>
+#include <thread>
 
 #include "internal.h"
 
@@ -201,9 +205,8 @@ void AppendInstance(Symbolic& S, const LocalSym& L, int col_off, int instance, s
 }
 
 /// Relative indices, level lists and task lists once all supernodes exist.
-void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int tile) {
-  S.panel_width = panel_width;
-  S.tile = tile;
+/// Position of every front row in its parent's front (extend-add map).
+void ComputeRel(Symbolic& S) {
   const int Sn = static_cast<int>(S.sn.size());
   S.sn_rel.assign(S.sn_rows.size(), 0);
   for (int s = 0; s < Sn; ++s) {
@@ -212,11 +215,28 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
       continue;
     }
     const SupernodeRec& p = S.sn[static_cast<size_t>(r.parent)];
+    // both row lists ascend: one merge walk
+    const int32_t* prow = S.sn_rows.data() + p.rows_off;
+    int j = 0;
     for (int q = 0; q < r.nrows; ++q) {
-      S.sn_rel[static_cast<size_t>(r.rows_off + q)] =
-          LocalIndex(p, S.sn_rows.data() + p.rows_off, S.sn_rows[static_cast<size_t>(r.rows_off + q)]);
+      const int32_t row = S.sn_rows[static_cast<size_t>(r.rows_off + q)];
+      if (row < p.first_col + p.ncols) {
+        S.sn_rel[static_cast<size_t>(r.rows_off + q)] = row - p.first_col;
+        continue;
+      }
+      while (j < p.nrows && prow[j] < row) {
+        ++j;
+      }
+      S.sn_rel[static_cast<size_t>(r.rows_off + q)] = p.ncols + j;
     }
   }
+}
+
+/// Level lists and task lists once all supernodes exist.
+void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int tile) {
+  S.panel_width = panel_width;
+  S.tile = tile;
+  const int Sn = static_cast<int>(S.sn.size());
   int levels = 0;
   for (const int h : height) {
     levels = std::max(levels, h + 1);
@@ -281,7 +301,7 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
     const int qb = S.level_begin[static_cast<size_t>(l)];
     const int qe = S.level_begin[static_cast<size_t>(l) + 1];
     // extend-add: parent columns in chunks, only for supernodes with children
-    S.ea_range[static_cast<size_t>(l)].begin = static_cast<int64_t>(S.ea_tasks.size() / 3);
+    S.ea_range[static_cast<size_t>(l)].begin = static_cast<int64_t>(S.ea_tasks.size() / 4);
     for (int q = qb; q < qe; ++q) {
       const int s = S.level_sn[static_cast<size_t>(q)];
       const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
@@ -289,13 +309,22 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
         continue;
       }
       for (int c = 0; c < r.F; c += kEaCols) {
+        const int chi = std::min(r.F, c + kEaCols);
         S.ea_tasks.push_back(s);
         S.ea_tasks.push_back(c);
-        S.ea_tasks.push_back(std::min(r.F, c + kEaCols));
+        S.ea_tasks.push_back(chi);
+        S.ea_tasks.push_back(static_cast<int32_t>(S.ea_child.size()));
+        // per child: the range of its update columns that land in [c, chi)
+        for (int ci = 0; ci < r.child_count; ++ci) {
+          const SupernodeRec& ch = S.sn[static_cast<size_t>(S.child_list[static_cast<size_t>(r.child_begin + ci)])];
+          const int32_t* rel = S.sn_rel.data() + ch.rows_off;
+          S.ea_child.push_back(static_cast<int32_t>(std::lower_bound(rel, rel + ch.nrows, c) - rel));
+          S.ea_child.push_back(static_cast<int32_t>(std::lower_bound(rel, rel + ch.nrows, chi) - rel));
+        }
       }
     }
     S.ea_range[static_cast<size_t>(l)].count =
-        static_cast<int64_t>(S.ea_tasks.size() / 3) - S.ea_range[static_cast<size_t>(l)].begin;
+        static_cast<int64_t>(S.ea_tasks.size() / 4) - S.ea_range[static_cast<size_t>(l)].begin;
     for (int t = 0; t < S.level_panels[static_cast<size_t>(l)]; ++t) {
       const size_t slot = static_cast<size_t>(S.panel_index_base[static_cast<size_t>(l)] + t);
       S.panel_range[slot].begin = static_cast<int64_t>(S.panel_tasks.size() / 3);
@@ -361,238 +390,444 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
 
 }  // namespace
 
-Symbolic Analyze(const std::vector<HostProblem>& problems, const std::vector<InstanceLayout>& layout,
-                 int panel_width, int tile) {
+SymPiece AnalyzeInstance(const HostProblem& hp, int margin) {
   // The per-pose coupling sets are derived from the current cells of every
-  // point row, dilated by the margin below (in cells).
-  constexpr int kMargin = 2;
-  Symbolic S;
-  int n = 0;
-  for (const HostProblem& hp : problems) {
-    n += hp.num_params();
-  }
+  // point row, dilated by `margin` cells.
+  SymPiece piece;
+  piece.margin = margin;
+  Symbolic& S = piece.s;
+  std::vector<int>& height = piece.height;
+  const int n = hp.num_params();
   S.n = n;
   S.perm.assign(static_cast<size_t>(n), 0);
   S.pinv.assign(static_cast<size_t>(n), 0);
   S.col_owner.assign(static_cast<size_t>(n), -1);
-  std::vector<int> height;
   S.mm_off.assign(static_cast<size_t>(n) * 9, -1);
   S.mp_ptr.assign(static_cast<size_t>(n) + 1, 0);
-  S.mp_frame.clear();
-  S.mp_off.clear();
-  S.allow_off.assign(problems.size(), 0);
-  S.allow_words.assign(problems.size(), 0);
-  std::vector<std::vector<int>> mp_frames_by_col(static_cast<size_t>(n));
-  std::vector<std::vector<int64_t>> mp_offs_by_col(static_cast<size_t>(n));
-  S.pp_base.assign(problems.size(), -1);
-  S.pp_ld.assign(problems.size(), 0);
-  S.pp_first.assign(problems.size(), 0);
-  for (size_t i = 0; i < problems.size(); ++i) {
-    (void)layout;
-    const HostProblem& hp = problems[i];
-    const int A = hp.num_active();
-    const int Fr = hp.num_frames();
-    const int np = hp.num_params();
-    const int col_off = layout[i].col_off;
-    // 1. partition and permutation (local)
-    std::vector<std::vector<int>> groups;
-    Dissect(hp, 0, hp.nx, 0, hp.ny, groups);
-    std::vector<int> lperm;
-    std::vector<int> sn_begin{0};
-    for (const auto& g : groups) {
-      lperm.insert(lperm.end(), g.begin(), g.end());
-      sn_begin.push_back(static_cast<int>(lperm.size()));
+  S.allow_off.assign(1, 0);
+  S.allow_words.assign(1, 0);
+  S.pp_base.assign(1, -1);
+  S.pp_ld.assign(1, 0);
+  S.pp_first.assign(1, 0);
+  const int A = hp.num_active();
+  const int Fr = hp.num_frames();
+  const int np = hp.num_params();
+  const int col_off = 0;
+  // 1. partition and permutation (local)
+  std::vector<std::vector<int>> groups;
+  Dissect(hp, 0, hp.nx, 0, hp.ny, groups);
+  std::vector<int> lperm;
+  std::vector<int> sn_begin{0};
+  for (const auto& g : groups) {
+    lperm.insert(lperm.end(), g.begin(), g.end());
+    sn_begin.push_back(static_cast<int>(lperm.size()));
+  }
+  if (static_cast<int>(lperm.size()) != A) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT, "nested dissection lost active nodes");
+  }
+  if (Fr > 1) {
+    for (int c = A; c < np; ++c) {
+      lperm.push_back(c);
     }
-    if (static_cast<int>(lperm.size()) != A) {
-      Fail(SDFGPU_ERR_INVALID_ARGUMENT, "nested dissection lost active nodes");
+    sn_begin.push_back(np);
+  }
+  std::vector<int> lpinv(static_cast<size_t>(np));
+  for (int k = 0; k < np; ++k) {
+    lpinv[static_cast<size_t>(lperm[static_cast<size_t>(k)])] = k;
+    S.perm[static_cast<size_t>(col_off + k)] = col_off + lperm[static_cast<size_t>(k)];
+    S.pinv[static_cast<size_t>(col_off + lperm[static_cast<size_t>(k)])] = col_off + k;
+  }
+  // 2. pose coupling: frames coupled to each active node (ascending). The
+  // points of each frame (in any order in the caller's specs) give the cells
+  // they occupy; that set dilated by `margin` cells is the frame's allowed
+  // set (one bitmap row per frame), and the corner nodes of the allowed
+  // cells are coupled to the frame. Frames are processed in parallel.
+  // node_frames as CSR over active columns: nf_ptr[c]..nf_ptr[c + 1] in nf
+  std::vector<int64_t> nf_ptr(static_cast<size_t>(A) + 1, 0);
+  std::vector<int32_t> nf;
+  {
+    const int cw = hp.nx - 1;
+    const int chh = hp.ny - 1;
+    const int words = (cw * chh + 31) / 32;
+    S.allow_off[0] = 0;
+    S.allow_words[0] = words;
+    S.allow_bits.assign(static_cast<size_t>(words) * Fr, 0u);
+    std::vector<int> fptr(static_cast<size_t>(Fr) + 1, 0);
+    for (const int32_t f : hp.pt_frame) {
+      ++fptr[static_cast<size_t>(f) + 1];
     }
-    if (Fr > 1) {
-      for (int c = A; c < np; ++c) {
-        lperm.push_back(c);
-      }
-      sn_begin.push_back(np);
+    for (int f = 0; f < Fr; ++f) {
+      fptr[static_cast<size_t>(f) + 1] += fptr[static_cast<size_t>(f)];
     }
-    std::vector<int> lpinv(static_cast<size_t>(np));
-    for (int k = 0; k < np; ++k) {
-      lpinv[static_cast<size_t>(lperm[static_cast<size_t>(k)])] = k;
-      S.perm[static_cast<size_t>(col_off + k)] = col_off + lperm[static_cast<size_t>(k)];
-      S.pinv[static_cast<size_t>(col_off + lperm[static_cast<size_t>(k)])] = col_off + k;
-    }
-    // 2. pose coupling: frames coupled to each active node (sorted)
-    std::vector<std::vector<int>> node_frames(static_cast<size_t>(A));
+    std::vector<int> fpts(hp.pt_frame.size());
     {
-      const int cw = hp.nx - 1;
-      const int chh = hp.ny - 1;
-      const int words = (cw * chh + 31) / 32;
-      S.allow_off[i] = static_cast<int64_t>(S.allow_bits.size());
-      S.allow_words[i] = words;
-      S.allow_bits.resize(S.allow_bits.size() + static_cast<size_t>(words) * Fr, 0u);
-      uint32_t* allow = S.allow_bits.data() + S.allow_off[i];
+      std::vector<int> fill(fptr.begin(), fptr.end() - 1);
+      for (size_t q = 0; q < hp.pt_frame.size(); ++q) {
+        fpts[static_cast<size_t>(fill[static_cast<size_t>(hp.pt_frame[q])]++)] = static_cast<int>(q);
+      }
+    }
+    std::vector<std::vector<int32_t>> frame_cols(static_cast<size_t>(Fr));
+    const double dxg = hp.dx();
+    const double dyg = hp.dy();
+    auto frame_work = [&](int f0, int f1) {
       std::vector<int> stamp(static_cast<size_t>(cw) * chh, -1);
+      std::vector<int> node_stamp(static_cast<size_t>(hp.nx) * hp.ny, -1);
+      std::vector<int> base;
       std::vector<int> cells;
-      const double dxg = hp.dx();
-      const double dyg = hp.dy();
-      int s = 0;
-      for (int f = 0; f < Fr; ++f) {
-        cells.clear();
+      for (int f = std::max(f0, 1); f < f1; ++f) {
         const double* pose = &hp.poses[3 * static_cast<size_t>(f)];
         const double c = std::cos(pose[2]);
         const double sn = std::sin(pose[2]);
-        for (; s < hp.num_points() && hp.pt_frame[static_cast<size_t>(s)] == f; ++s) {
-          const double px = hp.pt_xy[2 * static_cast<size_t>(s)];
-          const double py = hp.pt_xy[2 * static_cast<size_t>(s) + 1];
+        base.clear();
+        for (int q = fptr[static_cast<size_t>(f)]; q < fptr[static_cast<size_t>(f) + 1]; ++q) {
+          const size_t pt = static_cast<size_t>(fpts[static_cast<size_t>(q)]);
+          const double px = hp.pt_xy[2 * pt];
+          const double py = hp.pt_xy[2 * pt + 1];
           const double gx = (c * px + (-sn) * py) + pose[0];
           const double gy = (sn * px + c * py) + pose[1];
           const double fx = (gx - hp.min_x) / dxg;
           const double fy = (gy - hp.min_y) / dyg;
-          if (!(fx >= -kMargin) || !(fy >= -kMargin) || !(fx <= hp.nx - 1 + kMargin) || !(fy <= hp.ny - 1 + kMargin)) {
+          if (!(fx >= -margin) || !(fy >= -margin) || !(fx <= hp.nx - 1 + margin) || !(fy <= hp.ny - 1 + margin)) {
             continue;
           }
           const int w = std::clamp(static_cast<int>(std::floor(fx)), 0, cw - 1);
           const int h = std::clamp(static_cast<int>(std::floor(fy)), 0, chh - 1);
-          for (int hh = std::max(0, h - kMargin); hh <= std::min(chh - 1, h + kMargin); ++hh) {
-            for (int ww = std::max(0, w - kMargin); ww <= std::min(cw - 1, w + kMargin); ++ww) {
-              const int cell = hh * cw + ww;
-              if (stamp[static_cast<size_t>(cell)] != f) {
-                stamp[static_cast<size_t>(cell)] = f;
-                cells.push_back(cell);
+          const int cell = h * cw + w;
+          if (stamp[static_cast<size_t>(cell)] != 2 * f) {
+            stamp[static_cast<size_t>(cell)] = 2 * f;
+            base.push_back(cell);
+          }
+        }
+        // dilation of the occupied cells
+        cells.clear();
+        uint32_t* allow = S.allow_bits.data() + static_cast<size_t>(f) * words;
+        for (const int cell : base) {
+          const int w = cell % cw;
+          const int h = cell / cw;
+          for (int hh = std::max(0, h - margin); hh <= std::min(chh - 1, h + margin); ++hh) {
+            for (int ww = std::max(0, w - margin); ww <= std::min(cw - 1, w + margin); ++ww) {
+              const int d = hh * cw + ww;
+              const uint32_t bit = 1u << (d & 31);
+              if ((allow[d >> 5] & bit) == 0u) {
+                allow[d >> 5] |= bit;
+                cells.push_back(d);
               }
             }
           }
         }
-        if (f == 0) {
-          continue;
-        }
-        for (const int cell : cells) {
-          allow[static_cast<size_t>(f) * words + static_cast<size_t>(cell >> 5)] |= 1u << (cell & 31);
-        }
-        // nodes of the coupled cells
+        // active corner nodes of the allowed cells
+        std::vector<int32_t>& cols = frame_cols[static_cast<size_t>(f)];
         for (const int cell : cells) {
           const int ww = cell % cw;
           const int hh = cell / cw;
           for (int q = 0; q < 4; ++q) {
             const int node = (hh + (q >> 1)) * hp.nx + ww + (q & 1);
             const int col = hp.node_to_active[static_cast<size_t>(node)];
-            if (col >= 0) {
-              auto& v = node_frames[static_cast<size_t>(col)];
-              if (v.empty() || v.back() != f) {
-                v.push_back(f);
-              }
+            if (col >= 0 && node_stamp[static_cast<size_t>(node)] != f) {
+              node_stamp[static_cast<size_t>(node)] = f;
+              cols.push_back(col);
             }
-          }
-        }
-      }
-      // the point specs of a frame need not be contiguous in a caller's desc
-      for (auto& v : node_frames) {
-        std::sort(v.begin(), v.end());
-        v.erase(std::unique(v.begin(), v.end()), v.end());
-      }
-    }
-    // pose pairs linked by odometry / relation rows
-    std::vector<std::vector<int>> frame_links(static_cast<size_t>(Fr));
-    for (int o = 0; o < hp.num_odom(); ++o) {
-      const int fi = hp.odom_ij[2 * static_cast<size_t>(o)];
-      const int fj = hp.odom_ij[2 * static_cast<size_t>(o) + 1];
-      if (fi >= 1 && fj >= 1) {
-        frame_links[static_cast<size_t>(std::min(fi, fj))].push_back(std::max(fi, fj));
-      }
-    }
-    // 3. lower pattern in local permuted order
-    auto lower = [&](int pc, std::vector<int>& out) {
-      const int c = lperm[static_cast<size_t>(pc)];
-      if (c < A) {
-        const int node = hp.active_to_node[static_cast<size_t>(c)];
-        const int w = node % hp.nx;
-        const int h = node / hp.nx;
-        for (int dh = -1; dh <= 1; ++dh) {
-          for (int dw = -1; dw <= 1; ++dw) {
-            const int ww = w + dw;
-            const int hh = h + dh;
-            if (ww < 0 || hh < 0 || ww >= hp.nx || hh >= hp.ny) {
-              continue;
-            }
-            const int c2 = hp.node_to_active[static_cast<size_t>(hh) * hp.nx + ww];
-            if (c2 >= 0 && lpinv[static_cast<size_t>(c2)] > pc) {
-              out.push_back(lpinv[static_cast<size_t>(c2)]);
-            }
-          }
-        }
-        for (const int f : node_frames[static_cast<size_t>(c)]) {
-          for (int a = 0; a < 3; ++a) {
-            out.push_back(A + 3 * (f - 1) + a);
-          }
-        }
-      } else {
-        const int f = (c - A) / 3 + 1;
-        for (int a = (c - A) % 3 + 1; a < 3; ++a) {
-          out.push_back(A + 3 * (f - 1) + a);
-        }
-        for (const int g : frame_links[static_cast<size_t>(f)]) {
-          for (int a = 0; a < 3; ++a) {
-            out.push_back(A + 3 * (g - 1) + a);
           }
         }
       }
     };
-    const LocalSym L = SupernodalSymbolic(np, lower, sn_begin);
-    const int S0 = static_cast<int>(S.sn.size());
-    AppendInstance(S, L, col_off, static_cast<int>(i), height);
-    // 4. assembly offsets for this instance
+    const int workers =
+        std::clamp(static_cast<int>(std::thread::hardware_concurrency()), 1, std::max(1, (Fr + 7) / 8));
+    if (workers <= 1) {
+      frame_work(0, Fr);
+    } else {
+      std::vector<std::thread> pool;
+      const int per = (Fr + workers - 1) / workers;
+      for (int w = 1; w < workers; ++w) {
+        const int f0 = w * per;
+        const int f1 = std::min(Fr, f0 + per);
+        if (f0 < f1) {
+          pool.emplace_back(frame_work, f0, f1);
+        }
+      }
+      frame_work(0, std::min(Fr, per));
+      for (std::thread& t : pool) {
+        t.join();
+      }
+    }
+    // CSR by column; frames enter in ascending order
+    for (int f = 1; f < Fr; ++f) {
+      for (const int32_t col : frame_cols[static_cast<size_t>(f)]) {
+        ++nf_ptr[static_cast<size_t>(col) + 1];
+      }
+    }
     for (int c = 0; c < A; ++c) {
-      const int pc = lpinv[static_cast<size_t>(c)];
-      const int s = S.col_owner[static_cast<size_t>(col_off + pc)];
-      const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
-      const int32_t* rows = S.sn_rows.data() + r.rows_off;
+      nf_ptr[static_cast<size_t>(c) + 1] += nf_ptr[static_cast<size_t>(c)];
+    }
+    nf.resize(static_cast<size_t>(nf_ptr[static_cast<size_t>(A)]));
+    std::vector<int64_t> fill(nf_ptr.begin(), nf_ptr.end() - 1);
+    for (int f = 1; f < Fr; ++f) {
+      for (const int32_t col : frame_cols[static_cast<size_t>(f)]) {
+        nf[static_cast<size_t>(fill[static_cast<size_t>(col)]++)] = f;
+      }
+    }
+  }
+  // pose pairs linked by odometry / relation rows
+  std::vector<std::vector<int>> frame_links(static_cast<size_t>(Fr));
+  for (int o = 0; o < hp.num_odom(); ++o) {
+    const int fi = hp.odom_ij[2 * static_cast<size_t>(o)];
+    const int fj = hp.odom_ij[2 * static_cast<size_t>(o) + 1];
+    if (fi >= 1 && fj >= 1) {
+      frame_links[static_cast<size_t>(std::min(fi, fj))].push_back(std::max(fi, fj));
+    }
+  }
+  // 3. lower pattern in local permuted order
+  auto lower = [&](int pc, std::vector<int>& out) {
+    const int c = lperm[static_cast<size_t>(pc)];
+    if (c < A) {
       const int node = hp.active_to_node[static_cast<size_t>(c)];
       const int w = node % hp.nx;
       const int h = node / hp.nx;
-      const int64_t col_base = r.front_off + static_cast<int64_t>(col_off + pc - r.first_col) * r.F;
       for (int dh = -1; dh <= 1; ++dh) {
         for (int dw = -1; dw <= 1; ++dw) {
-          const int slot = (dh + 1) * 3 + (dw + 1);
           const int ww = w + dw;
           const int hh = h + dh;
           if (ww < 0 || hh < 0 || ww >= hp.nx || hh >= hp.ny) {
             continue;
           }
           const int c2 = hp.node_to_active[static_cast<size_t>(hh) * hp.nx + ww];
-          if (c2 < 0) {
-            continue;
+          if (c2 >= 0 && lpinv[static_cast<size_t>(c2)] > pc) {
+            out.push_back(lpinv[static_cast<size_t>(c2)]);
           }
-          const int pc2 = lpinv[static_cast<size_t>(c2)];
-          if (pc2 < pc) {
-            continue;  // stored in the neighbour's column
-          }
-          S.mm_off[static_cast<size_t>(col_off + c) * 9 + static_cast<size_t>(slot)] =
-              col_base + LocalIndex(r, rows, col_off + pc2);
         }
       }
-      for (const int f : node_frames[static_cast<size_t>(c)]) {
-        mp_frames_by_col[static_cast<size_t>(col_off + c)].push_back(f);
-        mp_offs_by_col[static_cast<size_t>(col_off + c)].push_back(
-            col_base + LocalIndex(r, rows, col_off + A + 3 * (f - 1)));
+      for (int64_t e = nf_ptr[static_cast<size_t>(c)]; e < nf_ptr[static_cast<size_t>(c) + 1]; ++e) {
+        const int f = nf[static_cast<size_t>(e)];
+        for (int a = 0; a < 3; ++a) {
+          out.push_back(A + 3 * (f - 1) + a);
+        }
+      }
+    } else {
+      const int f = (c - A) / 3 + 1;
+      for (int a = (c - A) % 3 + 1; a < 3; ++a) {
+        out.push_back(A + 3 * (f - 1) + a);
+      }
+      for (const int g : frame_links[static_cast<size_t>(f)]) {
+        for (int a = 0; a < 3; ++a) {
+          out.push_back(A + 3 * (g - 1) + a);
+        }
       }
     }
-    (void)S0;
-    // pose root
-    if (Fr > 1) {
-      const int s = S.col_owner[static_cast<size_t>(col_off + A)];
-      const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
-      S.pp_base[i] = r.front_off;
-      S.pp_ld[i] = r.F;
-      S.pp_first[i] = col_off + A - r.first_col;
+  };
+  const LocalSym L = SupernodalSymbolic(np, lower, sn_begin);
+  AppendInstance(S, L, col_off, 0, height);
+  // 4. assembly offsets for this instance: 9 stencil slots per node column
+  // and one (node, frame) entry per coupled frame, found by walking the
+  // front's sorted rows (the frames' pose rows ascend with the frame)
+  for (int c = 0; c < n; ++c) {
+    S.mp_ptr[static_cast<size_t>(c) + 1] = nf_ptr[static_cast<size_t>(std::min(c + 1, A))];
+  }
+  S.mp_frame.assign(nf.begin(), nf.end());
+  S.mp_off.resize(S.mp_frame.size());
+  for (int c = 0; c < A; ++c) {
+    const int pc = lpinv[static_cast<size_t>(c)];
+    const int s = S.col_owner[static_cast<size_t>(col_off + pc)];
+    const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
+    const int32_t* rows = S.sn_rows.data() + r.rows_off;
+    const int node = hp.active_to_node[static_cast<size_t>(c)];
+    const int w = node % hp.nx;
+    const int h = node / hp.nx;
+    const int64_t col_base = r.front_off + static_cast<int64_t>(col_off + pc - r.first_col) * r.F;
+    for (int dh = -1; dh <= 1; ++dh) {
+      for (int dw = -1; dw <= 1; ++dw) {
+        const int slot = (dh + 1) * 3 + (dw + 1);
+        const int ww = w + dw;
+        const int hh = h + dh;
+        if (ww < 0 || hh < 0 || ww >= hp.nx || hh >= hp.ny) {
+          continue;
+        }
+        const int c2 = hp.node_to_active[static_cast<size_t>(hh) * hp.nx + ww];
+        if (c2 < 0) {
+          continue;
+        }
+        const int pc2 = lpinv[static_cast<size_t>(c2)];
+        if (pc2 < pc) {
+          continue;  // stored in the neighbour's column
+        }
+        S.mm_off[static_cast<size_t>(col_off + c) * 9 + static_cast<size_t>(slot)] =
+            col_base + LocalIndex(r, rows, col_off + pc2);
+      }
+    }
+    // pose rows lie below the pivot block of a grid supernode; the frames
+    // ascend, so each search starts where the previous one ended
+    const int32_t* q = rows;
+    for (int64_t e = nf_ptr[static_cast<size_t>(c)]; e < nf_ptr[static_cast<size_t>(c) + 1]; ++e) {
+      const int32_t target = col_off + A + 3 * (nf[static_cast<size_t>(e)] - 1);
+      q = std::lower_bound(q, rows + r.nrows, target);
+      if (q == rows + r.nrows || *q != target) {
+        Fail(SDFGPU_ERR_CUDA, "pose row missing from a node's front");
+      }
+      S.mp_off[static_cast<size_t>(e)] = col_base + r.ncols + (q - rows);
     }
   }
-  for (int c = 0; c < n; ++c) {
-    S.mp_ptr[static_cast<size_t>(c) + 1] =
-        S.mp_ptr[static_cast<size_t>(c)] + static_cast<int64_t>(mp_frames_by_col[static_cast<size_t>(c)].size());
-    S.mp_frame.insert(S.mp_frame.end(), mp_frames_by_col[static_cast<size_t>(c)].begin(),
-                      mp_frames_by_col[static_cast<size_t>(c)].end());
-    S.mp_off.insert(S.mp_off.end(), mp_offs_by_col[static_cast<size_t>(c)].begin(),
-                    mp_offs_by_col[static_cast<size_t>(c)].end());
+  // pose root
+  if (Fr > 1) {
+    const int s = S.col_owner[static_cast<size_t>(col_off + A)];
+    const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
+    S.pp_base[0] = r.front_off;
+    S.pp_ld[0] = r.F;
+    S.pp_first[0] = col_off + A - r.first_col;
+  }
+  ComputeRel(S);
+  return piece;
+}
+
+Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<InstanceLayout>& layout,
+                     int panel_width, int tile) {
+  Symbolic S;
+  int n = 0;
+  size_t nsn = 0;
+  size_t nrows = 0;
+  size_t nchild = 0;
+  size_t nmp = 0;
+  size_t nallow = 0;
+  for (const SymPiece& p : pieces) {
+    n += p.s.n;
+    nsn += p.s.sn.size();
+    nrows += p.s.sn_rows.size();
+    nchild += p.s.child_list.size();
+    nmp += p.s.mp_frame.size();
+    nallow += p.s.allow_bits.size();
+  }
+  const size_t I = pieces.size();
+  S.n = n;
+  S.perm.resize(static_cast<size_t>(n));
+  S.pinv.resize(static_cast<size_t>(n));
+  S.col_owner.resize(static_cast<size_t>(n));
+  S.sn.reserve(nsn);
+  S.sn_rows.reserve(nrows);
+  S.sn_rel.reserve(nrows);
+  S.child_list.reserve(nchild);
+  S.mm_off.resize(static_cast<size_t>(n) * 9);
+  S.mp_ptr.assign(static_cast<size_t>(n) + 1, 0);
+  S.mp_frame.reserve(nmp);
+  S.mp_off.reserve(nmp);
+  S.allow_bits.reserve(nallow);
+  S.allow_off.assign(I, 0);
+  S.allow_words.assign(I, 0);
+  S.pp_base.assign(I, -1);
+  S.pp_ld.assign(I, 0);
+  S.pp_first.assign(I, 0);
+  std::vector<int> height;
+  height.reserve(nsn);
+  for (size_t i = 0; i < I; ++i) {
+    const Symbolic& L = pieces[i].s;
+    const int col_off = layout[i].col_off;
+    const int32_t s0 = static_cast<int32_t>(S.sn.size());
+    const int64_t f0 = S.front_doubles;
+    const int64_t u0 = S.update_doubles;
+    const int64_t r0 = static_cast<int64_t>(S.sn_rows.size());
+    const int32_t c0 = static_cast<int32_t>(S.child_list.size());
+    for (int k = 0; k < L.n; ++k) {
+      S.perm[static_cast<size_t>(col_off + k)] = col_off + L.perm[static_cast<size_t>(k)];
+      S.pinv[static_cast<size_t>(col_off + k)] = col_off + L.pinv[static_cast<size_t>(k)];
+      S.col_owner[static_cast<size_t>(col_off + k)] = s0 + L.col_owner[static_cast<size_t>(k)];
+    }
+    for (SupernodeRec r : L.sn) {
+      r.front_off += f0;
+      r.rows_off += r0;
+      r.upd_off += u0;
+      r.first_col += col_off;
+      r.child_begin += c0;
+      r.parent = r.parent >= 0 ? r.parent + s0 : -1;
+      r.instance = static_cast<int32_t>(i);
+      S.sn.push_back(r);
+    }
+    for (const int32_t row : L.sn_rows) {
+      S.sn_rows.push_back(col_off + row);
+    }
+    S.sn_rel.insert(S.sn_rel.end(), L.sn_rel.begin(), L.sn_rel.end());
+    for (const int32_t c : L.child_list) {
+      S.child_list.push_back(s0 + c);
+    }
+    height.insert(height.end(), pieces[i].height.begin(), pieces[i].height.end());
+    S.front_doubles += L.front_doubles;
+    S.update_doubles += L.update_doubles;
+    S.total_flops += L.total_flops;
+    for (size_t q = 0; q < L.mm_off.size(); ++q) {
+      const int64_t v = L.mm_off[q];
+      S.mm_off[static_cast<size_t>(col_off) * 9 + q] = v >= 0 ? v + f0 : -1;
+    }
+    const int64_t m0 = static_cast<int64_t>(S.mp_frame.size());
+    for (int k = 0; k < L.n; ++k) {
+      S.mp_ptr[static_cast<size_t>(col_off + k) + 1] = m0 + L.mp_ptr[static_cast<size_t>(k) + 1];
+    }
+    S.mp_frame.insert(S.mp_frame.end(), L.mp_frame.begin(), L.mp_frame.end());
+    for (const int64_t v : L.mp_off) {
+      S.mp_off.push_back(v + f0);
+    }
+    S.allow_off[i] = static_cast<int64_t>(S.allow_bits.size());
+    S.allow_words[i] = L.allow_words[0];
+    S.allow_bits.insert(S.allow_bits.end(), L.allow_bits.begin(), L.allow_bits.end());
+    S.pp_base[i] = L.pp_base[0] >= 0 ? L.pp_base[0] + f0 : -1;
+    S.pp_ld[i] = L.pp_ld[0];
+    S.pp_first[i] = L.pp_first[0];
   }
   Finalize(S, height, panel_width, tile);
   return S;
+}
+
+Symbolic Analyze(const std::vector<HostProblem>& problems, const std::vector<InstanceLayout>& layout,
+                 int panel_width, int tile) {
+  std::vector<SymPiece> pieces(problems.size());
+  AnalyzeInstances(problems, std::vector<int>(problems.size(), kDefaultMargin), pieces, nullptr);
+  return Concatenate(pieces, layout, panel_width, tile);
+}
+
+void AnalyzeInstances(const std::vector<HostProblem>& problems, const std::vector<int>& margin,
+                      std::vector<SymPiece>& pieces, const std::vector<int>* which) {
+  std::vector<int> todo;
+  if (which != nullptr) {
+    todo = *which;
+  } else {
+    todo.resize(problems.size());
+    std::iota(todo.begin(), todo.end(), 0);
+  }
+  const int workers = std::min<int>(static_cast<int>(todo.size()),
+                                    std::max(1, static_cast<int>(std::thread::hardware_concurrency())));
+  if (workers <= 1) {
+    for (const int i : todo) {
+      pieces[static_cast<size_t>(i)] = AnalyzeInstance(problems[static_cast<size_t>(i)], margin[static_cast<size_t>(i)]);
+    }
+    return;
+  }
+  std::atomic<size_t> next{0};
+  std::exception_ptr error;
+  std::mutex error_mu;
+  auto work = [&]() {
+    for (;;) {
+      const size_t q = next.fetch_add(1);
+      if (q >= todo.size()) {
+        return;
+      }
+      const int i = todo[q];
+      try {
+        pieces[static_cast<size_t>(i)] =
+            AnalyzeInstance(problems[static_cast<size_t>(i)], margin[static_cast<size_t>(i)]);
+      } catch (...) {
+        const std::lock_guard<std::mutex> lock(error_mu);
+        if (!error) {
+          error = std::current_exception();
+        }
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int w = 1; w < workers; ++w) {
+    pool.emplace_back(work);
+  }
+  work();
+  for (std::thread& t : pool) {
+    t.join();
+  }
+  if (error) {
+    std::rethrow_exception(error);
+  }
 }
 
 Symbolic AnalyzeGeneral(int n, const int32_t* outer, const int32_t* inner, const std::vector<int32_t>& perm_in,
@@ -656,6 +891,7 @@ Symbolic AnalyzeGeneral(int n, const int32_t* outer, const int32_t* inner, const
   const LocalSym L = SupernodalSymbolic(n, lower, sn_begin);
   std::vector<int> height;
   AppendInstance(S, L, 0, 0, height);
+  ComputeRel(S);
   value_offsets.assign(static_cast<size_t>(outer[n]), -1);
   for (int j = 0; j < n; ++j) {
     for (int p = outer[j]; p < outer[j + 1]; ++p) {

@@ -193,6 +193,40 @@ def test_batch_matches_individual_solves():
         assert np.array_equal(bm, sm) and np.array_equal(bp, sp)
 
 
+def test_state_outside_pattern_reanalyses_only_that_instance():
+    # Poses moved by set_state leave the analysed coupling pattern: the cost
+    # evaluation that opens the solve sees it and that instance alone is
+    # re-analysed (with a wider margin) before its first linearization.
+    scs = [scenes.room_scene(seed=s, grid=g, frames=f, beams=b)
+           for s, g, f, b in [(20, 44, 9, 120), (21, 48, 11, 150), (22, 40, 8, 90)]]
+    specs = [scene_specs(sc, P.ProblemOptions(hallucination_points=3))[0] for sc in scs]
+    batch = P.Problem.batch(specs)
+    m1, p1 = batch.state(1)
+    moved = p1.copy()
+    moved[1:, 0] += 0.9
+    moved[1:, 2] += 0.05
+    batch.set_state(m1, moved, index=1)
+    opts = P.SolverOptions(max_iterations=4)
+    rb = P.solve(batch, [opts] * 3)
+    assert batch.last_profile()["reanalyses"] >= 1
+    for i, s in enumerate(specs):
+        single = P.Problem.from_specs(s)
+        if i == 1:
+            single.set_state(m1, moved)
+        r1 = P.solve(single, opts)
+        assert rb[i].cost_history == r1.cost_history
+        bm, bp = batch.state(i)
+        sm, sp = single.state()
+        assert np.array_equal(bm, sm) and np.array_equal(bp, sp)
+    # the re-analysed solve still follows the oracle
+    orc = oracle_from_specs(specs[1])
+    orc.set_state(m1, moved)
+    ro = orc.solve(max_iterations=4, num_threads=4)
+    hg = np.array(rb[1].cost_history)
+    ho = np.array(ro["cost_history"])
+    assert hg.shape == ho.shape and np.max(np.abs(hg - ho) / np.abs(ho)) <= 1e-8
+
+
 def test_server_results_equal_alone_and_in_mix():
     scs = [scenes.request_scene(seed=100 + i, grid_range=(40, 70), pose_range=(8, 24), iterations=6)
            for i in range(5)]
