@@ -316,6 +316,13 @@ def run_serve(P, args):
             "workload": "room-style requests, grid log-U[40,200] @0.25 m, 10-400 poses, 180 beams"}
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# factor-phase kernels (KFactorFront, KUpdate, KPanel, KExtendAdd) in one LM
+# iteration, from one ncu capture of `profile_run.py floorplan 2`; L2 is not
+# flushed inside that capture, so writes that stay in L2 are not counted.
+FACTOR_TRAFFIC_BYTES = {"floorplan": 104.3e6}
+
+
 def run_gpu(args, dist, world, rank, local):
     import numpy as np
     P = _load_package()
@@ -393,7 +400,8 @@ def run_gpu(args, dist, world, rank, local):
     assemble_bytes = P_rows * (40 + 64 + 4) + P_rows * 4 * 2 * 2 * 2
     roofline_factor = {
         "bound": "tensor", "achieved": flops / per_step[2] / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
-        "frac": flops / per_step[2] / 1e12 / fp64_peak, "traffic": None,
+        "frac": flops / per_step[2] / 1e12 / fp64_peak,
+        "traffic": FACTOR_TRAFFIC_BYTES.get(args.workload),
         "kernel": "multifrontal LDL^T (KPanel + KUpdate + KExtendAdd), FP64",
         "peak_source": "nominal B200 FP64 (no measured FP64 peak on this pool)"}
     roofline_assemble = {
