@@ -253,7 +253,10 @@ def run_reference(args, dist, rank):
 
 def run_batch(P, args, flusher):
     """Uneven independent instances solved together in one engine (every
-    kernel of an iteration covers all of them): aggregate LM iterations/s."""
+    kernel of an iteration covers all of them): aggregate LM iterations/s,
+    plain FP64 and mixed, and the mixed instances' final-cost error against
+    their FP64 solves after the same iterations."""
+    import numpy as np
     import sdf_slam_b200.scenes as scenes
     scs = scenes.batch_scenes(seed=3, count=args.batch_count)
     specs = []
@@ -261,22 +264,65 @@ def run_batch(P, args, flusher):
         opts = P.ProblemOptions(hallucination_points=4, active_region=sc.options["active_region"])
         prob = P.Problem.from_scene(sc, opts)
         specs.append(prob.specs(min_corner=sc.min_corner, max_corner=sc.max_corner))
-    batch = P.Problem.batch(specs)
     count = len(specs)
-    opts1 = [P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=args.precision)] * count
-    for _ in range(2):
-        P.solve(batch, opts1)
-    device = 0.0
+    steps = max(3, min(20, args.steps // 5))
+    out = {"instances": count, "unit": "LM iters/s (all instances)",
+           "point_rows": sum(len(s.pt_frame) for s in specs),
+           "workload": "uneven room-style instances, grid 40-150 @0.25 m, 10-200 poses, 90-360 beams, "
+                       "every other one active-region", "steps": steps}
+    final = {}
+    for precision in ("fp64", "mixed"):
+        batch = P.Problem.batch(specs)
+        opts1 = [P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=precision)] * count
+        for _ in range(2):
+            P.solve(batch, opts1)
+        device = 0.0
+        for _ in range(steps):
+            flusher.flush()
+            P.solve(batch, opts1)
+            device += batch.last_profile()["span"]
+        final[precision] = np.array([batch.cost(i) for i in range(count)])
+        out[precision] = {"value": count * steps / device, "ms_per_batched_iteration": 1000.0 * device / steps}
+        batch.close()
+    out["value"] = out["fp64"]["value"]
+    out["mixed"]["max_final_cost_rel_err_vs_fp64"] = float(
+        np.max(np.abs(final["mixed"] - final["fp64"]) / np.abs(final["fp64"])))
+    return out
+
+
+def run_mixed(P, args, specs, flusher):
+    """The same workload with precision "mixed": LM iterations/s (one-iteration
+    solves, L2 flushed between them) and, after 10 iterations from the same
+    start, the final-cost and pose differences against the FP64 path."""
+    import numpy as np
+    prob = P.Problem.from_specs(specs)
+    opts1 = P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision="mixed",
+                            refine_steps=args.refine_steps)
+    for _ in range(args.warmup):
+        P.solve(prob, opts1)
     steps = max(3, args.steps // 2)
+    device = 0.0
+    phases = np.zeros(5)
     for _ in range(steps):
         flusher.flush()
-        P.solve(batch, opts1)
-        device += batch.last_profile()["span"]
-    rows = sum(len(s.pt_frame) for s in specs)
-    return {"instances": count, "value": count * steps / device, "unit": "LM iters/s (all instances)",
-            "ms_per_batched_iteration": 1000.0 * device / steps, "point_rows": rows,
-            "workload": "uneven room-style instances, grid 40-150 @0.25 m, 10-200 poses, 90-360 beams, "
-                        "every other one active-region"}
+        P.solve(prob, opts1)
+        prof = prob.last_profile()
+        device += prof["span"]
+        phases += [prof["assemble"], prof["normal"], prof["factor"], prof["solve"], prof["update"]]
+    prob.close()
+    res = {}
+    for precision in ("fp64", "mixed"):
+        p = P.Problem.from_specs(specs)
+        r = P.solve(p, P.SolverOptions(max_iterations=10, step_tolerance=0.0, precision=precision,
+                                       refine_steps=args.refine_steps))
+        res[precision] = (r.final_cost, *p.state())
+        p.close()
+    names = ["assemble", "normal", "factor", "solve", "update"]
+    return {"value": steps / device, "unit": "LM iters/s", "refine_steps": args.refine_steps,
+            "phase_ms_per_step": {k: 1000.0 * v / steps for k, v in zip(names, phases)},
+            "final_cost_rel_err_vs_fp64_10_iters": abs(res["mixed"][0] - res["fp64"][0]) / abs(res["fp64"][0]),
+            "max_pose_err_m_vs_fp64_10_iters": float(np.max(np.abs(res["mixed"][2][:, :2] - res["fp64"][2][:, :2]))),
+            "max_map_err_vs_fp64_10_iters": float(np.max(np.abs(res["mixed"][1] - res["fp64"][1])))}
 
 
 def run_serve(P, args):
@@ -377,6 +423,7 @@ def run_gpu(args, dist, world, rank, local):
         e2e_t += time.perf_counter() - t0
         d2h = m.nbytes + poses.nbytes + 8 * len(r.cost_history)
         p2.close()
+    mixed = run_mixed(P, args, specs, flusher) if (world == 1 and not args.no_mixed) else None
     batched = run_batch(P, args, flusher) if (args.batch_count > 0 and world == 1) else None
     flusher.close()
     served = run_serve(P, args) if (args.serve_requests > 0 and world == 1) else None
@@ -433,6 +480,7 @@ def run_gpu(args, dist, world, rank, local):
         "e2e": {"value": e2e_value, "unit": "LM iters/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "iterations_per_step": e2e_iters},
         "clocks": clocks,
+        "mixed": mixed,
         "batched": batched,
         "served": served,
     }
@@ -453,6 +501,8 @@ def main():
     ap.add_argument("--e2e-iterations", type=int, default=10)
     ap.add_argument("--cpu-iterations", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--refine-steps", type=int, default=3)
     ap.add_argument("--batch-count", type=int, default=64)
     ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--serve-rate", type=float, default=100.0)

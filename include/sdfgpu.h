@@ -34,9 +34,10 @@ extern "C" {
 #define SDFGPU_ERR_NOT_READY 6        /* serving: the request has not finished yet */
 
 /* Precision of a solve. FP64 runs every step in double precision (the plain
- * path that matches the reference). MIXED assembles and factors in FP32 and
- * recovers the FP64 step by iterative refinement against a matrix-free FP64
- * J^T J product; cost, gain ratio and acceptance stay FP64. */
+ * path that matches the reference). MIXED factors the grid supernodes in
+ * FP32 (the dense pose-block root stays FP64) and recovers the FP64 step by
+ * refine_steps rounds of iterative refinement against the FP64 normal
+ * matrix; residuals, J^T J, cost, gain ratio and acceptance stay FP64. */
 #define SDFGPU_PRECISION_FP64 0
 #define SDFGPU_PRECISION_MIXED 1
 
@@ -185,6 +186,7 @@ typedef struct sdfgpu_solver_options {
   int32_t trust_region;
   int32_t num_threads; /* accepted for interface parity; unused on the GPU */
   int32_t precision;   /* SDFGPU_PRECISION_* */
+  int32_t refine_steps; /* MIXED: refinement rounds per LM step (0..16) */
 } sdfgpu_solver_options;
 
 typedef struct sdfgpu_solve_result {

@@ -123,6 +123,7 @@ class SolverOptions:
     trust_region: bool = False
     num_threads: int = 0
     precision: str = "fp64"
+    refine_steps: int = 3
 
     def to_c(self) -> _capi.SolverOptionsC:
         if self.backend != "gpu":
@@ -133,7 +134,7 @@ class SolverOptions:
         return _capi.SolverOptionsC(int(self.max_iterations), self.step_tolerance, self.lambda_init,
                                     self.lambda_factor, int(self.reject_worse_steps),
                                     int(self.marquardt_scaling), int(self.trust_region),
-                                    int(self.num_threads), prec)
+                                    int(self.num_threads), prec, int(self.refine_steps))
 
 
 @dataclass

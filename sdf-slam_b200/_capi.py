@@ -63,6 +63,7 @@ class SolverOptionsC(ctypes.Structure):
         ("reject_worse_steps", ctypes.c_int32), ("marquardt_scaling", ctypes.c_int32),
         ("trust_region", ctypes.c_int32), ("num_threads", ctypes.c_int32),
         ("precision", ctypes.c_int32),
+        ("refine_steps", ctypes.c_int32),
     ]
 
 

@@ -29,6 +29,7 @@ SOURCES = {
     "engine.cu": [],
     "ldlt.cu": [],
     "noalloc.cu": [],
+    "refine.cu": [],
     "problem_build.cpp": ["-x", "cu"],
     "symbolic.cpp": ["-x", "cu"],
     "capi.cpp": ["-x", "cu"],

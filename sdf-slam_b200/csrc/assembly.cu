@@ -484,9 +484,9 @@ __global__ void KCellPass(DeviceView V, int pass) {
         if (col[aa] >= 0) {
           const int64_t off = offs[aa];
           if (off >= 0) {
-            V.fronts[off] += v[3 * aa];
-            V.fronts[off + 1] += v[3 * aa + 1];
-            V.fronts[off + 2] += v[3 * aa + 2];
+            V.asm_fronts[off] += v[3 * aa];
+            V.asm_fronts[off + 1] += v[3 * aa + 1];
+            V.asm_fronts[off + 2] += v[3 * aa + 2];
           } else {
             overflow = true;
           }
@@ -513,7 +513,7 @@ __global__ void KCellPass(DeviceView V, int pass) {
         if (lane == q) {
           const int64_t off = PairOffset(V, col, aa, bb);
           if (off >= 0) {
-            V.fronts[off] += mm[q];
+            V.asm_fronts[off] += mm[q];
           }
         }
         ++q;
@@ -537,7 +537,7 @@ __global__ void KCellPass(DeviceView V, int pass) {
       for (int b = a; b < 3; ++b) {
         const int64_t off = PairOffset(V, col, corner[a], corner[b]);
         if (off >= 0) {
-          V.fronts[off] += r[a] * r[b];
+          V.asm_fronts[off] += r[a] * r[b];
         }
       }
       V.rhs[col[corner[a]]] += r[a] * r[3];
@@ -631,7 +631,7 @@ __global__ void __launch_bounds__(256) KPoseFrames(DeviceView V) {
   }
   const int base = I.pp_first + 3 * (fl - 1);
   for (int e = 0; e < 6; ++e) {
-    V.fronts[I.pp_base + static_cast<int64_t>(base + bb[e]) * I.pp_ld + (base + aa[e])] = acc[e];
+    V.asm_fronts[I.pp_base + static_cast<int64_t>(base + bb[e]) * I.pp_ld + (base + aa[e])] = acc[e];
   }
   const int c0 = V.frame_col[f];
   V.rhs[c0] = acc[6];
@@ -660,9 +660,9 @@ __global__ void KFinalizeNormal(DeviceView V) {
     const int rel = I.pp_first + (col - I.col_off - I.num_active);
     off = I.pp_base + static_cast<int64_t>(rel) * I.pp_ld + rel;
   }
-  const double d = V.fronts[off];
+  const double d = V.asm_fronts[off];
   const double lam = V.lam[i];
-  V.fronts[off] = V.marquardt[i] != 0 ? d + lam * fmax(d, 1e-12) : d + lam;
+  V.asm_fronts[off] = V.marquardt[i] != 0 ? d + lam * fmax(d, 1e-12) : d + lam;
 }
 
 /// Cross-frame pose blocks of frame pairs linked by odometry / relation rows.
@@ -696,7 +696,7 @@ __global__ void KPosePairs(DeviceView V) {
   const int gl = g - I.frame_off;
   const int colf = I.pp_first + 3 * (fl - 1) + b;
   const int rowg = I.pp_first + 3 * (gl - 1) + a;
-  V.fronts[I.pp_base + static_cast<int64_t>(colf) * I.pp_ld + rowg] = acc;
+  V.asm_fronts[I.pp_base + static_cast<int64_t>(colf) * I.pp_ld + rowg] = acc;
 }
 
 /// Saves or restores the state of active instances (backup for revert,

@@ -135,6 +135,7 @@ void sdfgpu_solver_options_default(sdfgpu_solver_options* o) {
   o->trust_region = 0;
   o->num_threads = 0;
   o->precision = SDFGPU_PRECISION_FP64;
+  o->refine_steps = 3;
 }
 
 int sdfgpu_problem_build(int32_t nx, int32_t ny, double min_x, double min_y, double max_x, double max_y,
@@ -312,6 +313,9 @@ int sdfgpu_solve(sdfgpu_problem* problem, const sdfgpu_solver_options* options, 
       }
       if (o.precision != SDFGPU_PRECISION_FP64 && o.precision != SDFGPU_PRECISION_MIXED) {
         sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "unknown precision");
+      }
+      if (o.refine_steps < 0 || o.refine_steps > 16) {
+        sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "refine_steps must lie in [0, 16]");
       }
     }
     e.Solve(opts, results, cost_history, capacity > 0 ? capacity : 0);

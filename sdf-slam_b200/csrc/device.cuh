@@ -33,6 +33,7 @@ struct InstDev {
   int64_t pp_base;
   int32_t pp_first;
   int32_t num_params;
+  int32_t mixed;  // 1: this solve factors the grid supernodes in FP32
 };
 
 /// Status bits per instance.
@@ -118,8 +119,20 @@ struct DeviceView {
   const int32_t* mp_frame;
   const int64_t* mp_off;
   const uint32_t* allow_bits;
-  double* fronts;
+  double* fronts;     // factorization work fronts (FP64 supernodes)
+  float* fronts32;    // factorization work fronts of FP32 supernodes (mixed solves), else null
+  double* asm_fronts; // assembly target: the FP64 normal matrix (== fronts when no solve is mixed)
   double* upd;
+  // map-pose entries grouped by frame (transpose of mp_*): per global frame
+  // the node columns coupled to it and the front offset of (pose var 0, node)
+  const int64_t* fmp_ptr;
+  const int32_t* fmp_col;
+  const int64_t* fmp_off;
 };
+
+/// True when supernode S is factored in FP32 (a mixed solve's grid supernode).
+__device__ __forceinline__ bool Fp32Front(const DeviceView& V, const SupernodeRec& S) {
+  return V.fronts32 != nullptr && S.pose_root == 0 && V.inst[S.instance].mixed != 0;
+}
 
 }  // namespace sdfgpu

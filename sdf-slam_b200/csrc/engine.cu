@@ -26,6 +26,11 @@ __global__ void KCostTerms(DeviceView V, double* terms);
 __global__ void KStepTerms(DeviceView V, double* sq, double* pred);
 __global__ void KSegmentPartial(const double* x, const int64_t* seg_begin, const int64_t* seg_end, double* partial);
 __global__ void KSegmentFinal(const double* partial, int num_segments, double* out);
+__global__ void KConvertFronts(DeviceView V, const int32_t* tasks, int chunk);
+__global__ void KNormalMatVecMap(DeviceView V, const double* x, double* y);
+__global__ void KNormalMatVecPose(DeviceView V, const double* x, double* y);
+__global__ void KRefineResidual(DeviceView V, const double* y, double* r);
+__global__ void KAddCorrection(DeviceView V, const double* corr);
 void LaunchCellSort(const int32_t* pt_cell, int64_t n, int64_t num_cells, int32_t* keys_a, int32_t* vals_a,
                     int32_t* keys_b, int32_t* vals_b, int32_t* hist, cudaStream_t stream, bool* result_in_a);
 
@@ -427,8 +432,16 @@ void Engine::UploadSymbolic() {
     d.pp_ld = sym_.pp_ld[i];
     d.pp_first = sym_.pp_first[i];
     d.num_params = host_[i].num_params();
+    d.mixed = i < mixed_.size() ? mixed_[i] : 0;
   }
+  inst_host_ = inst;
   inst_.Upload(inst, s);
+  fmp_ptr_.Upload(sym_.fmp_ptr, s);
+  fmp_col_.Upload(sym_.fmp_col, s);
+  fmp_off_.Upload(sym_.fmp_off, s);
+  if (any_mixed_) {
+    AllocMixed();
+  }
   device_bytes_ = 0;
   device_bytes_ += static_cast<int64_t>(fronts_.size()) * 8 + static_cast<int64_t>(pt_rec_.size()) * 8 +
                    static_cast<int64_t>(mp_off_.size()) * 12 + static_cast<int64_t>(mm_off_.size()) * 8 +
@@ -504,7 +517,50 @@ void Engine::RefreshView() {
   V.mp_off = mp_off_.get();
   V.allow_bits = allow_bits_.get();
   V.fronts = fronts_.get();
+  V.fronts32 = any_mixed_ ? fronts32_.get() : nullptr;
+  V.asm_fronts = any_mixed_ ? amat_.get() : fronts_.get();
   V.upd = upd_.get();
+  V.fmp_ptr = fmp_ptr_.get();
+  V.fmp_col = fmp_col_.get();
+  V.fmp_off = fmp_off_.get();
+}
+
+void Engine::AllocMixed() {
+  amat_.Alloc(static_cast<size_t>(sym_.front_doubles));
+  fronts32_.Alloc(static_cast<size_t>(sym_.front_doubles));
+  std::vector<int32_t> tasks;
+  for (size_t s = 0; s < sym_.sn.size(); ++s) {
+    const int64_t total = static_cast<int64_t>(sym_.sn[s].F) * sym_.sn[s].F;
+    for (int64_t b = 0; b < total; b += kConvertChunk) {
+      tasks.push_back(static_cast<int32_t>(s));
+      tasks.push_back(static_cast<int32_t>(b));
+    }
+  }
+  conv_count_ = static_cast<int64_t>(tasks.size() / 2);
+  conv_tasks_.Upload(tasks, stream_);
+  res_.Alloc(static_cast<size_t>(std::max(n_, 1)));
+  ax_.Alloc(static_cast<size_t>(std::max(n_, 1)));
+  corr_.Alloc(static_cast<size_t>(std::max(n_, 1)));
+}
+
+void Engine::SetMode(const std::vector<int32_t>& mixed, int refine_steps) {
+  if (mixed == mixed_ && refine_steps == refine_steps_) {
+    return;
+  }
+  CudaCheck(cudaStreamSynchronize(stream_), "mode sync");
+  mixed_ = mixed;
+  refine_steps_ = refine_steps;
+  any_mixed_ = std::any_of(mixed_.begin(), mixed_.end(), [](int32_t v) { return v != 0; });
+  for (size_t i = 0; i < inst_host_.size(); ++i) {
+    inst_host_[i].mixed = mixed_[i];
+  }
+  inst_.Upload(inst_host_, stream_);
+  if (any_mixed_) {
+    AllocMixed();
+  }
+  RefreshView();
+  DropGraph();
+  CudaCheck(cudaStreamSynchronize(stream_), "mode upload");
 }
 
 void Engine::SetActive(const std::vector<int32_t>& active) {
@@ -569,7 +625,7 @@ void Engine::LaunchRows() {
 }
 
 void Engine::LaunchNormal() {
-  CudaCheck(cudaMemsetAsync(fronts_.get(), 0, static_cast<size_t>(sym_.front_doubles) * sizeof(double), stream_),
+  CudaCheck(cudaMemsetAsync(V_.asm_fronts, 0, static_cast<size_t>(sym_.front_doubles) * sizeof(double), stream_),
             "front memset");
   CudaCheck(cudaMemsetAsync(rhs_.get(), 0, static_cast<size_t>(n_) * sizeof(double), stream_), "rhs memset");
   if (total_cells_ > 0) {
@@ -610,9 +666,37 @@ FactorPlan Engine::Plan() {
   return P;
 }
 
-void Engine::LaunchFactor() { times_.launches += LaunchFactorLevels(sym_, V_, Plan(), stream_); }
+void Engine::LaunchFactor() {
+  if (any_mixed_ && conv_count_ > 0) {
+    // work copies of the assembled fronts (FP32 for mixed grid supernodes)
+    KConvertFronts<<<static_cast<unsigned>(conv_count_), 256, 0, stream_>>>(V_, conv_tasks_.get(), kConvertChunk);
+    CudaCheck(cudaGetLastError(), "convert fronts");
+    ++times_.launches;
+  }
+  times_.launches += LaunchFactorLevels(sym_, V_, Plan(), stream_);
+}
 
-void Engine::LaunchSolve() { times_.launches += LaunchSolveLevels(sym_, V_, Plan(), stream_); }
+void Engine::LaunchSolve() {
+  times_.launches += LaunchSolveLevels(sym_, V_, Plan(), stream_);
+  if (!any_mixed_ || n_ == 0) {
+    return;
+  }
+  // iterative refinement of the mixed instances' steps against the FP64
+  // normal matrix: r = rhs - A delta, delta += (LDL^T)^-1 r
+  DeviceView Vr = V_;
+  Vr.rhs = res_.get();
+  Vr.step = corr_.get();
+  for (int round = 0; round < refine_steps_; ++round) {
+    KNormalMatVecMap<<<Blocks(n_, 128), 128, 0, stream_>>>(V_, step_.get(), ax_.get());
+    KNormalMatVecPose<<<Blocks(3 * static_cast<int64_t>(total_frames_) * 32, 256), 256, 0, stream_>>>(
+        V_, step_.get(), ax_.get());
+    KRefineResidual<<<Blocks(n_, 256), 256, 0, stream_>>>(V_, ax_.get(), res_.get());
+    times_.launches += 3 + LaunchSolveLevels(sym_, Vr, Plan(), stream_);
+    KAddCorrection<<<Blocks(n_, 256), 256, 0, stream_>>>(V_, corr_.get());
+    ++times_.launches;
+  }
+  CudaCheck(cudaGetLastError(), "refinement kernels");
+}
 
 void Engine::LaunchCost(std::vector<double>& cost) {
   const int64_t terms = total_points_ + total_eik_ + total_odom_;
@@ -676,7 +760,7 @@ void Engine::Reanalyze(const std::vector<int>& which) {
     std::copy(poses.begin() + 3 * L.frame_off, poses.begin() + 3 * (L.frame_off + L.num_frames),
               host_[static_cast<size_t>(i)].poses.begin());
     // a pattern that was left once is widened so that it is left less often
-    margin_[static_cast<size_t>(i)] = std::min(margin_[static_cast<size_t>(i)] + 1, kMaxMargin);
+    margin_[static_cast<size_t>(i)] = std::min(margin_[static_cast<size_t>(i)] + kMarginStep, kMaxMargin);
   }
   AnalyzeInstances(host_, margin_, pieces_, &which);
   sym_ = Concatenate(pieces_, layout_, 32, 64);
@@ -782,6 +866,7 @@ void Engine::ApplyStep(int i, const double* step) {
 
 void Engine::Linearize(int i, double lambda, bool marquardt, bool compute_step) {
   const size_t I = host_.size();
+  SetMode(std::vector<int32_t>(I, 0), 0);
   const HostProblem& hp = host_[static_cast<size_t>(i)];
   const InstanceLayout& L = layout_[static_cast<size_t>(i)];
   std::vector<int32_t> active(I, 0);
@@ -1003,6 +1088,17 @@ void Engine::LinearizationGet(double* residuals, int32_t* point_cell, int32_t* j
 
 void Engine::BeginSolve(const std::vector<sdfgpu_solver_options>& options) {
   const size_t I = host_.size();
+  {
+    std::vector<int32_t> mixed(I, 0);
+    int refine = 0;
+    for (size_t i = 0; i < I; ++i) {
+      if (options[i].precision == SDFGPU_PRECISION_MIXED) {
+        mixed[i] = 1;
+        refine = std::max(refine, options[i].refine_steps);
+      }
+    }
+    SetMode(mixed, refine);
+  }
   t_start_ = std::chrono::steady_clock::now();
   times_ = IterTimes{};
   lm_.assign(I, LmInst{});

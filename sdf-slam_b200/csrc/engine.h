@@ -42,7 +42,13 @@ class DevBuf {
     if (count <= count_ && ptr_ != nullptr) {
       return;
     }
+    // a buffer that has to grow (a re-analysis widened the pattern) gets a
+    // quarter of headroom, so that the next growth reuses it
+    const bool regrow = ptr_ != nullptr;
     Free();
+    if (regrow) {
+      count += count / 4;
+    }
     const size_t bytes = std::max<size_t>(1, count) * sizeof(T);
     const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&ptr_), bytes);
     if (e != cudaSuccess) {
@@ -172,6 +178,11 @@ class Engine {
   /// Copies results and cost histories (rows of `capacity`).
   void EndSolve(sdfgpu_solve_result* results, double* cost_history, int capacity);
   [[nodiscard]] cudaStream_t stream() const { return stream_; }
+  /// True when an instance's state left its pattern and the next
+  /// LaunchIteration would re-analyse it first.
+  [[nodiscard]] bool NeedsReanalysis() const { return !pending_.empty(); }
+  /// Runs that re-analysis now (the serving loop does it off its own thread).
+  void ReanalyzeNow() { ReanalyzePending(); }
   [[nodiscard]] const IterTimes& times() const { return times_; }
   [[nodiscard]] int64_t factor_flops() const { return sym_.total_flops; }
   [[nodiscard]] const Symbolic& symbolic() const { return sym_; }
@@ -181,6 +192,10 @@ class Engine {
   void UploadProblem();
   void Analyze();
   void UploadSymbolic();
+  /// Per-instance precision of the coming solve (1: mixed) and refinement
+  /// rounds; re-uploads flags and drops the graphs when they change.
+  void SetMode(const std::vector<int32_t>& mixed, int refine_steps);
+  void AllocMixed();
   void RefreshView();
   void SetActive(const std::vector<int32_t>& active);
   void SetLambda(const std::vector<double>& lam, const std::vector<int32_t>& marquardt);
@@ -256,6 +271,20 @@ class Engine {
   DevBuf<uint32_t> allow_bits_;
   DevBuf<int32_t> ea_tasks_, ea_child_, panel_tasks_, update_tasks_, small_tasks_;
   DevBuf<double> fronts_, upd_;
+  // mixed precision: assembled FP64 normal matrix, FP32 work fronts, the
+  // conversion tasks and the refinement vectors
+  static constexpr int kConvertChunk = 16384;
+  DevBuf<double> amat_;
+  DevBuf<float> fronts32_;
+  DevBuf<int32_t> conv_tasks_;
+  int64_t conv_count_{0};
+  DevBuf<double> res_, ax_, corr_;
+  DevBuf<int64_t> fmp_ptr_, fmp_off_;
+  DevBuf<int32_t> fmp_col_;
+  std::vector<int32_t> mixed_;
+  int refine_steps_{0};
+  bool any_mixed_{false};
+  std::vector<InstDev> inst_host_;
   int32_t* cell_rows_ptr_{nullptr};
   HostBuf<double> h_seg_;      // 5 per instance: cost parts x3, |delta|^2, prediction
   HostBuf<int32_t> h_status_;

@@ -1,5 +1,8 @@
 // Multifrontal supernodal LDL^T of the damped normal equations and its
-// triangular solves (FP64), level by level over the assembly tree.
+// triangular solves, level by level over the assembly tree. Fronts are FP64;
+// in a mixed-precision solve the grid supernodes are factored in FP32 copies
+// (every kernel picks the element type per supernode) while the dense pose
+// root stays FP64; the solve vectors are always FP64.
 //
 // Replaces ParallelSimplicialLdlt::FactorizeParallel / Eigen's solve
 // (src/solvers/parallel_ldlt.hpp:44-51,150-244; src/solvers/lm_solver.cpp:
@@ -24,10 +27,16 @@ constexpr int kPanel = 32;
 constexpr int kTile = 64;
 constexpr int kPanelRowsPerBlock = 128;
 
-/// L(i, j), i > j, of front s (local indices), honouring the transposed
-/// storage of diagonal panel blocks.
-__device__ __forceinline__ double LoadL(const double* Fs, int F, int i, int j) {
-  return (i / kPanel == j / kPanel) ? Fs[static_cast<int64_t>(i) * F + j] : Fs[static_cast<int64_t>(j) * F + i];
+/// Work front of supernode S in the element type it is factored in.
+template <typename T>
+__device__ __forceinline__ T* WorkFront(const DeviceView& V, const SupernodeRec& S);
+template <>
+__device__ __forceinline__ double* WorkFront<double>(const DeviceView& V, const SupernodeRec& S) {
+  return V.fronts + S.front_off;
+}
+template <>
+__device__ __forceinline__ float* WorkFront<float>(const DeviceView& V, const SupernodeRec& S) {
+  return V.fronts32 + S.front_off;
 }
 
 /// LDL^T of the w x w diagonal block at B (row r, column c at B[r * ld + c],
@@ -35,26 +44,27 @@ __device__ __forceinline__ double LoadL(const double* Fs, int F, int i, int j) {
 /// its registers hold columns j.., so every register index is static while
 /// the step loop stays rolled (a small code footprint). Writes L below the
 /// diagonal and D on it; returns true when a pivot is exactly zero.
-__device__ __noinline__ bool DiagonalBlockLdlt(double* B, int ld, int w) {
+template <typename T>
+__device__ __noinline__ bool DiagonalBlockLdlt(T* B, int ld, int w) {
   const int lane = threadIdx.x & 31;
-  double row[kPanel];
+  T row[kPanel];
 #pragma unroll
   for (int c = 0; c < kPanel; ++c) {
-    row[c] = (lane < w && c <= lane) ? B[lane * ld + c] : (c == lane ? 1.0 : 0.0);
+    row[c] = (lane < w && c <= lane) ? B[lane * ld + c] : (c == lane ? T(1) : T(0));
   }
   bool zero = false;
   for (int j = 0; j < w; ++j) {
-    const double dj = __shfl_sync(0xffffffffu, row[0], j);
-    zero = zero || (dj == 0.0);
-    const double wij = row[0];
-    const double lij = wij / dj;
+    const T dj = __shfl_sync(0xffffffffu, row[0], j);
+    zero = zero || (dj == T(0));
+    const T wij = row[0];
+    const T lij = wij / dj;
     if (lane < w && lane >= j) {
       B[lane * ld + j] = lane == j ? dj : lij;
     }
 #pragma unroll
     for (int c = 1; c < kPanel; ++c) {
       // column j + c: A(i, j + c) -= W(i, j) L(j + c, j) for j < i, j + c <= i
-      const double lcj = __shfl_sync(0xffffffffu, lij, (j + c) & 31);
+      const T lcj = __shfl_sync(0xffffffffu, lij, (j + c) & 31);
       if (lane > j && j + c <= lane) {
         row[c] -= wij * lcj;
       }
@@ -63,9 +73,44 @@ __device__ __noinline__ bool DiagonalBlockLdlt(double* B, int ld, int w) {
     for (int c = 0; c + 1 < kPanel; ++c) {
       row[c] = row[c + 1];
     }
-    row[kPanel - 1] = 0.0;
+    row[kPanel - 1] = T(0);
   }
   return zero;
+}
+
+/// Adds one child's update columns [cbeg, cend) into the parent front.
+template <typename TP, typename TC>
+__device__ __forceinline__ void ExtendAddChild(TP* Fp, int PF, const TC* U, int CF, const int32_t* rel, int m,
+                                               int cbeg, int cend) {
+  const int lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  for (int cc = cbeg + (threadIdx.x >> 5); cc < cend; cc += nwarps) {
+    TP* __restrict__ dst = Fp + static_cast<int64_t>(rel[cc]) * PF;
+    const TC* __restrict__ src = U + static_cast<int64_t>(cc) * CF;
+#pragma unroll 4
+    for (int r = cc + lane; r < m; r += 32) {
+      dst[rel[r]] += static_cast<TP>(src[r]);
+    }
+  }
+}
+
+template <typename TP>
+__device__ __forceinline__ void ExtendAddBody(const DeviceView& V, const SupernodeRec& P, const int32_t* ranges) {
+  TP* Fp = WorkFront<TP>(V, P);
+  for (int ci = 0; ci < P.child_count; ++ci) {
+    const SupernodeRec C = V.sn[V.child_list[P.child_begin + ci]];
+    const int32_t* rel = V.sn_rel + C.rows_off;
+    // update columns of this child that land in the task's parent columns
+    const int cbeg = ranges[2 * ci];
+    const int cend = ranges[2 * ci + 1];
+    const int64_t uoff = static_cast<int64_t>(C.ncols) * C.F + C.ncols;
+    if (Fp32Front(V, C)) {
+      ExtendAddChild<TP, float>(Fp, P.F, WorkFront<float>(V, C) + uoff, C.F, rel, C.nrows, cbeg, cend);
+    } else {
+      ExtendAddChild<TP, double>(Fp, P.F, WorkFront<double>(V, C) + uoff, C.F, rel, C.nrows, cbeg, cend);
+    }
+    __syncthreads();
+  }
 }
 
 /// Adds the children's update matrices into each parent front. A task owns a
@@ -73,76 +118,49 @@ __device__ __noinline__ bool DiagonalBlockLdlt(double* B, int ld, int w) {
 /// are added in their fixed order.
 __global__ void KExtendAdd(DeviceView V, const int32_t* tasks, const int32_t* child_ranges) {
   const int32_t* t = tasks + 4 * static_cast<int64_t>(blockIdx.x);
-  const int p = t[0];
-  const SupernodeRec P = V.sn[p];
+  const SupernodeRec P = V.sn[t[0]];
   if (V.active[P.instance] == 0) {
     return;
   }
-  const int32_t* ranges = child_ranges + t[3];
-  double* Fp = V.fronts + P.front_off;
-  for (int ci = 0; ci < P.child_count; ++ci) {
-    const SupernodeRec C = V.sn[V.child_list[P.child_begin + ci]];
-    const int32_t* rel = V.sn_rel + C.rows_off;
-    const int m = C.nrows;
-    // update columns of this child that land in the task's parent columns
-    const int cbeg = ranges[2 * ci];
-    const int cend = ranges[2 * ci + 1];
-    const double* U = V.fronts + C.front_off + static_cast<int64_t>(C.ncols) * C.F + C.ncols;
-    const int lane = threadIdx.x & 31;
-    const int nwarps = blockDim.x >> 5;
-    for (int cc = cbeg + (threadIdx.x >> 5); cc < cend; cc += nwarps) {
-      double* __restrict__ dst = Fp + static_cast<int64_t>(rel[cc]) * P.F;
-      const double* __restrict__ src = U + static_cast<int64_t>(cc) * C.F;
-#pragma unroll 4
-      for (int r = cc + lane; r < m; r += 32) {
-        dst[rel[r]] += src[r];
-      }
-    }
-    __syncthreads();
+  if (Fp32Front(V, P)) {
+    ExtendAddBody<float>(V, P, child_ranges + t[3]);
+  } else {
+    ExtendAddBody<double>(V, P, child_ranges + t[3]);
   }
 }
 
-/// Panel factorization: LDL^T of the panel's diagonal block (redundantly in
-/// every block of the panel, written back by the first), then
-/// L(r, panel) = A(r, panel) L11^-T D^-1 for a chunk of rows below it.
-__global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const int32_t* tasks, double* dvec) {
-  const int32_t* t = tasks + 3 * static_cast<int64_t>(blockIdx.x);
-  const int s = t[0];
-  const int panel = t[1];
-  const int row_begin = t[2];
-  const SupernodeRec S = V.sn[s];
-  if (V.active[S.instance] == 0) {
-    return;
-  }
+template <typename T>
+__device__ __forceinline__ void PanelBody(const DeviceView& V, const SupernodeRec& S, int s, int panel,
+                                          int row_begin, double* dvec, T (*D)[kPanel + 1]) {
+  (void)s;
   const int F = S.F;
   const int c0 = panel * kPanel;
   const int w = min(kPanel, S.ncols - c0);
   const int c1 = c0 + w;
-  double* Fs = V.fronts + S.front_off;
-  __shared__ double D[kPanel][kPanel + 1];
+  T* Fs = WorkFront<T>(V, S);
   const int tid = threadIdx.x;
   for (int idx = tid; idx < kPanel * kPanel; idx += blockDim.x) {
     const int i = idx % kPanel;
     const int j = idx / kPanel;
-    double v;
+    T v;
     if (i < w && j < w) {
-      v = i >= j ? Fs[static_cast<int64_t>(c0 + j) * F + (c0 + i)] : 0.0;
+      v = i >= j ? Fs[static_cast<int64_t>(c0 + j) * F + (c0 + i)] : T(0);
     } else {
-      v = (i == j) ? 1.0 : 0.0;
+      v = (i == j) ? T(1) : T(0);
     }
     D[i][j] = v;
   }
   __syncthreads();
   bool zero_pivot = false;
   if ((tid >> 5) == 0) {
-    zero_pivot = DiagonalBlockLdlt(&D[0][0], kPanel + 1, w);
+    zero_pivot = DiagonalBlockLdlt<T>(&D[0][0], kPanel + 1, w);
   }
   __syncthreads();
   if (row_begin == c1) {
     // first block of the panel: D into dvec, L11 transposed into the upper
     // triangle of the diagonal block
     if (tid < w) {
-      dvec[S.first_col + c0 + tid] = D[tid][tid];
+      dvec[S.first_col + c0 + tid] = static_cast<double>(D[tid][tid]);
     }
     for (int idx = tid; idx < kPanel * kPanel; idx += blockDim.x) {
       const int i = idx % kPanel;
@@ -157,10 +175,10 @@ __global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const
   }
   const int r = row_begin + tid;
   if (r < F && r >= c1) {
-    double y[kPanel];
+    T y[kPanel];
 #pragma unroll
     for (int j = 0; j < kPanel; ++j) {
-      y[j] = j < w ? Fs[static_cast<int64_t>(c0 + j) * F + r] : 0.0;
+      y[j] = j < w ? Fs[static_cast<int64_t>(c0 + j) * F + r] : T(0);
     }
 #pragma unroll
     for (int j = 1; j < kPanel; ++j) {
@@ -178,6 +196,23 @@ __global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const
   }
 }
 
+/// Panel factorization: LDL^T of the panel's diagonal block (redundantly in
+/// every block of the panel, written back by the first), then
+/// L(r, panel) = A(r, panel) L11^-T D^-1 for a chunk of rows below it.
+__global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const int32_t* tasks, double* dvec) {
+  const int32_t* t = tasks + 3 * static_cast<int64_t>(blockIdx.x);
+  const SupernodeRec S = V.sn[t[0]];
+  if (V.active[S.instance] == 0) {
+    return;
+  }
+  __shared__ double buf[kPanel * (kPanel + 1)];
+  if (Fp32Front(V, S)) {
+    PanelBody<float>(V, S, t[0], t[1], t[2], dvec, reinterpret_cast<float(*)[kPanel + 1]>(buf));
+  } else {
+    PanelBody<double>(V, S, t[0], t[1], t[2], dvec, reinterpret_cast<double(*)[kPanel + 1]>(buf));
+  }
+}
+
 /// Pivot block of a front with at most kSmallPivots columns, factored in
 /// one block: blocked LDL^T of the k x k pivot block in shared memory (warp 0
 /// factors each 32-wide diagonal block, all threads solve the rows below it
@@ -185,26 +220,18 @@ __global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const
 /// the pivot block, `row_begin` onwards, get L(r, :) = A(r, :) L11^-T D^-1,
 /// panel by panel, in registers. Every block of a front repeats the pivot
 /// factorization; the one with row_begin == k writes L11 (the transposed
-/// storage of LoadL) and D.
+/// storage of the diagonal panel blocks) and D.
 constexpr int kSmallPivots = 128;
 constexpr int kFrontRows = 256;
 
-__global__ void __launch_bounds__(256) KFactorFront(DeviceView V, const int32_t* tasks, double* dvec) {
-  extern __shared__ double sm[];
-  const int32_t* t = tasks + 2 * static_cast<int64_t>(blockIdx.x);
-  const int s = t[0];
-  const int row_begin = t[1];
-  const SupernodeRec S = V.sn[s];
-  if (V.active[S.instance] == 0) {
-    return;
-  }
+template <typename T>
+__device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const SupernodeRec& S, int row_begin,
+                                                double* dvec, T* D) {
   const int k = S.ncols;
   const int F = S.F;
   const int ld = k + 1;
-  double* D = sm;  // D[r * ld + c], lower triangle of the pivot block
-  double* Fs = V.fronts + S.front_off;
+  T* Fs = WorkFront<T>(V, S);
   const int tid = threadIdx.x;
-  const int lane = tid & 31;
   const int warp = tid >> 5;
   for (int idx = tid; idx < k * k; idx += blockDim.x) {
     const int r = idx % k;
@@ -218,14 +245,14 @@ __global__ void __launch_bounds__(256) KFactorFront(DeviceView V, const int32_t*
   for (int p0 = 0; p0 < k; p0 += kPanel) {
     const int w = min(kPanel, k - p0);
     if (warp == 0) {
-      zero_pivot = DiagonalBlockLdlt(D + p0 * ld + p0, ld, w) || zero_pivot;
+      zero_pivot = DiagonalBlockLdlt<T>(D + p0 * ld + p0, ld, w) || zero_pivot;
     }
     __syncthreads();
     // rows of the pivot block below this diagonal block (registers; the
     // panel is full width here because a later row exists)
     for (int r = p0 + w + tid; r < k; r += blockDim.x) {
-      double* row = D + r * ld + p0;
-      double y[kPanel];
+      T* row = D + r * ld + p0;
+      T y[kPanel];
 #pragma unroll
       for (int j = 0; j < kPanel; ++j) {
         y[j] = row[j];
@@ -249,7 +276,7 @@ __global__ void __launch_bounds__(256) KFactorFront(DeviceView V, const int32_t*
       const int r = p0 + w + idx % rest;
       const int c = p0 + w + idx / rest;
       if (r >= c) {
-        double acc = 0.0;
+        T acc = T(0);
         for (int l = 0; l < w; ++l) {
           acc += (D[r * ld + p0 + l] * D[(p0 + l) * ld + p0 + l]) * D[c * ld + p0 + l];
         }
@@ -268,7 +295,7 @@ __global__ void __launch_bounds__(256) KFactorFront(DeviceView V, const int32_t*
       }
     }
     for (int j = tid; j < k; j += blockDim.x) {
-      dvec[S.first_col + j] = D[j * ld + j];
+      dvec[S.first_col + j] = static_cast<double>(D[j * ld + j]);
     }
     if (tid == 0 && zero_pivot) {
       atomicOr(V.status + S.instance, kStatusZeroPivot);
@@ -281,26 +308,26 @@ __global__ void __launch_bounds__(256) KFactorFront(DeviceView V, const int32_t*
   }
   for (int p0 = 0; p0 < k; p0 += kPanel) {
     const int w = min(kPanel, k - p0);
-    double y[kPanel];
+    T y[kPanel];
 #pragma unroll
     for (int j = 0; j < kPanel; ++j) {
-      y[j] = j < w ? Fs[static_cast<int64_t>(p0 + j) * F + r] : 0.0;
+      y[j] = j < w ? Fs[static_cast<int64_t>(p0 + j) * F + r] : T(0);
     }
     // contributions of the earlier panels (each panel's 32 values of this
     // row loaded together, then 32 x 32 multiply-adds)
     for (int q0 = 0; q0 < p0; q0 += kPanel) {
-      double yq[kPanel];
+      T yq[kPanel];
 #pragma unroll
       for (int l = 0; l < kPanel; ++l) {
         yq[l] = Fs[static_cast<int64_t>(q0 + l) * F + r];
       }
 #pragma unroll
       for (int l = 0; l < kPanel; ++l) {
-        const double yl = yq[l] * D[(q0 + l) * ld + q0 + l];
+        const T yl = yq[l] * D[(q0 + l) * ld + q0 + l];
 #pragma unroll
         for (int j = 0; j < kPanel; ++j) {
           // rows p0 + j >= k (a narrow last panel) lie outside the pivot block
-          const double ljl = j < w ? D[(p0 + j) * ld + q0 + l] : 0.0;
+          const T ljl = j < w ? D[(p0 + j) * ld + q0 + l] : T(0);
           y[j] -= yl * ljl;
         }
       }
@@ -324,19 +351,23 @@ __global__ void __launch_bounds__(256) KFactorFront(DeviceView V, const int32_t*
   }
 }
 
-/// Tiled rank-k update C -= L_I D L_J^T (lower part only). panel >= 0:
-/// update of the remaining pivot columns by one panel; panel == -1: Schur
-/// complement of the trailing m x m block by all k pivots.
-__global__ void __launch_bounds__(256) KUpdate(DeviceView V, const int32_t* tasks, const double* dvec) {
-  const int32_t* t = tasks + 4 * static_cast<int64_t>(blockIdx.x);
-  const int s = t[0];
-  const int panel = t[1];
-  const int ti = t[2];
-  const int tj = t[3];
-  const SupernodeRec S = V.sn[s];
+__global__ void __launch_bounds__(256) KFactorFront(DeviceView V, const int32_t* tasks, double* dvec) {
+  extern __shared__ double sm[];
+  const int32_t* t = tasks + 2 * static_cast<int64_t>(blockIdx.x);
+  const SupernodeRec S = V.sn[t[0]];
   if (V.active[S.instance] == 0) {
     return;
   }
+  if (Fp32Front(V, S)) {
+    FactorFrontBody<float>(V, S, t[1], dvec, reinterpret_cast<float*>(sm));
+  } else {
+    FactorFrontBody<double>(V, S, t[1], dvec, sm);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeRec& S, int panel, int ti, int tj,
+                                           const double* dvec, T (*As)[kTile], T (*Bs)[kTile]) {
   const int F = S.F;
   int kb;
   int ke;
@@ -356,19 +387,17 @@ __global__ void __launch_bounds__(256) KUpdate(DeviceView V, const int32_t* task
     cc0 = S.ncols + tj * kTile;
     clim = F;
   }
-  double* Fs = V.fronts + S.front_off;
+  T* Fs = WorkFront<T>(V, S);
   const double* d = dvec + S.first_col;
-  __shared__ double As[kPanel][kTile];
-  __shared__ double Bs[kPanel][kTile];
   const int tid = threadIdx.x;
   const int tx = tid % 16;
   const int ty = tid / 16;
-  double acc[4][4];
+  T acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
-      acc[a][b] = 0.0;
+      acc[a][b] = T(0);
     }
   }
   for (int kk = kb; kk < ke; kk += kPanel) {
@@ -378,12 +407,12 @@ __global__ void __launch_bounds__(256) KUpdate(DeviceView V, const int32_t* task
       const int idx = tid + 256 * q;
       const int rr = idx % kTile;
       const int l = idx / kTile;
-      double av = 0.0;
-      double bv = 0.0;
+      T av = T(0);
+      T bv = T(0);
       if (l < kw) {
         const int64_t colbase = static_cast<int64_t>(kk + l) * F;
         if (r0 + rr < F) {
-          av = Fs[colbase + r0 + rr] * d[kk + l];
+          av = Fs[colbase + r0 + rr] * static_cast<T>(d[kk + l]);
         }
         if (cc0 + rr < clim) {
           bv = Fs[colbase + cc0 + rr];
@@ -395,8 +424,8 @@ __global__ void __launch_bounds__(256) KUpdate(DeviceView V, const int32_t* task
     __syncthreads();
 #pragma unroll 8
     for (int l = 0; l < kPanel; ++l) {
-      double av[4];
-      double bv[4];
+      T av[4];
+      T bv[4];
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
         av[a] = As[l][tx + 16 * a];
@@ -428,22 +457,32 @@ __global__ void __launch_bounds__(256) KUpdate(DeviceView V, const int32_t* task
   }
 }
 
-/// Forward solve of one level: gathers the children's update vectors,
-/// solves L11 y = v in 32-wide panels (warp 0 solves each panel's unit
-/// triangle with shuffles, then all threads update every row below it,
-/// including the front's m rows), stores the parent's update vector
-/// u = v_m - L21 y and D^-1 y (Eigen's solve applies the inverse diagonal
-/// between the two triangular sweeps).
-__global__ void __launch_bounds__(256) KForward(DeviceView V, const int32_t* level_sn, const double* dvec) {
-  extern __shared__ double v[];
-  const int s = level_sn[blockIdx.x];
-  const SupernodeRec S = V.sn[s];
+/// Tiled rank-k update C -= L_I D L_J^T (lower part only). panel >= 0:
+/// update of the remaining pivot columns by one panel; panel == -1: Schur
+/// complement of the trailing m x m block by all k pivots.
+__global__ void __launch_bounds__(256) KUpdate(DeviceView V, const int32_t* tasks, const double* dvec) {
+  const int32_t* t = tasks + 4 * static_cast<int64_t>(blockIdx.x);
+  const SupernodeRec S = V.sn[t[0]];
   if (V.active[S.instance] == 0) {
     return;
   }
+  __shared__ double as_buf[kPanel * kTile];
+  __shared__ double bs_buf[kPanel * kTile];
+  if (Fp32Front(V, S)) {
+    UpdateBody<float>(V, S, t[1], t[2], t[3], dvec, reinterpret_cast<float(*)[kTile]>(as_buf),
+                      reinterpret_cast<float(*)[kTile]>(bs_buf));
+  } else {
+    UpdateBody<double>(V, S, t[1], t[2], t[3], dvec, reinterpret_cast<double(*)[kTile]>(as_buf),
+                       reinterpret_cast<double(*)[kTile]>(bs_buf));
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void ForwardBody(const DeviceView& V, const SupernodeRec& S, const double* dvec,
+                                            double* v) {
   const int k = S.ncols;
   const int F = S.F;
-  const double* Fs = V.fronts + S.front_off;
+  const T* Fs = WorkFront<T>(V, S);
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   for (int j = threadIdx.x; j < F; j += blockDim.x) {
@@ -467,7 +506,8 @@ __global__ void __launch_bounds__(256) KForward(DeviceView V, const int32_t* lev
       double lrow[kPanel];
 #pragma unroll
       for (int j = 0; j < kPanel; ++j) {
-        lrow[j] = (j < lane && lane < w) ? Fs[static_cast<int64_t>(p0 + lane) * F + (p0 + j)] : 0.0;
+        lrow[j] = (j < lane && lane < w) ? static_cast<double>(Fs[static_cast<int64_t>(p0 + lane) * F + (p0 + j)])
+                                         : 0.0;
       }
       double y = lane < w ? v[p0 + lane] : 0.0;
 #pragma unroll
@@ -483,7 +523,7 @@ __global__ void __launch_bounds__(256) KForward(DeviceView V, const int32_t* lev
     for (int r = p0 + w + threadIdx.x; r < F; r += blockDim.x) {
       double acc = v[r];
       for (int j = 0; j < w; ++j) {
-        acc -= Fs[static_cast<int64_t>(p0 + j) * F + r] * v[p0 + j];
+        acc -= static_cast<double>(Fs[static_cast<int64_t>(p0 + j) * F + r]) * v[p0 + j];
       }
       v[r] = acc;
     }
@@ -497,31 +537,41 @@ __global__ void __launch_bounds__(256) KForward(DeviceView V, const int32_t* lev
   }
 }
 
-/// Backward solve of one level (root first): z = x_k - L21^T x_R with one
-/// warp per column, then L11^T x = z in 32-wide panels from the last (all
-/// threads subtract the later pivots' contribution, warp 0 solves the
-/// panel's unit upper triangle with shuffles); writes the step in natural
-/// order.
-__global__ void __launch_bounds__(256) KBackward(DeviceView V, const int32_t* level_sn) {
-  extern __shared__ double z[];
-  const int s = level_sn[blockIdx.x];
-  const SupernodeRec S = V.sn[s];
+/// Forward solve of one level: gathers the children's update vectors,
+/// solves L11 y = v in 32-wide panels (warp 0 solves each panel's unit
+/// triangle with shuffles, then all threads update every row below it,
+/// including the front's m rows), stores the parent's update vector
+/// u = v_m - L21 y and D^-1 y (Eigen's solve applies the inverse diagonal
+/// between the two triangular sweeps). Vectors are FP64 whatever the
+/// front's element type.
+__global__ void __launch_bounds__(256) KForward(DeviceView V, const int32_t* level_sn, const double* dvec) {
+  extern __shared__ double v[];
+  const SupernodeRec S = V.sn[level_sn[blockIdx.x]];
   if (V.active[S.instance] == 0) {
     return;
   }
+  if (Fp32Front(V, S)) {
+    ForwardBody<float>(V, S, dvec, v);
+  } else {
+    ForwardBody<double>(V, S, dvec, v);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void BackwardBody(const DeviceView& V, const SupernodeRec& S, double* z) {
   const int k = S.ncols;
   const int m = S.nrows;
   const int F = S.F;
-  const double* Fs = V.fronts + S.front_off;
+  const T* Fs = WorkFront<T>(V, S);
   const int32_t* rows = V.sn_rows + S.rows_off;
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
   for (int j = warp; j < k; j += nwarps) {
     double acc = 0.0;
-    const double* col = Fs + static_cast<int64_t>(j) * F + k;
+    const T* col = Fs + static_cast<int64_t>(j) * F + k;
     for (int r = lane; r < m; r += 32) {
-      acc += col[r] * V.xs[rows[r]];
+      acc += static_cast<double>(col[r]) * V.xs[rows[r]];
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -538,9 +588,9 @@ __global__ void __launch_bounds__(256) KBackward(DeviceView V, const int32_t* le
     // later pivots of this front: z[p0 + j] -= sum_{i >= p0 + w} L(i, p0 + j) x_i
     for (int j = warp; j < w; j += nwarps) {
       double acc = 0.0;
-      const double* col = Fs + static_cast<int64_t>(p0 + j) * F;
+      const T* col = Fs + static_cast<int64_t>(p0 + j) * F;
       for (int i = p0 + w + lane; i < k; i += 32) {
-        acc += col[i] * z[i];
+        acc += static_cast<double>(col[i]) * z[i];
       }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
@@ -557,7 +607,8 @@ __global__ void __launch_bounds__(256) KBackward(DeviceView V, const int32_t* le
       double lcolv[kPanel];
 #pragma unroll
       for (int j = 0; j < kPanel; ++j) {
-        lcolv[j] = (lane < j && j < w) ? Fs[static_cast<int64_t>(p0 + j) * F + (p0 + lane)] : 0.0;
+        lcolv[j] = (lane < j && j < w) ? static_cast<double>(Fs[static_cast<int64_t>(p0 + j) * F + (p0 + lane)])
+                                       : 0.0;
       }
       double x = lane < w ? z[p0 + lane] : 0.0;
 #pragma unroll
@@ -574,6 +625,24 @@ __global__ void __launch_bounds__(256) KBackward(DeviceView V, const int32_t* le
   for (int j = threadIdx.x; j < k; j += blockDim.x) {
     V.xs[S.first_col + j] = z[j];
     V.step[V.perm[S.first_col + j]] = z[j];
+  }
+}
+
+/// Backward solve of one level (root first): z = x_k - L21^T x_R with one
+/// warp per column, then L11^T x = z in 32-wide panels from the last (all
+/// threads subtract the later pivots' contribution, warp 0 solves the
+/// panel's unit upper triangle with shuffles); writes the step in natural
+/// order.
+__global__ void __launch_bounds__(256) KBackward(DeviceView V, const int32_t* level_sn) {
+  extern __shared__ double z[];
+  const SupernodeRec S = V.sn[level_sn[blockIdx.x]];
+  if (V.active[S.instance] == 0) {
+    return;
+  }
+  if (Fp32Front(V, S)) {
+    BackwardBody<float>(V, S, z);
+  } else {
+    BackwardBody<double>(V, S, z);
   }
 }
 

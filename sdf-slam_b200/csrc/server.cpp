@@ -6,15 +6,16 @@
 
 namespace sdfgpu {
 
-int64_t EstimateDeviceBytes(const HostProblem& hp) {
+int64_t EstimateDeviceBytes(const HostProblem& hp, bool mixed) {
   std::vector<HostProblem> v{hp};
   InstanceLayout L{};
   L.col_off = 0;
   const Symbolic S = Analyze(v, {L}, 32, 64);
   const int64_t P = hp.num_points();
   const int64_t nodes = static_cast<int64_t>(hp.nx) * hp.ny;
-  // fronts grow when a re-analysis widens the coupling margin
-  int64_t bytes = S.front_doubles * 8 * 3 / 2;
+  // fronts grow when a re-analysis widens the coupling margin; a mixed solve
+  // adds the FP64 assembled copy and the FP32 work copy
+  int64_t bytes = S.front_doubles * (mixed ? 20 : 8) * 2;
   bytes += P * (8 * 8 + 4 * 8 + 4 * 8 + 48);       // row records, pose offsets, cells, sort buffers, specs
   bytes += nodes * (8 * 3 + 4 * 4);                 // map, backup, index maps
   bytes += static_cast<int64_t>(S.mm_off.size()) * 8 + static_cast<int64_t>(S.mp_off.size()) * 12;
@@ -25,7 +26,30 @@ int64_t EstimateDeviceBytes(const HostProblem& hp) {
 
 Server::Server(int64_t budget_bytes, int max_batch)
     : budget_(budget_bytes), max_batch_(max_batch), created_(std::chrono::steady_clock::now()) {
-  worker_ = std::thread([this] { Loop(); });
+  CudaCheck(cudaGetDevice(&device_), "cudaGetDevice");
+  worker_ = std::thread([this] {
+    cudaSetDevice(device_);
+    Loop();
+  });
+}
+
+bool Server::Busy(Request& r) {
+  if (!r.job.valid()) {
+    return false;
+  }
+  if (r.job.wait_for(std::chrono::seconds(0)) != std::future_status::ready) {
+    return true;
+  }
+  try {
+    r.job.get();
+  } catch (const Error& e) {
+    r.engine.reset();
+    r.result.status = e.code();
+  } catch (...) {
+    r.engine.reset();
+    r.result.status = SDFGPU_ERR_CUDA;
+  }
+  return false;
 }
 
 Server::~Server() {
@@ -40,10 +64,12 @@ Server::~Server() {
 }
 
 int64_t Server::Submit(HostProblem hp, const sdfgpu_solver_options& options) {
-  if (options.max_iterations < 0 || !(options.lambda_init >= 0.0) || !(options.lambda_factor > 0.0)) {
+  if (options.max_iterations < 0 || !(options.lambda_init >= 0.0) || !(options.lambda_factor > 0.0) ||
+      (options.precision != SDFGPU_PRECISION_FP64 && options.precision != SDFGPU_PRECISION_MIXED) ||
+      options.refine_steps < 0 || options.refine_steps > 16) {
     Fail(SDFGPU_ERR_INVALID_ARGUMENT, "invalid solver options");
   }
-  const int64_t bytes = EstimateDeviceBytes(hp);
+  const int64_t bytes = EstimateDeviceBytes(hp, options.precision == SDFGPU_PRECISION_MIXED);
   if (bytes > budget_) {
     Fail(SDFGPU_ERR_OUT_OF_MEMORY, "request footprint " + std::to_string(bytes) + " bytes exceeds the budget");
   }
@@ -163,27 +189,50 @@ void Server::Loop() {
       }
     }
     for (Request* r : admitted) {
-      try {
+      // engine setup (upload, symbolic analysis, initial cost) off this thread
+      r->job = std::async(std::launch::async, [this, r] {
+        cudaSetDevice(device_);
         std::vector<HostProblem> v{r->hp};
         r->engine = std::make_unique<Engine>(std::move(v));
         r->engine->BeginSolve({r->options});
-      } catch (const Error& e) {
-        r->engine.reset();
-        r->result.status = e.code();
-      }
+      });
       std::lock_guard<std::mutex> lk(mu_);
       running_.push_back(r);
     }
-    // one round: enqueue every running solve's iteration, then finish them
+    // one round: enqueue every running solve's iteration, then finish them;
+    // a request whose state left its pattern is re-analysed off this thread
     std::vector<Request*> launched;
+    bool waiting = false;
     for (Request* r : running_) {
+      if (Busy(*r)) {
+        waiting = true;
+        continue;
+      }
       if (r->engine && r->state == State::kRunning && !r->engine->SolveDone()) {
+        if (r->engine->NeedsReanalysis()) {
+          Engine* e = r->engine.get();
+          r->job = std::async(std::launch::async, [this, e] {
+            cudaSetDevice(device_);
+            e->ReanalyzeNow();
+          });
+          waiting = true;
+          continue;
+        }
         try {
           r->engine->LaunchIteration();
           launched.push_back(r);
         } catch (const Error& e) {
           r->result.status = e.code();
           r->engine.reset();
+        }
+      }
+    }
+    if (launched.empty() && waiting) {
+      // only host jobs are in flight: wait for one of them briefly
+      for (Request* r : running_) {
+        if (r->job.valid()) {
+          r->job.wait_for(std::chrono::milliseconds(1));
+          break;
         }
       }
     }
@@ -200,6 +249,10 @@ void Server::Loop() {
     // retire finished, failed and cancelled requests
     std::vector<Request*> still;
     for (Request* r : running_) {
+      if (r->job.valid()) {
+        still.push_back(r);  // its host job must end first
+        continue;
+      }
       const bool cancelled = r->state == State::kCancelled;
       const bool failed = !r->engine;
       const bool done = !failed && r->engine->SolveDone();
@@ -238,6 +291,9 @@ void Server::Loop() {
     }
   }
   for (Request* r : running_) {
+    if (r->job.valid()) {
+      r->job.wait();
+    }
     r->engine.reset();
   }
 }

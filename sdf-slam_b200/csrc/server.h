@@ -3,12 +3,15 @@
 // engine (own CUDA stream); every round enqueues one LM iteration of every
 // running request before waiting for any of them, so their kernels overlap
 // on the GPU. Requests are admitted while their estimated device footprint
-// fits the budget and retire as soon as their solve ends.
+// fits the budget and retire as soon as their solve ends. Host work of a
+// request (building its engine, re-analysing a pattern its state left) runs
+// on a helper thread while the other requests keep iterating.
 #pragma once
 
 #include <condition_variable>
 #include <cstdint>
 #include <deque>
+#include <future>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -20,8 +23,9 @@
 namespace sdfgpu {
 
 /// Device bytes an engine for `hp` will hold (state, specs, symbolic
-/// structure, fronts), from a host-side symbolic analysis.
-int64_t EstimateDeviceBytes(const HostProblem& hp);
+/// structure, fronts; the mixed-precision copies when `mixed`), from a
+/// host-side symbolic analysis.
+int64_t EstimateDeviceBytes(const HostProblem& hp, bool mixed);
 
 class Server {
  public:
@@ -46,15 +50,20 @@ class Server {
     State state{State::kQueued};
     std::chrono::steady_clock::time_point submitted;
     std::unique_ptr<Engine> engine;
+    std::future<void> job;  // host work in flight (engine setup, re-analysis)
     sdfgpu_solve_result result{};
     std::vector<double> map_values;
     std::vector<double> poses;
   };
   void Loop();
   void Retire(Request& r);
+  /// True while the request's host job runs; collects a finished job (a
+  /// failure marks the request failed).
+  bool Busy(Request& r);
 
   int64_t budget_;
   int max_batch_;
+  int device_{0};
   std::mutex mu_;
   std::condition_variable cv_;
   std::condition_variable done_cv_;

@@ -669,9 +669,30 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin) {
   if (Fr > 1) {
     const int s = S.col_owner[static_cast<size_t>(col_off + A)];
     const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
+    S.sn[static_cast<size_t>(s)].pose_root = 1;
     S.pp_base[0] = r.front_off;
     S.pp_ld[0] = r.F;
     S.pp_first[0] = col_off + A - r.first_col;
+  }
+  // map-pose entries grouped by frame (for the FP64 normal-matrix product)
+  S.fmp_ptr.assign(static_cast<size_t>(Fr) + 1, 0);
+  for (int64_t e = 0; e < static_cast<int64_t>(S.mp_frame.size()); ++e) {
+    ++S.fmp_ptr[static_cast<size_t>(S.mp_frame[static_cast<size_t>(e)]) + 1];
+  }
+  for (int f = 0; f < Fr; ++f) {
+    S.fmp_ptr[static_cast<size_t>(f) + 1] += S.fmp_ptr[static_cast<size_t>(f)];
+  }
+  S.fmp_col.resize(S.mp_frame.size());
+  S.fmp_off.resize(S.mp_frame.size());
+  {
+    std::vector<int64_t> fill(S.fmp_ptr.begin(), S.fmp_ptr.end() - 1);
+    for (int c = 0; c < A; ++c) {
+      for (int64_t e = S.mp_ptr[static_cast<size_t>(c)]; e < S.mp_ptr[static_cast<size_t>(c) + 1]; ++e) {
+        const int64_t q = fill[static_cast<size_t>(S.mp_frame[static_cast<size_t>(e)])]++;
+        S.fmp_col[static_cast<size_t>(q)] = c;
+        S.fmp_off[static_cast<size_t>(q)] = S.mp_off[static_cast<size_t>(e)];
+      }
+    }
   }
   ComputeRel(S);
   return piece;
@@ -713,6 +734,13 @@ Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<Inst
   S.pp_base.assign(I, -1);
   S.pp_ld.assign(I, 0);
   S.pp_first.assign(I, 0);
+  int frames = 0;
+  for (size_t i = 0; i < I; ++i) {
+    frames = std::max(frames, layout[i].frame_off + static_cast<int>(pieces[i].s.fmp_ptr.size()) - 1);
+  }
+  S.fmp_ptr.assign(static_cast<size_t>(frames) + 1, 0);
+  S.fmp_col.reserve(nmp);
+  S.fmp_off.reserve(nmp);
   std::vector<int> height;
   height.reserve(nsn);
   for (size_t i = 0; i < I; ++i) {
@@ -767,6 +795,18 @@ Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<Inst
     S.pp_base[i] = L.pp_base[0] >= 0 ? L.pp_base[0] + f0 : -1;
     S.pp_ld[i] = L.pp_ld[0];
     S.pp_first[i] = L.pp_first[0];
+    // instances are laid out in frame order, so frames fill fmp_ptr in order
+    const int64_t q0 = static_cast<int64_t>(S.fmp_col.size());
+    const int fr = static_cast<int>(L.fmp_ptr.size()) - 1;
+    for (int f = 0; f < fr; ++f) {
+      S.fmp_ptr[static_cast<size_t>(layout[i].frame_off + f) + 1] = q0 + L.fmp_ptr[static_cast<size_t>(f) + 1];
+    }
+    for (const int32_t c : L.fmp_col) {
+      S.fmp_col.push_back(col_off + c);
+    }
+    for (const int64_t v : L.fmp_off) {
+      S.fmp_off.push_back(v + f0);
+    }
   }
   Finalize(S, height, panel_width, tile);
   return S;

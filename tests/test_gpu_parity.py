@@ -227,6 +227,54 @@ def test_state_outside_pattern_reanalyses_only_that_instance():
     assert hg.shape == ho.shape and np.max(np.abs(hg - ho) / np.abs(ho)) <= 1e-8
 
 
+def test_mixed_precision_solve_follows_fp64_oracle():
+    # Mixed: FP32 grid fronts, FP64 pose root, FP64 refinement. With three
+    # refinement rounds the LM trajectory stays on the FP64 oracle's within
+    # the contract (final cost 1e-8 relative, poses 1e-4 m); without
+    # refinement the FP32 factors show.
+    sc = scenes.room_scene(seed=0)
+    specs, _ = scene_specs(sc, P.ProblemOptions(hallucination_points=4))
+    orc = oracle_from_specs(specs)
+    ro = orc.solve(max_iterations=10, num_threads=4)
+    ho = np.array(ro["cost_history"])
+    om, op = orc.state()
+    gpu = P.Problem.from_specs(specs)
+    rg = P.solve(gpu, P.SolverOptions(max_iterations=10, precision="mixed", refine_steps=3))
+    hg = np.array(rg.cost_history)
+    assert hg.shape == ho.shape
+    assert abs(hg[-1] - ho[-1]) <= 1e-8 * abs(ho[-1])
+    gm, gp = gpu.state()
+    assert np.max(np.abs(gp[:, :2] - op[:, :2])) <= 1e-4
+    assert np.max(np.abs(gm - om)) <= 1e-4
+    raw = P.Problem.from_specs(specs)
+    r0 = P.solve(raw, P.SolverOptions(max_iterations=10, precision="mixed", refine_steps=0))
+    h0 = np.array(r0.cost_history)
+    assert np.max(np.abs(h0 - ho) / np.abs(ho)) > 1e-12
+
+
+def test_mixed_and_plain_instances_in_one_batch():
+    scs = [scenes.room_scene(seed=s, grid=g, frames=f, beams=b)
+           for s, g, f, b in [(30, 44, 9, 120), (31, 48, 11, 150)]]
+    specs = [scene_specs(sc, P.ProblemOptions(hallucination_points=3))[0] for sc in scs]
+    batch = P.Problem.batch(specs)
+    opts = [P.SolverOptions(max_iterations=5), P.SolverOptions(max_iterations=5, precision="mixed")]
+    rb = P.solve(batch, opts)
+    # the plain instance is bitwise its own plain solve
+    single = P.Problem.from_specs(specs[0])
+    r1 = P.solve(single, opts[0])
+    assert rb[0].cost_history == r1.cost_history
+    assert all(np.array_equal(a, b) for a, b in zip(batch.state(0), single.state()))
+    # the mixed one follows its FP64 solve within the contract
+    plain = P.Problem.from_specs(specs[1])
+    rp = P.solve(plain, P.SolverOptions(max_iterations=5))
+    hb = np.array(rb[1].cost_history)
+    hp = np.array(rp.cost_history)
+    assert hb.shape == hp.shape and np.max(np.abs(hb - hp) / np.abs(hp)) <= 1e-8
+    bm, bp = batch.state(1)
+    pm, pp = plain.state()
+    assert np.max(np.abs(bp[:, :2] - pp[:, :2])) <= 1e-4
+
+
 def test_server_results_equal_alone_and_in_mix():
     scs = [scenes.request_scene(seed=100 + i, grid_range=(40, 70), pose_range=(8, 24), iterations=6)
            for i in range(5)]
