@@ -276,6 +276,8 @@ def run_batch(P, args, flusher):
         opts1 = [P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=precision)] * count
         for _ in range(2):
             P.solve(batch, opts1)
+        if not args.no_autotune:
+            out.setdefault("schedule", {})[precision] = batch.autotune()["schedule"]
         device = 0.0
         for _ in range(steps):
             flusher.flush()
@@ -300,6 +302,8 @@ def run_mixed(P, args, specs, flusher):
                             refine_steps=args.refine_steps)
     for _ in range(args.warmup):
         P.solve(prob, opts1)
+    if not args.no_autotune:
+        prob.autotune()
     steps = max(3, args.steps // 2)
     device = 0.0
     phases = np.zeros(5)
@@ -377,9 +381,12 @@ def run_gpu(args, dist, world, rank, local):
     flusher = L2Flusher()
     opts1 = P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=args.precision)
     prob = P.Problem.from_specs(specs)
-    # warm-up: upload, symbolic analysis, first iterations
+    # warm-up: upload, symbolic analysis, first iterations; then the
+    # autotuner picks the factorization schedule
     for _ in range(args.warmup):
         P.solve(prob, opts1)
+    tune = prob.autotune() if not args.no_autotune else None
+    P.solve(prob, opts1)
     flusher.sync()
     _barrier(dist)
     sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) \
@@ -480,6 +487,9 @@ def run_gpu(args, dist, world, rank, local):
         "e2e": {"value": e2e_value, "unit": "LM iters/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "iterations_per_step": e2e_iters},
         "clocks": clocks,
+        "schedule": {"small_pivots": tune["schedule"][0], "front_rows": tune["schedule"][1],
+                     "panel_rows": tune["schedule"][2], "factor_ms": tune["factor_ms"],
+                     "trials": len(tune["trials"])} if tune else None,
         "mixed": mixed,
         "batched": batched,
         "served": served,
@@ -502,6 +512,7 @@ def main():
     ap.add_argument("--cpu-iterations", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--refine-steps", type=int, default=3)
     ap.add_argument("--batch-count", type=int, default=64)
     ap.add_argument("--serve-requests", type=int, default=32)

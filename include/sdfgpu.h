@@ -243,6 +243,18 @@ int sdfgpu_linearization_get(sdfgpu_problem* problem, double* residuals, int32_t
  * phases must hold 12 doubles. */
 int sdfgpu_last_profile(sdfgpu_problem* problem, double* phases);
 
+/* Autotuner (no counterpart in the reference): times the factorization of
+ * the handle's current normal matrix under each candidate schedule (the
+ * pivot count up to which a front is factored by one kernel, that kernel's
+ * rows per block, the rows per panel block) and keeps the fastest for the
+ * handle's later solves, also across pattern re-analyses. schedule (3
+ * int32, may be NULL) receives the chosen one, factor_ms (may be NULL) its
+ * factorization time; trials (may be NULL) receives up to max_trials rows
+ * of 4 doubles (small_pivots, front_rows, panel_rows, ms). Returns the
+ * number of candidates timed in *num_trials when not NULL. */
+int sdfgpu_autotune(sdfgpu_problem* problem, int32_t* schedule, double* factor_ms, double* trials,
+                    int32_t max_trials, int32_t* num_trials);
+
 /* ------------------------------------------------------------ factor only --
  * LinearSolver::kGpu: ParallelSimplicialLdlt's interface
  * (src/solvers/parallel_ldlt.hpp:38-51 and Eigen's solve) for any symmetric

@@ -368,6 +368,18 @@ class Problem:
             _d(out["n_values"]), _d(out["rhs"]), _d(out["step"]) if compute_step else None))
         return out
 
+    def autotune(self) -> dict:
+        """Picks the fastest factorization schedule for this handle (kept for
+        its later solves): {"schedule": (small_pivots, front_rows,
+        panel_rows), "factor_ms": ..., "trials": [(s, f, p, ms), ...]}."""
+        sched = (ctypes.c_int32 * 3)()
+        best = ctypes.c_double()
+        trials = np.zeros((16, 4))
+        n = ctypes.c_int32()
+        _check(lib().sdfgpu_autotune(self._h, sched, ctypes.byref(best), _d(trials), 16, ctypes.byref(n)))
+        return {"schedule": tuple(int(v) for v in sched), "factor_ms": best.value,
+                "trials": [tuple(r) for r in trials[:n.value]]}
+
     def last_profile(self) -> dict:
         ph = np.zeros(12)
         _check(lib().sdfgpu_last_profile(self._h, _d(ph)))

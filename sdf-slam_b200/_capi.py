@@ -109,6 +109,8 @@ SIGNATURES = {
     "sdfgpu_linearization_get": (ctypes.c_int, [vp, c_dbl_p, c_int_p, c_int_p, c_int_p, c_dbl_p,
                                                 c_int_p, c_int_p, c_dbl_p, c_dbl_p, c_dbl_p]),
     "sdfgpu_last_profile": (ctypes.c_int, [vp, c_dbl_p]),
+    "sdfgpu_autotune": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int32), c_dbl_p, c_dbl_p, ctypes.c_int32,
+                                       ctypes.POINTER(ctypes.c_int32)]),
     "sdfgpu_ldlt_create": (ctypes.c_int, [ctypes.c_int32, c_int_p, c_int_p, c_int_p,
                                           ctypes.POINTER(vp)]),
     "sdfgpu_ldlt_factorize": (ctypes.c_int, [vp, c_dbl_p]),

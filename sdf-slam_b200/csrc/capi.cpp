@@ -377,6 +377,34 @@ int sdfgpu_last_profile(sdfgpu_problem* problem, double* phases) {
   });
 }
 
+int sdfgpu_autotune(sdfgpu_problem* problem, int32_t* schedule, double* factor_ms, double* trials,
+                    int32_t max_trials, int32_t* num_trials) {
+  return Guard([&] {
+    std::vector<std::pair<sdfgpu::Schedule, double>> t;
+    const double best = Eng(problem).Autotune(&t);
+    const sdfgpu::Schedule& s = Eng(problem).schedule();
+    if (schedule != nullptr) {
+      schedule[0] = s.small_pivots;
+      schedule[1] = s.front_rows;
+      schedule[2] = s.panel_rows;
+    }
+    if (factor_ms != nullptr) {
+      *factor_ms = best;
+    }
+    if (trials != nullptr) {
+      for (size_t q = 0; q < t.size() && static_cast<int32_t>(q) < max_trials; ++q) {
+        trials[4 * q] = t[q].first.small_pivots;
+        trials[4 * q + 1] = t[q].first.front_rows;
+        trials[4 * q + 2] = t[q].first.panel_rows;
+        trials[4 * q + 3] = t[q].second;
+      }
+    }
+    if (num_trials != nullptr) {
+      *num_trials = static_cast<int32_t>(t.size());
+    }
+  });
+}
+
 int sdfgpu_ldlt_create(int32_t n, const int32_t* outer, const int32_t* inner, const int32_t* perm,
                        sdfgpu_ldlt** out) {
   return Guard([&] {

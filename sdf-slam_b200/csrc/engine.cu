@@ -368,7 +368,7 @@ void Engine::Analyze() {
   pieces_.assign(host_.size(), SymPiece{});
   pending_.clear();
   AnalyzeInstances(host_, margin_, pieces_, nullptr);
-  sym_ = Concatenate(pieces_, layout_, 32, 64);
+  sym_ = Concatenate(pieces_, layout_, 32, 64, sched_);
   UploadSymbolic();
 }
 
@@ -763,10 +763,65 @@ void Engine::Reanalyze(const std::vector<int>& which) {
     margin_[static_cast<size_t>(i)] = std::min(margin_[static_cast<size_t>(i)] + kMarginStep, kMaxMargin);
   }
   AnalyzeInstances(host_, margin_, pieces_, &which);
-  sym_ = Concatenate(pieces_, layout_, 32, 64);
+  sym_ = Concatenate(pieces_, layout_, 32, 64, sched_);
   UploadSymbolic();
   ++times_.reanalyses;
   times_.reanalysis_host += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void Engine::UploadSchedule() {
+  DropGraph();
+  CudaCheck(cudaStreamSynchronize(stream_), "schedule sync");
+  ea_tasks_.Upload(sym_.ea_tasks, stream_);
+  ea_child_.Upload(sym_.ea_child, stream_);
+  panel_tasks_.Upload(sym_.panel_tasks, stream_);
+  update_tasks_.Upload(sym_.update_tasks, stream_);
+  small_tasks_.Upload(sym_.small_tasks, stream_);
+  level_sn_.Upload(sym_.level_sn, stream_);
+  CudaCheck(cudaStreamSynchronize(stream_), "schedule upload");
+}
+
+double Engine::Autotune(std::vector<std::pair<Schedule, double>>* trials) {
+  // Candidate schedules: the pivot count below which a front is factored by
+  // one kernel, that kernel's rows per block, and the rows per panel block.
+  const std::vector<Schedule> candidates = {
+      {128, 256, 128}, {128, 128, 128}, {96, 256, 128}, {64, 256, 128}, {64, 128, 64}, {128, 256, 64}};
+  const size_t I = host_.size();
+  SetMode(std::vector<int32_t>(I, 0), 0);
+  SetActive(std::vector<int32_t>(I, 1));
+  SetLambda(std::vector<double>(I, 1.0), std::vector<int32_t>(I, 0));
+  double best = 0.0;
+  Schedule best_sched = sched_;
+  for (const Schedule& c : candidates) {
+    Reschedule(sym_, c);
+    UploadSchedule();
+    double ms_min = 0.0;
+    for (int rep = 0; rep < 3; ++rep) {
+      // factor the current state's normal matrix (reassembled each time:
+      // the factorization overwrites it)
+      ClearStatus();
+      LaunchRows();
+      LaunchNormal();
+      CudaCheck(cudaEventRecord(ev_[0], stream_), "event");
+      LaunchFactor();
+      CudaCheck(cudaEventRecord(ev_[1], stream_), "event");
+      CudaCheck(cudaStreamSynchronize(stream_), "autotune");
+      float ms = 0.0f;
+      CudaCheck(cudaEventElapsedTime(&ms, ev_[0], ev_[1]), "autotune timing");
+      ms_min = rep == 0 ? ms : std::min(ms_min, static_cast<double>(ms));
+    }
+    if (trials != nullptr) {
+      trials->emplace_back(c, ms_min);
+    }
+    if (best == 0.0 || ms_min < best) {
+      best = ms_min;
+      best_sched = c;
+    }
+  }
+  sched_ = best_sched;
+  Reschedule(sym_, sched_);
+  UploadSchedule();
+  return best;
 }
 
 void Engine::ReanalyzePending() {
@@ -1224,6 +1279,15 @@ void Engine::EnqueueIteration() {
   if (use_graph_) {
     times_.launches += graph_launches_;
   }
+}
+
+bool Engine::IterationReady() const {
+  const cudaError_t e = cudaEventQuery(ev_[5]);
+  if (e == cudaErrorNotReady) {
+    return false;
+  }
+  CudaCheck(e, "iteration event");
+  return true;
 }
 
 void Engine::FinishIteration() {

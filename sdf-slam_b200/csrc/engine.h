@@ -183,6 +183,14 @@ class Engine {
   [[nodiscard]] bool NeedsReanalysis() const { return !pending_.empty(); }
   /// Runs that re-analysis now (the serving loop does it off its own thread).
   void ReanalyzeNow() { ReanalyzePending(); }
+  /// True when the iteration enqueued by LaunchIteration has finished on the
+  /// device (FinishIteration will not wait).
+  [[nodiscard]] bool IterationReady() const;
+  /// Times the factorization of the current state's normal matrix under each
+  /// candidate schedule and keeps the fastest (also across re-analyses).
+  /// Returns its time in ms; trials receives every candidate's time.
+  double Autotune(std::vector<std::pair<Schedule, double>>* trials);
+  [[nodiscard]] const Schedule& schedule() const { return sched_; }
   [[nodiscard]] const IterTimes& times() const { return times_; }
   [[nodiscard]] int64_t factor_flops() const { return sym_.total_flops; }
   [[nodiscard]] const Symbolic& symbolic() const { return sym_; }
@@ -192,6 +200,7 @@ class Engine {
   void UploadProblem();
   void Analyze();
   void UploadSymbolic();
+  void UploadSchedule();
   /// Per-instance precision of the coming solve (1: mixed) and refinement
   /// rounds; re-uploads flags and drops the graphs when they change.
   void SetMode(const std::vector<int32_t>& mixed, int refine_steps);
@@ -222,6 +231,7 @@ class Engine {
   std::vector<SymPiece> pieces_;   // per-instance analyses (local numbering)
   std::vector<int> margin_;        // per instance: coupling margin of its piece
   std::vector<int> pending_;       // instances whose current state overflows their pattern
+  Schedule sched_;                 // factorization schedule (autotuned or default)
   Symbolic sym_;
   cudaStream_t stream_{nullptr};
   cudaEvent_t ev_[6]{};

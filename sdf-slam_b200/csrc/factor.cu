@@ -222,7 +222,6 @@ __global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const
 /// factorization; the one with row_begin == k writes L11 (the transposed
 /// storage of the diagonal panel blocks) and D.
 constexpr int kSmallPivots = 128;
-constexpr int kFrontRows = 256;
 
 template <typename T>
 __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const SupernodeRec& S, int row_begin,
@@ -303,7 +302,7 @@ __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const Super
   }
   // rows below the pivot block: thread per row, panel by panel
   const int r = row_begin + tid;
-  if (r >= F || r >= row_begin + kFrontRows) {
+  if (r >= F || r >= row_begin + static_cast<int>(blockDim.x)) {
     return;
   }
   for (int p0 = 0; p0 < k; p0 += kPanel) {
@@ -694,7 +693,7 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
     if (sm.count > 0) {
       const int kmax = S.small_max_k[static_cast<size_t>(l)];
       const size_t bytes = static_cast<size_t>(kmax) * (kmax + 1) * sizeof(double);
-      KFactorFront<<<static_cast<unsigned>(sm.count), kFrontRows, bytes, stream>>>(V, P.small_tasks + 2 * sm.begin,
+      KFactorFront<<<static_cast<unsigned>(sm.count), S.front_rows, bytes, stream>>>(V, P.small_tasks + 2 * sm.begin,
                                                                                   P.dvec);
       ++launches;
     }
@@ -702,7 +701,7 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
       const size_t slot = static_cast<size_t>(S.panel_index_base[static_cast<size_t>(l)] + t);
       const TaskRange pr = S.panel_range[slot];
       if (pr.count > 0) {
-        KPanel<<<static_cast<unsigned>(pr.count), kPanelRowsPerBlock, 0, stream>>>(V, P.panel_tasks + 3 * pr.begin,
+        KPanel<<<static_cast<unsigned>(pr.count), S.panel_rows, 0, stream>>>(V, P.panel_tasks + 3 * pr.begin,
                                                                                    P.dvec);
         ++launches;
       }

@@ -129,8 +129,13 @@ struct Symbolic {
   std::vector<TaskRange> update_range;       // per (level, panel) flattened
   std::vector<int32_t> panel_index_base;     // level -> first (level,panel) slot
   // fronts with at most small_pivots pivots: one factorization kernel per
-  // level, tasks (sn, first row of the chunk below the pivot block)
+  // level, tasks (sn, first row of the chunk below the pivot block) of
+  // front_rows rows (the block size); larger fronts: panel tasks of
+  // panel_rows rows. The three are the schedule an autotuner picks.
   int small_pivots{128};
+  int front_rows{256};
+  int panel_rows{128};
+  std::vector<int> height;                   // per supernode: height in the assembly tree
   std::vector<int32_t> small_tasks;
   std::vector<TaskRange> small_range;        // per level
   std::vector<int32_t> small_max_k;          // per level
@@ -201,10 +206,20 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin);
 void AnalyzeInstances(const std::vector<HostProblem>& problems, const std::vector<int>& margin,
                       std::vector<SymPiece>& pieces, const std::vector<int>* which);
 
+/// Schedule parameters of the factorization (see Symbolic).
+struct Schedule {
+  int small_pivots{128};
+  int front_rows{256};
+  int panel_rows{128};
+};
+
 /// Global structure (task lists, level schedule) of pieces laid out by
 /// `layout`.
 Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<InstanceLayout>& layout,
-                     int panel_width, int tile);
+                     int panel_width, int tile, const Schedule& sched = Schedule{});
+
+/// Rebuilds the level schedule and task lists of S for another schedule.
+void Reschedule(Symbolic& S, const Schedule& sched);
 
 /// Builds the supernodal symbolic factorization for a set of instances.
 Symbolic Analyze(const std::vector<HostProblem>& problems, const std::vector<InstanceLayout>& layout,

@@ -199,58 +199,57 @@ void Server::Loop() {
       std::lock_guard<std::mutex> lk(mu_);
       running_.push_back(r);
     }
-    // one round: enqueue every running solve's iteration, then finish them;
-    // a request whose state left its pattern is re-analysed off this thread
-    std::vector<Request*> launched;
-    bool waiting = false;
+    // one pass: finish every iteration whose device work is done, enqueue
+    // the next iteration of every idle request; a request whose state left
+    // its pattern is re-analysed off this thread
+    bool progressed = false;
     for (Request* r : running_) {
       if (Busy(*r)) {
-        waiting = true;
         continue;
       }
-      if (r->engine && r->state == State::kRunning && !r->engine->SolveDone()) {
+      if (!r->engine) {
+        continue;
+      }
+      try {
+        if (r->in_flight) {
+          if (!r->engine->IterationReady()) {
+            continue;
+          }
+          r->in_flight = false;
+          r->engine->FinishIteration();
+          progressed = true;
+          std::lock_guard<std::mutex> lk(mu_);
+          ++iterations_;
+        }
+        if (r->state != State::kRunning || r->engine->SolveDone()) {
+          continue;
+        }
         if (r->engine->NeedsReanalysis()) {
           Engine* e = r->engine.get();
           r->job = std::async(std::launch::async, [this, e] {
             cudaSetDevice(device_);
             e->ReanalyzeNow();
           });
-          waiting = true;
           continue;
         }
-        try {
-          r->engine->LaunchIteration();
-          launched.push_back(r);
-        } catch (const Error& e) {
-          r->result.status = e.code();
-          r->engine.reset();
-        }
-      }
-    }
-    if (launched.empty() && waiting) {
-      // only host jobs are in flight: wait for one of them briefly
-      for (Request* r : running_) {
-        if (r->job.valid()) {
-          r->job.wait_for(std::chrono::milliseconds(1));
-          break;
-        }
-      }
-    }
-    for (Request* r : launched) {
-      try {
-        r->engine->FinishIteration();
-        std::lock_guard<std::mutex> lk(mu_);
-        ++iterations_;
+        r->engine->LaunchIteration();
+        r->in_flight = true;
+        progressed = true;
       } catch (const Error& e) {
+        r->in_flight = false;
         r->result.status = e.code();
         r->engine.reset();
       }
     }
+    if (!progressed) {
+      // nothing finished and nothing new to enqueue: yield briefly
+      std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
     // retire finished, failed and cancelled requests
     std::vector<Request*> still;
     for (Request* r : running_) {
-      if (r->job.valid()) {
-        still.push_back(r);  // its host job must end first
+      if (r->job.valid() || r->in_flight) {
+        still.push_back(r);  // its host job or device iteration must end first
         continue;
       }
       const bool cancelled = r->state == State::kCancelled;
@@ -293,6 +292,9 @@ void Server::Loop() {
   for (Request* r : running_) {
     if (r->job.valid()) {
       r->job.wait();
+    }
+    if (r->engine && r->in_flight) {
+      cudaStreamSynchronize(r->engine->stream());
     }
     r->engine.reset();
   }

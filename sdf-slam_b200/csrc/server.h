@@ -1,8 +1,9 @@
 // Serving loop with continuous batching. Each admitted request keeps its
 // state, symbolic analysis and factors resident on the device in its own
-// engine (own CUDA stream); every round enqueues one LM iteration of every
-// running request before waiting for any of them, so their kernels overlap
-// on the GPU. Requests are admitted while their estimated device footprint
+// engine (own CUDA stream). The loop keeps one LM iteration of every running
+// request in flight: it finishes an iteration as soon as its stream's event
+// reports it done and enqueues that request's next one, so requests of very
+// different sizes overlap on the GPU without waiting for one another. Requests are admitted while their estimated device footprint
 // fits the budget and retire as soon as their solve ends. Host work of a
 // request (building its engine, re-analysing a pattern its state left) runs
 // on a helper thread while the other requests keep iterating.
@@ -51,6 +52,7 @@ class Server {
     std::chrono::steady_clock::time_point submitted;
     std::unique_ptr<Engine> engine;
     std::future<void> job;  // host work in flight (engine setup, re-analysis)
+    bool in_flight{false};  // an LM iteration is enqueued on the device
     sdfgpu_solve_result result{};
     std::vector<double> map_values;
     std::vector<double> poses;

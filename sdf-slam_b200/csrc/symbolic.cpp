@@ -236,6 +236,7 @@ void ComputeRel(Symbolic& S) {
 void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int tile) {
   S.panel_width = panel_width;
   S.tile = tile;
+  S.height = height;
   const int Sn = static_cast<int>(S.sn.size());
   int levels = 0;
   for (const int h : height) {
@@ -258,9 +259,9 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   }
   const int B = panel_width;
   const int T = tile;
-  constexpr int kPanelRows = 128;
+  const int kPanelRows = S.panel_rows;
   constexpr int kEaCols = 16;
-  constexpr int kFrontRows = 256;
+  const int kFrontRows = S.front_rows;
   const int small = S.small_pivots;
   S.level_panels.assign(static_cast<size_t>(levels), 0);
   S.panel_index_base.assign(static_cast<size_t>(levels) + 1, 0);
@@ -699,8 +700,11 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin) {
 }
 
 Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<InstanceLayout>& layout,
-                     int panel_width, int tile) {
+                     int panel_width, int tile, const Schedule& sched) {
   Symbolic S;
+  S.small_pivots = sched.small_pivots;
+  S.front_rows = sched.front_rows;
+  S.panel_rows = sched.panel_rows;
   int n = 0;
   size_t nsn = 0;
   size_t nrows = 0;
@@ -810,6 +814,26 @@ Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<Inst
   }
   Finalize(S, height, panel_width, tile);
   return S;
+}
+
+void Reschedule(Symbolic& S, const Schedule& sched) {
+  S.small_pivots = sched.small_pivots;
+  S.front_rows = sched.front_rows;
+  S.panel_rows = sched.panel_rows;
+  S.ea_tasks.clear();
+  S.ea_child.clear();
+  S.panel_tasks.clear();
+  S.update_tasks.clear();
+  S.small_tasks.clear();
+  S.ea_range.clear();
+  S.panel_range.clear();
+  S.update_range.clear();
+  S.small_range.clear();
+  S.small_max_k.clear();
+  S.level_panels.clear();
+  S.panel_index_base.clear();
+  const std::vector<int> height = S.height;
+  Finalize(S, height, S.panel_width, S.tile);
 }
 
 Symbolic Analyze(const std::vector<HostProblem>& problems, const std::vector<InstanceLayout>& layout,

@@ -275,6 +275,21 @@ def test_mixed_and_plain_instances_in_one_batch():
     assert np.max(np.abs(bp[:, :2] - pp[:, :2])) <= 1e-4
 
 
+def test_autotuned_schedule_keeps_parity():
+    sc = scenes.room_scene(seed=0)
+    specs, _ = scene_specs(sc, P.ProblemOptions(hallucination_points=4))
+    gpu = P.Problem.from_specs(specs)
+    tune = gpu.autotune()
+    assert len(tune["trials"]) >= 2 and tune["factor_ms"] > 0
+    assert tune["schedule"] in [tuple(int(v) for v in t[:3]) for t in tune["trials"]]
+    assert tune["factor_ms"] == min(t[3] for t in tune["trials"])
+    rg = P.solve(gpu, P.SolverOptions(max_iterations=10))
+    ro = oracle_from_specs(specs).solve(max_iterations=10, num_threads=4)
+    hg = np.array(rg.cost_history)
+    ho = np.array(ro["cost_history"])
+    assert hg.shape == ho.shape and np.max(np.abs(hg - ho) / np.abs(ho)) <= 1e-8
+
+
 def test_server_results_equal_alone_and_in_mix():
     scs = [scenes.request_scene(seed=100 + i, grid_range=(40, 70), pose_range=(8, 24), iterations=6)
            for i in range(5)]
