@@ -39,10 +39,27 @@ __device__ __forceinline__ float* WorkFront<float>(const DeviceView& V, const Su
   return V.fronts32 + S.front_off;
 }
 
+/// 1 / d by Newton-Raphson iteration x <- x + x (1 - d x), seeded with the
+/// hardware's approximate reciprocal (two steps square its ~2^-23 error
+/// below FP64 precision). Much shorter latency than a correctly rounded
+/// division on the pivot chain; the result may differ from 1.0 / d in the
+/// last bit.
+__device__ __forceinline__ double Recip(double d) {
+  double x;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(d));
+  double e = fma(-d, x, 1.0);
+  x = fma(x, e, x);
+  e = fma(-d, x, 1.0);
+  return fma(x, e, x);
+}
+__device__ __forceinline__ float Recip(float d) { return 1.0f / d; }
+
 /// LDL^T of the w x w diagonal block at B (row r, column c at B[r * ld + c],
 /// lower triangle) by one warp in registers: lane i owns row i; at step j
 /// its registers hold columns j.., so every register index is static while
-/// the step loop stays rolled (a small code footprint). Writes L below the
+/// the step loop stays rolled (a small code footprint). The trailing update
+/// is branch-free (lanes that must not change a column subtract zero): a
+/// per-column branch costs more than the multiply-add. Writes L below the
 /// diagonal and D on it; returns true when a pivot is exactly zero.
 template <typename T>
 __device__ __noinline__ bool DiagonalBlockLdlt(T* B, int ld, int w) {
@@ -57,7 +74,7 @@ __device__ __noinline__ bool DiagonalBlockLdlt(T* B, int ld, int w) {
     const T dj = __shfl_sync(0xffffffffu, row[0], j);
     zero = zero || (dj == T(0));
     const T wij = row[0];
-    const T lij = wij / dj;
+    const T lij = wij * Recip(dj);
     if (lane < w && lane >= j) {
       B[lane * ld + j] = lane == j ? dj : lij;
     }
@@ -65,9 +82,8 @@ __device__ __noinline__ bool DiagonalBlockLdlt(T* B, int ld, int w) {
     for (int c = 1; c < kPanel; ++c) {
       // column j + c: A(i, j + c) -= W(i, j) L(j + c, j) for j < i, j + c <= i
       const T lcj = __shfl_sync(0xffffffffu, lij, (j + c) & 31);
-      if (lane > j && j + c <= lane) {
-        row[c] -= wij * lcj;
-      }
+      const T m = (lane > j && j + c <= lane) ? wij : T(0);
+      row[c] = fma(-m, lcj, row[c]);
     }
 #pragma unroll
     for (int c = 0; c + 1 < kPanel; ++c) {
@@ -152,8 +168,11 @@ __device__ __forceinline__ void PanelBody(const DeviceView& V, const SupernodeRe
   }
   __syncthreads();
   bool zero_pivot = false;
+  __shared__ T dinv[kPanel];
   if ((tid >> 5) == 0) {
     zero_pivot = DiagonalBlockLdlt<T>(&D[0][0], kPanel + 1, w);
+    __syncwarp();
+    dinv[tid] = Recip(D[tid][tid]);
   }
   __syncthreads();
   if (row_begin == c1) {
@@ -190,7 +209,7 @@ __device__ __forceinline__ void PanelBody(const DeviceView& V, const SupernodeRe
 #pragma unroll
     for (int j = 0; j < kPanel; ++j) {
       if (j < w) {
-        Fs[static_cast<int64_t>(c0 + j) * F + r] = y[j] / D[j][j];
+        Fs[static_cast<int64_t>(c0 + j) * F + r] = y[j] * dinv[j];
       }
     }
   }
@@ -220,15 +239,26 @@ __global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const
 /// the pivot block, `row_begin` onwards, get L(r, :) = A(r, :) L11^-T D^-1,
 /// panel by panel, in registers. Every block of a front repeats the pivot
 /// factorization; the one with row_begin == k writes L11 (the transposed
-/// storage of the diagonal panel blocks) and D.
+/// storage of the diagonal panel blocks) and D. Shared memory holds the pivot
+/// block padded to a multiple of 32 rows and columns (the padding is zero, so
+/// a narrow last panel needs no per-entry tests in the unrolled loops) and
+/// the reciprocals of the pivots.
 constexpr int kSmallPivots = 128;
+
+/// Dynamic shared memory of KFactorFront for fronts of at most k pivots.
+__host__ __device__ constexpr size_t FactorFrontSmem(int k) {
+  const size_t kpad = static_cast<size_t>((k + kPanel - 1) / kPanel * kPanel);
+  return (kpad * (kpad + 1) + kpad) * sizeof(double);
+}
 
 template <typename T>
 __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const SupernodeRec& S, int row_begin,
                                                 double* dvec, T* D) {
   const int k = S.ncols;
   const int F = S.F;
-  const int ld = k + 1;
+  const int kpad = (k + kPanel - 1) / kPanel * kPanel;
+  const int ld = kpad + 1;
+  T* dinv = D + kpad * ld;
   T* Fs = WorkFront<T>(V, S);
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
@@ -239,12 +269,19 @@ __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const Super
       D[r * ld + c] = Fs[static_cast<int64_t>(c) * F + r];
     }
   }
+  for (int idx = k * ld + tid; idx < kpad * ld; idx += blockDim.x) {
+    D[idx] = T(0);
+  }
   __syncthreads();
   bool zero_pivot = false;
   for (int p0 = 0; p0 < k; p0 += kPanel) {
     const int w = min(kPanel, k - p0);
     if (warp == 0) {
       zero_pivot = DiagonalBlockLdlt<T>(D + p0 * ld + p0, ld, w) || zero_pivot;
+      __syncwarp();
+      if (tid < w) {
+        dinv[p0 + tid] = Recip(D[(p0 + tid) * ld + p0 + tid]);
+      }
     }
     __syncthreads();
     // rows of the pivot block below this diagonal block (registers; the
@@ -265,7 +302,7 @@ __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const Super
       }
 #pragma unroll
       for (int j = 0; j < kPanel; ++j) {
-        row[j] = y[j] / D[(p0 + j) * ld + p0 + j];
+        row[j] = y[j] * dinv[p0 + j];
       }
     }
     __syncthreads();
@@ -325,26 +362,23 @@ __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const Super
         const T yl = yq[l] * D[(q0 + l) * ld + q0 + l];
 #pragma unroll
         for (int j = 0; j < kPanel; ++j) {
-          // rows p0 + j >= k (a narrow last panel) lie outside the pivot block
-          const T ljl = j < w ? D[(p0 + j) * ld + q0 + l] : T(0);
-          y[j] -= yl * ljl;
+          // rows p0 + j >= k (a narrow last panel) are the zero padding
+          y[j] -= yl * D[(p0 + j) * ld + q0 + l];
         }
       }
     }
-    // this panel's triangle
+    // this panel's triangle (padding rows leave y[j >= w] unchanged)
 #pragma unroll
     for (int j = 1; j < kPanel; ++j) {
 #pragma unroll
       for (int l = 0; l < j; ++l) {
-        if (j < w) {
-          y[j] -= y[l] * D[(p0 + j) * ld + p0 + l];
-        }
+        y[j] -= y[l] * D[(p0 + j) * ld + p0 + l];
       }
     }
 #pragma unroll
     for (int j = 0; j < kPanel; ++j) {
       if (j < w) {
-        Fs[static_cast<int64_t>(p0 + j) * F + r] = y[j] / D[(p0 + j) * ld + p0 + j];
+        Fs[static_cast<int64_t>(p0 + j) * F + r] = y[j] * dinv[p0 + j];
       }
     }
   }
@@ -664,7 +698,7 @@ void ConfigureSolveKernels(int max_front) {
   {
     std::lock_guard<std::mutex> lk(mu);
     if (!front_configured) {
-      const int bytes = kSmallPivots * (kSmallPivots + 1) * static_cast<int>(sizeof(double));
+      const int bytes = static_cast<int>(FactorFrontSmem(kSmallPivots));
       CudaCheck(cudaFuncSetAttribute(KFactorFront, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "smem attr");
       front_configured = true;
     }
@@ -692,7 +726,7 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
     const TaskRange sm = S.small_range[static_cast<size_t>(l)];
     if (sm.count > 0) {
       const int kmax = S.small_max_k[static_cast<size_t>(l)];
-      const size_t bytes = static_cast<size_t>(kmax) * (kmax + 1) * sizeof(double);
+      const size_t bytes = FactorFrontSmem(kmax);
       KFactorFront<<<static_cast<unsigned>(sm.count), S.front_rows, bytes, stream>>>(V, P.small_tasks + 2 * sm.begin,
                                                                                   P.dvec);
       ++launches;
