@@ -198,8 +198,9 @@ constexpr int kDefaultMargin = 3;
 constexpr int kMarginStep = 2;
 constexpr int kMaxMargin = 7;
 
-/// Analyses one instance at its current state.
-SymPiece AnalyzeInstance(const HostProblem& hp, int margin);
+/// Analyses one instance at its current state on up to `threads` host
+/// threads (0: all hardware threads).
+SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads = 0);
 
 /// Analyses the instances listed in `which` (all when null) into
 /// pieces[i], on up to hardware_concurrency threads.

@@ -152,6 +152,40 @@ void Dissect(const HostProblem& hp, int w0, int w1, int h0, int h1, std::vector<
   }
 }
 
+/// Runs fn(begin, end) over `threads` contiguous ranges of [0, n) (inline
+/// when one range suffices) and rethrows the first failure after all joined.
+template <typename Fn>
+void ParallelRanges(int threads, int64_t n, int64_t min_per_thread, Fn fn) {
+  const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(threads, n / std::max<int64_t>(1, min_per_thread)));
+  if (parts <= 1) {
+    fn(int64_t{0}, n);
+    return;
+  }
+  std::exception_ptr error;
+  std::mutex mu;
+  auto run = [&](int64_t b, int64_t e) {
+    try {
+      fn(b, e);
+    } catch (...) {
+      const std::lock_guard<std::mutex> lock(mu);
+      if (!error) {
+        error = std::current_exception();
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int64_t t = 1; t < parts; ++t) {
+    pool.emplace_back(run, n * t / parts, n * (t + 1) / parts);
+  }
+  run(0, n / parts);
+  for (std::thread& t : pool) {
+    t.join();
+  }
+  if (error) {
+    std::rethrow_exception(error);
+  }
+}
+
 /// Position of permuted row r inside the front index list of supernode s.
 inline int LocalIndex(const SupernodeRec& s, const int32_t* rows, int r) {
   if (r < s.first_col + s.ncols) {
@@ -391,7 +425,10 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
 
 }  // namespace
 
-SymPiece AnalyzeInstance(const HostProblem& hp, int margin) {
+SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
+  if (threads <= 0) {
+    threads = std::max(1, static_cast<int>(std::thread::hardware_concurrency()));
+  }
   // The per-pose coupling sets are derived from the current cells of every
   // point row, dilated by `margin` cells.
   SymPiece piece;
@@ -533,7 +570,7 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin) {
       }
     };
     const int workers =
-        std::clamp(static_cast<int>(std::thread::hardware_concurrency()), 1, std::max(1, (Fr + 7) / 8));
+        std::clamp(threads, 1, std::max(1, (Fr + 7) / 8));
     if (workers <= 1) {
       frame_work(0, Fr);
     } else {
@@ -551,22 +588,36 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin) {
         t.join();
       }
     }
-    // CSR by column; frames enter in ascending order
+    // CSR by column; frames enter in ascending order. Each thread owns a
+    // range of columns and scans every frame's list.
+    int64_t entries = 0;
     for (int f = 1; f < Fr; ++f) {
-      for (const int32_t col : frame_cols[static_cast<size_t>(f)]) {
-        ++nf_ptr[static_cast<size_t>(col) + 1];
-      }
+      entries += static_cast<int64_t>(frame_cols[static_cast<size_t>(f)].size());
     }
+    const int csr_threads = entries > (int64_t{1} << 15) ? threads : 1;
+    ParallelRanges(csr_threads, A, 1024, [&](int64_t c0, int64_t c1) {
+      for (int f = 1; f < Fr; ++f) {
+        for (const int32_t col : frame_cols[static_cast<size_t>(f)]) {
+          if (col >= c0 && col < c1) {
+            ++nf_ptr[static_cast<size_t>(col) + 1];
+          }
+        }
+      }
+    });
     for (int c = 0; c < A; ++c) {
       nf_ptr[static_cast<size_t>(c) + 1] += nf_ptr[static_cast<size_t>(c)];
     }
     nf.resize(static_cast<size_t>(nf_ptr[static_cast<size_t>(A)]));
     std::vector<int64_t> fill(nf_ptr.begin(), nf_ptr.end() - 1);
-    for (int f = 1; f < Fr; ++f) {
-      for (const int32_t col : frame_cols[static_cast<size_t>(f)]) {
-        nf[static_cast<size_t>(fill[static_cast<size_t>(col)]++)] = f;
+    ParallelRanges(csr_threads, A, 1024, [&](int64_t c0, int64_t c1) {
+      for (int f = 1; f < Fr; ++f) {
+        for (const int32_t col : frame_cols[static_cast<size_t>(f)]) {
+          if (col >= c0 && col < c1) {
+            nf[static_cast<size_t>(fill[static_cast<size_t>(col)]++)] = f;
+          }
+        }
       }
-    }
+    });
   }
   // pose pairs linked by odometry / relation rows
   std::vector<std::vector<int>> frame_links(static_cast<size_t>(Fr));
@@ -625,7 +676,9 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin) {
   }
   S.mp_frame.assign(nf.begin(), nf.end());
   S.mp_off.resize(S.mp_frame.size());
-  for (int c = 0; c < A; ++c) {
+  // columns are independent: each writes its own stencil slots and entries
+  ParallelRanges(threads, A, 512, [&](int64_t cb, int64_t ce) {
+  for (int c = static_cast<int>(cb); c < static_cast<int>(ce); ++c) {
     const int pc = lpinv[static_cast<size_t>(c)];
     const int s = S.col_owner[static_cast<size_t>(col_off + pc)];
     const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
@@ -666,6 +719,7 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin) {
       S.mp_off[static_cast<size_t>(e)] = col_base + r.ncols + (q - rows);
     }
   }
+  });
   // pose root
   if (Fr > 1) {
     const int s = S.col_owner[static_cast<size_t>(col_off + A)];
@@ -686,14 +740,21 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin) {
   S.fmp_col.resize(S.mp_frame.size());
   S.fmp_off.resize(S.mp_frame.size());
   {
+    // each thread owns a range of frames and scans every column in order
     std::vector<int64_t> fill(S.fmp_ptr.begin(), S.fmp_ptr.end() - 1);
-    for (int c = 0; c < A; ++c) {
-      for (int64_t e = S.mp_ptr[static_cast<size_t>(c)]; e < S.mp_ptr[static_cast<size_t>(c) + 1]; ++e) {
-        const int64_t q = fill[static_cast<size_t>(S.mp_frame[static_cast<size_t>(e)])]++;
-        S.fmp_col[static_cast<size_t>(q)] = c;
-        S.fmp_off[static_cast<size_t>(q)] = S.mp_off[static_cast<size_t>(e)];
+    const int tr_threads = S.mp_frame.size() > (size_t{1} << 15) ? threads : 1;
+    ParallelRanges(tr_threads, Fr, 8, [&](int64_t f0, int64_t f1) {
+      for (int c = 0; c < A; ++c) {
+        for (int64_t e = S.mp_ptr[static_cast<size_t>(c)]; e < S.mp_ptr[static_cast<size_t>(c) + 1]; ++e) {
+          const int f = S.mp_frame[static_cast<size_t>(e)];
+          if (f >= f0 && f < f1) {
+            const int64_t q = fill[static_cast<size_t>(f)]++;
+            S.fmp_col[static_cast<size_t>(q)] = c;
+            S.fmp_off[static_cast<size_t>(q)] = S.mp_off[static_cast<size_t>(e)];
+          }
+        }
       }
-    }
+    });
   }
   ComputeRel(S);
   return piece;
@@ -856,10 +917,13 @@ void AnalyzeInstances(const std::vector<HostProblem>& problems, const std::vecto
                                     std::max(1, static_cast<int>(std::thread::hardware_concurrency())));
   if (workers <= 1) {
     for (const int i : todo) {
-      pieces[static_cast<size_t>(i)] = AnalyzeInstance(problems[static_cast<size_t>(i)], margin[static_cast<size_t>(i)]);
+      pieces[static_cast<size_t>(i)] =
+          AnalyzeInstance(problems[static_cast<size_t>(i)], margin[static_cast<size_t>(i)], 0);
     }
     return;
   }
+  // instances in parallel, each analysis on the threads left over
+  const int inner = std::max(1, static_cast<int>(std::thread::hardware_concurrency()) / workers);
   std::atomic<size_t> next{0};
   std::exception_ptr error;
   std::mutex error_mu;
@@ -872,7 +936,7 @@ void AnalyzeInstances(const std::vector<HostProblem>& problems, const std::vecto
       const int i = todo[q];
       try {
         pieces[static_cast<size_t>(i)] =
-            AnalyzeInstance(problems[static_cast<size_t>(i)], margin[static_cast<size_t>(i)]);
+            AnalyzeInstance(problems[static_cast<size_t>(i)], margin[static_cast<size_t>(i)], inner);
       } catch (...) {
         const std::lock_guard<std::mutex> lock(error_mu);
         if (!error) {
