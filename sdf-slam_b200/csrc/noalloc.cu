@@ -28,7 +28,7 @@
 
 namespace sdfgpu {
 
-__global__ void KPanel(DeviceView V, const int32_t* tasks, double* dvec);
+__global__ void KPanel(DeviceView V, const int32_t* tasks, double* dvec, int rows);
 __global__ void KUpdate(DeviceView V, const int32_t* tasks, const double* dvec);
 __global__ void KForward(DeviceView V, const int32_t* level_sn, const double* dvec);
 __global__ void KBackward(DeviceView V, const int32_t* level_sn);
@@ -188,7 +188,8 @@ void DenseLdltSolveNoAlloc(int n, const double* a, const double* b, double* x) {
   V.active = d_active;
   double* dvec = base + kDvecOff;
   for (int t = 0; t < panels; ++t) {
-    KPanel<<<static_cast<unsigned>(panel_count[t]), kPanelRows, 0, s>>>(V, d_ptasks + 3 * kRowChunks * t, dvec);
+    KPanel<<<static_cast<unsigned>(panel_count[t]), kPanelRows, 0, s>>>(V, d_ptasks + 3 * kRowChunks * t, dvec,
+                                                                        kPanelRows);
     if (update_count[t] > 0) {
       KUpdate<<<static_cast<unsigned>(update_count[t]), 256, 0, s>>>(V, d_utasks + 4 * kTiles * kTiles * t, dvec);
     }
