@@ -31,6 +31,7 @@ SOURCES = {
     "noalloc.cu": [],
     "refine.cu": [],
     "problem_build.cpp": ["-x", "cu"],
+    "alloc.cpp": ["-x", "cu"],
     "symbolic.cpp": ["-x", "cu"],
     "capi.cpp": ["-x", "cu"],
     "server.cpp": ["-x", "cu"],

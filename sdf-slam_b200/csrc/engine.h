@@ -23,7 +23,16 @@ inline void CudaCheck(cudaError_t e, const char* what) {
   }
 }
 
-/// Owning device buffer.
+/// Block allocators with a per-device cache of freed blocks (alloc.cpp):
+/// `got` receives the block's size (the request rounded up to its class).
+/// A block may only be freed once no enqueued work uses it.
+void* CachedDeviceAlloc(size_t bytes, size_t* got);
+void CachedDeviceFree(void* p, size_t bytes);
+void* CachedHostAlloc(size_t bytes, size_t* got);
+void CachedHostFree(void* p, size_t bytes);
+
+/// Owning device buffer. Owners free (or grow) it only after their stream
+/// has drained.
 template <typename T>
 class DevBuf {
  public:
@@ -33,9 +42,10 @@ class DevBuf {
   ~DevBuf() { Free(); }
   void Free() {
     if (ptr_ != nullptr) {
-      cudaFree(ptr_);
+      CachedDeviceFree(ptr_, bytes_);
       ptr_ = nullptr;
       count_ = 0;
+      bytes_ = 0;
     }
   }
   void Alloc(size_t count) {
@@ -50,13 +60,8 @@ class DevBuf {
       count += count / 4;
     }
     const size_t bytes = std::max<size_t>(1, count) * sizeof(T);
-    const cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&ptr_), bytes);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      ptr_ = nullptr;
-      Fail(SDFGPU_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) + " bytes failed");
-    }
-    count_ = count;
+    ptr_ = static_cast<T*>(CachedDeviceAlloc(bytes, &bytes_));
+    count_ = bytes_ / sizeof(T);
   }
   void Upload(const std::vector<T>& v, cudaStream_t s) {
     Alloc(v.size());
@@ -70,6 +75,7 @@ class DevBuf {
  private:
   T* ptr_{nullptr};
   size_t count_{0};
+  size_t bytes_{0};
 };
 
 /// Device task lists of a symbolic analysis plus the launch parameters of
@@ -102,7 +108,7 @@ class HostBuf {
   HostBuf& operator=(const HostBuf&) = delete;
   ~HostBuf() {
     if (ptr_ != nullptr) {
-      cudaFreeHost(ptr_);
+      CachedHostFree(ptr_, bytes_);
     }
   }
   void Alloc(size_t count) {
@@ -110,12 +116,11 @@ class HostBuf {
       return;
     }
     if (ptr_ != nullptr) {
-      cudaFreeHost(ptr_);
+      CachedHostFree(ptr_, bytes_);
       ptr_ = nullptr;
     }
-    CudaCheck(cudaMallocHost(reinterpret_cast<void**>(&ptr_), std::max<size_t>(1, count) * sizeof(T)),
-              "cudaMallocHost");
-    count_ = count;
+    ptr_ = static_cast<T*>(CachedHostAlloc(std::max<size_t>(1, count) * sizeof(T), &bytes_));
+    count_ = bytes_ / sizeof(T);
   }
   T* get() const { return ptr_; }
   T& operator[](size_t i) const { return ptr_[i]; }
@@ -123,6 +128,7 @@ class HostBuf {
  private:
   T* ptr_{nullptr};
   size_t count_{0};
+  size_t bytes_{0};
 };
 
 struct IterTimes {
