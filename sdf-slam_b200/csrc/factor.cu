@@ -617,11 +617,19 @@ __device__ __forceinline__ void BackwardBody(const DeviceView& V, const Supernod
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int nwarps = blockDim.x >> 5;
+  // the ancestors' solution at this front's rows, gathered once into shared
+  // memory behind the k pivot slots (the gather's latency is paid once, not
+  // once per column)
+  double* xr = z + k;
+  for (int r = threadIdx.x; r < m; r += blockDim.x) {
+    xr[r] = V.xs[rows[r]];
+  }
+  __syncthreads();
   for (int j = warp; j < k; j += nwarps) {
     double acc = 0.0;
     const T* col = Fs + static_cast<int64_t>(j) * F + k;
     for (int r = lane; r < m; r += 32) {
-      acc += static_cast<double>(col[r]) * V.xs[rows[r]];
+      acc += static_cast<double>(col[r]) * xr[r];
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
