@@ -778,6 +778,7 @@ void Engine::UploadSchedule() {
   update_tasks_.Upload(sym_.update_tasks, stream_);
   small_tasks_.Upload(sym_.small_tasks, stream_);
   level_sn_.Upload(sym_.level_sn, stream_);
+  sn_.Upload(sym_.sn, stream_);
   CudaCheck(cudaStreamSynchronize(stream_), "schedule upload");
 }
 

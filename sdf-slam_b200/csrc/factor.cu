@@ -268,7 +268,7 @@ __host__ __device__ constexpr size_t FactorFrontSmem(int k) {
 }
 
 template <typename T>
-__device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const SupernodeRec& S, int row_begin,
+__device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const SupernodeRec& S, int row_begin, int rows,
                                                 double* dvec, T* D, T (*lbuf)[kPanel], T (*wbuf)[kPanel]) {
   const int k = S.ncols;
   const int F = S.F;
@@ -278,11 +278,14 @@ __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const Super
   T* Fs = WorkFront<T>(V, S);
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
-  for (int idx = tid; idx < k * k; idx += blockDim.x) {
-    const int r = idx % k;
-    const int c = idx / k;
-    if (r >= c) {
-      D[r * ld + c] = Fs[static_cast<int64_t>(c) * F + r];
+  const int nwarps = static_cast<int>(blockDim.x >> 5);
+  const int lane = tid & 31;
+  // one warp per column: coalesced loads of the column's lower part
+  for (int c = warp; c < k; c += nwarps) {
+    const T* src = Fs + static_cast<int64_t>(c) * F;
+#pragma unroll 4
+    for (int r = c + lane; r < k; r += 32) {
+      D[r * ld + c] = src[r];
     }
   }
   for (int idx = k * ld + tid; idx < kpad * ld; idx += blockDim.x) {
@@ -321,28 +324,36 @@ __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const Super
       }
     }
     __syncthreads();
-    // rank-w update of the trailing pivot block
-    const int rest = k - p0 - w;
-    for (int idx = tid; idx < rest * rest; idx += blockDim.x) {
-      const int r = p0 + w + idx % rest;
-      const int c = p0 + w + idx / rest;
-      if (r >= c) {
-        T acc = T(0);
-        for (int l = 0; l < w; ++l) {
-          acc += (D[r * ld + p0 + l] * D[(p0 + l) * ld + p0 + l]) * D[c * ld + p0 + l];
+    // rank-w update of the trailing pivot block: thread per column c with
+    // d_l L(c, l) in registers, rows r >= c read as broadcasts (the panel is
+    // full width here because a trailing column exists)
+    for (int c = p0 + w + tid; c < k; c += blockDim.x) {
+      T wc[kPanel];
+#pragma unroll
+      for (int l = 0; l < kPanel; ++l) {
+        wc[l] = D[c * ld + p0 + l] * D[(p0 + l) * ld + p0 + l];
+      }
+      for (int r = c; r < k; ++r) {
+        const T* lr = D + r * ld + p0;
+        T a0 = T(0);
+        T a1 = T(0);
+#pragma unroll
+        for (int l = 0; l < kPanel; l += 2) {
+          a0 = fma(lr[l], wc[l], a0);
+          a1 = fma(lr[l + 1], wc[l + 1], a1);
         }
-        D[r * ld + c] -= acc;
+        D[r * ld + c] -= a0 + a1;
       }
     }
     __syncthreads();
   }
   if (row_begin == k) {
-    for (int idx = tid; idx < k * k; idx += blockDim.x) {
-      const int r = idx % k;
-      const int c = idx / k;
-      if (r > c) {
-        const bool same = (r / kPanel) == (c / kPanel);
-        Fs[same ? static_cast<int64_t>(r) * F + c : static_cast<int64_t>(c) * F + r] = D[r * ld + c];
+    // L11 goes to the pivot block's upper triangle only: the other tasks of
+    // this front may still be reading its lower triangle (the assembled A11)
+    for (int r = warp; r < k; r += nwarps) {
+      T* dst = Fs + static_cast<int64_t>(r) * F;
+      for (int c = lane; c < r; c += 32) {
+        dst[c] = D[r * ld + c];
       }
     }
     for (int j = tid; j < k; j += blockDim.x) {
@@ -354,7 +365,7 @@ __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const Super
   }
   // rows below the pivot block: thread per row, panel by panel
   const int r = row_begin + tid;
-  if (r >= F || r >= row_begin + static_cast<int>(blockDim.x)) {
+  if (r >= F || tid >= rows) {
     return;
   }
   for (int p0 = 0; p0 < k; p0 += kPanel) {
@@ -401,7 +412,7 @@ __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const Super
 
 __global__ void __launch_bounds__(256) KFactorFront(DeviceView V, const int32_t* tasks, double* dvec) {
   extern __shared__ double sm[];
-  const int32_t* t = tasks + 2 * static_cast<int64_t>(blockIdx.x);
+  const int32_t* t = tasks + 3 * static_cast<int64_t>(blockIdx.x);
   const SupernodeRec S = V.sn[t[0]];
   if (V.active[S.instance] == 0) {
     return;
@@ -409,9 +420,9 @@ __global__ void __launch_bounds__(256) KFactorFront(DeviceView V, const int32_t*
   __shared__ double lw[4][kPanel];
   if (Fp32Front(V, S)) {
     auto* l = reinterpret_cast<float(*)[kPanel]>(&lw[0][0]);
-    FactorFrontBody<float>(V, S, t[1], dvec, reinterpret_cast<float*>(sm), l, l + 2);
+    FactorFrontBody<float>(V, S, t[1], t[2], dvec, reinterpret_cast<float*>(sm), l, l + 2);
   } else {
-    FactorFrontBody<double>(V, S, t[1], dvec, sm, lw, lw + 2);
+    FactorFrontBody<double>(V, S, t[1], t[2], dvec, sm, lw, lw + 2);
   }
 }
 
@@ -572,8 +583,15 @@ __device__ __forceinline__ void ForwardBody(const DeviceView& V, const Supernode
     __syncthreads();
     for (int r = p0 + w + threadIdx.x; r < F; r += blockDim.x) {
       double acc = v[r];
-      for (int j = 0; j < w; ++j) {
-        acc -= static_cast<double>(Fs[static_cast<int64_t>(p0 + j) * F + r]) * v[p0 + j];
+      if (S.upper_l11 != 0 && r < k) {
+        const T* lr = Fs + static_cast<int64_t>(r) * F + p0;
+        for (int j = 0; j < w; ++j) {
+          acc -= static_cast<double>(lr[j]) * v[p0 + j];
+        }
+      } else {
+        for (int j = 0; j < w; ++j) {
+          acc -= static_cast<double>(Fs[static_cast<int64_t>(p0 + j) * F + r]) * v[p0 + j];
+        }
       }
       v[r] = acc;
     }
@@ -646,9 +664,15 @@ __device__ __forceinline__ void BackwardBody(const DeviceView& V, const Supernod
     // later pivots of this front: z[p0 + j] -= sum_{i >= p0 + w} L(i, p0 + j) x_i
     for (int j = warp; j < w; j += nwarps) {
       double acc = 0.0;
-      const T* col = Fs + static_cast<int64_t>(p0 + j) * F;
-      for (int i = p0 + w + lane; i < k; i += 32) {
-        acc += static_cast<double>(col[i]) * z[i];
+      if (S.upper_l11 != 0) {
+        for (int i = p0 + w + lane; i < k; i += 32) {
+          acc += static_cast<double>(Fs[static_cast<int64_t>(i) * F + p0 + j]) * z[i];
+        }
+      } else {
+        const T* col = Fs + static_cast<int64_t>(p0 + j) * F;
+        for (int i = p0 + w + lane; i < k; i += 32) {
+          acc += static_cast<double>(col[i]) * z[i];
+        }
       }
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
@@ -756,7 +780,7 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
     if (sm.count > 0) {
       const int kmax = S.small_max_k[static_cast<size_t>(l)];
       const size_t bytes = FactorFrontSmem(kmax);
-      KFactorFront<<<static_cast<unsigned>(sm.count), S.front_rows, bytes, stream>>>(V, P.small_tasks + 2 * sm.begin,
+      KFactorFront<<<static_cast<unsigned>(sm.count), S.front_rows, bytes, stream>>>(V, P.small_tasks + 3 * sm.begin,
                                                                                   P.dvec);
       ++launches;
     }

@@ -89,6 +89,7 @@ struct SupernodeRec {
   int32_t parent;     // -1 for a root
   int32_t instance;
   int32_t pose_root;  // 1: the dense pose block of its instance
+  int32_t upper_l11;  // 1: L of the pivot block is stored transposed in its upper triangle
 };
 
 /// A contiguous block of work items of one kernel launch in the level
@@ -129,9 +130,10 @@ struct Symbolic {
   std::vector<TaskRange> update_range;       // per (level, panel) flattened
   std::vector<int32_t> panel_index_base;     // level -> first (level,panel) slot
   // fronts with at most small_pivots pivots: one factorization kernel per
-  // level, tasks (sn, first row of the chunk below the pivot block) of
-  // front_rows rows (the block size); larger fronts: panel tasks of
-  // panel_rows rows. The three are the schedule an autotuner picks.
+  // level, tasks (sn, first row of the chunk below the pivot block, rows in
+  // the chunk) with front_rows threads per block (rows per chunk shrink to
+  // 64 or 32 on levels that would not fill the GPU); larger fronts: panel
+  // tasks of panel_rows rows. The three are the schedule an autotuner picks.
   int small_pivots{128};
   int front_rows{256};
   int panel_rows{128};

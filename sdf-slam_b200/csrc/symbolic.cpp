@@ -296,6 +296,13 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   const int kPanelRows = S.panel_rows;
   constexpr int kEaCols = 16;
   const int kFrontRows = S.front_rows;
+  // fronts factored by the single-kernel path keep the pivot block's lower
+  // triangle (read by every task of the front) and store L11 transposed
+  for (SupernodeRec& r : S.sn) {
+    r.upper_l11 = r.ncols <= S.small_pivots ? 1 : 0;
+  }
+  // blocks that keep every SM of a B200 (148) busy
+  constexpr int64_t kFillBlocks = 148;
   const int small = S.small_pivots;
   S.level_panels.assign(static_cast<size_t>(levels), 0);
   S.panel_index_base.assign(static_cast<size_t>(levels) + 1, 0);
@@ -304,15 +311,33 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   S.small_tasks.clear();
   for (int l = 0; l < levels; ++l) {
     int maxp = 0;
-    S.small_range[static_cast<size_t>(l)].begin = static_cast<int64_t>(S.small_tasks.size() / 2);
+    S.small_range[static_cast<size_t>(l)].begin = static_cast<int64_t>(S.small_tasks.size() / 3);
+    // Rows per single-kernel task: the schedule's front_rows, or fewer where
+    // the level would not fill the GPU (every task repeats the pivot block,
+    // so small chunks shorten the level when SMs would otherwise idle).
+    int chunk = kFrontRows;
+    for (const int cand : {kFrontRows, 64, 32}) {
+      chunk = cand;
+      int64_t blocks = 0;
+      for (int q = S.level_begin[static_cast<size_t>(l)]; q < S.level_begin[static_cast<size_t>(l) + 1]; ++q) {
+        const SupernodeRec& r = S.sn[static_cast<size_t>(S.level_sn[static_cast<size_t>(q)])];
+        if (r.ncols <= small) {
+          blocks += std::max(1, (r.nrows + cand - 1) / cand);
+        }
+      }
+      if (blocks >= kFillBlocks) {
+        break;
+      }
+    }
     for (int q = S.level_begin[static_cast<size_t>(l)]; q < S.level_begin[static_cast<size_t>(l) + 1]; ++q) {
       const int sid = S.level_sn[static_cast<size_t>(q)];
       const SupernodeRec& r = S.sn[static_cast<size_t>(sid)];
       if (r.ncols <= small) {
-        const int chunks = std::max(1, (r.nrows + kFrontRows - 1) / kFrontRows);
+        const int chunks = std::max(1, (r.nrows + chunk - 1) / chunk);
         for (int ch = 0; ch < chunks; ++ch) {
           S.small_tasks.push_back(sid);
-          S.small_tasks.push_back(r.ncols + ch * kFrontRows);
+          S.small_tasks.push_back(r.ncols + ch * chunk);
+          S.small_tasks.push_back(chunk);
         }
         S.small_max_k[static_cast<size_t>(l)] = std::max(S.small_max_k[static_cast<size_t>(l)], r.ncols);
         continue;
@@ -320,7 +345,7 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
       maxp = std::max(maxp, (r.ncols + B - 1) / B);
     }
     S.small_range[static_cast<size_t>(l)].count =
-        static_cast<int64_t>(S.small_tasks.size() / 2) - S.small_range[static_cast<size_t>(l)].begin;
+        static_cast<int64_t>(S.small_tasks.size() / 3) - S.small_range[static_cast<size_t>(l)].begin;
     S.level_panels[static_cast<size_t>(l)] = maxp;
     S.panel_index_base[static_cast<size_t>(l) + 1] = S.panel_index_base[static_cast<size_t>(l)] + maxp;
   }
