@@ -461,10 +461,27 @@ __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeR
       acc[a][b] = T(0);
     }
   }
-  for (int kk = kb; kk < ke; kk += kPanel) {
+  // the tile's current values, loaded now so that their latency hides
+  // behind the K loop (no other block touches this tile)
+  T cur[4][4];
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int c = cc0 + ty + 16 * b;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int r = r0 + tx + 16 * a;
+      cur[a][b] = (c < clim && r < F && r >= c) ? Fs[static_cast<int64_t>(c) * F + r] : T(0);
+    }
+  }
+  // K chunks of kPanel columns: the next chunk is loaded into registers
+  // while the current one is multiplied out of shared memory
+  constexpr int kPerThread = (kPanel * kTile) / 256;
+  T ra[kPerThread];
+  T rb[kPerThread];
+  auto load_chunk = [&](int kk) {
     const int kw = min(kPanel, ke - kk);
 #pragma unroll
-    for (int q = 0; q < (kPanel * kTile) / 256; ++q) {
+    for (int q = 0; q < kPerThread; ++q) {
       const int idx = tid + 256 * q;
       const int rr = idx % kTile;
       const int l = idx / kTile;
@@ -479,10 +496,24 @@ __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeR
           bv = Fs[colbase + cc0 + rr];
         }
       }
-      As[l][rr] = av;
-      Bs[l][rr] = bv;
+      ra[q] = av;
+      rb[q] = bv;
+    }
+  };
+  if (kb < ke) {
+    load_chunk(kb);
+  }
+  for (int kk = kb; kk < ke; kk += kPanel) {
+#pragma unroll
+    for (int q = 0; q < kPerThread; ++q) {
+      const int idx = tid + 256 * q;
+      As[idx / kTile][idx % kTile] = ra[q];
+      Bs[idx / kTile][idx % kTile] = rb[q];
     }
     __syncthreads();
+    if (kk + kPanel < ke) {
+      load_chunk(kk + kPanel);
+    }
 #pragma unroll 8
     for (int l = 0; l < kPanel; ++l) {
       T av[4];
@@ -512,7 +543,7 @@ __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeR
     for (int a = 0; a < 4; ++a) {
       const int r = r0 + tx + 16 * a;
       if (r < F && r >= c) {
-        Fs[static_cast<int64_t>(c) * F + r] -= acc[a][b];
+        Fs[static_cast<int64_t>(c) * F + r] = cur[a][b] - acc[a][b];
       }
     }
   }
@@ -521,7 +552,7 @@ __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeR
 /// Tiled rank-k update C -= L_I D L_J^T (lower part only). panel >= 0:
 /// update of the remaining pivot columns by one panel; panel == -1: Schur
 /// complement of the trailing m x m block by all k pivots.
-__global__ void __launch_bounds__(256) KUpdate(DeviceView V, const int32_t* tasks, const double* dvec) {
+__global__ void __launch_bounds__(256, 2) KUpdate(DeviceView V, const int32_t* tasks, const double* dvec) {
   const int32_t* t = tasks + 4 * static_cast<int64_t>(blockIdx.x);
   const SupernodeRec S = V.sn[t[0]];
   if (V.active[S.instance] == 0) {

@@ -362,14 +362,28 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
     const int qe = S.level_begin[static_cast<size_t>(l) + 1];
     // extend-add: parent columns in chunks, only for supernodes with children
     S.ea_range[static_cast<size_t>(l)].begin = static_cast<int64_t>(S.ea_tasks.size() / 4);
+    // narrower column ranges on levels that would not fill the GPU
+    int ea_cols = kEaCols;
+    {
+      int64_t tasks = 0;
+      for (int q = qb; q < qe; ++q) {
+        const SupernodeRec& r = S.sn[static_cast<size_t>(S.level_sn[static_cast<size_t>(q)])];
+        if (r.child_count > 0) {
+          tasks += (r.F + kEaCols - 1) / kEaCols;
+        }
+      }
+      if (tasks < 2 * kFillBlocks) {
+        ea_cols = 4;
+      }
+    }
     for (int q = qb; q < qe; ++q) {
       const int s = S.level_sn[static_cast<size_t>(q)];
       const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
       if (r.child_count == 0) {
         continue;
       }
-      for (int c = 0; c < r.F; c += kEaCols) {
-        const int chi = std::min(r.F, c + kEaCols);
+      for (int c = 0; c < r.F; c += ea_cols) {
+        const int chi = std::min(r.F, c + ea_cols);
         S.ea_tasks.push_back(s);
         S.ea_tasks.push_back(c);
         S.ea_tasks.push_back(chi);
