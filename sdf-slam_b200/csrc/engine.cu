@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <future>
 #include <map>
 #include <utility>
 
@@ -85,8 +86,17 @@ Engine::Engine(std::vector<HostProblem> problems) : host_(std::move(problems)) {
   h_lam_.Alloc(host_.size());
   h_seg_.Alloc(5 * host_.size());
   h_status_.Alloc(host_.size());
-  UploadProblem();
-  Analyze();
+  // the symbolic analysis (host only) runs while the problem is uploaded
+  std::future<void> analysis = std::async(std::launch::async, [this] { AnalyzeHost(); });
+  try {
+    UploadProblem();
+  } catch (...) {
+    analysis.wait();
+    throw;
+  }
+  analysis.get();
+  mixed_.assign(host_.size(), 0);  // plain FP64 until a solve asks otherwise
+  UploadSymbolic();
 }
 
 void Engine::DropGraph() {
@@ -363,13 +373,12 @@ void Engine::UploadProblem() {
   CudaCheck(cudaStreamSynchronize(s), "upload");
 }
 
-void Engine::Analyze() {
+void Engine::AnalyzeHost() {
   margin_.assign(host_.size(), kDefaultMargin);
   pieces_.assign(host_.size(), SymPiece{});
   pending_.clear();
   AnalyzeInstances(host_, margin_, pieces_, nullptr);
   sym_ = Concatenate(pieces_, layout_, 32, 64, sched_);
-  UploadSymbolic();
 }
 
 void Engine::UploadSymbolic() {

@@ -204,7 +204,8 @@ class Engine {
  private:
   void BuildLayout();
   void UploadProblem();
-  void Analyze();
+  /// Symbolic analysis of every instance at its current state (host only).
+  void AnalyzeHost();
   void UploadSymbolic();
   void UploadSchedule();
   /// Per-instance precision of the coming solve (1: mixed) and refinement
