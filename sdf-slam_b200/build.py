@@ -32,11 +32,12 @@ SOURCES = {
     "refine.cu": [],
     "problem_build.cpp": ["-x", "cu"],
     "alloc.cpp": ["-x", "cu"],
+    "host_pool.cpp": ["-x", "cu"],
     "symbolic.cpp": ["-x", "cu"],
     "capi.cpp": ["-x", "cu"],
     "server.cpp": ["-x", "cu"],
 }
-HEADERS = ["internal.h", "device.cuh", "engine.h", "ldlt.h", "server.h"]
+HEADERS = ["internal.h", "device.cuh", "engine.h", "ldlt.h", "server.h", "host_pool.h"]
 
 
 def _newest_header() -> float:

@@ -378,7 +378,16 @@ void Engine::AnalyzeHost() {
   pieces_.assign(host_.size(), SymPiece{});
   pending_.clear();
   AnalyzeInstances(host_, margin_, pieces_, nullptr);
-  sym_ = Concatenate(pieces_, layout_, 32, 64, sched_);
+  sym_ = GlobalStructure();
+}
+
+Symbolic Engine::GlobalStructure() {
+  // a single instance's piece is re-analysed whenever its structure changes,
+  // so it is not kept
+  if (pieces_.size() == 1) {
+    return ConcatenateOne(std::move(pieces_[0]), 32, 64, sched_);
+  }
+  return Concatenate(pieces_, layout_, 32, 64, sched_);
 }
 
 void Engine::UploadSymbolic() {
@@ -772,7 +781,7 @@ void Engine::Reanalyze(const std::vector<int>& which) {
     margin_[static_cast<size_t>(i)] = std::min(margin_[static_cast<size_t>(i)] + kMarginStep, kMaxMargin);
   }
   AnalyzeInstances(host_, margin_, pieces_, &which);
-  sym_ = Concatenate(pieces_, layout_, 32, 64, sched_);
+  sym_ = GlobalStructure();
   UploadSymbolic();
   ++times_.reanalyses;
   times_.reanalysis_host += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

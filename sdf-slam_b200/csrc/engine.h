@@ -206,6 +206,8 @@ class Engine {
   void UploadProblem();
   /// Symbolic analysis of every instance at its current state (host only).
   void AnalyzeHost();
+  /// Global structure of the current pieces (a single piece is taken over).
+  Symbolic GlobalStructure();
   void UploadSymbolic();
   void UploadSchedule();
   /// Per-instance precision of the coming solve (1: mixed) and refinement

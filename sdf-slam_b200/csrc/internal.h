@@ -205,7 +205,8 @@ constexpr int kMaxMargin = 7;
 SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads = 0);
 
 /// Analyses the instances listed in `which` (all when null) into
-/// pieces[i], on up to hardware_concurrency threads.
+/// pieces[i] on the host pool: one instance per thread when there are at
+/// least as many instances as threads, else one after another on all.
 void AnalyzeInstances(const std::vector<HostProblem>& problems, const std::vector<int>& margin,
                       std::vector<SymPiece>& pieces, const std::vector<int>* which);
 
@@ -220,6 +221,10 @@ struct Schedule {
 /// `layout`.
 Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<InstanceLayout>& layout,
                      int panel_width, int tile, const Schedule& sched = Schedule{});
+
+/// Concatenate for a single instance: takes the piece's arrays over instead
+/// of copying them (the piece is left empty).
+Symbolic ConcatenateOne(SymPiece&& piece, int panel_width, int tile, const Schedule& sched = Schedule{});
 
 /// Rebuilds the level schedule and task lists of S for another schedule.
 void Reschedule(Symbolic& S, const Schedule& sched);

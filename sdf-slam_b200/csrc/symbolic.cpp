@@ -22,14 +22,11 @@
 // that structure. Any contiguous partition gives a valid assembly tree this
 // way.
 #include <algorithm>
-#include <atomic>
 #include <cmath>
-#include <exception>
 #include <functional>
-#include <mutex>
 #include <numeric>
-#include <thread>
 
+#include "host_pool.h"
 #include "internal.h"
 
 namespace sdfgpu {
@@ -45,10 +42,47 @@ struct LocalSym {
   std::vector<std::vector<int>> children;
 };
 
+/// Per-thread map from a column to a value, valid while the column's stamp
+/// equals the current generation: starting a new map costs nothing. Pool
+/// workers keep theirs from one problem to the next.
+struct ColumnMap {
+  std::vector<uint32_t> stamp;
+  std::vector<int32_t> value;
+  uint32_t gen = 0;
+  void Begin(size_t n) {
+    if (stamp.size() < n) {
+      stamp.resize(n, 0u);
+      value.resize(n, 0);
+    }
+    if (++gen == 0u) {
+      std::fill(stamp.begin(), stamp.end(), 0u);
+      gen = 1u;
+    }
+  }
+  bool Has(int i) const { return stamp[static_cast<size_t>(i)] == gen; }
+  void Set(int i, int32_t v) {
+    stamp[static_cast<size_t>(i)] = gen;
+    value[static_cast<size_t>(i)] = v;
+  }
+  int32_t Get(int i) const { return value[static_cast<size_t>(i)]; }
+};
+
+ColumnMap& ThreadColumnMap() {
+  thread_local ColumnMap map;
+  return map;
+}
+
 /// Generic supernodal symbolic factorization over a partition of the
 /// permuted columns. lower(col, out) appends the pattern rows > col.
+///
+/// `subtrees` lists ranges [begin, end) of supernodes that are closed under
+/// the assembly tree below them (every child of a member is a member, as
+/// for the groups of one nested-dissection region): those ranges run in
+/// parallel, the remaining supernodes afterwards in order. Children lists
+/// ascend, so the result equals the plain sequential pass.
 LocalSym SupernodalSymbolic(int n, const std::function<void(int, std::vector<int>&)>& lower,
-                            const std::vector<int>& sn_begin) {
+                            const std::vector<int>& sn_begin,
+                            const std::vector<std::pair<int, int>>& subtrees = {}) {
   LocalSym L;
   L.sn_begin = sn_begin;
   const int S = static_cast<int>(sn_begin.size()) - 1;
@@ -61,26 +95,35 @@ LocalSym SupernodalSymbolic(int n, const std::function<void(int, std::vector<int
       owner[static_cast<size_t>(c)] = s;
     }
   }
-  std::vector<int> mark(static_cast<size_t>(n), -1);
-  std::vector<int> tmp;
-  for (int s = 0; s < S; ++s) {
+  // range of the subtree holding each supernode (-1: none)
+  std::vector<int> in_range(static_cast<size_t>(S), -1);
+  for (size_t t = 0; t < subtrees.size(); ++t) {
+    for (int s = subtrees[t].first; s < subtrees[t].second; ++s) {
+      in_range[static_cast<size_t>(s)] = static_cast<int>(t);
+    }
+  }
+  // Structure of supernode s. It joins its parent's children list here when
+  // link_all is set or the parent lies in the same subtree range; the other
+  // links are made after the parallel part.
+  auto structure = [&](int s, std::vector<int>& tmp, ColumnMap& mark, bool link_all, int range) {
     const int b = sn_begin[static_cast<size_t>(s)];
     const int e = sn_begin[static_cast<size_t>(s) + 1];
     std::vector<int>& R = L.rows[static_cast<size_t>(s)];
+    mark.Begin(static_cast<size_t>(n));
     for (int c = b; c < e; ++c) {
       tmp.clear();
       lower(c, tmp);
       for (const int r : tmp) {
-        if (r >= e && mark[static_cast<size_t>(r)] != s) {
-          mark[static_cast<size_t>(r)] = s;
+        if (r >= e && !mark.Has(r)) {
+          mark.Set(r, 0);
           R.push_back(r);
         }
       }
     }
     for (const int ch : L.children[static_cast<size_t>(s)]) {
       for (const int r : L.rows[static_cast<size_t>(ch)]) {
-        if (r >= e && mark[static_cast<size_t>(r)] != s) {
-          mark[static_cast<size_t>(r)] = s;
+        if (r >= e && !mark.Has(r)) {
+          mark.Set(r, 0);
           R.push_back(r);
         }
       }
@@ -89,15 +132,56 @@ LocalSym SupernodalSymbolic(int n, const std::function<void(int, std::vector<int
     if (!R.empty()) {
       const int p = owner[static_cast<size_t>(R.front())];
       L.parent[static_cast<size_t>(s)] = p;
+      if (link_all || in_range[static_cast<size_t>(p)] == range) {
+        L.children[static_cast<size_t>(p)].push_back(s);
+      }
+    }
+  };
+  PoolRun(static_cast<int>(subtrees.size()), [&](int t) {
+    std::vector<int> tmp;
+    ColumnMap& mark = ThreadColumnMap();
+    for (int s = subtrees[static_cast<size_t>(t)].first; s < subtrees[static_cast<size_t>(t)].second; ++s) {
+      structure(s, tmp, mark, false, t);
+    }
+  });
+  // links from the subtrees to the supernodes above them, ascending
+  for (int s = 0; s < S; ++s) {
+    const int p = L.parent[static_cast<size_t>(s)];
+    if (in_range[static_cast<size_t>(s)] >= 0 && p >= 0 &&
+        in_range[static_cast<size_t>(p)] != in_range[static_cast<size_t>(s)]) {
       L.children[static_cast<size_t>(p)].push_back(s);
     }
+  }
+  {
+    std::vector<int> tmp;
+    ColumnMap& mark = ThreadColumnMap();
+    for (int s = 0; s < S; ++s) {
+      if (in_range[static_cast<size_t>(s)] < 0) {
+        structure(s, tmp, mark, true, -1);
+      }
+    }
+  }
+  for (std::vector<int>& ch : L.children) {
+    std::sort(ch.begin(), ch.end());
   }
   return L;
 }
 
 /// Geometric nested dissection of the active nodes of a grid. Appends groups
-/// of local natural columns in postorder (halves, then separator).
-void Dissect(const HostProblem& hp, int w0, int w1, int h0, int h1, std::vector<std::vector<int>>& groups) {
+/// of local natural columns in postorder (halves, then separator). The
+/// regions `split` levels down each record their range of groups in
+/// `subtrees` (none when split < 0).
+void Dissect(const HostProblem& hp, int w0, int w1, int h0, int h1, std::vector<std::vector<int>>& groups,
+             int depth, int split, std::vector<std::pair<int, int>>& subtrees) {
+  if (depth == split) {
+    // the groups of this region form one subtree of the assembly tree
+    const int begin = static_cast<int>(groups.size());
+    Dissect(hp, w0, w1, h0, h1, groups, depth + 1, split, subtrees);
+    if (static_cast<int>(groups.size()) > begin) {
+      subtrees.emplace_back(begin, static_cast<int>(groups.size()));
+    }
+    return;
+  }
   const int width = w1 - w0;
   const int height = h1 - h0;
   if (width <= 0 || height <= 0) {
@@ -128,8 +212,8 @@ void Dissect(const HostProblem& hp, int w0, int w1, int h0, int h1, std::vector<
   std::vector<int> sep;
   if (width >= height) {
     const int mid = w0 + width / 2;
-    Dissect(hp, w0, mid, h0, h1, groups);
-    Dissect(hp, mid + 1, w1, h0, h1, groups);
+    Dissect(hp, w0, mid, h0, h1, groups, depth + 1, split, subtrees);
+    Dissect(hp, mid + 1, w1, h0, h1, groups, depth + 1, split, subtrees);
     for (int h = h0; h < h1; ++h) {
       const int c = hp.node_to_active[static_cast<size_t>(h) * hp.nx + mid];
       if (c >= 0) {
@@ -138,8 +222,8 @@ void Dissect(const HostProblem& hp, int w0, int w1, int h0, int h1, std::vector<
     }
   } else {
     const int mid = h0 + height / 2;
-    Dissect(hp, w0, w1, h0, mid, groups);
-    Dissect(hp, w0, w1, mid + 1, h1, groups);
+    Dissect(hp, w0, w1, h0, mid, groups, depth + 1, split, subtrees);
+    Dissect(hp, w0, w1, mid + 1, h1, groups, depth + 1, split, subtrees);
     for (int w = w0; w < w1; ++w) {
       const int c = hp.node_to_active[static_cast<size_t>(mid) * hp.nx + w];
       if (c >= 0) {
@@ -149,40 +233,6 @@ void Dissect(const HostProblem& hp, int w0, int w1, int h0, int h1, std::vector<
   }
   if (!sep.empty()) {
     groups.push_back(std::move(sep));
-  }
-}
-
-/// Runs fn(begin, end) over `threads` contiguous ranges of [0, n) (inline
-/// when one range suffices) and rethrows the first failure after all joined.
-template <typename Fn>
-void ParallelRanges(int threads, int64_t n, int64_t min_per_thread, Fn fn) {
-  const int64_t parts = std::max<int64_t>(1, std::min<int64_t>(threads, n / std::max<int64_t>(1, min_per_thread)));
-  if (parts <= 1) {
-    fn(int64_t{0}, n);
-    return;
-  }
-  std::exception_ptr error;
-  std::mutex mu;
-  auto run = [&](int64_t b, int64_t e) {
-    try {
-      fn(b, e);
-    } catch (...) {
-      const std::lock_guard<std::mutex> lock(mu);
-      if (!error) {
-        error = std::current_exception();
-      }
-    }
-  };
-  std::vector<std::thread> pool;
-  for (int64_t t = 1; t < parts; ++t) {
-    pool.emplace_back(run, n * t / parts, n * (t + 1) / parts);
-  }
-  run(0, n / parts);
-  for (std::thread& t : pool) {
-    t.join();
-  }
-  if (error) {
-    std::rethrow_exception(error);
   }
 }
 
@@ -376,24 +426,31 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
         ea_cols = 4;
       }
     }
+    std::vector<int32_t> cursor;
     for (int q = qb; q < qe; ++q) {
       const int s = S.level_sn[static_cast<size_t>(q)];
       const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
       if (r.child_count == 0) {
         continue;
       }
+      // per child: the range of its update columns that land in [c, chi);
+      // the positions ascend, so one cursor per child walks them once
+      cursor.assign(static_cast<size_t>(r.child_count), 0);
       for (int c = 0; c < r.F; c += ea_cols) {
         const int chi = std::min(r.F, c + ea_cols);
         S.ea_tasks.push_back(s);
         S.ea_tasks.push_back(c);
         S.ea_tasks.push_back(chi);
         S.ea_tasks.push_back(static_cast<int32_t>(S.ea_child.size()));
-        // per child: the range of its update columns that land in [c, chi)
         for (int ci = 0; ci < r.child_count; ++ci) {
           const SupernodeRec& ch = S.sn[static_cast<size_t>(S.child_list[static_cast<size_t>(r.child_begin + ci)])];
           const int32_t* rel = S.sn_rel.data() + ch.rows_off;
-          S.ea_child.push_back(static_cast<int32_t>(std::lower_bound(rel, rel + ch.nrows, c) - rel));
-          S.ea_child.push_back(static_cast<int32_t>(std::lower_bound(rel, rel + ch.nrows, chi) - rel));
+          int32_t& k = cursor[static_cast<size_t>(ci)];
+          S.ea_child.push_back(k);
+          while (k < ch.nrows && rel[k] < chi) {
+            ++k;
+          }
+          S.ea_child.push_back(k);
         }
       }
     }
@@ -466,7 +523,10 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
 
 SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
   if (threads <= 0) {
-    threads = std::max(1, static_cast<int>(std::thread::hardware_concurrency()));
+    threads = PoolThreads();
+  }
+  if (margin < 0) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT, "negative coupling margin");
   }
   // The per-pose coupling sets are derived from the current cells of every
   // point row, dilated by `margin` cells.
@@ -490,9 +550,15 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
   const int Fr = hp.num_frames();
   const int np = hp.num_params();
   const int col_off = 0;
-  // 1. partition and permutation (local)
+  // 1. partition and permutation (local); the regions a few levels down the
+  // dissection are subtrees of the assembly tree, analysed in parallel
   std::vector<std::vector<int>> groups;
-  Dissect(hp, 0, hp.nx, 0, hp.ny, groups);
+  std::vector<std::pair<int, int>> subtrees;
+  int split = 0;
+  while (split < 4 && (1 << split) < threads) {
+    ++split;
+  }
+  Dissect(hp, 0, hp.nx, 0, hp.ny, groups, 0, threads > 1 ? split : -1, subtrees);
   std::vector<int> lperm;
   std::vector<int> sn_begin{0};
   for (const auto& g : groups) {
@@ -516,12 +582,13 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
   }
   // 2. pose coupling: frames coupled to each active node (ascending). The
   // points of each frame (in any order in the caller's specs) give the cells
-  // they occupy; that set dilated by `margin` cells is the frame's allowed
-  // set (one bitmap row per frame), and the corner nodes of the allowed
-  // cells are coupled to the frame. Frames are processed in parallel.
-  // node_frames as CSR over active columns: nf_ptr[c]..nf_ptr[c + 1] in nf
-  std::vector<int64_t> nf_ptr(static_cast<size_t>(A) + 1, 0);
-  std::vector<int32_t> nf;
+  // they occupy; that set dilated by `margin` cells (clipped to the grid) is
+  // the frame's allowed set (one bitmap row per frame), and the corner nodes
+  // of the allowed cells are coupled to the frame. Frames run in parallel on
+  // row-major 64-bit bitmaps of the cell grid.
+  // frame-major lists: the coupled columns of frame f, ascending, at
+  // fmp_ptr[f]..fmp_ptr[f + 1] of fmp_col
+  std::vector<std::vector<int32_t>> frame_cols(static_cast<size_t>(std::max(Fr, 1)));
   {
     const int cw = hp.nx - 1;
     const int chh = hp.ny - 1;
@@ -543,19 +610,26 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
         fpts[static_cast<size_t>(fill[static_cast<size_t>(hp.pt_frame[q])]++)] = static_cast<int>(q);
       }
     }
-    std::vector<std::vector<int32_t>> frame_cols(static_cast<size_t>(Fr));
     const double dxg = hp.dx();
     const double dyg = hp.dy();
+    // 64-bit words per bitmap row, wide enough for a row of nodes (cw + 1)
+    const int rw = (hp.nx + 63) / 64;
+    std::vector<uint64_t> row_mask(static_cast<size_t>(rw), 0);
+    for (int w = 0; w < cw; ++w) {
+      row_mask[static_cast<size_t>(w >> 6)] |= uint64_t{1} << (w & 63);
+    }
     auto frame_work = [&](int f0, int f1) {
-      std::vector<int> stamp(static_cast<size_t>(cw) * chh, -1);
-      std::vector<int> node_stamp(static_cast<size_t>(hp.nx) * hp.ny, -1);
-      std::vector<int> base;
-      std::vector<int> cells;
+      const size_t cells = static_cast<size_t>(rw) * static_cast<size_t>(std::max(chh, 0));
+      std::vector<uint64_t> occ(cells);
+      std::vector<uint64_t> horiz(cells);
+      std::vector<uint64_t> allowed(cells);
+      std::vector<uint64_t> tmp(static_cast<size_t>(rw));
+      std::vector<uint64_t> nodes(static_cast<size_t>(rw));
       for (int f = std::max(f0, 1); f < f1; ++f) {
         const double* pose = &hp.poses[3 * static_cast<size_t>(f)];
         const double c = std::cos(pose[2]);
         const double sn = std::sin(pose[2]);
-        base.clear();
+        std::fill(occ.begin(), occ.end(), uint64_t{0});
         for (int q = fptr[static_cast<size_t>(f)]; q < fptr[static_cast<size_t>(f) + 1]; ++q) {
           const size_t pt = static_cast<size_t>(fpts[static_cast<size_t>(q)]);
           const double px = hp.pt_xy[2 * pt];
@@ -569,95 +643,128 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
           }
           const int w = std::clamp(static_cast<int>(std::floor(fx)), 0, cw - 1);
           const int h = std::clamp(static_cast<int>(std::floor(fy)), 0, chh - 1);
-          const int cell = h * cw + w;
-          if (stamp[static_cast<size_t>(cell)] != 2 * f) {
-            stamp[static_cast<size_t>(cell)] = 2 * f;
-            base.push_back(cell);
+          occ[static_cast<size_t>(h) * rw + static_cast<size_t>(w >> 6)] |= uint64_t{1} << (w & 63);
+        }
+        // horizontal dilation: `margin` passes of a one-cell shift both ways;
+        // bits past the last cell only regenerate cells already reached
+        for (int h = 0; h < chh; ++h) {
+          uint64_t* row = &horiz[static_cast<size_t>(h) * rw];
+          std::copy(&occ[static_cast<size_t>(h) * rw], &occ[static_cast<size_t>(h) * rw] + rw, row);
+          for (int pass = 0; pass < margin; ++pass) {
+            for (int k = 0; k < rw; ++k) {
+              const uint64_t up = (row[k] << 1) | (k > 0 ? row[k - 1] >> 63 : 0);
+              const uint64_t down = (row[k] >> 1) | (k + 1 < rw ? row[k + 1] << 63 : 0);
+              tmp[static_cast<size_t>(k)] = row[k] | up | down;
+            }
+            std::copy(tmp.begin(), tmp.end(), row);
+          }
+          for (int k = 0; k < rw; ++k) {
+            row[k] &= row_mask[static_cast<size_t>(k)];
           }
         }
-        // dilation of the occupied cells
-        cells.clear();
+        // vertical dilation, clipped to the grid
         uint32_t* allow = S.allow_bits.data() + static_cast<size_t>(f) * words;
-        for (const int cell : base) {
-          const int w = cell % cw;
-          const int h = cell / cw;
+        for (int h = 0; h < chh; ++h) {
+          uint64_t* row = &allowed[static_cast<size_t>(h) * rw];
+          std::fill(row, row + rw, uint64_t{0});
           for (int hh = std::max(0, h - margin); hh <= std::min(chh - 1, h + margin); ++hh) {
-            for (int ww = std::max(0, w - margin); ww <= std::min(cw - 1, w + margin); ++ww) {
-              const int d = hh * cw + ww;
-              const uint32_t bit = 1u << (d & 31);
-              if ((allow[d >> 5] & bit) == 0u) {
-                allow[d >> 5] |= bit;
-                cells.push_back(d);
-              }
+            const uint64_t* src = &horiz[static_cast<size_t>(hh) * rw];
+            for (int k = 0; k < rw; ++k) {
+              row[k] |= src[k];
+            }
+          }
+          for (int k = 0; k < rw; ++k) {
+            for (uint64_t bits = row[k]; bits != 0; bits &= bits - 1) {
+              const int d = h * cw + k * 64 + __builtin_ctzll(bits);
+              allow[d >> 5] |= 1u << (d & 31);
             }
           }
         }
-        // active corner nodes of the allowed cells
+        // active corner nodes of the allowed cells, in node order (active
+        // columns ascend with the node)
         std::vector<int32_t>& cols = frame_cols[static_cast<size_t>(f)];
-        for (const int cell : cells) {
-          const int ww = cell % cw;
-          const int hh = cell / cw;
-          for (int q = 0; q < 4; ++q) {
-            const int node = (hh + (q >> 1)) * hp.nx + ww + (q & 1);
-            const int col = hp.node_to_active[static_cast<size_t>(node)];
-            if (col >= 0 && node_stamp[static_cast<size_t>(node)] != f) {
-              node_stamp[static_cast<size_t>(node)] = f;
-              cols.push_back(col);
+        cols.clear();
+        for (int y = 0; y < hp.ny; ++y) {
+          std::fill(nodes.begin(), nodes.end(), uint64_t{0});
+          for (const int h : {y - 1, y}) {
+            if (h < 0 || h >= chh) {
+              continue;
+            }
+            const uint64_t* a = &allowed[static_cast<size_t>(h) * rw];
+            for (int k = 0; k < rw; ++k) {
+              nodes[static_cast<size_t>(k)] |= a[k] | (a[k] << 1) | (k > 0 ? a[k - 1] >> 63 : 0);
+            }
+          }
+          for (int k = 0; k < rw; ++k) {
+            for (uint64_t bits = nodes[static_cast<size_t>(k)]; bits != 0; bits &= bits - 1) {
+              const int x = k * 64 + __builtin_ctzll(bits);
+              const int col = hp.node_to_active[static_cast<size_t>(y) * hp.nx + x];
+              if (col >= 0) {
+                cols.push_back(col);
+              }
             }
           }
         }
       }
     };
-    const int workers =
-        std::clamp(threads, 1, std::max(1, (Fr + 7) / 8));
-    if (workers <= 1) {
-      frame_work(0, Fr);
-    } else {
-      std::vector<std::thread> pool;
-      const int per = (Fr + workers - 1) / workers;
-      for (int w = 1; w < workers; ++w) {
-        const int f0 = w * per;
-        const int f1 = std::min(Fr, f0 + per);
-        if (f0 < f1) {
-          pool.emplace_back(frame_work, f0, f1);
-        }
-      }
-      frame_work(0, std::min(Fr, per));
-      for (std::thread& t : pool) {
-        t.join();
-      }
-    }
-    // CSR by column; frames enter in ascending order. Each thread owns a
-    // range of columns and scans every frame's list.
-    int64_t entries = 0;
-    for (int f = 1; f < Fr; ++f) {
-      entries += static_cast<int64_t>(frame_cols[static_cast<size_t>(f)].size());
-    }
-    const int csr_threads = entries > (int64_t{1} << 15) ? threads : 1;
-    ParallelRanges(csr_threads, A, 1024, [&](int64_t c0, int64_t c1) {
-      for (int f = 1; f < Fr; ++f) {
-        for (const int32_t col : frame_cols[static_cast<size_t>(f)]) {
-          if (col >= c0 && col < c1) {
-            ++nf_ptr[static_cast<size_t>(col) + 1];
-          }
-        }
-      }
-    });
-    for (int c = 0; c < A; ++c) {
-      nf_ptr[static_cast<size_t>(c) + 1] += nf_ptr[static_cast<size_t>(c)];
-    }
-    nf.resize(static_cast<size_t>(nf_ptr[static_cast<size_t>(A)]));
-    std::vector<int64_t> fill(nf_ptr.begin(), nf_ptr.end() - 1);
-    ParallelRanges(csr_threads, A, 1024, [&](int64_t c0, int64_t c1) {
-      for (int f = 1; f < Fr; ++f) {
-        for (const int32_t col : frame_cols[static_cast<size_t>(f)]) {
-          if (col >= c0 && col < c1) {
-            nf[static_cast<size_t>(fill[static_cast<size_t>(col)]++)] = f;
-          }
-        }
-      }
+    ParallelRanges(threads, Fr, 4, [&](int64_t f0, int64_t f1) {
+      frame_work(static_cast<int>(f0), static_cast<int>(f1));
     });
   }
+  // frame-major index of the coupling entries
+  S.fmp_ptr.assign(static_cast<size_t>(Fr) + 1, 0);
+  for (int f = 0; f < Fr; ++f) {
+    S.fmp_ptr[static_cast<size_t>(f) + 1] =
+        S.fmp_ptr[static_cast<size_t>(f)] + static_cast<int64_t>(frame_cols[static_cast<size_t>(f)].size());
+  }
+  const int64_t entries = Fr > 0 ? S.fmp_ptr[static_cast<size_t>(Fr)] : 0;
+  // node-major CSR (nf_ptr, nf): the frames of each active column, ascending.
+  // The frame lists ascend, so a thread owning a range of columns finds its
+  // part of every list by binary search.
+  std::vector<int64_t> nf_ptr(static_cast<size_t>(A) + 1, 0);
+  std::vector<int32_t> nf(static_cast<size_t>(entries));
+  S.fmp_col.resize(static_cast<size_t>(entries));
+  const int csr_threads = entries > (int64_t{1} << 14) ? threads : 1;
+  auto frame_part = [&](int f, int64_t c0, int64_t c1) {
+    const std::vector<int32_t>& cols = frame_cols[static_cast<size_t>(f)];
+    const auto lo = std::lower_bound(cols.begin(), cols.end(), static_cast<int32_t>(c0));
+    const auto hi = std::lower_bound(lo, cols.end(), static_cast<int32_t>(c1));
+    return std::make_pair(lo, hi);
+  };
+  ParallelRanges(csr_threads, A, 256, [&](int64_t c0, int64_t c1) {
+    for (int f = 1; f < Fr; ++f) {
+      const auto [lo, hi] = frame_part(f, c0, c1);
+      for (auto it = lo; it != hi; ++it) {
+        ++nf_ptr[static_cast<size_t>(*it) + 1];
+      }
+    }
+  });
+  for (int c = 0; c < A; ++c) {
+    nf_ptr[static_cast<size_t>(c) + 1] += nf_ptr[static_cast<size_t>(c)];
+  }
+  // rank[e]: position of node-major entry e within its frame's list
+  std::vector<int32_t> rank(static_cast<size_t>(entries));
+  ParallelRanges(csr_threads, A, 256, [&](int64_t c0, int64_t c1) {
+    std::vector<int64_t> fill(nf_ptr.begin() + c0, nf_ptr.begin() + c1);
+    for (int f = 1; f < Fr; ++f) {
+      const auto [lo, hi] = frame_part(f, c0, c1);
+      const auto begin = frame_cols[static_cast<size_t>(f)].begin();
+      for (auto it = lo; it != hi; ++it) {
+        const int64_t e = fill[static_cast<size_t>(*it - c0)]++;
+        nf[static_cast<size_t>(e)] = f;
+        rank[static_cast<size_t>(e)] = static_cast<int32_t>(it - begin);
+      }
+    }
+  });
+  ParallelRanges(csr_threads, Fr, 4, [&](int64_t f0, int64_t f1) {
+    for (int64_t f = f0; f < f1; ++f) {
+      const std::vector<int32_t>& cols = frame_cols[static_cast<size_t>(f)];
+      int32_t* out = S.fmp_col.data() + S.fmp_ptr[static_cast<size_t>(f)];
+      for (size_t k = 0; k < cols.size(); ++k) {
+        out[k] = col_off + cols[k];
+      }
+    }
+  });
   // pose pairs linked by odometry / relation rows
   std::vector<std::vector<int>> frame_links(static_cast<size_t>(Fr));
   for (int o = 0; o < hp.num_odom(); ++o) {
@@ -705,60 +812,79 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
       }
     }
   };
-  const LocalSym L = SupernodalSymbolic(np, lower, sn_begin);
+  const LocalSym L = SupernodalSymbolic(np, lower, sn_begin, subtrees);
   AppendInstance(S, L, col_off, 0, height);
   // 4. assembly offsets for this instance: 9 stencil slots per node column
-  // and one (node, frame) entry per coupled frame, found by walking the
-  // front's sorted rows (the frames' pose rows ascend with the frame)
+  // and one (node, frame) entry per coupled frame (stored node-major in
+  // mp_off and frame-major in fmp_off), looked up in a map from the front's
+  // rows to their positions. Supernodes are independent: each
+  // writes the slots and entries of its own columns.
   for (int c = 0; c < n; ++c) {
     S.mp_ptr[static_cast<size_t>(c) + 1] = nf_ptr[static_cast<size_t>(std::min(c + 1, A))];
   }
-  S.mp_frame.assign(nf.begin(), nf.end());
-  S.mp_off.resize(S.mp_frame.size());
-  // columns are independent: each writes its own stencil slots and entries
-  ParallelRanges(threads, A, 512, [&](int64_t cb, int64_t ce) {
-  for (int c = static_cast<int>(cb); c < static_cast<int>(ce); ++c) {
-    const int pc = lpinv[static_cast<size_t>(c)];
-    const int s = S.col_owner[static_cast<size_t>(col_off + pc)];
-    const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
-    const int32_t* rows = S.sn_rows.data() + r.rows_off;
-    const int node = hp.active_to_node[static_cast<size_t>(c)];
-    const int w = node % hp.nx;
-    const int h = node / hp.nx;
-    const int64_t col_base = r.front_off + static_cast<int64_t>(col_off + pc - r.first_col) * r.F;
-    for (int dh = -1; dh <= 1; ++dh) {
-      for (int dw = -1; dw <= 1; ++dw) {
-        const int slot = (dh + 1) * 3 + (dw + 1);
-        const int ww = w + dw;
-        const int hh = h + dh;
-        if (ww < 0 || hh < 0 || ww >= hp.nx || hh >= hp.ny) {
-          continue;
+  S.mp_off.resize(static_cast<size_t>(entries));
+  S.fmp_off.resize(static_cast<size_t>(entries));
+  const int Sn = static_cast<int>(S.sn.size());
+  const int offset_parts = std::min(Sn, 4 * threads);
+  PoolRun(threads > 1 ? offset_parts : std::min(Sn, 1), [&](int part) {
+    const int parts = threads > 1 ? offset_parts : 1;
+    ColumnMap& pos = ThreadColumnMap();
+    for (int s = part; s < Sn; s += parts) {
+      const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
+      if (r.first_col >= col_off + A) {
+        continue;  // the pose root holds no node columns
+      }
+      const int32_t* rows = S.sn_rows.data() + r.rows_off;
+      pos.Begin(static_cast<size_t>(col_off + n));
+      for (int j = 0; j < r.ncols; ++j) {
+        pos.Set(r.first_col + j, j);
+      }
+      for (int q = 0; q < r.nrows; ++q) {
+        pos.Set(rows[q], r.ncols + q);
+      }
+      for (int pc = r.first_col - col_off; pc < r.first_col - col_off + r.ncols; ++pc) {
+        const int c = lperm[static_cast<size_t>(pc)];
+        const int node = hp.active_to_node[static_cast<size_t>(c)];
+        const int w = node % hp.nx;
+        const int h = node / hp.nx;
+        const int64_t col_base = r.front_off + static_cast<int64_t>(col_off + pc - r.first_col) * r.F;
+        for (int dh = -1; dh <= 1; ++dh) {
+          for (int dw = -1; dw <= 1; ++dw) {
+            const int slot = (dh + 1) * 3 + (dw + 1);
+            const int ww = w + dw;
+            const int hh = h + dh;
+            if (ww < 0 || hh < 0 || ww >= hp.nx || hh >= hp.ny) {
+              continue;
+            }
+            const int c2 = hp.node_to_active[static_cast<size_t>(hh) * hp.nx + ww];
+            if (c2 < 0) {
+              continue;
+            }
+            const int pc2 = lpinv[static_cast<size_t>(c2)];
+            if (pc2 < pc) {
+              continue;  // stored in the neighbour's column
+            }
+            if (!pos.Has(col_off + pc2)) {
+              Fail(SDFGPU_ERR_CUDA, "stencil row missing from a node's front");
+            }
+            S.mm_off[static_cast<size_t>(col_off + c) * 9 + static_cast<size_t>(slot)] = col_base + pos.Get(col_off + pc2);
+          }
         }
-        const int c2 = hp.node_to_active[static_cast<size_t>(hh) * hp.nx + ww];
-        if (c2 < 0) {
-          continue;
+        // pose rows lie below the pivot block of a grid supernode
+        for (int64_t e = nf_ptr[static_cast<size_t>(c)]; e < nf_ptr[static_cast<size_t>(c) + 1]; ++e) {
+          const int32_t target = col_off + A + 3 * (nf[static_cast<size_t>(e)] - 1);
+          if (!pos.Has(target)) {
+            Fail(SDFGPU_ERR_CUDA, "pose row missing from a node's front");
+          }
+          const int64_t off = col_base + pos.Get(target);
+          S.mp_off[static_cast<size_t>(e)] = off;
+          S.fmp_off[static_cast<size_t>(S.fmp_ptr[static_cast<size_t>(nf[static_cast<size_t>(e)])] +
+                                        rank[static_cast<size_t>(e)])] = off;
         }
-        const int pc2 = lpinv[static_cast<size_t>(c2)];
-        if (pc2 < pc) {
-          continue;  // stored in the neighbour's column
-        }
-        S.mm_off[static_cast<size_t>(col_off + c) * 9 + static_cast<size_t>(slot)] =
-            col_base + LocalIndex(r, rows, col_off + pc2);
       }
     }
-    // pose rows lie below the pivot block of a grid supernode; the frames
-    // ascend, so each search starts where the previous one ended
-    const int32_t* q = rows;
-    for (int64_t e = nf_ptr[static_cast<size_t>(c)]; e < nf_ptr[static_cast<size_t>(c) + 1]; ++e) {
-      const int32_t target = col_off + A + 3 * (nf[static_cast<size_t>(e)] - 1);
-      q = std::lower_bound(q, rows + r.nrows, target);
-      if (q == rows + r.nrows || *q != target) {
-        Fail(SDFGPU_ERR_CUDA, "pose row missing from a node's front");
-      }
-      S.mp_off[static_cast<size_t>(e)] = col_base + r.ncols + (q - rows);
-    }
-  }
   });
+  S.mp_frame = std::move(nf);
   // pose root
   if (Fr > 1) {
     const int s = S.col_owner[static_cast<size_t>(col_off + A)];
@@ -767,33 +893,6 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
     S.pp_base[0] = r.front_off;
     S.pp_ld[0] = r.F;
     S.pp_first[0] = col_off + A - r.first_col;
-  }
-  // map-pose entries grouped by frame (for the FP64 normal-matrix product)
-  S.fmp_ptr.assign(static_cast<size_t>(Fr) + 1, 0);
-  for (int64_t e = 0; e < static_cast<int64_t>(S.mp_frame.size()); ++e) {
-    ++S.fmp_ptr[static_cast<size_t>(S.mp_frame[static_cast<size_t>(e)]) + 1];
-  }
-  for (int f = 0; f < Fr; ++f) {
-    S.fmp_ptr[static_cast<size_t>(f) + 1] += S.fmp_ptr[static_cast<size_t>(f)];
-  }
-  S.fmp_col.resize(S.mp_frame.size());
-  S.fmp_off.resize(S.mp_frame.size());
-  {
-    // each thread owns a range of frames and scans every column in order
-    std::vector<int64_t> fill(S.fmp_ptr.begin(), S.fmp_ptr.end() - 1);
-    const int tr_threads = S.mp_frame.size() > (size_t{1} << 15) ? threads : 1;
-    ParallelRanges(tr_threads, Fr, 8, [&](int64_t f0, int64_t f1) {
-      for (int c = 0; c < A; ++c) {
-        for (int64_t e = S.mp_ptr[static_cast<size_t>(c)]; e < S.mp_ptr[static_cast<size_t>(c) + 1]; ++e) {
-          const int f = S.mp_frame[static_cast<size_t>(e)];
-          if (f >= f0 && f < f1) {
-            const int64_t q = fill[static_cast<size_t>(f)]++;
-            S.fmp_col[static_cast<size_t>(q)] = c;
-            S.fmp_off[static_cast<size_t>(q)] = S.mp_off[static_cast<size_t>(e)];
-          }
-        }
-      }
-    });
   }
   ComputeRel(S);
   return piece;
@@ -916,6 +1015,21 @@ Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<Inst
   return S;
 }
 
+Symbolic ConcatenateOne(SymPiece&& piece, int panel_width, int tile, const Schedule& sched) {
+  // a lone piece is already numbered from column, frame and front 0
+  Symbolic S = std::move(piece.s);
+  const std::vector<int> height = std::move(piece.height);
+  piece = SymPiece{};
+  S.small_pivots = sched.small_pivots;
+  S.front_rows = sched.front_rows;
+  S.panel_rows = sched.panel_rows;
+  for (SupernodeRec& r : S.sn) {
+    r.instance = 0;
+  }
+  Finalize(S, height, panel_width, tile);
+  return S;
+}
+
 void Reschedule(Symbolic& S, const Schedule& sched) {
   S.small_pivots = sched.small_pivots;
   S.front_rows = sched.front_rows;
@@ -952,49 +1066,20 @@ void AnalyzeInstances(const std::vector<HostProblem>& problems, const std::vecto
     todo.resize(problems.size());
     std::iota(todo.begin(), todo.end(), 0);
   }
-  const int workers = std::min<int>(static_cast<int>(todo.size()),
-                                    std::max(1, static_cast<int>(std::thread::hardware_concurrency())));
-  if (workers <= 1) {
+  // Many instances: one instance per part, each analysed on one thread.
+  // Few: one after another, each on all threads.
+  if (static_cast<int>(todo.size()) < PoolThreads()) {
     for (const int i : todo) {
       pieces[static_cast<size_t>(i)] =
           AnalyzeInstance(problems[static_cast<size_t>(i)], margin[static_cast<size_t>(i)], 0);
     }
     return;
   }
-  // instances in parallel, each analysis on the threads left over
-  const int inner = std::max(1, static_cast<int>(std::thread::hardware_concurrency()) / workers);
-  std::atomic<size_t> next{0};
-  std::exception_ptr error;
-  std::mutex error_mu;
-  auto work = [&]() {
-    for (;;) {
-      const size_t q = next.fetch_add(1);
-      if (q >= todo.size()) {
-        return;
-      }
-      const int i = todo[q];
-      try {
-        pieces[static_cast<size_t>(i)] =
-            AnalyzeInstance(problems[static_cast<size_t>(i)], margin[static_cast<size_t>(i)], inner);
-      } catch (...) {
-        const std::lock_guard<std::mutex> lock(error_mu);
-        if (!error) {
-          error = std::current_exception();
-        }
-      }
-    }
-  };
-  std::vector<std::thread> pool;
-  for (int w = 1; w < workers; ++w) {
-    pool.emplace_back(work);
-  }
-  work();
-  for (std::thread& t : pool) {
-    t.join();
-  }
-  if (error) {
-    std::rethrow_exception(error);
-  }
+  PoolRun(static_cast<int>(todo.size()), [&](int q) {
+    const int i = todo[static_cast<size_t>(q)];
+    pieces[static_cast<size_t>(i)] =
+        AnalyzeInstance(problems[static_cast<size_t>(i)], margin[static_cast<size_t>(i)], 1);
+  });
 }
 
 Symbolic AnalyzeGeneral(int n, const int32_t* outer, const int32_t* inner, const std::vector<int32_t>& perm_in,
