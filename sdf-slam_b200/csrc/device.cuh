@@ -42,6 +42,9 @@ constexpr int kStatusPatternOverflow = 2;
 // set by the cost kernel: at the state it evaluated, a point lies outside its
 // pose's analysed cell set (the next linearization would overflow)
 constexpr int kStatusNextOverflow = 4;
+/// A wait on another block's flag ran out of its limit (the results of the
+/// launch are not valid).
+constexpr int kStatusWaitTimeout = 8;
 
 /// Per point row record: 4 node Jacobian entries, 3 pose entries, residual.
 constexpr int kPointRec = 8;

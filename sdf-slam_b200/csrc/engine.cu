@@ -419,6 +419,9 @@ void Engine::UploadSymbolic() {
     max_front_ = std::max(max_front_, r.F);
   }
   ConfigureSolveKernels(max_front_);
+  solve_sync_.Alloc(SolveSyncWords(static_cast<int>(sym_.sn.size())));
+  inv_tasks_.Upload(sym_.inv_tasks, s);
+  inv_.Alloc(std::max<size_t>(1, sym_.inv_tasks.size() / 2) * kInvBlockDoubles);
   std::vector<InstDev> inst(host_.size());
   for (size_t i = 0; i < host_.size(); ++i) {
     const InstanceLayout& L = layout_[i];
@@ -605,11 +608,26 @@ void Engine::ClearStatus() {
   CudaCheck(cudaMemsetAsync(status_.get(), 0, sizeof(int32_t) * host_.size(), stream_), "status");
 }
 
+namespace {
+
+/// A wait of the one-launch solve that ran out of its limit leaves no valid
+/// result behind: the call fails.
+void CheckWaits(const int32_t* st, size_t count) {
+  for (size_t i = 0; i < count; ++i) {
+    if ((st[i] & kStatusWaitTimeout) != 0) {
+      Fail(SDFGPU_ERR_CUDA, "a wait of the solve kernel ran out of its limit");
+    }
+  }
+}
+
+}  // namespace
+
 std::vector<int32_t> Engine::DownloadStatus() {
   std::vector<int32_t> st(host_.size());
   CudaCheck(cudaMemcpyAsync(st.data(), status_.get(), st.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_),
             "status");
   CudaCheck(cudaStreamSynchronize(stream_), "status sync");
+  CheckWaits(st.data(), st.size());
   return st;
 }
 
@@ -681,6 +699,10 @@ FactorPlan Engine::Plan() {
   P.level_sn = level_sn_.get();
   P.dvec = dvec_.get();
   P.max_front = max_front_;
+  P.solve_sync = solve_sync_.get();
+  P.inv_tasks = inv_tasks_.get();
+  P.num_inv = static_cast<int>(sym_.inv_tasks.size() / 2);
+  P.inv = inv_.get();
   return P;
 }
 
@@ -1312,6 +1334,7 @@ bool Engine::IterationReady() const {
 void Engine::FinishIteration() {
   const size_t I = host_.size();
   CudaCheck(cudaStreamSynchronize(stream_), "iteration");
+  CheckWaits(h_status_.get(), I);
   std::vector<int> overflow;
   for (size_t i = 0; i < I; ++i) {
     if (lm_[i].active != 0 && (h_status_[i] & kStatusPatternOverflow) != 0) {
@@ -1333,6 +1356,7 @@ void Engine::FinishIteration() {
     }
     EnqueueIteration();
     CudaCheck(cudaStreamSynchronize(stream_), "iteration");
+    CheckWaits(h_status_.get(), I);
     std::vector<char> rerun(I, 0);
     for (const int i : overflow) {
       rerun[static_cast<size_t>(i)] = 1;

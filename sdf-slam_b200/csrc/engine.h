@@ -89,7 +89,22 @@ struct FactorPlan {
   const int32_t* level_sn{nullptr};
   double* dvec{nullptr};
   int max_front{1};
+  /// Counter and flags of the one-launch solve (SolveSyncWords words); the
+  /// solve runs level by level when this or inv is null.
+  uint32_t* solve_sync{nullptr};
+  /// (sn, panel) pairs of the diagonal blocks and their inverses
+  /// (kInvBlockDoubles each), written after every factorization.
+  const int32_t* inv_tasks{nullptr};
+  int num_inv{0};
+  double* inv{nullptr};
 };
+
+/// Doubles per inverted 32 x 32 diagonal block (the inverse and its
+/// transpose).
+constexpr int kInvBlockDoubles = 2 * 32 * 32;
+
+/// Words of the one-launch solve's counter and flags for num_sn supernodes.
+inline size_t SolveSyncWords(int num_sn) { return 2 + 2 * static_cast<size_t>(num_sn); }
 
 /// Level-scheduled multifrontal LDL^T of the assembled fronts.
 /// Returns the number of kernels launched.
@@ -290,6 +305,9 @@ class Engine {
   DevBuf<uint32_t> allow_bits_;
   DevBuf<int32_t> ea_tasks_, ea_child_, panel_tasks_, update_tasks_, small_tasks_;
   DevBuf<double> fronts_, upd_;
+  DevBuf<uint32_t> solve_sync_;  // counter and flags of the one-launch solve
+  DevBuf<int32_t> inv_tasks_;     // diagonal blocks of L and their inverses
+  DevBuf<double> inv_;
   // mixed precision: assembled FP64 normal matrix, FP32 work fronts, the
   // conversion tasks and the refinement vectors
   static constexpr int kConvertChunk = 16384;

@@ -586,7 +586,8 @@ __device__ __forceinline__ void ForwardBody(const DeviceView& V, const Supernode
     const int32_t* rel = V.sn_rel + C.rows_off;
     const double* u = V.upd + C.upd_off;
     for (int r = threadIdx.x; r < C.nrows; r += blockDim.x) {
-      v[rel[r]] += u[r];
+      // L2 loads: another block of the same launch may have written them
+      v[rel[r]] += __ldcg(u + r);
     }
     __syncthreads();
   }
@@ -670,8 +671,9 @@ __device__ __forceinline__ void BackwardBody(const DeviceView& V, const Supernod
   // memory behind the k pivot slots (the gather's latency is paid once, not
   // once per column)
   double* xr = z + k;
+  // (L2 loads: another block of the same launch may have written them)
   for (int r = threadIdx.x; r < m; r += blockDim.x) {
-    xr[r] = V.xs[rows[r]];
+    xr[r] = __ldcg(V.xs + rows[r]);
   }
   __syncthreads();
   for (int j = warp; j < k; j += nwarps) {
@@ -685,7 +687,7 @@ __device__ __forceinline__ void BackwardBody(const DeviceView& V, const Supernod
       acc += __shfl_down_sync(0xffffffffu, acc, off);
     }
     if (lane == 0) {
-      z[j] = V.xs[S.first_col + j] - acc;
+      z[j] = __ldcg(V.xs + S.first_col + j) - acc;
     }
   }
   __syncthreads();
@@ -759,6 +761,478 @@ __global__ void __launch_bounds__(256) KBackward(DeviceView V, const int32_t* le
   }
 }
 
+/// Doubles per inverted diagonal block: M = L^-1 of the block's unit lower
+/// triangle, column major, then M^T, column major.
+constexpr int kInvBlock = 2 * kPanel * kPanel;
+
+/// Inverts the unit lower triangle of every kPanel-column diagonal block of
+/// L (one warp per block, four per thread block): lane c solves L m = e_c
+/// by forward substitution in registers, reading L from shared memory as
+/// broadcasts. Columns of a narrow last panel beyond the pivots invert to
+/// the identity. tasks: (sn, panel) pairs in panel_base order.
+__global__ void __launch_bounds__(128) KInvertDiagonal(DeviceView V, const int32_t* tasks, int count, double* inv) {
+  __shared__ double Ls[4][kPanel][kPanel + 1];
+  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int b = blockIdx.x * 4 + wib;
+  if (b >= count) {
+    return;
+  }
+  const SupernodeRec S = V.sn[tasks[2 * b]];
+  if (V.active[S.instance] == 0) {
+    return;
+  }
+  const int p0 = tasks[2 * b + 1] * kPanel;
+  const int w = min(kPanel, S.ncols - p0);
+  const int64_t F = S.F;
+  double(*L)[kPanel + 1] = Ls[wib];
+  // L(p0 + i, p0 + j), i > j, lives transposed in the block's upper
+  // triangle: row i of L is contiguous
+  if (Fp32Front(V, S)) {
+    const float* Fs = V.fronts32 + S.front_off;
+    for (int i = 0; i < kPanel; ++i) {
+      L[i][lane] = (i < w && lane < i) ? static_cast<double>(Fs[(p0 + i) * F + p0 + lane]) : 0.0;
+    }
+  } else {
+    const double* Fs = V.fronts + S.front_off;
+    for (int i = 0; i < kPanel; ++i) {
+      L[i][lane] = (i < w && lane < i) ? Fs[(p0 + i) * F + p0 + lane] : 0.0;
+    }
+  }
+  __syncwarp();
+  double m[kPanel];
+#pragma unroll
+  for (int i = 0; i < kPanel; ++i) {
+    double acc = i == lane ? 1.0 : 0.0;
+#pragma unroll
+    for (int j = 0; j < i; ++j) {
+      acc = fma(-L[i][j], m[j], acc);
+    }
+    m[i] = acc;
+  }
+  double* out = inv + static_cast<int64_t>(S.panel_base + p0 / kPanel) * kInvBlock;
+  // M^T column major: (i, j) of M^T = M(j, i) = m[j] of lane i
+#pragma unroll
+  for (int j = 0; j < kPanel; ++j) {
+    out[kPanel * kPanel + j * kPanel + lane] = m[j];
+  }
+  // M column major through shared memory: lane c holds column c
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < kPanel; ++i) {
+    L[i][lane] = m[i];
+  }
+  __syncwarp();
+  for (int j = 0; j < kPanel; ++j) {
+    out[j * kPanel + lane] = L[lane][j];
+  }
+}
+
+/// Issues an asynchronous copy of one kPanel x kPanel block of doubles
+/// (16-byte chunks, L2 only) into shared memory and commits it as a group.
+__device__ __forceinline__ void CopyBlockAsync(double* dst, const double* src) {
+  for (int c = threadIdx.x; c < kPanel * kPanel / 2; c += blockDim.x) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst + 2 * c));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src + 2 * c) : "memory");
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+/// Waits for this thread's asynchronous copies.
+__device__ __forceinline__ void WaitBlockCopies() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+/// Global loads a thread of the solve issues before using the first one.
+constexpr int kBatch = 16;
+
+/// Rows (or columns) of a panel update that lane pairs of the 224 threads
+/// past warp 0 take with early loads.
+constexpr int kPairRows = 112;
+
+/// Doubles of shared memory the one-launch solve needs for fronts of at
+/// most max_front rows: two inverted blocks, then the front's vector.
+__host__ __device__ constexpr size_t SolveTreeSmem(int max_front) {
+  return (2 * static_cast<size_t>(kPanel) * kPanel + static_cast<size_t>(max_front)) * sizeof(double);
+}
+
+/// L(r, c) of a front for a pivot-block row r below column c's panel:
+/// transposed storage (row r contiguous) in single-kernel fronts, column
+/// major otherwise.
+template <typename T>
+__device__ __forceinline__ T PivotL(const T* Fs, int64_t F, bool upper, int r, int c) {
+  return upper ? Fs[r * F + c] : Fs[c * F + r];
+}
+
+/// Forward solve of one front for the one-launch solve. Gathers the
+/// right-hand side and the children's update vectors, then per panel: warp 0
+/// forms y_p = M_p v_p (M_p the inverted diagonal block, copied into shared
+/// memory during the previous panel) while the threads that update the
+/// later pivot rows load their L values; after a barrier those rows
+/// subtract L(r, p) y_p. The m rows below the pivot block get
+/// u = v_m - L21 y in one pass at the end; D^-1 y goes to xs. Every sum
+/// runs in a fixed order. buf: two blocks for M, then F doubles for v.
+template <typename T>
+__device__ __forceinline__ void ForwardTreeBody(const DeviceView& V, const SupernodeRec& S, const double* dvec,
+                                                const double* inv, double* buf) {
+  const int k = S.ncols;
+  const int F = S.F;
+  const int64_t F64 = F;
+  const T* Fs = WorkFront<T>(V, S);
+  const bool upper = S.upper_l11 != 0;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int nthreads = blockDim.x;
+  double* Ms = buf;
+  double* v = buf + 2 * kPanel * kPanel;
+  const double* Mb = inv + static_cast<int64_t>(S.panel_base) * kInvBlock;
+  CopyBlockAsync(Ms, Mb);
+  for (int j = tid; j < F; j += nthreads) {
+    v[j] = j < k ? V.rhs[V.perm[S.first_col + j]] : 0.0;
+  }
+  __syncthreads();
+  for (int ci = 0; ci < S.child_count; ++ci) {
+    const SupernodeRec C = V.sn[V.child_list[S.child_begin + ci]];
+    const int32_t* rel = V.sn_rel + C.rows_off;
+    const double* u = V.upd + C.upd_off;
+    for (int r = tid; r < C.nrows; r += nthreads) {
+      v[rel[r]] += __ldcg(u + r);
+    }
+    __syncthreads();
+  }
+  WaitBlockCopies();
+  __syncthreads();
+  for (int p0 = 0, q = 0; p0 < k; p0 += kPanel, ++q) {
+    if (p0 + kPanel < k) {
+      CopyBlockAsync(Ms + ((q + 1) & 1) * kPanel * kPanel, Mb + static_cast<int64_t>(q + 1) * kInvBlock);
+    }
+    // later pivot rows: lane pairs of warps 1.. own one row each (16 of its
+    // L values per lane, loaded before the barrier); rows past the first
+    // kPairRows loop below without the early loads
+    const int r = p0 + kPanel + ((tid - 32) >> 1);
+    const int half = (tid & 1) * (kPanel / 2);
+    T lr[kPanel / 2];
+    if (warp > 0 && r < k) {
+      const T* src = upper ? Fs + r * F64 + p0 + half : Fs + (p0 + half) * F64 + r;
+      const int64_t step = upper ? 1 : F64;
+#pragma unroll
+      for (int j = 0; j < kPanel / 2; ++j) {
+        lr[j] = *src;
+        src += step;
+      }
+    }
+    if (warp == 0) {
+      const double* M = Ms + (q & 1) * kPanel * kPanel;
+      double a0 = 0.0;
+      double a1 = 0.0;
+#pragma unroll
+      for (int j = 0; j < kPanel; j += 2) {
+        // past the pivots (a narrow last panel) M is the identity's zero part
+        const double v0 = p0 + j < k ? v[p0 + j] : 0.0;
+        const double v1 = p0 + j + 1 < k ? v[p0 + j + 1] : 0.0;
+        a0 = fma(M[j * kPanel + lane], v0, a0);
+        a1 = fma(M[(j + 1) * kPanel + lane], v1, a1);
+      }
+      __syncwarp();
+      if (p0 + lane < k) {
+        v[p0 + lane] = a0 + a1;
+      }
+    }
+    __syncthreads();
+    if (warp > 0) {
+      double part = 0.0;
+      if (r < k) {
+#pragma unroll
+        for (int j = 0; j < kPanel / 2; ++j) {
+          part = fma(static_cast<double>(lr[j]), v[p0 + half + j], part);
+        }
+      }
+      part += __shfl_xor_sync(0xffffffffu, part, 1);
+      if (half == 0 && r < k) {
+        v[r] -= part;
+      }
+      for (int r2 = p0 + kPanel + kPairRows + tid - 32; r2 < k; r2 += nthreads - 32) {
+        const T* src = upper ? Fs + r2 * F64 + p0 : Fs + p0 * F64 + r2;
+        const int64_t step = upper ? 1 : F64;
+        T l2[kPanel];
+#pragma unroll
+        for (int j = 0; j < kPanel; ++j) {
+          l2[j] = *src;
+          src += step;
+        }
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < kPanel; ++j) {
+          acc = fma(static_cast<double>(l2[j]), v[p0 + j], acc);
+        }
+        v[r2] -= acc;
+      }
+    }
+    WaitBlockCopies();
+    __syncthreads();
+  }
+  // u = v_m - L21 y: thread per row, L21 column major (coalesced over
+  // rows), 16 loads in flight per batch
+  for (int r = tid; r < F - k; r += nthreads) {
+    const T* col = Fs + k + r;
+    double a0 = v[k + r];
+    double a1 = 0.0;
+    for (int j0 = 0; j0 < k; j0 += kBatch) {
+      T lv[kBatch];
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        lv[j] = j0 + j < k ? col[(j0 + j) * F64] : T(0);
+      }
+#pragma unroll
+      for (int j = 0; j < kBatch; j += 2) {
+        a0 = fma(-static_cast<double>(lv[j]), j0 + j < k ? v[j0 + j] : 0.0, a0);
+        a1 = fma(-static_cast<double>(lv[j + 1]), j0 + j + 1 < k ? v[j0 + j + 1] : 0.0, a1);
+      }
+    }
+    V.upd[S.upd_off + r] = a0 + a1;
+  }
+  for (int j = tid; j < k; j += nthreads) {
+    V.xs[S.first_col + j] = (1.0 / dvec[S.first_col + j]) * v[j];
+  }
+}
+
+/// Backward solve of one front for the one-launch solve: z = x_k - L21^T x_R
+/// (warps over columns, four columns per pass, lanes over the m rows), then
+/// panels from the last: warp 0 forms x_p = M_p^T z_p, and after a barrier
+/// every earlier pivot column c subtracts L(p, c)^T x_p (its L values loaded
+/// before the barrier). Writes xs and the step in natural order. buf: two
+/// blocks for M^T, then F doubles (z, then the gathered x_R).
+template <typename T>
+__device__ __forceinline__ void BackwardTreeBody(const DeviceView& V, const SupernodeRec& S, const double* inv,
+                                                 double* buf) {
+  const int k = S.ncols;
+  const int m = S.nrows;
+  const int64_t F64 = S.F;
+  const T* Fs = WorkFront<T>(V, S);
+  const bool upper = S.upper_l11 != 0;
+  const int32_t* rows = V.sn_rows + S.rows_off;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const int nthreads = blockDim.x;
+  const int nwarps = nthreads >> 5;
+  double* Ms = buf;
+  double* z = buf + 2 * kPanel * kPanel;
+  double* xr = z + k;
+  const int last_q = (k - 1) / kPanel;
+  // M^T of panel q at Mb + q * kInvBlock
+  const double* Mb = inv + static_cast<int64_t>(S.panel_base) * kInvBlock + kPanel * kPanel;
+  CopyBlockAsync(Ms + (last_q & 1) * kPanel * kPanel, Mb + static_cast<int64_t>(last_q) * kInvBlock);
+  for (int r = tid; r < m; r += nthreads) {
+    xr[r] = __ldcg(V.xs + rows[r]);
+  }
+  __syncthreads();
+  for (int j0 = 4 * warp; j0 < k; j0 += 4 * nwarps) {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    // four rows per lane per batch: 16 loads in flight
+    for (int r0 = 0; r0 < m; r0 += 128) {
+      T lv[4][4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int r = r0 + 32 * u + lane;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          lv[u][q] = (r < m && j0 + q < k) ? Fs[(j0 + q) * F64 + k + r] : T(0);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int r = r0 + 32 * u + lane;
+        const double x = r < m ? xr[r] : 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          acc[q] = fma(static_cast<double>(lv[u][q]), x, acc[q]);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+      }
+    }
+    if (lane < 4 && j0 + lane < k) {
+      const double a = lane == 0 ? acc[0] : lane == 1 ? acc[1] : lane == 2 ? acc[2] : acc[3];
+      z[j0 + lane] = __ldcg(V.xs + S.first_col + j0 + lane) - a;
+    }
+  }
+  WaitBlockCopies();
+  __syncthreads();
+  for (int q = last_q; q >= 0; --q) {
+    const int p0 = q * kPanel;
+    if (q > 0) {
+      CopyBlockAsync(Ms + ((q - 1) & 1) * kPanel * kPanel, Mb + static_cast<int64_t>(q - 1) * kInvBlock);
+    }
+    // earlier pivot columns c < p0: lane pairs of warps 1.. own one column
+    // each (16 of its L values per lane, loaded before the barrier); columns
+    // past the first kPairRows loop below without the early loads
+    const int c = (tid - 32) >> 1;
+    const int half = (tid & 1) * (kPanel / 2);
+    T lc[kPanel / 2];
+    if (warp > 0 && c < p0) {
+      const T* src = upper ? Fs + (p0 + half) * F64 + c : Fs + c * F64 + p0 + half;
+      const int64_t step = upper ? F64 : 1;
+#pragma unroll
+      for (int i = 0; i < kPanel / 2; ++i) {
+        lc[i] = (p0 + half + i < k) ? *src : T(0);
+        src += step;
+      }
+    }
+    if (warp == 0) {
+      const double* M = Ms + (q & 1) * kPanel * kPanel;
+      double a0 = 0.0;
+      double a1 = 0.0;
+#pragma unroll
+      for (int j = 0; j < kPanel; j += 2) {
+        // past the pivots z holds x_R: weight zero there
+        const double z0 = p0 + j < k ? z[p0 + j] : 0.0;
+        const double z1 = p0 + j + 1 < k ? z[p0 + j + 1] : 0.0;
+        a0 = fma(M[j * kPanel + lane], z0, a0);
+        a1 = fma(M[(j + 1) * kPanel + lane], z1, a1);
+      }
+      __syncwarp();
+      if (p0 + lane < k) {
+        z[p0 + lane] = a0 + a1;
+      }
+    }
+    __syncthreads();
+    if (warp > 0) {
+      double part = 0.0;
+      if (c < p0) {
+#pragma unroll
+        for (int i = 0; i < kPanel / 2; ++i) {
+          part = fma(static_cast<double>(lc[i]), p0 + half + i < k ? z[p0 + half + i] : 0.0, part);
+        }
+      }
+      part += __shfl_xor_sync(0xffffffffu, part, 1);
+      if (half == 0 && c < p0) {
+        z[c] -= part;
+      }
+      for (int c2 = kPairRows + tid - 32; c2 < p0; c2 += nthreads - 32) {
+        const T* src = upper ? Fs + p0 * F64 + c2 : Fs + c2 * F64 + p0;
+        const int64_t step = upper ? F64 : 1;
+        T l2[kPanel];
+#pragma unroll
+        for (int i = 0; i < kPanel; ++i) {
+          l2[i] = (p0 + i < k) ? *src : T(0);
+          src += step;
+        }
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < kPanel; ++i) {
+          acc = fma(static_cast<double>(l2[i]), p0 + i < k ? z[p0 + i] : 0.0, acc);
+        }
+        z[c2] -= acc;
+      }
+    }
+    WaitBlockCopies();
+    __syncthreads();
+  }
+  for (int j = tid; j < k; j += nthreads) {
+    V.xs[S.first_col + j] = z[j];
+    V.step[V.perm[S.first_col + j]] = z[j];
+  }
+}
+
+/// Iterations of a bounded wait on another block's flag (about a second).
+constexpr uint32_t kWaitLimit = 1u << 21;
+
+/// Thread-level bounded wait until *flag != 0 (acquire at GPU scope); false
+/// when the limit ran out.
+__device__ __forceinline__ bool WaitFlag(const uint32_t* flag) {
+  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+    if (v != 0u) {
+      return true;
+    }
+    __nanosleep(100);
+  }
+  return false;
+}
+
+/// Publishes *flag = 1 (release at GPU scope).
+__device__ __forceinline__ void SetFlag(uint32_t* flag) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag), "r"(1u) : "memory");
+}
+
+/// Whole solve (forward sweep, diagonal, backward sweep) in one launch, with
+/// the inverted diagonal blocks of KInvertDiagonal.
+/// Blocks take tasks in order from a counter: tasks 0..S-1 are the forward
+/// solves of the supernodes in level order (leaves first), tasks S..2S-1
+/// the backward solves in the reverse order. A forward task waits for its
+/// children's forward flags, a backward task for its parent's backward flag
+/// (a root: its own forward flag). Every task waits only on tasks taken
+/// before it by running blocks, so the launch completes whatever the number
+/// of resident blocks; no level boundary holds fast fronts behind slow ones.
+/// sync: [0] task counter, [2, 2 + S) forward flags, [2 + S, 2 + 2S)
+/// backward flags, all zero at launch. A wait that runs out of its limit
+/// marks the instance kStatusWaitTimeout and lets the task's dependents go.
+__global__ void __launch_bounds__(256, 1) KSolveTree(DeviceView V, const int32_t* level_sn, int num_sn,
+                                                     const double* dvec, const double* inv, uint32_t* sync) {
+  extern __shared__ double buf[];
+  __shared__ int task;
+  __shared__ int go;
+  uint32_t* fdone = sync + 2;
+  uint32_t* bdone = sync + 2 + num_sn;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      task = static_cast<int>(atomicAdd(sync, 1u));
+    }
+    __syncthreads();
+    const int t = task;
+    if (t >= 2 * num_sn) {
+      return;
+    }
+    const bool forward = t < num_sn;
+    const int s = level_sn[forward ? t : 2 * num_sn - 1 - t];
+    const SupernodeRec S = V.sn[s];
+    const bool active = V.active[S.instance] != 0;
+    if (threadIdx.x == 0) {
+      bool ready = true;
+      if (active) {
+        if (forward) {
+          for (int ci = 0; ci < S.child_count && ready; ++ci) {
+            ready = WaitFlag(fdone + V.child_list[S.child_begin + ci]);
+          }
+        } else {
+          ready = WaitFlag(S.parent >= 0 ? bdone + S.parent : fdone + s);
+        }
+        if (!ready) {
+          atomicOr(V.status + S.instance, kStatusWaitTimeout);
+        }
+      }
+      go = active && ready ? 1 : 0;
+    }
+    __syncthreads();
+    if (go != 0) {
+      if (forward) {
+        if (Fp32Front(V, S)) {
+          ForwardTreeBody<float>(V, S, dvec, inv, buf);
+        } else {
+          ForwardTreeBody<double>(V, S, dvec, inv, buf);
+        }
+      } else {
+        if (Fp32Front(V, S)) {
+          BackwardTreeBody<float>(V, S, inv, buf);
+        } else {
+          BackwardTreeBody<double>(V, S, inv, buf);
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      SetFlag((forward ? fdone : bdone) + s);
+    }
+  }
+}
+
 }  // namespace sdfgpu
 
 // ------------------------------------------------------------ launchers --
@@ -768,6 +1242,11 @@ __global__ void __launch_bounds__(256) KBackward(DeviceView V, const int32_t* le
 #include "engine.h"
 
 namespace sdfgpu {
+
+static_assert(kInvBlock == kInvBlockDoubles, "inverted block size");
+
+/// Dynamic shared memory a block may use on B200.
+constexpr int kMaxSmem = 227 * 1024;
 
 void ConfigureSolveKernels(int max_front) {
   // The attribute belongs to the kernel, not to an engine: it only grows, so
@@ -784,7 +1263,7 @@ void ConfigureSolveKernels(int max_front) {
     }
   }
   const int smem = max_front * static_cast<int>(sizeof(double));
-  if (smem > 227 * 1024) {
+  if (smem > kMaxSmem) {
     Fail(SDFGPU_ERR_INVALID_ARGUMENT, "front too large for the solve kernels");
   }
   std::lock_guard<std::mutex> lk(mu);
@@ -792,6 +1271,12 @@ void ConfigureSolveKernels(int max_front) {
     CudaCheck(cudaFuncSetAttribute(KForward, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
     CudaCheck(cudaFuncSetAttribute(KBackward, cudaFuncAttributeMaxDynamicSharedMemorySize, smem), "smem attr");
     configured = smem;
+  }
+  static int tree_configured = 48 * 1024;
+  const int tree = static_cast<int>(SolveTreeSmem(max_front));
+  if (tree <= kMaxSmem && tree > tree_configured) {
+    CudaCheck(cudaFuncSetAttribute(KSolveTree, cudaFuncAttributeMaxDynamicSharedMemorySize, tree), "smem attr");
+    tree_configured = tree;
   }
 }
 
@@ -835,6 +1320,12 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
       ++launches;
     }
   }
+  if (P.inv != nullptr && P.num_inv > 0) {
+    // inverted diagonal blocks for the one-launch solve
+    KInvertDiagonal<<<static_cast<unsigned>((P.num_inv + 3) / 4), 128, 0, stream>>>(V, P.inv_tasks, P.num_inv,
+                                                                                   P.inv);
+    ++launches;
+  }
   CudaCheck(cudaGetLastError(), "factor kernels");
   return launches;
 }
@@ -842,6 +1333,28 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
 int LaunchSolveLevels(const Symbolic& S, const DeviceView& V, const FactorPlan& P, cudaStream_t stream) {
   int launches = 0;
   const size_t smem = static_cast<size_t>(P.max_front) * sizeof(double);
+  const int num_sn = static_cast<int>(S.sn.size());
+  const size_t tree_smem = SolveTreeSmem(P.max_front);
+  if (P.solve_sync != nullptr && P.inv != nullptr && tree_smem <= static_cast<size_t>(kMaxSmem)) {
+    if (num_sn == 0) {
+      return 0;
+    }
+    static const int sms = [] {
+      int dev = 0;
+      int count = 0;
+      CudaCheck(cudaGetDevice(&dev), "device");
+      CudaCheck(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev), "SM count");
+      return count;
+    }();
+    // one resident block per SM (the kernel's register bound); blocks that
+    // find no task left return at once
+    const int blocks = std::min(2 * num_sn, sms);
+    CudaCheck(cudaMemsetAsync(P.solve_sync, 0, SolveSyncWords(num_sn) * sizeof(uint32_t), stream), "solve flags");
+    KSolveTree<<<static_cast<unsigned>(blocks), 256, tree_smem, stream>>>(V, P.level_sn, num_sn, P.dvec, P.inv,
+                                                                          P.solve_sync);
+    CudaCheck(cudaGetLastError(), "solve kernel");
+    return 1;
+  }
   for (int l = 0; l < S.num_levels; ++l) {
     const int b = S.level_begin[static_cast<size_t>(l)];
     const int e = S.level_begin[static_cast<size_t>(l) + 1];

@@ -90,6 +90,7 @@ struct SupernodeRec {
   int32_t instance;
   int32_t pose_root;  // 1: the dense pose block of its instance
   int32_t upper_l11;  // 1: L of the pivot block is stored transposed in its upper triangle
+  int32_t panel_base; // first of its ceil(ncols / 32) inverted diagonal blocks
 };
 
 /// A contiguous block of work items of one kernel launch in the level
@@ -138,6 +139,9 @@ struct Symbolic {
   int front_rows{256};
   int panel_rows{128};
   std::vector<int> height;                   // per supernode: height in the assembly tree
+  // (sn, panel) of every 32-column diagonal block, in panel_base order: the
+  // inverted unit triangles the solve multiplies by
+  std::vector<int32_t> inv_tasks;
   std::vector<int32_t> small_tasks;
   std::vector<TaskRange> small_range;        // per level
   std::vector<int32_t> small_max_k;          // per level

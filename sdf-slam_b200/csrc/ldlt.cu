@@ -92,6 +92,13 @@ LdltEngine::LdltEngine(int n, const int32_t* outer, const int32_t* inner, const 
   plan_.level_sn = level_sn_.get();
   plan_.dvec = dvec_.get();
   plan_.max_front = max_front;
+  solve_sync_.Alloc(SolveSyncWords(static_cast<int>(sym_.sn.size())));
+  plan_.solve_sync = solve_sync_.get();
+  inv_tasks_.Upload(sym_.inv_tasks, s);
+  inv_.Alloc(std::max<size_t>(1, sym_.inv_tasks.size() / 2) * kInvBlockDoubles);
+  plan_.inv_tasks = inv_tasks_.get();
+  plan_.num_inv = static_cast<int>(sym_.inv_tasks.size() / 2);
+  plan_.inv = inv_.get();
   CudaCheck(cudaStreamSynchronize(s), "ldlt analyze");
 }
 
@@ -132,10 +139,16 @@ void LdltEngine::Solve(const double* b, double* x) {
   cudaStream_t s = stream_;
   CudaCheck(cudaMemcpyAsync(rhs_.get(), b, static_cast<size_t>(n_) * sizeof(double), cudaMemcpyHostToDevice, s),
             "b");
+  CudaCheck(cudaMemsetAsync(status_.get(), 0, sizeof(int32_t), s), "status");
   LaunchSolveLevels(sym_, V_, plan_, s);
+  int32_t st = 0;
+  CudaCheck(cudaMemcpyAsync(&st, status_.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, s), "status");
   CudaCheck(cudaMemcpyAsync(x, step_.get(), static_cast<size_t>(n_) * sizeof(double), cudaMemcpyDeviceToHost, s),
             "x");
   CudaCheck(cudaStreamSynchronize(s), "solve");
+  if ((st & kStatusWaitTimeout) != 0) {
+    Fail(SDFGPU_ERR_CUDA, "a wait of the solve kernel ran out of its limit");
+  }
 }
 
 }  // namespace sdfgpu

@@ -36,6 +36,9 @@ class LdltEngine {
   DevBuf<int64_t> value_off_;
   DevBuf<double> values_, fronts_, upd_, dvec_, rhs_, step_, xs_;
   DevBuf<int32_t> status_, active_;
+  DevBuf<uint32_t> solve_sync_;
+  DevBuf<int32_t> inv_tasks_;
+  DevBuf<double> inv_;
 };
 
 }  // namespace sdfgpu

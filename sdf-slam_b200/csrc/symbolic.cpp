@@ -351,6 +351,15 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   for (SupernodeRec& r : S.sn) {
     r.upper_l11 = r.ncols <= S.small_pivots ? 1 : 0;
   }
+  S.inv_tasks.clear();
+  for (int s = 0; s < Sn; ++s) {
+    SupernodeRec& r = S.sn[static_cast<size_t>(s)];
+    r.panel_base = static_cast<int32_t>(S.inv_tasks.size() / 2);
+    for (int p = 0; p * B < r.ncols; ++p) {
+      S.inv_tasks.push_back(s);
+      S.inv_tasks.push_back(p);
+    }
+  }
   // blocks that keep every SM of a B200 (148) busy
   constexpr int64_t kFillBlocks = 148;
   const int small = S.small_pivots;
