@@ -367,10 +367,11 @@ def run_serve(P, args):
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# factor-phase kernels (KFactorFront, KUpdate, KPanel, KExtendAdd) in one LM
-# iteration, from one ncu capture of `profile_run.py floorplan 2`; L2 is not
-# flushed inside that capture, so writes that stay in L2 are not counted.
-FACTOR_TRAFFIC_BYTES = {"floorplan": 104.3e6}
+# factor-phase kernels (KFactorFront, KUpdate, KPanel, KExtendAdd,
+# KInvertDiagonal) in one LM iteration, from one ncu capture of
+# `profile_run.py floorplan 2` (default schedule); L2 is not flushed inside
+# that capture, so writes that stay in L2 are not counted.
+FACTOR_TRAFFIC_BYTES = {"floorplan": 113.2e6}
 
 
 def run_gpu(args, dist, world, rank, local):
@@ -456,7 +457,7 @@ def run_gpu(args, dist, world, rank, local):
         "bound": "tensor", "achieved": flops / per_step[2] / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
         "frac": flops / per_step[2] / 1e12 / fp64_peak,
         "traffic": FACTOR_TRAFFIC_BYTES.get(args.workload),
-        "kernel": "multifrontal LDL^T (KPanel + KUpdate + KExtendAdd), FP64",
+        "kernel": "multifrontal LDL^T (KFactorFront + KPanel + KUpdate + KExtendAdd + KInvertDiagonal), FP64",
         "peak_source": "nominal B200 FP64 (no measured FP64 peak on this pool)"}
     roofline_assemble = {
         "bound": "hbm", "achieved": assemble_bytes / per_step[0] / 1e9, "peak": hbm, "unit": "GB/s",
