@@ -261,10 +261,99 @@ __global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const
 /// the reciprocals of the pivots.
 constexpr int kSmallPivots = 128;
 
-/// Dynamic shared memory of KFactorFront for fronts of at most k pivots.
+/// Dynamic shared memory of KFactorFront for fronts of at most k pivots: the
+/// padded pivot block, the pivots' reciprocals and W = L D of one panel for
+/// the trailing update (kPanel rows of kpad + 1).
 __host__ __device__ constexpr size_t FactorFrontSmem(int k) {
   const size_t kpad = static_cast<size_t>((k + kPanel - 1) / kPanel * kPanel);
-  return (kpad * (kpad + 1) + kpad) * sizeof(double);
+  return (kpad * (kpad + 1) + kpad + static_cast<size_t>(kPanel) * (kpad + 1)) * sizeof(double);
+}
+
+/// Rows per block up to which the rows below a pivot block are shared by
+/// eight threads each.
+constexpr int kRowsShared = 32;
+
+/// Rows below the pivot block, eight threads per row (row = tid / 8 of a
+/// pass over blockDim / 8 rows, the thread owning columns 4g..4g+3 of every
+/// panel, g = tid % 8): per panel
+/// the earlier panels' L values of the row (kept in shared memory) are
+/// subtracted, then the panel's triangle is solved with the pivot values
+/// passed between the row's threads by shuffles, then scaled by D^-1. Every
+/// entry sees the same operations in the same order as the thread-per-row
+/// path. Y: rows x (kpad + 1) values in shared memory.
+template <typename T>
+__device__ __forceinline__ void RowsBelowShared(T* Fs, int F, int k, int kpad, int ld, int row_begin, int rows,
+                                                const T* D, const T* dinv, T* Y) {
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int g = tid & 7;
+  const int base = lane & ~7;
+  const int ldy = kpad + 1;
+  const int np = (k + kPanel - 1) / kPanel;
+  const int64_t F64 = F;
+  const int per_pass = static_cast<int>(blockDim.x) >> 3;
+  for (int rb = 0; rb < rows; rb += per_pass) {
+    const int ri = rb + (tid >> 3);
+    const int r = row_begin + ri;
+    const bool live = ri < rows && r < F;
+    // the row's assembled values in this thread's columns of every panel
+    T a[kSmallPivots / kPanel][4];
+#pragma unroll
+    for (int p = 0; p < kSmallPivots / kPanel; ++p) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int j = p * kPanel + 4 * g + i;
+        a[p][i] = (live && j < k) ? Fs[j * F64 + r] : T(0);
+      }
+    }
+    T* yrow = Y + (live ? ri : 0) * ldy;
+#pragma unroll
+    for (int p = 0; p < kSmallPivots / kPanel; ++p) {
+      if (p >= np) {
+        break;
+      }
+      const int p0 = p * kPanel;
+      T acc[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        acc[i] = a[p][i];
+      }
+      const T* drow = D + (p0 + 4 * g) * ld;
+      // contributions of the earlier panels
+      for (int q = 0; q < p; ++q) {
+        const int q0 = q * kPanel;
+#pragma unroll 8
+        for (int l = 0; l < kPanel; ++l) {
+          const T yl = yrow[q0 + l] * D[(q0 + l) * ld + q0 + l];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            acc[i] -= yl * drow[i * ld + q0 + l];
+          }
+        }
+      }
+      // this panel's triangle: pivot l's final value comes from its owner
+#pragma unroll
+      for (int l = 0; l < kPanel; ++l) {
+        const T yl = __shfl_sync(0xffffffffu, acc[l & 3], base + (l >> 2));
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          if (4 * g + i > l) {
+            acc[i] -= yl * drow[i * ld + p0 + l];
+          }
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int j = p0 + 4 * g + i;
+        if (j < k && live) {
+          const T v = acc[i] * dinv[j];
+          yrow[j] = v;
+          Fs[j * F64 + r] = v;
+        }
+      }
+      __syncwarp();
+    }
+  }
 }
 
 template <typename T>
@@ -275,17 +364,35 @@ __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const Super
   const int kpad = (k + kPanel - 1) / kPanel * kPanel;
   const int ld = kpad + 1;
   T* dinv = D + kpad * ld;
+  T* W = dinv + kpad;  // [kPanel][ld]: W(c, l) = L(c, p0 + l) d_l at W[l * ld + c]
   T* Fs = WorkFront<T>(V, S);
   const int tid = threadIdx.x;
   const int warp = tid >> 5;
   const int nwarps = static_cast<int>(blockDim.x >> 5);
   const int lane = tid & 31;
-  // one warp per column: coalesced loads of the column's lower part
-  for (int c = warp; c < k; c += nwarps) {
-    const T* src = Fs + static_cast<int64_t>(c) * F;
-#pragma unroll 4
-    for (int r = c + lane; r < k; r += 32) {
-      D[r * ld + c] = src[r];
+  const int nthreads = static_cast<int>(blockDim.x);
+  // the pivot block's lower triangle, column by column over all threads
+  // (coalesced), eight loads in flight per thread
+  {
+    const int kk = k * k;
+    for (int base = tid; base < kk; base += 8 * nthreads) {
+      T val[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int i = base + u * nthreads;
+        const int c = i / k;
+        const int r = i - c * k;
+        val[u] = (i < kk && r >= c) ? Fs[static_cast<int64_t>(c) * F + r] : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int i = base + u * nthreads;
+        const int c = i / k;
+        const int r = i - c * k;
+        if (i < kk && r >= c) {
+          D[r * ld + c] = val[u];
+        }
+      }
     }
   }
   for (int idx = k * ld + tid; idx < kpad * ld; idx += blockDim.x) {
@@ -324,25 +431,52 @@ __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const Super
       }
     }
     __syncthreads();
-    // rank-w update of the trailing pivot block: thread per column c with
-    // d_l L(c, l) in registers, rows r >= c read as broadcasts (the panel is
-    // full width here because a trailing column exists)
-    for (int c = p0 + w + tid; c < k; c += blockDim.x) {
-      T wc[kPanel];
-#pragma unroll
-      for (int l = 0; l < kPanel; ++l) {
-        wc[l] = D[c * ld + p0 + l] * D[(p0 + l) * ld + p0 + l];
+    // rank-w update of the trailing pivot block (the panel is full width
+    // here because a trailing column exists): W = L(:, panel) D first, then
+    // one item per (4-row block, column) over all threads, rows read as
+    // broadcasts and W along the columns; even and odd l accumulate
+    // separately, as two chains per entry
+    const int t0 = p0 + w;
+    const int nt = k - t0;
+    if (nt > 0) {
+      for (int idx = tid; idx < kPanel * nt; idx += nthreads) {
+        const int l = idx / nt;
+        const int ci = idx - l * nt;
+        W[l * ld + ci] = D[(t0 + ci) * ld + p0 + l] * D[(p0 + l) * ld + p0 + l];
       }
-      for (int r = c; r < k; ++r) {
-        const T* lr = D + r * ld + p0;
-        T a0 = T(0);
-        T a1 = T(0);
+      __syncthreads();
+      const int nrb = (nt + 3) / 4;
+      for (int idx = tid; idx < nrb * nt; idx += nthreads) {
+        const int rb = idx / nt;
+        const int ci = idx - rb * nt;
+        if (4 * rb + 3 < ci) {
+          continue;  // the four rows lie above the diagonal
+        }
+        T a0[4];
+        T a1[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          a0[u] = T(0);
+          a1[u] = T(0);
+        }
+        const T* l0 = D + (t0 + 4 * rb) * ld + p0;
 #pragma unroll
         for (int l = 0; l < kPanel; l += 2) {
-          a0 = fma(lr[l], wc[l], a0);
-          a1 = fma(lr[l + 1], wc[l + 1], a1);
+          const T w0 = W[l * ld + ci];
+          const T w1 = W[(l + 1) * ld + ci];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            a0[u] = fma(l0[u * ld + l], w0, a0[u]);
+            a1[u] = fma(l0[u * ld + l + 1], w1, a1[u]);
+          }
         }
-        D[r * ld + c] -= a0 + a1;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int r = 4 * rb + u;
+          if (r < nt && r >= ci) {
+            D[(t0 + r) * ld + t0 + ci] -= a0[u] + a1[u];
+          }
+        }
       }
     }
     __syncthreads();
@@ -362,6 +496,10 @@ __device__ __forceinline__ void FactorFrontBody(const DeviceView& V, const Super
     if (tid == 0 && zero_pivot) {
       atomicOr(V.status + S.instance, kStatusZeroPivot);
     }
+  }
+  if (rows <= kRowsShared && k <= kSmallPivots) {
+    RowsBelowShared<T>(Fs, F, k, kpad, ld, row_begin, rows, D, dinv, W);
+    return;
   }
   // rows below the pivot block: thread per row, panel by panel
   const int r = row_begin + tid;
