@@ -107,14 +107,15 @@ __device__ __forceinline__ bool DiagonalBlockLdlt(T* B, int ld, int w, T (*lbuf)
   return zero;
 }
 
-/// Adds one child's update columns [cbeg, cend) into the parent front.
+/// Adds one child's update columns [cbeg, cend) in place into the parent
+/// front (fronts too wide to stage): warp per column, lanes over rows.
 template <typename TP, typename TC>
-__device__ __forceinline__ void ExtendAddChild(TP* Fp, int PF, const TC* U, int CF, const int32_t* rel, int m,
-                                               int cbeg, int cend) {
+__device__ __forceinline__ void ExtendAddDirect(TP* Fp, int64_t PF, const TC* U, int CF, const int32_t* rel, int m,
+                                                int cbeg, int cend) {
   const int lane = threadIdx.x & 31;
-  const int nwarps = blockDim.x >> 5;
-  for (int cc = cbeg + (threadIdx.x >> 5); cc < cend; cc += nwarps) {
-    TP* __restrict__ dst = Fp + static_cast<int64_t>(rel[cc]) * PF;
+  const int nwarps = static_cast<int>(blockDim.x >> 5);
+  for (int cc = cbeg + static_cast<int>(threadIdx.x >> 5); cc < cend; cc += nwarps) {
+    TP* __restrict__ dst = Fp + rel[cc] * PF;
     const TC* __restrict__ src = U + static_cast<int64_t>(cc) * CF;
 #pragma unroll 4
     for (int r = cc + lane; r < m; r += 32) {
@@ -123,38 +124,129 @@ __device__ __forceinline__ void ExtendAddChild(TP* Fp, int PF, const TC* U, int 
   }
 }
 
+/// Adds one child's update columns [cbeg, cend) into the staged parent
+/// columns (stage: `rows` values per parent column from row c). Four entries
+/// per thread per batch, their loads issued together.
+template <typename TP, typename TC>
+__device__ __forceinline__ void ExtendAddStaged(TP* stage, int c, int rows, const TC* U, int CF,
+                                                const int32_t* rel, int m, int cbeg, int cend) {
+  const int nthreads = static_cast<int>(blockDim.x);
+  const int items = (cend - cbeg) * m;
+  for (int base = threadIdx.x; base < items; base += 4 * nthreads) {
+    int dst[4];
+    TC val[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int idx = base + u * nthreads;
+      const int cq = idx / m;
+      const int r = idx - cq * m;
+      const int cc = cbeg + cq;
+      const bool ok = idx < items && r >= cc;
+      dst[u] = ok ? (rel[cc] - c) * rows + (rel[r] - c) : -1;
+      val[u] = ok ? U[static_cast<int64_t>(cc) * CF + r] : TC(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (dst[u] >= 0) {
+        stage[dst[u]] += static_cast<TP>(val[u]);
+      }
+    }
+  }
+}
+
+/// Extend-add of one task, parent columns [c, chi): with `stage` the
+/// columns' lower part is copied into shared memory (one coalesced pass),
+/// every child's entries are added there in the children's fixed order and
+/// the columns are written back, so each entry sees the same additions in
+/// the same order as an in-place add without a chain of dependent global
+/// read-modify-writes; without it (a front too wide to stage) the children
+/// are added in place.
 template <typename TP>
-__device__ __forceinline__ void ExtendAddBody(const DeviceView& V, const SupernodeRec& P, const int32_t* ranges) {
-  TP* Fp = WorkFront<TP>(V, P);
+__device__ __forceinline__ void ExtendAddBody(const DeviceView& V, const SupernodeRec& P, const int32_t* t,
+                                              const int32_t* ranges, TP* stage) {
+  const int tid = threadIdx.x;
+  const int nthreads = static_cast<int>(blockDim.x);
+  if (stage == nullptr) {
+    for (int ci = 0; ci < P.child_count; ++ci) {
+      const SupernodeRec C = V.sn[V.child_list[P.child_begin + ci]];
+      const int32_t* rel = V.sn_rel + C.rows_off;
+      const int64_t uoff = static_cast<int64_t>(C.ncols) * C.F + C.ncols;
+      if (Fp32Front(V, C)) {
+        ExtendAddDirect<TP, float>(WorkFront<TP>(V, P), P.F, WorkFront<float>(V, C) + uoff, C.F, rel, C.nrows,
+                                   ranges[2 * ci], ranges[2 * ci + 1]);
+      } else {
+        ExtendAddDirect<TP, double>(WorkFront<TP>(V, P), P.F, WorkFront<double>(V, C) + uoff, C.F, rel, C.nrows,
+                                    ranges[2 * ci], ranges[2 * ci + 1]);
+      }
+      __syncthreads();
+    }
+    return;
+  }
+  const int c = t[1];
+  const int width = t[2] - c;
+  const int rows = P.F - c;
+  const int n = width * rows;
+  const int64_t PF = P.F;
+  TP* Fp = WorkFront<TP>(V, P) + c * PF + c;
+  for (int base = tid; base < n; base += 4 * nthreads) {
+    TP v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int idx = base + u * nthreads;
+      const int jj = idx / rows;
+      const int ii = idx - jj * rows;
+      v[u] = (idx < n && ii >= jj) ? Fp[jj * PF + ii] : TP(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int idx = base + u * nthreads;
+      if (idx < n) {
+        stage[idx] = v[u];
+      }
+    }
+  }
+  __syncthreads();
   for (int ci = 0; ci < P.child_count; ++ci) {
     const SupernodeRec C = V.sn[V.child_list[P.child_begin + ci]];
     const int32_t* rel = V.sn_rel + C.rows_off;
-    // update columns of this child that land in the task's parent columns
-    const int cbeg = ranges[2 * ci];
-    const int cend = ranges[2 * ci + 1];
     const int64_t uoff = static_cast<int64_t>(C.ncols) * C.F + C.ncols;
     if (Fp32Front(V, C)) {
-      ExtendAddChild<TP, float>(Fp, P.F, WorkFront<float>(V, C) + uoff, C.F, rel, C.nrows, cbeg, cend);
+      ExtendAddStaged<TP, float>(stage, c, rows, WorkFront<float>(V, C) + uoff, C.F, rel, C.nrows,
+                                 ranges[2 * ci], ranges[2 * ci + 1]);
     } else {
-      ExtendAddChild<TP, double>(Fp, P.F, WorkFront<double>(V, C) + uoff, C.F, rel, C.nrows, cbeg, cend);
+      ExtendAddStaged<TP, double>(stage, c, rows, WorkFront<double>(V, C) + uoff, C.F, rel, C.nrows,
+                                  ranges[2 * ci], ranges[2 * ci + 1]);
     }
     __syncthreads();
+  }
+  for (int idx = tid; idx < n; idx += nthreads) {
+    const int jj = idx / rows;
+    const int ii = idx - jj * rows;
+    if (ii >= jj) {
+      Fp[jj * PF + ii] = stage[idx];
+    }
   }
 }
 
 /// Adds the children's update matrices into each parent front. A task owns a
 /// range of parent columns, so no two blocks write the same entry; children
-/// are added in their fixed order.
-__global__ void KExtendAdd(DeviceView V, const int32_t* tasks, const int32_t* child_ranges) {
+/// are added in their fixed order. staged != 0: the launch's dynamic shared
+/// memory holds the columns of every task whose front is at most
+/// kEaStageMaxF wide.
+__global__ void KExtendAdd(DeviceView V, const int32_t* tasks, const int32_t* child_ranges, int staged) {
+  extern __shared__ double stage[];
   const int32_t* t = tasks + 4 * static_cast<int64_t>(blockIdx.x);
   const SupernodeRec P = V.sn[t[0]];
   if (V.active[P.instance] == 0) {
     return;
   }
+  // the task's columns are staged when the front is narrow enough (the
+  // symbolic analysis sized the launch's shared memory for those)
+  const bool use_stage = staged != 0 && P.F <= kEaStageMaxF;
   if (Fp32Front(V, P)) {
-    ExtendAddBody<float>(V, P, child_ranges + t[3]);
+    ExtendAddBody<float>(V, P, t, child_ranges + t[3], use_stage ? reinterpret_cast<float*>(stage) : nullptr);
   } else {
-    ExtendAddBody<double>(V, P, child_ranges + t[3]);
+    ExtendAddBody<double>(V, P, t, child_ranges + t[3], use_stage ? stage : nullptr);
   }
 }
 
@@ -938,15 +1030,20 @@ __global__ void __launch_bounds__(128) KInvertDiagonal(DeviceView V, const int32
     }
   }
   __syncwarp();
+  // right-looking: once m[j] is final it is subtracted from every later
+  // row, so each step waits on one multiply-add only (each m[i] still sees
+  // its terms in ascending j)
   double m[kPanel];
 #pragma unroll
   for (int i = 0; i < kPanel; ++i) {
-    double acc = i == lane ? 1.0 : 0.0;
+    m[i] = i == lane ? 1.0 : 0.0;
+  }
 #pragma unroll
-    for (int j = 0; j < i; ++j) {
-      acc = fma(-L[i][j], m[j], acc);
+  for (int j = 0; j < kPanel; ++j) {
+#pragma unroll
+    for (int i = j + 1; i < kPanel; ++i) {
+      m[i] = fma(-L[i][j], m[j], m[i]);
     }
-    m[i] = acc;
   }
   double* out = inv + static_cast<int64_t>(S.panel_base + p0 / kPanel) * kInvBlock;
   // M^T column major: (i, j) of M^T = M(j, i) = m[j] of lane i
@@ -1397,6 +1494,9 @@ void ConfigureSolveKernels(int max_front) {
     if (!front_configured) {
       const int bytes = static_cast<int>(FactorFrontSmem(kSmallPivots));
       CudaCheck(cudaFuncSetAttribute(KFactorFront, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "smem attr");
+      CudaCheck(cudaFuncSetAttribute(KExtendAdd, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     kEaStageDoubles * static_cast<int>(sizeof(double))),
+                "smem attr");
       front_configured = true;
     }
   }
@@ -1427,7 +1527,11 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
   for (int l = 0; l < S.num_levels; ++l) {
     const TaskRange ea = S.ea_range[static_cast<size_t>(l)];
     if (ea.count > 0) {
-      KExtendAdd<<<static_cast<unsigned>(ea.count), 256, 0, stream>>>(V, P.ea_tasks + 4 * ea.begin, P.ea_child);
+      // staged in shared memory unless a front of the level is too wide
+      const size_t stage = static_cast<size_t>(S.ea_stage[static_cast<size_t>(l)]) * sizeof(double);
+      const bool staged = stage <= static_cast<size_t>(kEaStageDoubles) * sizeof(double);
+      KExtendAdd<<<static_cast<unsigned>(ea.count), 256, staged ? stage : 0, stream>>>(
+          V, P.ea_tasks + 4 * ea.begin, P.ea_child, staged ? 1 : 0);
       ++launches;
     }
     const TaskRange sm = S.small_range[static_cast<size_t>(l)];

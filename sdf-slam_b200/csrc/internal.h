@@ -125,6 +125,7 @@ struct Symbolic {
   std::vector<int32_t> ea_tasks;             // (sn, col_lo, col_hi, ea_child offset) quads
   std::vector<int32_t> ea_child;             // per task and child: update column range [begin, end)
   std::vector<TaskRange> ea_range;           // per level
+  std::vector<int32_t> ea_stage;             // per level: values a task stages in shared memory
   std::vector<int32_t> panel_tasks;          // (sn, panel, row_begin) triples
   std::vector<TaskRange> panel_range;        // per (level, panel) flattened
   std::vector<int32_t> update_tasks;         // (sn, panel, ti, tj) quads
@@ -213,6 +214,14 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads = 0);
 /// least as many instances as threads, else one after another on all.
 void AnalyzeInstances(const std::vector<HostProblem>& problems, const std::vector<int>& margin,
                       std::vector<SymPiece>& pieces, const std::vector<int>* which);
+
+/// Values (doubles) of a parent front's column range that one extend-add
+/// task stages in shared memory at most (96 KB).
+constexpr int kEaStageDoubles = 12288;
+/// Widest parent front whose extend-add is staged in shared memory; wider
+/// fronts (whose children touch a small part of each column) are added in
+/// place.
+constexpr int kEaStageMaxF = 384;
 
 /// Schedule parameters of the factorization (see Symbolic).
 struct Schedule {

@@ -412,6 +412,7 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   S.panel_range.assign(static_cast<size_t>(slots), {});
   S.update_range.assign(static_cast<size_t>(slots), {});
   S.ea_range.assign(static_cast<size_t>(levels), {});
+  S.ea_stage.assign(static_cast<size_t>(levels), 0);
   // Schur complement tasks (rank-k update of the trailing block) are stored
   // as update tasks with panel = -1 after the per-panel ones of each level;
   // update_range has one extra slot per level for them.
@@ -436,17 +437,25 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
       }
     }
     std::vector<int32_t> cursor;
+    int32_t stage = 0;
     for (int q = qb; q < qe; ++q) {
       const int s = S.level_sn[static_cast<size_t>(q)];
       const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
       if (r.child_count == 0) {
         continue;
       }
+      // a task of a front up to kEaStageMaxF wide stages its columns' lower
+      // part in shared memory (narrower ranges where they would not fit)
+      const bool staged = r.F <= kEaStageMaxF;
+      const int cols = staged ? std::max(1, std::min(ea_cols, kEaStageDoubles / r.F)) : ea_cols;
       // per child: the range of its update columns that land in [c, chi);
       // the positions ascend, so one cursor per child walks them once
       cursor.assign(static_cast<size_t>(r.child_count), 0);
-      for (int c = 0; c < r.F; c += ea_cols) {
-        const int chi = std::min(r.F, c + ea_cols);
+      for (int c = 0; c < r.F; c += cols) {
+        const int chi = std::min(r.F, c + cols);
+        if (staged) {
+          stage = std::max(stage, (chi - c) * (r.F - c));
+        }
         S.ea_tasks.push_back(s);
         S.ea_tasks.push_back(c);
         S.ea_tasks.push_back(chi);
@@ -465,6 +474,7 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
     }
     S.ea_range[static_cast<size_t>(l)].count =
         static_cast<int64_t>(S.ea_tasks.size() / 4) - S.ea_range[static_cast<size_t>(l)].begin;
+    S.ea_stage[static_cast<size_t>(l)] = stage;
     for (int t = 0; t < S.level_panels[static_cast<size_t>(l)]; ++t) {
       const size_t slot = static_cast<size_t>(S.panel_index_base[static_cast<size_t>(l)] + t);
       S.panel_range[slot].begin = static_cast<int64_t>(S.panel_tasks.size() / 3);
@@ -1049,6 +1059,7 @@ void Reschedule(Symbolic& S, const Schedule& sched) {
   S.update_tasks.clear();
   S.small_tasks.clear();
   S.ea_range.clear();
+  S.ea_stage.clear();
   S.panel_range.clear();
   S.update_range.clear();
   S.small_range.clear();
