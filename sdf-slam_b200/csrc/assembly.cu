@@ -361,20 +361,22 @@ __device__ __forceinline__ int FindInstanceByCell(const DeviceView& V, int64_t c
 
 }  // namespace
 
-/// One colour class of cells (cx % 2, cy % 2) = (pass & 1, pass >> 1): cells
-/// of one class share no node, so each adds its contributions to J^T J and
-/// J^T r with plain read-modify-writes. One warp per cell: the 4x4 map block
+/// One colour class of cells (cx % 2, cy % 2) = (pass & 1, pass >> 1), listed
+/// in `cells` (every launched warp has a cell): cells of one class share no
+/// node, so each adds its contributions to J^T J and J^T r with plain
+/// read-modify-writes. One warp per cell: the 4x4 map block
 /// and the corner gradients are lane-strided sums over the cell's point rows
 /// reduced by a fixed butterfly; the map-pose blocks are segmented sums over
 /// runs of rows of one frame (rows of a cell are sorted, so frames are
 /// contiguous); the cell's Eikonal row (spec at its lower-left node) follows.
 /// Passes run in a fixed order, so every entry is a deterministic sum.
-__global__ void KCellPass(DeviceView V, int pass) {
-  const int64_t cell = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+__global__ void KCellPass(DeviceView V, const int64_t* cells, int64_t count) {
+  const int64_t w = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (cell >= V.total_cells) {
+  if (w >= count) {
     return;
   }
+  const int64_t cell = cells[w];
   const int i = FindInstanceByCell(V, cell);
   const InstDev& I = V.inst[i];
   if (V.active[i] == 0) {
@@ -384,9 +386,6 @@ __global__ void KCellPass(DeviceView V, int pass) {
   const int local = static_cast<int>(cell - I.cell_off);
   const int cx = local % cw;
   const int cy = local / cw;
-  if ((cx & 1) != (pass & 1) || (cy & 1) != (pass >> 1)) {
-    return;
-  }
   const int64_t n0 = I.node_off + static_cast<int64_t>(cy) * I.nx + cx;
   int col[4];
   col[0] = V.node_col[n0];

@@ -17,7 +17,7 @@ __global__ void KPointRows(DeviceView V);
 __global__ void KEikonalRows(DeviceView V);
 __global__ void KOdomRows(DeviceView V);
 __global__ void KCellStart(const int32_t* keys, int64_t n, int64_t num_cells, int32_t* cell_start);
-__global__ void KCellPass(DeviceView V, int pass);
+__global__ void KCellPass(DeviceView V, const int64_t* cells, int64_t count);
 __global__ void KPoseFrames(DeviceView V);
 __global__ void KFinalizeNormal(DeviceView V);
 __global__ void KPosePairs(DeviceView V);
@@ -323,6 +323,25 @@ void Engine::UploadProblem() {
   eik_rec_.Alloc(static_cast<size_t>(total_eik_) * kEikRec);
   odom_rec_.Alloc(static_cast<size_t>(total_odom_) * kOdomRec);
   cell_start_.Alloc(static_cast<size_t>(total_cells_) + 2);
+  {
+    // the cells of each colour class (cx % 2, cy % 2) = (pass & 1, pass >> 1)
+    std::vector<int64_t> cells;
+    cells.reserve(static_cast<size_t>(total_cells_));
+    for (int pass = 0; pass < 4; ++pass) {
+      pass_begin_[pass] = static_cast<int64_t>(cells.size());
+      for (const InstanceLayout& L : layout_) {
+        const int cw = L.nx - 1;
+        const int ch = L.ny - 1;
+        for (int cy = pass >> 1; cy < ch; cy += 2) {
+          for (int cx = pass & 1; cx < cw; cx += 2) {
+            cells.push_back(L.cell_off + static_cast<int64_t>(cy) * cw + cx);
+          }
+        }
+      }
+    }
+    pass_begin_[4] = static_cast<int64_t>(cells.size());
+    pass_cells_.Upload(cells, stream_);
+  }
   sort_keys_a_.Alloc(static_cast<size_t>(total_points_));
   sort_vals_a_.Alloc(static_cast<size_t>(total_points_));
   sort_keys_b_.Alloc(static_cast<size_t>(total_points_));
@@ -666,7 +685,10 @@ void Engine::LaunchNormal() {
   CudaCheck(cudaMemsetAsync(rhs_.get(), 0, static_cast<size_t>(n_) * sizeof(double), stream_), "rhs memset");
   if (total_cells_ > 0) {
     for (int pass = 0; pass < 4; ++pass) {
-      KCellPass<<<Blocks(total_cells_ * 32, 256), 256, 0, stream_>>>(V_, pass);
+      const int64_t count = pass_begin_[pass + 1] - pass_begin_[pass];
+      if (count > 0) {
+        KCellPass<<<Blocks(count * 32, 256), 256, 0, stream_>>>(V_, pass_cells_.get() + pass_begin_[pass], count);
+      }
     }
   }
   KPoseFrames<<<static_cast<unsigned>(total_frames_), 256, 0, stream_>>>(V_);

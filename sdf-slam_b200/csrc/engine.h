@@ -266,6 +266,7 @@ class Engine {
   DeviceView V_{};
   IterTimes times_;
   int64_t total_cells_{0};
+  int64_t pass_begin_[5]{};   // colour class p's cells: pass_cells_[pass_begin_[p], pass_begin_[p + 1])
   int64_t total_points_{0};
   int64_t total_eik_{0};
   int64_t total_odom_{0};
@@ -293,6 +294,7 @@ class Engine {
   DevBuf<double> pt_rec_, eik_rec_, odom_rec_;
   DevBuf<int64_t> pt_poff_;
   DevBuf<int32_t> pt_cell_, cell_start_, sort_keys_a_, sort_vals_a_, sort_keys_b_, sort_vals_b_, sort_hist_;
+  DevBuf<int64_t> pass_cells_;
   DevBuf<double> rhs_, step_, xs_, lam_, dvec_;
   DevBuf<int32_t> marq_, status_, active_, revert_;
   DevBuf<double> terms_, sq_terms_, pred_terms_, seg_out_, seg_partial_;
