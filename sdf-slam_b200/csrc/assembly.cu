@@ -401,8 +401,9 @@ __global__ void KCellPass(DeviceView V, const int64_t* cells, int64_t count) {
   // One pass over the cell's rows in chunks of 32 (lane l takes rows
   // rb + l + 32 t): the 4x4 map block and corner gradients accumulate per
   // lane and are reduced by a fixed butterfly at the end; the map-pose
-  // blocks are segmented sums over runs of one frame inside each chunk. The
-  // next chunk's row indices are loaded ahead.
+  // blocks are segmented sums over runs of one frame inside each chunk. A
+  // chunk's records, frames and front offsets are loaded while the previous
+  // chunk is scanned and written (the row indices one chunk further ahead).
   double mm[10];
   double g[4];
 #pragma unroll
@@ -414,30 +415,47 @@ __global__ void KCellPass(DeviceView V, const int64_t* cells, int64_t count) {
     g[q] = 0.0;
   }
   bool overflow = false;
-  int k_next = (rb + lane < re) ? V.cell_rows[rb + lane] : -1;
+  struct ChunkRow {
+    double2 a01, a23, p01, p2r;
+    longlong2 o01, o23;
+    int f;
+  };
+  auto fetch = [&](int kk, ChunkRow& R) {
+    if (kk >= 0) {
+      const double2* r2 = reinterpret_cast<const double2*>(V.pt_rec + static_cast<int64_t>(kk) * kPointRec);
+      const longlong2* po = reinterpret_cast<const longlong2*>(V.pt_poff + 4 * static_cast<int64_t>(kk));
+      R.a01 = r2[0];
+      R.a23 = r2[1];
+      R.p01 = r2[2];
+      R.p2r = r2[3];
+      R.o01 = po[0];
+      R.o23 = po[1];
+      R.f = V.pt_frame[kk];
+    } else {
+      R.a01 = R.a23 = R.p01 = R.p2r = make_double2(0.0, 0.0);
+      R.o01 = R.o23 = make_longlong2(-1, -1);
+      R.f = -1;
+    }
+  };
+  int k = (rb + lane < re) ? V.cell_rows[rb + lane] : -1;
+  ChunkRow cur;
+  fetch(k, cur);
+  int k_next = (rb + 32 + lane < re) ? V.cell_rows[rb + 32 + lane] : -1;
   for (int base = rb; base < re; base += 32) {
-    const int k = k_next;
+    ChunkRow nxt;
+    int k_after = -1;
+    if (base + 32 < re) {
+      fetch(k_next, nxt);
+      k_after = (base + 64 + lane < re) ? V.cell_rows[base + 64 + lane] : -1;
+    } else {
+      fetch(-1, nxt);
+    }
     const bool in = k >= 0;
-    k_next = (base + 32 + lane < re) ? V.cell_rows[base + 32 + lane] : -1;
-    int f = -1;
-    double J[4] = {0.0, 0.0, 0.0, 0.0};
-    double jp[3] = {0.0, 0.0, 0.0};
-    double r = 0.0;
+    const int f = in ? cur.f : -1;
+    double J[4] = {cur.a01.x, cur.a01.y, cur.a23.x, cur.a23.y};
+    const double jp[3] = {cur.p01.x, cur.p01.y, cur.p2r.x};
+    const double r = cur.p2r.y;
     if (in) {
-      const double2* r2 = reinterpret_cast<const double2*>(V.pt_rec + static_cast<int64_t>(k) * kPointRec);
-      const double2 a01 = r2[0];
-      const double2 a23 = r2[1];
-      const double2 p01 = r2[2];
-      const double2 p2r = r2[3];
-      J[0] = a01.x;
-      J[1] = a01.y;
-      J[2] = a23.x;
-      J[3] = a23.y;
-      jp[0] = p01.x;
-      jp[1] = p01.y;
-      jp[2] = p2r.x;
-      r = p2r.y;
-      f = V.pt_frame[k];
       int q = 0;
 #pragma unroll
       for (int aa = 0; aa < 4; ++aa) {
@@ -474,10 +492,7 @@ __global__ void KCellPass(DeviceView V, const int64_t* cells, int64_t count) {
     const bool tail = in && (lane == 31 || p + 1 >= re || fn != f);
     const int fl = f - I.frame_off;
     if (tail && fl >= 1) {
-      const longlong2* po = reinterpret_cast<const longlong2*>(V.pt_poff + 4 * static_cast<int64_t>(k));
-      const longlong2 o01 = po[0];
-      const longlong2 o23 = po[1];
-      const int64_t offs[4] = {o01.x, o01.y, o23.x, o23.y};
+      const int64_t offs[4] = {cur.o01.x, cur.o01.y, cur.o23.x, cur.o23.y};
 #pragma unroll
       for (int aa = 0; aa < 4; ++aa) {
         if (col[aa] >= 0) {
@@ -493,6 +508,9 @@ __global__ void KCellPass(DeviceView V, const int64_t* cells, int64_t count) {
       }
     }
     __syncwarp();
+    cur = nxt;
+    k = k_next;
+    k_next = k_after;
   }
 #pragma unroll
   for (int q = 0; q < 10; ++q) {
