@@ -5,7 +5,7 @@
 // ascending row order, src/solvers/lm_solver.cpp:113-172). Rows arrive in
 // row order, so a stable sort on the cell key alone gives that order.
 // 8-bit digits; per pass: a per-tile digit histogram, one exclusive scan over
-// (digit, tile), and a stable scatter that ranks equal digits inside a warp
+// (digit, tile) (KDigitScan), and a stable scatter that ranks equal digits inside a warp
 // with __match_any_sync and across warps with shared counters.
 #include <cuda_runtime.h>
 
@@ -32,48 +32,96 @@ __global__ void KRadixHist(const int32_t* keys, int64_t n, int shift, int32_t* h
   hist[static_cast<int64_t>(threadIdx.x) * num_tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-/// Exclusive scan of `count` int32 values in place by one block of 1024
-/// threads (counts here are at most 256 * tiles): thread t owns a contiguous
-/// segment, whose loads are all in flight together; one block scan of the
-/// segment sums gives each segment's start.
-__global__ void KExclusiveScan(int32_t* data, int64_t count) {
-  __shared__ int32_t warp_sums[32];
+/// Exclusive scan, in place, of the digit histogram hist[digit * tiles +
+/// tile] in (digit, tile) order, by one block of 1024 threads: warp w owns
+/// digits 8w..8w+7 and walks their rows in chunks of 32 tiles (lane = tile,
+/// coalesced, the eight rows' loads in flight together). Pass one sums each
+/// row, a scan of the 256 row totals gives every digit's start, pass two
+/// scans each row chunk by chunk with a carry.
+__global__ void __launch_bounds__(1024) KDigitScan(int32_t* hist, int tiles) {
+  __shared__ int32_t start[256];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const int64_t per = (count + blockDim.x - 1) / blockDim.x;
-  const int64_t b = min(count, static_cast<int64_t>(threadIdx.x) * per);
-  const int64_t e = min(count, b + per);
-  int32_t local = 0;
-  for (int64_t q = b; q < e; ++q) {
-    local += data[q];
+  int32_t* rows = hist + static_cast<int64_t>(8 * warp) * tiles;
+  int32_t sum[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    sum[i] = 0;
   }
-  int32_t x = local;
-  for (int d = 1; d < 32; d <<= 1) {
-    const int32_t y = __shfl_up_sync(0xffffffffu, x, d);
-    if (lane >= d) {
-      x += y;
+#pragma unroll 2
+  for (int c0 = 0; c0 < tiles; c0 += 32) {
+    const int t = c0 + lane;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      sum[i] += t < tiles ? rows[static_cast<int64_t>(i) * tiles + t] : 0;
     }
   }
-  if (lane == 31) {
-    warp_sums[warp] = x;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      sum[i] += __shfl_xor_sync(0xffffffffu, sum[i], d);
+    }
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      start[8 * warp + i] = sum[i];
+    }
   }
   __syncthreads();
   if (warp == 0) {
-    int32_t s = lane < static_cast<int>(blockDim.x >> 5) ? warp_sums[lane] : 0;
+    // exclusive scan of the 256 totals: lane l owns digits 8l..8l+7
+    int32_t v[8];
+    int32_t own = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      v[i] = start[8 * lane + i];
+      own += v[i];
+    }
+    int32_t x = own;
+#pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-      const int32_t y = __shfl_up_sync(0xffffffffu, s, d);
+      const int32_t y = __shfl_up_sync(0xffffffffu, x, d);
       if (lane >= d) {
-        s += y;
+        x += y;
       }
     }
-    warp_sums[lane] = s;
+    int32_t run = x - own;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      start[8 * lane + i] = run;
+      run += v[i];
+    }
   }
   __syncthreads();
-  int32_t run = (warp > 0 ? warp_sums[warp - 1] : 0) + x - local;
-  for (int64_t q = b; q < e; ++q) {
-    const int32_t v = data[q];
-    data[q] = run;
-    run += v;
+  int32_t carry[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    carry[i] = start[8 * warp + i];
+  }
+  for (int c0 = 0; c0 < tiles; c0 += 32) {
+    const int t = c0 + lane;
+    int32_t v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      v[i] = t < tiles ? rows[static_cast<int64_t>(i) * tiles + t] : 0;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      int32_t x = v[i];
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) {
+          x += y;
+        }
+      }
+      if (t < tiles) {
+        rows[static_cast<int64_t>(i) * tiles + t] = carry[i] + x - v[i];
+      }
+      carry[i] += __shfl_sync(0xffffffffu, x, 31);
+    }
   }
 }
 
@@ -166,7 +214,7 @@ void LaunchCellSort(const int32_t* pt_cell, int64_t n, int64_t num_cells, int32_
   bool in_a = true;
   for (int shift = 0; shift < bits; shift += 8) {
     KRadixHist<<<tiles, kSortThreads, 0, stream>>>(kin, n, shift, hist, tiles);
-    KExclusiveScan<<<1, 1024, 0, stream>>>(hist, static_cast<int64_t>(256) * tiles);
+    KDigitScan<<<1, 1024, 0, stream>>>(hist, tiles);
     KRadixScatter<<<tiles, kSortThreads, 0, stream>>>(kin, vin, n, shift, hist, tiles, kout, vout);
     std::swap(kin, kout);
     std::swap(vin, vout);
