@@ -141,20 +141,50 @@ __device__ __forceinline__ double WrapAngle(double a) {
 
 }  // namespace
 
-/// Offset of (pose var (frame, 0), node column) in the front, or -1 when the
-/// frame is not in the node's analysed coupling set.
-__device__ __forceinline__ int64_t PoseOffset(const DeviceView& V, int col, int frame_local) {
-  int64_t lo = V.mp_ptr[col];
-  int64_t hi = V.mp_ptr[col + 1];
-  while (lo < hi) {
-    const int64_t mid = (lo + hi) >> 1;
-    if (V.mp_frame[mid] < frame_local) {
-      lo = mid + 1;
-    } else {
-      hi = mid;
-    }
+/// Offsets of the (pose var (frame, 0), node column) entries in the front for
+/// the four corner nodes of a cell (lower-left node n0, row length nx), -1
+/// where the frame is not in the node's analysed coupling set. The four
+/// lower-bound searches over the nodes' ascending frames advance in lock
+/// step, so every step's four loads are in flight together.
+__device__ __forceinline__ void PoseOffsets4(const DeviceView& V, int64_t n0, int nx, int frame_local,
+                                             int64_t off[4]) {
+  int col[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    col[q] = V.node_col[n0 + (q >> 1) * nx + (q & 1)];
   }
-  return (lo < V.mp_ptr[col + 1] && V.mp_frame[lo] == frame_local) ? V.mp_off[lo] : -1;
+  int64_t base[4];
+  int64_t end[4];
+  int64_t len[4];
+  int64_t longest = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    base[q] = col[q] >= 0 ? V.mp_ptr[col[q]] : 0;
+    end[q] = col[q] >= 0 ? V.mp_ptr[col[q] + 1] : 0;
+    len[q] = end[q] - base[q];
+    longest = max(longest, len[q]);
+  }
+  // lower bound of frame_local in mp_frame[base, end)
+  while (longest > 0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (len[q] > 0) {
+        const int64_t half = len[q] >> 1;
+        if (V.mp_frame[base[q] + half] < frame_local) {
+          base[q] += half + 1;
+          len[q] -= half + 1;
+        } else {
+          len[q] = half;
+        }
+      }
+    }
+    longest >>= 1;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const bool hit = col[q] >= 0 && base[q] < end[q] && V.mp_frame[base[q]] == frame_local;
+    off[q] = hit ? V.mp_off[base[q]] : -1;
+  }
 }
 
 /// Point rows: AssemblePointRows (lm_solver.cpp:30-61) with HuberWeight
@@ -212,11 +242,7 @@ __global__ void KPointRows(DeviceView V) {
     // instead of searching
     const int64_t n0 = I.node_off + static_cast<int64_t>(ev.h) * I.nx + ev.w;
     int64_t off[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const int col = V.node_col[n0 + (q >> 1) * I.nx + (q & 1)];
-      off[q] = col >= 0 ? PoseOffset(V, col, local) : -1;
-    }
+    PoseOffsets4(V, n0, I.nx, local, off);
     longlong2* po = reinterpret_cast<longlong2*>(V.pt_poff + 4 * k);
     po[0] = make_longlong2(off[0], off[1]);
     po[1] = make_longlong2(off[2], off[3]);
