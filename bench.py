@@ -371,7 +371,7 @@ def run_serve(P, args):
 # KInvertDiagonal) in one LM iteration, from one ncu capture of
 # `profile_run.py floorplan 2` (default schedule); L2 is not flushed inside
 # that capture, so writes that stay in L2 are not counted.
-FACTOR_TRAFFIC_BYTES = {"floorplan": 113.2e6}
+FACTOR_TRAFFIC_BYTES = {"floorplan": 114.5e6}
 
 
 def run_gpu(args, dist, world, rank, local):
@@ -422,6 +422,14 @@ def run_gpu(args, dist, world, rank, local):
     h2d = specs.host_bytes()
     e2e_t = 0.0
     d2h = 0
+    if args.e2e_steps > 0:
+        # one untimed call: the first in a process pays one-time costs (the
+        # caching allocators' first device and pinned blocks for a second
+        # resident problem), as the warm-up steps do for the device loop
+        w2 = P.Problem.from_specs(specs)
+        P.solve(w2, P.SolverOptions(max_iterations=e2e_iters, step_tolerance=0.0, precision=args.precision))
+        w2.state()
+        w2.close()
     for _ in range(args.e2e_steps):
         flusher.sync()
         t0 = time.perf_counter()
@@ -508,7 +516,7 @@ def main():
     ap.add_argument("--workload", default="floorplan", choices=list(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--e2e-iterations", type=int, default=10)
     ap.add_argument("--cpu-iterations", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
