@@ -1538,8 +1538,8 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
     if (sm.count > 0) {
       const int kmax = S.small_max_k[static_cast<size_t>(l)];
       const size_t bytes = FactorFrontSmem(kmax);
-      KFactorFront<<<static_cast<unsigned>(sm.count), S.front_rows, bytes, stream>>>(V, P.small_tasks + 3 * sm.begin,
-                                                                                  P.dvec);
+      KFactorFront<<<static_cast<unsigned>(sm.count), S.small_threads[static_cast<size_t>(l)], bytes, stream>>>(
+          V, P.small_tasks + 3 * sm.begin, P.dvec);
       ++launches;
     }
     for (int t = 0; t < S.level_panels[static_cast<size_t>(l)]; ++t) {

@@ -146,6 +146,7 @@ struct Symbolic {
   std::vector<int32_t> small_tasks;
   std::vector<TaskRange> small_range;        // per level
   std::vector<int32_t> small_max_k;          // per level
+  std::vector<int32_t> small_threads;        // per level: threads per single-kernel block
   // Assembly offsets of J^T J entries into the front buffer, indexed by the
   // global natural column of a node.
   std::vector<int64_t> mm_off;               // 9 stencil slots per column (-1: stored elsewhere)

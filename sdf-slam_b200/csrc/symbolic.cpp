@@ -367,6 +367,7 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   S.panel_index_base.assign(static_cast<size_t>(levels) + 1, 0);
   S.small_range.assign(static_cast<size_t>(levels), {});
   S.small_max_k.assign(static_cast<size_t>(levels), 0);
+  S.small_threads.assign(static_cast<size_t>(levels), S.front_rows);
   S.small_tasks.clear();
   for (int l = 0; l < levels; ++l) {
     int maxp = 0;
@@ -375,7 +376,15 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
     // the level would not fill the GPU (every task repeats the pivot block,
     // so small chunks shorten the level when SMs would otherwise idle).
     int chunk = kFrontRows;
-    for (const int cand : {kFrontRows, 64, 32}) {
+    int threads = kFrontRows;
+    int fronts = 0;
+    for (int q = S.level_begin[static_cast<size_t>(l)]; q < S.level_begin[static_cast<size_t>(l) + 1]; ++q) {
+      fronts += S.sn[static_cast<size_t>(S.level_sn[static_cast<size_t>(q)])].ncols <= small ? 1 : 0;
+    }
+    // more fronts than SMs: blocks of 128 threads (two per SM by registers)
+    // and chunks of 128 rows keep the level in about one wave
+    const bool many = fronts > kFillBlocks && kFrontRows > 128;
+    for (const int cand : {many ? 128 : kFrontRows, 64, 32}) {
       chunk = cand;
       int64_t blocks = 0;
       for (int q = S.level_begin[static_cast<size_t>(l)]; q < S.level_begin[static_cast<size_t>(l) + 1]; ++q) {
@@ -388,6 +397,10 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
         break;
       }
     }
+    if (many) {
+      threads = 128;
+    }
+    S.small_threads[static_cast<size_t>(l)] = threads;
     for (int q = S.level_begin[static_cast<size_t>(l)]; q < S.level_begin[static_cast<size_t>(l) + 1]; ++q) {
       const int sid = S.level_sn[static_cast<size_t>(q)];
       const SupernodeRec& r = S.sn[static_cast<size_t>(sid)];
@@ -1064,6 +1077,7 @@ void Reschedule(Symbolic& S, const Schedule& sched) {
   S.update_range.clear();
   S.small_range.clear();
   S.small_max_k.clear();
+  S.small_threads.clear();
   S.level_panels.clear();
   S.panel_index_base.clear();
   const std::vector<int> height = S.height;
