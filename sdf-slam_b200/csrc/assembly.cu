@@ -387,22 +387,15 @@ __device__ __forceinline__ int FindInstanceByCell(const DeviceView& V, int64_t c
 
 }  // namespace
 
-/// One colour class of cells (cx % 2, cy % 2) = (pass & 1, pass >> 1), listed
-/// in `cells` (every launched warp has a cell): cells of one class share no
-/// node, so each adds its contributions to J^T J and J^T r with plain
-/// read-modify-writes. One warp per cell: the 4x4 map block
+/// One cell of a colour class (cx % 2, cy % 2) = (pass & 1, pass >> 1): cells
+/// of one class share no node, so each adds its contributions to J^T J and
+/// J^T r with plain read-modify-writes. One warp per cell: the 4x4 map block
 /// and the corner gradients are lane-strided sums over the cell's point rows
 /// reduced by a fixed butterfly; the map-pose blocks are segmented sums over
 /// runs of rows of one frame (rows of a cell are sorted, so frames are
 /// contiguous); the cell's Eikonal row (spec at its lower-left node) follows.
 /// Passes run in a fixed order, so every entry is a deterministic sum.
-__global__ void KCellPass(DeviceView V, const int64_t* cells, int64_t count) {
-  const int64_t w = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (w >= count) {
-    return;
-  }
-  const int64_t cell = cells[w];
+__device__ __forceinline__ void CellPassOne(const DeviceView& V, int64_t cell, int lane) {
   const int i = FindInstanceByCell(V, cell);
   const InstDev& I = V.inst[i];
   if (V.active[i] == 0) {
@@ -518,15 +511,28 @@ __global__ void KCellPass(DeviceView V, const int64_t* cells, int64_t count) {
     const bool tail = in && (lane == 31 || p + 1 >= re || fn != f);
     const int fl = f - I.frame_off;
     if (tail && fl >= 1) {
+      // the (up to 12) entries are distinct: all loads first, then the
+      // stores, so their latencies overlap
       const int64_t offs[4] = {cur.o01.x, cur.o01.y, cur.o23.x, cur.o23.y};
+      double old[12];
+#pragma unroll
+      for (int aa = 0; aa < 4; ++aa) {
+        if (col[aa] >= 0 && offs[aa] >= 0) {
+          old[3 * aa] = V.asm_fronts[offs[aa]];
+          old[3 * aa + 1] = V.asm_fronts[offs[aa] + 1];
+          old[3 * aa + 2] = V.asm_fronts[offs[aa] + 2];
+        } else {
+          old[3 * aa] = old[3 * aa + 1] = old[3 * aa + 2] = 0.0;
+        }
+      }
 #pragma unroll
       for (int aa = 0; aa < 4; ++aa) {
         if (col[aa] >= 0) {
           const int64_t off = offs[aa];
           if (off >= 0) {
-            V.asm_fronts[off] += v[3 * aa];
-            V.asm_fronts[off + 1] += v[3 * aa + 1];
-            V.asm_fronts[off + 2] += v[3 * aa + 2];
+            V.asm_fronts[off] = old[3 * aa] + v[3 * aa];
+            V.asm_fronts[off + 1] = old[3 * aa + 1] + v[3 * aa + 1];
+            V.asm_fronts[off + 2] = old[3 * aa + 2] + v[3 * aa + 2];
           } else {
             overflow = true;
           }
@@ -570,24 +576,36 @@ __global__ void KCellPass(DeviceView V, const int64_t* cells, int64_t count) {
     }
   }
   __syncwarp();
-  // the cell's Eikonal row: nodes (cx,cy), (cx+1,cy), (cx,cy+1) = corners 0, 1, 2
-  if (lane == 0 && eik >= 0) {
+  // the cell's Eikonal row: nodes (cx,cy), (cx+1,cy), (cx,cy+1) = corners
+  // 0, 1, 2; lanes 0..5 add the six pairs, lanes 6..8 the three gradient
+  // entries (distinct entries, one per lane)
+  if (eik >= 0 && lane < 9) {
     const double* r = V.eik_rec + static_cast<int64_t>(eik) * kEikRec;
-    const int corner[3] = {0, 1, 2};
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-#pragma unroll
-      for (int b = a; b < 3; ++b) {
-        const int64_t off = PairOffset(V, col, corner[a], corner[b]);
-        if (off >= 0) {
-          V.asm_fronts[off] += r[a] * r[b];
-        }
+    if (lane < 6) {
+      const int a = lane < 3 ? 0 : (lane < 5 ? 1 : 2);
+      const int b = lane < 3 ? lane : (lane < 5 ? lane - 2 : 2);
+      const int64_t off = PairOffset(V, col, a, b);
+      if (off >= 0) {
+        V.asm_fronts[off] += r[a] * r[b];
       }
-      V.rhs[col[corner[a]]] += r[a] * r[3];
+    } else {
+      const int a = lane - 6;
+      V.rhs[col[a]] += r[a] * r[3];
     }
   }
   if (overflow) {
     atomicOr(V.status + i, kStatusPatternOverflow);
+  }
+}
+
+/// Warps walk the pass's cell list with a grid stride (the launch holds as
+/// many blocks as are resident, so no cell waits for a second wave behind a
+/// busy one).
+__global__ void __launch_bounds__(256, 2) KCellPass(DeviceView V, const int64_t* cells, int64_t count) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t w = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; w < count; w += warps) {
+    CellPassOne(V, cells[w], lane);
   }
 }
 

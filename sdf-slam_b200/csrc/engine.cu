@@ -684,10 +684,22 @@ void Engine::LaunchNormal() {
             "front memset");
   CudaCheck(cudaMemsetAsync(rhs_.get(), 0, static_cast<size_t>(n_) * sizeof(double), stream_), "rhs memset");
   if (total_cells_ > 0) {
+    // as many blocks as are resident at once
+    static const int64_t resident = [] {
+      int dev = 0;
+      int sms = 0;
+      int per_sm = 0;
+      CudaCheck(cudaGetDevice(&dev), "device");
+      CudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+      CudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, KCellPass, 256, 0), "occupancy");
+      return static_cast<int64_t>(std::max(1, per_sm)) * sms;
+    }();
     for (int pass = 0; pass < 4; ++pass) {
       const int64_t count = pass_begin_[pass + 1] - pass_begin_[pass];
       if (count > 0) {
-        KCellPass<<<Blocks(count * 32, 256), 256, 0, stream_>>>(V_, pass_cells_.get() + pass_begin_[pass], count);
+        const int64_t blocks = std::min<int64_t>(Blocks(count * 32, 256), resident);
+        KCellPass<<<static_cast<unsigned>(blocks), 256, 0, stream_>>>(V_, pass_cells_.get() + pass_begin_[pass],
+                                                                      count);
       }
     }
   }
