@@ -631,28 +631,51 @@ __global__ void __launch_bounds__(256) KPoseFrames(DeviceView V) {
   }
   const int64_t rb = V.frame_rows_ptr[f];
   const int64_t re = V.frame_rows_ptr[f + 1];
-#pragma unroll 2
-  for (int64_t q = rb + threadIdx.x; q < re; q += blockDim.x) {
-    const int k = V.frame_rows[q];
-    if (V.pt_cell[k] < 0) {
-      continue;
+  // four rows per thread per pass, their loads issued together; a thread's
+  // rows are still added in ascending order
+  const int64_t stride = blockDim.x;
+  for (int64_t q0 = rb + threadIdx.x; q0 < re; q0 += 4 * stride) {
+    int kk[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int64_t q = q0 + u * stride;
+      kk[u] = q < re ? V.frame_rows[q] : -1;
     }
-    const double2* r2 = reinterpret_cast<const double2*>(V.pt_rec + static_cast<int64_t>(k) * kPointRec);
-    const double2 j01 = r2[2];
-    const double2 j2r = r2[3];
-    const double j0 = j01.x;
-    const double j1 = j01.y;
-    const double j2 = j2r.x;
-    const double r = j2r.y;
-    acc[0] = acc[0] + j0 * j0;
-    acc[1] = acc[1] + j1 * j0;
-    acc[2] = acc[2] + j2 * j0;
-    acc[3] = acc[3] + j1 * j1;
-    acc[4] = acc[4] + j2 * j1;
-    acc[5] = acc[5] + j2 * j2;
-    acc[6] = acc[6] + j0 * r;
-    acc[7] = acc[7] + j1 * r;
-    acc[8] = acc[8] + j2 * r;
+    int cellv[4];
+    double2 j01[4];
+    double2 j2r[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (kk[u] >= 0) {
+        const double2* r2 = reinterpret_cast<const double2*>(V.pt_rec + static_cast<int64_t>(kk[u]) * kPointRec);
+        cellv[u] = V.pt_cell[kk[u]];
+        j01[u] = r2[2];
+        j2r[u] = r2[3];
+      } else {
+        cellv[u] = -1;
+        j01[u] = make_double2(0.0, 0.0);
+        j2r[u] = make_double2(0.0, 0.0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (cellv[u] < 0) {
+        continue;
+      }
+      const double j0 = j01[u].x;
+      const double j1 = j01[u].y;
+      const double j2 = j2r[u].x;
+      const double r = j2r[u].y;
+      acc[0] = acc[0] + j0 * j0;
+      acc[1] = acc[1] + j1 * j0;
+      acc[2] = acc[2] + j2 * j0;
+      acc[3] = acc[3] + j1 * j1;
+      acc[4] = acc[4] + j2 * j1;
+      acc[5] = acc[5] + j2 * j2;
+      acc[6] = acc[6] + j0 * r;
+      acc[7] = acc[7] + j1 * r;
+      acc[8] = acc[8] + j2 * r;
+    }
   }
 #pragma unroll
   for (int q = 0; q < 9; ++q) {

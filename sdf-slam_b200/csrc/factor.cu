@@ -145,10 +145,16 @@ __device__ __forceinline__ void ExtendAddStaged(TP* stage, int c, int rows, cons
       dst[u] = ok ? (rel[cc] - c) * rows + (rel[r] - c) : -1;
       val[u] = ok ? U[static_cast<int64_t>(cc) * CF + r] : TC(0);
     }
+    // one child's entries are distinct: all reads, then all writes
+    TP old[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      old[u] = dst[u] >= 0 ? stage[dst[u]] : TP(0);
+    }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       if (dst[u] >= 0) {
-        stage[dst[u]] += static_cast<TP>(val[u]);
+        stage[dst[u]] = old[u] + static_cast<TP>(val[u]);
       }
     }
   }
