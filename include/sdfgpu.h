@@ -131,6 +131,22 @@ int sdfgpu_problem_build(int32_t nx, int32_t ny, double min_x, double min_y, dou
                          const double* relation_sqrt_weight, const sdfgpu_problem_options* options,
                          sdfgpu_problem** out);
 
+/* sdfgpu_problem_build with the point specs (scan rows, then hallucinated
+ * rows, frame by frame; src/core/hallucination.cpp:5-28), the active-region
+ * maps (problem.cpp:39-70) and the Eikonal spec list (problem.cpp:79-94)
+ * computed by CUDA kernels on the current device; the per-node normals are
+ * still the host's k-NN PCA (normals.cpp:70-220). The resulting problem is
+ * the one sdfgpu_problem_build returns, bit for bit. Fails with
+ * SDFGPU_ERR_CUDA when no device is usable. */
+int sdfgpu_problem_build_device(int32_t nx, int32_t ny, double min_x, double min_y, double max_x,
+                                double max_y, const double* map_values, int32_t num_frames,
+                                const double* poses, const int32_t* scan_offsets,
+                                const double* scan_xy, const double* odometry,
+                                int32_t num_odometry, int32_t num_relations,
+                                const int32_t* relation_ij, const double* relation_meas,
+                                const double* relation_sqrt_weight,
+                                const sdfgpu_problem_options* options, sdfgpu_problem** out);
+
 /* Copies a problem given by its spec arrays (the drop-in path: the caller's
  * own Problem is marshalled into a desc). Validation and spec queries run on
  * the host; the first call that needs the GPU (cost, step, solve, state,

@@ -210,12 +210,14 @@ class Problem:
     """The joint SLAM problem on the device (Problem, problem.hpp:92-161).
 
     ``Problem(grid, poses, scans, odometry, options, relations)`` builds the
-    specs like the reference constructor; ``Problem.from_specs`` uploads an
+    specs like the reference constructor (``on_device=True``: the point rows,
+    active maps and Eikonal spec list by CUDA kernels, with the same
+    result); ``Problem.from_specs`` uploads an
     existing problem's spec arrays; ``Problem.batch`` uploads several
     independent problems that are solved together."""
 
     def __init__(self, nx, ny, min_corner, max_corner, poses, scans, odometry=(), options=None,
-                 relations=(), map_values=None, _handle=None):
+                 relations=(), map_values=None, _handle=None, on_device=False):
         L = lib()
         if _handle is not None:
             self._h = _handle
@@ -236,7 +238,8 @@ class Problem:
         mv = None if map_values is None else np.ascontiguousarray(map_values, np.float64)
         opts = options.to_c()
         h = ctypes.c_void_p()
-        _check(L.sdfgpu_problem_build(
+        build = L.sdfgpu_problem_build_device if on_device else L.sdfgpu_problem_build
+        _check(build(
             int(nx), int(ny), float(min_corner[0]), float(min_corner[1]), float(max_corner[0]),
             float(max_corner[1]), _d(mv) if mv is not None else None, len(poses), _d(poses),
             _i(offsets), _d(xy), _d(odo) if len(odo) else None, len(odo), len(rel_ij),
@@ -245,13 +248,13 @@ class Problem:
         self._h = h
 
     @classmethod
-    def from_scene(cls, scene, options: ProblemOptions | None = None):
+    def from_scene(cls, scene, options: ProblemOptions | None = None, on_device: bool = False):
         opts = options or ProblemOptions()
         for k, v in scene.options.items():
             if k != "active_region" or options is None:
                 setattr(opts, k, v)
         return cls(scene.nx, scene.ny, scene.min_corner, scene.max_corner, scene.poses, scene.scans,
-                   scene.odometry, opts)
+                   scene.odometry, opts, on_device=on_device)
 
     @classmethod
     def from_specs(cls, specs: Specs):

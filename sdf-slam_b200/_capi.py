@@ -87,6 +87,11 @@ SIGNATURES = {
         ctypes.c_double, c_dbl_p, ctypes.c_int32, c_dbl_p, c_int_p, c_dbl_p, c_dbl_p,
         ctypes.c_int32, ctypes.c_int32, c_int_p, c_dbl_p, c_dbl_p,
         ctypes.POINTER(ProblemOptionsC), ctypes.POINTER(vp)]),
+    "sdfgpu_problem_build_device": (ctypes.c_int, [
+        ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+        ctypes.c_double, c_dbl_p, ctypes.c_int32, c_dbl_p, c_int_p, c_dbl_p, c_dbl_p,
+        ctypes.c_int32, ctypes.c_int32, c_int_p, c_dbl_p, c_dbl_p,
+        ctypes.POINTER(ProblemOptionsC), ctypes.POINTER(vp)]),
     "sdfgpu_problem_create": (ctypes.c_int, [ctypes.POINTER(ProblemDesc), ctypes.POINTER(vp)]),
     "sdfgpu_problem_create_batch": (ctypes.c_int, [ctypes.POINTER(ProblemDesc), ctypes.c_int32,
                                                    ctypes.POINTER(vp)]),

@@ -30,6 +30,7 @@ SOURCES = {
     "ldlt.cu": [],
     "noalloc.cu": [],
     "refine.cu": [],
+    "problem_device.cu": [],
     "problem_build.cpp": ["-x", "cu"],
     "alloc.cpp": ["-x", "cu"],
     "host_pool.cpp": ["-x", "cu"],

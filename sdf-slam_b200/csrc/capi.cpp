@@ -138,12 +138,14 @@ void sdfgpu_solver_options_default(sdfgpu_solver_options* o) {
   o->refine_steps = 3;
 }
 
-int sdfgpu_problem_build(int32_t nx, int32_t ny, double min_x, double min_y, double max_x, double max_y,
-                         const double* map_values, int32_t num_frames, const double* poses,
-                         const int32_t* scan_offsets, const double* scan_xy, const double* odometry,
-                         int32_t num_odometry, int32_t num_relations, const int32_t* relation_ij,
-                         const double* relation_meas, const double* relation_sqrt_weight,
-                         const sdfgpu_problem_options* options, sdfgpu_problem** out) {
+// sdfgpu_problem_build and sdfgpu_problem_build_device (on_device: the point
+// specs, active maps and Eikonal spec list by CUDA kernels).
+static int BuildProblemHandle(bool on_device, int32_t nx, int32_t ny, double min_x, double min_y, double max_x,
+                              double max_y, const double* map_values, int32_t num_frames, const double* poses,
+                              const int32_t* scan_offsets, const double* scan_xy, const double* odometry,
+                              int32_t num_odometry, int32_t num_relations, const int32_t* relation_ij,
+                              const double* relation_meas, const double* relation_sqrt_weight,
+                              const sdfgpu_problem_options* options, sdfgpu_problem** out) {
   return Guard([&] {
     NeedHandle(out, "out");
     *out = nullptr;
@@ -162,11 +164,33 @@ int sdfgpu_problem_build(int32_t nx, int32_t ny, double min_x, double min_y, dou
     std::vector<sdfgpu::HostProblem> v;
     v.push_back(sdfgpu::BuildProblem(nx, ny, min_x, min_y, max_x, max_y, map_values, num_frames, poses,
                                      scan_offsets, scan_xy, odometry, num_odometry, num_relations, relation_ij,
-                                     relation_meas, relation_sqrt_weight, o));
+                                     relation_meas, relation_sqrt_weight, o, on_device));
     auto h = std::make_unique<sdfgpu_problem>();
     h->host = std::move(v);
     *out = h.release();
   });
+}
+
+int sdfgpu_problem_build(int32_t nx, int32_t ny, double min_x, double min_y, double max_x, double max_y,
+                         const double* map_values, int32_t num_frames, const double* poses,
+                         const int32_t* scan_offsets, const double* scan_xy, const double* odometry,
+                         int32_t num_odometry, int32_t num_relations, const int32_t* relation_ij,
+                         const double* relation_meas, const double* relation_sqrt_weight,
+                         const sdfgpu_problem_options* options, sdfgpu_problem** out) {
+  return BuildProblemHandle(false, nx, ny, min_x, min_y, max_x, max_y, map_values, num_frames, poses, scan_offsets,
+                            scan_xy, odometry, num_odometry, num_relations, relation_ij, relation_meas,
+                            relation_sqrt_weight, options, out);
+}
+
+int sdfgpu_problem_build_device(int32_t nx, int32_t ny, double min_x, double min_y, double max_x, double max_y,
+                                const double* map_values, int32_t num_frames, const double* poses,
+                                const int32_t* scan_offsets, const double* scan_xy, const double* odometry,
+                                int32_t num_odometry, int32_t num_relations, const int32_t* relation_ij,
+                                const double* relation_meas, const double* relation_sqrt_weight,
+                                const sdfgpu_problem_options* options, sdfgpu_problem** out) {
+  return BuildProblemHandle(true, nx, ny, min_x, min_y, max_x, max_y, map_values, num_frames, poses, scan_offsets,
+                            scan_xy, odometry, num_odometry, num_relations, relation_ij, relation_meas,
+                            relation_sqrt_weight, options, out);
 }
 
 int sdfgpu_problem_create(const sdfgpu_problem_desc* desc, sdfgpu_problem** out) {

@@ -71,7 +71,18 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
                          const int32_t* scan_offsets, const double* scan_xy,
                          const double* odometry, int num_odometry, int num_relations,
                          const int32_t* relation_ij, const double* relation_meas,
-                         const double* relation_sqrt_weight, const sdfgpu_problem_options& options);
+                         const double* relation_sqrt_weight, const sdfgpu_problem_options& options,
+                         bool device_stages = false);
+
+/// The device stages of BuildProblem (device_stages = true): the point specs
+/// (scan rows, then hallucinated rows, frame by frame), the active-region
+/// maps and the Eikonal spec list, computed by CUDA kernels on the current
+/// device from the scans, the poses and the host's per-node normals
+/// (node_normal: 2 values per node) and scales, then copied into hp. Same
+/// values, bit for bit, as the host stages.
+void DeviceBuildSpecs(HostProblem& hp, int num_frames, const int32_t* scan_offsets, const double* scan_xy,
+                      const std::vector<double>& node_normal, const std::vector<double>& node_scale,
+                      const sdfgpu_problem_options& options);
 
 // ------------------------------------------------------------- symbolic --
 

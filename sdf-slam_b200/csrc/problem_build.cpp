@@ -332,7 +332,8 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
                          const int32_t* scan_offsets, const double* scan_xy,
                          const double* odometry, int num_odometry, int num_relations,
                          const int32_t* relation_ij, const double* relation_meas,
-                         const double* relation_sqrt_weight, const sdfgpu_problem_options& o) {
+                         const double* relation_sqrt_weight, const sdfgpu_problem_options& o,
+                         bool device_stages) {
   auto bad = [](const std::string& m) { Fail(SDFGPU_ERR_INVALID_ARGUMENT, m); };
   if (nx < 2 || ny < 2 || !(max_x > min_x) || !(max_y > min_y)) {
     bad("GridMap needs nx, ny >= 2 and max > min");
@@ -360,6 +361,12 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
   hp.smooth_gradient = o.smooth_gradient != 0;
   hp.smooth_gradient_step = o.smooth_gradient_step;
 
+  for (int f = 0; f < num_frames; ++f) {
+    if (scan_offsets[f + 1] < scan_offsets[f]) {
+      bad("scan offsets must not decrease");
+    }
+  }
+  if (!device_stages) {
   // Point specs (problem.cpp:26-37) with hallucinated points
   // (hallucination.cpp:5-28): toward = (-p / |p|) * step; interleaved
   // p + toward*j (expected +step*j) and p - toward*j (expected -step*j).
@@ -371,9 +378,6 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
   for (int f = 0; f < num_frames; ++f) {
     const int b = scan_offsets[f];
     const int e = scan_offsets[f + 1];
-    if (e < b) {
-      bad("scan offsets must not decrease");
-    }
     for (int q = b; q < e; ++q) {
       hp.pt_frame.push_back(f);
       hp.pt_xy.push_back(scan_xy[2 * q]);
@@ -435,6 +439,7 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
       hp.active_to_node.push_back(static_cast<int32_t>(node));
     }
   }
+  }  // host point specs and active maps
 
   // Scan normals over the union of all scans at the current poses, or per
   // scan in the sensor frame (normals.cpp:102-160).
@@ -521,6 +526,15 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
       }
     }
   }
+  if (device_stages) {
+    // point specs, active maps and the Eikonal spec list by CUDA kernels
+    std::vector<double> nn(2 * nodes);
+    for (size_t q = 0; q < nodes; ++q) {
+      nn[2 * q] = node_normal[q].x;
+      nn[2 * q + 1] = node_normal[q].y;
+    }
+    DeviceBuildSpecs(hp, num_frames, scan_offsets, scan_xy, nn, node_scale, o);
+  } else {
   const double sqrt_we = std::sqrt(o.weight_eikonal);
   for (int h = 0; h + 1 < ny; ++h) {
     for (int w = 0; w + 1 < nx; ++w) {
@@ -539,6 +553,7 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
       hp.eik_sqrtw.push_back(sqrt_we * std::sqrt(scale));
     }
   }
+  }  // host Eikonal specs
 
   // Odometry and relation specs (problem.cpp:96-114).
   const double sqrt_wo = std::sqrt(o.weight_odometry);
