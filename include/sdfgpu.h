@@ -133,11 +133,13 @@ int sdfgpu_problem_build(int32_t nx, int32_t ny, double min_x, double min_y, dou
 
 /* sdfgpu_problem_build with the point specs (scan rows, then hallucinated
  * rows, frame by frame; src/core/hallucination.cpp:5-28), the active-region
- * maps (problem.cpp:39-70) and the Eikonal spec list (problem.cpp:79-94)
- * computed by CUDA kernels on the current device; the per-node normals are
- * still the host's k-NN PCA (normals.cpp:70-220). The resulting problem is
- * the one sdfgpu_problem_build returns, bit for bit. Fails with
- * SDFGPU_ERR_CUDA when no device is usable. */
+ * maps (problem.cpp:39-70), the k-NN PCA scan normals and per-node normals
+ * (normals.cpp:70-220) and the Eikonal spec list (problem.cpp:79-94)
+ * computed by CUDA kernels on the current device (the k-NN bucket grids are
+ * built on the host). The resulting problem is the one sdfgpu_problem_build
+ * returns, bit for bit. Fails with SDFGPU_ERR_CUDA when no device is usable
+ * and with SDFGPU_ERR_INVALID_ARGUMENT for normals.k_neighbors above 64 or
+ * non-finite poses or scan points. */
 int sdfgpu_problem_build_device(int32_t nx, int32_t ny, double min_x, double min_y, double max_x,
                                 double max_y, const double* map_values, int32_t num_frames,
                                 const double* poses, const int32_t* scan_offsets,

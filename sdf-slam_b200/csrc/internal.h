@@ -74,14 +74,41 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
                          const double* relation_sqrt_weight, const sdfgpu_problem_options& options,
                          bool device_stages = false);
 
+/// A bucket grid over a point set for exact k-nearest-neighbour search: the
+/// bucket of a point is its clamped cell (floor((p - origin) / cell) per
+/// axis, row-major over gx * gy); start holds gx * gy + 1 offsets into items,
+/// the point indices bucket by bucket.
+struct KnnBuckets {
+  double ox{0.0};
+  double oy{0.0};
+  double cell{1.0};
+  int gx{1};
+  int gy{1};
+  std::vector<int> start;
+  std::vector<int> items;
+};
+
+/// The host part of the on-device normals (src/core/normals.cpp:102-220):
+/// every scan point in world coordinates at its frame's pose (2 values per
+/// point, frame by frame), the bucket grid over those world points (for the
+/// per-node nearest point, and for the scan normals unless per_scan), and
+/// with per_scan one grid per frame over its sensor-frame points. The
+/// grids are the host builder's, so a device search over them finds the
+/// host's neighbours in the host's order.
+struct NormalGrids {
+  std::vector<double> world;
+  KnnBuckets world_grid;
+  std::vector<KnnBuckets> frame_grids;
+};
+void PrepareNormalGrids(const HostProblem& hp, int num_frames, const int32_t* scan_offsets, const double* scan_xy,
+                        bool per_scan, NormalGrids* out);
+
 /// The device stages of BuildProblem (device_stages = true): the point specs
 /// (scan rows, then hallucinated rows, frame by frame), the active-region
-/// maps and the Eikonal spec list, computed by CUDA kernels on the current
-/// device from the scans, the poses and the host's per-node normals
-/// (node_normal: 2 values per node) and scales, then copied into hp. Same
-/// values, bit for bit, as the host stages.
+/// maps, the scan-point and per-node normals and the Eikonal spec list,
+/// computed by CUDA kernels on the current device from the scans and the
+/// poses, then copied into hp. Same values, bit for bit, as the host stages.
 void DeviceBuildSpecs(HostProblem& hp, int num_frames, const int32_t* scan_offsets, const double* scan_xy,
-                      const std::vector<double>& node_normal, const std::vector<double>& node_scale,
                       const sdfgpu_problem_options& options);
 
 // ------------------------------------------------------------- symbolic --

@@ -85,14 +85,25 @@ class BucketKnn {
     }
   }
 
+  /// The grid's parameters and arrays (for the device search).
+  void Export(KnnBuckets* b) const {
+    b->ox = ox_;
+    b->oy = oy_;
+    b->cell = cell_;
+    b->gx = gx_;
+    b->gy = gy_;
+    b->start = start_;
+    b->items = items_;
+  }
+
   void Query(P2 q, size_t k, std::vector<std::pair<double, int>>& out) const {
     out.clear();
     if (pts_.empty() || k == 0) {
       return;
     }
     const size_t want = std::min(k, pts_.size());
-    const int cx = std::clamp(static_cast<int>((q.x - ox_) / cell_), 0, gx_ - 1);
-    const int cy = std::clamp(static_cast<int>((q.y - oy_) / cell_), 0, gy_ - 1);
+    const int cx = CellOf((q.x - ox_) / cell_, gx_);
+    const int cy = CellOf((q.y - oy_) / cell_, gy_);
     const double bx0 = ox_ + cx * cell_;
     const double by0 = oy_ + cy * cell_;
     const double inner = std::max(0.0, std::min({q.x - bx0, bx0 + cell_ - q.x, q.y - by0, by0 + cell_ - q.y}));
@@ -138,11 +149,18 @@ class BucketKnn {
   }
 
  private:
-  int Bucket(P2 p) const {
-    const int x = std::clamp(static_cast<int>((p.x - ox_) / cell_), 0, gx_ - 1);
-    const int y = std::clamp(static_cast<int>((p.y - oy_) / cell_), 0, gy_ - 1);
-    return y * gx_ + x;
+  /// floor(f) clamped to [0, g - 1]; NaN goes to 0. (The comparisons come
+  /// first so that no out-of-range value is converted.)
+  static int CellOf(double f, int g) {
+    if (!(f > 0.0)) {
+      return 0;
+    }
+    if (f >= static_cast<double>(g - 1)) {
+      return g - 1;
+    }
+    return static_cast<int>(f);
   }
+  int Bucket(P2 p) const { return CellOf((p.y - oy_) / cell_, gy_) * gx_ + CellOf((p.x - ox_) / cell_, gx_); }
   const std::vector<P2>& pts_;
   double ox_{0.0};
   double oy_{0.0};
@@ -327,6 +345,141 @@ HostProblem FromDesc(const sdfgpu_problem_desc& d) {
   return hp;
 }
 
+namespace {
+
+/// Scan-point normals and per-node normals and Eikonal scales (two values
+/// and one per node, row-major) on the host.
+void HostNodeNormals(const HostProblem& hp, int num_frames, const int32_t* scan_offsets, const double* scan_xy,
+                     const sdfgpu_problem_options& o, std::vector<double>& node_normal_out,
+                     std::vector<double>& node_scale_out) {
+  auto bad = [](const std::string& m) { Fail(SDFGPU_ERR_INVALID_ARGUMENT, m); };
+  const int nx = hp.nx;
+  const int ny = hp.ny;
+  const double min_x = hp.min_x;
+  const double min_y = hp.min_y;
+  const size_t nodes = static_cast<size_t>(nx) * static_cast<size_t>(ny);
+  // Scan normals over the union of all scans at the current poses, or per
+  // scan in the sensor frame (normals.cpp:102-160).
+  const size_t k = static_cast<size_t>(std::max(2, o.normals_k_neighbors));
+  std::vector<P2> spts;
+  std::vector<P2> snorm;
+  std::vector<double> scorner;
+  std::vector<std::pair<double, int>> nb;
+  if (o.normals_per_scan != 0) {
+    for (int f = 0; f < num_frames; ++f) {
+      std::vector<P2> local;
+      for (int q = scan_offsets[f]; q < scan_offsets[f + 1]; ++q) {
+        local.push_back({scan_xy[2 * q], scan_xy[2 * q + 1]});
+      }
+      const BucketKnn knn(local);
+      const double* pose = &hp.poses[3 * static_cast<size_t>(f)];
+      const double c = std::cos(pose[2]);
+      const double s = std::sin(pose[2]);
+      for (size_t i = 0; i < local.size(); ++i) {
+        P2 n{};
+        double corner = 0.0;
+        PcaNormal(local, knn, i, std::min(k, local.size()), {0.0, 0.0}, &n, &corner, nb);
+        spts.push_back(ApplyPose(pose, local[i]));
+        snorm.push_back({c * n.x + (-s) * n.y, s * n.x + c * n.y});
+        scorner.push_back(corner);
+      }
+    }
+  } else {
+    std::vector<P2> origins;
+    for (int f = 0; f < num_frames; ++f) {
+      const double* pose = &hp.poses[3 * static_cast<size_t>(f)];
+      for (int q = scan_offsets[f]; q < scan_offsets[f + 1]; ++q) {
+        spts.push_back(ApplyPose(pose, {scan_xy[2 * q], scan_xy[2 * q + 1]}));
+        origins.push_back({pose[0], pose[1]});
+      }
+    }
+    snorm.resize(spts.size());
+    scorner.resize(spts.size());
+    if (!spts.empty()) {
+      const BucketKnn knn(spts);
+      for (size_t i = 0; i < spts.size(); ++i) {
+        PcaNormal(spts, knn, i, std::min(k, spts.size()), origins[i], &snorm[i], &scorner[i], nb);
+      }
+    }
+  }
+
+  // Node normals (normals.cpp:162-220).
+  std::vector<P2> node_normal(nodes, P2{0.0, 0.0});
+  std::vector<double> node_scale(nodes, 1.0);
+  if (!spts.empty()) {
+    const BucketKnn knn(spts);
+    const double dxg = hp.dx();
+    const double dyg = hp.dy();
+    for (int h = 0; h < ny; ++h) {
+      for (int w = 0; w < nx; ++w) {
+        const P2 node{min_x + w * dxg, min_y + h * dyg};
+        knn.Query(node, 1, nb);
+        const size_t nearest = static_cast<size_t>(nb[0].second);
+        const P2 npca = snorm[nearest];
+        const double corner = std::clamp(scorner[nearest] / o.normals_corner_threshold, 0.0, 1.0);
+        const size_t id = static_cast<size_t>(h) * nx + w;
+        if (o.normals_method == 0) {
+          node_normal[id] = npca;
+        } else if (o.normals_method == 1) {
+          const P2 ts{spts[nearest].x - node.x, spts[nearest].y - node.y};
+          const double tn = std::sqrt(ts.x * ts.x + ts.y * ts.y);
+          if (tn < 1e-9) {
+            node_normal[id] = npca;
+          } else {
+            P2 cue{ts.x / tn, ts.y / tn};
+            if (cue.x * npca.x + cue.y * npca.y < 0.0) {
+              cue = {-cue.x, -cue.y};
+            }
+            const P2 bl{(1.0 - corner) * npca.x + corner * cue.x, (1.0 - corner) * npca.y + corner * cue.y};
+            const double bn = std::sqrt(bl.x * bl.x + bl.y * bl.y);
+            node_normal[id] = bn > 1e-9 ? P2{bl.x / bn, bl.y / bn} : npca;
+          }
+        } else if (o.normals_method == 2) {
+          node_normal[id] = npca;
+          node_scale[id] = 1.0 - corner;
+        } else {
+          bad("unknown normals.method");
+        }
+      }
+    }
+  }
+  node_normal_out.resize(2 * nodes);
+  for (size_t q = 0; q < nodes; ++q) {
+    node_normal_out[2 * q] = node_normal[q].x;
+    node_normal_out[2 * q + 1] = node_normal[q].y;
+  }
+  node_scale_out = std::move(node_scale);
+}
+
+}  // namespace
+
+void PrepareNormalGrids(const HostProblem& hp, int num_frames, const int32_t* scan_offsets, const double* scan_xy,
+                        bool per_scan, NormalGrids* out) {
+  std::vector<P2> world;
+  world.reserve(static_cast<size_t>(scan_offsets[num_frames]));
+  out->frame_grids.clear();
+  std::vector<P2> local;
+  for (int f = 0; f < num_frames; ++f) {
+    const double* pose = &hp.poses[3 * static_cast<size_t>(f)];
+    const double c = std::cos(pose[2]);  // ApplyPose with the frame's cos and sin taken once
+    const double sn = std::sin(pose[2]);
+    local.clear();
+    for (int q = scan_offsets[f]; q < scan_offsets[f + 1]; ++q) {
+      const P2 p{scan_xy[2 * q], scan_xy[2 * q + 1]};
+      local.push_back(p);
+      world.push_back({(c * p.x + (-sn) * p.y) + pose[0], (sn * p.x + c * p.y) + pose[1]});
+    }
+    if (per_scan) {
+      out->frame_grids.emplace_back();
+      BucketKnn(local).Export(&out->frame_grids.back());
+    }
+  }
+  BucketKnn(world).Export(&out->world_grid);
+  out->world.resize(2 * world.size());
+  static_assert(sizeof(P2) == 2 * sizeof(double));
+  std::memcpy(out->world.data(), world.data(), world.size() * sizeof(P2));
+}
+
 HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_x, double max_y,
                          const double* map_values, int num_frames, const double* poses,
                          const int32_t* scan_offsets, const double* scan_xy,
@@ -441,99 +594,15 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
   }
   }  // host point specs and active maps
 
-  // Scan normals over the union of all scans at the current poses, or per
-  // scan in the sensor frame (normals.cpp:102-160).
-  const size_t k = static_cast<size_t>(std::max(2, o.normals_k_neighbors));
-  std::vector<P2> spts;
-  std::vector<P2> snorm;
-  std::vector<double> scorner;
-  std::vector<std::pair<double, int>> nb;
-  if (o.normals_per_scan != 0) {
-    for (int f = 0; f < num_frames; ++f) {
-      std::vector<P2> local;
-      for (int q = scan_offsets[f]; q < scan_offsets[f + 1]; ++q) {
-        local.push_back({scan_xy[2 * q], scan_xy[2 * q + 1]});
-      }
-      const BucketKnn knn(local);
-      const double* pose = &hp.poses[3 * static_cast<size_t>(f)];
-      const double c = std::cos(pose[2]);
-      const double s = std::sin(pose[2]);
-      for (size_t i = 0; i < local.size(); ++i) {
-        P2 n{};
-        double corner = 0.0;
-        PcaNormal(local, knn, i, std::min(k, local.size()), {0.0, 0.0}, &n, &corner, nb);
-        spts.push_back(ApplyPose(pose, local[i]));
-        snorm.push_back({c * n.x + (-s) * n.y, s * n.x + c * n.y});
-        scorner.push_back(corner);
-      }
-    }
-  } else {
-    std::vector<P2> origins;
-    for (int f = 0; f < num_frames; ++f) {
-      const double* pose = &hp.poses[3 * static_cast<size_t>(f)];
-      for (int q = scan_offsets[f]; q < scan_offsets[f + 1]; ++q) {
-        spts.push_back(ApplyPose(pose, {scan_xy[2 * q], scan_xy[2 * q + 1]}));
-        origins.push_back({pose[0], pose[1]});
-      }
-    }
-    snorm.resize(spts.size());
-    scorner.resize(spts.size());
-    if (!spts.empty()) {
-      const BucketKnn knn(spts);
-      for (size_t i = 0; i < spts.size(); ++i) {
-        PcaNormal(spts, knn, i, std::min(k, spts.size()), origins[i], &snorm[i], &scorner[i], nb);
-      }
-    }
-  }
-
-  // Node normals (normals.cpp:162-220) and Eikonal specs (problem.cpp:79-94).
-  std::vector<P2> node_normal(nodes, P2{0.0, 0.0});
-  std::vector<double> node_scale(nodes, 1.0);
-  if (!spts.empty()) {
-    const BucketKnn knn(spts);
-    const double dxg = hp.dx();
-    const double dyg = hp.dy();
-    for (int h = 0; h < ny; ++h) {
-      for (int w = 0; w < nx; ++w) {
-        const P2 node{min_x + w * dxg, min_y + h * dyg};
-        knn.Query(node, 1, nb);
-        const size_t nearest = static_cast<size_t>(nb[0].second);
-        const P2 npca = snorm[nearest];
-        const double corner = std::clamp(scorner[nearest] / o.normals_corner_threshold, 0.0, 1.0);
-        const size_t id = static_cast<size_t>(h) * nx + w;
-        if (o.normals_method == 0) {
-          node_normal[id] = npca;
-        } else if (o.normals_method == 1) {
-          const P2 ts{spts[nearest].x - node.x, spts[nearest].y - node.y};
-          const double tn = std::sqrt(ts.x * ts.x + ts.y * ts.y);
-          if (tn < 1e-9) {
-            node_normal[id] = npca;
-          } else {
-            P2 cue{ts.x / tn, ts.y / tn};
-            if (cue.x * npca.x + cue.y * npca.y < 0.0) {
-              cue = {-cue.x, -cue.y};
-            }
-            const P2 bl{(1.0 - corner) * npca.x + corner * cue.x, (1.0 - corner) * npca.y + corner * cue.y};
-            const double bn = std::sqrt(bl.x * bl.x + bl.y * bl.y);
-            node_normal[id] = bn > 1e-9 ? P2{bl.x / bn, bl.y / bn} : npca;
-          }
-        } else if (o.normals_method == 2) {
-          node_normal[id] = npca;
-          node_scale[id] = 1.0 - corner;
-        } else {
-          bad("unknown normals.method");
-        }
-      }
-    }
+  std::vector<double> node_normal;
+  std::vector<double> node_scale;
+  if (!device_stages) {
+    HostNodeNormals(hp, num_frames, scan_offsets, scan_xy, o, node_normal, node_scale);
   }
   if (device_stages) {
-    // point specs, active maps and the Eikonal spec list by CUDA kernels
-    std::vector<double> nn(2 * nodes);
-    for (size_t q = 0; q < nodes; ++q) {
-      nn[2 * q] = node_normal[q].x;
-      nn[2 * q + 1] = node_normal[q].y;
-    }
-    DeviceBuildSpecs(hp, num_frames, scan_offsets, scan_xy, nn, node_scale, o);
+    // point specs, active maps, node normals and the Eikonal spec list by
+    // CUDA kernels
+    DeviceBuildSpecs(hp, num_frames, scan_offsets, scan_xy, o);
   } else {
   const double sqrt_we = std::sqrt(o.weight_eikonal);
   for (int h = 0; h + 1 < ny; ++h) {
@@ -548,8 +617,8 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
       }
       hp.eik_wh.push_back(w);
       hp.eik_wh.push_back(h);
-      hp.eik_n.push_back(node_normal[id].x);
-      hp.eik_n.push_back(node_normal[id].y);
+      hp.eik_n.push_back(node_normal[2 * id]);
+      hp.eik_n.push_back(node_normal[2 * id + 1]);
       hp.eik_sqrtw.push_back(sqrt_we * std::sqrt(scale));
     }
   }
