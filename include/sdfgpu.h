@@ -273,6 +273,62 @@ int sdfgpu_last_profile(sdfgpu_problem* problem, double* phases);
 int sdfgpu_autotune(sdfgpu_problem* problem, int32_t* schedule, double* factor_ms, double* trials,
                     int32_t max_trials, int32_t* num_trials);
 
+/* ----------------------------------------------------------- incremental --
+ * Run in incremental mode (src/pipeline/runner.cpp:226-285, without its file
+ * output): the dataset's odometry is poses[i].RelativeTo(poses[i + 1]); frame
+ * 0 starts at its dataset pose; each step appends increment_size frames,
+ * composing each new pose from the previous one and the odometry, rebuilds
+ * the problem over the frames so far from the current map and poses (as
+ * sdfgpu_problem_build, or sdfgpu_problem_build_device when build_on_device
+ * is set) and runs SolveLm with max_iterations = iterations_per_increment.
+ * The step results are summed as the runner does: the first step's initial
+ * cost, the last step's final cost and convergence, the iterations and
+ * durations summed, the cost histories concatenated. With warm_analysis set,
+ * the next step's symbolic analysis runs on a host thread during the
+ * current step's GPU iterations, from the poses the step started with; the
+ * iterations re-analyse if the solved poses leave that pattern. */
+typedef void (*sdfgpu_snapshot_fn)(void* user, int32_t num_frames, const double* map_values,
+                                   const double* poses);
+
+typedef struct sdfgpu_incremental_desc {
+  int32_t nx;
+  int32_t ny;
+  double min_x;
+  double min_y;
+  double max_x;
+  double max_y;
+  const double* map_values;      /* nx * ny initial SDF values, NULL: zeros */
+  int32_t num_frames;            /* >= 2 */
+  const double* poses;           /* dataset poses, 3 per frame */
+  const int32_t* scan_offsets;   /* num_frames + 1 */
+  const double* scan_xy;         /* sensor-frame points, 2 per point */
+  int32_t num_relations;
+  const int32_t* relation_ij;
+  const double* relation_meas;
+  const double* relation_sqrt_weight; /* NULL: 1 */
+  int32_t increment_size;        /* frames appended per step, >= 1 */
+  int32_t iterations_per_increment;
+  int32_t snapshot_every;        /* call snapshot every N steps and after the last; 0: never */
+  sdfgpu_snapshot_fn snapshot;   /* may be NULL */
+  void* snapshot_user;
+  int32_t build_on_device;
+  int32_t warm_analysis;
+} sdfgpu_incremental_desc;
+
+/* Runs the incremental driver on the current device. map_out (nx * ny) and
+ * poses_out (3 * num_frames) receive the final state, total the summed
+ * result; cost_history (may be NULL) receives the first `capacity` entries
+ * of the concatenated histories (total->cost_history_length of them).
+ * phases (8 doubles, may be NULL): host seconds spent building problems,
+ * waiting for overlapped analyses, setting engines up, iterating and reading
+ * state back, the run's wall time, the number of steps and the number of
+ * steps whose analysis overlapped the previous step. Fails with the step's
+ * status (SDFGPU_ERR_NUMERICAL for a failed factorization) and stops there. */
+int sdfgpu_run_incremental(const sdfgpu_incremental_desc* desc, const sdfgpu_problem_options* problem_options,
+                           const sdfgpu_solver_options* solver_options, double* map_out, double* poses_out,
+                           sdfgpu_solve_result* total, double* cost_history, int32_t capacity,
+                           double* phases);
+
 /* ------------------------------------------------------------ factor only --
  * LinearSolver::kGpu: ParallelSimplicialLdlt's interface
  * (src/solvers/parallel_ldlt.hpp:38-51 and Eigen's solve) for any symmetric

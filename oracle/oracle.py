@@ -307,6 +307,43 @@ class OracleProblem:
                     cost_history=hist[: ri[2]].copy())
 
 
+def run_incremental(nx, ny, min_corner, max_corner, poses, scans, options, relations=(),
+                    map_values=None, increment_size=1, iterations_per_increment=10,
+                    solver=None, num_threads=0):
+    """Run in incremental mode (src/pipeline/runner.cpp:226-285) on the
+    oracle: odometry = RelativeTo of consecutive dataset poses (:52-59); each
+    step appends frames composed from the last optimized pose, rebuilds the
+    Problem over the frames so far from the current map and poses (:247-258)
+    and solves it for iterations_per_increment iterations (:259), summing the
+    step results as :264-272 do. Returns (map, poses, summed result dict)."""
+    poses = np.asarray(poses, dtype=np.float64).reshape(-1, 3)
+    F = len(poses)
+    odometry = [pose_op(2, poses[i], poses[i + 1]) for i in range(F - 1)]
+    m = np.zeros(nx * ny) if map_values is None else np.asarray(map_values, np.float64).reshape(-1).copy()
+    est = [poses[0].copy()]
+    solver = dict(solver or {})
+    solver["max_iterations"] = iterations_per_increment
+    total = dict(converged=False, iterations=0, initial_cost=-1.0, final_cost=0.0, cost_history=[])
+    next_frame = 1
+    while next_frame < F:
+        last = min(F, next_frame + increment_size)
+        for i in range(next_frame, last):
+            est.append(pose_op(1, est[-1], odometry[i - 1]))
+        next_frame = last
+        prob = OracleProblem.build(nx, ny, min_corner, max_corner, np.array(est), scans[:next_frame],
+                                   np.array(odometry[: next_frame - 1]), options, relations, m)
+        r = prob.solve(num_threads=num_threads, **solver)
+        m, p = prob.state()
+        est = [row.copy() for row in p]
+        if total["initial_cost"] < 0.0:
+            total["initial_cost"] = r["initial_cost"]
+        total["iterations"] += r["iterations"]
+        total["final_cost"] = r["final_cost"]
+        total["converged"] = r["converged"]
+        total["cost_history"].extend(r["cost_history"].tolist())
+    return m, np.array(est), total
+
+
 def ldlt_solve(n, outer, inner, values, b, perm=None, num_threads=1):
     """Factor + solve of a full symmetric CSC matrix; returns (x, diag) or
     raises on a zero pivot (parallel_ldlt.hpp NumericalIssue)."""

@@ -28,6 +28,7 @@ from ._capi import (SDFGPU_ERR_INVALID_ARGUMENT, SDFGPU_ERR_NOT_READY, SDFGPU_ER
                     SDFGPU_ERR_OUT_OF_MEMORY, SDFGPU_ERR_TIMEOUT, SDFGPU_OK)
 
 __all__ = ["ProblemOptions", "SolverOptions", "SolveResult", "Problem", "Specs", "solve",
+           "run_incremental", "run_incremental_scene", "IncrementalResult",
            "LdltSolver", "Server", "GpuError", "NotReady", "device_count", "lib"]
 
 NORMAL_METHODS = {"pca": 0, "hybrid": 1, "weighted": 2}
@@ -424,6 +425,83 @@ def solve(problem: Problem, options: SolverOptions | list | None = None):
     if rc not in (SDFGPU_OK, SDFGPU_ERR_NUMERICAL):
         _check(rc)
     return out
+
+
+@dataclass
+class IncrementalResult:
+    """Final state and summed result of an incremental run."""
+    map_values: np.ndarray
+    poses: np.ndarray
+    result: SolveResult
+    phases: dict
+
+
+def run_incremental(nx, ny, min_corner, max_corner, poses, scans, options: ProblemOptions | None = None,
+                    solver: SolverOptions | None = None, relations=(), map_values=None, increment_size=1,
+                    iterations_per_increment=10, snapshot_every=0, snapshot=None, on_device=True,
+                    warm_analysis=True) -> IncrementalResult:
+    """Run in incremental mode (runner.cpp:226-285) on the GPU: `poses` are
+    the dataset poses (their consecutive RelativeTo is the odometry), each
+    step appends `increment_size` frames and runs `iterations_per_increment`
+    LM iterations over all frames so far. snapshot(frames, map_values, poses)
+    is called every `snapshot_every` steps and after the last."""
+    L = lib()
+    options = options or ProblemOptions()
+    solver = solver or SolverOptions()
+    poses = np.ascontiguousarray(poses, np.float64).reshape(-1, 3)
+    if len(scans) != len(poses):
+        raise ValueError("scan count != pose count")
+    offsets = np.zeros(len(scans) + 1, np.int32)
+    for f, s in enumerate(scans):
+        offsets[f + 1] = offsets[f] + len(s)
+    xy = (np.ascontiguousarray(np.concatenate([np.asarray(s, np.float64).reshape(-1, 2) for s in scans]))
+          if len(scans) else np.zeros((0, 2)))
+    rel_ij = np.ascontiguousarray([[r[0], r[1]] for r in relations], np.int32).reshape(-1, 2)
+    rel_meas = np.ascontiguousarray([r[2] for r in relations], np.float64).reshape(-1, 3)
+    rel_w = np.ascontiguousarray([r[3] if len(r) > 3 else 1.0 for r in relations], np.float64)
+    mv = None if map_values is None else np.ascontiguousarray(map_values, np.float64).reshape(-1)
+
+    def _snap(_user, frames, m, p):
+        snapshot(int(frames), np.ctypeslib.as_array(m, (int(nx) * int(ny),)).copy(),
+                 np.ctypeslib.as_array(p, (int(frames) * 3,)).reshape(-1, 3).copy())
+
+    cb = _capi.SnapshotFn(_snap) if snapshot is not None else _capi.SnapshotFn()
+    d = _capi.IncrementalDesc(
+        int(nx), int(ny), float(min_corner[0]), float(min_corner[1]), float(max_corner[0]),
+        float(max_corner[1]), _d(mv) if mv is not None else None, len(poses), _d(poses), _i(offsets),
+        _d(xy), len(rel_ij), _i(rel_ij) if len(rel_ij) else None,
+        _d(rel_meas) if len(rel_meas) else None, _d(rel_w) if len(rel_w) else None,
+        int(increment_size), int(iterations_per_increment), int(snapshot_every), cb, None,
+        int(bool(on_device)), int(bool(warm_analysis)))
+    po = options.to_c()
+    so = solver.to_c()
+    map_out = np.zeros(int(nx) * int(ny))
+    poses_out = np.zeros_like(poses)
+    total = _capi.SolveResultC()
+    steps = -(-max(len(poses) - 1, 0) // max(int(increment_size), 1))
+    cap = steps * (max(int(iterations_per_increment), 0) + 2)
+    hist = np.zeros(max(cap, 1))
+    ph = np.zeros(8)
+    _check(L.sdfgpu_run_incremental(ctypes.byref(d), ctypes.byref(po), ctypes.byref(so), _d(map_out),
+                                    _d(poses_out), ctypes.byref(total), _d(hist), cap, _d(ph)))
+    res = SolveResult(bool(total.converged), int(total.iterations), total.initial_cost, total.final_cost,
+                      total.duration_seconds, hist[: total.cost_history_length].tolist(), int(total.status))
+    keys = ["build", "wait_analysis", "setup", "solve", "readback", "wall"]
+    phases = dict(zip(keys, ph[:6].tolist()))
+    phases["increments"] = int(ph[6])
+    phases["warm_analyses"] = int(ph[7])
+    return IncrementalResult(map_out, poses_out, res, phases)
+
+
+def run_incremental_scene(scene, options: ProblemOptions | None = None, **kwargs) -> IncrementalResult:
+    """run_incremental over a synthetic scene (its options applied as
+    Problem.from_scene does)."""
+    opts = options or ProblemOptions()
+    for k, v in scene.options.items():
+        if k != "active_region" or options is None:
+            setattr(opts, k, v)
+    return run_incremental(scene.nx, scene.ny, scene.min_corner, scene.max_corner, scene.poses, scene.scans,
+                           opts, **kwargs)
 
 
 def _solve_batch(problem, c_opts, results, hist, cap):

@@ -76,6 +76,25 @@ class SolveResultC(ctypes.Structure):
     ]
 
 
+SnapshotFn = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int32, c_dbl_p, c_dbl_p)
+
+
+class IncrementalDesc(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32),
+        ("min_x", ctypes.c_double), ("min_y", ctypes.c_double),
+        ("max_x", ctypes.c_double), ("max_y", ctypes.c_double),
+        ("map_values", c_dbl_p),
+        ("num_frames", ctypes.c_int32), ("poses", c_dbl_p),
+        ("scan_offsets", c_int_p), ("scan_xy", c_dbl_p),
+        ("num_relations", ctypes.c_int32), ("relation_ij", c_int_p), ("relation_meas", c_dbl_p),
+        ("relation_sqrt_weight", c_dbl_p),
+        ("increment_size", ctypes.c_int32), ("iterations_per_increment", ctypes.c_int32),
+        ("snapshot_every", ctypes.c_int32), ("snapshot", SnapshotFn), ("snapshot_user", ctypes.c_void_p),
+        ("build_on_device", ctypes.c_int32), ("warm_analysis", ctypes.c_int32),
+    ]
+
+
 # name -> (restype, argtypes); every exported symbol of include/sdfgpu.h
 SIGNATURES = {
     "sdfgpu_last_error_message": (ctypes.c_char_p, []),
@@ -116,6 +135,9 @@ SIGNATURES = {
     "sdfgpu_last_profile": (ctypes.c_int, [vp, c_dbl_p]),
     "sdfgpu_autotune": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int32), c_dbl_p, c_dbl_p, ctypes.c_int32,
                                        ctypes.POINTER(ctypes.c_int32)]),
+    "sdfgpu_run_incremental": (ctypes.c_int, [ctypes.POINTER(IncrementalDesc), ctypes.POINTER(ProblemOptionsC),
+                                              ctypes.POINTER(SolverOptionsC), c_dbl_p, c_dbl_p,
+                                              ctypes.POINTER(SolveResultC), c_dbl_p, ctypes.c_int32, c_dbl_p]),
     "sdfgpu_ldlt_create": (ctypes.c_int, [ctypes.c_int32, c_int_p, c_int_p, c_int_p,
                                           ctypes.POINTER(vp)]),
     "sdfgpu_ldlt_factorize": (ctypes.c_int, [vp, c_dbl_p]),

@@ -36,9 +36,10 @@ SOURCES = {
     "host_pool.cpp": ["-x", "cu"],
     "symbolic.cpp": ["-x", "cu"],
     "capi.cpp": ["-x", "cu"],
+    "incremental.cpp": ["-x", "cu"],
     "server.cpp": ["-x", "cu"],
 }
-HEADERS = ["internal.h", "device.cuh", "engine.h", "ldlt.h", "server.h", "host_pool.h"]
+HEADERS = ["internal.h", "device.cuh", "engine.h", "ldlt.h", "server.h", "host_pool.h", "incremental.h"]
 
 
 def _newest_header() -> float:

@@ -3,6 +3,7 @@
 // sdfgpu_last_error_message().
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <new>
@@ -10,6 +11,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "incremental.h"
 #include "internal.h"
 #include "ldlt.h"
 #include "server.h"
@@ -319,6 +321,18 @@ int sdfgpu_apply_step(sdfgpu_problem* problem, int32_t index, const double* step
   });
 }
 
+static void CheckSolverOptions(const sdfgpu_solver_options& o) {
+  if (o.max_iterations < 0 || !(o.lambda_init >= 0.0) || !(o.lambda_factor > 0.0)) {
+    sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "invalid solver options");
+  }
+  if (o.precision != SDFGPU_PRECISION_FP64 && o.precision != SDFGPU_PRECISION_MIXED) {
+    sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "unknown precision");
+  }
+  if (o.refine_steps < 0 || o.refine_steps > 16) {
+    sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "refine_steps must lie in [0, 16]");
+  }
+}
+
 int sdfgpu_solve(sdfgpu_problem* problem, const sdfgpu_solver_options* options, sdfgpu_solve_result* results,
                  double* cost_history, int32_t capacity) {
   int first_status = SDFGPU_OK;
@@ -332,15 +346,7 @@ int sdfgpu_solve(sdfgpu_problem* problem, const sdfgpu_solver_options* options, 
       opts.assign(options, options + e.count());
     }
     for (const auto& o : opts) {
-      if (o.max_iterations < 0 || !(o.lambda_init >= 0.0) || !(o.lambda_factor > 0.0)) {
-        sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "invalid solver options");
-      }
-      if (o.precision != SDFGPU_PRECISION_FP64 && o.precision != SDFGPU_PRECISION_MIXED) {
-        sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "unknown precision");
-      }
-      if (o.refine_steps < 0 || o.refine_steps > 16) {
-        sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "refine_steps must lie in [0, 16]");
-      }
+      CheckSolverOptions(o);
     }
     e.Solve(opts, results, cost_history, capacity > 0 ? capacity : 0);
     for (int i = 0; i < e.count(); ++i) {
@@ -356,6 +362,75 @@ int sdfgpu_solve(sdfgpu_problem* problem, const sdfgpu_solver_options* options, 
     g_last_error = "sparse Cholesky factorization failed";
   }
   return first_status;
+}
+
+int sdfgpu_run_incremental(const sdfgpu_incremental_desc* desc, const sdfgpu_problem_options* problem_options,
+                           const sdfgpu_solver_options* solver_options, double* map_out, double* poses_out,
+                           sdfgpu_solve_result* total, double* cost_history, int32_t capacity, double* phases) {
+  return Guard([&] {
+    NeedHandle(desc, "desc");
+    NeedHandle(map_out, "map_out");
+    NeedHandle(poses_out, "poses_out");
+    NeedHandle(total, "total");
+    sdfgpu_problem_options po;
+    if (problem_options != nullptr) {
+      po = *problem_options;
+    } else {
+      sdfgpu_problem_options_default(&po);
+    }
+    sdfgpu_solver_options so;
+    if (solver_options != nullptr) {
+      so = *solver_options;
+    } else {
+      sdfgpu_solver_options_default(&so);
+    }
+    CheckSolverOptions(so);
+    sdfgpu::IncrementalInput in;
+    in.nx = desc->nx;
+    in.ny = desc->ny;
+    in.min_x = desc->min_x;
+    in.min_y = desc->min_y;
+    in.max_x = desc->max_x;
+    in.max_y = desc->max_y;
+    in.map_values = desc->map_values;
+    in.num_frames = desc->num_frames;
+    in.poses = desc->poses;
+    in.scan_offsets = desc->scan_offsets;
+    in.scan_xy = desc->scan_xy;
+    in.num_relations = desc->num_relations;
+    in.relation_ij = desc->relation_ij;
+    in.relation_meas = desc->relation_meas;
+    in.relation_sqrt_weight = desc->relation_sqrt_weight;
+    in.increment_size = desc->increment_size;
+    in.iterations_per_increment = desc->iterations_per_increment;
+    in.snapshot_every = desc->snapshot_every;
+    in.snapshot = desc->snapshot;
+    in.snapshot_user = desc->snapshot_user;
+    in.build_on_device = desc->build_on_device;
+    in.warm_analysis = desc->warm_analysis;
+    if (in.nx < 2 || in.ny < 2) {
+      sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "GridMap needs nx, ny >= 2 and max > min");
+    }
+    sdfgpu::IncrementalOutput out;
+    sdfgpu::RunIncremental(in, po, so, &out);
+    std::copy(out.map.begin(), out.map.end(), map_out);
+    std::copy(out.poses.begin(), out.poses.end(), poses_out);
+    *total = out.total;
+    const size_t n = std::min(out.cost_history.size(), static_cast<size_t>(std::max(0, capacity)));
+    if (cost_history != nullptr) {
+      std::copy(out.cost_history.begin(), out.cost_history.begin() + static_cast<std::ptrdiff_t>(n), cost_history);
+      total->cost_history_length = static_cast<int32_t>(n);
+    } else {
+      total->cost_history_length = 0;
+    }
+    total->status = SDFGPU_OK;
+    if (phases != nullptr) {
+      const sdfgpu::IncrementalPhases& p = out.phases;
+      const double v[8] = {p.build, p.wait_analysis, p.setup, p.solve, p.readback, p.wall,
+                           static_cast<double>(p.increments), static_cast<double>(p.warm_analyses)};
+      std::copy(v, v + 8, phases);
+    }
+  });
 }
 
 int sdfgpu_linearize(sdfgpu_problem* problem, int32_t index, double lambda, int32_t marquardt,

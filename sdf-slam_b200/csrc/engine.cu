@@ -61,7 +61,14 @@ int FrontIndex(const Symbolic& S, const SupernodeRec& s, int r) {
 
 }  // namespace
 
-Engine::Engine(std::vector<HostProblem> problems) : host_(std::move(problems)) {
+Engine::Engine(std::vector<HostProblem> problems) : host_(std::move(problems)) { Init(nullptr); }
+
+Engine::Engine(HostProblem problem, SymPiece piece) {
+  host_.push_back(std::move(problem));
+  Init(&piece);
+}
+
+void Engine::Init(SymPiece* piece) {
   if (host_.empty()) {
     Fail(SDFGPU_ERR_INVALID_ARGUMENT, "no problems");
   }
@@ -86,8 +93,19 @@ Engine::Engine(std::vector<HostProblem> problems) : host_(std::move(problems)) {
   h_lam_.Alloc(host_.size());
   h_seg_.Alloc(5 * host_.size());
   h_status_.Alloc(host_.size());
-  // the symbolic analysis (host only) runs while the problem is uploaded
-  std::future<void> analysis = std::async(std::launch::async, [this] { AnalyzeHost(); });
+  // the symbolic analysis (host only) runs while the problem is uploaded; a
+  // given analysis only needs its global structure
+  std::future<void> analysis = std::async(std::launch::async, [this, piece] {
+    if (piece == nullptr) {
+      AnalyzeHost();
+      return;
+    }
+    margin_.assign(1, piece->margin);
+    pieces_.clear();
+    pieces_.push_back(std::move(*piece));
+    pending_.clear();
+    sym_ = GlobalStructure();
+  });
   try {
     UploadProblem();
   } catch (...) {

@@ -163,6 +163,10 @@ struct IterTimes {
 class Engine {
  public:
   explicit Engine(std::vector<HostProblem> problems);
+  /// One problem with its symbolic analysis done already (AnalyzeInstance
+  /// of a problem with the same columns, frames and point rows; the
+  /// iterations re-analyse if the state leaves its pattern).
+  Engine(HostProblem problem, SymPiece piece);
   ~Engine();
   Engine(const Engine&) = delete;
   Engine& operator=(const Engine&) = delete;
@@ -217,6 +221,7 @@ class Engine {
   [[nodiscard]] const Symbolic& symbolic() const { return sym_; }
 
  private:
+  void Init(SymPiece* piece);
   void BuildLayout();
   void UploadProblem();
   /// Symbolic analysis of every instance at its current state (host only).

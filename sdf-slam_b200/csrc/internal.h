@@ -66,13 +66,15 @@ struct HostProblem {
 HostProblem FromDesc(const sdfgpu_problem_desc& desc);
 
 /// Problem::Problem (src/problem/problem.cpp:11-115) on the host.
+/// pattern_only (host stages only): no normals and no Eikonal specs, the
+/// fields a symbolic analysis reads and nothing more.
 HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_x, double max_y,
                          const double* map_values, int num_frames, const double* poses,
                          const int32_t* scan_offsets, const double* scan_xy,
                          const double* odometry, int num_odometry, int num_relations,
                          const int32_t* relation_ij, const double* relation_meas,
                          const double* relation_sqrt_weight, const sdfgpu_problem_options& options,
-                         bool device_stages = false);
+                         bool device_stages = false, bool pattern_only = false);
 
 /// A bucket grid over a point set for exact k-nearest-neighbour search: the
 /// bucket of a point is its clamped cell (floor((p - origin) / cell) per

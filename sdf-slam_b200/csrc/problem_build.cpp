@@ -486,8 +486,11 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
                          const double* odometry, int num_odometry, int num_relations,
                          const int32_t* relation_ij, const double* relation_meas,
                          const double* relation_sqrt_weight, const sdfgpu_problem_options& o,
-                         bool device_stages) {
+                         bool device_stages, bool pattern_only) {
   auto bad = [](const std::string& m) { Fail(SDFGPU_ERR_INVALID_ARGUMENT, m); };
+  if (device_stages && pattern_only) {
+    bad("a pattern-only build runs on the host");
+  }
   if (nx < 2 || ny < 2 || !(max_x > min_x) || !(max_y > min_y)) {
     bad("GridMap needs nx, ny >= 2 and max > min");
   }
@@ -596,10 +599,12 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
 
   std::vector<double> node_normal;
   std::vector<double> node_scale;
-  if (!device_stages) {
+  if (!device_stages && !pattern_only) {
     HostNodeNormals(hp, num_frames, scan_offsets, scan_xy, o, node_normal, node_scale);
   }
-  if (device_stages) {
+  if (pattern_only) {
+    // no Eikonal specs
+  } else if (device_stages) {
     // point specs, active maps, node normals and the Eikonal spec list by
     // CUDA kernels
     DeviceBuildSpecs(hp, num_frames, scan_offsets, scan_xy, o);
