@@ -329,6 +329,33 @@ int sdfgpu_run_incremental(const sdfgpu_incremental_desc* desc, const sdfgpu_pro
                            sdfgpu_solve_result* total, double* cost_history, int32_t capacity,
                            double* phases);
 
+/* -------------------------------------------------------------- outputs --
+ * run_slam's output files (src/pipeline/runner.cpp:82-192), same formats:
+ * poses as "x,y,theta" CSV with 17 significant digits (WritePoses :82-88);
+ * the map as a "nx ny min_x min_y dx dy" line and ny lines of nx values
+ * (WriteMap :90-99); every scan point at its frame's pose as "x,y" CSV with
+ * 9 digits (WriteGlobalScanPoints :101-114); the result and, when metrics is
+ * not NULL, the four trajectory errors as JSON (WriteJson :172-192). No GPU
+ * is needed. */
+int sdfgpu_write_poses(const char* path, const double* poses, int32_t num_frames);
+int sdfgpu_write_map(const char* path, int32_t nx, int32_t ny, double min_x, double min_y, double max_x,
+                     double max_y, const double* map_values);
+int sdfgpu_write_scan_points(const char* path, int32_t num_frames, const double* poses,
+                             const int32_t* scan_offsets, const double* scan_xy);
+int sdfgpu_write_metrics(const char* path, const sdfgpu_solve_result* result, const double* metrics);
+
+/* Evaluate (runner.cpp:145-170): metrics[0..3] = mean translation error, mean
+ * |rotation error|, and the same two over consecutive relative poses, of the
+ * estimated poses against ground truth (num_frames >= 2 each). */
+int sdfgpu_evaluate_trajectory(const double* estimated, const double* ground_truth, int32_t num_frames,
+                               double* metrics);
+
+/* The scan points WarnIfPointsOutsideMap (runner.cpp:116-137) counts: those
+ * whose global position lies outside the grid's domain, and all of them. */
+int sdfgpu_points_outside_map(int32_t nx, int32_t ny, double min_x, double min_y, double max_x, double max_y,
+                              int32_t num_frames, const double* poses, const int32_t* scan_offsets,
+                              const double* scan_xy, int64_t* outside, int64_t* total);
+
 /* ------------------------------------------------------------ factor only --
  * LinearSolver::kGpu: ParallelSimplicialLdlt's interface
  * (src/solvers/parallel_ldlt.hpp:38-51 and Eigen's solve) for any symmetric

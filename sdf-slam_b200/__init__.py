@@ -19,6 +19,7 @@ CPU fallback: without the built library or a GPU every entry point raises.
 from __future__ import annotations
 
 import ctypes
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -28,7 +29,8 @@ from ._capi import (SDFGPU_ERR_INVALID_ARGUMENT, SDFGPU_ERR_NOT_READY, SDFGPU_ER
                     SDFGPU_ERR_OUT_OF_MEMORY, SDFGPU_ERR_TIMEOUT, SDFGPU_OK)
 
 __all__ = ["ProblemOptions", "SolverOptions", "SolveResult", "Problem", "Specs", "solve",
-           "run_incremental", "run_incremental_scene", "IncrementalResult",
+           "run_incremental", "run_incremental_scene", "IncrementalResult", "write_run_outputs",
+           "evaluate_trajectory",
            "LdltSolver", "Server", "GpuError", "NotReady", "device_count", "lib"]
 
 NORMAL_METHODS = {"pca": 0, "hybrid": 1, "weighted": 2}
@@ -502,6 +504,72 @@ def run_incremental_scene(scene, options: ProblemOptions | None = None, **kwargs
             setattr(opts, k, v)
     return run_incremental(scene.nx, scene.ny, scene.min_corner, scene.max_corner, scene.poses, scene.scans,
                            opts, **kwargs)
+
+
+def _scan_arrays(scans):
+    offsets = np.zeros(len(scans) + 1, np.int32)
+    for f, s in enumerate(scans):
+        offsets[f + 1] = offsets[f] + len(s)
+    xy = (np.ascontiguousarray(np.concatenate([np.asarray(s, np.float64).reshape(-1, 2) for s in scans]))
+          if len(scans) else np.zeros((0, 2)))
+    return offsets, xy
+
+
+def evaluate_trajectory(estimated, ground_truth) -> dict:
+    """Evaluate (runner.cpp:145-170): the four mean trajectory errors."""
+    est = np.ascontiguousarray(estimated, np.float64).reshape(-1, 3)
+    gt = np.ascontiguousarray(ground_truth, np.float64).reshape(-1, 3)
+    if len(est) != len(gt):
+        raise ValueError("pose count mismatch between estimate and ground truth")
+    m = np.zeros(4)
+    _check(lib().sdfgpu_evaluate_trajectory(_d(est), _d(gt), len(est), _d(m)))
+    return dict(zip(["mean_translation_error", "mean_rotation_error", "mean_relative_translation_error",
+                     "mean_relative_rotation_error"], m.tolist()))
+
+
+def write_run_outputs(output_dir, nx, ny, min_corner, max_corner, dataset_poses, scans, estimated, map_values,
+                      result: SolveResult, ground_truth=None):
+    """The output section of Run (runner.cpp:288-303): poses_odometry.csv,
+    poses_estimated.csv, map.txt, scan_points_global.csv, the out-of-domain
+    warning on stderr, and metrics.json (with the trajectory errors and
+    poses_ground_truth.csv when ground truth is given). Returns the metrics
+    (None without ground truth)."""
+    import sys
+    L = lib()
+    os.makedirs(output_dir, exist_ok=True)
+
+    def path(name):
+        return os.path.join(os.fspath(output_dir), name).encode()
+
+    dp = np.ascontiguousarray(dataset_poses, np.float64).reshape(-1, 3)
+    est = np.ascontiguousarray(estimated, np.float64).reshape(-1, 3)
+    mv = np.ascontiguousarray(map_values, np.float64).reshape(-1)
+    offsets, xy = _scan_arrays(scans)
+    mn, mx = (float(min_corner[0]), float(min_corner[1])), (float(max_corner[0]), float(max_corner[1]))
+    _check(L.sdfgpu_write_poses(path("poses_odometry.csv"), _d(dp), len(dp)))
+    _check(L.sdfgpu_write_poses(path("poses_estimated.csv"), _d(est), len(est)))
+    _check(L.sdfgpu_write_map(path("map.txt"), int(nx), int(ny), *mn, *mx, _d(mv)))
+    _check(L.sdfgpu_write_scan_points(path("scan_points_global.csv"), len(est), _d(est), _i(offsets), _d(xy)))
+    outside = ctypes.c_int64()
+    total = ctypes.c_int64()
+    _check(L.sdfgpu_points_outside_map(int(nx), int(ny), *mn, *mx, len(est), _d(est), _i(offsets), _d(xy),
+                                       ctypes.byref(outside), ctypes.byref(total)))
+    if outside.value > 0:
+        print(f"WARNING: {outside.value} of {total.value} scan points "
+              f"({100.0 * outside.value / total.value:g}%) fall outside the map domain and are unanchored "
+              "(SDF 0, no gradient). Widen the map domain or disable auto_domain with explicit corners.",
+              file=sys.stderr)
+    r = _capi.SolveResultC(int(result.converged), int(result.iterations), float(result.initial_cost),
+                           float(result.final_cost), float(result.duration_seconds), 0, 0)
+    metrics = None
+    m = None
+    if ground_truth is not None:
+        gt = np.ascontiguousarray(ground_truth, np.float64).reshape(-1, 3)
+        _check(L.sdfgpu_write_poses(path("poses_ground_truth.csv"), _d(gt), len(gt)))
+        metrics = evaluate_trajectory(est, gt)
+        m = np.array(list(metrics.values()))
+    _check(L.sdfgpu_write_metrics(path("metrics.json"), ctypes.byref(r), _d(m) if m is not None else None))
+    return metrics
 
 
 def _solve_batch(problem, c_opts, results, hist, cap):

@@ -138,6 +138,15 @@ SIGNATURES = {
     "sdfgpu_run_incremental": (ctypes.c_int, [ctypes.POINTER(IncrementalDesc), ctypes.POINTER(ProblemOptionsC),
                                               ctypes.POINTER(SolverOptionsC), c_dbl_p, c_dbl_p,
                                               ctypes.POINTER(SolveResultC), c_dbl_p, ctypes.c_int32, c_dbl_p]),
+    "sdfgpu_write_poses": (ctypes.c_int, [ctypes.c_char_p, c_dbl_p, ctypes.c_int32]),
+    "sdfgpu_write_map": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_double, ctypes.c_double, c_dbl_p]),
+    "sdfgpu_write_scan_points": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, c_dbl_p, c_int_p, c_dbl_p]),
+    "sdfgpu_write_metrics": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(SolveResultC), c_dbl_p]),
+    "sdfgpu_evaluate_trajectory": (ctypes.c_int, [c_dbl_p, c_dbl_p, ctypes.c_int32, c_dbl_p]),
+    "sdfgpu_points_outside_map": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                                 ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                                 ctypes.c_int32, c_dbl_p, c_int_p, c_dbl_p, c_i64_p, c_i64_p]),
     "sdfgpu_ldlt_create": (ctypes.c_int, [ctypes.c_int32, c_int_p, c_int_p, c_int_p,
                                           ctypes.POINTER(vp)]),
     "sdfgpu_ldlt_factorize": (ctypes.c_int, [vp, c_dbl_p]),

@@ -37,6 +37,7 @@ SOURCES = {
     "symbolic.cpp": ["-x", "cu"],
     "capi.cpp": ["-x", "cu"],
     "incremental.cpp": ["-x", "cu"],
+    "writers.cpp": ["-x", "cu"],
     "server.cpp": ["-x", "cu"],
 }
 HEADERS = ["internal.h", "device.cuh", "engine.h", "ldlt.h", "server.h", "host_pool.h", "incremental.h"]

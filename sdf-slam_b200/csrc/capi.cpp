@@ -433,6 +433,86 @@ int sdfgpu_run_incremental(const sdfgpu_incremental_desc* desc, const sdfgpu_pro
   });
 }
 
+static void CheckGrid(int32_t nx, int32_t ny, double min_x, double min_y, double max_x, double max_y) {
+  if (nx < 2 || ny < 2 || !(max_x > min_x) || !(max_y > min_y)) {
+    sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "GridMap needs nx, ny >= 2 and max > min");
+  }
+}
+
+static void CheckScans(int32_t num_frames, const double* poses, const int32_t* scan_offsets,
+                       const double* scan_xy) {
+  if (num_frames < 0 || (num_frames > 0 && (poses == nullptr || scan_offsets == nullptr))) {
+    sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "poses and scans are required");
+  }
+  for (int32_t f = 0; f < num_frames; ++f) {
+    if (scan_offsets[f + 1] < scan_offsets[f]) {
+      sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "scan offsets must not decrease");
+    }
+  }
+  if (num_frames > 0 && scan_offsets[0] != 0) {
+    sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "scan offsets must start at 0");
+  }
+  if (num_frames > 0 && scan_offsets[num_frames] > 0 && scan_xy == nullptr) {
+    sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "scan points missing");
+  }
+}
+
+int sdfgpu_write_poses(const char* path, const double* poses, int32_t num_frames) {
+  return Guard([&] {
+    if (num_frames < 0 || (num_frames > 0 && poses == nullptr)) {
+      sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "poses missing");
+    }
+    sdfgpu::WritePoses(path, poses, num_frames);
+  });
+}
+
+int sdfgpu_write_map(const char* path, int32_t nx, int32_t ny, double min_x, double min_y, double max_x,
+                     double max_y, const double* map_values) {
+  return Guard([&] {
+    CheckGrid(nx, ny, min_x, min_y, max_x, max_y);
+    NeedHandle(map_values, "map_values");
+    sdfgpu::WriteMap(path, nx, ny, min_x, min_y, max_x, max_y, map_values);
+  });
+}
+
+int sdfgpu_write_scan_points(const char* path, int32_t num_frames, const double* poses,
+                             const int32_t* scan_offsets, const double* scan_xy) {
+  return Guard([&] {
+    CheckScans(num_frames, poses, scan_offsets, scan_xy);
+    sdfgpu::WriteScanPoints(path, num_frames, poses, scan_offsets, scan_xy);
+  });
+}
+
+int sdfgpu_write_metrics(const char* path, const sdfgpu_solve_result* result, const double* metrics) {
+  return Guard([&] {
+    NeedHandle(result, "result");
+    sdfgpu::WriteMetrics(path, *result, metrics);
+  });
+}
+
+int sdfgpu_evaluate_trajectory(const double* estimated, const double* ground_truth, int32_t num_frames,
+                               double* metrics) {
+  return Guard([&] {
+    NeedHandle(estimated, "estimated");
+    NeedHandle(ground_truth, "ground_truth");
+    NeedHandle(metrics, "metrics");
+    sdfgpu::EvaluateTrajectory(estimated, ground_truth, num_frames, metrics);
+  });
+}
+
+int sdfgpu_points_outside_map(int32_t nx, int32_t ny, double min_x, double min_y, double max_x, double max_y,
+                              int32_t num_frames, const double* poses, const int32_t* scan_offsets,
+                              const double* scan_xy, int64_t* outside, int64_t* total) {
+  return Guard([&] {
+    CheckGrid(nx, ny, min_x, min_y, max_x, max_y);
+    CheckScans(num_frames, poses, scan_offsets, scan_xy);
+    NeedHandle(outside, "outside");
+    NeedHandle(total, "total");
+    sdfgpu::PointsOutsideMap(nx, ny, min_x, min_y, max_x, max_y, num_frames, poses, scan_offsets, scan_xy,
+                             outside, total);
+  });
+}
+
 int sdfgpu_linearize(sdfgpu_problem* problem, int32_t index, double lambda, int32_t marquardt,
                      int32_t compute_step) {
   return Guard([&] {

@@ -113,6 +113,19 @@ void PrepareNormalGrids(const HostProblem& hp, int num_frames, const int32_t* sc
 void DeviceBuildSpecs(HostProblem& hp, int num_frames, const int32_t* scan_offsets, const double* scan_xy,
                       const sdfgpu_problem_options& options);
 
+// -------------------------------------------------------------- writers --
+// run_slam's output files and metrics (src/pipeline/runner.cpp:82-192).
+void WritePoses(const char* path, const double* poses, int num_frames);
+void WriteMap(const char* path, int nx, int ny, double min_x, double min_y, double max_x, double max_y,
+              const double* values);
+void WriteScanPoints(const char* path, int num_frames, const double* poses, const int32_t* offsets,
+                     const double* xy);
+void PointsOutsideMap(int nx, int ny, double min_x, double min_y, double max_x, double max_y, int num_frames,
+                      const double* poses, const int32_t* offsets, const double* xy, int64_t* outside,
+                      int64_t* total);
+void EvaluateTrajectory(const double* est, const double* gt, int num_frames, double* metrics);
+void WriteMetrics(const char* path, const sdfgpu_solve_result& result, const double* metrics);
+
 // ------------------------------------------------------------- symbolic --
 
 /// Per-supernode record uploaded to the device.
