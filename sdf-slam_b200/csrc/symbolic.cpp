@@ -673,8 +673,10 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
           if (!(fx >= -margin) || !(fy >= -margin) || !(fx <= hp.nx - 1 + margin) || !(fy <= hp.ny - 1 + margin)) {
             continue;
           }
-          const int w = std::clamp(static_cast<int>(std::floor(fx)), 0, cw - 1);
-          const int h = std::clamp(static_cast<int>(std::floor(fy)), 0, chh - 1);
+          // clamp(floor(f), 0, cells - 1) for the bounded f above: truncation
+          // equals floor for f >= 0, and every f < 0 maps to cell 0
+          const int w = fx > 0.0 ? std::min(static_cast<int>(fx), cw - 1) : 0;
+          const int h = fy > 0.0 ? std::min(static_cast<int>(fy), chh - 1) : 0;
           occ[static_cast<size_t>(h) * rw + static_cast<size_t>(w >> 6)] |= uint64_t{1} << (w & 63);
         }
         // horizontal dilation: `margin` passes of a one-cell shift both ways;
