@@ -9,6 +9,7 @@
 // owner whose stream has drained, so a reused block has no work in flight.
 #include <cuda_runtime.h>
 
+#include <deque>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -31,9 +32,11 @@ size_t SizeClass(size_t bytes) {
 
 struct Cache {
   std::mutex mu;
-  // (device, class) -> free blocks; device -1 for pinned host blocks
-  std::map<std::pair<int, size_t>, std::vector<void*>> free_blocks;
+  // (device, class) -> free blocks with the stamp of their release, oldest
+  // first; device -1 for pinned host blocks
+  std::map<std::pair<int, size_t>, std::deque<std::pair<void*, uint64_t>>> free_blocks;
   std::map<int, size_t> cached_bytes;
+  uint64_t stamp{0};
 };
 
 Cache& TheCache() {
@@ -45,6 +48,14 @@ Cache& TheCache() {
 constexpr size_t kMaxCachedDevice = size_t{8} << 30;
 constexpr size_t kMaxCachedHost = size_t{256} << 20;
 
+void Release(int dev, void* p) {
+  if (dev < 0) {
+    cudaFreeHost(p);
+  } else {
+    cudaFree(p);
+  }
+}
+
 void* Take(int dev, size_t cls) {
   Cache& c = TheCache();
   const std::lock_guard<std::mutex> lock(c.mu);
@@ -52,21 +63,47 @@ void* Take(int dev, size_t cls) {
   if (it == c.free_blocks.end() || it->second.empty()) {
     return nullptr;
   }
-  void* p = it->second.back();
+  void* p = it->second.back().first;
   it->second.pop_back();
   c.cached_bytes[dev] -= cls;
   return p;
 }
 
-bool Keep(int dev, size_t cls, void* p, size_t limit) {
+/// Caches a released block. Over the limit, the blocks of `dev` released
+/// longest ago go first: a workload whose sizes drift (a problem growing
+/// frame by frame) leaves blocks of classes it no longer asks for, and the
+/// working set of the latest sizes must stay cached.
+void Keep(int dev, size_t cls, void* p, size_t limit) {
   Cache& c = TheCache();
-  const std::lock_guard<std::mutex> lock(c.mu);
-  if (c.cached_bytes[dev] + cls > limit) {
-    return false;
+  std::vector<void*> victims;
+  {
+    const std::lock_guard<std::mutex> lock(c.mu);
+    if (cls > limit) {
+      victims.push_back(p);
+    } else {
+      while (c.cached_bytes[dev] + cls > limit) {
+        auto oldest = c.free_blocks.end();
+        for (auto it = c.free_blocks.lower_bound({dev, 0}); it != c.free_blocks.end() && it->first.first == dev;
+             ++it) {
+          if (!it->second.empty() &&
+              (oldest == c.free_blocks.end() || it->second.front().second < oldest->second.front().second)) {
+            oldest = it;
+          }
+        }
+        if (oldest == c.free_blocks.end()) {
+          break;
+        }
+        victims.push_back(oldest->second.front().first);
+        oldest->second.pop_front();
+        c.cached_bytes[dev] -= oldest->first.second;
+      }
+      c.free_blocks[{dev, cls}].emplace_back(p, ++c.stamp);
+      c.cached_bytes[dev] += cls;
+    }
   }
-  c.free_blocks[{dev, cls}].push_back(p);
-  c.cached_bytes[dev] += cls;
-  return true;
+  for (void* v : victims) {
+    Release(dev, v);
+  }
 }
 
 /// Releases every cached block of `dev` (before retrying a failed allocation).
@@ -77,7 +114,9 @@ void Drop(int dev) {
     const std::lock_guard<std::mutex> lock(c.mu);
     for (auto it = c.free_blocks.begin(); it != c.free_blocks.end();) {
       if (it->first.first == dev) {
-        blocks.insert(blocks.end(), it->second.begin(), it->second.end());
+        for (const auto& b : it->second) {
+          blocks.push_back(b.first);
+        }
         it = c.free_blocks.erase(it);
       } else {
         ++it;
@@ -86,11 +125,7 @@ void Drop(int dev) {
     c.cached_bytes[dev] = 0;
   }
   for (void* p : blocks) {
-    if (dev < 0) {
-      cudaFreeHost(p);
-    } else {
-      cudaFree(p);
-    }
+    Release(dev, p);
   }
 }
 
@@ -123,12 +158,7 @@ void* CachedDeviceAlloc(size_t bytes, size_t* got) {
   return p;
 }
 
-void CachedDeviceFree(void* p, size_t cls) {
-  const int dev = CurrentDevice();
-  if (!Keep(dev, cls, p, kMaxCachedDevice)) {
-    cudaFree(p);
-  }
-}
+void CachedDeviceFree(void* p, size_t cls) { Keep(CurrentDevice(), cls, p, kMaxCachedDevice); }
 
 void* CachedHostAlloc(size_t bytes, size_t* got) {
   const size_t cls = SizeClass(bytes);
@@ -141,10 +171,6 @@ void* CachedHostAlloc(size_t bytes, size_t* got) {
   return p;
 }
 
-void CachedHostFree(void* p, size_t cls) {
-  if (!Keep(-1, cls, p, kMaxCachedHost)) {
-    cudaFreeHost(p);
-  }
-}
+void CachedHostFree(void* p, size_t cls) { Keep(-1, cls, p, kMaxCachedHost); }
 
 }  // namespace sdfgpu

@@ -166,7 +166,8 @@ static int BuildProblemHandle(bool on_device, int32_t nx, int32_t ny, double min
     std::vector<sdfgpu::HostProblem> v;
     v.push_back(sdfgpu::BuildProblem(nx, ny, min_x, min_y, max_x, max_y, map_values, num_frames, poses,
                                      scan_offsets, scan_xy, odometry, num_odometry, num_relations, relation_ij,
-                                     relation_meas, relation_sqrt_weight, o, on_device));
+                                     relation_meas, relation_sqrt_weight, o,
+                                     sdfgpu::BuildMode{on_device, false, true}));
     auto h = std::make_unique<sdfgpu_problem>();
     h->host = std::move(v);
     *out = h.release();
@@ -426,9 +427,9 @@ int sdfgpu_run_incremental(const sdfgpu_incremental_desc* desc, const sdfgpu_pro
     total->status = SDFGPU_OK;
     if (phases != nullptr) {
       const sdfgpu::IncrementalPhases& p = out.phases;
-      const double v[8] = {p.build, p.wait_analysis, p.setup, p.solve, p.readback, p.wall,
+      const double v[9] = {p.build,    p.wait_analysis, p.setup, p.solve, p.readback, p.teardown, p.wall,
                            static_cast<double>(p.increments), static_cast<double>(p.warm_analyses)};
-      std::copy(v, v + 8, phases);
+      std::copy(v, v + 9, phases);
     }
   });
 }

@@ -93,6 +93,11 @@ void Engine::Init(SymPiece* piece) {
   h_lam_.Alloc(host_.size());
   h_seg_.Alloc(5 * host_.size());
   h_status_.Alloc(host_.size());
+  mixed_.assign(host_.size(), 0);  // plain FP64 until a solve asks otherwise
+  AnalyzeAndUpload(piece, 0);
+}
+
+void Engine::AnalyzeAndUpload(SymPiece* piece, int64_t keep_rows) {
   // the symbolic analysis (host only) runs while the problem is uploaded; a
   // given analysis only needs its global structure
   std::future<void> analysis = std::async(std::launch::async, [this, piece] {
@@ -107,14 +112,35 @@ void Engine::Init(SymPiece* piece) {
     sym_ = GlobalStructure();
   });
   try {
-    UploadProblem();
+    UploadProblem(keep_rows);
   } catch (...) {
     analysis.wait();
     throw;
   }
   analysis.get();
-  mixed_.assign(host_.size(), 0);  // plain FP64 until a solve asks otherwise
   UploadSymbolic();
+}
+
+bool Engine::CanReplace(const HostProblem& next) const {
+  if (host_.size() != 1) {
+    return false;
+  }
+  const HostProblem& cur = host_[0];
+  return next.nx == cur.nx && next.ny == cur.ny && next.min_x == cur.min_x && next.min_y == cur.min_y &&
+         next.max_x == cur.max_x && next.max_y == cur.max_y && next.node_to_active == cur.node_to_active;
+}
+
+void Engine::Replace(HostProblem next, SymPiece* piece, int64_t keep_rows) {
+  if (!CanReplace(next)) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT, "replacement problem has another grid or other active columns");
+  }
+  keep_rows = std::max<int64_t>(0, std::min<int64_t>({keep_rows, host_[0].num_points(), next.num_points()}));
+  // nothing enqueued may still read the current problem's buffers
+  CudaCheck(cudaStreamSynchronize(stream_), "replace sync");
+  DropGraph();
+  host_[0] = std::move(next);
+  BuildLayout();
+  AnalyzeAndUpload(piece, keep_rows);
 }
 
 void Engine::DropGraph() {
@@ -197,17 +223,25 @@ void Engine::BuildLayout() {
   total_odom_ = odom;
 }
 
-void Engine::UploadProblem() {
+void Engine::UploadProblem(int64_t keep_rows) {
   const size_t I = host_.size();
+  // One instance: its point rows go up from its own arrays (rows before
+  // keep_rows are on the device already) and only the frame index of the
+  // rows is built here; several: every array is gathered first.
+  const bool direct = I == 1;
+  if (!direct) {
+    keep_rows = 0;
+  }
   std::vector<int32_t> node_col(static_cast<size_t>(total_nodes_), -1);
   std::vector<int32_t> col_node(static_cast<size_t>(n_), -1);
   std::vector<int32_t> col_inst(static_cast<size_t>(n_), 0);
   std::vector<int32_t> frame_inst(static_cast<size_t>(total_frames_), 0);
   std::vector<int32_t> frame_col(static_cast<size_t>(total_frames_), -1);
-  std::vector<int32_t> pt_frame(static_cast<size_t>(total_points_));
-  std::vector<double2> pt_xy(static_cast<size_t>(total_points_));
-  std::vector<double> pt_exp(static_cast<size_t>(total_points_));
-  std::vector<double> pt_sw(static_cast<size_t>(total_points_));
+  const size_t gathered = direct ? 0 : static_cast<size_t>(total_points_);
+  std::vector<int32_t> pt_frame(gathered);
+  std::vector<double2> pt_xy(gathered);
+  std::vector<double> pt_exp(gathered);
+  std::vector<double> pt_sw(gathered);
   std::vector<int32_t> eik_node(static_cast<size_t>(total_eik_));
   std::vector<int32_t> eik_index(static_cast<size_t>(total_nodes_), -1);
   std::vector<double2> eik_n(static_cast<size_t>(total_eik_));
@@ -243,13 +277,19 @@ void Engine::UploadProblem() {
       frame_inst[static_cast<size_t>(L.frame_off + f)] = static_cast<int32_t>(i);
       frame_col[static_cast<size_t>(L.frame_off + f)] = f >= 1 ? L.col_off + hp.num_active() + 3 * (f - 1) : -1;
     }
-    for (int k = 0; k < hp.num_points(); ++k) {
-      const size_t g = static_cast<size_t>(L.pt_off + k);
-      pt_frame[g] = L.frame_off + hp.pt_frame[static_cast<size_t>(k)];
-      pt_xy[g] = make_double2(hp.pt_xy[2 * static_cast<size_t>(k)], hp.pt_xy[2 * static_cast<size_t>(k) + 1]);
-      pt_exp[g] = hp.pt_expected[static_cast<size_t>(k)];
-      pt_sw[g] = hp.pt_sqrtw[static_cast<size_t>(k)];
-      ++frame_rows_ptr[static_cast<size_t>(pt_frame[g]) + 1];
+    if (direct) {
+      for (const int32_t f : hp.pt_frame) {
+        ++frame_rows_ptr[static_cast<size_t>(f) + 1];
+      }
+    } else {
+      for (int k = 0; k < hp.num_points(); ++k) {
+        const size_t g = static_cast<size_t>(L.pt_off + k);
+        pt_frame[g] = L.frame_off + hp.pt_frame[static_cast<size_t>(k)];
+        pt_xy[g] = make_double2(hp.pt_xy[2 * static_cast<size_t>(k)], hp.pt_xy[2 * static_cast<size_t>(k) + 1]);
+        pt_exp[g] = hp.pt_expected[static_cast<size_t>(k)];
+        pt_sw[g] = hp.pt_sqrtw[static_cast<size_t>(k)];
+        ++frame_rows_ptr[static_cast<size_t>(pt_frame[g]) + 1];
+      }
     }
     for (int e = 0; e < hp.num_eikonal(); ++e) {
       const size_t g = static_cast<size_t>(L.eik_off + e);
@@ -290,11 +330,21 @@ void Engine::UploadProblem() {
     frame_rows_ptr[static_cast<size_t>(f) + 1] += frame_rows_ptr[static_cast<size_t>(f)];
     frame_odom_ptr[static_cast<size_t>(f) + 1] += frame_odom_ptr[static_cast<size_t>(f)];
   }
+  const std::vector<int32_t>& row_frame = direct ? host_[0].pt_frame : pt_frame;
+  // rows ordered by frame (as the builders emit them) make the frame index
+  // the identity, of which a kept prefix is on the device already
+  const bool identity = std::is_sorted(row_frame.begin(), row_frame.end());
   {
-    std::vector<int64_t> fill(frame_rows_ptr.begin(), frame_rows_ptr.end() - 1);
-    for (int64_t k = 0; k < total_points_; ++k) {
-      frame_rows[static_cast<size_t>(fill[static_cast<size_t>(pt_frame[static_cast<size_t>(k)])]++)] =
-          static_cast<int32_t>(k);
+    if (identity) {
+      for (int64_t k = frame_rows_identity_ ? keep_rows : 0; k < total_points_; ++k) {
+        frame_rows[static_cast<size_t>(k)] = static_cast<int32_t>(k);
+      }
+    } else {
+      std::vector<int64_t> fill(frame_rows_ptr.begin(), frame_rows_ptr.end() - 1);
+      for (int64_t k = 0; k < total_points_; ++k) {
+        frame_rows[static_cast<size_t>(fill[static_cast<size_t>(row_frame[static_cast<size_t>(k)])]++)] =
+            static_cast<int32_t>(k);
+      }
     }
     std::vector<int64_t> ofill(frame_odom_ptr.begin(), frame_odom_ptr.end() - 1);
     for (int64_t o = 0; o < total_odom_; ++o) {
@@ -311,10 +361,21 @@ void Engine::UploadProblem() {
   col_inst_.Upload(col_inst, s);
   frame_inst_.Upload(frame_inst, s);
   frame_col_.Upload(frame_col, s);
-  pt_frame_.Upload(pt_frame, s);
-  pt_xy_.Upload(pt_xy, s);
-  pt_exp_.Upload(pt_exp, s);
-  pt_sw_.Upload(pt_sw, s);
+  if (direct) {
+    const HostProblem& hp = host_[0];
+    const auto rows = static_cast<size_t>(total_points_);
+    const auto keep = static_cast<size_t>(keep_rows);
+    static_assert(sizeof(double2) == 2 * sizeof(double));
+    pt_frame_.UploadKeep(hp.pt_frame.data(), rows, keep, s);
+    pt_xy_.UploadKeep(reinterpret_cast<const double2*>(hp.pt_xy.data()), rows, keep, s);
+    pt_exp_.UploadKeep(hp.pt_expected.data(), rows, keep, s);
+    pt_sw_.UploadKeep(hp.pt_sqrtw.data(), rows, keep, s);
+  } else {
+    pt_frame_.Upload(pt_frame, s);
+    pt_xy_.Upload(pt_xy, s);
+    pt_exp_.Upload(pt_exp, s);
+    pt_sw_.Upload(pt_sw, s);
+  }
   eik_node_.Upload(eik_node, s);
   eik_index_.Upload(eik_index, s);
   eik_n_.Upload(eik_n, s);
@@ -324,7 +385,9 @@ void Engine::UploadProblem() {
   odom_meas_.Upload(odom_meas, s);
   odom_sw_.Upload(odom_sw, s);
   frame_rows_ptr_.Upload(frame_rows_ptr, s);
-  frame_rows_.Upload(frame_rows, s);
+  frame_rows_.UploadKeep(frame_rows.data(), frame_rows.size(),
+                         identity && frame_rows_identity_ ? static_cast<size_t>(keep_rows) : 0, s);
+  frame_rows_identity_ = identity;
   frame_odom_ptr_.Upload(frame_odom_ptr, s);
   frame_odom_.Upload(frame_odom, s);
   pair_f_.Upload(pair_f, s);

@@ -69,6 +69,33 @@ class DevBuf {
       CudaCheck(cudaMemcpyAsync(ptr_, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
     }
   }
+  /// Holds src[0, count) afterwards, of which [0, keep) is on the device
+  /// already: a buffer that has to grow copies that prefix over (with a
+  /// quarter of headroom), then src[keep, count) is uploaded.
+  void UploadKeep(const T* src, size_t count, size_t keep, cudaStream_t s) {
+    keep = std::min(keep, count);
+    if (ptr_ == nullptr) {
+      keep = 0;
+    }
+    if (count > count_ || ptr_ == nullptr) {
+      size_t got = 0;
+      const size_t want = count + count / 4;
+      T* fresh = static_cast<T*>(CachedDeviceAlloc(std::max<size_t>(1, want) * sizeof(T), &got));
+      if (keep > 0) {
+        CudaCheck(cudaMemcpyAsync(fresh, ptr_, keep * sizeof(T), cudaMemcpyDeviceToDevice, s), "keep");
+        // the old block goes back to the cache only after the copy read it
+        CudaCheck(cudaStreamSynchronize(s), "keep");
+      }
+      Free();
+      ptr_ = fresh;
+      bytes_ = got;
+      count_ = got / sizeof(T);
+    }
+    if (count > keep) {
+      CudaCheck(cudaMemcpyAsync(ptr_ + keep, src + keep, (count - keep) * sizeof(T), cudaMemcpyHostToDevice, s),
+                "upload");
+    }
+  }
   T* get() const { return ptr_; }
   [[nodiscard]] size_t size() const { return count_; }
 
@@ -167,6 +194,13 @@ class Engine {
   /// of a problem with the same columns, frames and point rows; the
   /// iterations re-analyse if the state leaves its pattern).
   Engine(HostProblem problem, SymPiece piece);
+  /// Replaces this engine's single problem by `next` on the same grid with
+  /// the same active columns, whose first `keep_rows` point rows are the
+  /// current problem's (they stay on the device; the rest is uploaded). The
+  /// state becomes next's. piece: its analysis, or null to analyse here.
+  void Replace(HostProblem next, SymPiece* piece, int64_t keep_rows);
+  /// True when Replace accepts `next`.
+  [[nodiscard]] bool CanReplace(const HostProblem& next) const;
   ~Engine();
   Engine(const Engine&) = delete;
   Engine& operator=(const Engine&) = delete;
@@ -222,8 +256,11 @@ class Engine {
 
  private:
   void Init(SymPiece* piece);
+  /// The analysis of host_ (or the given piece's structure) while the
+  /// problem uploads (keep_rows of its point rows are on the device).
+  void AnalyzeAndUpload(SymPiece* piece, int64_t keep_rows);
   void BuildLayout();
-  void UploadProblem();
+  void UploadProblem(int64_t keep_rows = 0);
   /// Symbolic analysis of every instance at its current state (host only).
   void AnalyzeHost();
   /// Global structure of the current pieces (a single piece is taken over).
@@ -294,6 +331,7 @@ class Engine {
   DevBuf<int64_t> frame_rows_ptr_, frame_odom_ptr_, pair_ptr_;
   DevBuf<int32_t> frame_rows_, frame_odom_, pair_f_, pair_g_, pair_spec_;
   int num_pairs_{0};
+  bool frame_rows_identity_{false};  // frame_rows_ holds 0, 1, 2, ... (rows ordered by frame)
   // state and per-iteration buffers
   DevBuf<double> map_, poses_, map_backup_, poses_backup_;
   DevBuf<double> pt_rec_, eik_rec_, odom_rec_;

@@ -5,13 +5,16 @@
 // frames so far is rebuilt (map and poses carried over) and solved for
 // `iterations_per_increment` LM iterations on the GPU engine.
 //
-// Per increment the problem is built (optionally by the device builder), a
-// GPU engine is set up for it and solved, and the state comes back to the
-// host for the next build. The next increment's symbolic analysis does not
-// wait for the solve: it runs on a host thread while the GPU iterates, on the
-// problem the next increment would have if the solve left the poses where
-// they are, and the engine checks every iteration that the solved state still
-// lies in that pattern (re-analysing when a point left it).
+// Per increment the problem is built (optionally by the device builder) and
+// replaces the previous one in the same GPU engine: the point rows of the
+// frames already there stay on the device and only the new frames' rows go
+// up. The state comes back to the host for the next build. The next
+// increment's symbolic analysis does not wait for the solve: it runs on a
+// host thread while the GPU iterates, on the problem the next increment
+// would have if the solve left the poses where they are (whose point rows
+// the next build takes over), and the engine checks every iteration that the
+// solved state still lies in that pattern (re-analysing when a point left
+// it).
 #include <chrono>
 #include <cmath>
 #include <future>
@@ -106,10 +109,10 @@ void RunIncremental(const IncrementalInput& in, const sdfgpu_problem_options& po
       poses.push_back(p.theta);
     }
   };
-  auto build = [&](const std::vector<double>& m, const std::vector<double>& poses, int frames) {
+  auto build = [&](const std::vector<double>& m, const std::vector<double>& poses, int frames, bool rows) {
     return BuildProblem(in.nx, in.ny, in.min_x, in.min_y, in.max_x, in.max_y, m.data(), frames, poses.data(),
                         in.scan_offsets, in.scan_xy, odometry.data(), frames - 1, in.num_relations, in.relation_ij,
-                        in.relation_meas, in.relation_sqrt_weight, po, in.build_on_device != 0);
+                        in.relation_meas, in.relation_sqrt_weight, po, BuildMode{in.build_on_device != 0, false, rows});
   };
   sdfgpu_solver_options step_options = so;
   step_options.max_iterations = in.iterations_per_increment;
@@ -121,56 +124,77 @@ void RunIncremental(const IncrementalInput& in, const sdfgpu_problem_options& po
   std::vector<double> hist(static_cast<size_t>(in.iterations_per_increment) + 2);
   int next_frame = 1;
   int increment = 0;
-  // the analysis of the coming increment, started while the GPU iterates,
-  // with the active map it analysed
-  std::future<std::pair<SymPiece, std::vector<int32_t>>> speculative;
+  // The engine stays across steps: each step's problem replaces the last
+  // one's, whose point rows (a prefix of the new rows: rows depend on the
+  // scans alone and come frame by frame) stay on the device.
+  std::unique_ptr<Engine> engine;
+  int64_t engine_rows = 0;
+  // The coming step's pattern-only problem (point rows, active map and pose
+  // pairs at the poses the current step started from) and its analysis,
+  // made on a host thread while the GPU iterates.
+  struct Speculative {
+    HostProblem problem;
+    SymPiece piece;
+  };
+  std::future<Speculative> speculative;
   int speculative_frames = 0;
   while (next_frame < F) {
     const int last = std::min(F, next_frame + in.increment_size);
     append(est, next_frame, last);
     next_frame = last;
     auto t0 = std::chrono::steady_clock::now();
-    HostProblem hp = build(map, est, next_frame);
-    out->phases.build += Seconds(t0);
-    t0 = std::chrono::steady_clock::now();
-    SymPiece piece;
-    bool have_piece = false;
+    Speculative spec;
+    bool have_spec = false;
     if (speculative.valid()) {
-      auto [p, active] = speculative.get();
-      // usable when it analysed the same columns (the active set can move
-      // with the poses when the active region is on)
-      if (speculative_frames == next_frame && active == hp.node_to_active) {
-        piece = std::move(p);
-        have_piece = true;
-        ++out->phases.warm_analyses;
-      }
+      spec = speculative.get();
+      have_spec = speculative_frames == next_frame;
     }
     out->phases.wait_analysis += Seconds(t0);
     t0 = std::chrono::steady_clock::now();
-    std::unique_ptr<Engine> engine;
+    // the device builder leaves out the point rows when the speculative
+    // problem has them (the same rows)
+    const bool rows_given = have_spec && in.build_on_device != 0;
+    HostProblem hp = build(map, est, next_frame, !rows_given);
+    if (rows_given) {
+      hp.pt_frame = std::move(spec.problem.pt_frame);
+      hp.pt_xy = std::move(spec.problem.pt_xy);
+      hp.pt_expected = std::move(spec.problem.pt_expected);
+      hp.pt_sqrtw = std::move(spec.problem.pt_sqrtw);
+    }
+    out->phases.build += Seconds(t0);
+    // the analysis is usable when it analysed the same columns (the active
+    // set can move with the poses when the active region is on)
+    const bool have_piece = have_spec && spec.problem.node_to_active == hp.node_to_active;
     if (have_piece) {
-      engine = std::make_unique<Engine>(std::move(hp), std::move(piece));
+      ++out->phases.warm_analyses;
+    }
+    t0 = std::chrono::steady_clock::now();
+    if (engine != nullptr && engine->CanReplace(hp)) {
+      engine->Replace(std::move(hp), have_piece ? &spec.piece : nullptr, engine_rows);
+    } else if (have_piece) {
+      engine.reset();
+      engine = std::make_unique<Engine>(std::move(hp), std::move(spec.piece));
     } else {
+      engine.reset();
       std::vector<HostProblem> v;
       v.push_back(std::move(hp));
       engine = std::make_unique<Engine>(std::move(v));
     }
+    engine_rows = engine->host(0).num_points();
     out->phases.setup += Seconds(t0);
-    // the next increment's problem if this solve left the poses where they
-    // are (point rows, active map and pose pairs: what the analysis reads),
-    // built and analysed on a host thread while the GPU iterates
     if (in.warm_analysis != 0 && next_frame < F) {
       const int frames = std::min(F, next_frame + in.increment_size);
       std::vector<double> guess = est;
       append(guess, next_frame, frames);
       speculative_frames = frames;
       speculative = std::async(std::launch::async, [&, guess = std::move(guess), frames] {
-        HostProblem next = BuildProblem(in.nx, in.ny, in.min_x, in.min_y, in.max_x, in.max_y, nullptr, frames,
-                                        guess.data(), in.scan_offsets, in.scan_xy, odometry.data(), frames - 1,
-                                        in.num_relations, in.relation_ij, in.relation_meas, in.relation_sqrt_weight,
-                                        po, false, true);
-        SymPiece p = AnalyzeInstance(next, kDefaultMargin);
-        return std::make_pair(std::move(p), std::move(next.node_to_active));
+        Speculative next;
+        next.problem = BuildProblem(in.nx, in.ny, in.min_x, in.min_y, in.max_x, in.max_y, nullptr, frames,
+                                    guess.data(), in.scan_offsets, in.scan_xy, odometry.data(), frames - 1,
+                                    in.num_relations, in.relation_ij, in.relation_meas, in.relation_sqrt_weight, po,
+                                    BuildMode{false, true, true});
+        next.piece = AnalyzeInstance(next.problem, kDefaultMargin);
+        return next;
       });
     }
     t0 = std::chrono::steady_clock::now();
@@ -201,6 +225,9 @@ void RunIncremental(const IncrementalInput& in, const sdfgpu_problem_options& po
       in.snapshot(in.snapshot_user, next_frame, map.data(), est.data());
     }
   }
+  const auto t0 = std::chrono::steady_clock::now();
+  engine.reset();
+  out->phases.teardown += Seconds(t0);
   out->map = std::move(map);
   out->poses = std::move(est);
   out->phases.increments = increment;

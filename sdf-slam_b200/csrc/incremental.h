@@ -40,6 +40,7 @@ struct IncrementalPhases {
   double setup{0};          // engine set-up: upload, analysis (when not overlapped), structure
   double solve{0};          // the LM iterations
   double readback{0};       // state back to the host
+  double teardown{0};       // releasing the step's engine
   double wall{0};           // the whole run
   int increments{0};
   int warm_analyses{0};     // increments whose analysis overlapped the previous solve

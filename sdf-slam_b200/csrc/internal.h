@@ -65,16 +65,26 @@ struct HostProblem {
 /// SDFGPU_ERR_INVALID_ARGUMENT).
 HostProblem FromDesc(const sdfgpu_problem_desc& desc);
 
-/// Problem::Problem (src/problem/problem.cpp:11-115) on the host.
-/// pattern_only (host stages only): no normals and no Eikonal specs, the
-/// fields a symbolic analysis reads and nothing more.
+/// How BuildProblem computes a problem: device_stages runs the point rows,
+/// active maps, normals and Eikonal specs as CUDA kernels (the same values);
+/// pattern_only (host only) stops after what a symbolic analysis reads (no
+/// normals, no Eikonal specs); without rows, the device stages leave the
+/// point rows out of the result (the caller supplies them: they depend on
+/// the scans alone).
+struct BuildMode {
+  bool device_stages{false};
+  bool pattern_only{false};
+  bool rows{true};
+};
+
+/// Problem::Problem (src/problem/problem.cpp:11-115).
 HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_x, double max_y,
                          const double* map_values, int num_frames, const double* poses,
                          const int32_t* scan_offsets, const double* scan_xy,
                          const double* odometry, int num_odometry, int num_relations,
                          const int32_t* relation_ij, const double* relation_meas,
                          const double* relation_sqrt_weight, const sdfgpu_problem_options& options,
-                         bool device_stages = false, bool pattern_only = false);
+                         const BuildMode& mode = BuildMode{});
 
 /// A bucket grid over a point set for exact k-nearest-neighbour search: the
 /// bucket of a point is its clamped cell (floor((p - origin) / cell) per
@@ -111,7 +121,7 @@ void PrepareNormalGrids(const HostProblem& hp, int num_frames, const int32_t* sc
 /// computed by CUDA kernels on the current device from the scans and the
 /// poses, then copied into hp. Same values, bit for bit, as the host stages.
 void DeviceBuildSpecs(HostProblem& hp, int num_frames, const int32_t* scan_offsets, const double* scan_xy,
-                      const sdfgpu_problem_options& options);
+                      const sdfgpu_problem_options& options, bool download_rows = true);
 
 // -------------------------------------------------------------- writers --
 // run_slam's output files and metrics (src/pipeline/runner.cpp:82-192).

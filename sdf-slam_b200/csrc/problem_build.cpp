@@ -486,10 +486,15 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
                          const double* odometry, int num_odometry, int num_relations,
                          const int32_t* relation_ij, const double* relation_meas,
                          const double* relation_sqrt_weight, const sdfgpu_problem_options& o,
-                         bool device_stages, bool pattern_only) {
+                         const BuildMode& mode) {
+  const bool device_stages = mode.device_stages;
+  const bool pattern_only = mode.pattern_only;
   auto bad = [](const std::string& m) { Fail(SDFGPU_ERR_INVALID_ARGUMENT, m); };
   if (device_stages && pattern_only) {
     bad("a pattern-only build runs on the host");
+  }
+  if (!mode.rows && !device_stages) {
+    bad("the host stages always build the point rows");
   }
   if (nx < 2 || ny < 2 || !(max_x > min_x) || !(max_y > min_y)) {
     bad("GridMap needs nx, ny >= 2 and max > min");
@@ -607,7 +612,7 @@ HostProblem BuildProblem(int nx, int ny, double min_x, double min_y, double max_
   } else if (device_stages) {
     // point specs, active maps, node normals and the Eikonal spec list by
     // CUDA kernels
-    DeviceBuildSpecs(hp, num_frames, scan_offsets, scan_xy, o);
+    DeviceBuildSpecs(hp, num_frames, scan_offsets, scan_xy, o, mode.rows);
   } else {
   const double sqrt_we = std::sqrt(o.weight_eikonal);
   for (int h = 0; h + 1 < ny; ++h) {

@@ -613,7 +613,7 @@ void Download(std::vector<T>& dst, const T* src, size_t count, cudaStream_t s) {
 }  // namespace
 
 void DeviceBuildSpecs(HostProblem& hp, int num_frames, const int32_t* scan_offsets, const double* scan_xy,
-                      const sdfgpu_problem_options& o) {
+                      const sdfgpu_problem_options& o, bool download_rows) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
@@ -819,10 +819,12 @@ void DeviceBuildSpecs(HostProblem& hp, int num_frames, const int32_t* scan_offse
                                                  std::sqrt(o.weight_eikonal), d_eik_wh.get(), d_eik_n.get(),
                                                  d_eik_sw.get());
   CudaCheck(cudaGetLastError(), "device builder kernels");
-  Download(hp.pt_frame, d_pt_frame.get(), static_cast<size_t>(rows), s);
-  Download(hp.pt_xy, d_pt_xy.get(), 2 * static_cast<size_t>(rows), s);
-  Download(hp.pt_expected, d_pt_exp.get(), static_cast<size_t>(rows), s);
-  Download(hp.pt_sqrtw, d_pt_sw.get(), static_cast<size_t>(rows), s);
+  if (download_rows) {
+    Download(hp.pt_frame, d_pt_frame.get(), static_cast<size_t>(rows), s);
+    Download(hp.pt_xy, d_pt_xy.get(), 2 * static_cast<size_t>(rows), s);
+    Download(hp.pt_expected, d_pt_exp.get(), static_cast<size_t>(rows), s);
+    Download(hp.pt_sqrtw, d_pt_sw.get(), static_cast<size_t>(rows), s);
+  }
   Download(hp.node_to_active, d_n2a.get(), static_cast<size_t>(nodes), s);
   Download(hp.active_to_node, d_a2n.get(), static_cast<size_t>(num_active), s);
   Download(hp.eik_wh, d_eik_wh.get(), 2 * static_cast<size_t>(num_eik), s);
