@@ -319,10 +319,13 @@ typedef struct sdfgpu_incremental_desc {
  * poses_out (3 * num_frames) receive the final state, total the summed
  * result; cost_history (may be NULL) receives the first `capacity` entries
  * of the concatenated histories (total->cost_history_length of them).
- * phases (9 doubles, may be NULL): host seconds spent building problems,
- * waiting for overlapped analyses, setting engines up, iterating, reading
- * state back and releasing engines, the run's wall time, the number of steps
- * and the number of steps whose analysis overlapped the previous step. Fails with the step's
+ * phases (12 doubles, may be NULL): host seconds spent building problems,
+ * waiting for overlapped analyses, setting the engine up, iterating, reading
+ * state back and releasing the engine, the run's wall time, the number of
+ * steps, the number of steps whose analysis overlapped the previous step,
+ * the pattern re-analyses inside the iterations, their host seconds and the
+ * host seconds spent capturing iteration graphs (both part of iterating).
+ * Fails with the step's
  * status (SDFGPU_ERR_NUMERICAL for a failed factorization) and stops there. */
 int sdfgpu_run_incremental(const sdfgpu_incremental_desc* desc, const sdfgpu_problem_options* problem_options,
                            const sdfgpu_solver_options* solver_options, double* map_out, double* poses_out,

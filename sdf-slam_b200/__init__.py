@@ -483,7 +483,7 @@ def run_incremental(nx, ny, min_corner, max_corner, poses, scans, options: Probl
     steps = -(-max(len(poses) - 1, 0) // max(int(increment_size), 1))
     cap = steps * (max(int(iterations_per_increment), 0) + 2)
     hist = np.zeros(max(cap, 1))
-    ph = np.zeros(9)
+    ph = np.zeros(12)
     _check(L.sdfgpu_run_incremental(ctypes.byref(d), ctypes.byref(po), ctypes.byref(so), _d(map_out),
                                     _d(poses_out), ctypes.byref(total), _d(hist), cap, _d(ph)))
     res = SolveResult(bool(total.converged), int(total.iterations), total.initial_cost, total.final_cost,
@@ -492,6 +492,9 @@ def run_incremental(nx, ny, min_corner, max_corner, poses, scans, options: Probl
     phases = dict(zip(keys, ph[:7].tolist()))
     phases["increments"] = int(ph[7])
     phases["warm_analyses"] = int(ph[8])
+    phases["reanalyses"] = int(ph[9])
+    phases["reanalysis"] = float(ph[10])
+    phases["capture"] = float(ph[11])
     return IncrementalResult(map_out, poses_out, res, phases)
 
 

@@ -427,9 +427,10 @@ int sdfgpu_run_incremental(const sdfgpu_incremental_desc* desc, const sdfgpu_pro
     total->status = SDFGPU_OK;
     if (phases != nullptr) {
       const sdfgpu::IncrementalPhases& p = out.phases;
-      const double v[9] = {p.build,    p.wait_analysis, p.setup, p.solve, p.readback, p.teardown, p.wall,
-                           static_cast<double>(p.increments), static_cast<double>(p.warm_analyses)};
-      std::copy(v, v + 9, phases);
+      const double v[12] = {p.build,    p.wait_analysis, p.setup, p.solve, p.readback, p.teardown, p.wall,
+                            static_cast<double>(p.increments), static_cast<double>(p.warm_analyses),
+                            static_cast<double>(p.reanalyses), p.reanalysis, p.capture};
+      std::copy(v, v + 12, phases);
     }
   });
 }

@@ -201,6 +201,9 @@ void RunIncremental(const IncrementalInput& in, const sdfgpu_problem_options& po
     sdfgpu_solve_result step{};
     engine->Solve({step_options}, &step, hist.data(), static_cast<int>(hist.size()));
     out->phases.solve += Seconds(t0);
+    out->phases.reanalyses += engine->times().reanalyses;
+    out->phases.reanalysis += engine->times().reanalysis_host;
+    out->phases.capture += engine->times().capture_host;
     if (step.status != SDFGPU_OK) {
       if (speculative.valid()) {
         speculative.wait();

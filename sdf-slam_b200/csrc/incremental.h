@@ -44,6 +44,9 @@ struct IncrementalPhases {
   double wall{0};           // the whole run
   int increments{0};
   int warm_analyses{0};     // increments whose analysis overlapped the previous solve
+  int reanalyses{0};        // pattern re-analyses inside the steps' iterations
+  double reanalysis{0};     // host seconds of those re-analyses (part of solve)
+  double capture{0};        // host seconds capturing iteration graphs (part of solve)
 };
 
 struct IncrementalOutput {
