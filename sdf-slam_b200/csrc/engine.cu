@@ -278,8 +278,18 @@ void Engine::UploadProblem(int64_t keep_rows) {
       frame_col[static_cast<size_t>(L.frame_off + f)] = f >= 1 ? L.col_off + hp.num_active() + 3 * (f - 1) : -1;
     }
     if (direct) {
-      for (const int32_t f : hp.pt_frame) {
-        ++frame_rows_ptr[static_cast<size_t>(f) + 1];
+      // rows ordered by frame (as the builders emit them): the frame ranges
+      // by binary search, else counted
+      if (std::is_sorted(hp.pt_frame.begin(), hp.pt_frame.end())) {
+        for (int f = 0; f < hp.num_frames(); ++f) {
+          frame_rows_ptr[static_cast<size_t>(f) + 1] = static_cast<int64_t>(
+              std::upper_bound(hp.pt_frame.begin(), hp.pt_frame.end(), f) -
+              std::lower_bound(hp.pt_frame.begin(), hp.pt_frame.end(), f));
+        }
+      } else {
+        for (const int32_t f : hp.pt_frame) {
+          ++frame_rows_ptr[static_cast<size_t>(f) + 1];
+        }
       }
     } else {
       for (int k = 0; k < hp.num_points(); ++k) {

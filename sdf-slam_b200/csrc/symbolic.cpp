@@ -628,15 +628,26 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
     S.allow_off[0] = 0;
     S.allow_words[0] = words;
     S.allow_bits.assign(static_cast<size_t>(words) * Fr, 0u);
+    // the rows of each frame; rows ordered by frame (as the builders emit
+    // them) index themselves and their frame ranges come from binary
+    // searches, other rows are counting-sorted
+    const bool by_frame = std::is_sorted(hp.pt_frame.begin(), hp.pt_frame.end());
     std::vector<int> fptr(static_cast<size_t>(Fr) + 1, 0);
-    for (const int32_t f : hp.pt_frame) {
-      ++fptr[static_cast<size_t>(f) + 1];
+    if (by_frame) {
+      for (int f = 0; f <= Fr; ++f) {
+        fptr[static_cast<size_t>(f)] = static_cast<int>(
+            std::lower_bound(hp.pt_frame.begin(), hp.pt_frame.end(), f) - hp.pt_frame.begin());
+      }
+    } else {
+      for (const int32_t f : hp.pt_frame) {
+        ++fptr[static_cast<size_t>(f) + 1];
+      }
+      for (int f = 0; f < Fr; ++f) {
+        fptr[static_cast<size_t>(f) + 1] += fptr[static_cast<size_t>(f)];
+      }
     }
-    for (int f = 0; f < Fr; ++f) {
-      fptr[static_cast<size_t>(f) + 1] += fptr[static_cast<size_t>(f)];
-    }
-    std::vector<int> fpts(hp.pt_frame.size());
-    {
+    std::vector<int> fpts(by_frame ? 0 : hp.pt_frame.size());
+    if (!by_frame) {
       std::vector<int> fill(fptr.begin(), fptr.end() - 1);
       for (size_t q = 0; q < hp.pt_frame.size(); ++q) {
         fpts[static_cast<size_t>(fill[static_cast<size_t>(hp.pt_frame[q])]++)] = static_cast<int>(q);
@@ -663,7 +674,7 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
         const double sn = std::sin(pose[2]);
         std::fill(occ.begin(), occ.end(), uint64_t{0});
         for (int q = fptr[static_cast<size_t>(f)]; q < fptr[static_cast<size_t>(f) + 1]; ++q) {
-          const size_t pt = static_cast<size_t>(fpts[static_cast<size_t>(q)]);
+          const size_t pt = static_cast<size_t>(by_frame ? q : fpts[static_cast<size_t>(q)]);
           const double px = hp.pt_xy[2 * pt];
           const double py = hp.pt_xy[2 * pt + 1];
           const double gx = (c * px + (-sn) * py) + pose[0];
