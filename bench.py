@@ -371,7 +371,7 @@ def run_serve(P, args):
 # KInvertDiagonal) in one LM iteration, from one ncu capture of
 # `profile_run.py floorplan 2` (default schedule); L2 is not flushed inside
 # that capture, so writes that stay in L2 are not counted.
-FACTOR_TRAFFIC_BYTES = {"floorplan": 114.5e6}
+FACTOR_TRAFFIC_BYTES = {"floorplan": 126.3e6}
 
 
 def run_gpu(args, dist, world, rank, local):

@@ -497,7 +497,7 @@ Symbolic Engine::GlobalStructure() {
   if (pieces_.size() == 1) {
     return ConcatenateOne(std::move(pieces_[0]), 32, 64, sched_);
   }
-  return Concatenate(pieces_, layout_, 32, 64, sched_);
+  return Concatenate(pieces_, layout_, 32, 64, sched_, std::move(sym_));
 }
 
 void Engine::UploadSymbolic() {

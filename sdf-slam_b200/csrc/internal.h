@@ -262,9 +262,14 @@ struct SymPiece {
   int margin{0};            // coupling dilation (cells) the piece was built with
 };
 
-/// Coupling dilation (cells) of a first analysis (3: the 76-pose floor plan
-/// runs 100 LM iterations without leaving it, at 7 % more factor flops than 2).
-constexpr int kDefaultMargin = 3;
+/// Coupling dilation (cells) of a first analysis. 5: in a batch of 64
+/// uneven instances some instance leaves a 3-cell pattern in most early
+/// iterations, and each re-analysis re-concatenates and re-uploads every
+/// instance's structure (B200: 4 re-analyses in 20 iterations instead of 11,
+/// 1717 against 1081 LM iterations/s); the floor plan's iteration costs
+/// 0.7 % more than at 3. The same for one instance as for a batch, so that a
+/// problem follows the same steps alone and in a batch.
+constexpr int kDefaultMargin = 5;
 /// Growth of the dilation at each re-analysis, and its cap.
 constexpr int kMarginStep = 2;
 constexpr int kMaxMargin = 7;
@@ -295,9 +300,10 @@ struct Schedule {
 };
 
 /// Global structure (task lists, level schedule) of pieces laid out by
-/// `layout`.
+/// `layout`. `recycle` (a previous result, may be empty) lends its large
+/// arrays, so that a re-concatenation writes into memory already mapped.
 Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<InstanceLayout>& layout,
-                     int panel_width, int tile, const Schedule& sched = Schedule{});
+                     int panel_width, int tile, const Schedule& sched = Schedule{}, Symbolic recycle = Symbolic{});
 
 /// Concatenate for a single instance: takes the piece's arrays over instead
 /// of copying them (the piece is left empty).

@@ -944,118 +944,139 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
 }
 
 Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<InstanceLayout>& layout,
-                     int panel_width, int tile, const Schedule& sched) {
+                     int panel_width, int tile, const Schedule& sched, Symbolic recycle) {
   Symbolic S;
+  // every element of these arrays is written below; resizing a recycled
+  // array initializes only growth
+  S.perm = std::move(recycle.perm);
+  S.pinv = std::move(recycle.pinv);
+  S.col_owner = std::move(recycle.col_owner);
+  S.sn = std::move(recycle.sn);
+  S.sn_rows = std::move(recycle.sn_rows);
+  S.sn_rel = std::move(recycle.sn_rel);
+  S.child_list = std::move(recycle.child_list);
+  S.mm_off = std::move(recycle.mm_off);
+  S.mp_frame = std::move(recycle.mp_frame);
+  S.mp_off = std::move(recycle.mp_off);
+  S.allow_bits = std::move(recycle.allow_bits);
+  S.fmp_col = std::move(recycle.fmp_col);
+  S.fmp_off = std::move(recycle.fmp_off);
   S.small_pivots = sched.small_pivots;
   S.front_rows = sched.front_rows;
   S.panel_rows = sched.panel_rows;
-  int n = 0;
-  size_t nsn = 0;
-  size_t nrows = 0;
-  size_t nchild = 0;
-  size_t nmp = 0;
-  size_t nallow = 0;
-  for (const SymPiece& p : pieces) {
-    n += p.s.n;
-    nsn += p.s.sn.size();
-    nrows += p.s.sn_rows.size();
-    nchild += p.s.child_list.size();
-    nmp += p.s.mp_frame.size();
-    nallow += p.s.allow_bits.size();
-  }
   const size_t I = pieces.size();
-  S.n = n;
-  S.perm.resize(static_cast<size_t>(n));
-  S.pinv.resize(static_cast<size_t>(n));
-  S.col_owner.resize(static_cast<size_t>(n));
-  S.sn.reserve(nsn);
-  S.sn_rows.reserve(nrows);
-  S.sn_rel.reserve(nrows);
-  S.child_list.reserve(nchild);
-  S.mm_off.resize(static_cast<size_t>(n) * 9);
-  S.mp_ptr.assign(static_cast<size_t>(n) + 1, 0);
-  S.mp_frame.reserve(nmp);
-  S.mp_off.reserve(nmp);
-  S.allow_bits.reserve(nallow);
+  // where each instance's part starts in every global array (a prefix pass),
+  // then the parts are copied and rebased in parallel
+  struct Base {
+    int32_t sn;
+    int64_t rows;
+    int32_t child;
+    int64_t front;
+    int64_t upd;
+    int64_t mp;
+    int64_t allow;
+    int64_t fmp;
+  };
+  std::vector<Base> base(I);
+  Base t{0, 0, 0, 0, 0, 0, 0, 0};
+  int n = 0;
+  int frames = 0;
   S.allow_off.assign(I, 0);
   S.allow_words.assign(I, 0);
   S.pp_base.assign(I, -1);
   S.pp_ld.assign(I, 0);
   S.pp_first.assign(I, 0);
-  int frames = 0;
-  for (size_t i = 0; i < I; ++i) {
-    frames = std::max(frames, layout[i].frame_off + static_cast<int>(pieces[i].s.fmp_ptr.size()) - 1);
-  }
-  S.fmp_ptr.assign(static_cast<size_t>(frames) + 1, 0);
-  S.fmp_col.reserve(nmp);
-  S.fmp_off.reserve(nmp);
-  std::vector<int> height;
-  height.reserve(nsn);
   for (size_t i = 0; i < I; ++i) {
     const Symbolic& L = pieces[i].s;
+    base[i] = t;
+    t.sn += static_cast<int32_t>(L.sn.size());
+    t.rows += static_cast<int64_t>(L.sn_rows.size());
+    t.child += static_cast<int32_t>(L.child_list.size());
+    t.front += L.front_doubles;
+    t.upd += L.update_doubles;
+    t.mp += static_cast<int64_t>(L.mp_frame.size());
+    t.allow += static_cast<int64_t>(L.allow_bits.size());
+    t.fmp += static_cast<int64_t>(L.fmp_col.size());
+    n += L.n;
+    frames = std::max(frames, layout[i].frame_off + static_cast<int>(L.fmp_ptr.size()) - 1);
+    S.total_flops += L.total_flops;
+    S.allow_off[i] = base[i].allow;
+    S.allow_words[i] = L.allow_words[0];
+    S.pp_base[i] = L.pp_base[0] >= 0 ? L.pp_base[0] + base[i].front : -1;
+    S.pp_ld[i] = L.pp_ld[0];
+    S.pp_first[i] = L.pp_first[0];
+  }
+  S.n = n;
+  S.front_doubles = t.front;
+  S.update_doubles = t.upd;
+  S.perm.resize(static_cast<size_t>(n));
+  S.pinv.resize(static_cast<size_t>(n));
+  S.col_owner.resize(static_cast<size_t>(n));
+  S.sn.resize(static_cast<size_t>(t.sn));
+  S.sn_rows.resize(static_cast<size_t>(t.rows));
+  S.sn_rel.resize(static_cast<size_t>(t.rows));
+  S.child_list.resize(static_cast<size_t>(t.child));
+  S.mm_off.resize(static_cast<size_t>(n) * 9);
+  S.mp_ptr.assign(static_cast<size_t>(n) + 1, 0);
+  S.mp_frame.resize(static_cast<size_t>(t.mp));
+  S.mp_off.resize(static_cast<size_t>(t.mp));
+  S.allow_bits.resize(static_cast<size_t>(t.allow));
+  S.fmp_ptr.assign(static_cast<size_t>(frames) + 1, 0);
+  S.fmp_col.resize(static_cast<size_t>(t.fmp));
+  S.fmp_off.resize(static_cast<size_t>(t.fmp));
+  std::vector<int> height(static_cast<size_t>(t.sn));
+  PoolRun(static_cast<int>(I), [&](int part) {
+    const auto i = static_cast<size_t>(part);
+    const Symbolic& L = pieces[i].s;
+    const Base& B = base[i];
     const int col_off = layout[i].col_off;
-    const int32_t s0 = static_cast<int32_t>(S.sn.size());
-    const int64_t f0 = S.front_doubles;
-    const int64_t u0 = S.update_doubles;
-    const int64_t r0 = static_cast<int64_t>(S.sn_rows.size());
-    const int32_t c0 = static_cast<int32_t>(S.child_list.size());
     for (int k = 0; k < L.n; ++k) {
       S.perm[static_cast<size_t>(col_off + k)] = col_off + L.perm[static_cast<size_t>(k)];
       S.pinv[static_cast<size_t>(col_off + k)] = col_off + L.pinv[static_cast<size_t>(k)];
-      S.col_owner[static_cast<size_t>(col_off + k)] = s0 + L.col_owner[static_cast<size_t>(k)];
+      S.col_owner[static_cast<size_t>(col_off + k)] = B.sn + L.col_owner[static_cast<size_t>(k)];
     }
-    for (SupernodeRec r : L.sn) {
-      r.front_off += f0;
-      r.rows_off += r0;
-      r.upd_off += u0;
+    for (size_t q = 0; q < L.sn.size(); ++q) {
+      SupernodeRec r = L.sn[q];
+      r.front_off += B.front;
+      r.rows_off += B.rows;
+      r.upd_off += B.upd;
       r.first_col += col_off;
-      r.child_begin += c0;
-      r.parent = r.parent >= 0 ? r.parent + s0 : -1;
+      r.child_begin += B.child;
+      r.parent = r.parent >= 0 ? r.parent + B.sn : -1;
       r.instance = static_cast<int32_t>(i);
-      S.sn.push_back(r);
+      S.sn[static_cast<size_t>(B.sn) + q] = r;
+      height[static_cast<size_t>(B.sn) + q] = pieces[i].height[q];
     }
-    for (const int32_t row : L.sn_rows) {
-      S.sn_rows.push_back(col_off + row);
+    for (size_t q = 0; q < L.sn_rows.size(); ++q) {
+      S.sn_rows[static_cast<size_t>(B.rows) + q] = col_off + L.sn_rows[q];
     }
-    S.sn_rel.insert(S.sn_rel.end(), L.sn_rel.begin(), L.sn_rel.end());
-    for (const int32_t c : L.child_list) {
-      S.child_list.push_back(s0 + c);
+    std::copy(L.sn_rel.begin(), L.sn_rel.end(), S.sn_rel.begin() + B.rows);
+    for (size_t q = 0; q < L.child_list.size(); ++q) {
+      S.child_list[static_cast<size_t>(B.child) + q] = B.sn + L.child_list[q];
     }
-    height.insert(height.end(), pieces[i].height.begin(), pieces[i].height.end());
-    S.front_doubles += L.front_doubles;
-    S.update_doubles += L.update_doubles;
-    S.total_flops += L.total_flops;
     for (size_t q = 0; q < L.mm_off.size(); ++q) {
       const int64_t v = L.mm_off[q];
-      S.mm_off[static_cast<size_t>(col_off) * 9 + q] = v >= 0 ? v + f0 : -1;
+      S.mm_off[static_cast<size_t>(col_off) * 9 + q] = v >= 0 ? v + B.front : -1;
     }
-    const int64_t m0 = static_cast<int64_t>(S.mp_frame.size());
     for (int k = 0; k < L.n; ++k) {
-      S.mp_ptr[static_cast<size_t>(col_off + k) + 1] = m0 + L.mp_ptr[static_cast<size_t>(k) + 1];
+      S.mp_ptr[static_cast<size_t>(col_off + k) + 1] = B.mp + L.mp_ptr[static_cast<size_t>(k) + 1];
     }
-    S.mp_frame.insert(S.mp_frame.end(), L.mp_frame.begin(), L.mp_frame.end());
-    for (const int64_t v : L.mp_off) {
-      S.mp_off.push_back(v + f0);
+    std::copy(L.mp_frame.begin(), L.mp_frame.end(), S.mp_frame.begin() + B.mp);
+    for (size_t q = 0; q < L.mp_off.size(); ++q) {
+      S.mp_off[static_cast<size_t>(B.mp) + q] = L.mp_off[q] + B.front;
     }
-    S.allow_off[i] = static_cast<int64_t>(S.allow_bits.size());
-    S.allow_words[i] = L.allow_words[0];
-    S.allow_bits.insert(S.allow_bits.end(), L.allow_bits.begin(), L.allow_bits.end());
-    S.pp_base[i] = L.pp_base[0] >= 0 ? L.pp_base[0] + f0 : -1;
-    S.pp_ld[i] = L.pp_ld[0];
-    S.pp_first[i] = L.pp_first[0];
-    // instances are laid out in frame order, so frames fill fmp_ptr in order
-    const int64_t q0 = static_cast<int64_t>(S.fmp_col.size());
+    std::copy(L.allow_bits.begin(), L.allow_bits.end(), S.allow_bits.begin() + B.allow);
+    // instances are laid out in frame order, so their frame ranges are
+    // disjoint
     const int fr = static_cast<int>(L.fmp_ptr.size()) - 1;
     for (int f = 0; f < fr; ++f) {
-      S.fmp_ptr[static_cast<size_t>(layout[i].frame_off + f) + 1] = q0 + L.fmp_ptr[static_cast<size_t>(f) + 1];
+      S.fmp_ptr[static_cast<size_t>(layout[i].frame_off + f) + 1] = B.fmp + L.fmp_ptr[static_cast<size_t>(f) + 1];
     }
-    for (const int32_t c : L.fmp_col) {
-      S.fmp_col.push_back(col_off + c);
+    for (size_t q = 0; q < L.fmp_col.size(); ++q) {
+      S.fmp_col[static_cast<size_t>(B.fmp) + q] = col_off + L.fmp_col[q];
+      S.fmp_off[static_cast<size_t>(B.fmp) + q] = L.fmp_off[q] + B.front;
     }
-    for (const int64_t v : L.fmp_off) {
-      S.fmp_off.push_back(v + f0);
-    }
-  }
+  });
   Finalize(S, height, panel_width, tile);
   return S;
 }

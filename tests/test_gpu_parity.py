@@ -201,9 +201,10 @@ def test_state_outside_pattern_reanalyses_only_that_instance():
            for s, g, f, b in [(20, 44, 9, 120), (21, 48, 11, 150), (22, 40, 8, 90)]]
     specs = [scene_specs(sc, P.ProblemOptions(hallucination_points=3))[0] for sc in scs]
     batch = P.Problem.batch(specs)
+    batch.cost(0)  # the device problem and its analysis at the scenes' poses
     m1, p1 = batch.state(1)
     moved = p1.copy()
-    moved[1:, 0] += 0.9
+    moved[1:, 0] += 1.7  # beyond the 5-cell coupling margin of 0.25 m cells
     moved[1:, 2] += 0.05
     batch.set_state(m1, moved, index=1)
     opts = P.SolverOptions(max_iterations=4)
@@ -212,6 +213,7 @@ def test_state_outside_pattern_reanalyses_only_that_instance():
     for i, s in enumerate(specs):
         single = P.Problem.from_specs(s)
         if i == 1:
+            single.cost()
             single.set_state(m1, moved)
         r1 = P.solve(single, opts)
         assert rb[i].cost_history == r1.cost_history
