@@ -9,12 +9,14 @@
 // owner whose stream has drained, so a reused block has no work in flight.
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <deque>
 #include <map>
 #include <mutex>
 #include <vector>
 
 #include "engine.h"
+#include "host_pool.h"
 
 namespace sdfgpu {
 
@@ -172,5 +174,61 @@ void* CachedHostAlloc(size_t bytes, size_t* got) {
 }
 
 void CachedHostFree(void* p, size_t cls) { Keep(-1, cls, p, kMaxCachedHost); }
+
+namespace {
+
+// Copies below this size go straight from pageable memory (a few MB move
+// about as fast either way); larger ones are staged in chunks of kStageBytes.
+constexpr size_t kStageThreshold = size_t{4} << 20;
+constexpr size_t kStageBytes = size_t{16} << 20;
+
+/// Two pinned staging buffers with an event each (the transfer last
+/// enqueued from it), shared by the process; one upload at a time.
+struct Staging {
+  std::mutex mu;
+  void* buf[2]{nullptr, nullptr};
+  cudaEvent_t done[2]{nullptr, nullptr};
+  bool ready{false};
+};
+
+Staging& TheStaging() {
+  static Staging* st = new Staging;  // kept for the life of the process
+  return *st;
+}
+
+}  // namespace
+
+void UploadAsync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+  if (bytes < kStageThreshold) {
+    CudaCheck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "upload");
+    return;
+  }
+  Staging& st = TheStaging();
+  const std::lock_guard<std::mutex> lock(st.mu);
+  if (!st.ready) {
+    for (int b = 0; b < 2; ++b) {
+      CudaCheck(cudaMallocHost(&st.buf[b], kStageBytes), "staging buffer");
+      CudaCheck(cudaEventCreateWithFlags(&st.done[b], cudaEventDisableTiming), "staging event");
+    }
+    st.ready = true;
+  }
+  const auto* from = static_cast<const char*>(src);
+  auto* to = static_cast<char*>(dst);
+  for (size_t off = 0, k = 0; off < bytes; off += kStageBytes, ++k) {
+    const size_t len = std::min(kStageBytes, bytes - off);
+    const int b = static_cast<int>(k & 1);
+    // the buffer's previous transfer has read it
+    CudaCheck(cudaEventSynchronize(st.done[b]), "staging wait");
+    char* stage = static_cast<char*>(st.buf[b]);
+    constexpr size_t kPiece = size_t{2} << 20;
+    const int pieces = static_cast<int>((len + kPiece - 1) / kPiece);
+    PoolRun(pieces, [&](int p) {
+      const size_t a = static_cast<size_t>(p) * kPiece;
+      std::memcpy(stage + a, from + off + a, std::min(kPiece, len - a));
+    });
+    CudaCheck(cudaMemcpyAsync(to + off, stage, len, cudaMemcpyHostToDevice, s), "upload");
+    CudaCheck(cudaEventRecord(st.done[b], s), "staging event");
+  }
+}
 
 }  // namespace sdfgpu

@@ -31,6 +31,12 @@ void CachedDeviceFree(void* p, size_t bytes);
 void* CachedHostAlloc(size_t bytes, size_t* got);
 void CachedHostFree(void* p, size_t bytes);
 
+/// Host-to-device copy of `bytes` from pageable memory, enqueued on `s`.
+/// Large copies go through two pinned staging buffers, filled by the host
+/// pool's threads while the other buffer's transfer runs; `src` may be
+/// reused as soon as this returns.
+void UploadAsync(void* dst, const void* src, size_t bytes, cudaStream_t s);
+
 /// Owning device buffer. Owners free (or grow) it only after their stream
 /// has drained.
 template <typename T>
@@ -66,7 +72,7 @@ class DevBuf {
   void Upload(const std::vector<T>& v, cudaStream_t s) {
     Alloc(v.size());
     if (!v.empty()) {
-      CudaCheck(cudaMemcpyAsync(ptr_, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
+      UploadAsync(ptr_, v.data(), v.size() * sizeof(T), s);
     }
   }
   /// Holds src[0, count) afterwards, of which [0, keep) is on the device
@@ -92,8 +98,7 @@ class DevBuf {
       count_ = got / sizeof(T);
     }
     if (count > keep) {
-      CudaCheck(cudaMemcpyAsync(ptr_ + keep, src + keep, (count - keep) * sizeof(T), cudaMemcpyHostToDevice, s),
-                "upload");
+      UploadAsync(ptr_ + keep, src + keep, (count - keep) * sizeof(T), s);
     }
   }
   T* get() const { return ptr_; }
