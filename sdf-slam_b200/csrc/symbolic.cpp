@@ -943,6 +943,23 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
   return piece;
 }
 
+namespace {
+
+/// Sizes a recycled array for n elements that are all written afterwards:
+/// one too small is replaced (its contents are not copied) by one with half
+/// again the room, so that the next growth fits.
+template <typename T>
+void Regrow(std::vector<T>& v, size_t n) {
+  if (v.capacity() < n) {
+    std::vector<T> fresh;
+    fresh.reserve(n + n / 2);
+    v.swap(fresh);
+  }
+  v.resize(n);
+}
+
+}  // namespace
+
 Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<InstanceLayout>& layout,
                      int panel_width, int tile, const Schedule& sched, Symbolic recycle) {
   Symbolic S;
@@ -1009,21 +1026,21 @@ Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<Inst
   S.n = n;
   S.front_doubles = t.front;
   S.update_doubles = t.upd;
-  S.perm.resize(static_cast<size_t>(n));
-  S.pinv.resize(static_cast<size_t>(n));
-  S.col_owner.resize(static_cast<size_t>(n));
-  S.sn.resize(static_cast<size_t>(t.sn));
-  S.sn_rows.resize(static_cast<size_t>(t.rows));
-  S.sn_rel.resize(static_cast<size_t>(t.rows));
-  S.child_list.resize(static_cast<size_t>(t.child));
-  S.mm_off.resize(static_cast<size_t>(n) * 9);
+  Regrow(S.perm, static_cast<size_t>(n));
+  Regrow(S.pinv, static_cast<size_t>(n));
+  Regrow(S.col_owner, static_cast<size_t>(n));
+  Regrow(S.sn, static_cast<size_t>(t.sn));
+  Regrow(S.sn_rows, static_cast<size_t>(t.rows));
+  Regrow(S.sn_rel, static_cast<size_t>(t.rows));
+  Regrow(S.child_list, static_cast<size_t>(t.child));
+  Regrow(S.mm_off, static_cast<size_t>(n) * 9);
   S.mp_ptr.assign(static_cast<size_t>(n) + 1, 0);
-  S.mp_frame.resize(static_cast<size_t>(t.mp));
-  S.mp_off.resize(static_cast<size_t>(t.mp));
-  S.allow_bits.resize(static_cast<size_t>(t.allow));
+  Regrow(S.mp_frame, static_cast<size_t>(t.mp));
+  Regrow(S.mp_off, static_cast<size_t>(t.mp));
+  Regrow(S.allow_bits, static_cast<size_t>(t.allow));
   S.fmp_ptr.assign(static_cast<size_t>(frames) + 1, 0);
-  S.fmp_col.resize(static_cast<size_t>(t.fmp));
-  S.fmp_off.resize(static_cast<size_t>(t.fmp));
+  Regrow(S.fmp_col, static_cast<size_t>(t.fmp));
+  Regrow(S.fmp_off, static_cast<size_t>(t.fmp));
   std::vector<int> height(static_cast<size_t>(t.sn));
   PoolRun(static_cast<int>(I), [&](int part) {
     const auto i = static_cast<size_t>(part);
