@@ -16,7 +16,6 @@
 #include <vector>
 
 #include "engine.h"
-#include "host_pool.h"
 
 namespace sdfgpu {
 
@@ -183,7 +182,9 @@ constexpr size_t kStageThreshold = size_t{4} << 20;
 constexpr size_t kStageBytes = size_t{16} << 20;
 
 /// Two pinned staging buffers with an event each (the transfer last
-/// enqueued from it), shared by the process; one upload at a time.
+/// enqueued from it). A few such slots serve the process; an upload takes a
+/// free one or, when all are busy on other threads, copies from pageable
+/// memory instead of waiting.
 struct Staging {
   std::mutex mu;
   void* buf[2]{nullptr, nullptr};
@@ -191,9 +192,11 @@ struct Staging {
   bool ready{false};
 };
 
-Staging& TheStaging() {
-  static Staging* st = new Staging;  // kept for the life of the process
-  return *st;
+constexpr int kStagingSlots = 3;
+
+Staging* TheStaging() {
+  static Staging* st = new Staging[kStagingSlots];  // kept for the life of the process
+  return st;
 }
 
 }  // namespace
@@ -203,8 +206,19 @@ void UploadAsync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     CudaCheck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "upload");
     return;
   }
-  Staging& st = TheStaging();
-  const std::lock_guard<std::mutex> lock(st.mu);
+  Staging* slots = TheStaging();
+  int slot = -1;
+  for (int k = 0; k < kStagingSlots && slot < 0; ++k) {
+    if (slots[k].mu.try_lock()) {
+      slot = k;
+    }
+  }
+  if (slot < 0) {
+    CudaCheck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "upload");
+    return;
+  }
+  Staging& st = slots[slot];
+  const std::lock_guard<std::mutex> lock(st.mu, std::adopt_lock);
   if (!st.ready) {
     for (int b = 0; b < 2; ++b) {
       CudaCheck(cudaMallocHost(&st.buf[b], kStageBytes), "staging buffer");
@@ -219,13 +233,9 @@ void UploadAsync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     const int b = static_cast<int>(k & 1);
     // the buffer's previous transfer has read it
     CudaCheck(cudaEventSynchronize(st.done[b]), "staging wait");
-    char* stage = static_cast<char*>(st.buf[b]);
-    constexpr size_t kPiece = size_t{2} << 20;
-    const int pieces = static_cast<int>((len + kPiece - 1) / kPiece);
-    PoolRun(pieces, [&](int p) {
-      const size_t a = static_cast<size_t>(p) * kPiece;
-      std::memcpy(stage + a, from + off + a, std::min(kPiece, len - a));
-    });
+    // one thread: the host pool belongs to the symbolic analysis, which
+    // often runs beside an upload and is the longer of the two
+    std::memcpy(st.buf[b], from + off, len);
     CudaCheck(cudaMemcpyAsync(to + off, stage, len, cudaMemcpyHostToDevice, s), "upload");
     CudaCheck(cudaEventRecord(st.done[b], s), "staging event");
   }
