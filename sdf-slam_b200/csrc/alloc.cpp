@@ -236,7 +236,7 @@ void UploadAsync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     // one thread: the host pool belongs to the symbolic analysis, which
     // often runs beside an upload and is the longer of the two
     std::memcpy(st.buf[b], from + off, len);
-    CudaCheck(cudaMemcpyAsync(to + off, stage, len, cudaMemcpyHostToDevice, s), "upload");
+    CudaCheck(cudaMemcpyAsync(to + off, st.buf[b], len, cudaMemcpyHostToDevice, s), "upload");
     CudaCheck(cudaEventRecord(st.done[b], s), "staging event");
   }
 }
