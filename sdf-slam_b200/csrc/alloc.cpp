@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "host_pool.h"
 
 namespace sdfgpu {
 
@@ -233,9 +234,14 @@ void UploadAsync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     const int b = static_cast<int>(k & 1);
     // the buffer's previous transfer has read it
     CudaCheck(cudaEventSynchronize(st.done[b]), "staging wait");
-    // one thread: the host pool belongs to the symbolic analysis, which
-    // often runs beside an upload and is the longer of the two
-    std::memcpy(st.buf[b], from + off, len);
+    // filled by the host pool's threads (inline when the pool is busy)
+    char* stage = static_cast<char*>(st.buf[b]);
+    constexpr size_t kPiece = size_t{2} << 20;
+    const int pieces = static_cast<int>((len + kPiece - 1) / kPiece);
+    PoolRun(pieces, [&](int p) {
+      const size_t a = static_cast<size_t>(p) * kPiece;
+      std::memcpy(stage + a, from + off + a, std::min(kPiece, len - a));
+    });
     CudaCheck(cudaMemcpyAsync(to + off, st.buf[b], len, cudaMemcpyHostToDevice, s), "upload");
     CudaCheck(cudaEventRecord(st.done[b], s), "staging event");
   }

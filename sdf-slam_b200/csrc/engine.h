@@ -32,8 +32,9 @@ void* CachedHostAlloc(size_t bytes, size_t* got);
 void CachedHostFree(void* p, size_t bytes);
 
 /// Host-to-device copy of `bytes` from pageable memory, enqueued on `s`.
-/// Large copies go through two pinned staging buffers, one filled while the
-/// other's transfer runs; `src` may be reused as soon as this returns.
+/// Large copies go through two pinned staging buffers, one filled (by the
+/// host pool's threads) while the other's transfer runs; `src` may be
+/// reused as soon as this returns.
 void UploadAsync(void* dst, const void* src, size_t bytes, cudaStream_t s);
 
 /// Owning device buffer. Owners free (or grow) it only after their stream
