@@ -331,13 +331,31 @@ def run_mixed(P, args, specs, flusher):
 
 def run_serve(P, args):
     """Poisson stream of solve requests through the serving loop: p50/p99
-    latency and throughput."""
+    latency and throughput of a warm server. Two untimed passes over other
+    requests of the same distribution (other seeds) come first: the first
+    requests of a process take their device and pinned blocks from the
+    driver and load kernels, which measured 916 ms p50 on the first pass,
+    692 ms on the second and 220 ms from the third on. The first pass's
+    figures are reported as `cold_first_pass`."""
+    cold = None
+    for warm_seed in (1500, 2500):
+        r = _serve_pass(P, args, warm_seed)
+        cold = cold or {k: r[k] for k in ("p50_ms", "p99_ms", "throughput_req_s")}
+    out = _serve_pass(P, args, 500)
+    out["cold_first_pass"] = cold
+    out["warmup_passes"] = 2
+    return out
+
+
+def _serve_pass(P, args, seed0):
+    """One pass of args.serve_requests requests (scene seeds seed0, seed0+1,
+    ...) with Poisson arrivals, on a fresh server."""
     import numpy as np
     import sdf_slam_b200.scenes as scenes
-    rng = np.random.default_rng(7)
+    rng = np.random.default_rng(7 if seed0 == 500 else seed0)
     reqs = []
     for i in range(args.serve_requests):
-        sc = scenes.request_scene(seed=500 + i, iterations=args.serve_iterations)
+        sc = scenes.request_scene(seed=seed0 + i, iterations=args.serve_iterations)
         prob = P.Problem.from_scene(sc, P.ProblemOptions(hallucination_points=4))
         reqs.append(prob.specs(min_corner=sc.min_corner, max_corner=sc.max_corner))
     gaps = rng.exponential(1.0 / args.serve_rate, size=len(reqs))
