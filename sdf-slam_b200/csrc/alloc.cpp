@@ -7,6 +7,12 @@
 // blocks are kept here, per device and per rounded size, and handed to the
 // next allocation of the same size class. A block is only returned by an
 // owner whose stream has drained, so a reused block has no work in flight.
+// Device blocks come from a stream-ordered memory pool of the library's own
+// per device (cudaMallocFromPoolAsync / cudaFreeAsync on one allocator
+// stream per device):
+// returning an evicted block to the pool does not synchronise the device,
+// where cudaFree would stall every stream in flight (the served requests of
+// other threads included).
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -50,11 +56,45 @@ Cache& TheCache() {
 constexpr size_t kMaxCachedDevice = size_t{8} << 30;
 constexpr size_t kMaxCachedHost = size_t{256} << 20;
 
+/// Each pool keeps what it has reserved (up to the process's peak use) until
+/// an allocation fails, when the retry path trims it: with a lower release
+/// threshold every synchronisation handed memory back to the driver and the
+/// next allocations mapped it again.
+constexpr uint64_t kPoolKeepBytes = ~uint64_t{0};
+
+/// The library's own memory pool of a device and the stream on which blocks
+/// are taken from it and returned; an allocation synchronises that stream,
+/// so the block is ready for any stream. A private pool leaves the device's
+/// default pool (which the host application may use) as it was.
+struct DevicePool {
+  cudaMemPool_t pool{nullptr};
+  cudaStream_t stream{nullptr};
+};
+
+/// Created on first use, with device `dev` current.
+DevicePool& PoolOf(int dev) {
+  static std::mutex mu;
+  static std::map<int, DevicePool>* pools = new std::map<int, DevicePool>;  // for the process's life
+  const std::lock_guard<std::mutex> lock(mu);
+  DevicePool& d = (*pools)[dev];
+  if (d.pool == nullptr) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    CudaCheck(cudaMemPoolCreate(&d.pool, &props), "memory pool");
+    uint64_t keep = kPoolKeepBytes;
+    CudaCheck(cudaMemPoolSetAttribute(d.pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool release threshold");
+    CudaCheck(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking), "allocator stream");
+  }
+  return d;
+}
+
 void Release(int dev, void* p) {
   if (dev < 0) {
     cudaFreeHost(p);
   } else {
-    cudaFree(p);
+    cudaFreeAsync(p, PoolOf(dev).stream);
   }
 }
 
@@ -147,11 +187,22 @@ void* CachedDeviceAlloc(size_t bytes, size_t* got) {
     return p;
   }
   void* p = nullptr;
-  cudaError_t e = cudaMalloc(&p, cls);
+  DevicePool& pool = PoolOf(dev);
+  const cudaStream_t s = pool.stream;
+  cudaError_t e = cudaMallocFromPoolAsync(&p, cls, pool.pool, s);
+  if (e == cudaSuccess) {
+    e = cudaStreamSynchronize(s);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
+    // give the cached blocks and the pool's reserve back to the driver, retry
     Drop(dev);
-    e = cudaMalloc(&p, cls);
+    CudaCheck(cudaStreamSynchronize(s), "allocator stream");
+    CudaCheck(cudaMemPoolTrimTo(pool.pool, 0), "pool trim");
+    e = cudaMallocFromPoolAsync(&p, cls, pool.pool, s);
+    if (e == cudaSuccess) {
+      e = cudaStreamSynchronize(s);
+    }
     if (e != cudaSuccess) {
       cudaGetLastError();
       Fail(SDFGPU_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(bytes) + " bytes failed");
