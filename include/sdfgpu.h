@@ -165,6 +165,14 @@ int sdfgpu_problem_create_batch(const sdfgpu_problem_desc* descs, int32_t count,
 /* Frees the handle and its device memory. Accepts NULL. */
 int sdfgpu_problem_destroy(sdfgpu_problem* problem);
 
+/* No counterpart in the reference (whose solver allocates through Eigen and
+ * CHOLMOD on the host). Device blocks released by handles stay cached in the
+ * library (by size class, up to 8 GB) and in its own memory pool on the
+ * current device, so that the next handle allocates without cudaMalloc.
+ * This returns both to the driver; call it with no handle's work in flight
+ * on the current device when the host application needs the memory. */
+int sdfgpu_release_cached_memory(void);
+
 /* Number of instances in the handle (1 unless created as a batch). */
 int32_t sdfgpu_problem_count(const sdfgpu_problem* problem);
 

@@ -662,3 +662,10 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def release_cached_memory() -> None:
+    """Returns the device blocks that released handles left cached, and the
+    library's memory pool reserve on the current device, to the driver
+    (sdfgpu_release_cached_memory). No handle's work may be in flight."""
+    _check(lib().sdfgpu_release_cached_memory())

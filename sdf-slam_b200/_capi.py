@@ -115,6 +115,7 @@ SIGNATURES = {
     "sdfgpu_problem_create_batch": (ctypes.c_int, [ctypes.POINTER(ProblemDesc), ctypes.c_int32,
                                                    ctypes.POINTER(vp)]),
     "sdfgpu_problem_destroy": (ctypes.c_int, [vp]),
+    "sdfgpu_release_cached_memory": (ctypes.c_int, []),
     "sdfgpu_problem_count": (ctypes.c_int32, [vp]),
     "sdfgpu_problem_sizes": (ctypes.c_int, [vp, ctypes.c_int32, c_int_p]),
     "sdfgpu_problem_get_specs": (ctypes.c_int, [vp, ctypes.c_int32, c_int_p, c_dbl_p, c_dbl_p,

@@ -211,6 +211,14 @@ void* CachedDeviceAlloc(size_t bytes, size_t* got) {
   return p;
 }
 
+void ReleaseCachedDeviceMemory() {
+  const int dev = CurrentDevice();
+  Drop(dev);
+  DevicePool& pool = PoolOf(dev);
+  CudaCheck(cudaStreamSynchronize(pool.stream), "allocator stream");
+  CudaCheck(cudaMemPoolTrimTo(pool.pool, 0), "pool trim");
+}
+
 void CachedDeviceFree(void* p, size_t cls) { Keep(CurrentDevice(), cls, p, kMaxCachedDevice); }
 
 void* CachedHostAlloc(size_t bytes, size_t* got) {

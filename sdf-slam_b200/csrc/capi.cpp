@@ -223,6 +223,10 @@ int sdfgpu_problem_destroy(sdfgpu_problem* problem) {
   return Guard([&] { delete problem; });
 }
 
+int sdfgpu_release_cached_memory(void) {
+  return Guard([&] { sdfgpu::ReleaseCachedDeviceMemory(); });
+}
+
 int32_t sdfgpu_problem_count(const sdfgpu_problem* problem) {
   return problem == nullptr ? 0 : static_cast<int32_t>(problem->host.size());
 }

@@ -28,6 +28,9 @@ inline void CudaCheck(cudaError_t e, const char* what) {
 /// A block may only be freed once no enqueued work uses it.
 void* CachedDeviceAlloc(size_t bytes, size_t* got);
 void CachedDeviceFree(void* p, size_t bytes);
+/// Returns the current device's cached blocks and its pool's reserve to the
+/// driver.
+void ReleaseCachedDeviceMemory();
 void* CachedHostAlloc(size_t bytes, size_t* got);
 void CachedHostFree(void* p, size_t bytes);
 

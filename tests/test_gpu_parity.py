@@ -126,6 +126,23 @@ def test_solve_is_deterministic():
         assert np.array_equal(a, b)
 
 
+def test_solve_after_releasing_cached_memory_is_unchanged():
+    """sdfgpu_release_cached_memory hands the cached blocks and the pool's
+    reserve back to the driver; the next handle allocates afresh and solves
+    to the same bits."""
+    sc = scenes.room_scene(seed=2)
+    specs, _ = scene_specs(sc, P.ProblemOptions(hallucination_points=4))
+    outs = []
+    for _ in range(2):
+        gpu = P.Problem.from_specs(specs)
+        r = P.solve(gpu, P.SolverOptions(max_iterations=5))
+        outs.append((np.array(r.cost_history), *gpu.state()))
+        gpu.close()
+        P.release_cached_memory()
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("variant", ["lm", "relation", "trust_region", "huber", "active_region"])
 def test_e2e_corner_scan_gpu(variant):
     """tests/test_e2e.cpp:90-218 with the GPU backend."""
