@@ -15,6 +15,7 @@
 #include <climits>
 
 #include "device.cuh"
+#include "trig.cuh"
 
 namespace sdfgpu {
 
@@ -132,10 +133,12 @@ __device__ __forceinline__ int GradientMode(const InstDev& I) {
   return I.smooth_gradient != 0 ? 1 : 0;
 }
 
+/// WrapAngle (src/core/pose.hpp:9) of the odometry residual's angle:
+/// atan2(sin a, cos a) with correctly rounded sin and cos.
 __device__ __forceinline__ double WrapAngle(double a) {
   double s;
   double c;
-  sincos(a, &s, &c);
+  SinCosRn(a, &s, &c);
   return atan2(s, c);
 }
 
@@ -202,9 +205,9 @@ __global__ void KPointRows(DeviceView V) {
     return;
   }
   const double* pose = V.poses + 3 * static_cast<int64_t>(f);
-  double s;
-  double c;
-  sincos(pose[2], &s, &c);
+  const double2 cs = V.pose_cs[f];
+  const double c = cs.x;
+  const double s = cs.y;
   const double2 p = V.pt_xy[k];
   const double delta = V.pt_exp[k];
   const double sqrt_w = V.pt_sw[k];
@@ -293,9 +296,9 @@ __global__ void KOdomRows(DeviceView V) {
   const double* pj = V.poses + 3 * static_cast<int64_t>(fj);
   const double* m = V.odom_meas + 3 * o;
   const double sw = V.odom_sw[o];
-  double s;
-  double c;
-  sincos(pi[2], &s, &c);
+  const double2 cs = V.pose_cs[fi];
+  const double c = cs.x;
+  const double s = cs.y;
   const double dtx = pj[0] - pi[0];
   const double dty = pj[1] - pi[1];
   const double rx = c * dtx + s * dty;
@@ -813,9 +816,21 @@ __global__ void KBackup(DeviceView V, int dir, const int32_t* revert_mask) {
       }
     }
   }
+  if (t < V.total_frames) {
+    const int i = V.frame_inst[t];
+    if (dir == 0 ? V.active[i] != 0 : revert_mask[i] != 0) {
+      if (dir == 0) {
+        V.pose_cs_backup[t] = V.pose_cs[t];
+      } else {
+        V.pose_cs[t] = V.pose_cs_backup[t];
+      }
+    }
+  }
 }
 
-/// Problem::ApplyStep (problem.cpp:117-130).
+/// Problem::ApplyStep (problem.cpp:117-130), first half: map values and
+/// positions; each moved frame's angle theta + delta goes to theta_pre for
+/// the host's WrapAngle (KCommitPoses stores the result).
 __global__ void KApplyStep(DeviceView V) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= V.n) {
@@ -840,7 +855,19 @@ __global__ void KApplyStep(DeviceView V) {
   double* p = V.poses + 3 * static_cast<int64_t>(f);
   p[0] += V.step[col];
   p[1] += V.step[col + 1];
-  p[2] = WrapAngle(p[2] + V.step[col + 2]);
+  V.theta_pre[f] = p[2] + V.step[col + 2];
+  V.theta_upd[f] = 1;
+}
+
+/// Problem::ApplyStep, second half: the wrapped angles of the moved frames
+/// and their cos and sin, as the host computed them.
+__global__ void KCommitPoses(DeviceView V) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= V.total_frames || V.theta_upd[f] == 0) {
+    return;
+  }
+  V.poses[3 * static_cast<int64_t>(f) + 2] = V.theta_out[3 * f];
+  V.pose_cs[f] = make_double2(V.theta_out[3 * f + 1], V.theta_out[3 * f + 2]);
 }
 
 /// Per-row cost terms of Problem::Cost (problem.cpp:132-156): point rows with
@@ -853,9 +880,9 @@ __global__ void KCostTerms(DeviceView V, double* terms) {
     const int i = V.frame_inst[f];
     const InstDev& I = V.inst[i];
     const double* pose = V.poses + 3 * static_cast<int64_t>(f);
-    double s;
-    double c;
-    sincos(pose[2], &s, &c);
+    const double2 cs = V.pose_cs[f];
+    const double c = cs.x;
+    const double s = cs.y;
     const double2 p = V.pt_xy[t];
     PointEval ev;
     EvalPoint(V, I, c, s, pose, p.x, p.y, V.pt_exp[t], 0, false, ev);
@@ -898,9 +925,9 @@ __global__ void KCostTerms(DeviceView V, double* terms) {
     const double* pj = V.poses + 3 * static_cast<int64_t>(V.odom_fj[o]);
     const double* m = V.odom_meas + 3 * o;
     const double sw = V.odom_sw[o];
-    double s;
-    double c;
-    sincos(pi[2], &s, &c);
+    const double2 cs = V.pose_cs[V.odom_fi[o]];
+    const double c = cs.x;
+    const double s = cs.y;
     const double dtx = pj[0] - pi[0];
     const double dty = pj[1] - pi[1];
     const double e0 = sw * ((c * dtx + s * dty) - m[0]);

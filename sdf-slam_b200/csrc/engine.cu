@@ -23,6 +23,7 @@ __global__ void KFinalizeNormal(DeviceView V);
 __global__ void KPosePairs(DeviceView V);
 __global__ void KBackup(DeviceView V, int dir, const int32_t* revert_mask);
 __global__ void KApplyStep(DeviceView V);
+__global__ void KCommitPoses(DeviceView V);
 __global__ void KCostTerms(DeviceView V, double* terms);
 __global__ void KStepTerms(DeviceView V, double* sq, double* pred);
 __global__ void KSegmentPartial(const double* x, const int64_t* seg_begin, const int64_t* seg_end, double* partial);
@@ -408,6 +409,22 @@ void Engine::UploadProblem(int64_t keep_rows) {
   poses_.Upload(poses, s);
   map_backup_.Alloc(map.size());
   poses_backup_.Alloc(poses.size());
+  {
+    const size_t F = static_cast<size_t>(total_frames_);
+    pose_cs_.Alloc(F);
+    pose_cs_backup_.Alloc(F);
+    theta_pre_.Alloc(F);
+    theta_upd_.Alloc(F);
+    theta_out_.Alloc(3 * F);
+    h_theta_pre_.Alloc(F);
+    h_theta_upd_.Alloc(F);
+    h_theta_out_.Alloc(3 * F);
+    wrap_.frames = total_frames_;
+    wrap_.theta_pre = h_theta_pre_.get();
+    wrap_.upd = h_theta_upd_.get();
+    wrap_.out = h_theta_out_.get();
+    UploadPoseTrig(poses.data(), 0, total_frames_);
+  }
   pt_rec_.Alloc(static_cast<size_t>(total_points_) * kPointRec);
   pt_poff_.Alloc(static_cast<size_t>(total_points_) * 4);
   pt_cell_.Alloc(static_cast<size_t>(total_points_));
@@ -622,6 +639,11 @@ void Engine::RefreshView() {
   V.poses = poses_.get();
   V.map_backup = map_backup_.get();
   V.poses_backup = poses_backup_.get();
+  V.pose_cs = pose_cs_.get();
+  V.pose_cs_backup = pose_cs_backup_.get();
+  V.theta_pre = theta_pre_.get();
+  V.theta_upd = theta_upd_.get();
+  V.theta_out = theta_out_.get();
   V.pt_rec = pt_rec_.get();
   V.pt_poff = pt_poff_.get();
   V.pt_cell = pt_cell_.get();
@@ -893,7 +915,7 @@ void Engine::LaunchStepAndCost(bool backup) {
     KBackup<<<Blocks(big, 256), 256, 0, stream_>>>(V_, 0, revert_.get());
   }
   if (n_ > 0) {
-    KApplyStep<<<Blocks(n_, 256), 256, 0, stream_>>>(V_);
+    LaunchApplyStep();
     KStepTerms<<<Blocks(n_, 256), 256, 0, stream_>>>(V_, sq_terms_.get(), pred_terms_.get());
   }
   const size_t I = host_.size();
@@ -905,7 +927,7 @@ void Engine::LaunchStepAndCost(bool backup) {
     KCostTerms<<<Blocks(terms, 128), 128, 0, stream_>>>(V_, terms_.get());
   }
   SegmentSum(terms_.get(), seg_begin_.get(), seg_end_.get(), static_cast<int>(3 * I), seg_out_.get());
-  times_.launches += (backup ? 1 : 0) + (n_ > 0 ? 2 : 0) + (terms > 0 ? 1 : 0);
+  times_.launches += (backup ? 1 : 0) + (n_ > 0 ? 1 : 0) + (terms > 0 ? 1 : 0);
   CudaCheck(cudaMemcpyAsync(h_seg_.get(), seg_out_.get(), 5 * I * sizeof(double), cudaMemcpyDeviceToHost, stream_),
             "step terms");
   CudaCheck(cudaMemcpyAsync(h_status_.get(), status_.get(), I * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_),
@@ -1057,8 +1079,71 @@ void Engine::SetState(int i, const double* map_values, const double* poses) {
     CudaCheck(cudaMemcpyAsync(poses_.get() + 3 * L.frame_off, poses, sizeof(double) * 3 * L.num_frames,
                               cudaMemcpyHostToDevice, stream_),
               "set poses");
+    UploadPoseTrig(poses, L.frame_off, L.num_frames);
   }
   CudaCheck(cudaStreamSynchronize(stream_), "set state");
+}
+
+void Engine::UploadPoseTrig(const double* poses, int frame_off, int frames) {
+  if (frames <= 0) {
+    return;
+  }
+  // the reference's rotation (pose.hpp:19-25) with the platform's cos and sin
+  std::vector<double2> cs(static_cast<size_t>(frames));
+  for (int f = 0; f < frames; ++f) {
+    const double th = poses[3 * static_cast<size_t>(f) + 2];
+    cs[static_cast<size_t>(f)] = make_double2(std::cos(th), std::sin(th));
+  }
+  CudaCheck(cudaMemcpyAsync(pose_cs_.get() + frame_off, cs.data(), cs.size() * sizeof(double2),
+                            cudaMemcpyHostToDevice, stream_),
+            "pose trig");
+  // the pageable source must outlive the copy
+  CudaCheck(cudaStreamSynchronize(stream_), "pose trig");
+}
+
+namespace {
+
+/// Host half of ApplyStep for the frames the step moved: WrapAngle
+/// (pose.hpp:9) of theta + delta and the new angle's cos and sin, all from
+/// the platform's libm as in the reference (problem.cpp:117-130). Runs as a
+/// stream-ordered host function between the copies of KApplyStep's angles
+/// and KCommitPoses.
+void CUDART_CB WrapMovedAngles(void* user) {
+  const auto* w = static_cast<const AngleWrapHost*>(user);
+  for (int f = 0; f < w->frames; ++f) {
+    if (w->upd[f] == 0) {
+      continue;
+    }
+    const double t = w->theta_pre[f];
+    const double th = std::atan2(std::sin(t), std::cos(t));
+    w->out[3 * f] = th;
+    w->out[3 * f + 1] = std::cos(th);
+    w->out[3 * f + 2] = std::sin(th);
+  }
+}
+
+}  // namespace
+
+void Engine::LaunchApplyStep() {
+  if (n_ <= 0) {
+    return;
+  }
+  const size_t F = static_cast<size_t>(total_frames_);
+  CudaCheck(cudaMemsetAsync(theta_upd_.get(), 0, F * sizeof(int32_t), stream_), "angle flags");
+  KApplyStep<<<Blocks(n_, 256), 256, 0, stream_>>>(V_);
+  CudaCheck(cudaMemcpyAsync(h_theta_pre_.get(), theta_pre_.get(), F * sizeof(double), cudaMemcpyDeviceToHost,
+                            stream_),
+            "angles");
+  CudaCheck(cudaMemcpyAsync(h_theta_upd_.get(), theta_upd_.get(), F * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            stream_),
+            "angle flags");
+  CudaCheck(cudaLaunchHostFunc(stream_, WrapMovedAngles, &wrap_), "angle wrap");
+  CudaCheck(cudaMemcpyAsync(theta_out_.get(), h_theta_out_.get(), 3 * F * sizeof(double), cudaMemcpyHostToDevice,
+                            stream_),
+            "wrapped angles");
+  KCommitPoses<<<Blocks(static_cast<int64_t>(F), 128), 128, 0, stream_>>>(V_);
+  CudaCheck(cudaGetLastError(), "apply step");
+  times_.launches += 2;
 }
 
 double Engine::Cost(int i) {
@@ -1076,10 +1161,7 @@ void Engine::ApplyStep(int i, const double* step) {
   CudaCheck(cudaMemcpyAsync(step_.get() + L.col_off, step, sizeof(double) * host_[static_cast<size_t>(i)].num_params(),
                             cudaMemcpyHostToDevice, stream_),
             "step");
-  if (n_ > 0) {
-    KApplyStep<<<Blocks(n_, 256), 256, 0, stream_>>>(V_);
-  }
-  CudaCheck(cudaGetLastError(), "apply step");
+  LaunchApplyStep();
   std::vector<int32_t> ones(host_.size(), 1);
   SetActive(ones);
   CudaCheck(cudaStreamSynchronize(stream_), "apply step sync");

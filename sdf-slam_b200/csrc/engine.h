@@ -195,6 +195,16 @@ struct IterTimes {
   double capture_host{0};     // host seconds capturing and instantiating graphs
 };
 
+/// Pinned buffers of ApplyStep's host half (read by a stream-ordered host
+/// function, so that the step phase stays one captured graph): per frame the
+/// unwrapped angle and a moved flag in, (theta, cos, sin) out.
+struct AngleWrapHost {
+  int frames{0};
+  const double* theta_pre{nullptr};
+  const int32_t* upd{nullptr};
+  double* out{nullptr};
+};
+
 class Engine {
  public:
   explicit Engine(std::vector<HostProblem> problems);
@@ -289,6 +299,11 @@ class Engine {
   void LaunchFactor();
   void LaunchSolve();
   void LaunchStepAndCost(bool backup);
+  /// ApplyStep of the running instances: KApplyStep, the angles' wrap and
+  /// their cos / sin on the host (stream-ordered), KCommitPoses.
+  void LaunchApplyStep();
+  /// (cos, sin) of frames [frame_off, frame_off + frames) from host poses.
+  void UploadPoseTrig(const double* poses, int frame_off, int frames);
   void LaunchCost(std::vector<double>& cost);
   /// Re-analyses the listed instances at the current state (with a wider
   /// coupling margin) and rebuilds the global structure.
@@ -342,6 +357,12 @@ class Engine {
   bool frame_rows_identity_{false};  // frame_rows_ holds 0, 1, 2, ... (rows ordered by frame)
   // state and per-iteration buffers
   DevBuf<double> map_, poses_, map_backup_, poses_backup_;
+  DevBuf<double2> pose_cs_, pose_cs_backup_;
+  DevBuf<double> theta_pre_, theta_out_;
+  DevBuf<int32_t> theta_upd_;
+  AngleWrapHost wrap_;
+  HostBuf<double> h_theta_pre_, h_theta_out_;
+  HostBuf<int32_t> h_theta_upd_;
   DevBuf<double> pt_rec_, eik_rec_, odom_rec_;
   DevBuf<int64_t> pt_poff_;
   DevBuf<int32_t> pt_cell_, cell_start_, sort_keys_a_, sort_vals_a_, sort_keys_b_, sort_vals_b_, sort_hist_;

@@ -1,0 +1,118 @@
+"""GPU parity at the full benchmark sizes: the 910-pose office (200x200 grid
+at 0.15 m, 1,146,600 point rows, 42,727 unknowns) and the 76-pose floor plan
+(100x100 at 0.2 m, 191,520 point rows), through the C ABI against the CPU
+oracle from the same input state.
+
+Contract (the FP64 path):
+* point-to-cell assignment and the sparsity patterns of J and J^T J:
+  bit-exact (every rotated point uses the cos / sin of the platform's libm,
+  as the reference does; the number of rows whose cell differs is counted
+  and must be 0);
+* residuals, Jacobian entries, J^T J, -J^T r: <= 1e-12 relative;
+* the LM step delta: <= 1e-10 norm-wise relative;
+* LM solves: cost history <= 1e-8 relative, poses <= 1e-4 m.
+"""
+import numpy as np
+import pytest
+
+import sdf_slam_b200 as P
+import sdf_slam_b200.scenes as scenes
+from helpers import oracle_from_specs, rel_err, scene_specs
+
+pytestmark = pytest.mark.gpu
+
+TOL_EVAL = 1e-12
+TOL_STEP = 1e-10
+
+
+@pytest.fixture(scope="module")
+def office_specs():
+    specs, _ = scene_specs(scenes.office_scene(seed=2))
+    return specs
+
+
+def _linearization_report(g, o):
+    flips = int(np.count_nonzero(g["point_cell"] != o["point_cell"]))
+    return {
+        "cell_flips": flips,
+        "residuals": rel_err(g["residuals"], o["residuals"]),
+        "j_values": rel_err(g["j_values"], o["j_values"]),
+        "n_values": rel_err(g["n_values"], o["n_values"]),
+        "rhs": rel_err(g["rhs"], o["rhs"]),
+        "step": rel_err(g["step"], o["step"]),
+    }
+
+
+def test_office_linearization_parity(office_specs):
+    """One LM linearization of the office from a state two FP64 GPU
+    iterations away from the scene's start (the same state is set on both
+    sides)."""
+    specs = office_specs
+    gpu = P.Problem.from_specs(specs)
+    P.solve(gpu, P.SolverOptions(max_iterations=2, step_tolerance=0.0))
+    m, p = gpu.state()
+    orc = oracle_from_specs(specs)
+    orc.set_state(m, p)
+    g = gpu.linearize(1.0, False)
+    o = orc.linearize(1.0, False, 0, True)
+    rep = _linearization_report(g, o)
+    print("office linearization vs oracle:", rep)
+    assert rep["cell_flips"] == 0
+    assert np.array_equal(g["j_outer"], o["j_outer"]) and np.array_equal(g["j_inner"], o["j_inner"])
+    assert np.array_equal(g["n_outer"], o["n_outer"]) and np.array_equal(g["n_inner"], o["n_inner"])
+    for key in ("residuals", "j_values", "n_values", "rhs"):
+        assert rep[key] <= TOL_EVAL, key
+    assert rep["step"] <= TOL_STEP
+
+
+def test_office_three_iteration_solve_parity(office_specs):
+    """Three LM iterations of the office from the scene's start (odometry
+    poses, zero map): cost history, poses and map against the oracle's
+    SolveLm."""
+    specs = office_specs
+    gpu = P.Problem.from_specs(specs)
+    rg = P.solve(gpu, P.SolverOptions(max_iterations=3, step_tolerance=0.0))
+    orc = oracle_from_specs(specs)
+    ro = orc.solve(max_iterations=3, step_tolerance=0.0, num_threads=0)
+    hg = np.array(rg.cost_history)
+    ho = np.array(ro["cost_history"])
+    assert hg.shape == ho.shape
+    assert np.max(np.abs(hg - ho) / np.abs(ho)) <= 1e-8
+    gm, gp = gpu.state()
+    om, op = orc.state()
+    assert np.max(np.abs(gp[:, :2] - op[:, :2])) <= 1e-4
+    assert np.max(np.abs(gm - om)) <= 1e-4
+
+
+def test_floorplan_ten_iteration_solve_parity():
+    """Ten LM iterations of the 76-pose floor plan from the scene's start:
+    every iteration's cost, the final poses and the map against the
+    oracle."""
+    specs, _ = scene_specs(scenes.floorplan_scene(seed=1))
+    gpu = P.Problem.from_specs(specs)
+    rg = P.solve(gpu, P.SolverOptions(max_iterations=10, step_tolerance=0.0))
+    orc = oracle_from_specs(specs)
+    ro = orc.solve(max_iterations=10, step_tolerance=0.0, num_threads=0)
+    hg = np.array(rg.cost_history)
+    ho = np.array(ro["cost_history"])
+    assert hg.shape == ho.shape == (11,)
+    assert np.max(np.abs(hg - ho) / np.abs(ho)) <= 1e-8
+    gm, gp = gpu.state()
+    om, op = orc.state()
+    assert np.max(np.abs(gp[:, :2] - op[:, :2])) <= 1e-4
+    assert np.max(np.abs(gm - om)) <= 1e-4
+
+
+def test_floorplan_cells_bit_exact_after_steps():
+    """After GPU steps (the angles wrapped and rotated with the platform's
+    libm on the host side of ApplyStep) the state's cells still agree bit
+    for bit with the oracle evaluated at that same state."""
+    specs, _ = scene_specs(scenes.floorplan_scene(seed=1))
+    gpu = P.Problem.from_specs(specs)
+    P.solve(gpu, P.SolverOptions(max_iterations=4, step_tolerance=0.0))
+    m, p = gpu.state()
+    orc = oracle_from_specs(specs)
+    orc.set_state(m, p)
+    rep = _linearization_report(gpu.linearize(1.0, False), orc.linearize(1.0, False, 0, True))
+    assert rep["cell_flips"] == 0
+    assert rep["j_values"] <= TOL_EVAL and rep["step"] <= TOL_STEP
