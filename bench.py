@@ -1,27 +1,39 @@
 #!/usr/bin/env python
-"""LM iterations/s of the joint Levenberg-Marquardt path (plain FP64 GPU).
+"""LM iterations/s of the joint Levenberg-Marquardt path on one B200.
 
-Workload (default): the 76-pose indoor loop through a 20 m x 20 m floor plan
-with 6-10 rooms, 360 beams over 360 deg, range noise N(0, 0.02 m), odometry
-noise 0.02 m / 0.01 rad, 100x100 SDF grid at 0.2 m, 6 hallucinated points per
-beam: 191,520 point rows, ~5,000 Eikonal rows, 75 odometry rows, 10,225
+Workload (default, `--workload office`): the 910-pose, 3-lap trajectory
+through a 30 m x 30 m office (corridors 1.5-2 m, 20-30 rooms), 180 beams over
+180 deg, max range 30 m, range noise N(0, 0.01 m), 200x200 SDF grid at
+0.15 m, 6 hallucinated points per beam: 1,146,600 point rows, 42,727
 unknowns. Seeded synthetic data (sdf-slam_b200/scenes.py) stands in for the
-reference's datasets.
+reference's datasets. `--workload floorplan` is the 76-pose floor plan (100x100
+at 0.2 m, 360 beams).
 
 A step is one LM iteration (residuals and Jacobian, cell sort, J^T J and
--J^T r, supernodal LDL^T, triangular solves, step, cost). Each timed step is a
-one-iteration solve call; an L2 flush (a write of 2x the 126 MB L2) runs
-between steps outside the timed events. `value` is steps over the device time
-of the steps (CUDA events on the library's stream, max over ranks); `e2e`
-times complete solves through the public API from host buffers (problem
-upload, iterations, state download).
+-J^T r, supernodal LDL^T, triangular solves, step, cost) of the plain FP64
+path. Each timed step is a one-iteration solve call; an L2 flush (a write of
+2x the 126 MB L2) runs between steps outside the timed events. `value` is
+steps over the device time of the steps (CUDA events on the library's
+stream, max over ranks); `e2e` times complete solves through the public API
+from host buffers (problem upload, analysis, iterations, state download).
+
+Beside the headline the line carries, on one GPU: the FP64 path's and the
+mixed path's final cost, pose and map differences from the CPU oracle after
+the same iterations from the same state (the oracle's time is the
+`cpu_baseline`); mixed precision (`mixed`); 64 uneven instances in one engine
+(`batched`); the office's incremental run (`incremental`); the serving loop
+at several request rates (`served`).
 
 Multi-GPU: replicas only. Every rank solves its own independent problem of
 the same size (a different seed) on its own GPU; no data crosses GPUs; rank 0
 reports the aggregate (weak scaling).
 
---impl reference times the CPU restatement of the reference's LM (oracle/) on
-the host cores with all threads, on the same workload.
+--impl reference times the CPU restatement of the reference's LM (oracle/),
+built from the scene by the oracle's own Problem constructor, on the host
+cores with all threads; it loads no library of this package.
+
+--profile N runs N one-iteration solves of the workload and prints the
+per-phase device times (the command the committed ncu summaries capture).
 """
 from __future__ import annotations
 
@@ -50,12 +62,32 @@ def _load_package():
     return mod
 
 
+def _load_scenes():
+    """The scene generator alone (pure numpy), without the package and its
+    library."""
+    name = "sdf_slam_b200_scenes"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "sdf-slam_b200", "scenes.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    return O
+
+
 METRIC = "LM iters/s plain FP64 vs mixed+batched at equal final cost; served p50/p99 ms"
 WORKLOADS = {
+    "office": "910-pose 3-lap office, 200x200 grid @0.15 m, 180 beams/180 deg, 6 hallucinated/beam",
     "floorplan": "76-pose floor-plan loop, 100x100 grid @0.2 m, 360 beams, 6 hallucinated/beam",
     "room": "10-pose room loop, 40x40 grid @0.25 m, 180 beams, 4 hallucinated/beam",
-    "office": "910-pose 3-lap office, 200x200 grid @0.15 m, 180 beams/180 deg, 6 hallucinated/beam",
 }
+SEEDS = {"office": 2, "floorplan": 1, "room": 0}
 
 
 class ClockSampler:
@@ -75,7 +107,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.reader = threading.Thread(target=self._read, daemon=True)
             self.reader.start()
         except (OSError, ValueError):
@@ -143,21 +175,12 @@ def _init_dist(world):
     return dist
 
 
-def _reduce_max(dist, value):
+def _reduce(dist, value, op):
     if dist is None:
         return value
     import torch
     t = torch.tensor([float(value)], dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def _reduce_sum(dist, value):
-    if dist is None:
-        return value
-    import torch
-    t = torch.tensor([float(value)], dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    dist.all_reduce(t, op=getattr(dist.ReduceOp, op))
     return float(t.item())
 
 
@@ -166,37 +189,43 @@ def _barrier(dist):
         dist.barrier()
 
 
-def make_scene(workload, seed):
-    import sdf_slam_b200.scenes as scenes
-    if workload == "floorplan":
-        return scenes.floorplan_scene(seed=seed)
-    if workload == "room":
-        return scenes.room_scene(seed=seed)
-    if workload == "office":
-        return scenes.office_scene(seed=seed)
-    raise ValueError(workload)
+def make_scene(scenes, workload, seed):
+    return scenes.WORKLOADS[workload](seed=seed)
 
 
-def scene_specs(P, scene):
-    prob = P.Problem.from_scene(scene)
-    return prob.specs(min_corner=scene.min_corner, max_corner=scene.max_corner)
+def scene_specs(P, scene, options=None):
+    """The product's host builder (Problem::Problem) -> flat specs."""
+    prob = P.Problem.from_scene(scene, options)
+    out = prob.specs(min_corner=scene.min_corner, max_corner=scene.max_corner)
+    prob.close()
+    return out
 
 
 def _oracle_problem(specs):
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+    O = _oracle()
     s = O.Specs(**{k: getattr(specs, k) for k in O.Specs.__dataclass_fields__})
     return O.OracleProblem.from_specs(s)
 
 
-def cpu_reference_rate(specs, iterations, threads):
-    """The oracle's LM (CPU restatement of the reference) on the same problem:
-    iterations/s with `threads` host threads."""
-    orc = _oracle_problem(specs)
-    t0 = time.perf_counter()
-    res = orc.solve(max_iterations=iterations, step_tolerance=0.0, num_threads=threads)
-    dt = time.perf_counter() - t0
-    return res["iterations"] / dt, res, dt
+def _oracle_scene_problem(scene, options=None):
+    """The oracle's own Problem constructor on the scene (hallucination,
+    normals, Eikonal and odometry specs restated from the reference)."""
+    O = _oracle()
+    opts = O.OracleOptions()
+    for k, v in scene.options.items():
+        setattr(opts, k, v)
+    for k, v in (options or {}).items():
+        setattr(opts, k, v)
+    return O.OracleProblem.build(scene.nx, scene.ny, scene.min_corner, scene.max_corner, scene.poses,
+                                 scene.scans, scene.odometry, opts)
+
+
+def _state_errors(cost_a, state_a, cost_b, state_b):
+    import numpy as np
+    return {"final_cost_rel_err": abs(cost_a - cost_b) / abs(cost_b),
+            "max_pose_err_m": float(np.max(np.abs(state_a[1][:, :2] - state_b[1][:, :2]))),
+            "max_angle_err_rad": float(np.max(np.abs(state_a[1][:, 2] - state_b[1][:, 2]))),
+            "max_map_err": float(np.max(np.abs(state_a[0] - state_b[0])))}
 
 
 class L2Flusher:
@@ -226,51 +255,139 @@ class L2Flusher:
 
 
 def run_reference(args, dist, rank):
+    """The reference's CPU LM (the oracle port, all host threads) on the
+    same workload: one untimed iteration, then a bounded sample of the K
+    timed iterations (as many as fit args.ref_budget_s at the warm-up
+    iteration's pace, at least one)."""
     if rank != 0:
         return 0
-    P = _load_package()
-    scene = make_scene(args.workload, args.seed)
-    specs = scene_specs(P, scene)
+    scenes = _load_scenes()
+    scene = make_scene(scenes, args.workload, args.seed if args.seed is not None else SEEDS[args.workload])
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        cpu_reference_rate(specs, 1, threads)
     t0 = time.perf_counter()
-    rate, res, dt = cpu_reference_rate(specs, args.steps, threads)
+    _oracle_scene_problem(scene).solve(max_iterations=1, step_tolerance=0.0, num_threads=threads)
+    per_iter = time.perf_counter() - t0
+    timed = max(1, min(args.steps, int(args.ref_budget_s / max(per_iter, 1e-9))))
+    orc = _oracle_scene_problem(scene)
+    t0 = time.perf_counter()
+    res = orc.solve(max_iterations=timed, step_tolerance=0.0, num_threads=threads)
     wall = time.perf_counter() - t0
+    rate = res["iterations"] / wall
+    sample = (f"{res['iterations']} of the {args.steps} LM iterations from the scene's start "
+              f"({wall:.1f} s), after 1 untimed iteration")
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": "LM iters/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * wall / max(1, res["iterations"]),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded floor plan, scenes.py)",
-        "config": {"workload": WORKLOADS[args.workload], "seed": args.seed, "threads": threads},
+        "data": f"synthetic (seeded {args.workload}, scenes.py)",
+        "config": {"workload": WORKLOADS[args.workload], "threads": threads,
+                   "problem": "built by the oracle's Problem constructor"},
         "cpu_baseline": {"value": rate, "unit": "LM iters/s", "cores": threads, "kind": "port",
-                         "sample": f"{res['iterations']} LM iterations of the workload"},
+                         "sample": sample},
         "e2e": {"value": rate, "unit": "LM iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "phase_s": dict(zip(["assemble", "normal", "factor", "solve", "cost"],
+                            [float(v) for v in res["phase_seconds"]])),
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+def run_profile(args):
+    """One-iteration solves printing the per-phase device times; the process
+    loads no CUDA library but the package's (for ncu captures)."""
+    P = _load_package()
+    import sdf_slam_b200.scenes as scenes
+    scene = make_scene(scenes, args.workload, args.seed if args.seed is not None else SEEDS[args.workload])
+    specs = scene_specs(P, scene)
+    gpu = P.Problem.from_specs(specs)
+    opts = P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=args.precision,
+                           refine_steps=args.refine_steps)
+    for it in range(args.profile):
+        r = P.solve(gpu, opts)
+        prof = gpu.last_profile()
+        print(f"iteration {it}: cost {r.final_cost:.9e} " +
+              " ".join(f"{k}={v * 1e3:.3f}ms" if isinstance(v, float) and k != "factor_flops" else f"{k}={v}"
+                       for k, v in prof.items()), flush=True)
+    gpu.close()
+    return 0
+
+
+def _timed_solves(P, prob, opts1, steps, flusher):
+    import numpy as np
+    device = 0.0
+    launches = 0
+    phases = np.zeros(5)
+    for _ in range(steps):
+        flusher.flush()
+        P.solve(prob, opts1)
+        prof = prob.last_profile()
+        device += prof["span"]
+        launches += prof["launches"]
+        phases += [prof["assemble"], prof["normal"], prof["factor"], prof["solve"], prof["update"]]
+    return device, launches, phases
+
+
+PHASES = ["assemble", "normal", "factor", "solve", "update"]
+
+
+def run_oracle_comparison(P, args, specs):
+    """The FP64 and mixed GPU paths against the CPU oracle after the same
+    iterations from the same state (the scene's start); the oracle's run is
+    the CPU baseline."""
+    threads = os.cpu_count() or 1
+    iters = args.cpu_iterations
+    orc = _oracle_problem(specs)
+    t0 = time.perf_counter()
+    ro = orc.solve(max_iterations=iters, step_tolerance=0.0, num_threads=threads)
+    dt = time.perf_counter() - t0
+    ostate = orc.state()
+    out = {"iterations": iters}
+    for precision in ("fp64", "mixed"):
+        g = P.Problem.from_specs(specs)
+        r = P.solve(g, P.SolverOptions(max_iterations=iters, step_tolerance=0.0, precision=precision,
+                                       refine_steps=args.refine_steps))
+        out[precision] = _state_errors(r.final_cost, g.state(), ro["final_cost"], ostate)
+        out[precision]["final_cost"] = r.final_cost
+        g.close()
+    out["oracle_final_cost"] = ro["final_cost"]
+    cpu = {"value": ro["iterations"] / dt, "unit": "LM iters/s", "cores": threads, "kind": "port",
+           "sample": f"{ro['iterations']} LM iterations of the same workload from its start ({dt:.1f} s)"}
+    return out, cpu
+
+
+def run_mixed(P, args, specs, flusher):
+    """The same workload with precision "mixed": LM iterations/s
+    (one-iteration solves, L2 flushed between them)."""
+    prob = P.Problem.from_specs(specs)
+    opts1 = P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision="mixed",
+                            refine_steps=args.refine_steps)
+    for _ in range(args.warmup):
+        P.solve(prob, opts1)
+    if not args.no_autotune:
+        prob.autotune()
+    steps = max(3, args.steps // 2)
+    device, launches, phases = _timed_solves(P, prob, opts1, steps, flusher)
+    prob.close()
+    return {"value": steps / device, "unit": "LM iters/s", "refine_steps": args.refine_steps, "steps": steps,
+            "phase_ms_per_step": {k: 1000.0 * v / steps for k, v in zip(PHASES, phases)}}
+
+
 def run_batch(P, args, flusher):
     """Uneven independent instances solved together in one engine (every
     kernel of an iteration covers all of them): aggregate LM iterations/s,
-    plain FP64 and mixed, and the mixed instances' final-cost error against
-    their FP64 solves after the same iterations."""
+    plain FP64 and mixed, and the per-instance final cost against the CPU
+    oracle after the same iterations (on a sample of the instances)."""
     import numpy as np
     import sdf_slam_b200.scenes as scenes
     scs = scenes.batch_scenes(seed=3, count=args.batch_count)
-    specs = []
-    for sc in scs:
-        opts = P.ProblemOptions(hallucination_points=4, active_region=sc.options["active_region"])
-        prob = P.Problem.from_scene(sc, opts)
-        specs.append(prob.specs(min_corner=sc.min_corner, max_corner=sc.max_corner))
+    specs = [scene_specs(P, sc, P.ProblemOptions(hallucination_points=4, active_region=sc.options["active_region"]))
+             for sc in scs]
     count = len(specs)
     steps = max(3, min(20, args.steps // 5))
     out = {"instances": count, "unit": "LM iters/s (all instances)",
            "point_rows": sum(len(s.pt_frame) for s in specs),
            "workload": "uneven room-style instances, grid 40-150 @0.25 m, 10-200 poses, 90-360 beams, "
                        "every other one active-region", "steps": steps}
-    final = {}
     for precision in ("fp64", "mixed"):
         batch = P.Problem.batch(specs)
         opts1 = [P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=precision)] * count
@@ -283,82 +400,81 @@ def run_batch(P, args, flusher):
             flusher.flush()
             P.solve(batch, opts1)
             device += batch.last_profile()["span"]
-        final[precision] = np.array([batch.cost(i) for i in range(count)])
         out[precision] = {"value": count * steps / device, "ms_per_batched_iteration": 1000.0 * device / steps}
         batch.close()
+    # final cost after `iters` iterations from the scenes' start, against the
+    # oracle's, on every `stride`-th instance
+    iters, stride = 5, max(1, count // 8)
+    sample = list(range(0, count, stride))
+    errs = {"fp64": [], "mixed": []}
+    finals = {}
+    for precision in ("fp64", "mixed"):
+        batch = P.Problem.batch(specs)
+        res = P.solve(batch, [P.SolverOptions(max_iterations=iters, step_tolerance=0.0, precision=precision)] * count)
+        finals[precision] = [res[i].final_cost for i in range(count)]
+        batch.close()
+    for i in sample:
+        ro = _oracle_problem(specs[i]).solve(max_iterations=iters, step_tolerance=0.0, num_threads=0)
+        for precision in ("fp64", "mixed"):
+            errs[precision].append(abs(finals[precision][i] - ro["final_cost"]) / abs(ro["final_cost"]))
+    out["vs_oracle"] = {"iterations": iters, "instances": sample,
+                        "max_final_cost_rel_err": {k: float(np.max(v)) for k, v in errs.items()}}
     out["value"] = out["fp64"]["value"]
-    out["mixed"]["max_final_cost_rel_err_vs_fp64"] = float(
-        np.max(np.abs(final["mixed"] - final["fp64"]) / np.abs(final["fp64"])))
     return out
 
 
-def run_mixed(P, args, specs, flusher):
-    """The same workload with precision "mixed": LM iterations/s (one-iteration
-    solves, L2 flushed between them) and, after 10 iterations from the same
-    start, the final-cost and pose differences against the FP64 path."""
-    import numpy as np
-    prob = P.Problem.from_specs(specs)
-    opts1 = P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision="mixed",
-                            refine_steps=args.refine_steps)
-    for _ in range(args.warmup):
-        P.solve(prob, opts1)
-    if not args.no_autotune:
-        prob.autotune()
-    steps = max(3, args.steps // 2)
-    device = 0.0
-    phases = np.zeros(5)
-    for _ in range(steps):
-        flusher.flush()
-        P.solve(prob, opts1)
-        prof = prob.last_profile()
-        device += prof["span"]
-        phases += [prof["assemble"], prof["normal"], prof["factor"], prof["solve"], prof["update"]]
+def run_incremental(P, args, scene):
+    """The office's incremental run (runner.cpp:226-285): 909 steps of
+    `incremental_iterations` LM iterations over the frames so far, then a
+    100-iteration batch polish of the result, on the GPU."""
+    t0 = time.perf_counter()
+    inc = P.run_incremental_scene(scene, solver=P.SolverOptions(step_tolerance=0.0),
+                                  iterations_per_increment=args.incremental_iterations)
+    t_inc = time.perf_counter() - t0
+    prob = P.Problem.from_scene(scene)
+    prob.set_state(inc.map_values, inc.poses)
+    t0 = time.perf_counter()
+    pol = P.solve(prob, P.SolverOptions(max_iterations=100, step_tolerance=1e-3))
+    t_pol = time.perf_counter() - t0
     prob.close()
-    res = {}
-    for precision in ("fp64", "mixed"):
-        p = P.Problem.from_specs(specs)
-        r = P.solve(p, P.SolverOptions(max_iterations=10, step_tolerance=0.0, precision=precision,
-                                       refine_steps=args.refine_steps))
-        res[precision] = (r.final_cost, *p.state())
-        p.close()
-    names = ["assemble", "normal", "factor", "solve", "update"]
-    return {"value": steps / device, "unit": "LM iters/s", "refine_steps": args.refine_steps,
-            "phase_ms_per_step": {k: 1000.0 * v / steps for k, v in zip(names, phases)},
-            "final_cost_rel_err_vs_fp64_10_iters": abs(res["mixed"][0] - res["fp64"][0]) / abs(res["fp64"][0]),
-            "max_pose_err_m_vs_fp64_10_iters": float(np.max(np.abs(res["mixed"][2][:, :2] - res["fp64"][2][:, :2]))),
-            "max_map_err_vs_fp64_10_iters": float(np.max(np.abs(res["mixed"][1] - res["fp64"][1])))}
+    return {"steps": inc.phases["increments"], "iterations_per_step": args.incremental_iterations,
+            "seconds": t_inc, "lm_iterations": inc.result.iterations,
+            "lm_iters_s": inc.result.iterations / t_inc, "final_cost": inc.result.final_cost,
+            "phases_s": {k: inc.phases[k] for k in ("build", "setup", "solve", "reanalysis", "capture")},
+            "reanalyses": inc.phases["reanalyses"],
+            "polish": {"iterations": pol.iterations, "seconds": t_pol, "final_cost": pol.final_cost,
+                       "converged": pol.converged, "step_tolerance": 1e-3}}
 
 
 def run_serve(P, args):
-    """Poisson stream of solve requests through the serving loop: p50/p99
-    latency and throughput of a warm server. Two untimed passes over other
-    requests of the same distribution (other seeds) come first: the first
-    requests of a process take their device and pinned blocks from the
-    driver and load kernels, which measured 916 ms p50 on the first pass,
-    692 ms on the second and 220 ms from the third on. The first pass's
-    figures are reported as `cold_first_pass`."""
+    """Poisson streams of solve requests through the serving loop at each
+    rate of args.serve_rates: throughput and p50/p99 latency of a warm
+    server (two untimed passes over other requests of the same distribution
+    come first), and the final cost of a sample of requests against the CPU
+    oracle's 20-iteration solve of the same problem."""
     cold = None
     for warm_seed in (1500, 2500):
-        r = _serve_pass(P, args, warm_seed)
+        r = _serve_pass(P, args, warm_seed, args.serve_rates[0])
         cold = cold or {k: r[k] for k in ("p50_ms", "p99_ms", "throughput_req_s")}
-    out = _serve_pass(P, args, 500)
-    out["cold_first_pass"] = cold
-    out["warmup_passes"] = 2
-    return out
+    rates = {}
+    for q, rate in enumerate(args.serve_rates):
+        rates[str(rate)] = _serve_pass(P, args, 500 + 100 * q, rate, check_oracle=(q == 0))
+    return {"rates": rates, "cold_first_pass": cold, "warmup_passes": 2,
+            "iterations_per_request": args.serve_iterations,
+            "workload": "room-style requests, grid log-U[40,200] @0.25 m, 10-400 poses, 180 beams"}
 
 
-def _serve_pass(P, args, seed0):
+def _serve_pass(P, args, seed0, rate, check_oracle=False):
     """One pass of args.serve_requests requests (scene seeds seed0, seed0+1,
-    ...) with Poisson arrivals, on a fresh server."""
+    ...) with Poisson arrivals at `rate`, on a fresh server."""
     import numpy as np
     import sdf_slam_b200.scenes as scenes
-    rng = np.random.default_rng(7 if seed0 == 500 else seed0)
+    rng = np.random.default_rng(seed0 + 7)
     reqs = []
     for i in range(args.serve_requests):
         sc = scenes.request_scene(seed=seed0 + i, iterations=args.serve_iterations)
-        prob = P.Problem.from_scene(sc, P.ProblemOptions(hallucination_points=4))
-        reqs.append(prob.specs(min_corner=sc.min_corner, max_corner=sc.max_corner))
-    gaps = rng.exponential(1.0 / args.serve_rate, size=len(reqs))
+        reqs.append(scene_specs(P, sc, P.ProblemOptions(hallucination_points=4)))
+    gaps = rng.exponential(1.0 / rate, size=len(reqs))
     server = P.Server(memory_budget_bytes=int(args.serve_budget_gb * (1 << 30)), max_batch=args.serve_batch)
     opts = P.SolverOptions(max_iterations=args.serve_iterations, step_tolerance=0.0, precision=args.precision)
     t0 = time.perf_counter()
@@ -374,28 +490,45 @@ def _serve_pass(P, args, seed0):
     wall = time.perf_counter() - t0
     st = server.stats()
     ok = 0
+    finals = []
     for spec, rid in zip(reqs, ids):
         res, _, _ = server.poll(rid)
         ok += int(res.status == 0)
+        finals.append(res.final_cost)
     server.close()
-    return {"requests": len(reqs), "completed_ok": ok, "rate_req_s": args.serve_rate,
-            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "throughput_req_s": len(reqs) / wall,
-            "lm_iters_s": st["iterations_per_s"], "iterations_per_request": args.serve_iterations,
-            "workload": "room-style requests, grid log-U[40,200] @0.25 m, 10-400 poses, 180 beams"}
+    out = {"requests": len(reqs), "completed_ok": ok, "rate_req_s": rate,
+           "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "throughput_req_s": len(reqs) / wall,
+           "lm_iters_s": st["iterations_per_s"]}
+    if check_oracle:
+        # the oracle on the smallest requests of the pass, as many as fit
+        # args.serve_oracle_budget_s
+        order = sorted(range(len(reqs)), key=lambda i: len(reqs[i].pt_frame))
+        errs, idx = [], []
+        t0 = time.perf_counter()
+        for i in order:
+            if time.perf_counter() - t0 > args.serve_oracle_budget_s:
+                break
+            ro = _oracle_problem(reqs[i]).solve(max_iterations=args.serve_iterations, step_tolerance=0.0,
+                                                num_threads=0)
+            errs.append(abs(finals[i] - ro["final_cost"]) / abs(ro["final_cost"]))
+            idx.append(i)
+        out["vs_oracle"] = {"requests": idx, "max_final_cost_rel_err": float(max(errs)) if errs else None}
+    return out
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# factor-phase kernels (KFactorFront, KUpdate, KPanel, KExtendAdd,
-# KInvertDiagonal) in one LM iteration, from one ncu capture of
-# `profile_run.py floorplan 2` (default schedule); L2 is not flushed inside
-# that capture, so writes that stay in L2 are not counted.
-FACTOR_TRAFFIC_BYTES = {"floorplan": 126.3e6}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the factor
+# phase's kernels in one LM iteration, from the committed one-kernel ncu
+# captures named beside each entry (L2 flushed before the captured step, as
+# here).
+FACTOR_TRAFFIC_BYTES = {}
 
 
 def run_gpu(args, dist, world, rank, local):
     import numpy as np
     P = _load_package()
-    scene = make_scene(args.workload, args.seed + rank)
+    import sdf_slam_b200.scenes as scenes
+    seed = (args.seed if args.seed is not None else SEEDS[args.workload]) + rank
+    scene = make_scene(scenes, args.workload, seed)
     specs = scene_specs(P, scene)
     flusher = L2Flusher()
     opts1 = P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=args.precision)
@@ -417,24 +550,16 @@ def run_gpu(args, dist, world, rank, local):
     if sampler:
         sampler.mark()
     wall0 = time.perf_counter()
-    device_s = 0.0
-    launches = 0
-    phases = np.zeros(5)
-    for _ in range(args.steps):
-        flusher.flush()
-        P.solve(prob, opts1)
-        prof = prob.last_profile()
-        device_s += prof["span"]
-        launches += prof["launches"]
-        phases += [prof["assemble"], prof["normal"], prof["factor"], prof["solve"], prof["update"]]
+    device_s, launches, phases = _timed_solves(P, prob, opts1, args.steps, flusher)
     flusher.sync()
     _barrier(dist)
     wall = time.perf_counter() - wall0
     clocks = sampler.stop() if sampler else None
-    flops = prob.last_profile()["factor_flops"]
-    device_max = _reduce_max(dist, device_s)
-    wall_max = _reduce_max(dist, wall)
-    total_steps = _reduce_sum(dist, args.steps)
+    prof_last = prob.last_profile()
+    flops = prof_last["factor_flops"]
+    device_max = _reduce(dist, device_s, "MAX")
+    wall_max = _reduce(dist, wall, "MAX")
+    total_steps = _reduce(dist, args.steps, "SUM")
     # end to end through the public API from host buffers
     e2e_iters = args.e2e_iterations
     h2d = specs.host_bytes()
@@ -457,25 +582,32 @@ def run_gpu(args, dist, world, rank, local):
         e2e_t += time.perf_counter() - t0
         d2h = m.nbytes + poses.nbytes + 8 * len(r.cost_history)
         p2.close()
-    mixed = run_mixed(P, args, specs, flusher) if (world == 1 and not args.no_mixed) else None
-    batched = run_batch(P, args, flusher) if (args.batch_count > 0 and world == 1) else None
-    flusher.close()
-    served = run_serve(P, args) if (args.serve_requests > 0 and world == 1) else None
-    e2e_t = _reduce_max(dist, e2e_t)
+    e2e_t = _reduce(dist, e2e_t, "MAX")
     e2e_value = world * args.e2e_steps * e2e_iters / e2e_t if e2e_t > 0 else 0.0
+    single = world == 1
+    mixed = run_mixed(P, args, specs, flusher) if (single and not args.no_mixed) else None
+    batched = run_batch(P, args, flusher) if (args.batch_count > 0 and single) else None
+    flusher.close()
+    fp64_peak = P.measure_fp64_peak() if rank == 0 else None
+    vs_oracle, cpu = (None, None)
+    if single and not args.no_cpu_baseline:
+        vs_oracle, cpu = run_oracle_comparison(P, args, specs)
+    incremental = run_incremental(P, args, scene) if (single and args.workload == "office"
+                                                      and not args.no_incremental) else None
+    served = run_serve(P, args) if (args.serve_requests > 0 and single) else None
     if rank != 0:
         return 0
     z = prob.sizes()
     per_step = phases / args.steps
-    names = ["assemble", "normal", "factor", "solve", "update"]
-    dominant = names[int(np.argmax(per_step))]
     peaks = {}
     try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
     except OSError:
         pass
-    hbm = peaks.get("hbm_gbs", 6650.0)
-    fp64_peak = float(os.environ.get("SDFGPU_FP64_PEAK_TFLOPS", "37.0"))
+    hbm = peaks.get("hbm_gbs")
+    hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)" if hbm else "fallback 6650 GB/s"
+    hbm = hbm or 6650.0
     # algorithmic bytes of the assembly phase per iteration (row kernels + sort)
     P_rows = z["num_points"]
     assemble_bytes = P_rows * (40 + 64 + 4) + P_rows * 4 * 2 * 2 * 2
@@ -484,33 +616,30 @@ def run_gpu(args, dist, world, rank, local):
         "frac": flops / per_step[2] / 1e12 / fp64_peak,
         "traffic": FACTOR_TRAFFIC_BYTES.get(args.workload),
         "kernel": "multifrontal LDL^T (KFactorFront + KPanel + KUpdate + KExtendAdd + KInvertDiagonal), FP64",
-        "peak_source": "nominal B200 FP64 (no measured FP64 peak on this pool)"}
+        "peak_source": "measured FP64 FMA throughput of this GPU (sdfgpu_measure_fp64_peak)",
+        "useful_flop_per_launch": flops}
     roofline_assemble = {
         "bound": "hbm", "achieved": assemble_bytes / per_step[0] / 1e9, "peak": hbm, "unit": "GB/s",
         "frac": assemble_bytes / per_step[0] / 1e9 / hbm, "traffic": None,
-        "kernel": "point rows + cell sort", "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)"}
-    roofline = roofline_factor if dominant in ("factor",) else roofline_assemble
-    cpu = None
-    if world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        rate, res, dt = cpu_reference_rate(specs, args.cpu_iterations, threads)
-        cpu = {"value": rate, "unit": "LM iters/s", "cores": threads, "kind": "port",
-               "sample": f"{res['iterations']} LM iterations of the same workload ({dt:.1f} s)"}
+        "kernel": "point rows + cell sort", "peak_source": hbm_src}
+    dominant = PHASES[int(np.argmax(per_step))]
+    roofline = roofline_factor if dominant == "factor" else roofline_assemble
     line = {
         "metric": METRIC, "value": total_steps / device_max, "unit": "LM iters/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * device_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded floor plan, scenes.py)",
-        "config": {"workload": WORKLOADS[args.workload], "seed": args.seed, "precision": args.precision,
+        "data": f"synthetic (seeded {args.workload}, scenes.py)",
+        "config": {"workload": WORKLOADS[args.workload], "seed": seed, "precision": args.precision,
                    "unknowns": z["num_parameters"], "point_rows": z["num_points"],
                    "l2": "flushed between steps (2x126 MB write)", "parallelism": f"replicas x{world}"},
         "wall_ms_per_step": 1000.0 * wall_max / args.steps,
-        "phase_ms_per_step": {k: 1000.0 * v for k, v in zip(names, per_step)},
+        "phase_ms_per_step": {k: 1000.0 * v for k, v in zip(PHASES, per_step)},
         "factor_gflop_per_step": flops / 1e9,
         "gpu_launches": int(launches),
         "roofline": roofline,
         "roofline_other": roofline_assemble if roofline is roofline_factor else roofline_factor,
         "cpu_baseline": cpu,
+        "vs_oracle": vs_oracle,
         "e2e": {"value": e2e_value, "unit": "LM iters/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "iterations_per_step": e2e_iters},
         "clocks": clocks,
@@ -518,7 +647,9 @@ def run_gpu(args, dist, world, rank, local):
                      "panel_rows": tune["schedule"][2], "factor_ms": tune["factor_ms"],
                      "trials": len(tune["trials"])} if tune else None,
         "mixed": mixed,
+        "mixed_over_fp64": mixed["value"] / (total_steps / device_max) if mixed else None,
         "batched": batched,
+        "incremental": incremental,
         "served": served,
     }
     print(json.dumps(line), flush=True)
@@ -531,23 +662,30 @@ def main():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="floorplan", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="office", choices=list(WORKLOADS))
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--seed", type=int, default=None)
+    ap.add_argument("--profile", type=int, default=0, help="print per-phase times of N one-iteration solves")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--e2e-iterations", type=int, default=10)
     ap.add_argument("--cpu-iterations", type=int, default=3)
+    ap.add_argument("--ref-budget-s", type=float, default=90.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-incremental", action="store_true")
+    ap.add_argument("--incremental-iterations", type=int, default=5)
     ap.add_argument("--refine-steps", type=int, default=3)
     ap.add_argument("--batch-count", type=int, default=64)
     ap.add_argument("--serve-requests", type=int, default=32)
-    ap.add_argument("--serve-rate", type=float, default=100.0)
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[50.0, 100.0, 200.0, 500.0])
     ap.add_argument("--serve-iterations", type=int, default=20)
     ap.add_argument("--serve-batch", type=int, default=16)
     ap.add_argument("--serve-budget-gb", type=float, default=32.0)
+    ap.add_argument("--serve-oracle-budget-s", type=float, default=20.0)
     args = ap.parse_args()
+    if args.profile > 0:
+        return run_profile(args)
     world, rank, local = _dist()
     if world > 1 and args.impl == "b200":
         # one GPU per rank

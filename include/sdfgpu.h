@@ -173,6 +173,12 @@ int sdfgpu_problem_destroy(sdfgpu_problem* problem);
  * on the current device when the host application needs the memory. */
 int sdfgpu_release_cached_memory(void);
 
+/* No counterpart in the reference. Measures the current device's FP64
+ * fused-multiply-add throughput (TFLOP/s, best of five timed launches of
+ * independent FMA chains on every SM); the roofline denominator for the FP64
+ * factorization kernels. Synchronous. */
+int sdfgpu_measure_fp64_peak(double* tflops);
+
 /* Number of instances in the handle (1 unless created as a batch). */
 int32_t sdfgpu_problem_count(const sdfgpu_problem* problem);
 

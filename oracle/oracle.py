@@ -147,6 +147,30 @@ class Specs:
     smooth_gradient_step: float = 0.0
 
 
+@dataclass
+class OracleOptions:
+    """ProblemOptions with its Weights, HallucinationOptions and NormalOptions
+    at the reference's defaults (src/problem/problem.hpp:16-87,
+    src/core/hallucination.hpp:17-23, src/core/normals.hpp:44-57)."""
+    weights_scan: float = 1.0
+    weights_hallucination: float = 1.0
+    weights_eikonal: float = 1.0
+    weights_odometry: float = 1.0
+    weights_relation: float = 1.0
+    hallucination_points: int = 6
+    hallucination_step: float = 0.1
+    hallucination_both: bool = True
+    normal_method: int = 2
+    k_neighbors: int = 10
+    normals_per_scan: bool = False
+    corner_threshold: float = 0.2
+    huber_delta: float = 0.0
+    smooth_gradient: bool = True
+    smooth_gradient_step: float = 0.0
+    active_region: bool = False
+    active_margin: int = 2
+
+
 class OracleProblem:
     """The oracle's Problem (src/problem/problem.hpp:92-161)."""
 

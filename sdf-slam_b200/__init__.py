@@ -31,7 +31,8 @@ from ._capi import (SDFGPU_ERR_INVALID_ARGUMENT, SDFGPU_ERR_NOT_READY, SDFGPU_ER
 __all__ = ["ProblemOptions", "SolverOptions", "SolveResult", "Problem", "Specs", "solve",
            "run_incremental", "run_incremental_scene", "IncrementalResult", "write_run_outputs",
            "evaluate_trajectory",
-           "LdltSolver", "Server", "GpuError", "NotReady", "device_count", "lib"]
+           "LdltSolver", "Server", "GpuError", "NotReady", "device_count", "lib", "measure_fp64_peak",
+           "release_cached_memory"]
 
 NORMAL_METHODS = {"pca": 0, "hybrid": 1, "weighted": 2}
 
@@ -669,3 +670,12 @@ def release_cached_memory() -> None:
     library's memory pool reserve on the current device, to the driver
     (sdfgpu_release_cached_memory). No handle's work may be in flight."""
     _check(lib().sdfgpu_release_cached_memory())
+
+
+def measure_fp64_peak() -> float:
+    """The current device's measured FP64 FMA throughput in TFLOP/s
+    (sdfgpu_measure_fp64_peak), the denominator of the FP64 kernels'
+    roofline."""
+    v = ctypes.c_double()
+    _check(lib().sdfgpu_measure_fp64_peak(ctypes.byref(v)))
+    return v.value

@@ -116,6 +116,7 @@ SIGNATURES = {
                                                    ctypes.POINTER(vp)]),
     "sdfgpu_problem_destroy": (ctypes.c_int, [vp]),
     "sdfgpu_release_cached_memory": (ctypes.c_int, []),
+    "sdfgpu_measure_fp64_peak": (ctypes.c_int, [c_dbl_p]),
     "sdfgpu_problem_count": (ctypes.c_int32, [vp]),
     "sdfgpu_problem_sizes": (ctypes.c_int, [vp, ctypes.c_int32, c_int_p]),
     "sdfgpu_problem_get_specs": (ctypes.c_int, [vp, ctypes.c_int32, c_int_p, c_dbl_p, c_dbl_p,

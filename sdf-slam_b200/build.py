@@ -29,6 +29,8 @@ SOURCES = {
     "engine.cu": [],
     "ldlt.cu": [],
     "noalloc.cu": [],
+    "peak.cu": [],
+    "schur_tc.cu": [],
     "refine.cu": [],
     "problem_device.cu": [],
     "problem_build.cpp": ["-x", "cu"],
@@ -40,7 +42,8 @@ SOURCES = {
     "writers.cpp": ["-x", "cu"],
     "server.cpp": ["-x", "cu"],
 }
-HEADERS = ["internal.h", "device.cuh", "engine.h", "ldlt.h", "server.h", "host_pool.h", "incremental.h"]
+HEADERS = ["internal.h", "device.cuh", "engine.h", "ldlt.h", "server.h", "host_pool.h", "incremental.h", "schur_tc.h",
+           "trig.cuh"]
 
 
 def _newest_header() -> float:

@@ -227,6 +227,13 @@ int sdfgpu_release_cached_memory(void) {
   return Guard([&] { sdfgpu::ReleaseCachedDeviceMemory(); });
 }
 
+int sdfgpu_measure_fp64_peak(double* tflops) {
+  return Guard([&] {
+    NeedHandle(tflops, "tflops");
+    *tflops = sdfgpu::MeasureFp64PeakTflops();
+  });
+}
+
 int32_t sdfgpu_problem_count(const sdfgpu_problem* problem) {
   return problem == nullptr ? 0 : static_cast<int32_t>(problem->host.size());
 }

@@ -136,6 +136,7 @@ struct DeviceView {
   float* fronts32;    // factorization work fronts of FP32 supernodes (mixed solves), else null
   double* asm_fronts; // assembly target: the FP64 normal matrix (== fronts when no solve is mixed)
   double* upd;
+  int32_t tc_schur;   // 1: the wide FP32 fronts' Schur complements run on the tensor cores
   // map-pose entries grouped by frame (transpose of mp_*): per global frame
   // the node columns coupled to it and the front offset of (pose var 0, node)
   const int64_t* fmp_ptr;

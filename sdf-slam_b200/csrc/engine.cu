@@ -539,6 +539,8 @@ void Engine::UploadSymbolic() {
   panel_tasks_.Upload(sym_.panel_tasks, s);
   update_tasks_.Upload(sym_.update_tasks, s);
   small_tasks_.Upload(sym_.small_tasks, s);
+  pack_tasks_.Upload(sym_.pack_tasks, s);
+  tc_tasks_.Upload(sym_.tc_tasks, s);
   fronts_.Alloc(static_cast<size_t>(sym_.front_doubles));
   upd_.Alloc(static_cast<size_t>(std::max<int64_t>(1, sym_.update_doubles)));
   max_front_ = 1;
@@ -673,6 +675,7 @@ void Engine::RefreshView() {
   V.fronts32 = any_mixed_ ? fronts32_.get() : nullptr;
   V.asm_fronts = any_mixed_ ? amat_.get() : fronts_.get();
   V.upd = upd_.get();
+  V.tc_schur = (any_mixed_ && sym_.tc_pack_rows > 0 && tc_map_base_ != nullptr) ? 1 : 0;
   V.fmp_ptr = fmp_ptr_.get();
   V.fmp_col = fmp_col_.get();
   V.fmp_off = fmp_off_.get();
@@ -694,6 +697,15 @@ void Engine::AllocMixed() {
   res_.Alloc(static_cast<size_t>(std::max(n_, 1)));
   ax_.Alloc(static_cast<size_t>(std::max(n_, 1)));
   corr_.Alloc(static_cast<size_t>(std::max(n_, 1)));
+  if (sym_.tc_pack_rows > 0) {
+    pack_.Alloc(static_cast<size_t>(sym_.tc_pack_rows) * kTcChunk);
+    const int64_t rows = static_cast<int64_t>(pack_.size() / kTcChunk);
+    if (pack_.get() != tc_map_base_ || rows != tc_map_rows_) {
+      EncodePackMap(&tc_map_, pack_.get(), rows);
+      tc_map_base_ = pack_.get();
+      tc_map_rows_ = rows;
+    }
+  }
 }
 
 void Engine::SetMode(const std::vector<int32_t>& mixed, int refine_steps) {
@@ -850,6 +862,12 @@ FactorPlan Engine::Plan() {
   P.inv_tasks = inv_tasks_.get();
   P.num_inv = static_cast<int>(sym_.inv_tasks.size() / 2);
   P.inv = inv_.get();
+  if (any_mixed_ && sym_.tc_pack_rows > 0 && tc_map_base_ != nullptr) {
+    P.tc_map = &tc_map_;
+    P.pack_tasks = pack_tasks_.get();
+    P.tc_tasks = tc_tasks_.get();
+    P.tc = TcArgs{sn_.get(), fronts32_.get(), dvec_.get(), active_.get(), inst_.get(), status_.get(), pack_.get()};
+  }
   return P;
 }
 
@@ -964,6 +982,8 @@ void Engine::UploadSchedule() {
   panel_tasks_.Upload(sym_.panel_tasks, stream_);
   update_tasks_.Upload(sym_.update_tasks, stream_);
   small_tasks_.Upload(sym_.small_tasks, stream_);
+  pack_tasks_.Upload(sym_.pack_tasks, stream_);
+  tc_tasks_.Upload(sym_.tc_tasks, stream_);
   level_sn_.Upload(sym_.level_sn, stream_);
   sn_.Upload(sym_.sn, stream_);
   CudaCheck(cudaStreamSynchronize(stream_), "schedule upload");

@@ -12,6 +12,7 @@
 
 #include "device.cuh"
 #include "internal.h"
+#include "schur_tc.h"
 
 namespace sdfgpu {
 
@@ -31,6 +32,8 @@ void CachedDeviceFree(void* p, size_t bytes);
 /// Returns the current device's cached blocks and its pool's reserve to the
 /// driver.
 void ReleaseCachedDeviceMemory();
+/// FP64 FMA throughput of the current device in TFLOP/s (peak.cu).
+double MeasureFp64PeakTflops();
 void* CachedHostAlloc(size_t bytes, size_t* got);
 void CachedHostFree(void* p, size_t bytes);
 
@@ -132,6 +135,13 @@ struct FactorPlan {
   const int32_t* inv_tasks{nullptr};
   int num_inv{0};
   double* inv{nullptr};
+  /// Tensor-core Schur complements of the mixed solve's wide FP32 fronts:
+  /// the packed operands' tensor map (null: every Schur update on the SIMT
+  /// tiles), the task lists and what the kernels read.
+  const CUtensorMap* tc_map{nullptr};
+  const int32_t* pack_tasks{nullptr};
+  const int32_t* tc_tasks{nullptr};
+  TcArgs tc{};
 };
 
 /// Doubles per inverted 32 x 32 diagonal block (the inverse and its
@@ -390,6 +400,13 @@ class Engine {
   DevBuf<int32_t> conv_tasks_;
   int64_t conv_count_{0};
   DevBuf<double> res_, ax_, corr_;
+  // tensor-core Schur update of the wide FP32 fronts: packed operands of one
+  // level and their tensor map (re-encoded when the buffer moves)
+  DevBuf<int32_t> pack_tasks_, tc_tasks_;
+  DevBuf<float> pack_;
+  CUtensorMap tc_map_{};
+  const float* tc_map_base_{nullptr};
+  int64_t tc_map_rows_{0};
   DevBuf<int64_t> fmp_ptr_, fmp_off_;
   DevBuf<int32_t> fmp_col_;
   std::vector<int32_t> mixed_;

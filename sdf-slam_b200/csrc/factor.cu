@@ -794,6 +794,9 @@ __global__ void __launch_bounds__(256, 2) KUpdate(DeviceView V, const int32_t* t
   if (V.active[S.instance] == 0) {
     return;
   }
+  if (t[1] < 0 && V.tc_schur != 0 && S.tc_pack >= 0 && Fp32Front(V, S)) {
+    return;  // the tensor-core Schur kernels update this front
+  }
   __shared__ double as_buf[kPanel * kTile];
   __shared__ double bs_buf[kPanel * kTile];
   if (Fp32Front(V, S)) {
@@ -1561,6 +1564,14 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
         KUpdate<<<static_cast<unsigned>(ur.count), 256, 0, stream>>>(V, P.update_tasks + 4 * ur.begin, P.dvec);
         ++launches;
       }
+    }
+    if (P.tc_map != nullptr) {
+      // Schur complements of the level's wide FP32 fronts on the tensor
+      // cores (KUpdate skips their SIMT tiles)
+      const TaskRange pk = S.pack_range[static_cast<size_t>(l)];
+      const TaskRange tr = S.tc_range[static_cast<size_t>(l)];
+      launches += LaunchSchurTc(*P.tc_map, P.tc, P.pack_tasks + 3 * pk.begin, pk.count, P.tc_tasks + 3 * tr.begin,
+                                tr.count, stream);
     }
     const TaskRange sr = S.update_range[static_cast<size_t>(S.panel_index_base.back() + l)];
     if (sr.count > 0) {

@@ -154,6 +154,7 @@ struct SupernodeRec {
   int32_t pose_root;  // 1: the dense pose block of its instance
   int32_t upper_l11;  // 1: L of the pivot block is stored transposed in its upper triangle
   int32_t panel_base; // first of its ceil(ncols / 32) inverted diagonal blocks
+  int64_t tc_pack;    // first packed operand row of its tensor-core Schur update (within its level), or -1
 };
 
 /// A contiguous block of work items of one kernel launch in the level
@@ -194,6 +195,16 @@ struct Symbolic {
   std::vector<int32_t> update_tasks;         // (sn, panel, ti, tj) quads
   std::vector<TaskRange> update_range;       // per (level, panel) flattened
   std::vector<int32_t> panel_index_base;     // level -> first (level,panel) slot
+  // Tensor-core Schur complements of a mixed solve's FP32 fronts with at
+  // least kTcMinRows rows below the pivot block (their SIMT Schur tasks are
+  // skipped then): per level, operand packing tasks (sn, row tile, K chunk)
+  // and output tile tasks (sn, tile i, tile j), i >= j; the packed operand
+  // buffer is reused level after level (tc_pack_rows rows of the widest).
+  std::vector<int32_t> pack_tasks;
+  std::vector<TaskRange> pack_range;
+  std::vector<int32_t> tc_tasks;
+  std::vector<TaskRange> tc_range;
+  int64_t tc_pack_rows{0};
   // fronts with at most small_pivots pivots: one factorization kernel per
   // level, tasks (sn, first row of the chunk below the pivot block, rows in
   // the chunk) with front_rows threads per block (rows per chunk shrink to

@@ -1,0 +1,86 @@
+// FP64 peak of the current device, measured: the roofline denominator of the
+// FP64 factorization kernels (the vendor's FP64 figure is nominal and this
+// pool publishes no measured one).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "engine.h"
+
+namespace sdfgpu {
+
+namespace {
+
+constexpr int kChains = 8;
+constexpr int kPeakThreads = 256;
+
+/// kChains independent FMA chains per thread; the sum is stored so that the
+/// chains stay live.
+__global__ void __launch_bounds__(kPeakThreads) KFp64FmaChains(double* out, int iterations, double m, double c) {
+  double a[kChains];
+#pragma unroll
+  for (int q = 0; q < kChains; ++q) {
+    a[q] = 1e-3 * (threadIdx.x + q);
+  }
+  for (int it = 0; it < iterations; ++it) {
+#pragma unroll
+    for (int q = 0; q < kChains; ++q) {
+      a[q] = fma(a[q], m, c);
+    }
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int q = 0; q < kChains; ++q) {
+    s += a[q];
+  }
+  out[static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace
+
+double MeasureFp64PeakTflops() {
+  int dev = 0;
+  int sms = 0;
+  int per_sm = 0;
+  CudaCheck(cudaGetDevice(&dev), "device");
+  CudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "SM count");
+  CudaCheck(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, KFp64FmaChains, kPeakThreads, 0), "occupancy");
+  const int blocks = sms * std::max(1, per_sm);
+  const int iterations = 1 << 14;
+  size_t got = 0;
+  auto* out = static_cast<double*>(CachedDeviceAlloc(sizeof(double) * blocks * kPeakThreads, &got));
+  cudaStream_t s = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  double best = 0.0;
+  try {
+    CudaCheck(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+    CudaCheck(cudaEventCreate(&ev[0]), "event");
+    CudaCheck(cudaEventCreate(&ev[1]), "event");
+    for (int rep = 0; rep < 6; ++rep) {
+      CudaCheck(cudaEventRecord(ev[0], s), "event");
+      KFp64FmaChains<<<blocks, kPeakThreads, 0, s>>>(out, iterations, 0.9999999, 1e-7);
+      CudaCheck(cudaEventRecord(ev[1], s), "event");
+      CudaCheck(cudaEventSynchronize(ev[1]), "peak");
+      float ms = 0.0f;
+      CudaCheck(cudaEventElapsedTime(&ms, ev[0], ev[1]), "peak timing");
+      const double flops = 2.0 * kChains * static_cast<double>(iterations) * blocks * kPeakThreads;
+      if (rep > 0) {  // the first launch loads the module
+        best = std::max(best, flops / (ms * 1e-3) / 1e12);
+      }
+    }
+  } catch (...) {
+    if (s != nullptr) {
+      cudaStreamSynchronize(s);
+    }
+    CachedDeviceFree(out, got);
+    throw;
+  }
+  CudaCheck(cudaStreamSynchronize(s), "peak");
+  CachedDeviceFree(out, got);
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  cudaStreamDestroy(s);
+  return best;
+}
+
+}  // namespace sdfgpu

@@ -28,6 +28,7 @@
 
 #include "host_pool.h"
 #include "internal.h"
+#include "schur_tc.h"
 
 namespace sdfgpu {
 
@@ -548,6 +549,52 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   }
   for (int l = 0; l < levels; ++l) {
     S.update_range.push_back(schur_range[static_cast<size_t>(l)]);
+  }
+  // tensor-core Schur tasks of the wide grid fronts (used by mixed solves)
+  S.pack_tasks.clear();
+  S.tc_tasks.clear();
+  S.pack_range.assign(static_cast<size_t>(levels), {});
+  S.tc_range.assign(static_cast<size_t>(levels), {});
+  S.tc_pack_rows = 0;
+  for (SupernodeRec& r : S.sn) {
+    r.tc_pack = -1;
+  }
+  for (int l = 0; l < levels; ++l) {
+    const int qb = S.level_begin[static_cast<size_t>(l)];
+    const int qe = S.level_begin[static_cast<size_t>(l) + 1];
+    int64_t rows = 0;
+    S.pack_range[static_cast<size_t>(l)].begin = static_cast<int64_t>(S.pack_tasks.size() / 3);
+    S.tc_range[static_cast<size_t>(l)].begin = static_cast<int64_t>(S.tc_tasks.size() / 3);
+    for (int q = qb; q < qe; ++q) {
+      const int s = S.level_sn[static_cast<size_t>(q)];
+      SupernodeRec& r = S.sn[static_cast<size_t>(s)];
+      if (r.pose_root != 0 || r.nrows < kTcMinRows || r.ncols < 1) {
+        continue;
+      }
+      r.tc_pack = rows;
+      rows += TcPackRows(r.ncols, r.nrows);
+      const int nT = (r.nrows + kTcTile - 1) / kTcTile;
+      const int nC = (r.ncols + kTcChunk - 1) / kTcChunk;
+      for (int t = 0; t < nT; ++t) {
+        for (int c = 0; c < nC; ++c) {
+          S.pack_tasks.push_back(s);
+          S.pack_tasks.push_back(t);
+          S.pack_tasks.push_back(c);
+        }
+      }
+      for (int tj = 0; tj < nT; ++tj) {
+        for (int ti = tj; ti < nT; ++ti) {
+          S.tc_tasks.push_back(s);
+          S.tc_tasks.push_back(ti);
+          S.tc_tasks.push_back(tj);
+        }
+      }
+    }
+    S.pack_range[static_cast<size_t>(l)].count =
+        static_cast<int64_t>(S.pack_tasks.size() / 3) - S.pack_range[static_cast<size_t>(l)].begin;
+    S.tc_range[static_cast<size_t>(l)].count =
+        static_cast<int64_t>(S.tc_tasks.size() / 3) - S.tc_range[static_cast<size_t>(l)].begin;
+    S.tc_pack_rows = std::max(S.tc_pack_rows, rows);
   }
 }
 

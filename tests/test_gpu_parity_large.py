@@ -116,3 +116,28 @@ def test_floorplan_cells_bit_exact_after_steps():
     rep = _linearization_report(gpu.linearize(1.0, False), orc.linearize(1.0, False, 0, True))
     assert rep["cell_flips"] == 0
     assert rep["j_values"] <= TOL_EVAL and rep["step"] <= TOL_STEP
+
+
+@pytest.mark.parametrize("workload", ["floorplan", "office"])
+def test_mixed_step_tensor_core_fronts(workload, office_specs):
+    """Mixed precision factors the wide grid fronts in FP32 with their Schur
+    complements on the tensor cores (split TF32). One LM iteration from the
+    same state: without refinement the state differs from the FP64 path's by
+    an FP32-level fraction of the step; with three FP64 refinement rounds by
+    less than 1e-9 of it."""
+    specs = office_specs if workload == "office" else scene_specs(scenes.floorplan_scene(seed=1))[0]
+    base = P.Problem.from_specs(specs)
+    m0, p0 = base.state()
+    P.solve(base, P.SolverOptions(max_iterations=1, step_tolerance=0.0))
+    m64, p64 = base.state()
+    step = max(np.max(np.abs(m64 - m0)), np.max(np.abs(p64 - p0)))
+    for refine, bound in [(0, 1e-3), (3, 1e-9)]:
+        g = P.Problem.from_specs(specs)
+        r = P.solve(g, P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision="mixed",
+                                       refine_steps=refine))
+        assert r.status == 0
+        gm, gp = g.state()
+        dev = max(np.max(np.abs(gm - m64)), np.max(np.abs(gp - p64)))
+        print(f"{workload} mixed refine={refine}: max state difference {dev:.3e} of step {step:.3e}")
+        assert dev <= bound * step
+        g.close()

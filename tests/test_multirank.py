@@ -28,8 +28,8 @@ def _rank_main(rank, world, port, out_dir):
     dist = bench._init_dist(world)
     try:
         bench._barrier(dist)
-        mx = bench._reduce_max(dist, 1.5 + rank)
-        sm = bench._reduce_sum(dist, 10 * (rank + 1))
+        mx = bench._reduce(dist, 1.5 + rank, "MAX")
+        sm = bench._reduce(dist, 10 * (rank + 1), "SUM")
         w, r, lr = bench._dist()
         with open(os.path.join(out_dir, f"rank{rank}.json"), "w") as f:
             json.dump({"max": mx, "sum": sm, "world": w, "rank": r, "local": lr}, f)
@@ -52,8 +52,9 @@ def test_replicas_solve_distinct_problems():
     # each rank solves its own problem of the same size (seed + rank)
     sys.path.insert(0, ROOT)
     import bench
-    a = bench.make_scene("room", 1)
-    b = bench.make_scene("room", 2)
+    scenes = bench._load_scenes()
+    a = bench.make_scene(scenes, "room", 1)
+    b = bench.make_scene(scenes, "room", 2)
     assert (a.nx, a.ny, len(a.poses)) == (b.nx, b.ny, len(b.poses))
     assert any(pa.shape != pb.shape or (pa != pb).any() for pa, pb in zip(a.scans, b.scans))
 
@@ -72,3 +73,20 @@ def test_reference_arm_under_torchrun_prints_once():
     assert line["impl"] == "reference" and line["n_gpus"] == 2
     assert line["cpu_baseline"]["kind"] == "port" and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_reference_arm_maps_no_library_of_the_package():
+    """The reference arm builds its problem with the oracle's own Problem
+    constructor and times the oracle's LM: the process maps the oracle's
+    library and none of this package's."""
+    code = (
+        "import sys, json, types; sys.path.insert(0, %r); import bench;"
+        "args = types.SimpleNamespace(workload='room', seed=None, steps=2, warmup=0, gpus=1, ref_budget_s=5.0);"
+        "bench.run_reference(args, None, 0);"
+        "maps = open('/proc/self/maps').read();"
+        "print(json.dumps({'sdfgpu': 'libsdfgpu' in maps, 'oracle': 'liboracle' in maps}))" % ROOT)
+    res = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, cwd=ROOT, timeout=600)
+    assert res.returncode == 0, res.stderr[-2000:]
+    lines = [json.loads(ln) for ln in res.stdout.splitlines() if ln.startswith("{")]
+    assert lines[0]["impl"] == "reference" and lines[0]["value"] > 0
+    assert lines[-1] == {"sdfgpu": False, "oracle": True}
