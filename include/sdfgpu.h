@@ -179,6 +179,19 @@ int sdfgpu_release_cached_memory(void);
  * factorization kernels. Synchronous. */
 int sdfgpu_measure_fp64_peak(double* tflops);
 
+/* No counterpart in the reference: a test hook for the failure path of the
+ * one-launch triangular solve, whose blocks wait on flags that other blocks
+ * publish. From the next solve on, supernode `withhold_front` (an index into
+ * the handle's current symbolic structure) never publishes its forward flag
+ * and every wait gives up after `wait_polls` polls (0: the default of about
+ * a second); the wait that runs out ends the solve with SDFGPU_ERR_TIMEOUT,
+ * the state is not moved and the device stays usable. withhold_front = -1
+ * restores normal solves. */
+int sdfgpu_debug_solve_fault(sdfgpu_problem* problem, int32_t withhold_front, uint32_t wait_polls);
+/* Supernodes of the handle's current symbolic structure (0 before its first
+ * device use). */
+int32_t sdfgpu_debug_supernode_count(sdfgpu_problem* problem);
+
 /* Number of instances in the handle (1 unless created as a batch). */
 int32_t sdfgpu_problem_count(const sdfgpu_problem* problem);
 
@@ -420,12 +433,20 @@ int sdfgpu_server_destroy(sdfgpu_server* server);
  * with the library's LDL^T panel, update and triangular-solve kernels,
  * keeping every intermediate in one file-scope device array of about 8.6 MB
  * that each GPU loading the library holds until the process exits. Calls no
- * cudaMalloc / cudaFree and creates no stream. n above SDFGPU_NOALLOC_MAX_N
- * gives SDFGPU_ERR_INVALID_ARGUMENT; a zero pivot SDFGPU_ERR_NUMERICAL. The
- * first call on a device looks the array's address up with that device
- * current: make it before any stream capture. All calls share the array and
- * it keeps the last call's contents; calls whose GPU work overlaps (from
- * several host threads, for example) race and must be serialised. */
+ * cudaMalloc / cudaFree and creates no stream: its copies and kernels run on
+ * the calling thread's per-thread default stream (cudaStreamPerThread), which
+ * does not wait for the host application's other streams (it does order with
+ * the legacy default stream, if the application uses that one). n above
+ * SDFGPU_NOALLOC_MAX_N gives SDFGPU_ERR_INVALID_ARGUMENT; a zero pivot
+ * SDFGPU_ERR_NUMERICAL. The first call on a device looks the array's address
+ * up with that device current, and under CUDA's lazy module loading (the
+ * default) that first lookup is also when the driver loads the code holding
+ * the array and reserves its ~8.6 MB: make that first call (a call with
+ * n = 1 will do) at start-up, before the host framework's allocator takes
+ * the device's free memory and before any stream capture. All calls share
+ * the array and it keeps the last call's contents; calls whose GPU work
+ * overlaps (from several host threads, for example) race and must be
+ * serialised. */
 #define SDFGPU_NOALLOC_MAX_N 1024
 int sdfgpu_dense_ldlt_solve_noalloc(int32_t n, const double* a, const double* b, double* x);
 

@@ -387,6 +387,16 @@ class Problem:
         return {"schedule": tuple(int(v) for v in sched), "factor_ms": best.value,
                 "trials": [tuple(r) for r in trials[:n.value]]}
 
+    def debug_solve_fault(self, withhold_front: int, wait_polls: int = 0):
+        """Test hook (sdfgpu_debug_solve_fault): from the next solve on, the
+        one-launch triangular solve never publishes supernode
+        `withhold_front`'s forward flag and a wait gives up after `wait_polls`
+        polls, so the solve ends with TimeoutError; -1 restores it."""
+        _check(lib().sdfgpu_debug_solve_fault(self._h, int(withhold_front), int(wait_polls)))
+
+    def debug_supernode_count(self) -> int:
+        return int(lib().sdfgpu_debug_supernode_count(self._h))
+
     def last_profile(self) -> dict:
         ph = np.zeros(12)
         _check(lib().sdfgpu_last_profile(self._h, _d(ph)))

@@ -117,6 +117,8 @@ SIGNATURES = {
     "sdfgpu_problem_destroy": (ctypes.c_int, [vp]),
     "sdfgpu_release_cached_memory": (ctypes.c_int, []),
     "sdfgpu_measure_fp64_peak": (ctypes.c_int, [c_dbl_p]),
+    "sdfgpu_debug_solve_fault": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_uint32]),
+    "sdfgpu_debug_supernode_count": (ctypes.c_int32, [vp]),
     "sdfgpu_problem_count": (ctypes.c_int32, [vp]),
     "sdfgpu_problem_sizes": (ctypes.c_int, [vp, ctypes.c_int32, c_int_p]),
     "sdfgpu_problem_get_specs": (ctypes.c_int, [vp, ctypes.c_int32, c_int_p, c_dbl_p, c_dbl_p,

@@ -71,12 +71,29 @@ struct DevicePool {
   cudaStream_t stream{nullptr};
 };
 
+struct PoolTable {
+  std::mutex mu;
+  std::map<int, DevicePool> pools;
+};
+
+PoolTable& ThePools() {
+  static PoolTable* t = new PoolTable;  // for the process's life
+  return *t;
+}
+
+/// The pool of `dev`, or null when the library never allocated there.
+DevicePool* FindPool(int dev) {
+  PoolTable& t = ThePools();
+  const std::lock_guard<std::mutex> lock(t.mu);
+  auto it = t.pools.find(dev);
+  return it == t.pools.end() || it->second.pool == nullptr ? nullptr : &it->second;
+}
+
 /// Created on first use, with device `dev` current.
 DevicePool& PoolOf(int dev) {
-  static std::mutex mu;
-  static std::map<int, DevicePool>* pools = new std::map<int, DevicePool>;  // for the process's life
-  const std::lock_guard<std::mutex> lock(mu);
-  DevicePool& d = (*pools)[dev];
+  PoolTable& t = ThePools();
+  const std::lock_guard<std::mutex> lock(t.mu);
+  DevicePool& d = t.pools[dev];
   if (d.pool == nullptr) {
     cudaMemPoolProps props = {};
     props.allocType = cudaMemAllocationTypePinned;
@@ -93,8 +110,18 @@ DevicePool& PoolOf(int dev) {
 void Release(int dev, void* p) {
   if (dev < 0) {
     cudaFreeHost(p);
-  } else {
-    cudaFreeAsync(p, PoolOf(dev).stream);
+  } else if (DevicePool* pool = FindPool(dev)) {
+    // on the block's own device and pool stream, whichever device the
+    // caller has current
+    int cur = dev;
+    cudaGetDevice(&cur);
+    if (cur != dev) {
+      cudaSetDevice(dev);
+    }
+    cudaFreeAsync(p, pool->stream);
+    if (cur != dev) {
+      cudaSetDevice(cur);
+    }
   }
 }
 
@@ -179,10 +206,13 @@ int CurrentDevice() {
 
 }  // namespace
 
-void* CachedDeviceAlloc(size_t bytes, size_t* got) {
+void* CachedDeviceAlloc(size_t bytes, size_t* got, int* device) {
   const int dev = CurrentDevice();
   const size_t cls = SizeClass(bytes);
   *got = cls;
+  if (device != nullptr) {
+    *device = dev;
+  }
   if (void* p = Take(dev, cls)) {
     return p;
   }
@@ -213,13 +243,16 @@ void* CachedDeviceAlloc(size_t bytes, size_t* got) {
 
 void ReleaseCachedDeviceMemory() {
   const int dev = CurrentDevice();
+  DevicePool* pool = FindPool(dev);
+  if (pool == nullptr) {
+    return;  // nothing was allocated on this device
+  }
   Drop(dev);
-  DevicePool& pool = PoolOf(dev);
-  CudaCheck(cudaStreamSynchronize(pool.stream), "allocator stream");
-  CudaCheck(cudaMemPoolTrimTo(pool.pool, 0), "pool trim");
+  CudaCheck(cudaStreamSynchronize(pool->stream), "allocator stream");
+  CudaCheck(cudaMemPoolTrimTo(pool->pool, 0), "pool trim");
 }
 
-void CachedDeviceFree(void* p, size_t cls) { Keep(CurrentDevice(), cls, p, kMaxCachedDevice); }
+void CachedDeviceFree(void* p, size_t cls, int device) { Keep(device, cls, p, kMaxCachedDevice); }
 
 void* CachedHostAlloc(size_t bytes, size_t* got) {
   const size_t cls = SizeClass(bytes);
@@ -254,8 +287,17 @@ struct Staging {
 
 constexpr int kStagingSlots = 3;
 
-Staging* TheStaging() {
-  static Staging* st = new Staging[kStagingSlots];  // kept for the life of the process
+/// The staging slots of `dev`: their events are recorded on that device's
+/// streams only (an event and the stream it is recorded on must share a
+/// device).
+Staging* TheStaging(int dev) {
+  static std::mutex mu;
+  static std::map<int, Staging*>* slots = new std::map<int, Staging*>;  // kept for the life of the process
+  const std::lock_guard<std::mutex> lock(mu);
+  Staging*& st = (*slots)[dev];
+  if (st == nullptr) {
+    st = new Staging[kStagingSlots];
+  }
   return st;
 }
 
@@ -266,7 +308,7 @@ void UploadAsync(void* dst, const void* src, size_t bytes, cudaStream_t s) {
     CudaCheck(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s), "upload");
     return;
   }
-  Staging* slots = TheStaging();
+  Staging* slots = TheStaging(CurrentDevice());
   int slot = -1;
   for (int k = 0; k < kStagingSlots && slot < 0; ++k) {
     if (slots[k].mu.try_lock()) {

@@ -837,8 +837,10 @@ __global__ void KApplyStep(DeviceView V) {
     return;
   }
   const int i = V.col_inst[col];
-  // a failed factorization or a stale pattern leaves the state untouched
-  if (V.active[i] == 0 || (V.status[i] & (kStatusPatternOverflow | kStatusZeroPivot)) != 0) {
+  // a failed factorization, a solve whose wait ran out or a stale pattern
+  // leaves the state untouched
+  if (V.active[i] == 0 ||
+      (V.status[i] & (kStatusPatternOverflow | kStatusZeroPivot | kStatusWaitTimeout)) != 0) {
     return;
   }
   const int node = V.col_node[col];

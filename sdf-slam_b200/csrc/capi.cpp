@@ -234,6 +234,17 @@ int sdfgpu_measure_fp64_peak(double* tflops) {
   });
 }
 
+int sdfgpu_debug_solve_fault(sdfgpu_problem* problem, int32_t withhold_front, uint32_t wait_polls) {
+  return Guard([&] { Eng(problem).SetSolveFault(withhold_front, wait_polls); });
+}
+
+int32_t sdfgpu_debug_supernode_count(sdfgpu_problem* problem) {
+  if (problem == nullptr || !problem->engine) {
+    return 0;
+  }
+  return static_cast<int32_t>(problem->engine->symbolic().sn.size());
+}
+
 int32_t sdfgpu_problem_count(const sdfgpu_problem* problem) {
   return problem == nullptr ? 0 : static_cast<int32_t>(problem->host.size());
 }

@@ -66,10 +66,19 @@ Engine::Engine(std::vector<HostProblem> problems) : host_(std::move(problems)) {
 
 Engine::Engine(HostProblem problem, SymPiece piece) {
   host_.push_back(std::move(problem));
-  Init(&piece);
+  std::vector<SymPiece> pieces;
+  pieces.push_back(std::move(piece));
+  Init(&pieces);
 }
 
-void Engine::Init(SymPiece* piece) {
+Engine::Engine(std::vector<HostProblem> problems, std::vector<SymPiece> pieces) : host_(std::move(problems)) {
+  if (pieces.size() != host_.size()) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT, "one analysis per problem is required");
+  }
+  Init(&pieces);
+}
+
+void Engine::Init(std::vector<SymPiece>* pieces) {
   if (host_.empty()) {
     Fail(SDFGPU_ERR_INVALID_ARGUMENT, "no problems");
   }
@@ -95,20 +104,22 @@ void Engine::Init(SymPiece* piece) {
   h_seg_.Alloc(5 * host_.size());
   h_status_.Alloc(host_.size());
   mixed_.assign(host_.size(), 0);  // plain FP64 until a solve asks otherwise
-  AnalyzeAndUpload(piece, 0);
+  AnalyzeAndUpload(pieces, 0);
 }
 
-void Engine::AnalyzeAndUpload(SymPiece* piece, int64_t keep_rows) {
-  // the symbolic analysis (host only) runs while the problem is uploaded; a
-  // given analysis only needs its global structure
-  std::future<void> analysis = std::async(std::launch::async, [this, piece] {
-    if (piece == nullptr) {
+void Engine::AnalyzeAndUpload(std::vector<SymPiece>* pieces, int64_t keep_rows) {
+  // the symbolic analysis (host only) runs while the problem is uploaded;
+  // given analyses (one per instance) only need their global structure
+  std::future<void> analysis = std::async(std::launch::async, [this, pieces] {
+    if (pieces == nullptr) {
       AnalyzeHost();
       return;
     }
-    margin_.assign(1, piece->margin);
-    pieces_.clear();
-    pieces_.push_back(std::move(*piece));
+    margin_.clear();
+    for (const SymPiece& p : *pieces) {
+      margin_.push_back(p.margin);
+    }
+    pieces_ = std::move(*pieces);
     pending_.clear();
     sym_ = GlobalStructure();
   });
@@ -141,7 +152,13 @@ void Engine::Replace(HostProblem next, SymPiece* piece, int64_t keep_rows) {
   DropGraph();
   host_[0] = std::move(next);
   BuildLayout();
-  AnalyzeAndUpload(piece, keep_rows);
+  if (piece == nullptr) {
+    AnalyzeAndUpload(nullptr, keep_rows);
+  } else {
+    std::vector<SymPiece> pieces;
+    pieces.push_back(std::move(*piece));
+    AnalyzeAndUpload(&pieces, keep_rows);
+  }
 }
 
 void Engine::DropGraph() {
@@ -759,7 +776,7 @@ namespace {
 void CheckWaits(const int32_t* st, size_t count) {
   for (size_t i = 0; i < count; ++i) {
     if ((st[i] & kStatusWaitTimeout) != 0) {
-      Fail(SDFGPU_ERR_CUDA, "a wait of the solve kernel ran out of its limit");
+      Fail(SDFGPU_ERR_TIMEOUT, "a wait of the solve kernel ran out of its limit");
     }
   }
 }
@@ -862,6 +879,8 @@ FactorPlan Engine::Plan() {
   P.inv_tasks = inv_tasks_.get();
   P.num_inv = static_cast<int>(sym_.inv_tasks.size() / 2);
   P.inv = inv_.get();
+  P.solve_withhold = solve_withhold_;
+  P.solve_wait_polls = solve_wait_polls_;
   if (any_mixed_ && sym_.tc_pack_rows > 0 && tc_map_base_ != nullptr) {
     P.tc_map = &tc_map_;
     P.pack_tasks = pack_tasks_.get();
@@ -972,6 +991,15 @@ void Engine::Reanalyze(const std::vector<int>& which) {
   UploadSymbolic();
   ++times_.reanalyses;
   times_.reanalysis_host += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void Engine::SetSolveFault(int withhold, uint32_t wait_polls) {
+  if (withhold < -1 || withhold >= static_cast<int>(sym_.sn.size())) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT, "supernode index out of range");
+  }
+  solve_withhold_ = withhold;
+  solve_wait_polls_ = wait_polls;
+  DropGraph();  // the captured solve holds the previous parameters
 }
 
 void Engine::UploadSchedule() {
@@ -1684,6 +1712,22 @@ void Engine::FinishIteration() {
     CudaCheck(cudaStreamSynchronize(stream_), "restore");
   }
   ++iter_;
+}
+
+bool Engine::InstanceDone(int i) const {
+  const LmInst& L = lm_[static_cast<size_t>(i)];
+  return L.active == 0 || iter_ >= L.opt.max_iterations;
+}
+
+sdfgpu_solve_result Engine::InstanceResult(int i) const {
+  const LmInst& L = lm_[static_cast<size_t>(i)];
+  sdfgpu_solve_result r = L.res;
+  if (r.iterations == 0) {
+    r.final_cost = r.initial_cost;
+  }
+  r.duration_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start_).count();
+  r.cost_history_length = static_cast<int32_t>(L.hist.size());
+  return r;
 }
 
 void Engine::EndSolve(sdfgpu_solve_result* results, double* cost_history, int capacity) {

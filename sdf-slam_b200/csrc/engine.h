@@ -25,10 +25,12 @@ inline void CudaCheck(cudaError_t e, const char* what) {
 }
 
 /// Block allocators with a per-device cache of freed blocks (alloc.cpp):
-/// `got` receives the block's size (the request rounded up to its class).
-/// A block may only be freed once no enqueued work uses it.
-void* CachedDeviceAlloc(size_t bytes, size_t* got);
-void CachedDeviceFree(void* p, size_t bytes);
+/// `got` receives the block's size (the request rounded up to its class),
+/// `device` (when given) the device it lives on, which its free must name,
+/// whichever device is current then. A block may only be freed once no
+/// enqueued work uses it.
+void* CachedDeviceAlloc(size_t bytes, size_t* got, int* device = nullptr);
+void CachedDeviceFree(void* p, size_t bytes, int device);
 /// Returns the current device's cached blocks and its pool's reserve to the
 /// driver.
 void ReleaseCachedDeviceMemory();
@@ -54,7 +56,7 @@ class DevBuf {
   ~DevBuf() { Free(); }
   void Free() {
     if (ptr_ != nullptr) {
-      CachedDeviceFree(ptr_, bytes_);
+      CachedDeviceFree(ptr_, bytes_, device_);
       ptr_ = nullptr;
       count_ = 0;
       bytes_ = 0;
@@ -72,7 +74,7 @@ class DevBuf {
       count += count / 4;
     }
     const size_t bytes = std::max<size_t>(1, count) * sizeof(T);
-    ptr_ = static_cast<T*>(CachedDeviceAlloc(bytes, &bytes_));
+    ptr_ = static_cast<T*>(CachedDeviceAlloc(bytes, &bytes_, &device_));
     count_ = bytes_ / sizeof(T);
   }
   void Upload(const std::vector<T>& v, cudaStream_t s) {
@@ -91,8 +93,9 @@ class DevBuf {
     }
     if (count > count_ || ptr_ == nullptr) {
       size_t got = 0;
+      int dev = 0;
       const size_t want = count + count / 4;
-      T* fresh = static_cast<T*>(CachedDeviceAlloc(std::max<size_t>(1, want) * sizeof(T), &got));
+      T* fresh = static_cast<T*>(CachedDeviceAlloc(std::max<size_t>(1, want) * sizeof(T), &got, &dev));
       if (keep > 0) {
         CudaCheck(cudaMemcpyAsync(fresh, ptr_, keep * sizeof(T), cudaMemcpyDeviceToDevice, s), "keep");
         // the old block goes back to the cache only after the copy read it
@@ -101,6 +104,7 @@ class DevBuf {
       Free();
       ptr_ = fresh;
       bytes_ = got;
+      device_ = dev;
       count_ = got / sizeof(T);
     }
     if (count > keep) {
@@ -114,6 +118,7 @@ class DevBuf {
   T* ptr_{nullptr};
   size_t count_{0};
   size_t bytes_{0};
+  int device_{0};  // the device the block was allocated on
 };
 
 /// Device task lists of a symbolic analysis plus the launch parameters of
@@ -142,6 +147,11 @@ struct FactorPlan {
   const int32_t* pack_tasks{nullptr};
   const int32_t* tc_tasks{nullptr};
   TcArgs tc{};
+  /// Test hook of the one-launch solve: a supernode whose forward flag is
+  /// never published (-1: none) and the polls a wait may take (0: the
+  /// default of about a second).
+  int solve_withhold{-1};
+  uint32_t solve_wait_polls{0};
 };
 
 /// Doubles per inverted 32 x 32 diagonal block (the inverse and its
@@ -222,6 +232,9 @@ class Engine {
   /// of a problem with the same columns, frames and point rows; the
   /// iterations re-analyse if the state leaves its pattern).
   Engine(HostProblem problem, SymPiece piece);
+  /// Several problems with their analyses done already (one piece per
+  /// problem, as AnalyzeInstance returns them).
+  Engine(std::vector<HostProblem> problems, std::vector<SymPiece> pieces);
   /// Replaces this engine's single problem by `next` on the same grid with
   /// the same active columns, whose first `keep_rows` point rows are the
   /// current problem's (they stay on the device; the rest is uploaded). The
@@ -264,6 +277,10 @@ class Engine {
   void FinishIteration();
   /// Copies results and cost histories (rows of `capacity`).
   void EndSolve(sdfgpu_solve_result* results, double* cost_history, int capacity);
+  /// True once instance i's solve has ended (converged, failed or out of
+  /// iterations); its result as EndSolve would report it.
+  [[nodiscard]] bool InstanceDone(int i) const;
+  [[nodiscard]] sdfgpu_solve_result InstanceResult(int i) const;
   [[nodiscard]] cudaStream_t stream() const { return stream_; }
   /// True when an instance's state left its pattern and the next
   /// LaunchIteration would re-analyse it first.
@@ -281,12 +298,17 @@ class Engine {
   [[nodiscard]] const IterTimes& times() const { return times_; }
   [[nodiscard]] int64_t factor_flops() const { return sym_.total_flops; }
   [[nodiscard]] const Symbolic& symbolic() const { return sym_; }
+  /// Test hook: the next solves' one-launch triangular solve never
+  /// publishes supernode `withhold`'s forward flag (-1: normal) and a wait
+  /// takes at most `wait_polls` polls (0: the default).
+  void SetSolveFault(int withhold, uint32_t wait_polls);
 
  private:
-  void Init(SymPiece* piece);
-  /// The analysis of host_ (or the given piece's structure) while the
-  /// problem uploads (keep_rows of its point rows are on the device).
-  void AnalyzeAndUpload(SymPiece* piece, int64_t keep_rows);
+  void Init(std::vector<SymPiece>* pieces);
+  /// The analysis of host_ (or the given pieces' structure, one per
+  /// instance) while the problem uploads (keep_rows of its point rows are on
+  /// the device).
+  void AnalyzeAndUpload(std::vector<SymPiece>* pieces, int64_t keep_rows);
   void BuildLayout();
   void UploadProblem(int64_t keep_rows = 0);
   /// Symbolic analysis of every instance at its current state (host only).
@@ -407,6 +429,8 @@ class Engine {
   CUtensorMap tc_map_{};
   const float* tc_map_base_{nullptr};
   int64_t tc_map_rows_{0};
+  int solve_withhold_{-1};
+  uint32_t solve_wait_polls_{0};
   DevBuf<int64_t> fmp_ptr_, fmp_off_;
   DevBuf<int32_t> fmp_col_;
   std::vector<int32_t> mixed_;

@@ -1386,10 +1386,10 @@ __device__ __forceinline__ void BackwardTreeBody(const DeviceView& V, const Supe
 /// Iterations of a bounded wait on another block's flag (about a second).
 constexpr uint32_t kWaitLimit = 1u << 21;
 
-/// Thread-level bounded wait until *flag != 0 (acquire at GPU scope); false
-/// when the limit ran out.
-__device__ __forceinline__ bool WaitFlag(const uint32_t* flag) {
-  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+/// Thread-level bounded wait until *flag != 0 (acquire at GPU scope), at
+/// most `limit` polls; false when the limit ran out.
+__device__ __forceinline__ bool WaitFlag(const uint32_t* flag, uint32_t limit) {
+  for (uint32_t it = 0; it < limit; ++it) {
     uint32_t v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
     if (v != 0u) {
@@ -1416,9 +1416,12 @@ __device__ __forceinline__ void SetFlag(uint32_t* flag) {
 /// of resident blocks; no level boundary holds fast fronts behind slow ones.
 /// sync: [0] task counter, [2, 2 + S) forward flags, [2 + S, 2 + 2S)
 /// backward flags, all zero at launch. A wait that runs out of its limit
-/// marks the instance kStatusWaitTimeout and lets the task's dependents go.
+/// (wait_limit polls) marks the instance kStatusWaitTimeout and lets the
+/// task's dependents go. withhold: a supernode whose forward flag is never
+/// published (-1: none), the test hook that makes a wait run out.
 __global__ void __launch_bounds__(256, 1) KSolveTree(DeviceView V, const int32_t* level_sn, int num_sn,
-                                                     const double* dvec, const double* inv, uint32_t* sync) {
+                                                     const double* dvec, const double* inv, uint32_t* sync,
+                                                     int withhold, uint32_t wait_limit) {
   extern __shared__ double buf[];
   __shared__ int task;
   __shared__ int go;
@@ -1442,10 +1445,10 @@ __global__ void __launch_bounds__(256, 1) KSolveTree(DeviceView V, const int32_t
       if (active) {
         if (forward) {
           for (int ci = 0; ci < S.child_count && ready; ++ci) {
-            ready = WaitFlag(fdone + V.child_list[S.child_begin + ci]);
+            ready = WaitFlag(fdone + V.child_list[S.child_begin + ci], wait_limit);
           }
         } else {
-          ready = WaitFlag(S.parent >= 0 ? bdone + S.parent : fdone + s);
+          ready = WaitFlag(S.parent >= 0 ? bdone + S.parent : fdone + s, wait_limit);
         }
         if (!ready) {
           atomicOr(V.status + S.instance, kStatusWaitTimeout);
@@ -1470,7 +1473,7 @@ __global__ void __launch_bounds__(256, 1) KSolveTree(DeviceView V, const int32_t
       }
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && !(forward && s == withhold)) {
       __threadfence();
       SetFlag((forward ? fdone : bdone) + s);
     }
@@ -1609,8 +1612,9 @@ int LaunchSolveLevels(const Symbolic& S, const DeviceView& V, const FactorPlan& 
     // find no task left return at once
     const int blocks = std::min(2 * num_sn, sms);
     CudaCheck(cudaMemsetAsync(P.solve_sync, 0, SolveSyncWords(num_sn) * sizeof(uint32_t), stream), "solve flags");
-    KSolveTree<<<static_cast<unsigned>(blocks), 256, tree_smem, stream>>>(V, P.level_sn, num_sn, P.dvec, P.inv,
-                                                                          P.solve_sync);
+    KSolveTree<<<static_cast<unsigned>(blocks), 256, tree_smem, stream>>>(
+        V, P.level_sn, num_sn, P.dvec, P.inv, P.solve_sync, P.solve_withhold,
+        P.solve_wait_polls > 0 ? P.solve_wait_polls : kWaitLimit);
     CudaCheck(cudaGetLastError(), "solve kernel");
     return 1;
   }

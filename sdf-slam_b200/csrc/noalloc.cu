@@ -17,7 +17,11 @@
 // whose work overlaps on the GPU (from two host threads, for example) race on
 // the array and must be serialised by the caller. The first call on a device
 // looks up the array's device address (cudaGetSymbolAddress) with that device
-// current; make that first call before any stream capture.
+// current; with CUDA's lazy module loading that lookup also loads this code
+// and reserves the array, so the first call belongs at start-up, before the
+// host framework's allocator takes the free memory and before any stream
+// capture. The work runs on the calling thread's per-thread default stream,
+// which does not wait for the host application's other streams.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -121,7 +125,9 @@ void DenseLdltSolveNoAlloc(int n, const double* a, const double* b, double* x) {
     perm[i] = i;
   }
   int32_t consts[4] = {0, 0, 1, 0};  // level list {supernode 0}, status 0, active 1, no child
-  cudaStream_t s = 0;  // legacy default stream: no stream object is created
+  // the calling thread's per-thread default stream: no stream object is
+  // created and the host application's streams are not waited for
+  cudaStream_t s = cudaStreamPerThread;
   const size_t nn = static_cast<size_t>(n);
   CudaCheck(cudaMemcpyAsync(base + kFrontOff, a, nn * nn * sizeof(double), cudaMemcpyHostToDevice, s), "A");
   CudaCheck(cudaMemcpyAsync(base + kRhsOff, b, nn * sizeof(double), cudaMemcpyHostToDevice, s), "b");

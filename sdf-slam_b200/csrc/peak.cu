@@ -48,7 +48,7 @@ double MeasureFp64PeakTflops() {
   const int blocks = sms * std::max(1, per_sm);
   const int iterations = 1 << 14;
   size_t got = 0;
-  auto* out = static_cast<double*>(CachedDeviceAlloc(sizeof(double) * blocks * kPeakThreads, &got));
+  auto* out = static_cast<double*>(CachedDeviceAlloc(sizeof(double) * blocks * kPeakThreads, &got, &dev));
   cudaStream_t s = nullptr;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   double best = 0.0;
@@ -72,11 +72,11 @@ double MeasureFp64PeakTflops() {
     if (s != nullptr) {
       cudaStreamSynchronize(s);
     }
-    CachedDeviceFree(out, got);
+    CachedDeviceFree(out, got, dev);
     throw;
   }
   CudaCheck(cudaStreamSynchronize(s), "peak");
-  CachedDeviceFree(out, got);
+  CachedDeviceFree(out, got, dev);
   cudaEventDestroy(ev[0]);
   cudaEventDestroy(ev[1]);
   cudaStreamDestroy(s);

@@ -6,11 +6,8 @@
 
 namespace sdfgpu {
 
-int64_t EstimateDeviceBytes(const HostProblem& hp, bool mixed) {
-  std::vector<HostProblem> v{hp};
-  InstanceLayout L{};
-  L.col_off = 0;
-  const Symbolic S = Analyze(v, {L}, 32, 64);
+int64_t EstimateDeviceBytes(const HostProblem& hp, const SymPiece& piece, bool mixed) {
+  const Symbolic& S = piece.s;
   const int64_t P = hp.num_points();
   const int64_t nodes = static_cast<int64_t>(hp.nx) * hp.ny;
   // fronts grow when a re-analysis widens the coupling margin; a mixed solve
@@ -19,7 +16,7 @@ int64_t EstimateDeviceBytes(const HostProblem& hp, bool mixed) {
   bytes += P * (8 * 8 + 4 * 8 + 4 * 8 + 48);       // row records, pose offsets, cells, sort buffers, specs
   bytes += nodes * (8 * 3 + 4 * 4);                 // map, backup, index maps
   bytes += static_cast<int64_t>(S.mm_off.size()) * 8 + static_cast<int64_t>(S.mp_off.size()) * 12;
-  bytes += static_cast<int64_t>(S.sn_rows.size()) * 8 + static_cast<int64_t>(S.update_tasks.size()) * 4;
+  bytes += static_cast<int64_t>(S.sn_rows.size()) * 8 + static_cast<int64_t>(S.sn.size()) * 256;
   bytes += static_cast<int64_t>(hp.num_params()) * 8 * 8;
   return bytes;
 }
@@ -33,21 +30,21 @@ Server::Server(int64_t budget_bytes, int max_batch)
   });
 }
 
-bool Server::Busy(Request& r) {
-  if (!r.job.valid()) {
+bool Server::Busy(Cohort& c) {
+  if (!c.job.valid()) {
     return false;
   }
-  if (r.job.wait_for(std::chrono::seconds(0)) != std::future_status::ready) {
+  if (c.job.wait_for(std::chrono::seconds(0)) != std::future_status::ready) {
     return true;
   }
   try {
-    r.job.get();
+    c.job.get();
   } catch (const Error& e) {
-    r.engine.reset();
-    r.result.status = e.code();
+    c.failed = true;
+    c.status = e.code();
   } catch (...) {
-    r.engine.reset();
-    r.result.status = SDFGPU_ERR_CUDA;
+    c.failed = true;
+    c.status = SDFGPU_ERR_CUDA;
   }
   return false;
 }
@@ -69,12 +66,15 @@ int64_t Server::Submit(HostProblem hp, const sdfgpu_solver_options& options) {
       options.refine_steps < 0 || options.refine_steps > 16) {
     Fail(SDFGPU_ERR_INVALID_ARGUMENT, "invalid solver options");
   }
-  const int64_t bytes = EstimateDeviceBytes(hp, options.precision == SDFGPU_PRECISION_MIXED);
+  // the analysis that sizes the request is the one its engine will use
+  SymPiece piece = AnalyzeInstance(hp, kDefaultMargin);
+  const int64_t bytes = EstimateDeviceBytes(hp, piece, options.precision == SDFGPU_PRECISION_MIXED);
   if (bytes > budget_) {
     Fail(SDFGPU_ERR_OUT_OF_MEMORY, "request footprint " + std::to_string(bytes) + " bytes exceeds the budget");
   }
   auto r = std::make_unique<Request>();
   r->hp = std::move(hp);
+  r->piece = std::move(piece);
   r->options = options;
   r->bytes = bytes;
   r->submitted = std::chrono::steady_clock::now();
@@ -126,7 +126,9 @@ void Server::Cancel(int64_t id) {
     r.result.status = SDFGPU_ERR_INVALID_ARGUMENT;
     done_cv_.notify_all();
   } else if (r.state == State::kRunning) {
-    r.state = State::kCancelled;  // the worker frees it after the current round
+    // its cohort keeps iterating it; the result is dropped
+    r.state = State::kCancelled;
+    r.result.status = SDFGPU_ERR_INVALID_ARGUMENT;
   }
 }
 
@@ -145,7 +147,7 @@ void Server::Stats(double* stats) {
   stats[0] = static_cast<double>(submitted_);
   stats[1] = static_cast<double>(completed_);
   stats[2] = static_cast<double>(queue_.size());
-  stats[3] = static_cast<double>(running_.size());
+  stats[3] = static_cast<double>(running_);
   stats[4] = pct(0.50);
   stats[5] = pct(0.99);
   stats[6] = secs > 0 ? completed_ / secs : 0.0;
@@ -155,148 +157,179 @@ void Server::Stats(double* stats) {
 void Server::Drain(int64_t timeout_ms) {
   std::unique_lock<std::mutex> lk(mu_);
   const bool ok = done_cv_.wait_for(lk, std::chrono::milliseconds(timeout_ms),
-                                    [this] { return queue_.empty() && running_.empty(); });
+                                    [this] { return queue_.empty() && running_ == 0; });
   if (!ok) {
     Fail(SDFGPU_ERR_TIMEOUT, "requests still pending after the drain timeout");
   }
 }
 
-void Server::Retire(Request& r) {
-  // caller holds no lock; engine work happens outside the mutex
-  r.result.status = r.result.status;
-  r.engine.reset();
+void Server::Answer(Cohort& c) {
+  for (size_t i = 0; i < c.members.size(); ++i) {
+    Request& r = *c.members[i];
+    if (r.answered || (!c.failed && !c.engine->InstanceDone(static_cast<int>(i)))) {
+      continue;
+    }
+    sdfgpu_solve_result res{};
+    if (c.failed) {
+      res.status = c.status;
+    } else {
+      try {
+        res = c.engine->InstanceResult(static_cast<int>(i));
+        r.map_values.resize(static_cast<size_t>(r.hp.nx) * r.hp.ny);
+        r.poses.resize(3 * static_cast<size_t>(r.hp.num_frames()));
+        c.engine->GetState(static_cast<int>(i), r.map_values.data(), r.poses.data());
+      } catch (const Error& e) {
+        res.status = e.code();
+      }
+    }
+    r.answered = true;
+    std::lock_guard<std::mutex> lk(mu_);
+    --running_;
+    if (r.state == State::kCancelled) {
+      continue;
+    }
+    r.result = res;
+    r.state = State::kDone;
+    ++completed_;
+    latencies_ms_.push_back(
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - r.submitted).count());
+  }
 }
 
 void Server::Loop() {
+  // Cohorts running at once: a request that arrives while this many are on
+  // the GPU waits for the next cohort, which takes every request then
+  // waiting (up to max_batch running requests in all).
+  constexpr size_t kMaxCohorts = 4;
   for (;;) {
-    std::vector<Request*> admitted;
+    std::unique_ptr<Cohort> fresh;
     {
       std::unique_lock<std::mutex> lk(mu_);
-      cv_.wait_for(lk, std::chrono::milliseconds(50),
-                   [this] { return stop_ || !queue_.empty() || !running_.empty(); });
+      cv_.wait_for(lk, std::chrono::milliseconds(50), [this] { return stop_ || !queue_.empty() || running_ > 0; });
       if (stop_) {
         break;
       }
-      while (!queue_.empty() && static_cast<int>(running_.size() + admitted.size()) < max_batch_) {
-        Request& r = *requests_[queue_.front()];
-        if (used_bytes_ + r.bytes > budget_ && !(running_.empty() && admitted.empty())) {
-          break;  // wait for memory to free up
+      if (!queue_.empty() && cohorts_.size() < kMaxCohorts && running_ < max_batch_) {
+        auto c = std::make_unique<Cohort>();
+        while (!queue_.empty() && running_ + static_cast<int64_t>(c->members.size()) < max_batch_) {
+          Request& r = *requests_[queue_.front()];
+          if (used_bytes_ + c->bytes + r.bytes > budget_ && !(cohorts_.empty() && c->members.empty())) {
+            break;  // wait for memory to free up
+          }
+          queue_.pop_front();
+          c->bytes += r.bytes;
+          r.state = State::kRunning;
+          c->members.push_back(&r);
         }
-        queue_.pop_front();
-        used_bytes_ += r.bytes;
-        r.state = State::kRunning;
-        admitted.push_back(&r);
+        if (!c->members.empty()) {
+          used_bytes_ += c->bytes;
+          running_ += static_cast<int64_t>(c->members.size());
+          fresh = std::move(c);
+        }
       }
     }
-    for (Request* r : admitted) {
-      // engine setup (upload, symbolic analysis, initial cost) off this thread
-      r->job = std::async(std::launch::async, [this, r] {
+    if (fresh) {
+      // engine setup (concatenation of the members' analyses, upload,
+      // initial cost) off this thread
+      Cohort* c = fresh.get();
+      c->job = std::async(std::launch::async, [this, c] {
         cudaSetDevice(device_);
-        std::vector<HostProblem> v{r->hp};
-        r->engine = std::make_unique<Engine>(std::move(v));
-        r->engine->BeginSolve({r->options});
+        std::vector<HostProblem> problems;
+        std::vector<SymPiece> pieces;
+        std::vector<sdfgpu_solver_options> options;
+        for (Request* r : c->members) {
+          problems.push_back(r->hp);
+          pieces.push_back(std::move(r->piece));
+          options.push_back(r->options);
+        }
+        c->engine = std::make_unique<Engine>(std::move(problems), std::move(pieces));
+        c->engine->BeginSolve(options);
       });
-      std::lock_guard<std::mutex> lk(mu_);
-      running_.push_back(r);
+      cohorts_.push_back(std::move(fresh));
     }
-    // one pass: finish every iteration whose device work is done, enqueue
-    // the next iteration of every idle request; a request whose state left
-    // its pattern is re-analysed off this thread
+    // one pass: finish every iteration whose device work is done, answer the
+    // members whose solves ended, enqueue the next iteration of every idle
+    // cohort; a cohort with a member whose state left its pattern is
+    // re-analysed off this thread
     bool progressed = false;
-    for (Request* r : running_) {
-      if (Busy(*r)) {
-        continue;
-      }
-      if (!r->engine) {
+    for (auto& cp : cohorts_) {
+      Cohort& c = *cp;
+      if (Busy(c) || c.failed || !c.engine) {
         continue;
       }
       try {
-        if (r->in_flight) {
-          if (!r->engine->IterationReady()) {
+        if (c.in_flight) {
+          if (!c.engine->IterationReady()) {
             continue;
           }
-          r->in_flight = false;
-          r->engine->FinishIteration();
+          c.in_flight = false;
+          c.engine->FinishIteration();
           progressed = true;
+          int running = 0;
+          for (size_t i = 0; i < c.members.size(); ++i) {
+            running += c.engine->InstanceDone(static_cast<int>(i)) ? 0 : 1;
+          }
           std::lock_guard<std::mutex> lk(mu_);
-          ++iterations_;
+          iterations_ += running;
         }
-        if (r->state != State::kRunning || r->engine->SolveDone()) {
+        Answer(c);
+        if (c.engine->SolveDone()) {
           continue;
         }
-        if (r->engine->NeedsReanalysis()) {
-          Engine* e = r->engine.get();
-          r->job = std::async(std::launch::async, [this, e] {
+        if (c.engine->NeedsReanalysis()) {
+          Engine* e = c.engine.get();
+          c.job = std::async(std::launch::async, [this, e] {
             cudaSetDevice(device_);
             e->ReanalyzeNow();
           });
           continue;
         }
-        r->engine->LaunchIteration();
-        r->in_flight = true;
+        c.engine->LaunchIteration();
+        c.in_flight = true;
         progressed = true;
       } catch (const Error& e) {
-        r->in_flight = false;
-        r->result.status = e.code();
-        r->engine.reset();
+        c.in_flight = false;
+        c.failed = true;
+        c.status = e.code();
       }
     }
     if (!progressed) {
       // nothing finished and nothing new to enqueue: yield briefly
       std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
-    // retire finished, failed and cancelled requests
-    std::vector<Request*> still;
-    for (Request* r : running_) {
-      if (r->job.valid() || r->in_flight) {
-        still.push_back(r);  // its host job or device iteration must end first
+    // retire cohorts whose members are all answered (or that failed)
+    std::vector<std::unique_ptr<Cohort>> still;
+    for (auto& cp : cohorts_) {
+      Cohort& c = *cp;
+      if (c.job.valid() || c.in_flight) {
+        still.push_back(std::move(cp));  // its host job or device iteration must end first
         continue;
       }
-      const bool cancelled = r->state == State::kCancelled;
-      const bool failed = !r->engine;
-      const bool done = !failed && r->engine->SolveDone();
-      if (!(cancelled || failed || done)) {
-        still.push_back(r);
+      if (!c.failed && c.engine && !c.engine->SolveDone()) {
+        still.push_back(std::move(cp));
         continue;
       }
-      if (done && !cancelled) {
-        try {
-          r->engine->EndSolve(&r->result, nullptr, 0);
-          r->map_values.resize(static_cast<size_t>(r->hp.nx) * r->hp.ny);
-          r->poses.resize(3 * static_cast<size_t>(r->hp.num_frames()));
-          r->engine->GetState(0, r->map_values.data(), r->poses.data());
-        } catch (const Error& e) {
-          r->result.status = e.code();
-        }
-      }
-      Retire(*r);
+      Answer(c);
+      c.engine.reset();
       std::lock_guard<std::mutex> lk(mu_);
-      used_bytes_ -= r->bytes;
-      if (!cancelled) {
-        r->state = State::kDone;
-        ++completed_;
-        latencies_ms_.push_back(
-            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - r->submitted).count());
-      } else {
-        r->result.status = SDFGPU_ERR_INVALID_ARGUMENT;
-      }
+      used_bytes_ -= c.bytes;
     }
     {
       std::lock_guard<std::mutex> lk(mu_);
-      running_.swap(still);
-      if (queue_.empty() && running_.empty()) {
+      cohorts_.swap(still);
+      if (queue_.empty() && running_ == 0) {
         done_cv_.notify_all();
       }
     }
   }
-  for (Request* r : running_) {
-    if (r->job.valid()) {
-      r->job.wait();
+  for (auto& cp : cohorts_) {
+    if (cp->job.valid()) {
+      cp->job.wait();
     }
-    if (r->engine && r->in_flight) {
-      cudaStreamSynchronize(r->engine->stream());
+    if (cp->engine && cp->in_flight) {
+      cudaStreamSynchronize(cp->engine->stream());
     }
-    r->engine.reset();
+    cp->engine.reset();
   }
 }
 

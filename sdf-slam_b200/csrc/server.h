@@ -1,12 +1,19 @@
-// Serving loop with continuous batching. Each admitted request keeps its
-// state, symbolic analysis and factors resident on the device in its own
-// engine (own CUDA stream). The loop keeps one LM iteration of every running
-// request in flight: it finishes an iteration as soon as its stream's event
-// reports it done and enqueues that request's next one, so requests of very
-// different sizes overlap on the GPU without waiting for one another. Requests are admitted while their estimated device footprint
-// fits the budget and retire as soon as their solve ends. Host work of a
-// request (building its engine, re-analysing a pattern its state left) runs
-// on a helper thread while the other requests keep iterating.
+// Serving loop with continuous batching. Requests that are waiting when the
+// loop has room are merged into one batched engine (a cohort): every kernel
+// of an LM iteration covers all of its members, whatever their sizes, and
+// the cohort keeps their states, symbolic structure and factors resident on
+// the device. Several cohorts run at once on their own CUDA streams, so
+// requests that arrive while others are on the GPU are admitted as soon as a
+// cohort slot and memory are free and their work overlaps with the running
+// ones. The loop keeps one iteration of every cohort in flight, finishes it
+// when its stream's event reports it done and enqueues the next; a member
+// whose solve has ended is answered at once (its latency stops there) while
+// the others keep iterating. Admission is by device footprint (state,
+// specs, symbolic structure and factors) against the budget, computed from
+// the symbolic analysis that Submit runs and the cohort's engine then reuses.
+// Host work of a cohort (building its engine, re-analysing a member whose
+// state left its pattern) runs on a helper thread while the other cohorts
+// keep iterating. A member's iterations are bitwise those of its solve alone.
 #pragma once
 
 #include <condition_variable>
@@ -24,9 +31,9 @@
 namespace sdfgpu {
 
 /// Device bytes an engine for `hp` will hold (state, specs, symbolic
-/// structure, fronts; the mixed-precision copies when `mixed`), from a
-/// host-side symbolic analysis.
-int64_t EstimateDeviceBytes(const HostProblem& hp, bool mixed);
+/// structure, fronts; the mixed-precision copies when `mixed`), from its
+/// host-side symbolic analysis `piece`.
+int64_t EstimateDeviceBytes(const HostProblem& hp, const SymPiece& piece, bool mixed);
 
 class Server {
  public:
@@ -46,22 +53,32 @@ class Server {
   struct Request {
     int64_t id{0};
     HostProblem hp;
+    SymPiece piece;  // its symbolic analysis (handed to the cohort's engine)
+    sdfgpu_solve_result result{};
     sdfgpu_solver_options options{};
     int64_t bytes{0};
     State state{State::kQueued};
+    bool answered{false};  // result and state copied out
     std::chrono::steady_clock::time_point submitted;
-    std::unique_ptr<Engine> engine;
-    std::future<void> job;  // host work in flight (engine setup, re-analysis)
-    bool in_flight{false};  // an LM iteration is enqueued on the device
-    sdfgpu_solve_result result{};
     std::vector<double> map_values;
     std::vector<double> poses;
   };
+  /// Requests solved together in one batched engine.
+  struct Cohort {
+    std::vector<Request*> members;  // instance i of the engine is members[i]
+    std::unique_ptr<Engine> engine;
+    std::future<void> job;  // host work in flight (engine setup, re-analysis)
+    bool in_flight{false};  // an LM iteration is enqueued on the device
+    bool failed{false};
+    int status{SDFGPU_OK};
+    int64_t bytes{0};
+  };
   void Loop();
-  void Retire(Request& r);
-  /// True while the request's host job runs; collects a finished job (a
-  /// failure marks the request failed).
-  bool Busy(Request& r);
+  /// True while the cohort's host job runs; collects a finished job (a
+  /// failure marks the cohort failed).
+  bool Busy(Cohort& c);
+  /// Copies out the result and state of every member whose solve has ended.
+  void Answer(Cohort& c);
 
   int64_t budget_;
   int max_batch_;
@@ -72,7 +89,8 @@ class Server {
   bool stop_{false};
   std::deque<int64_t> queue_;
   std::map<int64_t, std::unique_ptr<Request>> requests_;
-  std::vector<Request*> running_;
+  std::vector<std::unique_ptr<Cohort>> cohorts_;
+  int64_t running_{0};  // requests in cohorts that have not been answered
   int64_t used_bytes_{0};
   int64_t next_id_{1};
   int64_t submitted_{0};

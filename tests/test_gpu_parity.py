@@ -314,6 +314,8 @@ def test_autotuned_schedule_keeps_parity():
 
 
 def test_server_results_equal_alone_and_in_mix():
+    """Requests merged into batched cohorts while others run give, each,
+    bitwise the result of their solve alone."""
     scs = [scenes.request_scene(seed=100 + i, grid_range=(40, 70), pose_range=(8, 24), iterations=6)
            for i in range(5)]
     specs = [scene_specs(sc, P.ProblemOptions(hallucination_points=4))[0] for sc in scs]
@@ -365,3 +367,61 @@ def test_ldlt_factor_only_singular():
     solver = P.LdltSolver(n, outer, inner)
     with pytest.raises(RuntimeError, match="factorization failed"):
         solver.factorize(vals)
+
+
+def test_solve_wait_that_runs_out_reports_timeout_and_keeps_state():
+    """The one-launch solve's blocks wait on flags other blocks publish, each
+    wait bounded. With a flag that is never published (test hook) and a
+    short limit the wait runs out: the solve fails with SDFGPU_ERR_TIMEOUT
+    (TimeoutError), the state is not moved, and the device keeps working."""
+    sc = scenes.room_scene(seed=1)
+    specs, _ = scene_specs(sc, P.ProblemOptions(hallucination_points=4))
+    gpu = P.Problem.from_specs(specs)
+    P.solve(gpu, P.SolverOptions(max_iterations=1))
+    assert gpu.debug_supernode_count() > 1
+    before = gpu.state()
+    gpu.debug_solve_fault(0, 4096)
+    with pytest.raises(TimeoutError):
+        P.solve(gpu, P.SolverOptions(max_iterations=2))
+    after = gpu.state()
+    assert np.array_equal(before[0], after[0]) and np.array_equal(before[1], after[1])
+    gpu.debug_solve_fault(-1, 0)
+    r = P.solve(gpu, P.SolverOptions(max_iterations=2))
+    assert r.status == 0 and r.iterations == 2
+    # two fresh handles still solve to the same bits
+    a = P.Problem.from_specs(specs)
+    b = P.Problem.from_specs(specs)
+    ra = P.solve(a, P.SolverOptions(max_iterations=3))
+    rb = P.solve(b, P.SolverOptions(max_iterations=3))
+    assert ra.cost_history == rb.cost_history
+
+
+def test_server_refuses_a_request_over_the_budget():
+    """Admission by device footprint: a request whose own footprint exceeds
+    the budget is refused at submit with SDFGPU_ERR_OUT_OF_MEMORY."""
+    sc = scenes.request_scene(seed=7, grid_range=(120, 120), pose_range=(60, 60), iterations=5)
+    specs, _ = scene_specs(sc, P.ProblemOptions(hallucination_points=4))
+    server = P.Server(memory_budget_bytes=1 << 20, max_batch=4)
+    with pytest.raises(MemoryError, match="exceeds the budget"):
+        server.submit(specs, P.SolverOptions(max_iterations=5))
+    assert server.stats()["submitted"] == 0
+    server.close()
+
+
+def test_server_cancels_a_queued_request():
+    """With one request running at a time the later ones queue; a queued
+    request that is cancelled is never run and polls with
+    SDFGPU_ERR_INVALID_ARGUMENT, the others complete normally."""
+    scs = [scenes.request_scene(seed=200 + i, grid_range=g, pose_range=f, iterations=40)
+           for i, (g, f) in enumerate([((150, 150), (200, 200)), ((50, 50), (12, 12)), ((50, 50), (12, 12))])]
+    specs = [scene_specs(sc, P.ProblemOptions(hallucination_points=4))[0] for sc in scs]
+    server = P.Server(memory_budget_bytes=16 << 30, max_batch=1)
+    ids = [server.submit(s, P.SolverOptions(max_iterations=40, step_tolerance=0.0)) for s in specs]
+    server.cancel(ids[2])
+    server.drain(300000)
+    results = [server.poll(rid)[0] for rid in ids]
+    assert results[0].status == 0 and results[1].status == 0
+    assert results[0].iterations == 40 and results[1].iterations == 40
+    assert results[2].status == P.SDFGPU_ERR_INVALID_ARGUMENT
+    assert server.stats()["completed"] == 2
+    server.close()

@@ -63,3 +63,18 @@ def test_noalloc_rejects_sizes_beyond_the_maximum():
     a = np.eye(n)
     with pytest.raises(ValueError, match="outside 1..1024"):
         _noalloc(a, np.ones(n))
+
+
+def test_noalloc_zero_pivot_fails_then_next_call_succeeds():
+    """A zero pivot gives SDFGPU_ERR_NUMERICAL with the reference's message
+    (lm_solver.cpp:354-362); the next call clears the shared status word and
+    solves normally."""
+    n = 200
+    d = np.full(n, 2.0)
+    d[n // 2] = 0.0
+    with pytest.raises(RuntimeError, match="factorization failed"):
+        _noalloc(np.diag(d), np.ones(n))
+    a, b = _spd(150, 3)
+    x = _noalloc(a, b)
+    ref = _existing(a, b)
+    assert np.linalg.norm(x - ref) / np.linalg.norm(ref) <= TOL
