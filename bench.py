@@ -367,9 +367,29 @@ def run_mixed(P, args, specs, flusher):
         prob.autotune()
     steps = max(3, args.steps // 2)
     device, launches, phases = _timed_solves(P, prob, opts1, steps, flusher)
+    kernels = kernel_profile(P, prob, opts1, flusher)
     prob.close()
-    return {"value": steps / device, "unit": "LM iters/s", "refine_steps": args.refine_steps, "steps": steps,
-            "phase_ms_per_step": {k: 1000.0 * v / steps for k, v in zip(PHASES, phases)}}
+    out = {"value": steps / device, "unit": "LM iters/s", "refine_steps": args.refine_steps, "steps": steps,
+           "phase_ms_per_step": {k: 1000.0 * v / steps for k, v in zip(PHASES, phases)}, "kernels": kernels}
+    tc = kernels.get("KSchurTc")
+    if tc:
+        # split TF32 runs three tensor-core products per useful one; the
+        # TF32 dense rate of B200 is half its BF16 rate
+        peaks = {}
+        try:
+            with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+                peaks = json.load(f)
+        except OSError:
+            pass
+        bf16 = peaks.get("bf16_tflops")
+        tf32 = bf16 / 2 if bf16 else 1590.0 / 2
+        out["roofline_tensor_core"] = {
+            "kernel": "KSchurTc", "bound": "tensor", "unit": "TFLOP/s",
+            "achieved_useful": tc["achieved"], "achieved_executed": 3 * tc["achieved"], "peak": tf32,
+            "frac": 3 * tc["achieved"] / tf32,
+            "peak_source": ("half the measured BF16 burst rate (MEASURED_PEAKS.json bf16_tflops): TF32 dense "
+                            "runs at half the BF16 rate" if bf16 else "half the fallback BF16 1590 TFLOP/s")}
+    return out
 
 
 def run_batch(P, args, flusher):
@@ -420,6 +440,52 @@ def run_batch(P, args, flusher):
     out["vs_oracle"] = {"iterations": iters, "instances": sample,
                         "max_final_cost_rel_err": {k: float(np.max(v)) for k, v in errs.items()}}
     out["value"] = out["fp64"]["value"]
+    return out
+
+
+def run_batch_office(P, args, flusher, plain_value):
+    """`office_batch` independent 910-pose offices (different seeds) in one
+    engine: every kernel of an iteration covers all of them. Aggregate LM
+    iterations/s with plain FP64 and mixed precision (one-iteration solves,
+    L2 flushed between them), against the single office's plain FP64
+    iterations/s, and each mixed instance's final cost against its FP64
+    solve after the same iterations from the same start."""
+    import numpy as np
+    import sdf_slam_b200.scenes as scenes
+    count = args.office_batch
+    specs = [scene_specs(P, scenes.office_scene(seed=100 + q)) for q in range(count)]
+    steps = max(3, min(10, args.steps // 4))
+    out = {"instances": count, "unit": "LM iters/s (all instances)", "steps": steps,
+           "workload": "910-pose offices (seeds 100..), 200x200 @0.15 m, 180 beams, 6 hallucinated/beam"}
+    for precision in ("fp64", "mixed"):
+        batch = P.Problem.batch(specs)
+        opts1 = [P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=precision,
+                                 refine_steps=args.refine_steps)] * count
+        for _ in range(2):
+            P.solve(batch, opts1)
+        device = 0.0
+        phases = np.zeros(5)
+        for _ in range(steps):
+            flusher.flush()
+            P.solve(batch, opts1)
+            prof = batch.last_profile()
+            device += prof["span"]
+            phases += [prof["assemble"], prof["normal"], prof["factor"], prof["solve"], prof["update"]]
+        out[precision] = {"value": count * steps / device, "ms_per_batched_iteration": 1000.0 * device / steps,
+                          "phase_ms": {k: 1000.0 * v / steps for k, v in zip(PHASES, phases)},
+                          "over_single_plain": count * steps / device / plain_value}
+        batch.close()
+    iters = 3
+    finals = {}
+    for precision in ("fp64", "mixed"):
+        batch = P.Problem.batch(specs)
+        res = P.solve(batch, [P.SolverOptions(max_iterations=iters, step_tolerance=0.0, precision=precision,
+                                              refine_steps=args.refine_steps)] * count)
+        finals[precision] = np.array([r.final_cost for r in res])
+        batch.close()
+    out["mixed"]["max_final_cost_rel_err_vs_fp64"] = float(
+        np.max(np.abs(finals["mixed"] - finals["fp64"]) / np.abs(finals["fp64"])))
+    out["mixed"]["iterations_compared"] = iters
     return out
 
 
@@ -516,11 +582,30 @@ def _serve_pass(P, args, seed0, rate, check_oracle=False):
     return out
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the factor
-# phase's kernels in one LM iteration, from the committed one-kernel ncu
-# captures named beside each entry (L2 flushed before the captured step, as
-# here).
-FACTOR_TRAFFIC_BYTES = {}
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of a
+# kernel class on a workload, from the committed one-kernel ncu captures
+# named beside each entry (L2 flushed before the captured step, as here).
+KERNEL_TRAFFIC_BYTES = {}
+
+
+def kernel_profile(P, prob, opts1, flusher, iterations=3):
+    """Device time, launches and achieved rate per kernel class over
+    `iterations` one-iteration solves with every class timed."""
+    prob.kernel_timing()
+    for _ in range(iterations):
+        flusher.flush()
+        P.solve(prob, opts1)
+    times = prob.kernel_times()
+    prob.kernel_timing([])
+    out = {}
+    for name, t in times.items():
+        if t["launches"] == 0:
+            continue
+        rate = t["work"] / (t["ms"] * 1e-3) if t["ms"] > 0 else 0.0
+        out[name] = {"ms_per_iteration": t["ms"] / iterations, "launches_per_iteration": t["launches"] / iterations,
+                     "achieved": rate / (1e9 if t["work_unit"] == "bytes" else 1e12),
+                     "achieved_unit": "GB/s" if t["work_unit"] == "bytes" else "TFLOP/s"}
+    return out
 
 
 def run_gpu(args, dist, world, rank, local):
@@ -539,6 +624,11 @@ def run_gpu(args, dist, world, rank, local):
         P.solve(prob, opts1)
     tune = prob.autotune() if not args.no_autotune else None
     P.solve(prob, opts1)
+    # per-kernel device times of three iterations (every kernel class timed),
+    # then the timed region times the dominant class alone
+    kernels = kernel_profile(P, prob, opts1, flusher)
+    dominant_kernel = max(kernels, key=lambda k: kernels[k]["ms_per_iteration"])
+    prob.kernel_timing([dominant_kernel])
     flusher.sync()
     _barrier(dist)
     sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0)) \
@@ -555,6 +645,8 @@ def run_gpu(args, dist, world, rank, local):
     _barrier(dist)
     wall = time.perf_counter() - wall0
     clocks = sampler.stop() if sampler else None
+    dom = prob.kernel_times()[dominant_kernel]
+    prob.kernel_timing([])
     prof_last = prob.last_profile()
     flops = prof_last["factor_flops"]
     device_max = _reduce(dist, device_s, "MAX")
@@ -587,6 +679,9 @@ def run_gpu(args, dist, world, rank, local):
     single = world == 1
     mixed = run_mixed(P, args, specs, flusher) if (single and not args.no_mixed) else None
     batched = run_batch(P, args, flusher) if (args.batch_count > 0 and single) else None
+    plain_value = total_steps / device_max
+    batched_office = (run_batch_office(P, args, flusher, plain_value)
+                      if (args.office_batch > 0 and single and args.workload == "office") else None)
     flusher.close()
     fp64_peak = P.measure_fp64_peak() if rank == 0 else None
     vs_oracle, cpu = (None, None)
@@ -611,19 +706,33 @@ def run_gpu(args, dist, world, rank, local):
     # algorithmic bytes of the assembly phase per iteration (row kernels + sort)
     P_rows = z["num_points"]
     assemble_bytes = P_rows * (40 + 64 + 4) + P_rows * 4 * 2 * 2 * 2
+    # the dominant kernel, timed live over the timed region (CUDA events on
+    # the library's stream around each of its launches)
+    launches_dom = max(1, dom["launches"])
+    avg_ms = dom["ms"] / launches_dom
+    work_per_launch = dom["work"] / launches_dom
+    if dom["work_unit"] == "bytes":
+        achieved = work_per_launch / (avg_ms * 1e-3) / 1e9
+        peak, unit, bound, src = hbm, "GB/s", "hbm", hbm_src
+    else:
+        achieved = work_per_launch / (avg_ms * 1e-3) / 1e12
+        peak, unit, bound = fp64_peak, "TFLOP/s", "tensor"
+        src = "measured FP64 FMA throughput of this GPU (sdfgpu_measure_fp64_peak): the FP64 pipe bounds it"
+    roofline = {
+        "bound": bound, "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak,
+        "traffic": KERNEL_TRAFFIC_BYTES.get((args.workload, dominant_kernel)),
+        "kernel": dominant_kernel, "peak_source": src, "launches_timed": dom["launches"],
+        "avg_launch_ms": avg_ms, "work_per_launch": work_per_launch, "work_unit": dom["work_unit"]}
     roofline_factor = {
         "bound": "tensor", "achieved": flops / per_step[2] / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
         "frac": flops / per_step[2] / 1e12 / fp64_peak,
-        "traffic": FACTOR_TRAFFIC_BYTES.get(args.workload),
-        "kernel": "multifrontal LDL^T (KFactorFront + KPanel + KUpdate + KExtendAdd + KInvertDiagonal), FP64",
+        "kernel": "factor phase (every factorization kernel), FP64",
         "peak_source": "measured FP64 FMA throughput of this GPU (sdfgpu_measure_fp64_peak)",
-        "useful_flop_per_launch": flops}
+        "useful_flop_per_iteration": flops}
     roofline_assemble = {
         "bound": "hbm", "achieved": assemble_bytes / per_step[0] / 1e9, "peak": hbm, "unit": "GB/s",
         "frac": assemble_bytes / per_step[0] / 1e9 / hbm, "traffic": None,
-        "kernel": "point rows + cell sort", "peak_source": hbm_src}
-    dominant = PHASES[int(np.argmax(per_step))]
-    roofline = roofline_factor if dominant == "factor" else roofline_assemble
+        "kernel": "assembly phase (point rows + cell sort)", "peak_source": hbm_src}
     line = {
         "metric": METRIC, "value": total_steps / device_max, "unit": "LM iters/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * device_max / args.steps,
@@ -637,7 +746,8 @@ def run_gpu(args, dist, world, rank, local):
         "factor_gflop_per_step": flops / 1e9,
         "gpu_launches": int(launches),
         "roofline": roofline,
-        "roofline_other": roofline_assemble if roofline is roofline_factor else roofline_factor,
+        "roofline_phases": {"factor": roofline_factor, "assemble": roofline_assemble},
+        "kernels": kernels,
         "cpu_baseline": cpu,
         "vs_oracle": vs_oracle,
         "e2e": {"value": e2e_value, "unit": "LM iters/s", "h2d_bytes_per_step": int(h2d),
@@ -649,6 +759,7 @@ def run_gpu(args, dist, world, rank, local):
         "mixed": mixed,
         "mixed_over_fp64": mixed["value"] / (total_steps / device_max) if mixed else None,
         "batched": batched,
+        "batched_office": batched_office,
         "incremental": incremental,
         "served": served,
     }
@@ -677,6 +788,7 @@ def main():
     ap.add_argument("--incremental-iterations", type=int, default=5)
     ap.add_argument("--refine-steps", type=int, default=3)
     ap.add_argument("--batch-count", type=int, default=64)
+    ap.add_argument("--office-batch", type=int, default=8)
     ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[50.0, 100.0, 200.0, 500.0])
     ap.add_argument("--serve-iterations", type=int, default=20)

@@ -192,6 +192,22 @@ int sdfgpu_debug_solve_fault(sdfgpu_problem* problem, int32_t withhold_front, ui
  * device use). */
 int32_t sdfgpu_debug_supernode_count(sdfgpu_problem* problem);
 
+/* No counterpart in the reference: device time per kernel class of the
+ * handle's LM iterations. From the next iteration on, CUDA events on the
+ * handle's stream bracket every launch of the factorization and solve kernel
+ * classes in `class_mask` (bit c for class c, named by
+ * sdfgpu_kernel_class_name(c)); the totals restart at zero. 0 stops the
+ * timing. sdfgpu_kernel_times returns, per class since then, the device
+ * milliseconds, the launches and the algorithmic work of those launches
+ * (useful flops, 2 per multiply-add; bytes for the classes for which
+ * sdfgpu_kernel_class_is_memory_bound is 1); count <= SDFGPU_KERNEL_CLASSES,
+ * any output may be NULL. */
+#define SDFGPU_KERNEL_CLASSES 9
+int sdfgpu_kernel_timing(sdfgpu_problem* problem, uint32_t class_mask);
+int sdfgpu_kernel_times(sdfgpu_problem* problem, double* ms, int64_t* launches, double* work, int32_t count);
+const char* sdfgpu_kernel_class_name(int32_t kernel_class);
+int32_t sdfgpu_kernel_class_is_memory_bound(int32_t kernel_class);
+
 /* Number of instances in the handle (1 unless created as a batch). */
 int32_t sdfgpu_problem_count(const sdfgpu_problem* problem);
 

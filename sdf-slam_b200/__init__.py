@@ -394,6 +394,27 @@ class Problem:
         polls, so the solve ends with TimeoutError; -1 restores it."""
         _check(lib().sdfgpu_debug_solve_fault(self._h, int(withhold_front), int(wait_polls)))
 
+    def kernel_timing(self, classes=None):
+        """Times the launches of the named kernel classes (all when None, none
+        for an empty list) from the next iteration on (sdfgpu_kernel_timing);
+        totals restart at zero."""
+        names = kernel_class_names()
+        mask = (1 << len(names)) - 1 if classes is None else sum(1 << names.index(c) for c in classes)
+        _check(lib().sdfgpu_kernel_timing(self._h, mask))
+
+    def kernel_times(self) -> dict:
+        """{class name: {"ms", "launches", "work", "work_unit"}} since
+        kernel_timing: device milliseconds, launches and their algorithmic
+        work (useful flops, or bytes for the memory-bound classes)."""
+        names = kernel_class_names()
+        ms = np.zeros(len(names))
+        n = np.zeros(len(names), np.int64)
+        w = np.zeros(len(names))
+        _check(lib().sdfgpu_kernel_times(self._h, _d(ms), n.ctypes.data_as(_capi.c_i64_p), _d(w), len(names)))
+        return {k: {"ms": float(ms[c]), "launches": int(n[c]), "work": float(w[c]),
+                    "work_unit": "bytes" if lib().sdfgpu_kernel_class_is_memory_bound(c) else "flop"}
+                for c, k in enumerate(names)}
+
     def debug_supernode_count(self) -> int:
         return int(lib().sdfgpu_debug_supernode_count(self._h))
 
@@ -689,3 +710,11 @@ def measure_fp64_peak() -> float:
     v = ctypes.c_double()
     _check(lib().sdfgpu_measure_fp64_peak(ctypes.byref(v)))
     return v.value
+
+
+KERNEL_CLASSES = 9
+
+
+def kernel_class_names() -> list:
+    """Names of the kernel classes sdfgpu_kernel_timing can time."""
+    return [lib().sdfgpu_kernel_class_name(c).decode() for c in range(KERNEL_CLASSES)]

@@ -119,6 +119,10 @@ SIGNATURES = {
     "sdfgpu_measure_fp64_peak": (ctypes.c_int, [c_dbl_p]),
     "sdfgpu_debug_solve_fault": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_uint32]),
     "sdfgpu_debug_supernode_count": (ctypes.c_int32, [vp]),
+    "sdfgpu_kernel_timing": (ctypes.c_int, [vp, ctypes.c_uint32]),
+    "sdfgpu_kernel_times": (ctypes.c_int, [vp, c_dbl_p, c_i64_p, c_dbl_p, ctypes.c_int32]),
+    "sdfgpu_kernel_class_name": (ctypes.c_char_p, [ctypes.c_int32]),
+    "sdfgpu_kernel_class_is_memory_bound": (ctypes.c_int32, [ctypes.c_int32]),
     "sdfgpu_problem_count": (ctypes.c_int32, [vp]),
     "sdfgpu_problem_sizes": (ctypes.c_int, [vp, ctypes.c_int32, c_int_p]),
     "sdfgpu_problem_get_specs": (ctypes.c_int, [vp, ctypes.c_int32, c_int_p, c_dbl_p, c_dbl_p,

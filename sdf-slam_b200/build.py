@@ -41,8 +41,9 @@ SOURCES = {
     "incremental.cpp": ["-x", "cu"],
     "writers.cpp": ["-x", "cu"],
     "server.cpp": ["-x", "cu"],
+    "kernel_timer.cpp": ["-x", "cu"],
 }
-HEADERS = ["internal.h", "device.cuh", "engine.h", "ldlt.h", "server.h", "host_pool.h", "incremental.h", "schur_tc.h",
+HEADERS = ["internal.h", "device.cuh", "engine.h", "ldlt.h", "server.h", "host_pool.h", "incremental.h", "schur_tc.h", "kernel_timer.h",
            "trig.cuh"]
 
 

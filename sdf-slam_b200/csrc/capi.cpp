@@ -245,6 +245,38 @@ int32_t sdfgpu_debug_supernode_count(sdfgpu_problem* problem) {
   return static_cast<int32_t>(problem->engine->symbolic().sn.size());
 }
 
+static_assert(sdfgpu::KernelTimer::kClasses == SDFGPU_KERNEL_CLASSES, "kernel class count");
+
+int sdfgpu_kernel_timing(sdfgpu_problem* problem, uint32_t class_mask) {
+  return Guard([&] { Eng(problem).SetKernelTiming(class_mask); });
+}
+
+int sdfgpu_kernel_times(sdfgpu_problem* problem, double* ms, int64_t* launches, double* work, int32_t count) {
+  return Guard([&] {
+    if (count < 0 || count > sdfgpu::KernelTimer::kClasses) {
+      sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "count is outside 0..SDFGPU_KERNEL_CLASSES");
+    }
+    const sdfgpu::KernelTimer& t = Eng(problem).kernel_timer();
+    for (int c = 0; c < count; ++c) {
+      if (ms != nullptr) {
+        ms[c] = t.Ms(c);
+      }
+      if (launches != nullptr) {
+        launches[c] = t.Launches(c);
+      }
+      if (work != nullptr) {
+        work[c] = t.Work(c);
+      }
+    }
+  });
+}
+
+const char* sdfgpu_kernel_class_name(int32_t kernel_class) { return sdfgpu::KernelTimer::Name(kernel_class); }
+
+int32_t sdfgpu_kernel_class_is_memory_bound(int32_t kernel_class) {
+  return sdfgpu::KernelTimer::ByteBound(kernel_class) ? 1 : 0;
+}
+
 int32_t sdfgpu_problem_count(const sdfgpu_problem* problem) {
   return problem == nullptr ? 0 : static_cast<int32_t>(problem->host.size());
 }

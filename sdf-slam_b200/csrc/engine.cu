@@ -881,6 +881,8 @@ FactorPlan Engine::Plan() {
   P.inv = inv_.get();
   P.solve_withhold = solve_withhold_;
   P.solve_wait_polls = solve_wait_polls_;
+  // only the iteration's own factor and solve phases are timed
+  P.timer = timing_phase_ ? &timer_ : nullptr;
   if (any_mixed_ && sym_.tc_pack_rows > 0 && tc_map_base_ != nullptr) {
     P.tc_map = &tc_map_;
     P.pack_tasks = pack_tasks_.get();
@@ -991,6 +993,12 @@ void Engine::Reanalyze(const std::vector<int>& which) {
   UploadSymbolic();
   ++times_.reanalyses;
   times_.reanalysis_host += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void Engine::SetKernelTiming(uint32_t mask) {
+  CudaCheck(cudaStreamSynchronize(stream_), "timing sync");
+  timer_.SetMask(mask);
+  DropGraph();  // the captured phases carry the previous event nodes
 }
 
 void Engine::SetSolveFault(int withhold, uint32_t wait_polls) {
@@ -1502,10 +1510,16 @@ void Engine::EnqueuePhase(int phase) {
       LaunchNormal();
       break;
     case 2:
+      // the timed launches of phases 2 and 3 are recorded afresh
+      timer_.NewSequence();
+      timing_phase_ = true;
       LaunchFactor();
+      timing_phase_ = false;
       break;
     case 3:
+      timing_phase_ = true;
       LaunchSolve();
+      timing_phase_ = false;
       break;
     default:
       LaunchStepAndCost(need_backup_);
@@ -1636,6 +1650,7 @@ void Engine::FinishIteration() {
     CudaCheck(cudaEventElapsedTime(&ms, ev_[q], ev_[q + 1]), "phase timing");
     *acc[q] += ms * 1e-3;
   }
+  timer_.Accumulate();
   ++times_.iterations;
   bool any_revert = false;
   std::vector<int32_t> revert(I, 0);

@@ -152,6 +152,8 @@ struct FactorPlan {
   /// default of about a second).
   int solve_withhold{-1};
   uint32_t solve_wait_polls{0};
+  /// Per-kernel device time of the launches (null: not timed).
+  KernelTimer* timer{nullptr};
 };
 
 /// Doubles per inverted 32 x 32 diagonal block (the inverse and its
@@ -302,6 +304,10 @@ class Engine {
   /// publishes supernode `withhold`'s forward flag (-1: normal) and a wait
   /// takes at most `wait_polls` polls (0: the default).
   void SetSolveFault(int withhold, uint32_t wait_polls);
+  /// Times the launches of the kernel classes in `mask` (KernelTimer) from
+  /// the next iteration on, with zeroed totals; 0 stops timing.
+  void SetKernelTiming(uint32_t mask);
+  [[nodiscard]] const KernelTimer& kernel_timer() const { return timer_; }
 
  private:
   void Init(std::vector<SymPiece>* pieces);
@@ -431,6 +437,8 @@ class Engine {
   int64_t tc_map_rows_{0};
   int solve_withhold_{-1};
   uint32_t solve_wait_polls_{0};
+  KernelTimer timer_;
+  bool timing_phase_{false};  // EnqueuePhase is inside the factor or solve phase
   DevBuf<int64_t> fmp_ptr_, fmp_off_;
   DevBuf<int32_t> fmp_col_;
   std::vector<int32_t> mixed_;

@@ -1536,12 +1536,34 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
     Fail(SDFGPU_ERR_INVALID_ARGUMENT, "factorization schedule out of range");
   }
   int launches = 0;
+  // algorithmic work of a level's launches (flops: 2 per multiply-add, the
+  // dense LDL^T operation counts; bytes for the memory-bound classes), for
+  // the kernel timer
+  const bool tc = P.tc_map != nullptr;
+  auto level_sum = [&S](int l, auto&& f) {
+    double w = 0.0;
+    for (int q = S.level_begin[static_cast<size_t>(l)]; q < S.level_begin[static_cast<size_t>(l) + 1]; ++q) {
+      w += f(S.sn[static_cast<size_t>(S.level_sn[static_cast<size_t>(q)])]);
+    }
+    return w;
+  };
   for (int l = 0; l < S.num_levels; ++l) {
     const TaskRange ea = S.ea_range[static_cast<size_t>(l)];
     if (ea.count > 0) {
       // staged in shared memory unless a front of the level is too wide
       const size_t stage = static_cast<size_t>(S.ea_stage[static_cast<size_t>(l)]) * sizeof(double);
       const bool staged = stage <= static_cast<size_t>(kEaStageDoubles) * sizeof(double);
+      const TimedLaunch tl(P.timer, KernelTimer::kExtendAdd, stream, [&] {
+        // each child's update entry read, its parent entry read and written
+        return level_sum(l, [&S](const SupernodeRec& r) {
+          double b = 0.0;
+          for (int ci = 0; ci < r.child_count; ++ci) {
+            const double m = S.sn[static_cast<size_t>(S.child_list[static_cast<size_t>(r.child_begin + ci)])].nrows;
+            b += 24.0 * m * (m + 1.0) / 2.0;
+          }
+          return b;
+        });
+      });
       KExtendAdd<<<static_cast<unsigned>(ea.count), 256, staged ? stage : 0, stream>>>(
           V, P.ea_tasks + 4 * ea.begin, P.ea_child, staged ? 1 : 0);
       ++launches;
@@ -1550,6 +1572,12 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
     if (sm.count > 0) {
       const int kmax = S.small_max_k[static_cast<size_t>(l)];
       const size_t bytes = FactorFrontSmem(kmax);
+      const TimedLaunch tl(P.timer, KernelTimer::kFactorFront, stream, [&] {
+        return level_sum(l, [&S](const SupernodeRec& r) {
+          const double k = r.ncols;
+          return r.ncols <= S.small_pivots ? 2.0 * k * k * k / 3.0 + static_cast<double>(r.nrows) * k * k : 0.0;
+        });
+      });
       KFactorFront<<<static_cast<unsigned>(sm.count), S.small_threads[static_cast<size_t>(l)], bytes, stream>>>(
           V, P.small_tasks + 3 * sm.begin, P.dvec);
       ++launches;
@@ -1558,12 +1586,35 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
       const size_t slot = static_cast<size_t>(S.panel_index_base[static_cast<size_t>(l)] + t);
       const TaskRange pr = S.panel_range[slot];
       if (pr.count > 0) {
+        const TimedLaunch tl(P.timer, KernelTimer::kPanel, stream, [&] {
+          return level_sum(l, [&S, t](const SupernodeRec& r) {
+            const int c0 = t * kPanel;
+            if (r.ncols <= S.small_pivots || c0 >= r.ncols) {
+              return 0.0;
+            }
+            const double w = std::min(kPanel, r.ncols - c0);
+            return 2.0 * w * w * w / 3.0 + static_cast<double>(r.F - c0 - w) * w * w;
+          });
+        });
         KPanel<<<static_cast<unsigned>(pr.count), kPanelRowsPerBlock, 0, stream>>>(V, P.panel_tasks + 3 * pr.begin,
                                                                                    P.dvec, S.panel_rows);
         ++launches;
       }
       const TaskRange ur = S.update_range[slot];
       if (ur.count > 0) {
+        const TimedLaunch tl(P.timer, KernelTimer::kUpdatePanel, stream, [&] {
+          return level_sum(l, [&S, t](const SupernodeRec& r) {
+            const int c0 = t * kPanel;
+            const int c1 = std::min(r.ncols, c0 + kPanel);
+            if (r.ncols <= S.small_pivots || c0 >= r.ncols || c1 >= r.ncols) {
+              return 0.0;
+            }
+            // columns [c1, k) of the rows [c1, F), lower part, by w pivots
+            const double nc = r.ncols - c1;
+            const double entries = nc * r.F - (static_cast<double>(c1) + r.ncols - 1) * nc / 2.0;
+            return 2.0 * (c1 - c0) * entries;
+          });
+        });
         KUpdate<<<static_cast<unsigned>(ur.count), 256, 0, stream>>>(V, P.update_tasks + 4 * ur.begin, P.dvec);
         ++launches;
       }
@@ -1573,17 +1624,38 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
       // cores (KUpdate skips their SIMT tiles)
       const TaskRange pk = S.pack_range[static_cast<size_t>(l)];
       const TaskRange tr = S.tc_range[static_cast<size_t>(l)];
+      double pack_bytes = 0.0;
+      double tc_flops = 0.0;
+      if (P.timer != nullptr) {
+        level_sum(l, [&](const SupernodeRec& r) {
+          if (r.tc_pack >= 0) {
+            const double m = r.nrows;
+            const double k = r.ncols;
+            pack_bytes += 4.0 * m * k + 4.0 * static_cast<double>(TcPackRows(r.ncols, r.nrows)) * kTcChunk;
+            tc_flops += k * m * (m + 1.0);
+          }
+          return 0.0;
+        });
+      }
       launches += LaunchSchurTc(*P.tc_map, P.tc, P.pack_tasks + 3 * pk.begin, pk.count, P.tc_tasks + 3 * tr.begin,
-                                tr.count, stream);
+                                tr.count, stream, P.timer, pack_bytes, tc_flops);
     }
     const TaskRange sr = S.update_range[static_cast<size_t>(S.panel_index_base.back() + l)];
     if (sr.count > 0) {
+      const TimedLaunch tl(P.timer, KernelTimer::kUpdateSchur, stream, [&] {
+        return level_sum(l, [tc](const SupernodeRec& r) {
+          const double m = r.nrows;
+          return tc && r.tc_pack >= 0 ? 0.0 : static_cast<double>(r.ncols) * m * (m + 1.0);
+        });
+      });
       KUpdate<<<static_cast<unsigned>(sr.count), 256, 0, stream>>>(V, P.update_tasks + 4 * sr.begin, P.dvec);
       ++launches;
     }
   }
   if (P.inv != nullptr && P.num_inv > 0) {
     // inverted diagonal blocks for the one-launch solve
+    const TimedLaunch tl(P.timer, KernelTimer::kInvertDiagonal, stream,
+                         [&] { return static_cast<double>(P.num_inv) * (8.0 + 16.0) * 1024.0; });
     KInvertDiagonal<<<static_cast<unsigned>((P.num_inv + 3) / 4), 128, 0, stream>>>(V, P.inv_tasks, P.num_inv,
                                                                                    P.inv);
     ++launches;
@@ -1612,6 +1684,17 @@ int LaunchSolveLevels(const Symbolic& S, const DeviceView& V, const FactorPlan& 
     // find no task left return at once
     const int blocks = std::min(2 * num_sn, sms);
     CudaCheck(cudaMemsetAsync(P.solve_sync, 0, SolveSyncWords(num_sn) * sizeof(uint32_t), stream), "solve flags");
+    const TimedLaunch tl(P.timer, KernelTimer::kSolveTree, stream, [&] {
+      // every entry of L read twice (forward, backward), FP32 in the grid
+      // fronts of a mixed solve, and the inverted diagonal blocks
+      double b = static_cast<double>(P.num_inv) * 2.0 * 8.0 * 1024.0;
+      for (const SupernodeRec& r : S.sn) {
+        const double k = r.ncols;
+        const double elem = (P.tc_map != nullptr && r.pose_root == 0) ? 4.0 : 8.0;
+        b += 2.0 * elem * (k * (k + 1.0) / 2.0 + static_cast<double>(r.nrows) * k);
+      }
+      return b;
+    });
     KSolveTree<<<static_cast<unsigned>(blocks), 256, tree_smem, stream>>>(
         V, P.level_sn, num_sn, P.dvec, P.inv, P.solve_sync, P.solve_withhold,
         P.solve_wait_polls > 0 ? P.solve_wait_polls : kWaitLimit);

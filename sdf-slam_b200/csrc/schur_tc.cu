@@ -387,7 +387,8 @@ void EncodePackMap(CUtensorMap* map, float* pack, int64_t rows) {
 size_t SchurTcSmemBytes() { return static_cast<size_t>(kStages) * kStageBytes + 1024; }
 
 int LaunchSchurTc(const CUtensorMap& map, const TcArgs& A, const int32_t* pack_tasks, int64_t pack_count,
-                  const int32_t* tc_tasks, int64_t tc_count, cudaStream_t stream) {
+                  const int32_t* tc_tasks, int64_t tc_count, cudaStream_t stream, KernelTimer* timer,
+                  double work_pack, double work_flops) {
   // the shared memory limit is a per-device attribute of the kernel
   static bool configured[64] = {};
   int dev = 0;
@@ -402,10 +403,12 @@ int LaunchSchurTc(const CUtensorMap& map, const TcArgs& A, const int32_t* pack_t
   }
   int launches = 0;
   if (pack_count > 0) {
+    const TimedLaunch tl(timer, KernelTimer::kPackSchur, stream, [&] { return work_pack; });
     KPackSchur<<<static_cast<unsigned>(pack_count), 256, 0, stream>>>(A, pack_tasks);
     ++launches;
   }
   if (tc_count > 0) {
+    const TimedLaunch tl(timer, KernelTimer::kSchurTc, stream, [&] { return work_flops; });
     KSchurTc<<<static_cast<unsigned>(tc_count), 128, SchurTcSmemBytes(), stream>>>(map, A, tc_tasks);
     ++launches;
   }

@@ -8,6 +8,7 @@
 #include <cstdint>
 
 #include "device.cuh"
+#include "kernel_timer.h"
 
 namespace sdfgpu {
 
@@ -45,8 +46,10 @@ void EncodePackMap(CUtensorMap* map, float* pack, int64_t rows);
 /// Dynamic shared memory of KSchurTc.
 size_t SchurTcSmemBytes();
 /// KPackSchur over (sn, row tile, chunk) triples, then KSchurTc over
-/// (sn, tile i, tile j) triples. Returns the kernels launched.
+/// (sn, tile i, tile j) triples. Returns the kernels launched. work_pack
+/// (bytes) and work_flops (useful flops) are what a timer records.
 int LaunchSchurTc(const CUtensorMap& map, const TcArgs& A, const int32_t* pack_tasks, int64_t pack_count,
-                  const int32_t* tc_tasks, int64_t tc_count, cudaStream_t stream);
+                  const int32_t* tc_tasks, int64_t tc_count, cudaStream_t stream, KernelTimer* timer,
+                  double work_pack, double work_flops);
 
 }  // namespace sdfgpu
