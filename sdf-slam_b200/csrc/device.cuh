@@ -137,6 +137,13 @@ struct DeviceView {
   double* asm_fronts; // assembly target: the FP64 normal matrix (== fronts when no solve is mixed)
   double* upd;
   int32_t tc_schur;   // 1: the wide FP32 fronts' Schur complements run on the tensor cores
+  // adaptive refinement of mixed steps: per instance 1 once its corrections
+  // became negligible (null outside the refinement rounds), per instance the
+  // largest |correction| and |step| of the round (bits of non-negative
+  // doubles, ordered like the values), and whether any instance still refines
+  int32_t* refine_done;
+  unsigned long long* refine_max;
+  int32_t* refine_left;
   // map-pose entries grouped by frame (transpose of mp_*): per global frame
   // the node columns coupled to it and the front offset of (pose var 0, node)
   const int64_t* fmp_ptr;

@@ -33,6 +33,8 @@ __global__ void KNormalMatVecMap(DeviceView V, const double* x, double* y);
 __global__ void KNormalMatVecPose(DeviceView V, const double* x, double* y);
 __global__ void KRefineResidual(DeviceView V, const double* y, double* r);
 __global__ void KAddCorrection(DeviceView V, const double* corr);
+__global__ void KRefineReset(DeviceView V);
+__global__ void KRefineCheck(DeviceView V, double tol);
 void LaunchCellSort(const int32_t* pt_cell, int64_t n, int64_t num_cells, int32_t* keys_a, int32_t* vals_a,
                     int32_t* keys_b, int32_t* vals_b, int32_t* hist, cudaStream_t stream, bool* result_in_a);
 
@@ -714,6 +716,9 @@ void Engine::AllocMixed() {
   res_.Alloc(static_cast<size_t>(std::max(n_, 1)));
   ax_.Alloc(static_cast<size_t>(std::max(n_, 1)));
   corr_.Alloc(static_cast<size_t>(std::max(n_, 1)));
+  refine_done_.Alloc(host_.size());
+  refine_max_.Alloc(2 * host_.size());
+  refine_left_.Alloc(1);
   if (sym_.tc_pack_rows > 0) {
     pack_.Alloc(static_cast<size_t>(sym_.tc_pack_rows) * kTcChunk);
     const int64_t rows = static_cast<int64_t>(pack_.size() / kTcChunk);
@@ -909,17 +914,31 @@ void Engine::LaunchSolve() {
   }
   // iterative refinement of the mixed instances' steps against the FP64
   // normal matrix: r = rhs - A delta, delta += (LDL^T)^-1 r
-  DeviceView Vr = V_;
+  // A round stops counting for an instance once its largest correction is
+  // below kRefineTol of its largest step entry: each round shrinks the
+  // error by about cond(A) * 2^-24, so the next one would move the step by
+  // far less than the FP64 path's own rounding differences.
+  constexpr double kRefineTol = 1e-13;
+  DeviceView Vm = V_;
+  Vm.refine_done = refine_done_.get();
+  Vm.refine_max = refine_max_.get();
+  Vm.refine_left = refine_left_.get();
+  DeviceView Vr = Vm;
   Vr.rhs = res_.get();
   Vr.step = corr_.get();
-  for (int round = 0; round < refine_steps_; ++round) {
-    KNormalMatVecMap<<<Blocks(n_, 128), 128, 0, stream_>>>(V_, step_.get(), ax_.get());
-    KNormalMatVecPose<<<Blocks(3 * static_cast<int64_t>(total_frames_) * 32, 256), 256, 0, stream_>>>(
-        V_, step_.get(), ax_.get());
-    KRefineResidual<<<Blocks(n_, 256), 256, 0, stream_>>>(V_, ax_.get(), res_.get());
-    times_.launches += 3 + LaunchSolveLevels(sym_, Vr, Plan(), stream_);
-    KAddCorrection<<<Blocks(n_, 256), 256, 0, stream_>>>(V_, corr_.get());
+  if (refine_steps_ > 0) {
+    KRefineReset<<<1, 128, 0, stream_>>>(Vm);
     ++times_.launches;
+  }
+  for (int round = 0; round < refine_steps_; ++round) {
+    KNormalMatVecMap<<<Blocks(n_, 128), 128, 0, stream_>>>(Vm, step_.get(), ax_.get());
+    KNormalMatVecPose<<<Blocks(3 * static_cast<int64_t>(total_frames_) * 32, 256), 256, 0, stream_>>>(
+        Vm, step_.get(), ax_.get());
+    KRefineResidual<<<Blocks(n_, 256), 256, 0, stream_>>>(Vm, ax_.get(), res_.get());
+    times_.launches += 3 + LaunchSolveLevels(sym_, Vr, Plan(), stream_);
+    KAddCorrection<<<Blocks(n_, 256), 256, 0, stream_>>>(Vm, corr_.get());
+    KRefineCheck<<<1, 256, 0, stream_>>>(Vm, kRefineTol);
+    times_.launches += 2;
   }
   CudaCheck(cudaGetLastError(), "refinement kernels");
 }

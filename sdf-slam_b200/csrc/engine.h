@@ -428,6 +428,8 @@ class Engine {
   DevBuf<int32_t> conv_tasks_;
   int64_t conv_count_{0};
   DevBuf<double> res_, ax_, corr_;
+  DevBuf<int32_t> refine_done_, refine_left_;
+  DevBuf<unsigned long long> refine_max_;
   // tensor-core Schur update of the wide FP32 fronts: packed operands of one
   // level and their tensor map (re-encoded when the buffer moves)
   DevBuf<int32_t> pack_tasks_, tc_tasks_;

@@ -1427,6 +1427,9 @@ __global__ void __launch_bounds__(256, 1) KSolveTree(DeviceView V, const int32_t
   __shared__ int go;
   uint32_t* fdone = sync + 2;
   uint32_t* bdone = sync + 2 + num_sn;
+  if (V.refine_left != nullptr && *V.refine_left == 0) {
+    return;  // a refinement round after every instance's step became final
+  }
   for (;;) {
     if (threadIdx.x == 0) {
       task = static_cast<int>(atomicAdd(sync, 1u));
@@ -1439,7 +1442,8 @@ __global__ void __launch_bounds__(256, 1) KSolveTree(DeviceView V, const int32_t
     const bool forward = t < num_sn;
     const int s = level_sn[forward ? t : 2 * num_sn - 1 - t];
     const SupernodeRec S = V.sn[s];
-    const bool active = V.active[S.instance] != 0;
+    // refinement rounds skip the instances whose step is final
+    const bool active = V.active[S.instance] != 0 && (V.refine_done == nullptr || V.refine_done[S.instance] == 0);
     if (threadIdx.x == 0) {
       bool ready = true;
       if (active) {

@@ -36,6 +36,51 @@ __global__ void KConvertFronts(DeviceView V, const int32_t* tasks, int chunk) {
   }
 }
 
+/// True when instance i takes no further refinement round.
+__device__ __forceinline__ bool RefineDone(const DeviceView& V, int i) {
+  return V.refine_done != nullptr && V.refine_done[i] != 0;
+}
+
+/// Opens the refinement rounds of a solve: no instance done, maxima zero.
+__global__ void KRefineReset(DeviceView V) {
+  for (int i = threadIdx.x; i < V.num_inst; i += blockDim.x) {
+    V.refine_done[i] = 0;
+    V.refine_max[2 * i] = 0ull;
+    V.refine_max[2 * i + 1] = 0ull;
+  }
+  if (threadIdx.x == 0) {
+    *V.refine_left = 1;
+  }
+}
+
+/// After a round: an instance whose largest correction is at most `tol`
+/// times its largest step entry is done (the next round would change its
+/// step by a fraction of that); the maxima restart and refine_left says
+/// whether any mixed instance still refines. One block.
+__global__ void KRefineCheck(DeviceView V, double tol) {
+  __shared__ int left;
+  if (threadIdx.x == 0) {
+    left = 0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < V.num_inst; i += blockDim.x) {
+    const double mc = __longlong_as_double(static_cast<long long>(V.refine_max[2 * i]));
+    const double ms = __longlong_as_double(static_cast<long long>(V.refine_max[2 * i + 1]));
+    if (V.refine_done[i] == 0 && mc <= tol * ms) {
+      V.refine_done[i] = 1;
+    }
+    V.refine_max[2 * i] = 0ull;
+    V.refine_max[2 * i + 1] = 0ull;
+    if (V.refine_done[i] == 0 && V.inst[i].mixed != 0 && V.active[i] != 0) {
+      left = 1;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *V.refine_left = left;
+  }
+}
+
 /// y = A x over the map columns of mixed instances (natural order), A read
 /// in FP64 from the assembled fronts: the 9-point map stencil (mm_off) and
 /// the node's map-pose blocks (mp_*). One thread per column; every sum runs
@@ -51,7 +96,7 @@ __global__ void KNormalMatVecMap(DeviceView V, const double* x, double* y) {
   }
   const int i = V.col_inst[c];
   const InstDev& I = V.inst[i];
-  if (I.mixed == 0 || V.active[i] == 0) {
+  if (I.mixed == 0 || V.active[i] == 0 || RefineDone(V, i)) {
     return;
   }
   const double* A = V.asm_fronts;
@@ -105,7 +150,7 @@ __global__ void KNormalMatVecPose(DeviceView V, const double* x, double* y) {
   const int c = fc + a;
   const int i = V.col_inst[c];
   const InstDev& I = V.inst[i];
-  if (I.mixed == 0 || V.active[i] == 0) {
+  if (I.mixed == 0 || V.active[i] == 0 || RefineDone(V, i)) {
     return;
   }
   const double* A = V.asm_fronts;
@@ -139,7 +184,7 @@ __global__ void KRefineResidual(DeviceView V, const double* y, double* r) {
     return;
   }
   const int i = V.col_inst[c];
-  r[c] = (V.inst[i].mixed != 0 && V.active[i] != 0) ? V.rhs[c] - y[c] : 0.0;
+  r[c] = (V.inst[i].mixed != 0 && V.active[i] != 0 && !RefineDone(V, i)) ? V.rhs[c] - y[c] : 0.0;
 }
 
 /// step += correction for the columns of mixed instances.
@@ -149,8 +194,13 @@ __global__ void KAddCorrection(DeviceView V, const double* corr) {
     return;
   }
   const int i = V.col_inst[c];
-  if (V.inst[i].mixed != 0 && V.active[i] != 0) {
-    V.step[c] += corr[c];
+  if (V.inst[i].mixed != 0 && V.active[i] != 0 && !RefineDone(V, i)) {
+    const double s = V.step[c] + corr[c];
+    V.step[c] = s;
+    if (V.refine_max != nullptr) {
+      atomicMax(V.refine_max + 2 * i, static_cast<unsigned long long>(__double_as_longlong(fabs(corr[c]))));
+      atomicMax(V.refine_max + 2 * i + 1, static_cast<unsigned long long>(__double_as_longlong(fabs(s))));
+    }
   }
 }
 
