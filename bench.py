@@ -303,11 +303,21 @@ def run_profile(args):
     opts = P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=args.precision,
                            refine_steps=args.refine_steps)
     for it in range(args.profile):
+        if it == 1:
+            gpu.kernel_timing()  # every kernel class, from the second iteration on
         r = P.solve(gpu, opts)
         prof = gpu.last_profile()
         print(f"iteration {it}: cost {r.final_cost:.9e} " +
               " ".join(f"{k}={v * 1e3:.3f}ms" if isinstance(v, float) and k != "factor_flops" else f"{k}={v}"
                        for k, v in prof.items()), flush=True)
+    if args.profile > 1:
+        n = args.profile - 1
+        for name, t in gpu.kernel_times().items():
+            if t["launches"]:
+                rate = t["work"] / (t["ms"] * 1e-3) / (1e9 if t["work_unit"] == "bytes" else 1e12)
+                unit = "GB/s" if t["work_unit"] == "bytes" else "TFLOP/s"
+                print(f"kernel {name}: {t['ms'] / n:.3f} ms/iteration, {t['launches'] / n:.1f} launches/iteration, "
+                      f"{rate:.2f} {unit}", flush=True)
     gpu.close()
     return 0
 
