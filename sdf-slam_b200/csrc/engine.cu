@@ -567,7 +567,8 @@ void Engine::UploadSymbolic() {
     max_front_ = std::max(max_front_, r.F);
   }
   ConfigureSolveKernels(max_front_);
-  solve_sync_.Alloc(SolveSyncWords(static_cast<int>(sym_.sn.size())));
+  solve_sync_.Alloc(SolveSyncWords(static_cast<int>(sym_.sn.size()), static_cast<int>(sym_.inv_tasks.size() / 2)));
+  UploadSolveTasks(s);
   inv_tasks_.Upload(sym_.inv_tasks, s);
   inv_.Alloc(std::max<size_t>(1, sym_.inv_tasks.size() / 2) * kInvBlockDoubles);
   std::vector<InstDev> inst(host_.size());
@@ -881,6 +882,12 @@ FactorPlan Engine::Plan() {
   P.dvec = dvec_.get();
   P.max_front = max_front_;
   P.solve_sync = solve_sync_.get();
+  P.solve_tasks = solve_tasks_.get();
+  P.num_solve_tasks = static_cast<int>(sym_.solve_tasks.size() / 4);
+  P.solve_parts = solve_parts_.get();
+  P.zpart_off = zpart_off_.get();
+  P.ys = ys_.get();
+  P.zpart = zpart_.get();
   P.inv_tasks = inv_tasks_.get();
   P.num_inv = static_cast<int>(sym_.inv_tasks.size() / 2);
   P.inv = inv_.get();
@@ -1029,6 +1036,14 @@ void Engine::SetSolveFault(int withhold, uint32_t wait_polls) {
   DropGraph();  // the captured solve holds the previous parameters
 }
 
+void Engine::UploadSolveTasks(cudaStream_t s) {
+  solve_tasks_.Upload(sym_.solve_tasks, s);
+  solve_parts_.Upload(sym_.solve_parts, s);
+  zpart_off_.Upload(sym_.zpart_off, s);
+  ys_.Alloc(static_cast<size_t>(std::max(n_, 1)));
+  zpart_.Alloc(static_cast<size_t>(std::max<int64_t>(1, sym_.zpart_doubles)));
+}
+
 void Engine::UploadSchedule() {
   DropGraph();
   CudaCheck(cudaStreamSynchronize(stream_), "schedule sync");
@@ -1041,6 +1056,7 @@ void Engine::UploadSchedule() {
   tc_tasks_.Upload(sym_.tc_tasks, stream_);
   level_sn_.Upload(sym_.level_sn, stream_);
   sn_.Upload(sym_.sn, stream_);
+  UploadSolveTasks(stream_);
   CudaCheck(cudaStreamSynchronize(stream_), "schedule upload");
 }
 

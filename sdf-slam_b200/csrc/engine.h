@@ -132,9 +132,16 @@ struct FactorPlan {
   const int32_t* level_sn{nullptr};
   double* dvec{nullptr};
   int max_front{1};
-  /// Counter and flags of the one-launch solve (SolveSyncWords words); the
-  /// solve runs level by level when this or inv is null.
+  /// Counter and flags of the one-launch solve (SolveSyncWords words), its
+  /// task list and scratch (Symbolic::solve_tasks); the solve runs level by
+  /// level when these or inv are null.
   uint32_t* solve_sync{nullptr};
+  const int32_t* solve_tasks{nullptr};
+  int num_solve_tasks{0};
+  const int32_t* solve_parts{nullptr};
+  const int64_t* zpart_off{nullptr};
+  double* ys{nullptr};
+  double* zpart{nullptr};
   /// (sn, panel) pairs of the diagonal blocks and their inverses
   /// (kInvBlockDoubles each), written after every factorization.
   const int32_t* inv_tasks{nullptr};
@@ -160,8 +167,11 @@ struct FactorPlan {
 /// transpose).
 constexpr int kInvBlockDoubles = 2 * 32 * 32;
 
-/// Words of the one-launch solve's counter and flags for num_sn supernodes.
-inline size_t SolveSyncWords(int num_sn) { return 2 + 2 * static_cast<size_t>(num_sn); }
+/// Words of the one-launch solve's counter and flags for num_sn supernodes
+/// and num_inv diagonal blocks.
+inline size_t SolveSyncWords(int num_sn, int num_inv) {
+  return 2 + 4 * static_cast<size_t>(num_sn) + 2 * static_cast<size_t>(num_inv);
+}
 
 /// Level-scheduled multifrontal LDL^T of the assembled fronts.
 /// Returns the number of kernels launched.
@@ -323,6 +333,8 @@ class Engine {
   Symbolic GlobalStructure();
   void UploadSymbolic();
   void UploadSchedule();
+  /// The one-launch solve's task list and its scratch.
+  void UploadSolveTasks(cudaStream_t s);
   /// Per-instance precision of the coming solve (1: mixed) and refinement
   /// rounds; re-uploads flags and drops the graphs when they change.
   void SetMode(const std::vector<int32_t>& mixed, int refine_steps);
@@ -418,6 +430,9 @@ class Engine {
   DevBuf<int32_t> ea_tasks_, ea_child_, panel_tasks_, update_tasks_, small_tasks_;
   DevBuf<double> fronts_, upd_;
   DevBuf<uint32_t> solve_sync_;  // counter and flags of the one-launch solve
+  DevBuf<int32_t> solve_tasks_, solve_parts_;
+  DevBuf<int64_t> zpart_off_;
+  DevBuf<double> ys_, zpart_;
   DevBuf<int32_t> inv_tasks_;     // diagonal blocks of L and their inverses
   DevBuf<double> inv_;
   // mixed precision: assembled FP64 normal matrix, FP32 work fronts, the

@@ -1106,6 +1106,35 @@ __device__ __forceinline__ T PivotL(const T* Fs, int64_t F, bool upper, int r, i
   return upper ? Fs[r * F + c] : Fs[c * F + r];
 }
 
+/// u = v_m - L21 y over rows [r0, r1) of the rows below the pivot block:
+/// thread per row, L21 column major (coalesced over rows), 16 loads in
+/// flight per batch. v = y (k values); v_m(r) from vm[r], or from upd when
+/// vm is null.
+template <typename T>
+__device__ __forceinline__ void ForwardRowsU(const DeviceView& V, const SupernodeRec& S, const T* Fs,
+                                             const double* v, const double* vm, int r0, int r1) {
+  const int k = S.ncols;
+  const int64_t F64 = S.F;
+  for (int r = r0 + static_cast<int>(threadIdx.x); r < r1; r += blockDim.x) {
+    const T* col = Fs + k + r;
+    double a0 = vm != nullptr ? vm[r] : V.upd[S.upd_off + r];
+    double a1 = 0.0;
+    for (int j0 = 0; j0 < k; j0 += kBatch) {
+      T lv[kBatch];
+#pragma unroll
+      for (int j = 0; j < kBatch; ++j) {
+        lv[j] = j0 + j < k ? col[(j0 + j) * F64] : T(0);
+      }
+#pragma unroll
+      for (int j = 0; j < kBatch; j += 2) {
+        a0 = fma(-static_cast<double>(lv[j]), j0 + j < k ? v[j0 + j] : 0.0, a0);
+        a1 = fma(-static_cast<double>(lv[j + 1]), j0 + j + 1 < k ? v[j0 + j + 1] : 0.0, a1);
+      }
+    }
+    V.upd[S.upd_off + r] = a0 + a1;
+  }
+}
+
 /// Forward solve of one front for the one-launch solve. Gathers the
 /// right-hand side and the children's update vectors, then per panel: warp 0
 /// forms y_p = M_p v_p (M_p the inverted diagonal block, copied into shared
@@ -1116,7 +1145,7 @@ __device__ __forceinline__ T PivotL(const T* Fs, int64_t F, bool upper, int r, i
 /// runs in a fixed order. buf: two blocks for M, then F doubles for v.
 template <typename T>
 __device__ __forceinline__ void ForwardTreeBody(const DeviceView& V, const SupernodeRec& S, const double* dvec,
-                                                const double* inv, double* buf) {
+                                                const double* inv, double* buf, double* ys) {
   const int k = S.ncols;
   const int F = S.F;
   const int64_t F64 = F;
@@ -1214,29 +1243,34 @@ __device__ __forceinline__ void ForwardTreeBody(const DeviceView& V, const Super
     WaitBlockCopies();
     __syncthreads();
   }
-  // u = v_m - L21 y: thread per row, L21 column major (coalesced over
-  // rows), 16 loads in flight per batch
-  for (int r = tid; r < F - k; r += nthreads) {
-    const T* col = Fs + k + r;
-    double a0 = v[k + r];
-    double a1 = 0.0;
-    for (int j0 = 0; j0 < k; j0 += kBatch) {
-      T lv[kBatch];
-#pragma unroll
-      for (int j = 0; j < kBatch; ++j) {
-        lv[j] = j0 + j < k ? col[(j0 + j) * F64] : T(0);
-      }
-#pragma unroll
-      for (int j = 0; j < kBatch; j += 2) {
-        a0 = fma(-static_cast<double>(lv[j]), j0 + j < k ? v[j0 + j] : 0.0, a0);
-        a1 = fma(-static_cast<double>(lv[j + 1]), j0 + j + 1 < k ? v[j0 + j + 1] : 0.0, a1);
-      }
+  if (ys != nullptr) {
+    // a wide front: v_m and y go out, KSolveTree's row-chunk tasks form u
+    for (int r = tid; r < F - k; r += nthreads) {
+      V.upd[S.upd_off + r] = v[k + r];
     }
-    V.upd[S.upd_off + r] = a0 + a1;
+    for (int j = tid; j < k; j += nthreads) {
+      ys[S.first_col + j] = v[j];
+    }
+  } else {
+    ForwardRowsU<T>(V, S, Fs, v, v + k, 0, F - k);
   }
   for (int j = tid; j < k; j += nthreads) {
     V.xs[S.first_col + j] = (1.0 / dvec[S.first_col + j]) * v[j];
   }
+}
+
+/// u = v_m - L21 y for the wide front's rows [r0, r1) (one row-chunk task):
+/// v_m from upd, y from ys.
+template <typename T>
+__device__ __forceinline__ void ForwardRowsTask(const DeviceView& V, const SupernodeRec& S, const double* ys,
+                                                int part, double* buf) {
+  const int k = S.ncols;
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    buf[j] = ys[S.first_col + j];
+  }
+  __syncthreads();
+  const int r0 = part * kSolveRowChunk;
+  ForwardRowsU<T>(V, S, WorkFront<T>(V, S), buf, nullptr, r0, min(S.nrows, r0 + kSolveRowChunk));
 }
 
 /// Backward solve of one front for the one-launch solve: z = x_k - L21^T x_R
@@ -1245,9 +1279,76 @@ __device__ __forceinline__ void ForwardTreeBody(const DeviceView& V, const Super
 /// every earlier pivot column c subtracts L(p, c)^T x_p (its L values loaded
 /// before the barrier). Writes xs and the step in natural order. buf: two
 /// blocks for M^T, then F doubles (z, then the gathered x_R).
+/// acc[q] = sum over rows r in [r0, r1) of L21(r, j0 + q) x_R(r), q < 4, for
+/// one warp (lanes over rows, four rows per lane per batch: 16 loads in
+/// flight), reduced by a fixed butterfly; xr indexed by r - r0.
+template <typename T>
+__device__ __forceinline__ void L21tColumns4(const T* Fs, int64_t F64, int k, int j0, int r0, int r1,
+                                             const double* xr, double (&acc)[4]) {
+  const int lane = threadIdx.x & 31;
+  acc[0] = acc[1] = acc[2] = acc[3] = 0.0;
+  for (int rb = r0; rb < r1; rb += 128) {
+    T lv[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int r = rb + 32 * u + lane;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        lv[u][q] = (r < r1 && j0 + q < k) ? Fs[(j0 + q) * F64 + k + r] : T(0);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int r = rb + 32 * u + lane;
+      const double x = r < r1 ? xr[r - r0] : 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        acc[q] = fma(static_cast<double>(lv[u][q]), x, acc[q]);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+    }
+  }
+}
+
+/// Backward row-chunk task of a wide front: the partial products
+/// L21(r0:r1, :)^T x_R(r0:r1) of its k pivot columns into zpart.
+template <typename T>
+__device__ __forceinline__ void BackwardRowsTask(const DeviceView& V, const SupernodeRec& S, int part,
+                                                 double* zpart, double* buf) {
+  const int k = S.ncols;
+  const int r0 = part * kSolveRowChunk;
+  const int r1 = min(S.nrows, r0 + kSolveRowChunk);
+  const int32_t* rows = V.sn_rows + S.rows_off;
+  for (int r = r0 + static_cast<int>(threadIdx.x); r < r1; r += blockDim.x) {
+    buf[r - r0] = __ldcg(V.xs + rows[r]);
+  }
+  __syncthreads();
+  const T* Fs = WorkFront<T>(V, S);
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  double* out = zpart + static_cast<int64_t>(part) * k;
+  for (int j0 = 4 * warp; j0 < k; j0 += 4 * nwarps) {
+    double acc[4];
+    L21tColumns4<T>(Fs, S.F, k, j0, r0, r1, buf, acc);
+    if (lane < 4 && j0 + lane < k) {
+      out[j0 + lane] = lane == 0 ? acc[0] : lane == 1 ? acc[1] : lane == 2 ? acc[2] : acc[3];
+    }
+  }
+}
+
+/// Backward solve of one front; zpart (parts > 0): the front's row-chunk
+/// partial products of L21^T x_R, summed in chunk order, in place of its own
+/// pass over L21.
 template <typename T>
 __device__ __forceinline__ void BackwardTreeBody(const DeviceView& V, const SupernodeRec& S, const double* inv,
-                                                 double* buf) {
+                                                 double* buf, const double* zpart, int parts) {
   const int k = S.ncols;
   const int m = S.nrows;
   const int64_t F64 = S.F;
@@ -1266,43 +1367,26 @@ __device__ __forceinline__ void BackwardTreeBody(const DeviceView& V, const Supe
   // M^T of panel q at Mb + q * kInvBlock
   const double* Mb = inv + static_cast<int64_t>(S.panel_base) * kInvBlock + kPanel * kPanel;
   CopyBlockAsync(Ms + (last_q & 1) * kPanel * kPanel, Mb + static_cast<int64_t>(last_q) * kInvBlock);
-  for (int r = tid; r < m; r += nthreads) {
-    xr[r] = __ldcg(V.xs + rows[r]);
-  }
-  __syncthreads();
-  for (int j0 = 4 * warp; j0 < k; j0 += 4 * nwarps) {
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-    // four rows per lane per batch: 16 loads in flight
-    for (int r0 = 0; r0 < m; r0 += 128) {
-      T lv[4][4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int r = r0 + 32 * u + lane;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          lv[u][q] = (r < m && j0 + q < k) ? Fs[(j0 + q) * F64 + k + r] : T(0);
-        }
+  if (parts > 0) {
+    for (int j = tid; j < k; j += nthreads) {
+      double a = 0.0;
+      for (int p = 0; p < parts; ++p) {
+        a += __ldcg(zpart + static_cast<int64_t>(p) * k + j);
       }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int r = r0 + 32 * u + lane;
-        const double x = r < m ? xr[r] : 0.0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          acc[q] = fma(static_cast<double>(lv[u][q]), x, acc[q]);
-        }
-      }
+      z[j] = __ldcg(V.xs + S.first_col + j) - a;
     }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
-      }
+  } else {
+    for (int r = tid; r < m; r += nthreads) {
+      xr[r] = __ldcg(V.xs + rows[r]);
     }
-    if (lane < 4 && j0 + lane < k) {
-      const double a = lane == 0 ? acc[0] : lane == 1 ? acc[1] : lane == 2 ? acc[2] : acc[3];
-      z[j0 + lane] = __ldcg(V.xs + S.first_col + j0 + lane) - a;
+    __syncthreads();
+    for (int j0 = 4 * warp; j0 < k; j0 += 4 * nwarps) {
+      double acc[4];
+      L21tColumns4<T>(Fs, F64, k, j0, 0, m, xr, acc);
+      if (lane < 4 && j0 + lane < k) {
+        const double a = lane == 0 ? acc[0] : lane == 1 ? acc[1] : lane == 2 ? acc[2] : acc[3];
+        z[j0 + lane] = __ldcg(V.xs + S.first_col + j0 + lane) - a;
+      }
     }
   }
   WaitBlockCopies();
@@ -1386,13 +1470,13 @@ __device__ __forceinline__ void BackwardTreeBody(const DeviceView& V, const Supe
 /// Iterations of a bounded wait on another block's flag (about a second).
 constexpr uint32_t kWaitLimit = 1u << 21;
 
-/// Thread-level bounded wait until *flag != 0 (acquire at GPU scope), at
-/// most `limit` polls; false when the limit ran out.
-__device__ __forceinline__ bool WaitFlag(const uint32_t* flag, uint32_t limit) {
+/// Thread-level bounded wait until *word >= expected (acquire at GPU
+/// scope), at most `limit` polls; false when the limit ran out.
+__device__ __forceinline__ bool WaitCount(const uint32_t* word, uint32_t expected, uint32_t limit) {
   for (uint32_t it = 0; it < limit; ++it) {
     uint32_t v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
-    if (v != 0u) {
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(word) : "memory");
+    if (v >= expected) {
       return true;
     }
     __nanosleep(100);
@@ -1400,59 +1484,280 @@ __device__ __forceinline__ bool WaitFlag(const uint32_t* flag, uint32_t limit) {
   return false;
 }
 
-/// Publishes *flag = 1 (release at GPU scope).
-__device__ __forceinline__ void SetFlag(uint32_t* flag) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag), "r"(1u) : "memory");
+/// Adds one to *word (release at GPU scope): a task's part is published.
+__device__ __forceinline__ void Publish(uint32_t* word) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(word), "r"(1u) : "memory");
+}
+
+/// What the one-launch solve's tasks read besides the view.
+struct SolveArgs {
+  const int32_t* tasks;   // (type, sn, part, 0) quads
+  int num_tasks;
+  const int32_t* parts;   // per sn: forward, backward parts
+  const int64_t* zoff;    // per sn: first partial-product double, or -1
+  double* ys;             // per pivot: y of wide fronts, v then y of panel-split roots
+  double* zpart;          // backward partial products of wide fronts
+  const double* dvec;
+  const double* inv;
+  uint32_t* sync;         // counter, then fdone, bdone, ydone, zdone per sn, then two flags per diagonal block
+  int num_sn;
+  int num_inv;
+  int withhold;
+  uint32_t wait_limit;
+};
+
+/// Whole-block bounded wait: thread 0 polls, every thread learns whether
+/// the wait succeeded; a wait that ran out marks the instance.
+__device__ __forceinline__ bool BlockWait(const DeviceView& V, const SupernodeRec& S, const uint32_t* word,
+                                          uint32_t expected, uint32_t limit) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = WaitCount(word, expected, limit) ? 1 : 0;
+    if (ok == 0) {
+      atomicOr(V.status + S.instance, kStatusWaitTimeout);
+    }
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+/// Right-hand side of a panel-split root: v = rhs plus the children's
+/// update vectors (children in their fixed order), into ys.
+__device__ __forceinline__ void RootGather(const DeviceView& V, const SupernodeRec& S, double* ys, double* v) {
+  const int k = S.ncols;
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    v[j] = V.rhs[V.perm[S.first_col + j]];
+  }
+  __syncthreads();
+  for (int ci = 0; ci < S.child_count; ++ci) {
+    const SupernodeRec C = V.sn[V.child_list[S.child_begin + ci]];
+    const int32_t* rel = V.sn_rel + C.rows_off;
+    const double* u = V.upd + C.upd_off;
+    for (int r = threadIdx.x; r < C.nrows; r += blockDim.x) {
+      v[rel[r]] += __ldcg(u + r);
+    }
+    __syncthreads();
+  }
+  for (int j = threadIdx.x; j < k; j += blockDim.x) {
+    ys[S.first_col + j] = v[j];
+  }
+}
+
+/// Forward panel q of a panel-split root (FP64, column-major L below the
+/// diagonal blocks): v_q -= L(q, p) y_p for every earlier panel p as its
+/// flag arrives (eight threads per row, four columns each, summed in a fixed
+/// order), then y_q = M_q v_q, D^-1 y_q into xs.
+template <typename T>
+__device__ __forceinline__ void RootForwardPanel(const DeviceView& V, const SupernodeRec& S, const SolveArgs& A,
+                                                 int q, uint32_t* pflag, double* buf) {
+  const int k = S.ncols;
+  const int64_t F64 = S.F;
+  const T* Fs = WorkFront<T>(V, S);
+  const int p0 = q * kPanel;
+  const int w = min(kPanel, k - p0);
+  const int tid = threadIdx.x;
+  double* vq = buf;                    // kPanel
+  double* yp = buf + kPanel;           // kPanel
+  double* part = buf + 2 * kPanel;     // 8 x kPanel
+  double* M = buf + 10 * kPanel;       // kPanel x kPanel
+  if (tid < kPanel) {
+    vq[tid] = tid < w ? A.ys[S.first_col + p0 + tid] : 0.0;
+  }
+  const int i = tid & (kPanel - 1);
+  const int g = tid >> 5;  // eight groups of four columns
+  for (int p = 0; p < q; ++p) {
+    // L(q, p) values of this thread, loaded before the wait
+    double l[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      l[c] = i < w ? static_cast<double>(Fs[static_cast<int64_t>(p * kPanel + 4 * g + c) * F64 + p0 + i]) : 0.0;
+    }
+    BlockWait(V, S, pflag + S.panel_base + p, 1u, A.wait_limit);
+    if (tid < kPanel) {
+      yp[tid] = __ldcg(A.ys + S.first_col + p * kPanel + tid);
+    }
+    __syncthreads();
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      acc = fma(l[c], yp[4 * g + c], acc);
+    }
+    part[g * kPanel + i] = acc;
+    __syncthreads();
+    if (tid < kPanel) {
+      const double s01 = part[i] + part[kPanel + i];
+      const double s23 = part[2 * kPanel + i] + part[3 * kPanel + i];
+      const double s45 = part[4 * kPanel + i] + part[5 * kPanel + i];
+      const double s67 = part[6 * kPanel + i] + part[7 * kPanel + i];
+      vq[i] -= (s01 + s23) + (s45 + s67);
+    }
+  }
+  const double* Mb = A.inv + static_cast<int64_t>(S.panel_base + q) * kInvBlock;
+  for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {
+    M[e] = Mb[e];
+  }
+  __syncthreads();
+  if (tid < kPanel) {
+    double a0 = 0.0;
+    double a1 = 0.0;
+#pragma unroll
+    for (int j = 0; j < kPanel; j += 2) {
+      a0 = fma(M[j * kPanel + tid], vq[j], a0);
+      a1 = fma(M[(j + 1) * kPanel + tid], vq[j + 1], a1);
+    }
+    if (tid < w) {
+      const double y = a0 + a1;
+      A.ys[S.first_col + p0 + tid] = y;
+      V.xs[S.first_col + p0 + tid] = (1.0 / A.dvec[S.first_col + p0 + tid]) * y;
+    }
+  }
+}
+
+/// Backward panel q of a panel-split root: z_q = (D^-1 y)_q minus
+/// L(p, q)^T x_p for every later panel p as its flag arrives, then
+/// x_q = M_q^T z_q into xs and the step.
+template <typename T>
+__device__ __forceinline__ void RootBackwardPanel(const DeviceView& V, const SupernodeRec& S, const SolveArgs& A,
+                                                  int q, uint32_t* bflag, double* buf) {
+  const int k = S.ncols;
+  const int64_t F64 = S.F;
+  const T* Fs = WorkFront<T>(V, S);
+  const int np = (k + kPanel - 1) / kPanel;
+  const int p0 = q * kPanel;
+  const int w = min(kPanel, k - p0);
+  const int tid = threadIdx.x;
+  double* zq = buf;
+  double* xp = buf + kPanel;
+  double* part = buf + 2 * kPanel;
+  double* M = buf + 10 * kPanel;
+  if (tid < kPanel) {
+    zq[tid] = tid < w ? __ldcg(V.xs + S.first_col + p0 + tid) : 0.0;
+  }
+  // thread (row i of z, group g of four rows of panel p)
+  const int i = tid >> 3;
+  const int g = tid & 7;
+  for (int p = np - 1; p > q; --p) {
+    const int wp = min(kPanel, k - p * kPanel);
+    double l[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const int r = 4 * g + c;
+      l[c] = (i < w && r < wp) ? static_cast<double>(Fs[static_cast<int64_t>(p0 + i) * F64 + p * kPanel + r]) : 0.0;
+    }
+    BlockWait(V, S, bflag + S.panel_base + p, 1u, A.wait_limit);
+    if (tid < kPanel) {
+      xp[tid] = tid < wp ? __ldcg(V.xs + S.first_col + p * kPanel + tid) : 0.0;
+    }
+    __syncthreads();
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      acc = fma(l[c], xp[4 * g + c], acc);
+    }
+    part[g * kPanel + i] = acc;
+    __syncthreads();
+    if (tid < kPanel) {
+      const double s01 = part[tid] + part[kPanel + tid];
+      const double s23 = part[2 * kPanel + tid] + part[3 * kPanel + tid];
+      const double s45 = part[4 * kPanel + tid] + part[5 * kPanel + tid];
+      const double s67 = part[6 * kPanel + tid] + part[7 * kPanel + tid];
+      zq[tid] -= (s01 + s23) + (s45 + s67);
+    }
+  }
+  // M_q^T, stored after M_q in the inverted block
+  const double* Mb = A.inv + static_cast<int64_t>(S.panel_base + q) * kInvBlock + kPanel * kPanel;
+  for (int e = tid; e < kPanel * kPanel; e += blockDim.x) {
+    M[e] = Mb[e];
+  }
+  __syncthreads();
+  if (tid < kPanel) {
+    double a0 = 0.0;
+    double a1 = 0.0;
+#pragma unroll
+    for (int j = 0; j < kPanel; j += 2) {
+      a0 = fma(M[j * kPanel + tid], zq[j], a0);
+      a1 = fma(M[(j + 1) * kPanel + tid], zq[j + 1], a1);
+    }
+    if (tid < w) {
+      const double x = a0 + a1;
+      V.xs[S.first_col + p0 + tid] = x;
+      V.step[V.perm[S.first_col + p0 + tid]] = x;
+    }
+  }
 }
 
 /// Whole solve (forward sweep, diagonal, backward sweep) in one launch, with
-/// the inverted diagonal blocks of KInvertDiagonal.
-/// Blocks take tasks in order from a counter: tasks 0..S-1 are the forward
-/// solves of the supernodes in level order (leaves first), tasks S..2S-1
-/// the backward solves in the reverse order. A forward task waits for its
-/// children's forward flags, a backward task for its parent's backward flag
-/// (a root: its own forward flag). Every task waits only on tasks taken
-/// before it by running blocks, so the launch completes whatever the number
-/// of resident blocks; no level boundary holds fast fronts behind slow ones.
-/// sync: [0] task counter, [2, 2 + S) forward flags, [2 + S, 2 + 2S)
-/// backward flags, all zero at launch. A wait that runs out of its limit
-/// (wait_limit polls) marks the instance kStatusWaitTimeout and lets the
-/// task's dependents go. withhold: a supernode whose forward flag is never
-/// published (-1: none), the test hook that makes a wait run out.
-__global__ void __launch_bounds__(256, 1) KSolveTree(DeviceView V, const int32_t* level_sn, int num_sn,
-                                                     const double* dvec, const double* inv, uint32_t* sync,
-                                                     int withhold, uint32_t wait_limit) {
+/// the inverted diagonal blocks of KInvertDiagonal. Blocks take the tasks of
+/// A.tasks in order from a counter (see Symbolic::solve_tasks): every task
+/// waits only on tasks taken before it by running blocks, so the launch
+/// completes whatever the number of resident blocks, and no level boundary
+/// holds fast fronts behind slow ones. A front's forward parts done counter
+/// (fdone) is what its parent waits for, its backward parts done (bdone)
+/// what its children wait for; ydone says a wide front's y (or a split
+/// root's right-hand side) is out, zdone counts a wide front's backward row
+/// chunks; a split root's panels publish one flag each per direction. A wait
+/// that runs out of its limit marks the instance kStatusWaitTimeout and lets
+/// the task's dependents go. withhold: a supernode whose forward parts are
+/// never published (-1: none), the test hook that makes a wait run out.
+__global__ void __launch_bounds__(256, 1) KSolveTree(DeviceView V, SolveArgs A) {
   extern __shared__ double buf[];
   __shared__ int task;
   __shared__ int go;
-  uint32_t* fdone = sync + 2;
-  uint32_t* bdone = sync + 2 + num_sn;
+  uint32_t* fdone = A.sync + 2;
+  uint32_t* bdone = fdone + A.num_sn;
+  uint32_t* ydone = bdone + A.num_sn;
+  uint32_t* zdone = ydone + A.num_sn;
+  uint32_t* pflag = zdone + A.num_sn;
+  uint32_t* bflag = pflag + A.num_inv;
   if (V.refine_left != nullptr && *V.refine_left == 0) {
     return;  // a refinement round after every instance's step became final
   }
   for (;;) {
     if (threadIdx.x == 0) {
-      task = static_cast<int>(atomicAdd(sync, 1u));
+      task = static_cast<int>(atomicAdd(A.sync, 1u));
     }
     __syncthreads();
     const int t = task;
-    if (t >= 2 * num_sn) {
+    if (t >= A.num_tasks) {
       return;
     }
-    const bool forward = t < num_sn;
-    const int s = level_sn[forward ? t : 2 * num_sn - 1 - t];
+    const int type = A.tasks[4 * t];
+    const int s = A.tasks[4 * t + 1];
+    const int part = A.tasks[4 * t + 2];
     const SupernodeRec S = V.sn[s];
     // refinement rounds skip the instances whose step is final
     const bool active = V.active[S.instance] != 0 && (V.refine_done == nullptr || V.refine_done[S.instance] == 0);
     if (threadIdx.x == 0) {
       bool ready = true;
       if (active) {
-        if (forward) {
-          for (int ci = 0; ci < S.child_count && ready; ++ci) {
-            ready = WaitFlag(fdone + V.child_list[S.child_begin + ci], wait_limit);
-          }
-        } else {
-          ready = WaitFlag(S.parent >= 0 ? bdone + S.parent : fdone + s, wait_limit);
+        switch (type) {
+          case kTaskForward:
+          case kTaskRootGather:
+            for (int ci = 0; ci < S.child_count && ready; ++ci) {
+              const int c = V.child_list[S.child_begin + ci];
+              ready = WaitCount(fdone + c, static_cast<uint32_t>(A.parts[2 * c]), A.wait_limit);
+            }
+            break;
+          case kTaskForwardRows:
+          case kTaskRootForward:
+            ready = WaitCount(ydone + s, 1u, A.wait_limit);
+            break;
+          case kTaskRootBackward:
+            ready = WaitCount(fdone + s, static_cast<uint32_t>(A.parts[2 * s]), A.wait_limit);
+            break;
+          case kTaskBackwardRows:
+            ready = WaitCount(bdone + S.parent, static_cast<uint32_t>(A.parts[2 * S.parent + 1]), A.wait_limit);
+            break;
+          default:  // kTaskBackward
+            if (A.zoff[s] >= 0) {
+              ready = WaitCount(zdone + s, static_cast<uint32_t>(A.parts[2 * s] - 1), A.wait_limit);
+            } else if (S.parent >= 0) {
+              ready = WaitCount(bdone + S.parent, static_cast<uint32_t>(A.parts[2 * S.parent + 1]), A.wait_limit);
+            } else {
+              ready = WaitCount(fdone + s, static_cast<uint32_t>(A.parts[2 * s]), A.wait_limit);
+            }
+            break;
         }
         if (!ready) {
           atomicOr(V.status + S.instance, kStatusWaitTimeout);
@@ -1461,25 +1766,98 @@ __global__ void __launch_bounds__(256, 1) KSolveTree(DeviceView V, const int32_t
       go = active && ready ? 1 : 0;
     }
     __syncthreads();
+    const bool f32 = Fp32Front(V, S);
     if (go != 0) {
-      if (forward) {
-        if (Fp32Front(V, S)) {
-          ForwardTreeBody<float>(V, S, dvec, inv, buf);
-        } else {
-          ForwardTreeBody<double>(V, S, dvec, inv, buf);
+      switch (type) {
+        case kTaskForward: {
+          double* ys = A.zoff[s] >= 0 ? A.ys : nullptr;
+          if (f32) {
+            ForwardTreeBody<float>(V, S, A.dvec, A.inv, buf, ys);
+          } else {
+            ForwardTreeBody<double>(V, S, A.dvec, A.inv, buf, ys);
+          }
+          break;
         }
-      } else {
-        if (Fp32Front(V, S)) {
-          BackwardTreeBody<float>(V, S, inv, buf);
-        } else {
-          BackwardTreeBody<double>(V, S, inv, buf);
+        case kTaskForwardRows:
+          if (f32) {
+            ForwardRowsTask<float>(V, S, A.ys, part, buf);
+          } else {
+            ForwardRowsTask<double>(V, S, A.ys, part, buf);
+          }
+          break;
+        case kTaskRootGather:
+          RootGather(V, S, A.ys, buf);
+          break;
+        case kTaskRootForward:
+          if (f32) {
+            RootForwardPanel<float>(V, S, A, part, pflag, buf);
+          } else {
+            RootForwardPanel<double>(V, S, A, part, pflag, buf);
+          }
+          break;
+        case kTaskRootBackward:
+          if (f32) {
+            RootBackwardPanel<float>(V, S, A, part, bflag, buf);
+          } else {
+            RootBackwardPanel<double>(V, S, A, part, bflag, buf);
+          }
+          break;
+        case kTaskBackwardRows:
+          if (f32) {
+            BackwardRowsTask<float>(V, S, part, A.zpart + A.zoff[s], buf);
+          } else {
+            BackwardRowsTask<double>(V, S, part, A.zpart + A.zoff[s], buf);
+          }
+          break;
+        default: {
+          const int parts = A.zoff[s] >= 0 ? A.parts[2 * s] - 1 : 0;
+          const double* zp = parts > 0 ? A.zpart + A.zoff[s] : nullptr;
+          if (f32) {
+            BackwardTreeBody<float>(V, S, A.inv, buf, zp, parts);
+          } else {
+            BackwardTreeBody<double>(V, S, A.inv, buf, zp, parts);
+          }
+          break;
         }
       }
     }
     __syncthreads();
-    if (threadIdx.x == 0 && !(forward && s == withhold)) {
+    if (threadIdx.x == 0) {
       __threadfence();
-      SetFlag((forward ? fdone : bdone) + s);
+      switch (type) {
+        case kTaskForward:
+          if (A.zoff[s] >= 0) {
+            Publish(ydone + s);
+          }
+          if (s != A.withhold) {
+            Publish(fdone + s);
+          }
+          break;
+        case kTaskForwardRows:
+          if (s != A.withhold) {
+            Publish(fdone + s);
+          }
+          break;
+        case kTaskRootGather:
+          Publish(ydone + s);
+          break;
+        case kTaskRootForward:
+          Publish(pflag + S.panel_base + part);
+          if (s != A.withhold) {
+            Publish(fdone + s);
+          }
+          break;
+        case kTaskRootBackward:
+          Publish(bflag + S.panel_base + part);
+          Publish(bdone + s);
+          break;
+        case kTaskBackwardRows:
+          Publish(zdone + s);
+          break;
+        default:
+          Publish(bdone + s);
+          break;
+      }
     }
   }
 }
@@ -1673,7 +2051,8 @@ int LaunchSolveLevels(const Symbolic& S, const DeviceView& V, const FactorPlan& 
   const size_t smem = static_cast<size_t>(P.max_front) * sizeof(double);
   const int num_sn = static_cast<int>(S.sn.size());
   const size_t tree_smem = SolveTreeSmem(P.max_front);
-  if (P.solve_sync != nullptr && P.inv != nullptr && tree_smem <= static_cast<size_t>(kMaxSmem)) {
+  if (P.solve_sync != nullptr && P.inv != nullptr && P.solve_tasks != nullptr &&
+      tree_smem <= static_cast<size_t>(kMaxSmem)) {
     if (num_sn == 0) {
       return 0;
     }
@@ -1686,8 +2065,9 @@ int LaunchSolveLevels(const Symbolic& S, const DeviceView& V, const FactorPlan& 
     }();
     // one resident block per SM (the kernel's register bound); blocks that
     // find no task left return at once
-    const int blocks = std::min(2 * num_sn, sms);
-    CudaCheck(cudaMemsetAsync(P.solve_sync, 0, SolveSyncWords(num_sn) * sizeof(uint32_t), stream), "solve flags");
+    const int blocks = std::min(P.num_solve_tasks, sms);
+    CudaCheck(cudaMemsetAsync(P.solve_sync, 0, SolveSyncWords(num_sn, P.num_inv) * sizeof(uint32_t), stream),
+              "solve flags");
     const TimedLaunch tl(P.timer, KernelTimer::kSolveTree, stream, [&] {
       // every entry of L read twice (forward, backward), FP32 in the grid
       // fronts of a mixed solve, and the inverted diagonal blocks
@@ -1699,9 +2079,21 @@ int LaunchSolveLevels(const Symbolic& S, const DeviceView& V, const FactorPlan& 
       }
       return b;
     });
-    KSolveTree<<<static_cast<unsigned>(blocks), 256, tree_smem, stream>>>(
-        V, P.level_sn, num_sn, P.dvec, P.inv, P.solve_sync, P.solve_withhold,
-        P.solve_wait_polls > 0 ? P.solve_wait_polls : kWaitLimit);
+    SolveArgs A{};
+    A.tasks = P.solve_tasks;
+    A.num_tasks = P.num_solve_tasks;
+    A.parts = P.solve_parts;
+    A.zoff = P.zpart_off;
+    A.ys = P.ys;
+    A.zpart = P.zpart;
+    A.dvec = P.dvec;
+    A.inv = P.inv;
+    A.sync = P.solve_sync;
+    A.num_sn = num_sn;
+    A.num_inv = P.num_inv;
+    A.withhold = P.solve_withhold;
+    A.wait_limit = P.solve_wait_polls > 0 ? P.solve_wait_polls : kWaitLimit;
+    KSolveTree<<<static_cast<unsigned>(blocks), 256, tree_smem, stream>>>(V, A);
     CudaCheck(cudaGetLastError(), "solve kernel");
     return 1;
   }

@@ -157,6 +157,20 @@ struct SupernodeRec {
   int64_t tc_pack;    // first packed operand row of its tensor-core Schur update (within its level), or -1
 };
 
+/// Task types of the one-launch solve.
+enum SolveTask : int32_t {
+  kTaskForward = 0,      // gather, pivot block solve, (narrow fronts) u = v_m - L21 y
+  kTaskForwardRows = 1,  // u for one chunk of rows of a wide front
+  kTaskRootGather = 2,   // right-hand side of a panel-split root
+  kTaskRootForward = 3,  // one 32-row panel of a panel-split root, forward
+  kTaskRootBackward = 4, // one 32-row panel of a panel-split root, backward
+  kTaskBackwardRows = 5, // L21^T x_R over one chunk of rows of a wide front
+  kTaskBackward = 6,     // z = x_k - L21^T x_R, pivot block back-substitution
+};
+constexpr int kSolveWideRows = 512;
+constexpr int kSolveRowChunk = 256;
+constexpr int kSolveRootSplit = 256;
+
 /// A contiguous block of work items of one kernel launch in the level
 /// schedule.
 struct TaskRange {
@@ -200,6 +214,21 @@ struct Symbolic {
   // skipped then): per level, operand packing tasks (sn, row tile, K chunk)
   // and output tile tasks (sn, tile i, tile j), i >= j; the packed operand
   // buffer is reused level after level (tc_pack_rows rows of the widest).
+  // Task list of the one-launch solve, in the order blocks take them: the
+  // forward tasks of every supernode in level order, then the backward
+  // tasks in reverse. (type, sn, part, 0) quads, SolveTask types. A front
+  // with at least kSolveWideRows rows below its pivots splits its forward
+  // update u = v_m - L21 y and its backward product L21^T x_R into chunks of
+  // kSolveRowChunk rows; a front without rows below and with more than
+  // small_pivots pivots (a dense pose root) solves its pivot block by
+  // 32-row panels, one task per panel, each waiting for the panels before
+  // it. solve_parts: per supernode, the forward and backward tasks whose
+  // completion its dependents wait for; zpart_off: per supernode the first
+  // double of its backward partial products (-1 when not split).
+  std::vector<int32_t> solve_tasks;
+  std::vector<int32_t> solve_parts;
+  std::vector<int64_t> zpart_off;
+  int64_t zpart_doubles{0};
   std::vector<int32_t> pack_tasks;
   std::vector<TaskRange> pack_range;
   std::vector<int32_t> tc_tasks;

@@ -92,8 +92,19 @@ LdltEngine::LdltEngine(int n, const int32_t* outer, const int32_t* inner, const 
   plan_.level_sn = level_sn_.get();
   plan_.dvec = dvec_.get();
   plan_.max_front = max_front;
-  solve_sync_.Alloc(SolveSyncWords(static_cast<int>(sym_.sn.size())));
+  solve_sync_.Alloc(SolveSyncWords(static_cast<int>(sym_.sn.size()), static_cast<int>(sym_.inv_tasks.size() / 2)));
   plan_.solve_sync = solve_sync_.get();
+  solve_tasks_.Upload(sym_.solve_tasks, s);
+  solve_parts_.Upload(sym_.solve_parts, s);
+  zpart_off_.Upload(sym_.zpart_off, s);
+  ys_.Alloc(static_cast<size_t>(std::max(n, 1)));
+  zpart_.Alloc(static_cast<size_t>(std::max<int64_t>(1, sym_.zpart_doubles)));
+  plan_.solve_tasks = solve_tasks_.get();
+  plan_.num_solve_tasks = static_cast<int>(sym_.solve_tasks.size() / 4);
+  plan_.solve_parts = solve_parts_.get();
+  plan_.zpart_off = zpart_off_.get();
+  plan_.ys = ys_.get();
+  plan_.zpart = zpart_.get();
   inv_tasks_.Upload(sym_.inv_tasks, s);
   inv_.Alloc(std::max<size_t>(1, sym_.inv_tasks.size() / 2) * kInvBlockDoubles);
   plan_.inv_tasks = inv_tasks_.get();
@@ -147,7 +158,7 @@ void LdltEngine::Solve(const double* b, double* x) {
             "x");
   CudaCheck(cudaStreamSynchronize(s), "solve");
   if ((st & kStatusWaitTimeout) != 0) {
-    Fail(SDFGPU_ERR_CUDA, "a wait of the solve kernel ran out of its limit");
+    Fail(SDFGPU_ERR_TIMEOUT, "a wait of the solve kernel ran out of its limit");
   }
 }
 

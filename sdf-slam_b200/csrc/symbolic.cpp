@@ -550,6 +550,60 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   for (int l = 0; l < levels; ++l) {
     S.update_range.push_back(schur_range[static_cast<size_t>(l)]);
   }
+  // one-launch solve tasks
+  S.solve_tasks.clear();
+  S.solve_parts.assign(2 * static_cast<size_t>(Sn), 1);
+  S.zpart_off.assign(static_cast<size_t>(Sn), -1);
+  S.zpart_doubles = 0;
+  auto push_task = [&S](int32_t type, int32_t sn, int32_t part) {
+    S.solve_tasks.push_back(type);
+    S.solve_tasks.push_back(sn);
+    S.solve_tasks.push_back(part);
+    S.solve_tasks.push_back(0);
+  };
+  auto root_split = [&S](const SupernodeRec& r) { return r.nrows == 0 && r.ncols >= kSolveRootSplit &&
+                                                         r.ncols > S.small_pivots; };
+  for (int q = 0; q < Sn; ++q) {
+    const int s = S.level_sn[static_cast<size_t>(q)];
+    const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
+    if (root_split(r)) {
+      const int np = (r.ncols + B - 1) / B;
+      push_task(kTaskRootGather, s, 0);
+      for (int p = 0; p < np; ++p) {
+        push_task(kTaskRootForward, s, p);
+      }
+      S.solve_parts[2 * static_cast<size_t>(s)] = np;
+      S.solve_parts[2 * static_cast<size_t>(s) + 1] = np;
+    } else if (r.nrows >= kSolveWideRows) {
+      const int chunks = (r.nrows + kSolveRowChunk - 1) / kSolveRowChunk;
+      push_task(kTaskForward, s, 0);
+      for (int p = 0; p < chunks; ++p) {
+        push_task(kTaskForwardRows, s, p);
+      }
+      S.solve_parts[2 * static_cast<size_t>(s)] = 1 + chunks;
+      S.zpart_off[static_cast<size_t>(s)] = S.zpart_doubles;
+      S.zpart_doubles += static_cast<int64_t>(chunks) * r.ncols;
+    } else {
+      push_task(kTaskForward, s, 0);
+    }
+  }
+  for (int q = Sn - 1; q >= 0; --q) {
+    const int s = S.level_sn[static_cast<size_t>(q)];
+    const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
+    if (root_split(r)) {
+      for (int p = (r.ncols + B - 1) / B - 1; p >= 0; --p) {
+        push_task(kTaskRootBackward, s, p);
+      }
+    } else if (r.nrows >= kSolveWideRows) {
+      const int chunks = (r.nrows + kSolveRowChunk - 1) / kSolveRowChunk;
+      for (int p = 0; p < chunks; ++p) {
+        push_task(kTaskBackwardRows, s, p);
+      }
+      push_task(kTaskBackward, s, 0);
+    } else {
+      push_task(kTaskBackward, s, 0);
+    }
+  }
   // tensor-core Schur tasks of the wide grid fronts (used by mixed solves)
   S.pack_tasks.clear();
   S.tc_tasks.clear();
