@@ -32,6 +32,23 @@ void KernelTimer::SetMask(uint32_t mask) {
   }
 }
 
+namespace {
+
+/// Records e on s; inside a stream capture as an event record node of the
+/// graph (an event recorded there without cudaEventRecordExternal would
+/// only order the capture's streams and never be recorded).
+void Record(cudaEvent_t e, cudaStream_t s) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  CudaCheck(cudaStreamIsCapturing(s, &st), "capture status");
+  if (st == cudaStreamCaptureStatusActive) {
+    CudaCheck(cudaEventRecordWithFlags(e, s, cudaEventRecordExternal), "timer event");
+  } else {
+    CudaCheck(cudaEventRecord(e, s), "timer event");
+  }
+}
+
+}  // namespace
+
 int KernelTimer::Begin(int c, cudaStream_t s, double work) {
   while (static_cast<int>(pool_.size()) < next_ + 2) {
     cudaEvent_t e = nullptr;
@@ -41,13 +58,11 @@ int KernelTimer::Begin(int c, cudaStream_t s, double work) {
   const int mark = next_;
   next_ += 2;
   marks_.push_back(Mark{c, mark, work});
-  CudaCheck(cudaEventRecord(pool_[static_cast<size_t>(mark)], s), "timer event");
+  Record(pool_[static_cast<size_t>(mark)], s);
   return mark;
 }
 
-void KernelTimer::End(int mark, cudaStream_t s) {
-  CudaCheck(cudaEventRecord(pool_[static_cast<size_t>(mark) + 1], s), "timer event");
-}
+void KernelTimer::End(int mark, cudaStream_t s) { Record(pool_[static_cast<size_t>(mark) + 1], s); }
 
 void KernelTimer::Accumulate() {
   for (const Mark& m : marks_) {
