@@ -677,6 +677,23 @@ __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeR
     r0 = ke + ti * kTile;
     cc0 = ke + tj * kTile;
     clim = S.ncols;
+  } else if (panel <= -2) {
+    // two-level blocking of wide pivot blocks (UpdateCode): the panel's
+    // update within its outer block of kOuterPanels panels, or the outer
+    // block's rank-(kOuterPanels * kPanel) update of the columns past it
+    const int x = -2 - panel;
+    const int outer = kOuterPanels * kPanel;
+    if ((x & 1) == 0) {
+      kb = (x >> 1) * kPanel;
+      ke = min(S.ncols, kb + kPanel);
+      clim = min(S.ncols, (kb / outer + 1) * outer);
+    } else {
+      kb = (x >> 1) * outer;
+      ke = min(S.ncols, kb + outer);
+      clim = S.ncols;
+    }
+    r0 = ke + ti * kTile;
+    cc0 = ke + tj * kTile;
   } else {
     kb = 0;
     ke = S.ncols;
@@ -785,7 +802,8 @@ __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeR
   }
 }
 
-/// Tiled rank-k update C -= L_I D L_J^T (lower part only). panel >= 0:
+/// Tiled rank-k update C -= L_I D L_J^T (lower part only). panel <= -2: the
+/// two-level updates of a wide pivot block (UpdateCode). panel >= 0:
 /// update of the remaining pivot columns by one panel; panel == -1: Schur
 /// complement of the trailing m x m block by all k pivots.
 __global__ void __launch_bounds__(256, 2) KUpdate(DeviceView V, const int32_t* tasks, const double* dvec) {
@@ -794,7 +812,7 @@ __global__ void __launch_bounds__(256, 2) KUpdate(DeviceView V, const int32_t* t
   if (V.active[S.instance] == 0) {
     return;
   }
-  if (t[1] < 0 && V.tc_schur != 0 && S.tc_pack >= 0 && Fp32Front(V, S)) {
+  if (t[1] == -1 && V.tc_schur != 0 && S.tc_pack >= 0 && Fp32Front(V, S)) {
     return;  // the tensor-core Schur kernels update this front
   }
   __shared__ double as_buf[kPanel * kTile];
@@ -1988,13 +2006,18 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
           return level_sum(l, [&S, t](const SupernodeRec& r) {
             const int c0 = t * kPanel;
             const int c1 = std::min(r.ncols, c0 + kPanel);
-            if (r.ncols <= S.small_pivots || c0 >= r.ncols || c1 >= r.ncols) {
+            if (r.ncols <= S.small_pivots || c0 >= r.ncols) {
               return 0.0;
             }
-            // columns [c1, k) of the rows [c1, F), lower part, by w pivots
-            const double nc = r.ncols - c1;
-            const double entries = nc * r.F - (static_cast<double>(c1) + r.ncols - 1) * nc / 2.0;
-            return 2.0 * (c1 - c0) * entries;
+            // lower-part entries of columns [a, b) over rows [a, F)
+            auto entries = [&r](double a, double b) { return (b - a) * r.F - (a + b - 1.0) * (b - a) / 2.0; };
+            const int outer = kOuterPanels * kPanel;
+            const int cend = std::min(r.ncols, (c0 / outer + 1) * outer);
+            if (c1 < cend) {
+              return 2.0 * (c1 - c0) * entries(c1, cend);
+            }
+            const int b0 = c0 / outer * outer;
+            return cend < r.ncols ? 2.0 * (cend - b0) * entries(cend, r.ncols) : 0.0;
           });
         });
         KUpdate<<<static_cast<unsigned>(ur.count), 256, 0, stream>>>(V, P.update_tasks + 4 * ur.begin, P.dvec);

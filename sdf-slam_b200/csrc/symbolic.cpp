@@ -509,10 +509,13 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
           S.panel_tasks.push_back(t);
           S.panel_tasks.push_back(c1 + ch * kPanelRows);
         }
-        // update of the remaining pivot columns [c1, k) for rows [c1, F)
-        if (c1 < r.ncols) {
-          const int nr = r.F - c1;
-          const int nc = r.ncols - c1;
+        // two-level blocking: the panel updates the pivot columns [c1, cend)
+        // left in its outer block, rows [c1, F); the outer block's last
+        // panel is followed by the block's update of the pivot columns
+        // [cend, k), rows [cend, F)
+        const int outer = kOuterPanels * B;
+        const int cend = std::min(r.ncols, (c0 / outer + 1) * outer);
+        auto tiles = [&S, s, T](int32_t code, int nr, int nc) {
           for (int tj = 0; tj * T < nc; ++tj) {
             for (int ti = 0; ti * T < nr; ++ti) {
               // lower part only: the tile must reach at or below the diagonal
@@ -520,11 +523,16 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
                 continue;
               }
               S.update_tasks.push_back(s);
-              S.update_tasks.push_back(t);
+              S.update_tasks.push_back(code);
               S.update_tasks.push_back(ti);
               S.update_tasks.push_back(tj);
             }
           }
+        };
+        if (c1 < cend) {
+          tiles(UpdateCodeInner(t), r.F - c1, cend - c1);
+        } else if (cend < r.ncols) {
+          tiles(UpdateCodeOuter(c0 / outer), r.F - cend, r.ncols - cend);
         }
       }
       S.panel_range[slot].count = static_cast<int64_t>(S.panel_tasks.size() / 3) - S.panel_range[slot].begin;
