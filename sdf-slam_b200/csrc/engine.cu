@@ -10,6 +10,7 @@
 #include <utility>
 
 #include "engine.h"
+#include "host_pool.h"
 
 namespace sdfgpu {
 
@@ -1201,16 +1202,20 @@ namespace {
 /// and KCommitPoses.
 void CUDART_CB WrapMovedAngles(void* user) {
   const auto* w = static_cast<const AngleWrapHost*>(user);
-  for (int f = 0; f < w->frames; ++f) {
-    if (w->upd[f] == 0) {
-      continue;
+  // on the host pool's threads when there are many frames (inline when the
+  // pool is busy with another job)
+  ParallelRanges(PoolThreads(), w->frames, 256, [w](int64_t b, int64_t e) {
+    for (int64_t f = b; f < e; ++f) {
+      if (w->upd[f] == 0) {
+        continue;
+      }
+      const double t = w->theta_pre[f];
+      const double th = std::atan2(std::sin(t), std::cos(t));
+      w->out[3 * f] = th;
+      w->out[3 * f + 1] = std::cos(th);
+      w->out[3 * f + 2] = std::sin(th);
     }
-    const double t = w->theta_pre[f];
-    const double th = std::atan2(std::sin(t), std::cos(t));
-    w->out[3 * f] = th;
-    w->out[3 * f + 1] = std::cos(th);
-    w->out[3 * f + 2] = std::sin(th);
-  }
+  });
 }
 
 }  // namespace
