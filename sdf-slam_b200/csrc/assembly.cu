@@ -828,9 +828,13 @@ __global__ void KBackup(DeviceView V, int dir, const int32_t* revert_mask) {
   }
 }
 
-/// Problem::ApplyStep (problem.cpp:117-130), first half: map values and
-/// positions; each moved frame's angle theta + delta goes to theta_pre for
-/// the host's WrapAngle (KCommitPoses stores the result).
+/// Problem::ApplyStep (problem.cpp:117-130): map values and positions; each
+/// moved frame's angle theta + delta goes to theta_pre, and the pose gets a
+/// provisional wrapped angle with correctly rounded cos and sin, which the
+/// cost of the candidate state uses. Once the LM step is decided, the host
+/// replaces the accepted angles and their cos / sin by the platform libm's
+/// (KCommitPoses), so that the next linearization rotates with the
+/// reference's bits.
 __global__ void KApplyStep(DeviceView V) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= V.n) {
@@ -857,19 +861,27 @@ __global__ void KApplyStep(DeviceView V) {
   double* p = V.poses + 3 * static_cast<int64_t>(f);
   p[0] += V.step[col];
   p[1] += V.step[col + 1];
-  V.theta_pre[f] = p[2] + V.step[col + 2];
+  const double t = p[2] + V.step[col + 2];
+  V.theta_pre[f] = t;
   V.theta_upd[f] = 1;
+  const double th = WrapAngle(t);
+  p[2] = th;
+  double sn;
+  double cs;
+  SinCosRn(th, &sn, &cs);
+  V.pose_cs[f] = make_double2(cs, sn);
 }
 
-/// Problem::ApplyStep, second half: the wrapped angles of the moved frames
-/// and their cos and sin, as the host computed them.
+/// The accepted angles of the moved frames and their cos and sin, as the
+/// host computed them with the platform's libm (WrapAngle, pose.hpp:9):
+/// theta_out holds (theta, cos, sin, flag) per frame, flag 1 to commit.
 __global__ void KCommitPoses(DeviceView V) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= V.total_frames || V.theta_upd[f] == 0) {
+  if (f >= V.total_frames || V.theta_out[4 * f + 3] == 0.0) {
     return;
   }
-  V.poses[3 * static_cast<int64_t>(f) + 2] = V.theta_out[3 * f];
-  V.pose_cs[f] = make_double2(V.theta_out[3 * f + 1], V.theta_out[3 * f + 2]);
+  V.poses[3 * static_cast<int64_t>(f) + 2] = V.theta_out[4 * f];
+  V.pose_cs[f] = make_double2(V.theta_out[4 * f + 1], V.theta_out[4 * f + 2]);
 }
 
 /// Per-row cost terms of Problem::Cost (problem.cpp:132-156): point rows with

@@ -96,15 +96,18 @@ struct DeviceView {
   double* map_backup;
   double* poses_backup;
   // (cos, sin) of every frame's angle, computed on the host with the
-  // platform's libm whenever an angle changes (upload, SetState, ApplyStep),
-  // so that every rotation of a scan point uses the reference's bits
+  // platform's libm whenever a state is set or a step accepted (upload,
+  // SetState, Engine::CommitAngles), so that every linearization rotates the
+  // scan points with the reference's bits; a candidate state whose cost
+  // decides the step holds correctly rounded device values until then
   double2* pose_cs;
   double2* pose_cs_backup;
   // ApplyStep hand-off: the unwrapped angle theta + delta of each frame the
-  // step moved (theta_upd 1), and the host's wrapped angle, cos and sin
+  // step moved (theta_upd 1), and the host's wrapped angle, cos, sin and a
+  // commit flag per frame
   double* theta_pre;
   int32_t* theta_upd;
-  const double* theta_out;  // 3 per frame
+  const double* theta_out;  // 4 per frame
   // per iteration
   double* pt_rec;                // kPointRec per point row
   int64_t* pt_poff;              // 4 per point row: front offsets of its (pose, corner node) blocks

@@ -391,6 +391,7 @@ void Engine::UploadProblem(int64_t keep_rows) {
   col_node_.Upload(col_node, s);
   col_inst_.Upload(col_inst, s);
   frame_inst_.Upload(frame_inst, s);
+  frame_inst_host_ = frame_inst;
   frame_col_.Upload(frame_col, s);
   if (direct) {
     const HostProblem& hp = host_[0];
@@ -435,14 +436,10 @@ void Engine::UploadProblem(int64_t keep_rows) {
     pose_cs_backup_.Alloc(F);
     theta_pre_.Alloc(F);
     theta_upd_.Alloc(F);
-    theta_out_.Alloc(3 * F);
+    theta_out_.Alloc(4 * F);
     h_theta_pre_.Alloc(F);
     h_theta_upd_.Alloc(F);
-    h_theta_out_.Alloc(3 * F);
-    wrap_.frames = total_frames_;
-    wrap_.theta_pre = h_theta_pre_.get();
-    wrap_.upd = h_theta_upd_.get();
-    wrap_.out = h_theta_out_.get();
+    h_theta_out_.Alloc(4 * F);
     UploadPoseTrig(poses.data(), 0, total_frames_);
   }
   pt_rec_.Alloc(static_cast<size_t>(total_points_) * kPointRec);
@@ -1193,33 +1190,6 @@ void Engine::UploadPoseTrig(const double* poses, int frame_off, int frames) {
   CudaCheck(cudaStreamSynchronize(stream_), "pose trig");
 }
 
-namespace {
-
-/// Host half of ApplyStep for the frames the step moved: WrapAngle
-/// (pose.hpp:9) of theta + delta and the new angle's cos and sin, all from
-/// the platform's libm as in the reference (problem.cpp:117-130). Runs as a
-/// stream-ordered host function between the copies of KApplyStep's angles
-/// and KCommitPoses.
-void CUDART_CB WrapMovedAngles(void* user) {
-  const auto* w = static_cast<const AngleWrapHost*>(user);
-  // on the host pool's threads when there are many frames (inline when the
-  // pool is busy with another job)
-  ParallelRanges(PoolThreads(), w->frames, 256, [w](int64_t b, int64_t e) {
-    for (int64_t f = b; f < e; ++f) {
-      if (w->upd[f] == 0) {
-        continue;
-      }
-      const double t = w->theta_pre[f];
-      const double th = std::atan2(std::sin(t), std::cos(t));
-      w->out[3 * f] = th;
-      w->out[3 * f + 1] = std::cos(th);
-      w->out[3 * f + 2] = std::sin(th);
-    }
-  });
-}
-
-}  // namespace
-
 void Engine::LaunchApplyStep() {
   if (n_ <= 0) {
     return;
@@ -1227,19 +1197,57 @@ void Engine::LaunchApplyStep() {
   const size_t F = static_cast<size_t>(total_frames_);
   CudaCheck(cudaMemsetAsync(theta_upd_.get(), 0, F * sizeof(int32_t), stream_), "angle flags");
   KApplyStep<<<Blocks(n_, 256), 256, 0, stream_>>>(V_);
+  // the moved frames' angles for the host's exact wrap (CommitAngles)
   CudaCheck(cudaMemcpyAsync(h_theta_pre_.get(), theta_pre_.get(), F * sizeof(double), cudaMemcpyDeviceToHost,
                             stream_),
             "angles");
   CudaCheck(cudaMemcpyAsync(h_theta_upd_.get(), theta_upd_.get(), F * sizeof(int32_t), cudaMemcpyDeviceToHost,
                             stream_),
             "angle flags");
-  CudaCheck(cudaLaunchHostFunc(stream_, WrapMovedAngles, &wrap_), "angle wrap");
-  CudaCheck(cudaMemcpyAsync(theta_out_.get(), h_theta_out_.get(), 3 * F * sizeof(double), cudaMemcpyHostToDevice,
+  CudaCheck(cudaGetLastError(), "apply step");
+  times_.launches += 1;
+}
+
+void Engine::CommitAngles(const std::vector<int32_t>* revert) {
+  // the stream has drained: h_theta_pre_ / h_theta_upd_ hold the last step's
+  // angles, and the previous commit's upload has read h_theta_out_
+  const int F = total_frames_;
+  if (F <= 0 || n_ <= 0) {
+    return;
+  }
+  const int32_t* upd = h_theta_upd_.get();
+  const double* pre = h_theta_pre_.get();
+  double* out = h_theta_out_.get();
+  bool any = false;
+  for (int f = 0; f < F; ++f) {
+    any = any || (upd[f] != 0 && (revert == nullptr || (*revert)[static_cast<size_t>(frame_inst_host_[f])] == 0));
+  }
+  if (!any) {
+    return;
+  }
+  // WrapAngle (pose.hpp:9) and the new angle's cos and sin with the
+  // platform's libm, as the reference computes them (problem.cpp:117-130);
+  // on the host pool's threads when there are many frames
+  ParallelRanges(PoolThreads(), F, 256, [&](int64_t b, int64_t e) {
+    for (int64_t f = b; f < e; ++f) {
+      const bool commit = upd[f] != 0 &&
+                          (revert == nullptr || (*revert)[static_cast<size_t>(frame_inst_host_[f])] == 0);
+      out[4 * f + 3] = commit ? 1.0 : 0.0;
+      if (commit) {
+        const double t = pre[f];
+        const double th = std::atan2(std::sin(t), std::cos(t));
+        out[4 * f] = th;
+        out[4 * f + 1] = std::cos(th);
+        out[4 * f + 2] = std::sin(th);
+      }
+    }
+  });
+  CudaCheck(cudaMemcpyAsync(theta_out_.get(), out, 4 * static_cast<size_t>(F) * sizeof(double), cudaMemcpyHostToDevice,
                             stream_),
             "wrapped angles");
-  KCommitPoses<<<Blocks(static_cast<int64_t>(F), 128), 128, 0, stream_>>>(V_);
-  CudaCheck(cudaGetLastError(), "apply step");
-  times_.launches += 2;
+  KCommitPoses<<<Blocks(F, 128), 128, 0, stream_>>>(V_);
+  CudaCheck(cudaGetLastError(), "commit angles");
+  ++times_.launches;
 }
 
 double Engine::Cost(int i) {
@@ -1258,6 +1266,8 @@ void Engine::ApplyStep(int i, const double* step) {
                             cudaMemcpyHostToDevice, stream_),
             "step");
   LaunchApplyStep();
+  CudaCheck(cudaStreamSynchronize(stream_), "apply step sync");
+  CommitAngles(nullptr);
   std::vector<int32_t> ones(host_.size(), 1);
   SetActive(ones);
   CudaCheck(cudaStreamSynchronize(stream_), "apply step sync");
@@ -1658,6 +1668,9 @@ void Engine::FinishIteration() {
     // the results (and the applied steps) of the first run.
     std::vector<double> seg(h_seg_.get(), h_seg_.get() + 5 * I);
     std::vector<int32_t> st(h_status_.get(), h_status_.get() + I);
+    const size_t F = static_cast<size_t>(total_frames_);
+    std::vector<double> pre(h_theta_pre_.get(), h_theta_pre_.get() + F);
+    std::vector<int32_t> upd(h_theta_upd_.get(), h_theta_upd_.get() + F);
     Reanalyze(overflow);
     std::fill(h_active_.get(), h_active_.get() + I, 0);
     for (const int i : overflow) {
@@ -1671,6 +1684,13 @@ void Engine::FinishIteration() {
       rerun[static_cast<size_t>(i)] = 1;
       if ((h_status_[i] & kStatusPatternOverflow) != 0) {
         Fail(SDFGPU_ERR_CUDA, "sparsity pattern still overflows after re-analysis");
+      }
+    }
+    for (size_t f = 0; f < F; ++f) {
+      if (rerun[static_cast<size_t>(frame_inst_host_[f])] == 0) {
+        // the first run's moved angles of the instances it kept
+        h_theta_pre_[f] = pre[f];
+        h_theta_upd_[f] = upd[f];
       }
     }
     for (size_t i = 0; i < I; ++i) {
@@ -1766,6 +1786,8 @@ void Engine::FinishIteration() {
     // the revert mask is read by the kernel; keep the host copy alive
     CudaCheck(cudaStreamSynchronize(stream_), "restore");
   }
+  // the accepted steps' angles with the reference's bits
+  CommitAngles(&revert);
   ++iter_;
 }
 

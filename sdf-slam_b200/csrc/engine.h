@@ -227,16 +227,6 @@ struct IterTimes {
   double capture_host{0};     // host seconds capturing and instantiating graphs
 };
 
-/// Pinned buffers of ApplyStep's host half (read by a stream-ordered host
-/// function, so that the step phase stays one captured graph): per frame the
-/// unwrapped angle and a moved flag in, (theta, cos, sin) out.
-struct AngleWrapHost {
-  int frames{0};
-  const double* theta_pre{nullptr};
-  const int32_t* upd{nullptr};
-  double* out{nullptr};
-};
-
 class Engine {
  public:
   explicit Engine(std::vector<HostProblem> problems);
@@ -349,9 +339,13 @@ class Engine {
   void LaunchFactor();
   void LaunchSolve();
   void LaunchStepAndCost(bool backup);
-  /// ApplyStep of the running instances: KApplyStep, the angles' wrap and
-  /// their cos / sin on the host (stream-ordered), KCommitPoses.
+  /// ApplyStep of the running instances (KApplyStep, provisional angles on
+  /// the device) and the copy of the moved frames' angles to the host.
   void LaunchApplyStep();
+  /// With the stream drained: the exact angles of the last step's moved
+  /// frames (the platform libm's WrapAngle, cos and sin), uploaded and
+  /// committed, except for the instances `revert` marks.
+  void CommitAngles(const std::vector<int32_t>* revert);
   /// (cos, sin) of frames [frame_off, frame_off + frames) from host poses.
   void UploadPoseTrig(const double* poses, int frame_off, int frames);
   void LaunchCost(std::vector<double>& cost);
@@ -410,7 +404,7 @@ class Engine {
   DevBuf<double2> pose_cs_, pose_cs_backup_;
   DevBuf<double> theta_pre_, theta_out_;
   DevBuf<int32_t> theta_upd_;
-  AngleWrapHost wrap_;
+  std::vector<int32_t> frame_inst_host_;  // global frame -> instance
   HostBuf<double> h_theta_pre_, h_theta_out_;
   HostBuf<int32_t> h_theta_upd_;
   DevBuf<double> pt_rec_, eik_rec_, odom_rec_;
