@@ -346,6 +346,145 @@ __global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const
   }
 }
 
+/// Outer-block factorization of a front with more than small_pivots pivots:
+/// the LDL^T of one outer block of kBlockCols pivot columns (after the
+/// updates of every earlier block) and L for a chunk of kBlockRows rows
+/// below it, in one CTA of 256 threads. The block's diagonal tile is held in
+/// shared memory and factored right-looking, one pivot per step (two
+/// barriers each); the chunk's rows get the same steps' updates in the same
+/// loop, so each CTA factors the tile redundantly and needs no other CTA
+/// (the first chunk's CTA writes the tile's L and D). L of the tile's 32 x
+/// 32 diagonal blocks goes transposed into their upper triangles, like the
+/// panel kernels store it; the rest of L column major.
+constexpr int kBlockCols = kOuterPanels * kPanel;  // 128
+constexpr int kBlockThreads = 256;
+
+/// Dynamic shared memory of KPanelBlock (FP64 tile and rows, pivots).
+__host__ __device__ constexpr size_t PanelBlockSmem() {
+  return (static_cast<size_t>(kBlockCols) * (kBlockCols + 1) + static_cast<size_t>(kBlockRows) * (kBlockCols + 1) +
+          2 * kBlockCols) *
+         sizeof(double);
+}
+
+template <typename T>
+__device__ __forceinline__ void PanelBlockBody(const DeviceView& V, const SupernodeRec& S, int block, int row_begin,
+                                               double* dvec, T* smem) {
+  constexpr int LD = kBlockCols + 1;
+  const int F = S.F;
+  const int64_t F64 = F;
+  const int c0 = block * kBlockCols;
+  const int w = min(kBlockCols, S.ncols - c0);
+  const int c1 = c0 + w;
+  const int rows = max(0, min(kBlockRows, F - row_begin));
+  T* Fs = WorkFront<T>(V, S);
+  T* A = smem;                      // kBlockCols x LD, row major: A[i * LD + l]
+  T* R = A + kBlockCols * LD;       // kBlockRows x LD
+  T* dv = R + kBlockRows * LD;      // pivots
+  T* dinv = dv + kBlockCols;
+  const int tid = threadIdx.x;
+  // tile (lower part; identity past the block's w columns) and the chunk's
+  // rows, read down the front's columns
+  for (int e = tid; e < kBlockCols * kBlockCols; e += kBlockThreads) {
+    const int l = e / kBlockCols;
+    const int i = e % kBlockCols;
+    T v;
+    if (i < w && l < w) {
+      v = i >= l ? Fs[(c0 + l) * F64 + c0 + i] : T(0);
+    } else {
+      v = i == l ? T(1) : T(0);
+    }
+    A[i * LD + l] = v;
+  }
+  for (int e = tid; e < kBlockRows * kBlockCols; e += kBlockThreads) {
+    const int l = e / kBlockRows;
+    const int r = e % kBlockRows;
+    R[r * LD + l] = (r < rows && l < w) ? Fs[(c0 + l) * F64 + row_begin + r] : T(0);
+  }
+  __syncthreads();
+  // thread (tx, ty) owns tile entries (tx + 16 a, ty + 16 b); chunk entries
+  // (r, lg + 4 c)
+  const int tx = tid & 15;
+  const int ty = tid >> 4;
+  const int r = tid & (kBlockRows - 1);
+  const int lg = tid >> 6;
+  bool zero = false;
+  for (int j = 0; j < kBlockCols; ++j) {
+    const T d = A[j * LD + j];
+    zero = zero || d == T(0);
+    const T di = Recip(d);
+    const int a0 = j + 1 > tx ? (j + 1 - tx + 15) / 16 : 0;
+    for (int a = a0; a < 8; ++a) {
+      const int i = tx + 16 * a;
+      const T ti = A[i * LD + j];
+      for (int b = 0; b < 8; ++b) {
+        const int l = ty + 16 * b;
+        if (l > j && l <= i) {
+          A[i * LD + l] -= ti * (A[l * LD + j] * di);
+        }
+      }
+    }
+    const T tr = R[r * LD + j];
+    for (int c = 0; c < kBlockCols / 4; ++c) {
+      const int l = lg + 4 * c;
+      if (l > j) {
+        R[r * LD + l] -= tr * (A[l * LD + j] * di);
+      }
+    }
+    __syncthreads();
+    if (tid < kBlockCols) {
+      if (tid > j) {
+        A[tid * LD + j] *= di;
+      }
+      if (tid == j) {
+        dv[j] = d;
+      }
+    } else if (tid < kBlockCols + kBlockRows) {
+      R[(tid - kBlockCols) * LD + j] *= di;
+    }
+    __syncthreads();
+  }
+  if (row_begin == c1) {
+    // the first chunk's CTA writes the tile's D and L
+    for (int j = tid; j < w; j += kBlockThreads) {
+      dvec[S.first_col + c0 + j] = static_cast<double>(dv[j]);
+    }
+    for (int e = tid; e < w * w; e += kBlockThreads) {
+      const int l = e / w;
+      const int i = e % w;
+      if (i > l) {
+        if (i / kPanel == l / kPanel) {
+          Fs[(c0 + i) * F64 + c0 + l] = A[i * LD + l];  // transposed in the diagonal block
+        } else {
+          Fs[(c0 + l) * F64 + c0 + i] = A[i * LD + l];
+        }
+      }
+    }
+    if (tid == 0 && zero) {
+      atomicOr(V.status + S.instance, kStatusZeroPivot);
+    }
+  }
+  for (int e = tid; e < rows * w; e += kBlockThreads) {
+    const int l = e / rows;
+    const int rr = e % rows;
+    Fs[(c0 + l) * F64 + row_begin + rr] = R[rr * LD + l];
+  }
+}
+
+/// Tasks (sn, outer block, first row of the chunk below it).
+__global__ void __launch_bounds__(kBlockThreads, 1) KPanelBlock(DeviceView V, const int32_t* tasks, double* dvec) {
+  extern __shared__ double block_smem[];
+  const int32_t* t = tasks + 3 * static_cast<int64_t>(blockIdx.x);
+  const SupernodeRec S = V.sn[t[0]];
+  if (V.active[S.instance] == 0) {
+    return;
+  }
+  if (Fp32Front(V, S)) {
+    PanelBlockBody<float>(V, S, t[1], t[2], dvec, reinterpret_cast<float*>(block_smem));
+  } else {
+    PanelBlockBody<double>(V, S, t[1], t[2], dvec, block_smem);
+  }
+}
+
 /// Pivot block of a front with at most kSmallPivots columns, factored in
 /// one block: blocked LDL^T of the k x k pivot block in shared memory (warp 0
 /// factors each 32-wide diagonal block, all threads solve the rows below it
@@ -678,20 +817,12 @@ __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeR
     cc0 = ke + tj * kTile;
     clim = S.ncols;
   } else if (panel <= -2) {
-    // two-level blocking of wide pivot blocks (UpdateCode): the panel's
-    // update within its outer block of kOuterPanels panels, or the outer
-    // block's rank-(kOuterPanels * kPanel) update of the columns past it
-    const int x = -2 - panel;
+    // outer block -2 - panel's rank-(kOuterPanels * kPanel) update of the
+    // pivot columns past it (UpdateCodeOuter)
     const int outer = kOuterPanels * kPanel;
-    if ((x & 1) == 0) {
-      kb = (x >> 1) * kPanel;
-      ke = min(S.ncols, kb + kPanel);
-      clim = min(S.ncols, (kb / outer + 1) * outer);
-    } else {
-      kb = (x >> 1) * outer;
-      ke = min(S.ncols, kb + outer);
-      clim = S.ncols;
-    }
+    kb = (-2 - panel) * outer;
+    ke = min(S.ncols, kb + outer);
+    clim = S.ncols;
     r0 = ke + ti * kTile;
     cc0 = ke + tj * kTile;
   } else {
@@ -802,8 +933,8 @@ __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeR
   }
 }
 
-/// Tiled rank-k update C -= L_I D L_J^T (lower part only). panel <= -2: the
-/// two-level updates of a wide pivot block (UpdateCode). panel >= 0:
+/// Tiled rank-k update C -= L_I D L_J^T (lower part only). panel <= -2: an
+/// outer block's update of the later pivot columns (UpdateCodeOuter). panel >= 0:
 /// update of the remaining pivot columns by one panel; panel == -1: Schur
 /// complement of the trailing m x m block by all k pivots.
 __global__ void __launch_bounds__(256, 2) KUpdate(DeviceView V, const int32_t* tasks, const double* dvec) {
@@ -1931,6 +2062,22 @@ void ConfigureSolveKernels(int max_front) {
 }
 
 int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan& P, cudaStream_t stream) {
+  {
+    // the block factorization's shared memory (a per-device attribute)
+    static std::mutex mu;
+    static bool configured[64] = {};
+    int dev = 0;
+    CudaCheck(cudaGetDevice(&dev), "device");
+    const std::lock_guard<std::mutex> lock(mu);
+    if (dev < 0 || dev >= 64 || !configured[dev]) {
+      CudaCheck(cudaFuncSetAttribute(KPanelBlock, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(PanelBlockSmem())),
+                "block smem attr");
+      if (dev >= 0 && dev < 64) {
+        configured[dev] = true;
+      }
+    }
+  }
   // the diagonal blocks are factored by four warps of every factor block
   if (S.front_rows < 128 || S.front_rows > 256 || S.panel_rows < 1 || S.panel_rows > kPanelRowsPerBlock) {
     Fail(SDFGPU_ERR_INVALID_ARGUMENT, "factorization schedule out of range");
@@ -1988,36 +2135,32 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
       if (pr.count > 0) {
         const TimedLaunch tl(P.timer, KernelTimer::kPanel, stream, [&] {
           return level_sum(l, [&S, t](const SupernodeRec& r) {
-            const int c0 = t * kPanel;
+            const int c0 = t * kBlockCols;
             if (r.ncols <= S.small_pivots || c0 >= r.ncols) {
               return 0.0;
             }
-            const double w = std::min(kPanel, r.ncols - c0);
+            // the block's LDL^T and the rows below it solved against it
+            const double w = std::min(kBlockCols, r.ncols - c0);
             return 2.0 * w * w * w / 3.0 + static_cast<double>(r.F - c0 - w) * w * w;
           });
         });
-        KPanel<<<static_cast<unsigned>(pr.count), kPanelRowsPerBlock, 0, stream>>>(V, P.panel_tasks + 3 * pr.begin,
-                                                                                   P.dvec, S.panel_rows);
+        KPanelBlock<<<static_cast<unsigned>(pr.count), kBlockThreads, PanelBlockSmem(), stream>>>(
+            V, P.panel_tasks + 3 * pr.begin, P.dvec);
         ++launches;
       }
       const TaskRange ur = S.update_range[slot];
       if (ur.count > 0) {
         const TimedLaunch tl(P.timer, KernelTimer::kUpdatePanel, stream, [&] {
           return level_sum(l, [&S, t](const SupernodeRec& r) {
-            const int c0 = t * kPanel;
-            const int c1 = std::min(r.ncols, c0 + kPanel);
-            if (r.ncols <= S.small_pivots || c0 >= r.ncols) {
+            const int c0 = t * kBlockCols;
+            const int c1 = std::min(r.ncols, c0 + kBlockCols);
+            if (r.ncols <= S.small_pivots || c0 >= r.ncols || c1 >= r.ncols) {
               return 0.0;
             }
-            // lower-part entries of columns [a, b) over rows [a, F)
-            auto entries = [&r](double a, double b) { return (b - a) * r.F - (a + b - 1.0) * (b - a) / 2.0; };
-            const int outer = kOuterPanels * kPanel;
-            const int cend = std::min(r.ncols, (c0 / outer + 1) * outer);
-            if (c1 < cend) {
-              return 2.0 * (c1 - c0) * entries(c1, cend);
-            }
-            const int b0 = c0 / outer * outer;
-            return cend < r.ncols ? 2.0 * (cend - b0) * entries(cend, r.ncols) : 0.0;
+            // lower-part entries of the pivot columns [c1, k) over rows [c1, F)
+            const double nc = r.ncols - c1;
+            const double entries = nc * r.F - (static_cast<double>(c1) + r.ncols - 1.0) * nc / 2.0;
+            return 2.0 * (c1 - c0) * entries;
           });
         });
         KUpdate<<<static_cast<unsigned>(ur.count), 256, 0, stream>>>(V, P.update_tasks + 4 * ur.begin, P.dvec);

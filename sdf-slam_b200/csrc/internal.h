@@ -167,17 +167,17 @@ enum SolveTask : int32_t {
   kTaskBackwardRows = 5, // L21^T x_R over one chunk of rows of a wide front
   kTaskBackward = 6,     // z = x_k - L21^T x_R, pivot block back-substitution
 };
-/// Two-level blocking of the pivot block of a front factored by panels:
-/// each 32-column panel updates only the rest of its outer block of
-/// kOuterPanels panels, and the finished outer block updates every later
-/// pivot column at once (a rank-128 update instead of four rank-32 ones).
-/// Update task codes (the task's panel field): -2 - 2 p for panel p's update
-/// within its outer block, -3 - 2 b for outer block b's update of the
-/// columns past it; -1 is a front's Schur complement, p >= 0 panel p's
-/// update of every later pivot column.
+/// Fronts with more than small_pivots pivots factor their pivot block by
+/// outer blocks of kOuterPanels 32-column panels: the block's LDL^T and the
+/// rows below it (KPanelBlock), then the block's rank-128 update of every
+/// later pivot column. Update task codes (the task's panel field): -2 - b
+/// for outer block b's update of the pivot columns past it, -1 a front's
+/// Schur complement, p >= 0 panel p's update of every later pivot column
+/// (the allocation-free dense solve's panel path).
 constexpr int kOuterPanels = 4;
-constexpr int32_t UpdateCodeInner(int panel) { return -2 - 2 * panel; }
-constexpr int32_t UpdateCodeOuter(int block) { return -3 - 2 * block; }
+constexpr int32_t UpdateCodeOuter(int block) { return -2 - block; }
+/// Rows below an outer block that one block-factorization task takes.
+constexpr int kBlockRows = 64;
 constexpr int kSolveWideRows = 512;
 constexpr int kSolveRowChunk = 256;
 constexpr int kSolveRootSplit = 256;

@@ -344,7 +344,6 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   }
   const int B = panel_width;
   const int T = tile;
-  const int kPanelRows = S.panel_rows;
   constexpr int kEaCols = 16;
   const int kFrontRows = S.front_rows;
   // fronts factored by the single-kernel path keep the pivot block's lower
@@ -496,43 +495,36 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
       for (int q = qb; q < qe; ++q) {
         const int s = S.level_sn[static_cast<size_t>(q)];
         const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
-        const int c0 = t * B;
+        // slot t: outer block t of kOuterPanels panels, factored with the
+        // rows below it by block tasks (sn, t, first row of a kBlockRows
+        // chunk; the first chunk writes the block), then the block's update
+        // of the pivot columns [c1, k), rows [c1, F)
+        const int outer = kOuterPanels * B;
+        const int c0 = t * outer;
         if (c0 >= r.ncols || r.ncols <= small) {
           continue;
         }
-        const int c1 = std::min(r.ncols, c0 + B);
-        // panel tasks: chunk 0 also owns the diagonal block
+        const int c1 = std::min(r.ncols, c0 + outer);
         const int below = r.F - c1;
-        const int chunks = std::max(1, (below + kPanelRows - 1) / kPanelRows);
+        const int chunks = std::max(1, (below + kBlockRows - 1) / kBlockRows);
         for (int ch = 0; ch < chunks; ++ch) {
           S.panel_tasks.push_back(s);
           S.panel_tasks.push_back(t);
-          S.panel_tasks.push_back(c1 + ch * kPanelRows);
+          S.panel_tasks.push_back(c1 + ch * kBlockRows);
         }
-        // two-level blocking: the panel updates the pivot columns [c1, cend)
-        // left in its outer block, rows [c1, F); the outer block's last
-        // panel is followed by the block's update of the pivot columns
-        // [cend, k), rows [cend, F)
-        const int outer = kOuterPanels * B;
-        const int cend = std::min(r.ncols, (c0 / outer + 1) * outer);
-        auto tiles = [&S, s, T](int32_t code, int nr, int nc) {
-          for (int tj = 0; tj * T < nc; ++tj) {
-            for (int ti = 0; ti * T < nr; ++ti) {
-              // lower part only: the tile must reach at or below the diagonal
-              if ((ti + 1) * T - 1 < tj * T) {
-                continue;
-              }
-              S.update_tasks.push_back(s);
-              S.update_tasks.push_back(code);
-              S.update_tasks.push_back(ti);
-              S.update_tasks.push_back(tj);
+        const int nr = r.F - c1;
+        const int nc = r.ncols - c1;
+        for (int tj = 0; tj * T < nc; ++tj) {
+          for (int ti = 0; ti * T < nr; ++ti) {
+            // lower part only: the tile must reach at or below the diagonal
+            if ((ti + 1) * T - 1 < tj * T) {
+              continue;
             }
+            S.update_tasks.push_back(s);
+            S.update_tasks.push_back(UpdateCodeOuter(t));
+            S.update_tasks.push_back(ti);
+            S.update_tasks.push_back(tj);
           }
-        };
-        if (c1 < cend) {
-          tiles(UpdateCodeInner(t), r.F - c1, cend - c1);
-        } else if (cend < r.ncols) {
-          tiles(UpdateCodeOuter(c0 / outer), r.F - cend, r.ncols - cend);
         }
       }
       S.panel_range[slot].count = static_cast<int64_t>(S.panel_tasks.size() / 3) - S.panel_range[slot].begin;
