@@ -114,12 +114,33 @@ __device__ __forceinline__ void ExtendAddDirect(TP* Fp, int64_t PF, const TC* U,
                                                 int cbeg, int cend) {
   const int lane = threadIdx.x & 31;
   const int nwarps = static_cast<int>(blockDim.x >> 5);
+  constexpr int kBatchRows = 8;
   for (int cc = cbeg + static_cast<int>(threadIdx.x >> 5); cc < cend; cc += nwarps) {
     TP* __restrict__ dst = Fp + rel[cc] * PF;
     const TC* __restrict__ src = U + static_cast<int64_t>(cc) * CF;
-#pragma unroll 4
-    for (int r = cc + lane; r < m; r += 32) {
-      dst[rel[r]] += static_cast<TP>(src[r]);
+    // a child's rows land on distinct parent rows: all reads of a batch,
+    // then all writes, so the batch's read-modify-writes overlap instead of
+    // each waiting for the one before
+    for (int r0 = cc + lane; r0 < m; r0 += 32 * kBatchRows) {
+      int d[kBatchRows];
+      TC u[kBatchRows];
+#pragma unroll
+      for (int q = 0; q < kBatchRows; ++q) {
+        const int r = r0 + 32 * q;
+        d[q] = r < m ? rel[r] : -1;
+        u[q] = r < m ? src[r] : TC(0);
+      }
+      TP old[kBatchRows];
+#pragma unroll
+      for (int q = 0; q < kBatchRows; ++q) {
+        old[q] = d[q] >= 0 ? dst[d[q]] : TP(0);
+      }
+#pragma unroll
+      for (int q = 0; q < kBatchRows; ++q) {
+        if (d[q] >= 0) {
+          dst[d[q]] = old[q] + static_cast<TP>(u[q]);
+        }
+      }
     }
   }
 }

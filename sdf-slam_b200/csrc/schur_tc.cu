@@ -324,15 +324,24 @@ __global__ void __launch_bounds__(128, 1) KSchurTc(const __grid_constant__ CUten
     float* Fs = A.fronts32 + S.front_off;
     const int row = ti * kRowsTile + warp * 32 + lane;
     const uint32_t taddr = tmem + (static_cast<uint32_t>(warp * 32) << 16);
-    for (int j0 = 0; j0 < kRowsTile; j0 += 16) {
-      uint32_t r[16];
-      TmemLoad16(taddr + static_cast<uint32_t>(j0), r);
+    // 32 columns per batch: the batch's C values are read before any is
+    // written (the compiler cannot prove the columns apart), so the reads
+    // overlap instead of each waiting for the previous write
+    for (int j0 = 0; j0 < kRowsTile; j0 += 32) {
+      float cv[32];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) {
+      for (int j = 0; j < 32; ++j) {
+        const int col = tj * kRowsTile + j0 + j;
+        cv[j] = (row < m && col <= row) ? Fs[(k + col) * F + k + row] : 0.0f;
+      }
+      uint32_t r[32];
+      TmemLoad16(taddr + static_cast<uint32_t>(j0), *reinterpret_cast<uint32_t(*)[16]>(r));
+      TmemLoad16(taddr + static_cast<uint32_t>(j0 + 16), *reinterpret_cast<uint32_t(*)[16]>(r + 16));
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
         const int col = tj * kRowsTile + j0 + j;
         if (row < m && col <= row) {
-          float* p = Fs + (k + col) * F + k + row;
-          *p -= __uint_as_float(r[j]);
+          Fs[(k + col) * F + k + row] = cv[j] - __uint_as_float(r[j]);
         }
       }
     }
