@@ -370,27 +370,34 @@ __global__ void __launch_bounds__(kPanelRowsPerBlock) KPanel(DeviceView V, const
 /// Outer-block factorization of a front with more than small_pivots pivots:
 /// the LDL^T of one outer block of kBlockCols pivot columns (after the
 /// updates of every earlier block) and L for a chunk of kBlockRows rows
-/// below it, in one CTA of 256 threads. The block's diagonal tile is held in
-/// shared memory and factored right-looking, one pivot per step (two
-/// barriers each); the chunk's rows get the same steps' updates in the same
-/// loop, so each CTA factors the tile redundantly and needs no other CTA
-/// (the first chunk's CTA writes the tile's L and D). L of the tile's 32 x
-/// 32 diagonal blocks goes transposed into their upper triangles, like the
-/// panel kernels store it; the rest of L column major.
+/// below it, in one CTA of 256 threads. Every CTA of a block factors the
+/// block's diagonal tile itself (no CTA waits for another; the first
+/// chunk's CTA writes the tile's L and D):
+///  * the tile right-looking with its entries in registers (thread (tx, ty)
+///    owns rows tx + 16 a and columns ty + 16 b), one pivot per step: the
+///    owners of column j publish it to shared memory (two buffers
+///    alternating with j, one barrier per step), every thread updates its
+///    entries and scales its part of column j;
+///  * the chunk's rows by forward substitution against L D: four threads
+///    per row, each summing every fourth earlier column, a fixed butterfly
+///    of two shuffles.
+/// L of the tile's 32 x 32 diagonal blocks goes transposed into their upper
+/// triangles, like the panel kernels store it; the rest of L column major.
 constexpr int kBlockCols = kOuterPanels * kPanel;  // 128
 constexpr int kBlockThreads = 256;
+constexpr int kBlockLd = kBlockCols + 1;
 
-/// Dynamic shared memory of KPanelBlock (FP64 tile and rows, pivots).
+/// Dynamic shared memory of KPanelBlock: W = L D of the tile, the chunk's
+/// rows, the column buffers and the pivots (FP64 sizes).
 __host__ __device__ constexpr size_t PanelBlockSmem() {
-  return (static_cast<size_t>(kBlockCols) * (kBlockCols + 1) + static_cast<size_t>(kBlockRows) * (kBlockCols + 1) +
-          2 * kBlockCols) *
+  return (static_cast<size_t>(kBlockCols) * kBlockLd + static_cast<size_t>(kBlockRows) * kBlockLd +
+          3 * kBlockCols) *
          sizeof(double);
 }
 
 template <typename T>
 __device__ __forceinline__ void PanelBlockBody(const DeviceView& V, const SupernodeRec& S, int block, int row_begin,
                                                double* dvec, T* smem) {
-  constexpr int LD = kBlockCols + 1;
   const int F = S.F;
   const int64_t F64 = F;
   const int c0 = block * kBlockCols;
@@ -398,85 +405,145 @@ __device__ __forceinline__ void PanelBlockBody(const DeviceView& V, const Supern
   const int c1 = c0 + w;
   const int rows = max(0, min(kBlockRows, F - row_begin));
   T* Fs = WorkFront<T>(V, S);
-  T* A = smem;                      // kBlockCols x LD, row major: A[i * LD + l]
-  T* R = A + kBlockCols * LD;       // kBlockRows x LD
-  T* dv = R + kBlockRows * LD;      // pivots
-  T* dinv = dv + kBlockCols;
+  T* Wt = smem;                          // kBlockCols x kBlockLd: W(j, l) = L(j, l) d_l, row major
+  T* R = Wt + kBlockCols * kBlockLd;     // kBlockRows x kBlockLd: the chunk's rows, then their L
+  T* colbuf = R + kBlockRows * kBlockLd; // 2 x kBlockCols
+  T* dv = colbuf + 2 * kBlockCols;       // pivots
   const int tid = threadIdx.x;
-  // tile (lower part; identity past the block's w columns) and the chunk's
-  // rows, read down the front's columns
-  for (int e = tid; e < kBlockCols * kBlockCols; e += kBlockThreads) {
-    const int l = e / kBlockCols;
-    const int i = e % kBlockCols;
-    T v;
-    if (i < w && l < w) {
-      v = i >= l ? Fs[(c0 + l) * F64 + c0 + i] : T(0);
-    } else {
-      v = i == l ? T(1) : T(0);
-    }
-    A[i * LD + l] = v;
-  }
+  const int tx = tid & 15;
+  const int ty = tid >> 4;
+  // the chunk's rows (read down the front's columns)
   for (int e = tid; e < kBlockRows * kBlockCols; e += kBlockThreads) {
     const int l = e / kBlockRows;
     const int r = e % kBlockRows;
-    R[r * LD + l] = (r < rows && l < w) ? Fs[(c0 + l) * F64 + row_begin + r] : T(0);
+    R[r * kBlockLd + l] = (r < rows && l < w) ? Fs[(c0 + l) * F64 + row_begin + r] : T(0);
   }
-  __syncthreads();
-  // thread (tx, ty) owns tile entries (tx + 16 a, ty + 16 b); chunk entries
-  // (r, lg + 4 c)
-  const int tx = tid & 15;
-  const int ty = tid >> 4;
-  const int r = tid & (kBlockRows - 1);
-  const int lg = tid >> 6;
+  // the tile in registers (lower part; identity past w)
+  T a[8][8];
+#pragma unroll
+  for (int ia = 0; ia < 8; ++ia) {
+#pragma unroll
+    for (int ib = 0; ib < 8; ++ib) {
+      const int i = tx + 16 * ia;
+      const int l = ty + 16 * ib;
+      T v;
+      if (i < w && l < w) {
+        v = i >= l ? Fs[(c0 + l) * F64 + c0 + i] : T(0);
+      } else {
+        v = i == l ? T(1) : T(0);
+      }
+      a[ia][ib] = v;
+    }
+  }
   bool zero = false;
   for (int j = 0; j < kBlockCols; ++j) {
-    const T d = A[j * LD + j];
-    zero = zero || d == T(0);
-    const T di = Recip(d);
-    const int a0 = j + 1 > tx ? (j + 1 - tx + 15) / 16 : 0;
-    for (int a = a0; a < 8; ++a) {
-      const int i = tx + 16 * a;
-      const T ti = A[i * LD + j];
-      for (int b = 0; b < 8; ++b) {
-        const int l = ty + 16 * b;
-        if (l > j && l <= i) {
-          A[i * LD + l] -= ti * (A[l * LD + j] * di);
+    T* cb = colbuf + (j & 1) * kBlockCols;
+    const int jb = j >> 4;
+    if (ty == (j & 15)) {
+      // publish column j (entries on and below the diagonal)
+#pragma unroll
+      for (int ib = 0; ib < 8; ++ib) {
+        if (ib == jb) {
+#pragma unroll
+          for (int ia = 0; ia < 8; ++ia) {
+            cb[tx + 16 * ia] = a[ia][ib];
+          }
         }
       }
     }
-    const T tr = R[r * LD + j];
-    for (int c = 0; c < kBlockCols / 4; ++c) {
-      const int l = lg + 4 * c;
-      if (l > j) {
-        R[r * LD + l] -= tr * (A[l * LD + j] * di);
+    __syncthreads();
+    const T d = cb[j];
+    zero = zero || d == T(0);
+    const T di = Recip(d);
+    T tl[8];
+#pragma unroll
+    for (int ib = 0; ib < 8; ++ib) {
+      const int l = ty + 16 * ib;
+      tl[ib] = l > j ? cb[l] * di : T(0);
+    }
+#pragma unroll
+    for (int ia = 0; ia < 8; ++ia) {
+      const int i = tx + 16 * ia;
+      if (i > j) {
+        const T ti = cb[i];
+#pragma unroll
+        for (int ib = 0; ib < 8; ++ib) {
+          const int l = ty + 16 * ib;
+          if (l > j && l <= i) {
+            a[ia][ib] -= ti * tl[ib];
+          }
+        }
       }
     }
-    __syncthreads();
-    if (tid < kBlockCols) {
-      if (tid > j) {
-        A[tid * LD + j] *= di;
+    // the owners of column j keep L(i, j) = A(i, j) / d below the diagonal
+    if (ty == (j & 15)) {
+#pragma unroll
+      for (int ib = 0; ib < 8; ++ib) {
+        if (ib == jb) {
+#pragma unroll
+          for (int ia = 0; ia < 8; ++ia) {
+            if (tx + 16 * ia > j) {
+              a[ia][ib] *= di;
+            }
+          }
+        }
       }
-      if (tid == j) {
-        dv[j] = d;
-      }
-    } else if (tid < kBlockCols + kBlockRows) {
-      R[(tid - kBlockCols) * LD + j] *= di;
     }
-    __syncthreads();
+    if (tid == 0) {
+      dv[j] = d;
+    }
   }
+  __syncthreads();
+  // W = L D for the substitution (diagonal: d)
+#pragma unroll
+  for (int ia = 0; ia < 8; ++ia) {
+#pragma unroll
+    for (int ib = 0; ib < 8; ++ib) {
+      const int i = tx + 16 * ia;
+      const int l = ty + 16 * ib;
+      if (l <= i) {
+        Wt[i * kBlockLd + l] = l < i ? a[ia][ib] * dv[l] : dv[i];
+      }
+    }
+  }
+  __syncthreads();
+  // rows below: L(r, j) = (A(r, j) - sum_{l<j} L(r, l) W(j, l)) / d_j
+  {
+    const int r = tid >> 2;
+    const int q = tid & 3;
+    T* Rr = R + r * kBlockLd;
+    for (int j = 0; j < w; ++j) {
+      const T* Wj = Wt + j * kBlockLd;
+      T part = T(0);
+      for (int l = q; l < j; l += 4) {
+        part = fma(Rr[l], Wj[l], part);
+      }
+      part += __shfl_xor_sync(0xffffffffu, part, 1);
+      part += __shfl_xor_sync(0xffffffffu, part, 2);
+      if (q == 0) {
+        Rr[j] = (Rr[j] - part) * Recip(Wj[j]);
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
   if (row_begin == c1) {
     // the first chunk's CTA writes the tile's D and L
     for (int j = tid; j < w; j += kBlockThreads) {
       dvec[S.first_col + c0 + j] = static_cast<double>(dv[j]);
     }
-    for (int e = tid; e < w * w; e += kBlockThreads) {
-      const int l = e / w;
-      const int i = e % w;
-      if (i > l) {
-        if (i / kPanel == l / kPanel) {
-          Fs[(c0 + i) * F64 + c0 + l] = A[i * LD + l];  // transposed in the diagonal block
-        } else {
-          Fs[(c0 + l) * F64 + c0 + i] = A[i * LD + l];
+#pragma unroll
+    for (int ia = 0; ia < 8; ++ia) {
+#pragma unroll
+      for (int ib = 0; ib < 8; ++ib) {
+        const int i = tx + 16 * ia;
+        const int l = ty + 16 * ib;
+        if (i < w && l < i) {
+          if (i / kPanel == l / kPanel) {
+            Fs[(c0 + i) * F64 + c0 + l] = a[ia][ib];  // transposed in the diagonal block
+          } else {
+            Fs[(c0 + l) * F64 + c0 + i] = a[ia][ib];
+          }
         }
       }
     }
@@ -487,7 +554,7 @@ __device__ __forceinline__ void PanelBlockBody(const DeviceView& V, const Supern
   for (int e = tid; e < rows * w; e += kBlockThreads) {
     const int l = e / rows;
     const int rr = e % rows;
-    Fs[(c0 + l) * F64 + row_begin + rr] = R[rr * LD + l];
+    Fs[(c0 + l) * F64 + row_begin + rr] = R[rr * kBlockLd + l];
   }
 }
 
