@@ -889,6 +889,7 @@ FactorPlan Engine::Plan() {
   P.inv_tasks = inv_tasks_.get();
   P.num_inv = static_cast<int>(sym_.inv_tasks.size() / 2);
   P.inv = inv_.get();
+  P.big_tasks = tc_tasks_.get();
   P.solve_withhold = solve_withhold_;
   P.solve_wait_polls = solve_wait_polls_;
   // only the iteration's own factor and solve phases are timed

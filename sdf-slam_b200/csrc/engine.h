@@ -154,6 +154,9 @@ struct FactorPlan {
   const int32_t* pack_tasks{nullptr};
   const int32_t* tc_tasks{nullptr};
   TcArgs tc{};
+  /// 128 x 128 Schur tiles of the wide fronts (the tensor-core task list),
+  /// taken by KUpdateBig for FP64 fronts.
+  const int32_t* big_tasks{nullptr};
   /// Test hook of the one-launch solve: a supernode whose forward flag is
   /// never published (-1: none) and the polls a wait may take (0: the
   /// default of about a second).

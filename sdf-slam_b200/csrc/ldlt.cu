@@ -99,6 +99,8 @@ LdltEngine::LdltEngine(int n, const int32_t* outer, const int32_t* inner, const 
   zpart_off_.Upload(sym_.zpart_off, s);
   ys_.Alloc(static_cast<size_t>(std::max(n, 1)));
   zpart_.Alloc(static_cast<size_t>(std::max<int64_t>(1, sym_.zpart_doubles)));
+  big_tasks_.Upload(sym_.tc_tasks, s);
+  plan_.big_tasks = big_tasks_.get();
   plan_.solve_tasks = solve_tasks_.get();
   plan_.num_solve_tasks = static_cast<int>(sym_.solve_tasks.size() / 4);
   plan_.solve_parts = solve_parts_.get();
