@@ -307,7 +307,9 @@ int sdfgpu_last_profile(sdfgpu_problem* problem, double* phases);
 /* Autotuner (no counterpart in the reference): times the factorization of
  * the handle's current normal matrix under each candidate schedule (the
  * pivot count up to which a front is factored by one kernel, that kernel's
- * rows per block, the rows per panel block) and keeps the fastest for the
+ * rows per block, the rows per panel block of the wide fronts, 0 meaning
+ * that each 128-column outer block is factored whole by one kernel) and
+ * keeps the fastest for the
  * handle's later solves, also across pattern re-analyses. schedule (3
  * int32, may be NULL) receives the chosen one, factor_ms (may be NULL) its
  * factorization time; trials (may be NULL) receives up to max_trials rows

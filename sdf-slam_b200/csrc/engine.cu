@@ -1061,9 +1061,10 @@ void Engine::UploadSchedule() {
 
 double Engine::Autotune(std::vector<std::pair<Schedule, double>>* trials) {
   // Candidate schedules: the pivot count below which a front is factored by
-  // one kernel, that kernel's rows per block, and the rows per panel block.
-  const std::vector<Schedule> candidates = {
-      {128, 256, 128}, {128, 128, 128}, {96, 256, 128}, {64, 256, 128}, {64, 128, 64}, {128, 256, 64}};
+  // one kernel, that kernel's rows per block, and the rows per panel task
+  // (0: wider fronts by whole outer blocks of 128 pivots, KPanelBlock).
+  const std::vector<Schedule> candidates = {{128, 256, 128}, {128, 128, 128}, {96, 256, 128}, {64, 256, 128},
+                                            {64, 128, 64},   {128, 256, 64},  {64, 128, 0},   {128, 256, 0}};
   const size_t I = host_.size();
   SetMode(std::vector<int32_t>(I, 0), 0);
   SetActive(std::vector<int32_t>(I, 1));

@@ -905,12 +905,20 @@ __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeR
     cc0 = ke + tj * kTile;
     clim = S.ncols;
   } else if (panel <= -2) {
-    // outer block -2 - panel's rank-(kOuterPanels * kPanel) update of the
-    // pivot columns past it (UpdateCodeOuter)
+    // outer blocks of kOuterPanels panels (UpdateCodeInner / Outer): a
+    // panel's update within its outer block, or the finished block's
+    // rank-(kOuterPanels * kPanel) update of the pivot columns past it
+    const int x = -2 - panel;
     const int outer = kOuterPanels * kPanel;
-    kb = (-2 - panel) * outer;
-    ke = min(S.ncols, kb + outer);
-    clim = S.ncols;
+    if ((x & 1) == 0) {
+      kb = (x >> 1) * kPanel;
+      ke = min(S.ncols, kb + kPanel);
+      clim = min(S.ncols, (kb / outer + 1) * outer);
+    } else {
+      kb = (x >> 1) * outer;
+      ke = min(S.ncols, kb + outer);
+      clim = S.ncols;
+    }
     r0 = ke + ti * kTile;
     cc0 = ke + tj * kTile;
   } else {
@@ -1155,8 +1163,8 @@ __global__ void __launch_bounds__(kBigThreads, 1) KUpdateBig(DeviceView V, const
   }
 }
 
-/// Tiled rank-k update C -= L_I D L_J^T (lower part only). panel <= -2: an
-/// outer block's update of the later pivot columns (UpdateCodeOuter). panel >= 0:
+/// Tiled rank-k update C -= L_I D L_J^T (lower part only). panel <= -2: the
+/// outer-block updates (UpdateCodeInner / Outer). panel >= 0:
 /// update of the remaining pivot columns by one panel; panel == -1: Schur
 /// complement of the trailing m x m block by all k pivots.
 __global__ void __launch_bounds__(256, 2) KUpdate(DeviceView V, const int32_t* tasks, const double* dvec) {
@@ -2304,7 +2312,7 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
     }
   }
   // the diagonal blocks are factored by four warps of every factor block
-  if (S.front_rows < 128 || S.front_rows > 256 || S.panel_rows < 1 || S.panel_rows > kPanelRowsPerBlock) {
+  if (S.front_rows < 128 || S.front_rows > 256 || S.panel_rows < 0 || S.panel_rows > kPanelRowsPerBlock) {
     Fail(SDFGPU_ERR_INVALID_ARGUMENT, "factorization schedule out of range");
   }
   int launches = 0;
@@ -2357,34 +2365,54 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
       const size_t slot = static_cast<size_t>(S.panel_index_base[static_cast<size_t>(l)] + t);
       const TaskRange pr = S.panel_range[slot];
       if (pr.count > 0) {
+        const bool blocks = S.panel_rows == 0;
         const TimedLaunch tl(P.timer, KernelTimer::kPanel, stream, [&] {
-          return level_sum(l, [&S, t](const SupernodeRec& r) {
-            const int c0 = t * kBlockCols;
+          return level_sum(l, [&S, t, blocks](const SupernodeRec& r) {
+            const int width = blocks ? kBlockCols : kPanel;
+            const int c0 = t * width;
             if (r.ncols <= S.small_pivots || c0 >= r.ncols) {
               return 0.0;
             }
             // the block's LDL^T and the rows below it solved against it
-            const double w = std::min(kBlockCols, r.ncols - c0);
+            const double w = std::min(width, r.ncols - c0);
             return 2.0 * w * w * w / 3.0 + static_cast<double>(r.F - c0 - w) * w * w;
           });
         });
-        KPanelBlock<<<static_cast<unsigned>(pr.count), kBlockThreads, PanelBlockSmem(), stream>>>(
-            V, P.panel_tasks + 3 * pr.begin, P.dvec);
+        if (blocks) {
+          KPanelBlock<<<static_cast<unsigned>(pr.count), kBlockThreads, PanelBlockSmem(), stream>>>(
+              V, P.panel_tasks + 3 * pr.begin, P.dvec);
+        } else {
+          KPanel<<<static_cast<unsigned>(pr.count), kPanelRowsPerBlock, 0, stream>>>(V, P.panel_tasks + 3 * pr.begin,
+                                                                                     P.dvec, S.panel_rows);
+        }
         ++launches;
       }
       const TaskRange ur = S.update_range[slot];
       if (ur.count > 0) {
         const TimedLaunch tl(P.timer, KernelTimer::kUpdatePanel, stream, [&] {
           return level_sum(l, [&S, t](const SupernodeRec& r) {
-            const int c0 = t * kBlockCols;
-            const int c1 = std::min(r.ncols, c0 + kBlockCols);
-            if (r.ncols <= S.small_pivots || c0 >= r.ncols || c1 >= r.ncols) {
+            if (r.ncols <= S.small_pivots) {
               return 0.0;
             }
-            // lower-part entries of the pivot columns [c1, k) over rows [c1, F)
-            const double nc = r.ncols - c1;
-            const double entries = nc * r.F - (static_cast<double>(c1) + r.ncols - 1.0) * nc / 2.0;
-            return 2.0 * (c1 - c0) * entries;
+            // lower-part entries of the pivot columns [a, b) over rows [a, F)
+            auto entries = [&r](double a, double b) { return (b - a) * r.F - (a + b - 1.0) * (b - a) / 2.0; };
+            const int outer = kOuterPanels * kPanel;
+            if (S.panel_rows == 0) {
+              const int c0 = t * outer;
+              const int c1 = std::min(r.ncols, c0 + outer);
+              return c0 < r.ncols && c1 < r.ncols ? 2.0 * (c1 - c0) * entries(c1, r.ncols) : 0.0;
+            }
+            const int c0 = t * kPanel;
+            if (c0 >= r.ncols) {
+              return 0.0;
+            }
+            const int c1 = std::min(r.ncols, c0 + kPanel);
+            const int cend = std::min(r.ncols, (c0 / outer + 1) * outer);
+            if (c1 < cend) {
+              return 2.0 * (c1 - c0) * entries(c1, cend);
+            }
+            const int b0 = c0 / outer * outer;
+            return cend < r.ncols ? 2.0 * (cend - b0) * entries(cend, r.ncols) : 0.0;
           });
         });
         KUpdate<<<static_cast<unsigned>(ur.count), 256, 0, stream>>>(V, P.update_tasks + 4 * ur.begin, P.dvec);

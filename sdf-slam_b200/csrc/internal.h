@@ -167,15 +167,20 @@ enum SolveTask : int32_t {
   kTaskBackwardRows = 5, // L21^T x_R over one chunk of rows of a wide front
   kTaskBackward = 6,     // z = x_k - L21^T x_R, pivot block back-substitution
 };
-/// Fronts with more than small_pivots pivots factor their pivot block by
-/// outer blocks of kOuterPanels 32-column panels: the block's LDL^T and the
-/// rows below it (KPanelBlock), then the block's rank-128 update of every
-/// later pivot column. Update task codes (the task's panel field): -2 - b
-/// for outer block b's update of the pivot columns past it, -1 a front's
-/// Schur complement, p >= 0 panel p's update of every later pivot column
-/// (the allocation-free dense solve's panel path).
+/// Fronts with more than small_pivots pivots factor their pivot block in
+/// outer blocks of kOuterPanels 32-column panels, one of two ways (the
+/// schedule's panel_rows picks it): panel_rows > 0, panel by panel (KPanel,
+/// panel_rows rows below per task), each panel updating the rest of its outer
+/// block; panel_rows == 0, the whole outer block with its rows below at once
+/// (KPanelBlock). Either way the finished outer block updates every later
+/// pivot column with one rank-128 update. Update task codes (the task's
+/// panel field): -2 - 2 p for panel p's update within its outer block,
+/// -3 - 2 b for outer block b's update of the pivot columns past it, -1 a
+/// front's Schur complement, p >= 0 panel p's update of every later pivot
+/// column (the allocation-free dense solve's panel path).
 constexpr int kOuterPanels = 4;
-constexpr int32_t UpdateCodeOuter(int block) { return -2 - block; }
+constexpr int32_t UpdateCodeInner(int panel) { return -2 - 2 * panel; }
+constexpr int32_t UpdateCodeOuter(int block) { return -3 - 2 * block; }
 /// Rows below an outer block that one block-factorization task takes.
 constexpr int kBlockRows = 64;
 constexpr int kSolveWideRows = 512;
@@ -249,7 +254,8 @@ struct Symbolic {
   // level, tasks (sn, first row of the chunk below the pivot block, rows in
   // the chunk) with front_rows threads per block (rows per chunk shrink to
   // 64 or 32 on levels that would not fill the GPU); larger fronts: panel
-  // tasks of panel_rows rows. The three are the schedule an autotuner picks.
+  // tasks of panel_rows rows (0: whole outer blocks, KPanelBlock). The three
+  // are the schedule an autotuner picks.
   int small_pivots{128};
   int front_rows{256};
   int panel_rows{128};
