@@ -318,6 +318,13 @@ int sdfgpu_last_profile(sdfgpu_problem* problem, double* phases);
 int sdfgpu_autotune(sdfgpu_problem* problem, int32_t* schedule, double* factor_ms, double* trials,
                     int32_t max_trials, int32_t* num_trials);
 
+/* Installs the factorization schedule (small_pivots, front_rows,
+ * panel_rows) for the handle's later solves, also across pattern
+ * re-analyses (no counterpart in the reference; the autotuner's choice made
+ * by hand). small_pivots 32..128, front_rows 128..256, panel_rows 0 (whole
+ * outer blocks) or 16..128; SDFGPU_ERR_INVALID_ARGUMENT otherwise. */
+int sdfgpu_set_schedule(sdfgpu_problem* problem, const int32_t* schedule);
+
 /* ----------------------------------------------------------- incremental --
  * Run in incremental mode (src/pipeline/runner.cpp:226-285, without its file
  * output): the dataset's odometry is poses[i].RelativeTo(poses[i + 1]); frame

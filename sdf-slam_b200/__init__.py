@@ -387,6 +387,15 @@ class Problem:
         return {"schedule": tuple(int(v) for v in sched), "factor_ms": best.value,
                 "trials": [tuple(r) for r in trials[:n.value]]}
 
+    def set_schedule(self, small_pivots: int, front_rows: int, panel_rows: int):
+        """Installs a factorization schedule for this handle's later solves
+        (sdfgpu_set_schedule): fronts with up to small_pivots pivots are
+        factored by one kernel of front_rows rows per block, wider ones panel
+        by panel with panel_rows rows per task, or by whole 128-column outer
+        blocks when panel_rows is 0."""
+        sched = (ctypes.c_int32 * 3)(int(small_pivots), int(front_rows), int(panel_rows))
+        _check(lib().sdfgpu_set_schedule(self._h, sched))
+
     def debug_solve_fault(self, withhold_front: int, wait_polls: int = 0):
         """Test hook (sdfgpu_debug_solve_fault): from the next solve on, the
         one-launch triangular solve never publishes supernode

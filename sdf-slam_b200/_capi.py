@@ -141,6 +141,7 @@ SIGNATURES = {
     "sdfgpu_linearization_get": (ctypes.c_int, [vp, c_dbl_p, c_int_p, c_int_p, c_int_p, c_dbl_p,
                                                 c_int_p, c_int_p, c_dbl_p, c_dbl_p, c_dbl_p]),
     "sdfgpu_last_profile": (ctypes.c_int, [vp, c_dbl_p]),
+    "sdfgpu_set_schedule": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int32)]),
     "sdfgpu_autotune": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int32), c_dbl_p, c_dbl_p, ctypes.c_int32,
                                        ctypes.POINTER(ctypes.c_int32)]),
     "sdfgpu_run_incremental": (ctypes.c_int, [ctypes.POINTER(IncrementalDesc), ctypes.POINTER(ProblemOptionsC),

@@ -69,7 +69,10 @@ __device__ void EvalPoint(const DeviceView& V, const InstDev& I, double c, doubl
   const double gy = (s * px + c * py) + pose[1];
   const double fx = (gx - I.min_x) / I.dx;
   const double fy = (gy - I.min_y) / I.dy;
-  if (fx < 0.0 || fy < 0.0 || fx > I.nx - 1 || fy > I.ny - 1) {
+  // the reference's bounds test, written so that a NaN coordinate (a pose
+  // driven to NaN by a failed step) is outside too instead of reaching the
+  // integer conversion
+  if (!(fx >= 0.0) || !(fy >= 0.0) || !(fx <= I.nx - 1) || !(fy <= I.ny - 1)) {
     out.valid = false;
     out.residual = -delta;
     return;

@@ -640,6 +640,15 @@ int sdfgpu_autotune(sdfgpu_problem* problem, int32_t* schedule, double* factor_m
   });
 }
 
+int sdfgpu_set_schedule(sdfgpu_problem* problem, const int32_t* schedule) {
+  return Guard([&] {
+    if (schedule == nullptr) {
+      sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "schedule is NULL");
+    }
+    Eng(problem).SetSchedule(sdfgpu::Schedule{schedule[0], schedule[1], schedule[2]});
+  });
+}
+
 int sdfgpu_ldlt_create(int32_t n, const int32_t* outer, const int32_t* inner, const int32_t* perm,
                        sdfgpu_ldlt** out) {
   return Guard([&] {

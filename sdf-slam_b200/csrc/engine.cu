@@ -1103,6 +1103,17 @@ double Engine::Autotune(std::vector<std::pair<Schedule, double>>* trials) {
   return best;
 }
 
+void Engine::SetSchedule(const Schedule& sched) {
+  if (sched.small_pivots < 32 || sched.small_pivots > 128 || sched.front_rows < 128 || sched.front_rows > 256 ||
+      (sched.panel_rows != 0 && (sched.panel_rows < 16 || sched.panel_rows > 128))) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT,
+         "schedule out of range (small_pivots 32..128, front_rows 128..256, panel_rows 0 or 16..128)");
+  }
+  sched_ = sched;
+  Reschedule(sym_, sched_);
+  UploadSchedule();
+}
+
 void Engine::ReanalyzePending() {
   if (pending_.empty()) {
     return;

@@ -299,6 +299,9 @@ class Engine {
   /// candidate schedule and keeps the fastest (also across re-analyses).
   /// Returns its time in ms; trials receives every candidate's time.
   double Autotune(std::vector<std::pair<Schedule, double>>* trials);
+  /// Installs a factorization schedule (checked against the ranges the
+  /// kernels support) for the later solves, also across re-analyses.
+  void SetSchedule(const Schedule& sched);
   [[nodiscard]] const Schedule& schedule() const { return sched_; }
   [[nodiscard]] const IterTimes& times() const { return times_; }
   [[nodiscard]] int64_t factor_flops() const { return sym_.total_flops; }

@@ -37,7 +37,8 @@ inline P2 ApplyPose(const double* pose, P2 p) {
 inline bool LocateCell(const HostProblem& hp, P2 g, int* w, int* h) {
   const double fx = (g.x - hp.min_x) / hp.dx();
   const double fy = (g.y - hp.min_y) / hp.dy();
-  if (fx < 0.0 || fy < 0.0 || fx > hp.nx - 1 || fy > hp.ny - 1) {
+  // NaN coordinates count as outside (never converted to a cell)
+  if (!(fx >= 0.0) || !(fy >= 0.0) || !(fx <= hp.nx - 1) || !(fy <= hp.ny - 1)) {
     return false;
   }
   *w = std::min(static_cast<int>(fx), hp.nx - 2);

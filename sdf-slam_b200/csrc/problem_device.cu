@@ -252,7 +252,9 @@ __global__ void KActiveMark(const int32_t* pt_frame, const double2* pt_xy, int64
   const double gy = __dadd_rn(__dadd_rn(__dmul_rn(sn, p.x), __dmul_rn(c, p.y)), t[3]);
   const double fx = __ddiv_rn(__dsub_rn(gx, g.min_x), g.dx);
   const double fy = __ddiv_rn(__dsub_rn(gy, g.min_y), g.dy);
-  if (fx < 0.0 || fy < 0.0 || fx > static_cast<double>(g.nx - 1) || fy > static_cast<double>(g.ny - 1)) {
+  // NaN coordinates count as outside (never converted to a cell)
+  if (!(fx >= 0.0) || !(fy >= 0.0) || !(fx <= static_cast<double>(g.nx - 1)) ||
+      !(fy <= static_cast<double>(g.ny - 1))) {
     return;
   }
   const int w = min(static_cast<int>(fx), g.nx - 2);

@@ -346,6 +346,10 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   const int T = tile;
   constexpr int kEaCols = 16;
   const int kFrontRows = S.front_rows;
+  // launch slots of the wide fronts: one per outer block when whole outer
+  // blocks are factored at once (panel_rows 0), else one per panel
+  const bool block_mode = S.panel_rows == 0;
+  const int slot_width = block_mode ? kOuterPanels * B : B;
   // fronts factored by the single-kernel path keep the pivot block's lower
   // triangle (read by every task of the front) and store L11 transposed
   for (SupernodeRec& r : S.sn) {
@@ -414,7 +418,7 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
         S.small_max_k[static_cast<size_t>(l)] = std::max(S.small_max_k[static_cast<size_t>(l)], r.ncols);
         continue;
       }
-      maxp = std::max(maxp, (r.ncols + B - 1) / B);
+      maxp = std::max(maxp, (r.ncols + slot_width - 1) / slot_width);
     }
     S.small_range[static_cast<size_t>(l)].count =
         static_cast<int64_t>(S.small_tasks.size() / 3) - S.small_range[static_cast<size_t>(l)].begin;
@@ -495,36 +499,61 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
       for (int q = qb; q < qe; ++q) {
         const int s = S.level_sn[static_cast<size_t>(q)];
         const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
-        // slot t: outer block t of kOuterPanels panels, factored with the
-        // rows below it by block tasks (sn, t, first row of a kBlockRows
-        // chunk; the first chunk writes the block), then the block's update
-        // of the pivot columns [c1, k), rows [c1, F)
         const int outer = kOuterPanels * B;
-        const int c0 = t * outer;
+        auto tiles = [&S, s, T](int32_t code, int nr, int nc) {
+          for (int tj = 0; tj * T < nc; ++tj) {
+            for (int ti = 0; ti * T < nr; ++ti) {
+              // lower part only: the tile must reach at or below the diagonal
+              if ((ti + 1) * T - 1 < tj * T) {
+                continue;
+              }
+              S.update_tasks.push_back(s);
+              S.update_tasks.push_back(code);
+              S.update_tasks.push_back(ti);
+              S.update_tasks.push_back(tj);
+            }
+          }
+        };
+        if (block_mode) {
+          // slot t: outer block t, factored with the rows below it by block
+          // tasks (sn, t, first row of a kBlockRows chunk; the first chunk
+          // writes the block), then the block's update of the pivot columns
+          // [c1, k), rows [c1, F)
+          const int c0 = t * outer;
+          if (c0 >= r.ncols || r.ncols <= small) {
+            continue;
+          }
+          const int c1 = std::min(r.ncols, c0 + outer);
+          const int chunks = std::max(1, (r.F - c1 + kBlockRows - 1) / kBlockRows);
+          for (int ch = 0; ch < chunks; ++ch) {
+            S.panel_tasks.push_back(s);
+            S.panel_tasks.push_back(t);
+            S.panel_tasks.push_back(c1 + ch * kBlockRows);
+          }
+          tiles(UpdateCodeOuter(t), r.F - c1, r.ncols - c1);
+          continue;
+        }
+        // slot t: panel t (sn, t, first row of a panel_rows chunk; chunk 0
+        // also owns the diagonal block), then the panel's update of the
+        // pivot columns [c1, cend) left in its outer block, rows [c1, F); the
+        // outer block's last panel is followed by the block's update of the
+        // pivot columns [cend, k), rows [cend, F)
+        const int c0 = t * B;
         if (c0 >= r.ncols || r.ncols <= small) {
           continue;
         }
-        const int c1 = std::min(r.ncols, c0 + outer);
-        const int below = r.F - c1;
-        const int chunks = std::max(1, (below + kBlockRows - 1) / kBlockRows);
+        const int c1 = std::min(r.ncols, c0 + B);
+        const int chunks = std::max(1, (r.F - c1 + S.panel_rows - 1) / S.panel_rows);
         for (int ch = 0; ch < chunks; ++ch) {
           S.panel_tasks.push_back(s);
           S.panel_tasks.push_back(t);
-          S.panel_tasks.push_back(c1 + ch * kBlockRows);
+          S.panel_tasks.push_back(c1 + ch * S.panel_rows);
         }
-        const int nr = r.F - c1;
-        const int nc = r.ncols - c1;
-        for (int tj = 0; tj * T < nc; ++tj) {
-          for (int ti = 0; ti * T < nr; ++ti) {
-            // lower part only: the tile must reach at or below the diagonal
-            if ((ti + 1) * T - 1 < tj * T) {
-              continue;
-            }
-            S.update_tasks.push_back(s);
-            S.update_tasks.push_back(UpdateCodeOuter(t));
-            S.update_tasks.push_back(ti);
-            S.update_tasks.push_back(tj);
-          }
+        const int cend = std::min(r.ncols, (c0 / outer + 1) * outer);
+        if (c1 < cend) {
+          tiles(UpdateCodeInner(t), r.F - c1, cend - c1);
+        } else if (cend < r.ncols) {
+          tiles(UpdateCodeOuter(c0 / outer), r.F - cend, r.ncols - cend);
         }
       }
       S.panel_range[slot].count = static_cast<int64_t>(S.panel_tasks.size() / 3) - S.panel_range[slot].begin;

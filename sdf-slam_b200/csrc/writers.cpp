@@ -113,7 +113,7 @@ void PointsOutsideMap(int nx, int ny, double min_x, double min_y, double max_x, 
       const double gy = (s * xy[2 * q] + c * xy[2 * q + 1]) + poses[3 * f + 1];
       const double fx = (gx - min_x) / dx;
       const double fy = (gy - min_y) / dy;
-      if (fx < 0.0 || fy < 0.0 || fx > nx - 1 || fy > ny - 1) {
+      if (!(fx >= 0.0) || !(fy >= 0.0) || !(fx <= nx - 1) || !(fy <= ny - 1)) {
         ++*outside;
       }
       ++*total;

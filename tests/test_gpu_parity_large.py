@@ -141,3 +141,35 @@ def test_mixed_step_tensor_core_fronts(workload, office_specs):
         print(f"{workload} mixed refine={refine}: max state difference {dev:.3e} of step {step:.3e}")
         assert dev <= bound * step
         g.close()
+
+
+@pytest.mark.parametrize("schedule", [(128, 256, 128), (64, 128, 64), (64, 128, 0), (128, 256, 0), (32, 256, 32)])
+def test_floorplan_every_factor_schedule(schedule):
+    """Each factorization schedule (single-kernel fronts up to small_pivots,
+    wider pivot blocks panel by panel or, with panel_rows 0, by whole outer
+    blocks) gives the oracle's three-iteration solve of the floor plan."""
+    specs, _ = scene_specs(scenes.floorplan_scene(seed=1))
+    gpu = P.Problem.from_specs(specs)
+    gpu.set_schedule(*schedule)
+    rg = P.solve(gpu, P.SolverOptions(max_iterations=3, step_tolerance=0.0))
+    ro = _floorplan_oracle_three()
+    hg = np.array(rg.cost_history)
+    ho = np.array(ro["cost_history"])
+    assert hg.shape == ho.shape
+    assert np.max(np.abs(hg - ho) / np.abs(ho)) <= 1e-8
+    gm, gp = gpu.state()
+    assert np.max(np.abs(gp[:, :2] - ro["poses"][:, :2])) <= 1e-4
+    assert np.max(np.abs(gm - ro["map"])) <= 1e-4
+
+
+_ORACLE_CACHE = {}
+
+
+def _floorplan_oracle_three():
+    if "floorplan3" not in _ORACLE_CACHE:
+        specs, _ = scene_specs(scenes.floorplan_scene(seed=1))
+        orc = oracle_from_specs(specs)
+        ro = orc.solve(max_iterations=3, step_tolerance=0.0, num_threads=0)
+        om, op = orc.state()
+        _ORACLE_CACHE["floorplan3"] = {"cost_history": ro["cost_history"], "poses": op, "map": om}
+    return _ORACLE_CACHE["floorplan3"]

@@ -137,3 +137,14 @@ def test_oracle_reproduces_committed_fixture():
     assert np.array_equal(lin["step"], g["step"])
     res = p.solve(max_iterations=10, num_threads=1)
     assert np.array_equal(np.array(res["cost_history"]), g["cost_history"])
+
+
+def test_set_schedule_rejects_out_of_range_values():
+    """sdfgpu_set_schedule checks its ranges before touching the handle (a
+    NULL handle fails as an invalid argument without a device)."""
+    import ctypes
+    from sdf_slam_b200 import _capi
+    L = _capi.load()
+    sched = (ctypes.c_int32 * 3)(128, 256, 128)
+    assert L.sdfgpu_set_schedule(None, sched) == 1
+    assert L.sdfgpu_set_schedule(None, None) == 1
