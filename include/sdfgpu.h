@@ -202,7 +202,7 @@ int32_t sdfgpu_debug_supernode_count(sdfgpu_problem* problem);
  * (useful flops, 2 per multiply-add; bytes for the classes for which
  * sdfgpu_kernel_class_is_memory_bound is 1); count <= SDFGPU_KERNEL_CLASSES,
  * any output may be NULL. */
-#define SDFGPU_KERNEL_CLASSES 9
+#define SDFGPU_KERNEL_CLASSES 10
 int sdfgpu_kernel_timing(sdfgpu_problem* problem, uint32_t class_mask);
 int sdfgpu_kernel_times(sdfgpu_problem* problem, double* ms, int64_t* launches, double* work, int32_t count);
 const char* sdfgpu_kernel_class_name(int32_t kernel_class);

@@ -721,7 +721,7 @@ def measure_fp64_peak() -> float:
     return v.value
 
 
-KERNEL_CLASSES = 9
+KERNEL_CLASSES = 10
 
 
 def kernel_class_names() -> list:

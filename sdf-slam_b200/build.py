@@ -31,6 +31,7 @@ SOURCES = {
     "noalloc.cu": [],
     "peak.cu": [],
     "schur_tc.cu": [],
+    "dense_root.cu": [],
     "refine.cu": [],
     "problem_device.cu": [],
     "problem_build.cpp": ["-x", "cu"],
@@ -43,7 +44,7 @@ SOURCES = {
     "server.cpp": ["-x", "cu"],
     "kernel_timer.cpp": ["-x", "cu"],
 }
-HEADERS = ["internal.h", "device.cuh", "engine.h", "ldlt.h", "server.h", "host_pool.h", "incremental.h", "schur_tc.h", "kernel_timer.h",
+HEADERS = ["internal.h", "device.cuh", "engine.h", "ldlt.h", "server.h", "host_pool.h", "incremental.h", "schur_tc.h", "kernel_timer.h", "dense_root.h", "front_ops.cuh",
            "trig.cuh"]
 
 

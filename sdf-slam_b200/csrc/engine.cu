@@ -890,6 +890,9 @@ FactorPlan Engine::Plan() {
   P.num_inv = static_cast<int>(sym_.inv_tasks.size() / 2);
   P.inv = inv_.get();
   P.big_tasks = tc_tasks_.get();
+  P.dense_tasks = dense_tasks_.get();
+  P.dense_sync = dense_sync_.get();
+  P.dense_inv = dense_inv_.get();
   P.solve_withhold = solve_withhold_;
   P.solve_wait_polls = solve_wait_polls_;
   // only the iteration's own factor and solve phases are timed
@@ -1036,6 +1039,9 @@ void Engine::SetSolveFault(int withhold, uint32_t wait_polls) {
 }
 
 void Engine::UploadSolveTasks(cudaStream_t s) {
+  dense_tasks_.Upload(sym_.dense_tasks, s);
+  dense_sync_.Alloc(DenseSyncWords(sym_));
+  dense_inv_.Alloc(static_cast<size_t>(std::max<int64_t>(1, sym_.dense_inv_doubles)));
   solve_tasks_.Upload(sym_.solve_tasks, s);
   solve_parts_.Upload(sym_.solve_parts, s);
   zpart_off_.Upload(sym_.zpart_off, s);

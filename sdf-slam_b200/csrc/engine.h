@@ -157,6 +157,12 @@ struct FactorPlan {
   /// 128 x 128 Schur tiles of the wide fronts (the tensor-core task list),
   /// taken by KUpdateBig for FP64 fronts.
   const int32_t* big_tasks{nullptr};
+  /// Tiled dense roots: task quads (Symbolic::dense_tasks), the sync words
+  /// (a claim counter per level, the abort flag, then the tile counters;
+  /// zeroed at the start of every factorization) and the inverse workspace.
+  const int32_t* dense_tasks{nullptr};
+  int32_t* dense_sync{nullptr};
+  double* dense_inv{nullptr};
   /// Test hook of the one-launch solve: a supernode whose forward flag is
   /// never published (-1: none) and the polls a wait may take (0: the
   /// default of about a second).
@@ -165,6 +171,12 @@ struct FactorPlan {
   /// Per-kernel device time of the launches (null: not timed).
   KernelTimer* timer{nullptr};
 };
+
+/// Words of the tiled dense roots' sync area: a claim counter per level,
+/// the abort flag, the tile counters.
+inline size_t DenseSyncWords(const Symbolic& S) {
+  return static_cast<size_t>(S.num_levels) + 1 + static_cast<size_t>(S.dense_cnt_words);
+}
 
 /// Doubles per inverted 32 x 32 diagonal block (the inverse and its
 /// transpose).
@@ -429,6 +441,8 @@ class Engine {
   DevBuf<uint32_t> allow_bits_;
   DevBuf<int32_t> ea_tasks_, ea_child_, panel_tasks_, update_tasks_, small_tasks_;
   DevBuf<double> fronts_, upd_;
+  DevBuf<int32_t> dense_tasks_, dense_sync_;  // tiled dense roots
+  DevBuf<double> dense_inv_;
   DevBuf<uint32_t> solve_sync_;  // counter and flags of the one-launch solve
   DevBuf<int32_t> solve_tasks_, solve_parts_;
   DevBuf<int64_t> zpart_off_;

@@ -20,10 +20,10 @@
 #include <cuda_runtime.h>
 
 #include "device.cuh"
+#include "front_ops.cuh"
 
 namespace sdfgpu {
 
-constexpr int kPanel = 32;
 constexpr int kTile = 64;
 constexpr int kPanelRowsPerBlock = 128;
 
@@ -37,74 +37,6 @@ __device__ __forceinline__ double* WorkFront<double>(const DeviceView& V, const 
 template <>
 __device__ __forceinline__ float* WorkFront<float>(const DeviceView& V, const SupernodeRec& S) {
   return V.fronts32 + S.front_off;
-}
-
-/// 1 / d by Newton-Raphson iteration x <- x + x (1 - d x), seeded with the
-/// hardware's approximate reciprocal (two steps square its ~2^-23 error
-/// below FP64 precision). Much shorter latency than a correctly rounded
-/// division on the pivot chain; the result may differ from 1.0 / d in the
-/// last bit.
-__device__ __forceinline__ double Recip(double d) {
-  double x;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(d));
-  double e = fma(-d, x, 1.0);
-  x = fma(x, e, x);
-  e = fma(-d, x, 1.0);
-  return fma(x, e, x);
-}
-__device__ __forceinline__ float Recip(float d) { return 1.0f / d; }
-
-/// LDL^T of the w x w (w <= 32) diagonal block at B (row r, column c at
-/// B[r * ld + c], lower triangle) by the block's first four warps (threads
-/// 0..127): lane i owns row i, warp q owns columns 8q..8q+7 in registers. At
-/// pivot j the owning warp inverts d_j (Newton reciprocal) and publishes
-/// W(:, j) and L(:, j) in shared memory (two buffers, alternating with j),
-/// one named barrier (id 1, 128 threads) later every warp subtracts
-/// W(i, j) L(c, j) from its columns; lanes that must not change a column
-/// subtract zero (a per-column branch costs more than the multiply-add).
-/// Measured on B200 for a 32x32 block: 10.7k cycles against 28k for one warp
-/// holding whole rows. Writes L below the diagonal and D on it; returns true
-/// when a pivot is exactly zero (in the four warps).
-template <typename T>
-__device__ __forceinline__ bool DiagonalBlockLdlt(T* B, int ld, int w, T (*lbuf)[kPanel], T (*wbuf)[kPanel]) {
-  const int lane = threadIdx.x & 31;
-  const int q = threadIdx.x >> 5;
-  T col[8];
-#pragma unroll
-  for (int t = 0; t < 8; ++t) {
-    const int c = 8 * q + t;
-    col[t] = (lane < w && c <= lane) ? B[lane * ld + c] : (c == lane ? T(1) : T(0));
-  }
-  bool zero = false;
-  for (int jb = 0; jb < 4; ++jb) {
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      const int j = 8 * jb + t;
-      if (j < w) {
-        const int b = j & 1;
-        if (q == jb) {
-          const T dj = __shfl_sync(0xffffffffu, col[t], j);
-          const T wij = col[t];
-          const T lij = wij * Recip(dj);
-          lbuf[b][lane] = lij;
-          wbuf[b][lane] = wij;
-          if (lane < w && lane >= j) {
-            B[lane * ld + j] = lane == j ? dj : lij;
-          }
-        }
-        asm volatile("bar.sync 1, 128;" ::: "memory");
-        zero = zero || (wbuf[b][j] == T(0));
-        const T m = lane > j ? wbuf[b][lane] : T(0);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int c = 8 * q + u;
-          const T mu = (c > j && c <= lane) ? m : T(0);
-          col[u] = fma(-mu, lbuf[b][c], col[u]);
-        }
-      }
-    }
-  }
-  return zero;
 }
 
 /// Adds one child's update columns [cbeg, cend) in place into the parent
@@ -2247,6 +2179,7 @@ __global__ void __launch_bounds__(256, 1) KSolveTree(DeviceView V, SolveArgs A) 
 
 #include <mutex>
 
+#include "dense_root.h"
 #include "engine.h"
 
 namespace sdfgpu {
@@ -2326,6 +2259,9 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
     }
     return w;
   };
+  if (P.dense_sync != nullptr && S.dense_cnt_words > 0) {
+    CudaCheck(cudaMemsetAsync(P.dense_sync, 0, DenseSyncWords(S) * sizeof(int32_t), stream), "dense sync reset");
+  }
   for (int l = 0; l < S.num_levels; ++l) {
     const TaskRange ea = S.ea_range[static_cast<size_t>(l)];
     if (ea.count > 0) {
@@ -2361,6 +2297,25 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
           V, P.small_tasks + 3 * sm.begin, P.dvec);
       ++launches;
     }
+    const TaskRange dr = S.dense_range[static_cast<size_t>(l)];
+    if (dr.count > 0 && P.dense_tasks != nullptr && P.dense_sync != nullptr) {
+      const TimedLaunch tl(P.timer, KernelTimer::kDenseRoot, stream, [&] {
+        return level_sum(l, [](const SupernodeRec& r) {
+          const double n = r.ncols;
+          return r.dense_cnt >= 0 ? 2.0 * n * n * n / 3.0 : 0.0;
+        });
+      });
+      DenseArgs A{};
+      A.tasks = P.dense_tasks + 4 * dr.begin;
+      A.count = dr.count;
+      A.claim = P.dense_sync + l;
+      A.abort = P.dense_sync + S.num_levels;
+      A.cnt = P.dense_sync + S.num_levels + 1;
+      A.inv = P.dense_inv;
+      A.dvec = P.dvec;
+      A.wait_limit = kWaitLimit;
+      launches += LaunchDenseRoots(V, A, stream);
+    }
     for (int t = 0; t < S.level_panels[static_cast<size_t>(l)]; ++t) {
       const size_t slot = static_cast<size_t>(S.panel_index_base[static_cast<size_t>(l)] + t);
       const TaskRange pr = S.panel_range[slot];
@@ -2370,7 +2325,7 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
           return level_sum(l, [&S, t, blocks](const SupernodeRec& r) {
             const int width = blocks ? kBlockCols : kPanel;
             const int c0 = t * width;
-            if (r.ncols <= S.small_pivots || c0 >= r.ncols) {
+            if (r.ncols <= S.small_pivots || c0 >= r.ncols || r.dense_cnt >= 0) {
               return 0.0;
             }
             // the block's LDL^T and the rows below it solved against it
@@ -2391,7 +2346,7 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
       if (ur.count > 0) {
         const TimedLaunch tl(P.timer, KernelTimer::kUpdatePanel, stream, [&] {
           return level_sum(l, [&S, t](const SupernodeRec& r) {
-            if (r.ncols <= S.small_pivots) {
+            if (r.ncols <= S.small_pivots || r.dense_cnt >= 0) {
               return 0.0;
             }
             // lower-part entries of the pivot columns [a, b) over rows [a, F)

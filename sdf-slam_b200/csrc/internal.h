@@ -155,6 +155,8 @@ struct SupernodeRec {
   int32_t upper_l11;  // 1: L of the pivot block is stored transposed in its upper triangle
   int32_t panel_base; // first of its ceil(ncols / 32) inverted diagonal blocks
   int64_t tc_pack;    // first packed operand row of its tensor-core Schur update (within its level), or -1
+  int64_t dense_cnt;  // a tiled dense root: first of its tile counters, else -1
+  int64_t dense_inv;  // a tiled dense root: first double of its diagonal-tile inverses
 };
 
 /// Task types of the one-launch solve.
@@ -181,6 +183,8 @@ enum SolveTask : int32_t {
 constexpr int kOuterPanels = 4;
 constexpr int32_t UpdateCodeInner(int panel) { return -2 - 2 * panel; }
 constexpr int32_t UpdateCodeOuter(int block) { return -3 - 2 * block; }
+/// Tile edge of the tiled dense-root factorization.
+constexpr int kDenseTileCols = 64;
 /// Rows below an outer block that one block-factorization task takes.
 constexpr int kBlockRows = 64;
 constexpr int kSolveWideRows = 512;
@@ -250,6 +254,16 @@ struct Symbolic {
   std::vector<int32_t> tc_tasks;
   std::vector<TaskRange> tc_range;
   int64_t tc_pack_rows{0};
+  // Dense pose roots (no rows below, more than small_pivots pivots) are
+  // factored by one persistent launch per level over 64 x 64 tiles instead
+  // of panels: (sn, i, j, k) task quads (FACTOR i == j == k, SOLVE j == k <
+  // i, UPDATE k < j <= i) in descending bottom level, dense_range per level,
+  // the tile counters (nt x nt per front) and the diagonal-tile inverses
+  // (64 x 64 doubles per tile) they use.
+  std::vector<int32_t> dense_tasks;
+  std::vector<TaskRange> dense_range;
+  int64_t dense_cnt_words{0};
+  int64_t dense_inv_doubles{0};
   // fronts with at most small_pivots pivots: one factorization kernel per
   // level, tasks (sn, first row of the chunk below the pivot block, rows in
   // the chunk) with front_rows threads per block (rows per chunk shrink to

@@ -8,7 +8,8 @@ namespace sdfgpu {
 const char* KernelTimer::Name(int c) {
   static const char* const kNames[kClasses] = {"KExtendAdd",     "KFactorFront", "KPanel",
                                                "KUpdate(panel)", "KUpdate(schur)", "KPackSchur",
-                                               "KSchurTc",       "KInvertDiagonal", "KSolveTree"};
+                                               "KSchurTc",       "KInvertDiagonal", "KSolveTree",
+                                               "KDenseRoot"};
   return c >= 0 && c < kClasses ? kNames[c] : "";
 }
 

@@ -23,6 +23,7 @@ class KernelTimer {
     kSchurTc,
     kInvertDiagonal,
     kSolveTree,
+    kDenseRoot,     // tiled LDL^T of the dense pose roots
     kClasses
   };
   static const char* Name(int c);

@@ -101,6 +101,12 @@ LdltEngine::LdltEngine(int n, const int32_t* outer, const int32_t* inner, const 
   zpart_.Alloc(static_cast<size_t>(std::max<int64_t>(1, sym_.zpart_doubles)));
   big_tasks_.Upload(sym_.tc_tasks, s);
   plan_.big_tasks = big_tasks_.get();
+  dense_tasks_.Upload(sym_.dense_tasks, s);
+  dense_sync_.Alloc(DenseSyncWords(sym_));
+  dense_inv_.Alloc(static_cast<size_t>(std::max<int64_t>(1, sym_.dense_inv_doubles)));
+  plan_.dense_tasks = dense_tasks_.get();
+  plan_.dense_sync = dense_sync_.get();
+  plan_.dense_inv = dense_inv_.get();
   plan_.solve_tasks = solve_tasks_.get();
   plan_.num_solve_tasks = static_cast<int>(sym_.solve_tasks.size() / 4);
   plan_.solve_parts = solve_parts_.get();

@@ -318,6 +318,62 @@ void ComputeRel(Symbolic& S) {
 }
 
 /// Level lists and task lists once all supernodes exist.
+/// One task of the tiled factorization of a dense root: FACTOR (i == j ==
+/// k), SOLVE (j == k < i) or UPDATE (k < j <= i), with its bottom level.
+struct DenseTileTask {
+  double prio;
+  int32_t sn;
+  int32_t i;
+  int32_t j;
+  int32_t k;
+};
+
+/// Appends the tasks of an n-column dense root's tiled LDL^T with their
+/// bottom levels: the longest path of task weights (FACTOR 8, SOLVE 2,
+/// UPDATE 2, about their relative durations) from the task to the end of
+/// the graph. A task's bottom level exceeds every successor's, so sorting
+/// by it descending lists each task after all the tasks it waits for.
+/// Successors: FACTOR(k) -> SOLVE(i, k); SOLVE(i, k) -> UPDATE(i, j, k) and
+/// UPDATE(i', i, k); UPDATE(i, j, k) -> UPDATE(i, j, k + 1) while k + 1 < j,
+/// else FACTOR(j) (i == j) or SOLVE(i, j).
+void AppendDenseTileTasks(int32_t sn, int n, std::vector<DenseTileTask>* out) {
+  const int nt = (n + kDenseTileCols - 1) / kDenseTileCols;
+  constexpr double kWFactor = 8.0;
+  constexpr double kWSolve = 2.0;
+  constexpr double kWUpdate = 2.0;
+  const size_t nn = static_cast<size_t>(nt) * nt;
+  std::vector<double> b_factor(static_cast<size_t>(nt), 0.0);
+  std::vector<double> b_solve(nn, 0.0);  // (i, k) at i * nt + k
+  std::vector<double> b_next(nn, 0.0);   // UPDATE(i, j, k + 1) at i * nt + j
+  std::vector<double> b_cur(nn, 0.0);    // UPDATE(i, j, k)
+  auto at = [nt](int i, int j) { return static_cast<size_t>(i) * nt + j; };
+  for (int k = nt - 1; k >= 0; --k) {
+    for (int j = k + 1; j < nt; ++j) {
+      for (int i = j; i < nt; ++i) {
+        const double succ = k + 1 < j ? b_next[at(i, j)] : (i == j ? b_factor[static_cast<size_t>(j)] : b_solve[at(i, j)]);
+        b_cur[at(i, j)] = kWUpdate + succ;
+        out->push_back({b_cur[at(i, j)], sn, i, j, k});
+      }
+    }
+    double fmax = 0.0;
+    for (int i = k + 1; i < nt; ++i) {
+      double m = 0.0;
+      for (int j = k + 1; j <= i; ++j) {
+        m = std::max(m, b_cur[at(i, j)]);
+      }
+      for (int i2 = i; i2 < nt; ++i2) {
+        m = std::max(m, b_cur[at(i2, i)]);
+      }
+      b_solve[at(i, k)] = kWSolve + m;
+      out->push_back({b_solve[at(i, k)], sn, i, k, k});
+      fmax = std::max(fmax, b_solve[at(i, k)]);
+    }
+    b_factor[static_cast<size_t>(k)] = kWFactor + fmax;
+    out->push_back({b_factor[static_cast<size_t>(k)], sn, k, k, k});
+    std::swap(b_next, b_cur);
+  }
+}
+
 void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int tile) {
   S.panel_width = panel_width;
   S.tile = tile;
@@ -350,6 +406,8 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   // blocks are factored at once (panel_rows 0), else one per panel
   const bool block_mode = S.panel_rows == 0;
   const int slot_width = block_mode ? kOuterPanels * B : B;
+  // dense pose roots take the tiled launch instead of panels
+  auto tiled = [&S](const SupernodeRec& r) { return r.pose_root != 0 && r.nrows == 0 && r.ncols > S.small_pivots; };
   // fronts factored by the single-kernel path keep the pivot block's lower
   // triangle (read by every task of the front) and store L11 transposed
   for (SupernodeRec& r : S.sn) {
@@ -418,7 +476,9 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
         S.small_max_k[static_cast<size_t>(l)] = std::max(S.small_max_k[static_cast<size_t>(l)], r.ncols);
         continue;
       }
-      maxp = std::max(maxp, (r.ncols + slot_width - 1) / slot_width);
+      if (!tiled(r)) {
+        maxp = std::max(maxp, (r.ncols + slot_width - 1) / slot_width);
+      }
     }
     S.small_range[static_cast<size_t>(l)].count =
         static_cast<int64_t>(S.small_tasks.size() / 3) - S.small_range[static_cast<size_t>(l)].begin;
@@ -499,6 +559,9 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
       for (int q = qb; q < qe; ++q) {
         const int s = S.level_sn[static_cast<size_t>(q)];
         const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
+        if (tiled(r)) {
+          continue;
+        }
         const int outer = kOuterPanels * B;
         auto tiles = [&S, s, T](int32_t code, int nr, int nc) {
           for (int tj = 0; tj * T < nc; ++tj) {
@@ -678,6 +741,55 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
     S.tc_range[static_cast<size_t>(l)].count =
         static_cast<int64_t>(S.tc_tasks.size() / 3) - S.tc_range[static_cast<size_t>(l)].begin;
     S.tc_pack_rows = std::max(S.tc_pack_rows, rows);
+  }
+  // tiled dense roots: counters, inverse workspace and task lists per level
+  S.dense_tasks.clear();
+  S.dense_range.assign(static_cast<size_t>(levels), {});
+  S.dense_cnt_words = 0;
+  S.dense_inv_doubles = 0;
+  for (SupernodeRec& r : S.sn) {
+    r.dense_cnt = -1;
+    r.dense_inv = 0;
+    if (tiled(r)) {
+      const int64_t nt = (r.ncols + kDenseTileCols - 1) / kDenseTileCols;
+      r.dense_cnt = S.dense_cnt_words;
+      r.dense_inv = S.dense_inv_doubles;
+      S.dense_cnt_words += nt * nt;
+      S.dense_inv_doubles += nt * kDenseTileCols * kDenseTileCols;
+    }
+  }
+  std::vector<DenseTileTask> level_tasks;
+  for (int l = 0; l < levels; ++l) {
+    level_tasks.clear();
+    for (int q = S.level_begin[static_cast<size_t>(l)]; q < S.level_begin[static_cast<size_t>(l) + 1]; ++q) {
+      const int s = S.level_sn[static_cast<size_t>(q)];
+      if (S.sn[static_cast<size_t>(s)].dense_cnt >= 0) {
+        AppendDenseTileTasks(s, S.sn[static_cast<size_t>(s)].ncols, &level_tasks);
+      }
+    }
+    std::sort(level_tasks.begin(), level_tasks.end(), [](const DenseTileTask& a, const DenseTileTask& b) {
+      if (a.prio != b.prio) {
+        return a.prio > b.prio;
+      }
+      if (a.k != b.k) {
+        return a.k < b.k;
+      }
+      if (a.i != b.i) {
+        return a.i < b.i;
+      }
+      if (a.j != b.j) {
+        return a.j < b.j;
+      }
+      return a.sn < b.sn;
+    });
+    S.dense_range[static_cast<size_t>(l)].begin = static_cast<int64_t>(S.dense_tasks.size() / 4);
+    for (const DenseTileTask& t : level_tasks) {
+      S.dense_tasks.push_back(t.sn);
+      S.dense_tasks.push_back(t.i);
+      S.dense_tasks.push_back(t.j);
+      S.dense_tasks.push_back(t.k);
+    }
+    S.dense_range[static_cast<size_t>(l)].count = static_cast<int64_t>(level_tasks.size());
   }
 }
 
