@@ -9,13 +9,18 @@
 // graph that every block of one launch works through:
 //
 //   FACTOR(k)      LDL^T of diagonal tile k (two 32-column halves), D into
-//                  dvec, L^-1 of the tile into the inverse workspace;
+//                  dvec, L^-1 of the tile into the inverse workspace; for
+//                  k >= 1 it first does
+//                  SOLVE(k, k - 1) and UPDATE(k, k, k - 1) itself (the
+//                  critical path: no hand-over between those three);
 //   SOLVE(i, k)    L(i, k) = A(i, k) L(k, k)^-T D(k)^-1, as a product with
-//                  the stored inverse;
-//   UPDATE(i,j,k)  A(i, j) -= L(i, k) D(k) L(j, k)^T, j <= i (lower part).
+//                  the stored inverse (i >= k + 2);
+//   UPDATE(i,j,k)  A(i, j) -= L(i, k) D(k) L(j, k)^T, j <= i (lower part;
+//                  not (k + 1, k + 1, k)).
 //
 // Each tile (i, j) has a counter: the updates applied to it (k of them before
-// step k), plus one once it is factored (i == j) or solved (i > j). A task
+// step k), plus one once it is factored (i == j) or solved (i > j); FACTOR(k)
+// publishes tile (k, k - 1) as solved before it goes on. A task
 // waits (one thread polling with acquire loads, bounded) until its inputs'
 // counters reach their values and publishes its own with a release store
 // after the block's writes; updates of a tile are applied in ascending k, so
@@ -70,6 +75,12 @@ __device__ __forceinline__ bool WaitTile(const int32_t* word, int32_t expected, 
     __nanosleep(64);
   }
   return false;
+}
+
+__device__ __forceinline__ uint64_t GlobalTimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
 }
 
 __device__ __forceinline__ void PublishTile(int32_t* word, int32_t value) {
@@ -136,9 +147,11 @@ __device__ __forceinline__ void TileProduct(const double* X, int64_t ldx, int xr
   __syncthreads();
 }
 
-/// Columns c of M = L^-1 for the unit lower w x w (w <= 32) triangle at
-/// T (row-major, ld kTLd, L(i, j) = T[i][j] for i > j), one warp: lane c
-/// solves L m = e_c by forward substitution. M(i, c) -> Mo[i * kHLd + c].
+/// Columns c of M = L^-1 for the unit lower 32 x 32 triangle at T
+/// (row-major, ld kTLd, L(i, j) = T[i][j] for i > j), one warp: lane c
+/// solves L m = e_c by forward substitution (unrolled: a loop over the
+/// pivots with the register vector indexed at run time measured three
+/// times slower). M(i, c) -> Mo[i * kHLd + c].
 __device__ __forceinline__ void InvertUnitLower32(const double* T, double* Mo) {
   const int lane = threadIdx.x & 31;
   double m[32];
@@ -159,17 +172,39 @@ __device__ __forceinline__ void InvertUnitLower32(const double* T, double* Mo) {
   }
 }
 
-/// FACTOR(k): LDL^T of diagonal tile k in shared memory as two 32-column
-/// halves (the second updated by the first's L21 D1 L21^T), then D, L and,
-/// when tiles below exist, L^-1 of the tile.
-__device__ void FactorTile(const DeviceView& V, const SupernodeRec& S, int k, int nt, const DenseArgs& A,
-                           double* sm) {
+/// out(r, c) = sum over l < 32 of X[r * xld + l] Y[c * yld + l] for the
+/// 32 x 32 block: thread (r = lane, c = warp + 8 q), four outputs each.
+template <typename F>
+__device__ __forceinline__ void Small32(const double* X, int xld, const double* Y, int yld, F&& sink) {
+  const int r = threadIdx.x & 31;
+  const int c0 = threadIdx.x >> 5;
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+  for (int l = 0; l < 32; ++l) {
+    const double x = X[r * xld + l];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      s[q] = fma(x, Y[(c0 + 8 * q) * yld + l], s[q]);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    sink(r, c0 + 8 * q, s[q]);
+  }
+}
+
+/// FACTOR(k) on the tile already in T (shared, row-major, lower triangle,
+/// the identity beyond w): LDL^T as two 32-column halves (the second
+/// updated by the first's L21 D1 L21^T), D into dvec, L into the front and,
+/// when tiles below exist, L^-1 into the inverse workspace.
+__device__ void FactorLoaded(const DeviceView& V, const SupernodeRec& S, int k, int nt, const DenseArgs& A,
+                             double* sm) {
   const int64_t F = S.F;
   const int c0 = k * kDT;
   const int w = min(kDT, S.ncols - c0);
   double* Fs = V.fronts + S.front_off;
   double(*T)[kTLd] = reinterpret_cast<double(*)[kTLd]>(sm);
-  double* M1 = sm + kDT * kTLd;  // L11^-1
+  double* M1 = sm + kDT * kTLd;  // L11^-1 (zero above the diagonal)
   double* Y = M1 + 32 * kHLd;    // A21 L11^-T = L21 D1, then L21 L11^-1
   double* M2 = Y + 32 * kHLd;    // L22^-1
   double* dinv = M2 + 32 * kHLd;
@@ -177,64 +212,42 @@ __device__ void FactorTile(const DeviceView& V, const SupernodeRec& S, int k, in
   double(*wbuf)[kPanel] = lbuf + 2;
   int* zflag = reinterpret_cast<int*>(dinv + kDT + 4 * kPanel);
   const int tid = threadIdx.x;
-  for (int e = tid; e < kDT * kDT; e += kDThreads) {
-    const int j = e >> 6;
-    const int i = e & 63;
-    double v;
-    if (i < w && j < w) {
-      v = i >= j ? Fs[static_cast<int64_t>(c0 + j) * F + c0 + i] : 0.0;
-    } else {
-      v = i == j ? 1.0 : 0.0;
-    }
-    T[i][j] = v;
-  }
-  if (tid == 0) {
-    *zflag = 0;
-  }
-  __syncthreads();
   if (tid < 128) {
     const bool z = DiagonalBlockLdlt<double>(&T[0][0], kTLd, min(32, w), lbuf, wbuf);
-    if (tid == 0 && z) {
-      *zflag = 1;
+    if (tid == 0) {
+      *zflag = z ? 1 : 0;
     }
   }
   __syncthreads();
-  const bool second = w > 32;
-  if (second) {
+  if (w > 32) {
     if (tid < 32) {
       InvertUnitLower32(&T[0][0], M1);
     } else if (tid < 64) {
       dinv[tid - 32] = Recip(T[tid - 32][tid - 32]);
     }
     __syncthreads();
-    // Y(r, j) = sum_{l <= j} A21(r, l) M1(j, l)
-    {
-      const int r = tid & 31;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int j = (tid >> 5) + 8 * q;
-        double s = 0.0;
-        for (int l = 0; l <= j; ++l) {
-          s = fma(T[32 + r][l], M1[j * kHLd + l], s);
-        }
-        Y[r * kHLd + j] = s;
-      }
-    }
+    // Y = A21 M1^T
+    Small32(&T[32][0], kTLd, M1, kHLd, [&](int r, int c, double v) { Y[r * kHLd + c] = v; });
     __syncthreads();
     // L21 = Y D1^-1 over A21; A22 -= L21 Y^T (lower part)
     {
       const int r = tid & 31;
+      const int cb = tid >> 5;
+      double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+      for (int j = 0; j < 32; ++j) {
+        const double lr = Y[r * kHLd + j] * dinv[j];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          acc[q] = fma(lr, Y[(cb + 8 * q) * kHLd + j], acc[q]);
+        }
+      }
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const int c = (tid >> 5) + 8 * q;
+        const int c = cb + 8 * q;
         T[32 + r][c] = Y[r * kHLd + c] * dinv[c];
         if (r >= c) {
-          double acc = 0.0;
-#pragma unroll 8
-          for (int j = 0; j < 32; ++j) {
-            acc = fma(Y[r * kHLd + j] * dinv[j], Y[c * kHLd + j], acc);
-          }
-          T[32 + r][32 + c] -= acc;
+          T[32 + r][32 + c] -= acc[q];
         }
       }
     }
@@ -272,44 +285,71 @@ __device__ void FactorTile(const DeviceView& V, const SupernodeRec& S, int k, in
     if (tid < 32) {
       InvertUnitLower32(&T[32][32], M2);
     }
+    // P = L21 M1 into Y: P(r, c) = sum_l L21(r, l) M1(l, c), with M1
+    // column c read as a row of its transpose
     __syncthreads();
-    // P = L21 M1 over Y (Y is no longer needed)
     {
       const int r = tid & 31;
-      double p[4];
+      const int cb = tid >> 5;
+      double p[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+      for (int l = 0; l < 32; ++l) {
+        const double x = T[32 + r][l];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int c = (tid >> 5) + 8 * q;
-        double s = 0.0;
-        for (int l = c; l < 32; ++l) {
-          s = fma(T[32 + r][l], M1[l * kHLd + c], s);
+        for (int q = 0; q < 4; ++q) {
+          p[q] = fma(x, M1[l * kHLd + cb + 8 * q], p[q]);
         }
-        p[q] = s;
       }
       __syncthreads();
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        Y[r * kHLd + (tid >> 5) + 8 * q] = p[q];
+        Y[r * kHLd + cb + 8 * q] = p[q];
       }
     }
     __syncthreads();
     {
       const int r = tid & 31;
+      const int cb = tid >> 5;
+      double m[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 8
+      for (int l = 0; l < 32; ++l) {
+        const double x = M2[r * kHLd + l];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          m[q] = fma(x, Y[l * kHLd + cb + 8 * q], m[q]);
+        }
+      }
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const int c = (tid >> 5) + 8 * q;
-        double s = 0.0;
-        for (int l = 0; l <= r; ++l) {
-          s = fma(M2[r * kHLd + l], Y[l * kHLd + c], s);
-        }
-        // M(32 + r, c) = -s; M(r, c) = M1; M(32 + r, 32 + c) = M2; upper 0
-        Mo[static_cast<int64_t>(c) * kDT + 32 + r] = -s;
+        const int c = cb + 8 * q;
+        Mo[static_cast<int64_t>(c) * kDT + 32 + r] = -m[q];
         Mo[static_cast<int64_t>(c) * kDT + r] = M1[r * kHLd + c];
         Mo[static_cast<int64_t>(32 + c) * kDT + 32 + r] = M2[r * kHLd + c];
         Mo[static_cast<int64_t>(32 + c) * kDT + r] = 0.0;
       }
     }
   }
+}
+
+/// Loads diagonal tile k's lower triangle into T (the identity beyond w),
+/// subtracting sub(r, c) when given (the update folded into the task).
+__device__ __forceinline__ void LoadDiagonal(const SupernodeRec& S, const double* Fs, int k, double* sm) {
+  const int64_t F = S.F;
+  const int c0 = k * kDT;
+  const int w = min(kDT, S.ncols - c0);
+  double(*T)[kTLd] = reinterpret_cast<double(*)[kTLd]>(sm);
+  for (int e = threadIdx.x; e < kDT * kDT; e += kDThreads) {
+    const int j = e >> 6;
+    const int i = e & 63;
+    double v;
+    if (i < w && j < w) {
+      v = i >= j ? Fs[static_cast<int64_t>(c0 + j) * F + c0 + i] : 0.0;
+    } else {
+      v = i == j ? 1.0 : 0.0;
+    }
+    T[i][j] = v;
+  }
+  __syncthreads();
 }
 
 /// SOLVE(i, k): L(i, k) = A(i, k) M^T D^-1 with M = L(k, k)^-1.
@@ -343,20 +383,29 @@ __device__ void SolveTile(const DeviceView& V, const SupernodeRec& S, int i, int
   }
 }
 
+/// acc = L(i, k) D(k) L(j, k)^T for output tile (i, j).
+__device__ __forceinline__ void UpdateProduct(const SupernodeRec& S, const double* Fs, int i, int j, int k,
+                                              const DenseArgs& A, double* sm, double acc[4][4]) {
+  const int64_t F = S.F;
+  const int c0 = k * kDT;
+  const int w = min(kDT, S.ncols - c0);
+  const int hi = min(kDT, S.ncols - i * kDT);
+  const int hj = min(kDT, S.ncols - j * kDT);
+  TileProduct(Fs + static_cast<int64_t>(c0) * F + i * kDT, F, hi, Fs + static_cast<int64_t>(c0) * F + j * kDT, F, hj,
+              w, A.dvec + S.first_col + c0, sm, acc);
+}
+
 /// UPDATE(i, j, k): A(i, j) -= L(i, k) D(k) L(j, k)^T, lower part.
 __device__ void UpdateTile(const DeviceView& V, const SupernodeRec& S, int i, int j, int k, const DenseArgs& A,
                            double* sm) {
   const int64_t F = S.F;
-  const int c0 = k * kDT;
   const int ri = i * kDT;
   const int rj = j * kDT;
-  const int w = min(kDT, S.ncols - c0);
   const int hi = min(kDT, S.ncols - ri);
   const int hj = min(kDT, S.ncols - rj);
   double* Fs = V.fronts + S.front_off;
   double acc[4][4] = {};
-  TileProduct(Fs + static_cast<int64_t>(c0) * F + ri, F, hi, Fs + static_cast<int64_t>(c0) * F + rj, F, hj, w,
-              A.dvec + S.first_col + c0, sm, acc);
+  UpdateProduct(S, Fs, i, j, k, A, sm, acc);
   const int tx = threadIdx.x & 15;
   const int ty = threadIdx.x >> 4;
   // all sixteen reads, then the writes
@@ -384,7 +433,51 @@ __device__ void UpdateTile(const DeviceView& V, const SupernodeRec& S, int i, in
   }
 }
 
-__global__ void __launch_bounds__(kDThreads, 2) KDenseRoot(DeviceView V, DenseArgs A) {
+/// FACTOR(k). For k >= 1 the task first does the two steps that feed it:
+/// SOLVE(k, k - 1) (published as soon as it is written, for the other
+/// updates of step k - 1) and UPDATE(k, k, k - 1), whose result goes
+/// straight into the shared-memory tile instead of the front.
+__device__ void FactorTask(const DeviceView& V, const SupernodeRec& S, int k, int nt, const DenseArgs& A,
+                           int32_t* cnt, double* sm) {
+  double* Fs = V.fronts + S.front_off;
+  if (k == 0) {
+    LoadDiagonal(S, Fs, 0, sm);
+  } else {
+    SolveTile(V, S, k, k - 1, A, sm);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      PublishTile(cnt + k * nt + (k - 1), k);
+    }
+    double acc[4][4] = {};
+    UpdateProduct(S, Fs, k, k, k - 1, A, sm, acc);
+    const int64_t F = S.F;
+    const int c0 = k * kDT;
+    const int w = min(kDT, S.ncols - c0);
+    double(*T)[kTLd] = reinterpret_cast<double(*)[kTLd]>(sm);
+    const int tx = threadIdx.x & 15;
+    const int ty = threadIdx.x >> 4;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int c = ty + 16 * b;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int r = tx + 16 * a;
+        double v;
+        if (r < w && c < w) {
+          v = r >= c ? Fs[static_cast<int64_t>(c0 + c) * F + c0 + r] - acc[a][b] : 0.0;
+        } else {
+          v = r == c ? 1.0 : 0.0;
+        }
+        T[r][c] = v;
+      }
+    }
+    __syncthreads();
+  }
+  FactorLoaded(V, S, k, nt, A, sm);
+}
+
+__global__ void __launch_bounds__(kDThreads, 1) KDenseRoot(DeviceView V, DenseArgs A) {
   extern __shared__ double dense_sm[];
   __shared__ int task;
   __shared__ int go;
@@ -411,9 +504,15 @@ __global__ void __launch_bounds__(kDThreads, 2) KDenseRoot(DeviceView V, DenseAr
     const int nt = (S.ncols + kDT - 1) / kDT;
     int32_t* cnt = A.cnt + S.dense_cnt;
     if (tid == 0) {
+      if (A.trace != nullptr) {
+        A.trace[3 * t] = GlobalTimer();
+      }
       bool ok;
       if (i == k) {
-        ok = WaitTile(cnt + k * nt + k, k, A.abort, A.wait_limit);
+        // FACTOR(k) with SOLVE(k, k - 1) and UPDATE(k, k, k - 1) folded in
+        ok = k == 0 || (WaitTile(cnt + (k - 1) * nt + (k - 1), k, A.abort, A.wait_limit) &&
+                        WaitTile(cnt + k * nt + (k - 1), k - 1, A.abort, A.wait_limit) &&
+                        WaitTile(cnt + k * nt + k, k - 1, A.abort, A.wait_limit));
       } else if (j == k) {
         ok = WaitTile(cnt + k * nt + k, k + 1, A.abort, A.wait_limit) &&
              WaitTile(cnt + i * nt + k, k, A.abort, A.wait_limit);
@@ -427,13 +526,16 @@ __global__ void __launch_bounds__(kDThreads, 2) KDenseRoot(DeviceView V, DenseAr
         atomicExch(A.abort, 1);
       }
       go = ok ? 1 : 0;
+      if (A.trace != nullptr) {
+        A.trace[3 * t + 1] = GlobalTimer();
+      }
     }
     __syncthreads();
     if (go == 0) {
       continue;
     }
     if (i == k) {
-      FactorTile(V, S, k, nt, A, dense_sm);
+      FactorTask(V, S, k, nt, A, cnt, dense_sm);
     } else if (j == k) {
       SolveTile(V, S, i, k, A, dense_sm);
     } else {
@@ -443,6 +545,9 @@ __global__ void __launch_bounds__(kDThreads, 2) KDenseRoot(DeviceView V, DenseAr
     if (tid == 0) {
       __threadfence();
       PublishTile(cnt + i * nt + j, k + 1);
+      if (A.trace != nullptr) {
+        A.trace[3 * t + 2] = GlobalTimer();
+      }
     }
   }
 }

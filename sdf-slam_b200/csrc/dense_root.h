@@ -19,10 +19,13 @@ struct DenseArgs {
   double* inv;           // per dense front (SupernodeRec::dense_inv): L^-1 of each diagonal tile, 64 x 64
   double* dvec;
   uint32_t wait_limit;
+  /// Optional task trace (null: off): per task, the global timer in ns when
+  /// a block took it, when its inputs were ready and when it published.
+  uint64_t* trace;
 };
 
 /// Launches the persistent tiled factorization over args.count tasks on
-/// `stream` (blocks: at most two per SM, never more than the tasks).
+/// `stream` (one block per SM, never more blocks than tasks).
 /// Returns the launches made (0 or 1).
 int LaunchDenseRoots(const DeviceView& V, const DenseArgs& args, cudaStream_t stream);
 

@@ -2314,6 +2314,7 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
       A.inv = P.dense_inv;
       A.dvec = P.dvec;
       A.wait_limit = kWaitLimit;
+      A.trace = nullptr;
       launches += LaunchDenseRoots(V, A, stream);
     }
     for (int t = 0; t < S.level_panels[static_cast<size_t>(l)]; ++t) {

@@ -185,6 +185,24 @@ constexpr int32_t UpdateCodeInner(int panel) { return -2 - 2 * panel; }
 constexpr int32_t UpdateCodeOuter(int block) { return -3 - 2 * block; }
 /// Tile edge of the tiled dense-root factorization.
 constexpr int kDenseTileCols = 64;
+/// One task of the tiled factorization of a dense root: FACTOR (i == j ==
+/// k), SOLVE (j == k < i) or UPDATE (k < j <= i), with its bottom level.
+struct DenseTileTask {
+  double prio;
+  int32_t sn;
+  int32_t i;
+  int32_t j;
+  int32_t k;
+};
+
+/// Appends the tasks of an n-column dense root's tiled LDL^T (kDenseTileCols
+/// tiles) with their bottom levels: the longest path of task weights
+/// (FACTOR 8, SOLVE 2, UPDATE 2) from the task to the end of the graph.
+/// Sorted by it descending, every task follows the tasks it waits for.
+void AppendDenseTileTasks(int32_t sn, int n, std::vector<DenseTileTask>* out);
+/// The order blocks take the tasks in: bottom level descending (ties by k,
+/// i, j, supernode).
+void OrderDenseTileTasks(std::vector<DenseTileTask>* tasks);
 /// Rows below an outer block that one block-factorization task takes.
 constexpr int kBlockRows = 64;
 constexpr int kSolveWideRows = 512;

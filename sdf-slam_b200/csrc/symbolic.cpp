@@ -318,62 +318,6 @@ void ComputeRel(Symbolic& S) {
 }
 
 /// Level lists and task lists once all supernodes exist.
-/// One task of the tiled factorization of a dense root: FACTOR (i == j ==
-/// k), SOLVE (j == k < i) or UPDATE (k < j <= i), with its bottom level.
-struct DenseTileTask {
-  double prio;
-  int32_t sn;
-  int32_t i;
-  int32_t j;
-  int32_t k;
-};
-
-/// Appends the tasks of an n-column dense root's tiled LDL^T with their
-/// bottom levels: the longest path of task weights (FACTOR 8, SOLVE 2,
-/// UPDATE 2, about their relative durations) from the task to the end of
-/// the graph. A task's bottom level exceeds every successor's, so sorting
-/// by it descending lists each task after all the tasks it waits for.
-/// Successors: FACTOR(k) -> SOLVE(i, k); SOLVE(i, k) -> UPDATE(i, j, k) and
-/// UPDATE(i', i, k); UPDATE(i, j, k) -> UPDATE(i, j, k + 1) while k + 1 < j,
-/// else FACTOR(j) (i == j) or SOLVE(i, j).
-void AppendDenseTileTasks(int32_t sn, int n, std::vector<DenseTileTask>* out) {
-  const int nt = (n + kDenseTileCols - 1) / kDenseTileCols;
-  constexpr double kWFactor = 8.0;
-  constexpr double kWSolve = 2.0;
-  constexpr double kWUpdate = 2.0;
-  const size_t nn = static_cast<size_t>(nt) * nt;
-  std::vector<double> b_factor(static_cast<size_t>(nt), 0.0);
-  std::vector<double> b_solve(nn, 0.0);  // (i, k) at i * nt + k
-  std::vector<double> b_next(nn, 0.0);   // UPDATE(i, j, k + 1) at i * nt + j
-  std::vector<double> b_cur(nn, 0.0);    // UPDATE(i, j, k)
-  auto at = [nt](int i, int j) { return static_cast<size_t>(i) * nt + j; };
-  for (int k = nt - 1; k >= 0; --k) {
-    for (int j = k + 1; j < nt; ++j) {
-      for (int i = j; i < nt; ++i) {
-        const double succ = k + 1 < j ? b_next[at(i, j)] : (i == j ? b_factor[static_cast<size_t>(j)] : b_solve[at(i, j)]);
-        b_cur[at(i, j)] = kWUpdate + succ;
-        out->push_back({b_cur[at(i, j)], sn, i, j, k});
-      }
-    }
-    double fmax = 0.0;
-    for (int i = k + 1; i < nt; ++i) {
-      double m = 0.0;
-      for (int j = k + 1; j <= i; ++j) {
-        m = std::max(m, b_cur[at(i, j)]);
-      }
-      for (int i2 = i; i2 < nt; ++i2) {
-        m = std::max(m, b_cur[at(i2, i)]);
-      }
-      b_solve[at(i, k)] = kWSolve + m;
-      out->push_back({b_solve[at(i, k)], sn, i, k, k});
-      fmax = std::max(fmax, b_solve[at(i, k)]);
-    }
-    b_factor[static_cast<size_t>(k)] = kWFactor + fmax;
-    out->push_back({b_factor[static_cast<size_t>(k)], sn, k, k, k});
-    std::swap(b_next, b_cur);
-  }
-}
-
 void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int tile) {
   S.panel_width = panel_width;
   S.tile = tile;
@@ -767,21 +711,7 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
         AppendDenseTileTasks(s, S.sn[static_cast<size_t>(s)].ncols, &level_tasks);
       }
     }
-    std::sort(level_tasks.begin(), level_tasks.end(), [](const DenseTileTask& a, const DenseTileTask& b) {
-      if (a.prio != b.prio) {
-        return a.prio > b.prio;
-      }
-      if (a.k != b.k) {
-        return a.k < b.k;
-      }
-      if (a.i != b.i) {
-        return a.i < b.i;
-      }
-      if (a.j != b.j) {
-        return a.j < b.j;
-      }
-      return a.sn < b.sn;
-    });
+    OrderDenseTileTasks(&level_tasks);
     S.dense_range[static_cast<size_t>(l)].begin = static_cast<int64_t>(S.dense_tasks.size() / 4);
     for (const DenseTileTask& t : level_tasks) {
       S.dense_tasks.push_back(t.sn);
@@ -794,6 +724,146 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
 }
 
 }  // namespace
+
+/// Appends the tasks of an n-column dense root's tiled LDL^T with their
+/// bottom levels: the longest path of task weights (about their relative
+/// durations) from the task to the end of the graph, so that sorting by it
+/// descending lists each task after the tasks it waits for. Tasks: FACTOR(k)
+/// (with SOLVE(k, k - 1) and UPDATE(k, k, k - 1) folded in for k >= 1),
+/// SOLVE(i, k) for i >= k + 2, UPDATE(i, j, k) for k < j <= i except
+/// (k + 1, k + 1, k). Successors:
+///   FACTOR(k)     -> FACTOR(k + 1), SOLVE(i, k), UPDATE(i, k, k - 1) (it
+///                    produces L(k, k - 1));
+///   SOLVE(i, k)   -> UPDATE(i, j, k), UPDATE(i', i, k);
+///   UPDATE(i,j,k) -> the next step's task on tile (i, j): UPDATE(i, j, k + 1)
+///                    or, folded into them, FACTOR(j) (i == j == k + 2) and
+///                    FACTOR(j + 1) (i == j + 1 == k + 2); SOLVE(i, j) when
+///                    j == k + 1 and i >= j + 2.
+/// A topological order is tau = 4k (FACTOR), 4k + 1 (SOLVE), 4k + 2 (UPDATE,
+/// j >= k + 2), 4k + 4.5 (UPDATE, j == k + 1); the bottom levels are
+/// computed in decreasing tau.
+void AppendDenseTileTasks(int32_t sn, int n, std::vector<DenseTileTask>* out) {
+  const int nt = (n + kDenseTileCols - 1) / kDenseTileCols;
+  constexpr double kWFactor = 6.0;     // FACTOR(0) alone
+  constexpr double kWFolded = 14.0;    // FACTOR(k >= 1) with its SOLVE and UPDATE
+  constexpr double kWSolve = 4.0;
+  constexpr double kWUpdate = 4.0;
+  struct Item {
+    double tau;
+    int32_t i, j, k;
+  };
+  std::vector<Item> items;
+  for (int k = 0; k < nt; ++k) {
+    items.push_back({4.0 * k, k, k, k});
+    for (int i = k + 2; i < nt; ++i) {
+      items.push_back({4.0 * k + 1.0, i, k, k});
+    }
+    for (int j = k + 1; j < nt; ++j) {
+      for (int i = j; i < nt; ++i) {
+        if (i == k + 1 && j == k + 1) {
+          continue;
+        }
+        items.push_back({j == k + 1 ? 4.0 * k + 4.5 : 4.0 * k + 2.0, i, j, k});
+      }
+    }
+  }
+  std::sort(items.begin(), items.end(), [](const Item& a, const Item& b) { return a.tau > b.tau; });
+  const size_t nn = static_cast<size_t>(nt) * nt;
+  // bottom levels: FACTOR per k, SOLVE per (i, k), UPDATE per (i, j) of the
+  // step being computed and of the step after it (tau orders steps so that
+  // both are all that is read)
+  std::vector<double> bf(static_cast<size_t>(nt), 0.0);
+  std::vector<double> bs(nn, 0.0);
+  std::vector<std::vector<double>> bu(static_cast<size_t>(nt) + 1);
+  auto ub = [&](int i, int j, int k) -> double {
+    if (k >= nt || bu[static_cast<size_t>(k)].empty()) {
+      return 0.0;
+    }
+    return bu[static_cast<size_t>(k)][static_cast<size_t>(i) * nt + j];
+  };
+  auto uset = [&](int i, int j, int k, double v) {
+    std::vector<double>& b = bu[static_cast<size_t>(k)];
+    if (b.empty()) {
+      b.assign(nn, 0.0);
+    }
+    b[static_cast<size_t>(i) * nt + j] = v;
+  };
+  auto next_on_tile = [&](int i, int j, int k) -> double {
+    // the task that next reads or writes tile (i, j) after UPDATE(i, j, k)
+    if (k + 1 < j) {
+      if (i == j && j == k + 2) {
+        return bf[static_cast<size_t>(j)];
+      }
+      if (i == j + 1 && j == k + 1) {
+        return bf[static_cast<size_t>(i)];
+      }
+      return ub(i, j, k + 1);
+    }
+    // j == k + 1: the tile is complete
+    if (i == j + 1) {
+      return bf[static_cast<size_t>(i)];
+    }
+    return bs[static_cast<size_t>(i) * nt + j];
+  };
+  std::vector<DenseTileTask> local;
+  local.reserve(items.size());
+  for (const Item& it : items) {
+    const int i = it.i;
+    const int j = it.j;
+    const int k = it.k;
+    double b;
+    if (i == k && j == k) {
+      double m = k + 1 < nt ? bf[static_cast<size_t>(k) + 1] : 0.0;
+      for (int r = k + 2; r < nt; ++r) {
+        m = std::max(m, bs[static_cast<size_t>(r) * nt + k]);
+      }
+      if (k >= 1) {
+        for (int r = k + 1; r < nt; ++r) {
+          m = std::max(m, ub(r, k, k - 1));
+        }
+      }
+      b = (k == 0 ? kWFactor : kWFolded) + m;
+      bf[static_cast<size_t>(k)] = b;
+    } else if (j == k) {
+      double m = 0.0;
+      for (int c = k + 1; c <= i; ++c) {
+        m = std::max(m, ub(i, c, k));
+      }
+      for (int r = i; r < nt; ++r) {
+        m = std::max(m, ub(r, i, k));
+      }
+      b = kWSolve + m;
+      bs[static_cast<size_t>(i) * nt + k] = b;
+    } else {
+      b = kWUpdate + next_on_tile(i, j, k);
+      uset(i, j, k, b);
+    }
+    local.push_back({b, sn, i, j, k});
+    // steps two behind the one being computed are no longer read
+    if (k + 3 <= nt && !bu[static_cast<size_t>(k) + 2].empty() && i == k && j == k) {
+      std::vector<double>().swap(bu[static_cast<size_t>(k) + 2]);
+    }
+  }
+  out->insert(out->end(), local.begin(), local.end());
+}
+
+void OrderDenseTileTasks(std::vector<DenseTileTask>* tasks) {
+  std::sort(tasks->begin(), tasks->end(), [](const DenseTileTask& a, const DenseTileTask& b) {
+    if (a.prio != b.prio) {
+      return a.prio > b.prio;
+    }
+    if (a.k != b.k) {
+      return a.k < b.k;
+    }
+    if (a.i != b.i) {
+      return a.i < b.i;
+    }
+    if (a.j != b.j) {
+      return a.j < b.j;
+    }
+    return a.sn < b.sn;
+  });
+}
 
 SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
   if (threads <= 0) {
