@@ -154,9 +154,6 @@ struct FactorPlan {
   const int32_t* pack_tasks{nullptr};
   const int32_t* tc_tasks{nullptr};
   TcArgs tc{};
-  /// 128 x 128 Schur tiles of the wide fronts (the tensor-core task list),
-  /// taken by KUpdateBig for FP64 fronts.
-  const int32_t* big_tasks{nullptr};
   /// Tiled dense roots: task quads (Symbolic::dense_tasks), the sync words
   /// (a claim counter per level, the abort flag, then the tile counters;
   /// zeroed at the start of every factorization) and the inverse workspace.

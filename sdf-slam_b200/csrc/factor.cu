@@ -961,140 +961,6 @@ __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeR
   }
 }
 
-/// FP64 Schur complement of a wide front (the fronts the tensor-core path
-/// takes in mixed solves): one 128 x 128 tile (ti, tj), ti >= tj, of the
-/// trailing block, C -= L_I D L_J^T over all k pivots. 256 threads, each
-/// holding an 8 x 8 block of the tile in registers (rows 4 tx + {0..3} and
-/// 64 + 4 tx + {0..3}, columns likewise with ty), K in chunks of 16 staged in
-/// shared memory (two buffers; the next chunk is loaded into registers, D
-/// applied, while the current one is multiplied): 64 multiply-adds per 16
-/// shared-memory doubles, which keeps the FP64 pipe rather than shared
-/// memory the bound (a 4 x 4 block per thread needs twice the bytes per
-/// multiply-add).
-constexpr int kBigTile = 128;
-constexpr int kBigK = 16;
-constexpr int kBigThreads = 256;
-constexpr size_t kBigSmem = 4 * static_cast<size_t>(kBigK) * kBigTile * sizeof(double);
-
-__global__ void __launch_bounds__(kBigThreads, 1) KUpdateBig(DeviceView V, const int32_t* tasks, const double* dvec) {
-  const int32_t* t = tasks + 3 * static_cast<int64_t>(blockIdx.x);
-  const SupernodeRec S = V.sn[t[0]];
-  // FP32 fronts of a mixed solve take the tensor-core path
-  if (V.active[S.instance] == 0 || Fp32Front(V, S)) {
-    return;
-  }
-  extern __shared__ __align__(16) double big_smem[];
-  auto As = reinterpret_cast<double(*)[kBigK][kBigTile]>(big_smem);
-  auto Bs = reinterpret_cast<double(*)[kBigK][kBigTile]>(big_smem + 2 * kBigK * kBigTile);
-  const int k = S.ncols;
-  const int m = S.nrows;
-  const int64_t F = S.F;
-  const int r0 = t[1] * kBigTile;  // rows of the trailing block
-  const int q0 = t[2] * kBigTile;  // columns of the trailing block
-  double* Fs = V.fronts + S.front_off;
-  const double* d = dvec + S.first_col;
-  const int tid = threadIdx.x;
-  const int tx = tid & 15;
-  const int ty = tid >> 4;
-  // staging: thread tid loads rows 4 (tid & 31) + {0..3} of K columns
-  // 2 (tid >> 5) + {0, 1} of the chunk, for A and for B
-  const int lr = 4 * (tid & 31);
-  const int lk = 2 * (tid >> 5);
-  double ra[2][4];
-  double rb[2][4];
-  auto load = [&](int kk) {
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      const int l = kk + lk + c;
-      const bool kin = l < k;
-      const double dl = kin ? d[l] : 0.0;
-      const double* col = Fs + static_cast<int64_t>(kin ? l : 0) * F + k;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int ra_row = r0 + lr + u;
-        const int rb_row = q0 + lr + u;
-        ra[c][u] = (kin && ra_row < m) ? col[ra_row] * dl : 0.0;
-        rb[c][u] = (kin && rb_row < m) ? col[rb_row] : 0.0;
-      }
-    }
-  };
-  auto stage = [&](int buf) {
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-      *reinterpret_cast<double2*>(&As[buf][lk + c][lr]) = make_double2(ra[c][0], ra[c][1]);
-      *reinterpret_cast<double2*>(&As[buf][lk + c][lr + 2]) = make_double2(ra[c][2], ra[c][3]);
-      *reinterpret_cast<double2*>(&Bs[buf][lk + c][lr]) = make_double2(rb[c][0], rb[c][1]);
-      *reinterpret_cast<double2*>(&Bs[buf][lk + c][lr + 2]) = make_double2(rb[c][2], rb[c][3]);
-    }
-  };
-  double acc[8][8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      acc[i][j] = 0.0;
-    }
-  }
-  load(0);
-  stage(0);
-  __syncthreads();
-  int buf = 0;
-  for (int kk = 0; kk < k; kk += kBigK) {
-    const bool more = kk + kBigK < k;
-    if (more) {
-      load(kk + kBigK);
-    }
-#pragma unroll
-    for (int l = 0; l < kBigK; ++l) {
-      double av[8];
-      double bv[8];
-      const double2 a0 = *reinterpret_cast<const double2*>(&As[buf][l][4 * tx]);
-      const double2 a1 = *reinterpret_cast<const double2*>(&As[buf][l][4 * tx + 2]);
-      const double2 a2 = *reinterpret_cast<const double2*>(&As[buf][l][64 + 4 * tx]);
-      const double2 a3 = *reinterpret_cast<const double2*>(&As[buf][l][64 + 4 * tx + 2]);
-      const double2 b0 = *reinterpret_cast<const double2*>(&Bs[buf][l][4 * ty]);
-      const double2 b1 = *reinterpret_cast<const double2*>(&Bs[buf][l][4 * ty + 2]);
-      const double2 b2 = *reinterpret_cast<const double2*>(&Bs[buf][l][64 + 4 * ty]);
-      const double2 b3 = *reinterpret_cast<const double2*>(&Bs[buf][l][64 + 4 * ty + 2]);
-      av[0] = a0.x; av[1] = a0.y; av[2] = a1.x; av[3] = a1.y;
-      av[4] = a2.x; av[5] = a2.y; av[6] = a3.x; av[7] = a3.y;
-      bv[0] = b0.x; bv[1] = b0.y; bv[2] = b1.x; bv[3] = b1.y;
-      bv[4] = b2.x; bv[5] = b2.y; bv[6] = b3.x; bv[7] = b3.y;
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          acc[i][j] = fma(av[i], bv[j], acc[i][j]);
-        }
-      }
-    }
-    if (more) {
-      stage(buf ^ 1);
-    }
-    __syncthreads();
-    buf ^= 1;
-  }
-  // C -= acc over the lower part; all of a column group's reads are issued
-  // before its writes
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int col = q0 + (j < 4 ? 4 * ty + j : 64 + 4 * ty + j - 4);
-    double cur[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int row = r0 + (i < 4 ? 4 * tx + i : 64 + 4 * tx + i - 4);
-      cur[i] = (row < m && col <= row) ? Fs[(k + col) * F + k + row] : 0.0;
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int row = r0 + (i < 4 ? 4 * tx + i : 64 + 4 * tx + i - 4);
-      if (row < m && col <= row) {
-        Fs[(k + col) * F + k + row] = cur[i] - acc[i][j];
-      }
-    }
-  }
-}
-
 /// Tiled rank-k update C -= L_I D L_J^T (lower part only). panel <= -2: the
 /// outer-block updates (UpdateCodeInner / Outer). panel >= 0:
 /// update of the remaining pivot columns by one panel; panel == -1: Schur
@@ -1105,8 +971,8 @@ __global__ void __launch_bounds__(256, 2) KUpdate(DeviceView V, const int32_t* t
   if (V.active[S.instance] == 0) {
     return;
   }
-  if (t[1] == -1 && S.tc_pack >= 0 && (Fp32Front(V, S) ? V.tc_schur != 0 : true)) {
-    return;  // a wide front: KUpdateBig (FP64) or the tensor-core kernels (FP32)
+  if (t[1] == -1 && S.tc_pack >= 0 && Fp32Front(V, S) && V.tc_schur != 0) {
+    return;  // a wide FP32 front: the tensor-core kernels
   }
   __shared__ double as_buf[kPanel * kTile];
   __shared__ double bs_buf[kPanel * kTile];
@@ -2236,9 +2102,6 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
       CudaCheck(cudaFuncSetAttribute(KPanelBlock, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(PanelBlockSmem())),
                 "block smem attr");
-      CudaCheck(cudaFuncSetAttribute(KUpdateBig, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(kBigSmem)),
-                "big tile smem attr");
       if (dev >= 0 && dev < 64) {
         configured[dev] = true;
       }
@@ -2375,22 +2238,6 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
         ++launches;
       }
     }
-    {
-      // Schur complements of the level's wide FP64 fronts in 128 x 128
-      // tiles (KUpdate skips their 64 x 64 tiles)
-      const TaskRange tr = S.tc_range[static_cast<size_t>(l)];
-      if (tr.count > 0 && P.big_tasks != nullptr) {
-        const TimedLaunch tl(P.timer, KernelTimer::kUpdateSchur, stream, [&] {
-          return level_sum(l, [](const SupernodeRec& r) {
-            const double m = r.nrows;
-            return r.tc_pack >= 0 ? static_cast<double>(r.ncols) * m * (m + 1.0) : 0.0;
-          });
-        });
-        KUpdateBig<<<static_cast<unsigned>(tr.count), kBigThreads, kBigSmem, stream>>>(
-            V, P.big_tasks + 3 * tr.begin, P.dvec);
-        ++launches;
-      }
-    }
     if (P.tc_map != nullptr) {
       // Schur complements of the level's wide FP32 fronts on the tensor
       // cores (KUpdate skips their SIMT tiles)
@@ -2414,10 +2261,12 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
     }
     const TaskRange sr = S.update_range[static_cast<size_t>(S.panel_index_base.back() + l)];
     if (sr.count > 0) {
+      // the wide FP32 fronts of a mixed solve are on the tensor cores
+      const bool tc = P.tc_map != nullptr;
       const TimedLaunch tl(P.timer, KernelTimer::kUpdateSchur, stream, [&] {
-        return level_sum(l, [](const SupernodeRec& r) {
+        return level_sum(l, [tc](const SupernodeRec& r) {
           const double m = r.nrows;
-          return r.tc_pack >= 0 ? 0.0 : static_cast<double>(r.ncols) * m * (m + 1.0);
+          return tc && r.tc_pack >= 0 ? 0.0 : static_cast<double>(r.ncols) * m * (m + 1.0);
         });
       });
       KUpdate<<<static_cast<unsigned>(sr.count), 256, 0, stream>>>(V, P.update_tasks + 4 * sr.begin, P.dvec);

@@ -99,8 +99,6 @@ LdltEngine::LdltEngine(int n, const int32_t* outer, const int32_t* inner, const 
   zpart_off_.Upload(sym_.zpart_off, s);
   ys_.Alloc(static_cast<size_t>(std::max(n, 1)));
   zpart_.Alloc(static_cast<size_t>(std::max<int64_t>(1, sym_.zpart_doubles)));
-  big_tasks_.Upload(sym_.tc_tasks, s);
-  plan_.big_tasks = big_tasks_.get();
   dense_tasks_.Upload(sym_.dense_tasks, s);
   dense_sync_.Alloc(DenseSyncWords(sym_));
   dense_inv_.Alloc(static_cast<size_t>(std::max<int64_t>(1, sym_.dense_inv_doubles)));

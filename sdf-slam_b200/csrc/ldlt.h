@@ -37,7 +37,7 @@ class LdltEngine {
   DevBuf<double> values_, fronts_, upd_, dvec_, rhs_, step_, xs_;
   DevBuf<int32_t> status_, active_;
   DevBuf<uint32_t> solve_sync_;
-  DevBuf<int32_t> solve_tasks_, solve_parts_, big_tasks_, dense_tasks_, dense_sync_;
+  DevBuf<int32_t> solve_tasks_, solve_parts_, dense_tasks_, dense_sync_;
   DevBuf<double> dense_inv_;
   DevBuf<int64_t> zpart_off_;
   DevBuf<double> ys_, zpart_;
