@@ -278,10 +278,18 @@ __device__ void FactorLoaded(const DeviceView& V, const SupernodeRec& S, int k, 
   if (tid == 0 && *zflag != 0) {
     atomicOr(V.status + S.instance, kStatusZeroPivot);
   }
-  if (k + 1 < nt) {
-    // tiles below exist, so this one is full (w == 64): L^-1 =
-    // [M1 0; -M2 L21 M1  M2], column major 64 x 64 into the workspace
+  {
+    // L^-1 = [M1 0; -M2 L21 M1  M2] of the tile (the identity beyond w),
+    // column major 64 x 64 into the workspace: the SOLVE tasks below the
+    // tile and the solve's 64-row panels multiply by it
     double* Mo = A.inv + S.dense_inv + static_cast<int64_t>(k) * kDT * kDT;
+    if (w <= 32) {
+      // a narrow last tile: L11^-1 was not needed above
+      if (tid < 32) {
+        InvertUnitLower32(&T[0][0], M1);
+      }
+      __syncthreads();
+    }
     if (tid < 32) {
       InvertUnitLower32(&T[32][32], M2);
     }

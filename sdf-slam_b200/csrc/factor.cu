@@ -120,6 +120,14 @@ __device__ __forceinline__ void ExtendAddStaged(TP* stage, int c, int rows, cons
 /// the same order as an in-place add without a chain of dependent global
 /// read-modify-writes; without it (a front too wide to stage) the children
 /// are added in place.
+/// A child whose update matrix is left in its own front for the extend-add:
+/// the wide FP32 fronts whose Schur complement the tensor cores compute in
+/// place. Every other front's Schur complement is added into its parent by
+/// the Schur update itself.
+__device__ __forceinline__ bool UpdateLeftInPlace(const DeviceView& V, const SupernodeRec& C) {
+  return C.tc_pack >= 0 && V.tc_schur != 0 && Fp32Front(V, C);
+}
+
 template <typename TP>
 __device__ __forceinline__ void ExtendAddBody(const DeviceView& V, const SupernodeRec& P, const int32_t* t,
                                               const int32_t* ranges, TP* stage) {
@@ -128,6 +136,9 @@ __device__ __forceinline__ void ExtendAddBody(const DeviceView& V, const Superno
   if (stage == nullptr) {
     for (int ci = 0; ci < P.child_count; ++ci) {
       const SupernodeRec C = V.sn[V.child_list[P.child_begin + ci]];
+      if (!UpdateLeftInPlace(V, C)) {
+        continue;
+      }
       const int32_t* rel = V.sn_rel + C.rows_off;
       const int64_t uoff = static_cast<int64_t>(C.ncols) * C.F + C.ncols;
       if (Fp32Front(V, C)) {
@@ -167,6 +178,9 @@ __device__ __forceinline__ void ExtendAddBody(const DeviceView& V, const Superno
   __syncthreads();
   for (int ci = 0; ci < P.child_count; ++ci) {
     const SupernodeRec C = V.sn[V.child_list[P.child_begin + ci]];
+    if (!UpdateLeftInPlace(V, C)) {
+      continue;
+    }
     const int32_t* rel = V.sn_rel + C.rows_off;
     const int64_t uoff = static_cast<int64_t>(C.ncols) * C.F + C.ncols;
     if (Fp32Front(V, C)) {
@@ -821,6 +835,45 @@ __global__ void __launch_bounds__(256) KFactorFront(DeviceView V, const int32_t*
   }
 }
 
+/// Adds one 64 x 64 tile of a front's Schur complement (cur - acc over the
+/// front's trailing rows r and columns c, r >= c; rows and columns counted
+/// from the front's first row, k pivots) into the parent front at the rows
+/// rel[r - k], rel[c - k]. All sixteen parent reads first, then the writes.
+template <typename TP, typename T>
+__device__ __forceinline__ void ScatterSchur(TP* Fp, int64_t PF, const int32_t* rel, int k, int F, int r0, int cc0,
+                                             const T (&cur)[4][4], const T (&acc)[4][4]) {
+  const int tx = threadIdx.x % 16;
+  const int ty = threadIdx.x / 16;
+  int64_t pos[4][4];
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int c = cc0 + ty + 16 * b;
+    const int64_t pc = c < F ? static_cast<int64_t>(rel[c - k]) * PF : -1;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int r = r0 + tx + 16 * a;
+      pos[a][b] = (pc >= 0 && r < F && r >= c) ? pc + rel[r - k] : -1;
+    }
+  }
+  TP old[4][4];
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      old[a][b] = pos[a][b] >= 0 ? Fp[pos[a][b]] : TP(0);
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      if (pos[a][b] >= 0) {
+        Fp[pos[a][b]] = old[a][b] + static_cast<TP>(static_cast<T>(cur[a][b] - acc[a][b]));
+      }
+    }
+  }
+}
+
 template <typename T>
 __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeRec& S, int panel, int ti, int tj,
                                            const double* dvec, T (*As)[kTile], T (*Bs)[kTile]) {
@@ -944,6 +997,18 @@ __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeR
       }
     }
     __syncthreads();
+  }
+  if (panel == -1 && S.parent >= 0) {
+    // the Schur complement goes straight into the parent's front (what the
+    // extend-add did with the update matrix), T-rounded as it was stored
+    const SupernodeRec P = V.sn[S.parent];
+    const int32_t* rel = V.sn_rel + S.rows_off;
+    if (Fp32Front(V, P)) {
+      ScatterSchur<float, T>(WorkFront<float>(V, P), P.F, rel, S.ncols, F, r0, cc0, cur, acc);
+    } else {
+      ScatterSchur<double, T>(WorkFront<double>(V, P), P.F, rel, S.ncols, F, r0, cc0, cur, acc);
+    }
+    return;
   }
 #pragma unroll
   for (int b = 0; b < 4; ++b) {
@@ -1676,6 +1741,7 @@ struct SolveArgs {
   double* zpart;          // backward partial products of wide fronts
   const double* dvec;
   const double* inv;
+  const double* dense_inv;  // tile inverses of the tiled dense roots (64-row panels)
   uint32_t* sync;         // counter, then fdone, bdone, ydone, zdone per sn, then two flags per diagonal block
   int num_sn;
   int num_inv;
@@ -1697,6 +1763,131 @@ __device__ __forceinline__ bool BlockWait(const DeviceView& V, const SupernodeRe
   }
   __syncthreads();
   return ok != 0;
+}
+
+/// Forward panel q of a tiled dense root (64-row panels, FP64): v_q -=
+/// L(q, p) y_p for every earlier panel p as its flag arrives (four threads
+/// per row, sixteen columns each, summed in a fixed order), then y_q = M_q
+/// v_q with M_q the tile inverse the factorization stored, D^-1 y_q into xs.
+__device__ __forceinline__ void RootForwardPanel64(const DeviceView& V, const SupernodeRec& S, const SolveArgs& A,
+                                                   int q, uint32_t* pflag, double* buf) {
+  constexpr int kW = kDenseTileCols;
+  const int k = S.ncols;
+  const int64_t F64 = S.F;
+  const double* Fs = V.fronts + S.front_off;
+  const int p0 = q * kW;
+  const int w = min(kW, k - p0);
+  const int tid = threadIdx.x;
+  double* vq = buf;           // kW
+  double* yp = buf + kW;      // kW
+  double* part = buf + 2 * kW;  // 4 x kW
+  const int i = tid & (kW - 1);
+  const int g = tid >> 6;  // four groups of sixteen columns
+  if (tid < kW) {
+    vq[tid] = tid < w ? A.ys[S.first_col + p0 + tid] : 0.0;
+  }
+  for (int p = 0; p < q; ++p) {
+    double l[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      l[c] = i < w ? Fs[static_cast<int64_t>(p * kW + 16 * g + c) * F64 + p0 + i] : 0.0;
+    }
+    BlockWait(V, S, pflag + S.panel_base + p, 1u, A.wait_limit);
+    if (tid < kW) {
+      yp[tid] = __ldcg(A.ys + S.first_col + p * kW + tid);
+    }
+    __syncthreads();
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      acc = fma(l[c], yp[16 * g + c], acc);
+    }
+    part[g * kW + i] = acc;
+    __syncthreads();
+    if (tid < kW) {
+      vq[i] -= (part[i] + part[kW + i]) + (part[2 * kW + i] + part[3 * kW + i]);
+    }
+  }
+  __syncthreads();
+  // y = M v: thread (row i, group g) sums sixteen columns of M
+  const double* M = A.dense_inv + S.dense_inv + static_cast<int64_t>(q) * kW * kW;
+  double acc = 0.0;
+#pragma unroll
+  for (int c = 0; c < 16; ++c) {
+    const int j = 16 * g + c;
+    acc = fma(M[static_cast<int64_t>(j) * kW + i], vq[j], acc);
+  }
+  part[g * kW + i] = acc;
+  __syncthreads();
+  if (tid < w) {
+    const double y = (part[i] + part[kW + i]) + (part[2 * kW + i] + part[3 * kW + i]);
+    A.ys[S.first_col + p0 + tid] = y;
+    V.xs[S.first_col + p0 + tid] = (1.0 / A.dvec[S.first_col + p0 + tid]) * y;
+  }
+}
+
+/// Backward panel q of a tiled dense root: z_q = (D^-1 y)_q minus
+/// L(p, q)^T x_p for every later panel p as its flag arrives, then x_q =
+/// M_q^T z_q into xs and the step.
+__device__ __forceinline__ void RootBackwardPanel64(const DeviceView& V, const SupernodeRec& S, const SolveArgs& A,
+                                                    int q, uint32_t* bflag, double* buf) {
+  constexpr int kW = kDenseTileCols;
+  const int k = S.ncols;
+  const int64_t F64 = S.F;
+  const double* Fs = V.fronts + S.front_off;
+  const int np = (k + kW - 1) / kW;
+  const int p0 = q * kW;
+  const int w = min(kW, k - p0);
+  const int tid = threadIdx.x;
+  double* zq = buf;
+  double* xp = buf + kW;
+  double* part = buf + 2 * kW;
+  // thread (row i of z, group g of sixteen rows of panel p)
+  const int i = tid >> 2;
+  const int g = tid & 3;
+  if (tid < kW) {
+    zq[tid] = tid < w ? __ldcg(V.xs + S.first_col + p0 + tid) : 0.0;
+  }
+  for (int p = np - 1; p > q; --p) {
+    const int wp = min(kW, k - p * kW);
+    double l[16];
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      const int r = 16 * g + c;
+      l[c] = (i < w && r < wp) ? Fs[static_cast<int64_t>(p0 + i) * F64 + p * kW + r] : 0.0;
+    }
+    BlockWait(V, S, bflag + S.panel_base + p, 1u, A.wait_limit);
+    if (tid < kW) {
+      xp[tid] = tid < wp ? __ldcg(V.xs + S.first_col + p * kW + tid) : 0.0;
+    }
+    __syncthreads();
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      acc = fma(l[c], xp[16 * g + c], acc);
+    }
+    part[g * kW + i] = acc;
+    __syncthreads();
+    if (tid < kW) {
+      zq[tid] -= (part[tid] + part[kW + tid]) + (part[2 * kW + tid] + part[3 * kW + tid]);
+    }
+  }
+  __syncthreads();
+  // x = M^T z: thread (row i, group g) sums sixteen entries of column i of M
+  const double* M = A.dense_inv + S.dense_inv + static_cast<int64_t>(q) * kW * kW;
+  double acc = 0.0;
+#pragma unroll
+  for (int c = 0; c < 16; ++c) {
+    const int j = 16 * g + c;
+    acc = fma(M[static_cast<int64_t>(i) * kW + j], zq[j], acc);
+  }
+  part[g * kW + i] = acc;
+  __syncthreads();
+  if (tid < w) {
+    const double x = (part[tid] + part[kW + tid]) + (part[2 * kW + tid] + part[3 * kW + tid]);
+    V.xs[S.first_col + p0 + tid] = x;
+    V.step[V.perm[S.first_col + p0 + tid]] = x;
+  }
 }
 
 /// Right-hand side of a panel-split root: v = rhs plus the children's
@@ -1966,14 +2157,18 @@ __global__ void __launch_bounds__(256, 1) KSolveTree(DeviceView V, SolveArgs A) 
           RootGather(V, S, A.ys, buf);
           break;
         case kTaskRootForward:
-          if (f32) {
+          if (S.dense_cnt >= 0) {
+            RootForwardPanel64(V, S, A, part, pflag, buf);
+          } else if (f32) {
             RootForwardPanel<float>(V, S, A, part, pflag, buf);
           } else {
             RootForwardPanel<double>(V, S, A, part, pflag, buf);
           }
           break;
         case kTaskRootBackward:
-          if (f32) {
+          if (S.dense_cnt >= 0) {
+            RootBackwardPanel64(V, S, A, part, bflag, buf);
+          } else if (f32) {
             RootBackwardPanel<float>(V, S, A, part, bflag, buf);
           } else {
             RootBackwardPanel<double>(V, S, A, part, bflag, buf);
@@ -2126,8 +2321,9 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
     CudaCheck(cudaMemsetAsync(P.dense_sync, 0, DenseSyncWords(S) * sizeof(int32_t), stream), "dense sync reset");
   }
   for (int l = 0; l < S.num_levels; ++l) {
+    // the extend-add only for update matrices the tensor cores left in place
     const TaskRange ea = S.ea_range[static_cast<size_t>(l)];
-    if (ea.count > 0) {
+    if (ea.count > 0 && P.tc_map != nullptr) {
       // staged in shared memory unless a front of the level is too wide
       const size_t stage = static_cast<size_t>(S.ea_stage[static_cast<size_t>(l)]) * sizeof(double);
       const bool staged = stage <= static_cast<size_t>(kEaStageDoubles) * sizeof(double);
@@ -2259,15 +2455,20 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
       launches += LaunchSchurTc(*P.tc_map, P.tc, P.pack_tasks + 3 * pk.begin, pk.count, P.tc_tasks + 3 * tr.begin,
                                 tr.count, stream, P.timer, pack_bytes, tc_flops);
     }
-    const TaskRange sr = S.update_range[static_cast<size_t>(S.panel_index_base.back() + l)];
-    if (sr.count > 0) {
-      // the wide FP32 fronts of a mixed solve are on the tensor cores
+    for (int q = S.schur_base[static_cast<size_t>(l)]; q < S.schur_base[static_cast<size_t>(l) + 1]; ++q) {
+      const TaskRange sr = S.schur_range[static_cast<size_t>(q)];
+      if (sr.count == 0) {
+        continue;
+      }
+      // the wide FP32 fronts of a mixed solve are on the tensor cores; the
+      // level's work is counted with its first sibling slot
       const bool tc = P.tc_map != nullptr;
+      const bool first = q == S.schur_base[static_cast<size_t>(l)];
       const TimedLaunch tl(P.timer, KernelTimer::kUpdateSchur, stream, [&] {
-        return level_sum(l, [tc](const SupernodeRec& r) {
+        return first ? level_sum(l, [tc](const SupernodeRec& r) {
           const double m = r.nrows;
           return tc && r.tc_pack >= 0 ? 0.0 : static_cast<double>(r.ncols) * m * (m + 1.0);
-        });
+        }) : 0.0;
       });
       KUpdate<<<static_cast<unsigned>(sr.count), 256, 0, stream>>>(V, P.update_tasks + 4 * sr.begin, P.dvec);
       ++launches;
@@ -2327,6 +2528,7 @@ int LaunchSolveLevels(const Symbolic& S, const DeviceView& V, const FactorPlan& 
     A.zpart = P.zpart;
     A.dvec = P.dvec;
     A.inv = P.inv;
+    A.dense_inv = P.dense_inv;
     A.sync = P.solve_sync;
     A.num_sn = num_sn;
     A.num_inv = P.num_inv;

@@ -247,6 +247,11 @@ struct Symbolic {
   std::vector<int32_t> update_tasks;         // (sn, panel, ti, tj) quads
   std::vector<TaskRange> update_range;       // per (level, panel) flattened
   std::vector<int32_t> panel_index_base;     // level -> first (level,panel) slot
+  // Schur complement tasks (update tasks with panel -1), per (level, sibling
+  // slot): schur_range[schur_base[l] + slot]; a task adds its tile of the
+  // front's Schur complement into the parent front
+  std::vector<TaskRange> schur_range;
+  std::vector<int32_t> schur_base;           // levels + 1 entries
   // Tensor-core Schur complements of a mixed solve's FP32 fronts with at
   // least kTcMinRows rows below the pivot block (their SIMT Schur tasks are
   // skipped then): per level, operand packing tasks (sn, row tile, K chunk)

@@ -434,10 +434,24 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   S.update_range.assign(static_cast<size_t>(slots), {});
   S.ea_range.assign(static_cast<size_t>(levels), {});
   S.ea_stage.assign(static_cast<size_t>(levels), 0);
-  // Schur complement tasks (rank-k update of the trailing block) are stored
-  // as update tasks with panel = -1 after the per-panel ones of each level;
-  // update_range has one extra slot per level for them.
-  std::vector<TaskRange> schur_range(static_cast<size_t>(levels));
+  // sibling slots (see the Schur tasks below)
+  std::vector<int32_t> sibling_slot(static_cast<size_t>(Sn), 0);
+  {
+    std::vector<int32_t> per_level(static_cast<size_t>(levels), 0);
+    for (int p = 0; p < Sn; ++p) {
+      const SupernodeRec& r = S.sn[static_cast<size_t>(p)];
+      for (int ci = 0; ci < r.child_count; ++ci) {
+        const int c = S.child_list[static_cast<size_t>(r.child_begin + ci)];
+        sibling_slot[static_cast<size_t>(c)] = per_level[static_cast<size_t>(height[static_cast<size_t>(c)])]++;
+      }
+      for (int ci = 0; ci < r.child_count; ++ci) {
+        const int c = S.child_list[static_cast<size_t>(r.child_begin + ci)];
+        per_level[static_cast<size_t>(height[static_cast<size_t>(c)])] = 0;
+      }
+    }
+  }
+  S.schur_range.clear();
+  S.schur_base.assign(static_cast<size_t>(levels) + 1, 0);
   for (int l = 0; l < levels; ++l) {
     const int qb = S.level_begin[static_cast<size_t>(l)];
     const int qe = S.level_begin[static_cast<size_t>(l) + 1];
@@ -566,26 +580,41 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
       S.panel_range[slot].count = static_cast<int64_t>(S.panel_tasks.size() / 3) - S.panel_range[slot].begin;
       S.update_range[slot].count = static_cast<int64_t>(S.update_tasks.size() / 4) - S.update_range[slot].begin;
     }
-    schur_range[static_cast<size_t>(l)].begin = static_cast<int64_t>(S.update_tasks.size() / 4);
-    for (int q = qb; q < qe; ++q) {
-      const int s = S.level_sn[static_cast<size_t>(q)];
-      const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
-      const int m = r.nrows;
-      for (int tj = 0; tj * T < m; ++tj) {
-        for (int ti = tj; ti * T < m; ++ti) {
-          S.update_tasks.push_back(s);
-          S.update_tasks.push_back(-1);
-          S.update_tasks.push_back(ti);
-          S.update_tasks.push_back(tj);
+    // Schur complements, added straight into the parents' fronts: fronts of
+    // the level that share a parent go in separate launches, one per sibling
+    // slot (the front's rank among its parent's children of this level, in
+    // child-list order), so no two blocks of a launch add into one entry
+    // and each parent entry takes its children's terms in a fixed order
+    S.schur_base[static_cast<size_t>(l)] = static_cast<int32_t>(S.schur_range.size());
+    for (int slot = 0;; ++slot) {
+      TaskRange range;
+      range.begin = static_cast<int64_t>(S.update_tasks.size() / 4);
+      bool any = false;
+      for (int q = qb; q < qe; ++q) {
+        const int s = S.level_sn[static_cast<size_t>(q)];
+        if (sibling_slot[static_cast<size_t>(s)] != slot) {
+          continue;
+        }
+        any = true;
+        const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
+        const int m = r.nrows;
+        for (int tj = 0; tj * T < m; ++tj) {
+          for (int ti = tj; ti * T < m; ++ti) {
+            S.update_tasks.push_back(s);
+            S.update_tasks.push_back(-1);
+            S.update_tasks.push_back(ti);
+            S.update_tasks.push_back(tj);
+          }
         }
       }
+      if (!any) {
+        break;
+      }
+      range.count = static_cast<int64_t>(S.update_tasks.size() / 4) - range.begin;
+      S.schur_range.push_back(range);
     }
-    schur_range[static_cast<size_t>(l)].count =
-        static_cast<int64_t>(S.update_tasks.size() / 4) - schur_range[static_cast<size_t>(l)].begin;
   }
-  for (int l = 0; l < levels; ++l) {
-    S.update_range.push_back(schur_range[static_cast<size_t>(l)]);
-  }
+  S.schur_base[static_cast<size_t>(levels)] = static_cast<int32_t>(S.schur_range.size());
   // one-launch solve tasks
   S.solve_tasks.clear();
   S.solve_parts.assign(2 * static_cast<size_t>(Sn), 1);
@@ -603,7 +632,9 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
     const int s = S.level_sn[static_cast<size_t>(q)];
     const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
     if (root_split(r)) {
-      const int np = (r.ncols + B - 1) / B;
+      // a tiled dense root solves by 64-row panels with its tile inverses
+      const int pw = tiled(r) ? kDenseTileCols : B;
+      const int np = (r.ncols + pw - 1) / pw;
       push_task(kTaskRootGather, s, 0);
       for (int p = 0; p < np; ++p) {
         push_task(kTaskRootForward, s, p);
@@ -627,7 +658,8 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
     const int s = S.level_sn[static_cast<size_t>(q)];
     const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
     if (root_split(r)) {
-      for (int p = (r.ncols + B - 1) / B - 1; p >= 0; --p) {
+      const int pw = tiled(r) ? kDenseTileCols : B;
+      for (int p = (r.ncols + pw - 1) / pw - 1; p >= 0; --p) {
         push_task(kTaskRootBackward, s, p);
       }
     } else if (r.nrows >= kSolveWideRows) {
