@@ -732,6 +732,25 @@ __global__ void __launch_bounds__(256) KPoseFrames(DeviceView V) {
 /// Turns the accumulated J^T r into -J^T r and applies the damping of
 /// lm_solver.cpp:321-330 to every diagonal entry (lambda, or lambda times
 /// max(diag, 1e-12) under Marquardt scaling).
+/// Zeroes the lower triangle of the assembly fronts before the row kernels
+/// add into them: one warp per column c, rows c..F-1 (coalesced); task (sn,
+/// first of kZeroCols columns). The upper triangles are never read before
+/// the factorization writes them, so they are left as they are (half the
+/// bytes of clearing the whole buffer).
+__global__ void KZeroFronts(DeviceView V, const int32_t* tasks) {
+  const int32_t* t = tasks + 2 * static_cast<int64_t>(blockIdx.x);
+  const SupernodeRec S = V.sn[t[0]];
+  const int c = t[1] + static_cast<int>(threadIdx.x >> 5);
+  const int lane = static_cast<int>(threadIdx.x & 31);
+  if (c >= S.F) {
+    return;
+  }
+  double* col = V.asm_fronts + S.front_off + static_cast<int64_t>(c) * S.F;
+  for (int r = c + lane; r < S.F; r += 32) {
+    col[r] = 0.0;
+  }
+}
+
 __global__ void KFinalizeNormal(DeviceView V) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= V.n) {

@@ -21,6 +21,7 @@ __global__ void KCellStart(const int32_t* keys, int64_t n, int64_t num_cells, in
 __global__ void KCellPass(DeviceView V, const int64_t* cells, int64_t count);
 __global__ void KPoseFrames(DeviceView V);
 __global__ void KFinalizeNormal(DeviceView V);
+__global__ void KZeroFronts(DeviceView V, const int32_t* tasks);
 __global__ void KPosePairs(DeviceView V);
 __global__ void KBackup(DeviceView V, int dir, const int32_t* revert_mask);
 __global__ void KApplyStep(DeviceView V);
@@ -826,8 +827,12 @@ void Engine::LaunchRows() {
 }
 
 void Engine::LaunchNormal() {
-  CudaCheck(cudaMemsetAsync(V_.asm_fronts, 0, static_cast<size_t>(sym_.front_doubles) * sizeof(double), stream_),
-            "front memset");
+  if (!sym_.zero_tasks.empty()) {
+    KZeroFronts<<<static_cast<unsigned>(sym_.zero_tasks.size() / 2), 32 * kZeroCols, 0, stream_>>>(
+        V_, zero_tasks_.get());
+    CudaCheck(cudaGetLastError(), "front zeroing");
+    ++times_.launches;
+  }
   CudaCheck(cudaMemsetAsync(rhs_.get(), 0, static_cast<size_t>(n_) * sizeof(double), stream_), "rhs memset");
   if (total_cells_ > 0) {
     // as many blocks as are resident at once
@@ -1038,6 +1043,7 @@ void Engine::SetSolveFault(int withhold, uint32_t wait_polls) {
 }
 
 void Engine::UploadSolveTasks(cudaStream_t s) {
+  zero_tasks_.Upload(sym_.zero_tasks, s);
   dense_tasks_.Upload(sym_.dense_tasks, s);
   dense_sync_.Alloc(DenseSyncWords(sym_));
   dense_inv_.Alloc(static_cast<size_t>(std::max<int64_t>(1, sym_.dense_inv_doubles)));

@@ -439,6 +439,7 @@ class Engine {
   DevBuf<int32_t> ea_tasks_, ea_child_, panel_tasks_, update_tasks_, small_tasks_;
   DevBuf<double> fronts_, upd_;
   DevBuf<int32_t> dense_tasks_, dense_sync_;  // tiled dense roots
+  DevBuf<int32_t> zero_tasks_;                // lower-triangle clearing of the fronts
   DevBuf<double> dense_inv_;
   DevBuf<uint32_t> solve_sync_;  // counter and flags of the one-launch solve
   DevBuf<int32_t> solve_tasks_, solve_parts_;

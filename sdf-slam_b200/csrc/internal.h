@@ -183,6 +183,8 @@ enum SolveTask : int32_t {
 constexpr int kOuterPanels = 4;
 constexpr int32_t UpdateCodeInner(int panel) { return -2 - 2 * panel; }
 constexpr int32_t UpdateCodeOuter(int block) { return -3 - 2 * block; }
+/// Columns per task of the front clearing (one warp each).
+constexpr int kZeroCols = 8;
 /// Tile edge of the tiled dense-root factorization.
 constexpr int kDenseTileCols = 64;
 /// One task of the tiled factorization of a dense root: FACTOR (i == j ==
@@ -283,6 +285,9 @@ struct Symbolic {
   // i, UPDATE k < j <= i) in descending bottom level, dense_range per level,
   // the tile counters (nt x nt per front) and the diagonal-tile inverses
   // (64 x 64 doubles per tile) they use.
+  // (sn, first column) pairs of kZeroCols columns: the fronts' lower
+  // triangles cleared before every assembly
+  std::vector<int32_t> zero_tasks;
   std::vector<int32_t> dense_tasks;
   std::vector<TaskRange> dense_range;
   int64_t dense_cnt_words{0};

@@ -718,6 +718,14 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
         static_cast<int64_t>(S.tc_tasks.size() / 3) - S.tc_range[static_cast<size_t>(l)].begin;
     S.tc_pack_rows = std::max(S.tc_pack_rows, rows);
   }
+  // front clearing tasks
+  S.zero_tasks.clear();
+  for (int s = 0; s < Sn; ++s) {
+    for (int c = 0; c < S.sn[static_cast<size_t>(s)].F; c += kZeroCols) {
+      S.zero_tasks.push_back(s);
+      S.zero_tasks.push_back(c);
+    }
+  }
   // tiled dense roots: counters, inverse workspace and task lists per level
   S.dense_tasks.clear();
   S.dense_range.assign(static_cast<size_t>(levels), {});
