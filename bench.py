@@ -322,19 +322,38 @@ def run_profile(args):
     return 0
 
 
-def _timed_solves(P, prob, opts1, steps, flusher):
+def _timed_solves(P, prob, opts1, steps, flusher, spans=None):
+    """One-iteration solves, L2 flushed before each; device span of each
+    (the library's events), launches and phase times summed. `spans`
+    (a dict, optional) receives every step's span and the pattern
+    re-analyses that ran inside the timed steps."""
     import numpy as np
     device = 0.0
     launches = 0
     phases = np.zeros(5)
+    each = []
+    reanalyses = 0
     for _ in range(steps):
         flusher.flush()
         P.solve(prob, opts1)
         prof = prob.last_profile()
         device += prof["span"]
+        each.append(prof["span"])
+        reanalyses += int(prof["reanalyses"])
         launches += prof["launches"]
         phases += [prof["assemble"], prof["normal"], prof["factor"], prof["solve"], prof["update"]]
+    if spans is not None:
+        spans["spans"] = each
+        spans["reanalyses"] = reanalyses
     return device, launches, phases
+
+
+def _span_summary(spans):
+    """Median step and the timed steps' pattern re-analyses: a step whose
+    state left the analysed pattern pays a host re-analysis inside it."""
+    import numpy as np
+    return {"median_ms_per_step": 1000.0 * float(np.median(spans["spans"])),
+            "reanalyses_in_timed_steps": spans["reanalyses"]}
 
 
 PHASES = ["assemble", "normal", "factor", "solve", "update"]
@@ -365,21 +384,29 @@ def run_oracle_comparison(P, args, specs):
     return out, cpu
 
 
-def run_mixed(P, args, specs, flusher):
+def run_mixed(P, args, specs, flusher, state0):
     """The same workload with precision "mixed": LM iterations/s
-    (one-iteration solves, L2 flushed between them)."""
+    (one-iteration solves, L2 flushed between them), timed from `state0`,
+    the state the plain FP64 timed steps started from (so that both meet
+    the same pattern re-analyses)."""
     prob = P.Problem.from_specs(specs)
     opts1 = P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision="mixed",
                             refine_steps=args.refine_steps)
+    prob.set_state(*state0)
     for _ in range(args.warmup):
         P.solve(prob, opts1)
     if not args.no_autotune:
         prob.autotune()
-    steps = max(3, args.steps // 2)
-    device, launches, phases = _timed_solves(P, prob, opts1, steps, flusher)
+    prob.set_state(*state0)
+    P.solve(prob, opts1)
+    prob.set_state(*state0)
+    steps = args.steps
+    spans = {}
+    device, launches, phases = _timed_solves(P, prob, opts1, steps, flusher, spans)
     kernels = kernel_profile(P, prob, opts1, flusher)
     prob.close()
     out = {"value": steps / device, "unit": "LM iters/s", "refine_steps": args.refine_steps, "steps": steps,
+           **_span_summary(spans),
            "phase_ms_per_step": {k: 1000.0 * v / steps for k, v in zip(PHASES, phases)}, "kernels": kernels}
     tc = kernels.get("KSchurTc")
     if tc:
@@ -426,11 +453,14 @@ def run_batch(P, args, flusher):
         if not args.no_autotune:
             out.setdefault("schedule", {})[precision] = batch.autotune()["schedule"]
         device = 0.0
+        reanalyses = 0
         for _ in range(steps):
             flusher.flush()
             P.solve(batch, opts1)
             device += batch.last_profile()["span"]
-        out[precision] = {"value": count * steps / device, "ms_per_batched_iteration": 1000.0 * device / steps}
+            reanalyses += int(batch.last_profile()["reanalyses"])
+        out[precision] = {"value": count * steps / device, "ms_per_batched_iteration": 1000.0 * device / steps,
+                          "reanalyses_in_timed_steps": reanalyses}
         batch.close()
     # final cost after `iters` iterations from the scenes' start, against the
     # oracle's, on every `stride`-th instance
@@ -471,17 +501,22 @@ def run_batch_office(P, args, flusher, plain_value):
         batch = P.Problem.batch(specs)
         opts1 = [P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=precision,
                                  refine_steps=args.refine_steps)] * count
-        for _ in range(2):
+        # past the first iterations, whose large pose moves re-analyse the
+        # patterns of most instances (the single office is timed as far in)
+        for _ in range(args.office_batch_warmup):
             P.solve(batch, opts1)
         device = 0.0
         phases = np.zeros(5)
+        reanalyses = 0
         for _ in range(steps):
             flusher.flush()
             P.solve(batch, opts1)
             prof = batch.last_profile()
             device += prof["span"]
+            reanalyses += int(prof["reanalyses"])
             phases += [prof["assemble"], prof["normal"], prof["factor"], prof["solve"], prof["update"]]
         out[precision] = {"value": count * steps / device, "ms_per_batched_iteration": 1000.0 * device / steps,
+                          "reanalyses_in_timed_steps": reanalyses, "warmup_iterations": args.office_batch_warmup,
                           "phase_ms": {k: 1000.0 * v / steps for k, v in zip(PHASES, phases)},
                           "over_single_plain": count * steps / device / plain_value}
         batch.close()
@@ -595,7 +630,16 @@ def _serve_pass(P, args, seed0, rate, check_oracle=False):
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of a
 # kernel class on a workload, from the committed one-kernel ncu captures
 # named beside each entry (L2 flushed before the captured step, as here).
-KERNEL_TRAFFIC_BYTES = {}
+# DRAM bytes (read + written) per launch of a kernel class, averaged over its
+# launches in one iteration of the workload, from the one-pass ncu launch
+# list (gpu__time_duration, dram__bytes_read / _write) summarised in
+# profiles/launch_list_office.md
+KERNEL_TRAFFIC_BYTES = {
+    ("office", "KUpdate(schur)"): 3054.4e6 / 20,   # the 20 Schur launches of the iteration
+    ("office", "KDenseRoot"): 33.4e6,
+    ("office", "KSolveTree"): 275.2e6,
+    ("office", "KFactorFront"): 137.0e6 / 10,
+}
 
 
 def kernel_profile(P, prob, opts1, flusher, iterations=3):
@@ -650,7 +694,9 @@ def run_gpu(args, dist, world, rank, local):
     if sampler:
         sampler.mark()
     wall0 = time.perf_counter()
-    device_s, launches, phases = _timed_solves(P, prob, opts1, args.steps, flusher)
+    state0 = prob.state()
+    spans = {}
+    device_s, launches, phases = _timed_solves(P, prob, opts1, args.steps, flusher, spans)
     flusher.sync()
     _barrier(dist)
     wall = time.perf_counter() - wall0
@@ -687,7 +733,7 @@ def run_gpu(args, dist, world, rank, local):
     e2e_t = _reduce(dist, e2e_t, "MAX")
     e2e_value = world * args.e2e_steps * e2e_iters / e2e_t if e2e_t > 0 else 0.0
     single = world == 1
-    mixed = run_mixed(P, args, specs, flusher) if (single and not args.no_mixed) else None
+    mixed = run_mixed(P, args, specs, flusher, state0) if (single and not args.no_mixed) else None
     batched = run_batch(P, args, flusher) if (args.batch_count > 0 and single) else None
     plain_value = total_steps / device_max
     batched_office = (run_batch_office(P, args, flusher, plain_value)
@@ -731,6 +777,7 @@ def run_gpu(args, dist, world, rank, local):
     roofline = {
         "bound": bound, "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak,
         "traffic": KERNEL_TRAFFIC_BYTES.get((args.workload, dominant_kernel)),
+        "traffic_source": "ncu one-pass launch list, DRAM bytes per launch (profiles/launch_list_office.md)",
         "kernel": dominant_kernel, "peak_source": src, "launches_timed": dom["launches"],
         "avg_launch_ms": avg_ms, "work_per_launch": work_per_launch, "work_unit": dom["work_unit"]}
     roofline_factor = {
@@ -752,6 +799,7 @@ def run_gpu(args, dist, world, rank, local):
                    "unknowns": z["num_parameters"], "point_rows": z["num_points"],
                    "l2": "flushed between steps (2x126 MB write)", "parallelism": f"replicas x{world}"},
         "wall_ms_per_step": 1000.0 * wall_max / args.steps,
+        **_span_summary(spans),
         "phase_ms_per_step": {k: 1000.0 * v for k, v in zip(PHASES, per_step)},
         "factor_gflop_per_step": flops / 1e9,
         "gpu_launches": int(launches),
@@ -799,6 +847,7 @@ def main():
     ap.add_argument("--refine-steps", type=int, default=3)
     ap.add_argument("--batch-count", type=int, default=64)
     ap.add_argument("--office-batch", type=int, default=8)
+    ap.add_argument("--office-batch-warmup", type=int, default=8)
     ap.add_argument("--serve-requests", type=int, default=32)
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[50.0, 100.0, 200.0, 500.0])
     ap.add_argument("--serve-iterations", type=int, default=20)
