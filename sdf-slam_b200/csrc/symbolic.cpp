@@ -22,6 +22,7 @@
 // that structure. Any contiguous partition gives a valid assembly tree this
 // way.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <functional>
 #include <numeric>
@@ -1139,8 +1140,9 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
   for (int c = 0; c < A; ++c) {
     nf_ptr[static_cast<size_t>(c) + 1] += nf_ptr[static_cast<size_t>(c)];
   }
-  // rank[e]: position of node-major entry e within its frame's list
-  std::vector<int32_t> rank(static_cast<size_t>(entries));
+  // emap[j]: the node-major entry of frame-major entry j (each thread writes
+  // contiguous runs of every frame's list, not one entry per frame per node)
+  std::vector<int64_t> emap(static_cast<size_t>(entries));
   ParallelRanges(csr_threads, A, 256, [&](int64_t c0, int64_t c1) {
     std::vector<int64_t> fill(nf_ptr.begin() + c0, nf_ptr.begin() + c1);
     for (int f = 1; f < Fr; ++f) {
@@ -1149,7 +1151,7 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
       for (auto it = lo; it != hi; ++it) {
         const int64_t e = fill[static_cast<size_t>(*it - c0)]++;
         nf[static_cast<size_t>(e)] = f;
-        rank[static_cast<size_t>(e)] = static_cast<int32_t>(it - begin);
+        emap[static_cast<size_t>(S.fmp_ptr[static_cast<size_t>(f)] + (it - begin))] = e;
       }
     }
   });
@@ -1222,15 +1224,31 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
   S.mp_off.resize(static_cast<size_t>(entries));
   S.fmp_off.resize(static_cast<size_t>(entries));
   const int Sn = static_cast<int>(S.sn.size());
-  const int offset_parts = std::min(Sn, 4 * threads);
-  PoolRun(threads > 1 ? offset_parts : std::min(Sn, 1), [&](int part) {
-    const int parts = threads > 1 ? offset_parts : 1;
+  // tasks of at most kOffsetCols pivot columns of one supernode, taken from
+  // a shared counter (wide separators hold most of the coupled entries)
+  constexpr int kOffsetCols = 16;
+  std::vector<std::pair<int32_t, int32_t>> offset_tasks;
+  for (int s = 0; s < Sn; ++s) {
+    const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
+    if (r.first_col >= col_off + A) {
+      continue;  // the pose root holds no node columns
+    }
+    for (int j = 0; j < r.ncols; j += kOffsetCols) {
+      offset_tasks.emplace_back(s, j);
+    }
+  }
+  std::atomic<int64_t> next_offset_task{0};
+  const int offset_parts = threads > 1 ? std::min<int>(static_cast<int>(offset_tasks.size()), threads) : 1;
+  PoolRun(std::max(1, offset_parts), [&](int) {
     ColumnMap& pos = ThreadColumnMap();
-    for (int s = part; s < Sn; s += parts) {
-      const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
-      if (r.first_col >= col_off + A) {
-        continue;  // the pose root holds no node columns
+    for (;;) {
+      const int64_t task = next_offset_task.fetch_add(1);
+      if (task >= static_cast<int64_t>(offset_tasks.size())) {
+        break;
       }
+      const int s = offset_tasks[static_cast<size_t>(task)].first;
+      const int j0 = offset_tasks[static_cast<size_t>(task)].second;
+      const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
       const int32_t* rows = S.sn_rows.data() + r.rows_off;
       pos.Begin(static_cast<size_t>(col_off + n));
       for (int j = 0; j < r.ncols; ++j) {
@@ -1239,7 +1257,8 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
       for (int q = 0; q < r.nrows; ++q) {
         pos.Set(rows[q], r.ncols + q);
       }
-      for (int pc = r.first_col - col_off; pc < r.first_col - col_off + r.ncols; ++pc) {
+      const int pc_end = r.first_col - col_off + std::min(r.ncols, j0 + kOffsetCols);
+      for (int pc = r.first_col - col_off + j0; pc < pc_end; ++pc) {
         const int c = lperm[static_cast<size_t>(pc)];
         const int node = hp.active_to_node[static_cast<size_t>(c)];
         const int w = node % hp.nx;
@@ -1275,10 +1294,14 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
           }
           const int64_t off = col_base + pos.Get(target);
           S.mp_off[static_cast<size_t>(e)] = off;
-          S.fmp_off[static_cast<size_t>(S.fmp_ptr[static_cast<size_t>(nf[static_cast<size_t>(e)])] +
-                                        rank[static_cast<size_t>(e)])] = off;
         }
       }
+    }
+  });
+  // the frame-major copy of the offsets: a gather, frame by frame
+  ParallelRanges(csr_threads, entries, 1 << 14, [&](int64_t j0, int64_t j1) {
+    for (int64_t j = j0; j < j1; ++j) {
+      S.fmp_off[static_cast<size_t>(j)] = S.mp_off[static_cast<size_t>(emap[static_cast<size_t>(j)])];
     }
   });
   S.mp_frame = std::move(nf);
