@@ -77,7 +77,8 @@ class DevBuf {
     ptr_ = static_cast<T*>(CachedDeviceAlloc(bytes, &bytes_, &device_));
     count_ = bytes_ / sizeof(T);
   }
-  void Upload(const std::vector<T>& v, cudaStream_t s) {
+  template <typename A>
+  void Upload(const std::vector<T, A>& v, cudaStream_t s) {
     Alloc(v.size());
     if (!v.empty()) {
       UploadAsync(ptr_, v.data(), v.size() * sizeof(T), s);

@@ -1120,7 +1120,7 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
   // The frame lists ascend, so a thread owning a range of columns finds its
   // part of every list by binary search.
   std::vector<int64_t> nf_ptr(static_cast<size_t>(A) + 1, 0);
-  std::vector<int32_t> nf(static_cast<size_t>(entries));
+  FillVector<int32_t> nf(static_cast<size_t>(entries));
   S.fmp_col.resize(static_cast<size_t>(entries));
   const int csr_threads = entries > (int64_t{1} << 14) ? threads : 1;
   auto frame_part = [&](int f, int64_t c0, int64_t c1) {
@@ -1142,7 +1142,7 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
   }
   // emap[j]: the node-major entry of frame-major entry j (each thread writes
   // contiguous runs of every frame's list, not one entry per frame per node)
-  std::vector<int64_t> emap(static_cast<size_t>(entries));
+  FillVector<int64_t> emap(static_cast<size_t>(entries));
   ParallelRanges(csr_threads, A, 256, [&](int64_t c0, int64_t c1) {
     std::vector<int64_t> fill(nf_ptr.begin() + c0, nf_ptr.begin() + c1);
     for (int f = 1; f < Fr; ++f) {
@@ -1323,10 +1323,10 @@ namespace {
 /// Sizes a recycled array for n elements that are all written afterwards:
 /// one too small is replaced (its contents are not copied) by one with half
 /// again the room, so that the next growth fits.
-template <typename T>
-void Regrow(std::vector<T>& v, size_t n) {
+template <typename Vec>
+void Regrow(Vec& v, size_t n) {
   if (v.capacity() < n) {
-    std::vector<T> fresh;
+    Vec fresh;
     fresh.reserve(n + n / 2);
     v.swap(fresh);
   }
