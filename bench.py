@@ -631,9 +631,9 @@ def _serve_pass(P, args, seed0, rate, check_oracle=False):
 # kernel class on a workload, from the committed one-kernel ncu captures
 # named beside each entry (L2 flushed before the captured step, as here).
 # DRAM bytes (read + written) per launch of a kernel class, averaged over its
-# launches in one iteration of the workload, from the one-pass ncu launch
-# list (gpu__time_duration, dram__bytes_read / _write) summarised in
-# profiles/launch_list_office.md
+# launches in one iteration of the workload, from one-kernel ncu captures
+# (-k <kernel>, one iteration's launches; dram__bytes_read / _write)
+# summarised in profiles/launch_list_office.md
 KERNEL_TRAFFIC_BYTES = {
     ("office", "KUpdate(schur)"): 3054.4e6 / 20,   # the 20 Schur launches of the iteration
     ("office", "KDenseRoot"): 33.4e6,
@@ -777,7 +777,7 @@ def run_gpu(args, dist, world, rank, local):
     roofline = {
         "bound": bound, "achieved": achieved, "peak": peak, "unit": unit, "frac": achieved / peak,
         "traffic": KERNEL_TRAFFIC_BYTES.get((args.workload, dominant_kernel)),
-        "traffic_source": "ncu one-pass launch list, DRAM bytes per launch (profiles/launch_list_office.md)",
+        "traffic_source": "one-kernel ncu capture, DRAM bytes per launch (profiles/launch_list_office.md)",
         "kernel": dominant_kernel, "peak_source": src, "launches_timed": dom["launches"],
         "avg_launch_ms": avg_ms, "work_per_launch": work_per_launch, "work_unit": dom["work_unit"]}
     roofline_factor = {
