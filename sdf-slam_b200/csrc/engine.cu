@@ -894,6 +894,7 @@ FactorPlan Engine::Plan() {
   P.inv_tasks = inv_tasks_.get();
   P.num_inv = static_cast<int>(sym_.inv_tasks.size() / 2);
   P.inv = inv_.get();
+  P.fp32_fronts = any_mixed_;
   P.dense_tasks = dense_tasks_.get();
   P.dense_sync = dense_sync_.get();
   P.dense_inv = dense_inv_.get();

@@ -155,6 +155,9 @@ struct FactorPlan {
   const int32_t* pack_tasks{nullptr};
   const int32_t* tc_tasks{nullptr};
   TcArgs tc{};
+  /// Whether any front may be factored in FP32 (a mixed instance): their
+  /// Schur tiles take KUpdate, the FP64 ones KSchur.
+  bool fp32_fronts{false};
   /// Tiled dense roots: task quads (Symbolic::dense_tasks), the sync words
   /// (a claim counter per level, the abort flag, then the tile counters;
   /// zeroed at the start of every factorization) and the inverse workspace.

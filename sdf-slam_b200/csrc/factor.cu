@@ -1036,8 +1036,8 @@ __global__ void __launch_bounds__(256, 2) KUpdate(DeviceView V, const int32_t* t
   if (V.active[S.instance] == 0) {
     return;
   }
-  if (t[1] == -1 && S.tc_pack >= 0 && Fp32Front(V, S) && V.tc_schur != 0) {
-    return;  // a wide FP32 front: the tensor-core kernels
+  if (t[1] == -1 && (!Fp32Front(V, S) || (S.tc_pack >= 0 && V.tc_schur != 0))) {
+    return;  // FP64 Schur tiles: KSchur; wide FP32 fronts: the tensor cores
   }
   __shared__ double as_buf[kPanel * kTile];
   __shared__ double bs_buf[kPanel * kTile];
@@ -1047,6 +1047,149 @@ __global__ void __launch_bounds__(256, 2) KUpdate(DeviceView V, const int32_t* t
   } else {
     UpdateBody<double>(V, S, t[1], t[2], t[3], dvec, reinterpret_cast<double(*)[kTile]>(as_buf),
                        reinterpret_cast<double(*)[kTile]>(bs_buf));
+  }
+}
+
+/// FP64 Schur complement tiles added into the parent front (the task list
+/// of the Schur update, panel -1), built for occupancy: the K chunks are
+/// copied global -> shared with cp.async (8-byte copies: a front's columns
+/// start at any 8-byte offset), two chunks in flight, so no staging
+/// registers; each thread then scales the A entries it copied by d (the
+/// same product the register path forms); the tile's current values are
+/// read after the K loop, one column group at a time. Three blocks per SM
+/// (64 KB of shared memory each) against two for KUpdate.
+constexpr int kSchurK = 32;
+constexpr size_t kSchurSmem = 2 * 2 * static_cast<size_t>(kSchurK) * 64 * sizeof(double);
+
+__device__ __forceinline__ void CpAsync8(double* dst, const double* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+
+__global__ void __launch_bounds__(256, 3) KSchur(DeviceView V, const int32_t* tasks, const double* dvec) {
+  const int32_t* t = tasks + 4 * static_cast<int64_t>(blockIdx.x);
+  const SupernodeRec S = V.sn[t[0]];
+  if (V.active[S.instance] == 0 || Fp32Front(V, S)) {
+    return;  // FP32 fronts of a mixed solve: KUpdate or the tensor cores
+  }
+  extern __shared__ __align__(16) double schur_sm[];
+  auto As = reinterpret_cast<double(*)[kSchurK][64]>(schur_sm);
+  auto Bs = reinterpret_cast<double(*)[kSchurK][64]>(schur_sm + 2 * kSchurK * 64);
+  const int k = S.ncols;
+  const int F = S.F;
+  const int r0 = k + t[2] * 64;
+  const int c0 = k + t[3] * 64;
+  double* Fs = V.fronts + S.front_off;
+  const double* d = dvec + S.first_col;
+  const int tid = threadIdx.x;
+  const int tx = tid & 15;
+  const int ty = tid >> 4;
+  auto issue = [&](int kk, int buf) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 256 * q;
+      const int l = e >> 6;
+      const int rr = e & 63;
+      const int col = kk + l;
+      const int64_t base = static_cast<int64_t>(col) * F;
+      if (col < k && r0 + rr < F) {
+        CpAsync8(&As[buf][l][rr], Fs + base + r0 + rr);
+      } else {
+        As[buf][l][rr] = 0.0;
+      }
+      if (col < k && c0 + rr < F) {
+        CpAsync8(&Bs[buf][l][rr], Fs + base + c0 + rr);
+      } else {
+        Bs[buf][l][rr] = 0.0;
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      acc[a][b] = 0.0;
+    }
+  }
+  const int chunks = (k + kSchurK - 1) / kSchurK;
+  issue(0, 0);
+  if (chunks > 1) {
+    issue(kSchurK, 1);
+  }
+  for (int ch = 0; ch < chunks; ++ch) {
+    const int buf = ch & 1;
+    if (ch + 1 < chunks) {
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    // the A entries this thread copied, times d (its own copies are
+    // complete; the barrier below publishes them)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = tid + 256 * q;
+      const int l = e >> 6;
+      const int col = ch * kSchurK + l;
+      if (col < k) {
+        As[buf][l][e & 63] *= d[col];
+      }
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int l = 0; l < kSchurK; ++l) {
+      double av[4];
+      double bv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        av[a] = As[buf][l][tx + 16 * a];
+        bv[a] = Bs[buf][l][ty + 16 * a];
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+        }
+      }
+    }
+    __syncthreads();
+    if (ch + 2 < chunks) {
+      issue((ch + 2) * kSchurK, buf);
+    }
+  }
+  // C - acc, added into the parent (or written in place for a front with no
+  // parent), one column group of four entries at a time
+  const bool scatter = S.parent >= 0;
+  const SupernodeRec P = scatter ? V.sn[S.parent] : S;
+  const int32_t* rel = V.sn_rel + S.rows_off;
+  double* Fp = scatter ? V.fronts + P.front_off : Fs;
+  const int64_t PF = P.F;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int c = c0 + ty + 16 * b;
+    double cur[4];
+    int64_t pos[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int r = r0 + tx + 16 * a;
+      const bool in = c < F && r < F && r >= c;
+      cur[a] = in ? Fs[static_cast<int64_t>(c) * F + r] : 0.0;
+      pos[a] = !in ? -1
+                   : (scatter ? static_cast<int64_t>(rel[c - k]) * PF + rel[r - k] : static_cast<int64_t>(c) * F + r);
+    }
+    double old[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      old[a] = (scatter && pos[a] >= 0) ? Fp[pos[a]] : 0.0;
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      if (pos[a] >= 0) {
+        Fp[pos[a]] = scatter ? old[a] + (cur[a] - acc[a][b]) : cur[a] - acc[a][b];
+      }
+    }
   }
 }
 
@@ -2297,6 +2440,9 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
       CudaCheck(cudaFuncSetAttribute(KPanelBlock, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(PanelBlockSmem())),
                 "block smem attr");
+      CudaCheck(cudaFuncSetAttribute(KSchur, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(kSchurSmem)),
+                "schur smem attr");
       if (dev >= 0 && dev < 64) {
         configured[dev] = true;
       }
@@ -2470,8 +2616,14 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
           return tc && r.tc_pack >= 0 ? 0.0 : static_cast<double>(r.ncols) * m * (m + 1.0);
         }) : 0.0;
       });
-      KUpdate<<<static_cast<unsigned>(sr.count), 256, 0, stream>>>(V, P.update_tasks + 4 * sr.begin, P.dvec);
+      KSchur<<<static_cast<unsigned>(sr.count), 256, kSchurSmem, stream>>>(V, P.update_tasks + 4 * sr.begin,
+                                                                            P.dvec);
       ++launches;
+      if (P.fp32_fronts) {
+        // the FP32 fronts of a mixed solve that the tensor cores do not take
+        KUpdate<<<static_cast<unsigned>(sr.count), 256, 0, stream>>>(V, P.update_tasks + 4 * sr.begin, P.dvec);
+        ++launches;
+      }
     }
   }
   if (P.inv != nullptr && P.num_inv > 0) {
