@@ -1059,6 +1059,8 @@ __global__ void __launch_bounds__(256, 2) KUpdate(DeviceView V, const int32_t* t
 /// read after the K loop, one column group at a time. Three blocks per SM
 /// (64 KB of shared memory each) against two for KUpdate.
 constexpr int kSchurK = 32;
+constexpr int kSchurBlocksPerSm = 3;
+constexpr int kSchurPerThread = kSchurK * 64 / 256;  // entries of a chunk each thread copies
 constexpr size_t kSchurSmem = 2 * 2 * static_cast<size_t>(kSchurK) * 64 * sizeof(double);
 
 __device__ __forceinline__ void CpAsync8(double* dst, const double* src) {
@@ -1066,7 +1068,8 @@ __device__ __forceinline__ void CpAsync8(double* dst, const double* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
 }
 
-__global__ void __launch_bounds__(256, 3) KSchur(DeviceView V, const int32_t* tasks, const double* dvec) {
+__global__ void __launch_bounds__(256, kSchurBlocksPerSm)
+    KSchur(DeviceView V, const int32_t* tasks, const double* dvec) {
   const int32_t* t = tasks + 4 * static_cast<int64_t>(blockIdx.x);
   const SupernodeRec S = V.sn[t[0]];
   if (V.active[S.instance] == 0 || Fp32Front(V, S)) {
@@ -1086,7 +1089,7 @@ __global__ void __launch_bounds__(256, 3) KSchur(DeviceView V, const int32_t* ta
   const int ty = tid >> 4;
   auto issue = [&](int kk, int buf) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < kSchurPerThread; ++q) {
       const int e = tid + 256 * q;
       const int l = e >> 6;
       const int rr = e & 63;
@@ -1128,7 +1131,7 @@ __global__ void __launch_bounds__(256, 3) KSchur(DeviceView V, const int32_t* ta
     // the A entries this thread copied, times d (its own copies are
     // complete; the barrier below publishes them)
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < kSchurPerThread; ++q) {
       const int e = tid + 256 * q;
       const int l = e >> 6;
       const int col = ch * kSchurK + l;
