@@ -392,17 +392,20 @@ struct SymPiece {
   int margin{0};            // coupling dilation (cells) the piece was built with
 };
 
-/// Coupling dilation (cells) of a first analysis. 5: in a batch of 64
-/// uneven instances some instance leaves a 3-cell pattern in most early
-/// iterations, and each re-analysis re-concatenates and re-uploads every
-/// instance's structure (B200: 4 re-analyses in 20 iterations instead of 11,
-/// 1717 against 1081 LM iterations/s); the floor plan's iteration costs
-/// 0.7 % more than at 3. The same for one instance as for a batch, so that a
-/// problem follows the same steps alone and in a batch.
-constexpr int kDefaultMargin = 5;
+/// Coupling dilation (cells) of a first analysis. 7: a re-analysis holds the
+/// GPU for the host analysis and the structure upload (about 30 ms for the
+/// 910-pose office on B200, more for a batch, whose every instance's
+/// structure is re-concatenated), and the first LM iterations from
+/// odometry poses move points by several cells; the wider pattern makes the
+/// office's factorization about 5 % slower per iteration than at 5 cells but
+/// saves most re-analyses (64 uneven instances: 1 re-analysis in 20
+/// iterations at 7 against 4 at 5 and 11 at 3). The same for one instance as
+/// for a batch, so that a problem follows the same steps alone and in a
+/// batch.
+constexpr int kDefaultMargin = 7;
 /// Growth of the dilation at each re-analysis, and its cap.
 constexpr int kMarginStep = 2;
-constexpr int kMaxMargin = 7;
+constexpr int kMaxMargin = 9;
 
 /// Analyses one instance at its current state on up to `threads` host
 /// threads (0: all hardware threads).

@@ -225,7 +225,7 @@ def test_state_outside_pattern_reanalyses_only_that_instance():
     batch.cost(0)  # the device problem and its analysis at the scenes' poses
     m1, p1 = batch.state(1)
     moved = p1.copy()
-    moved[1:, 0] += 1.7  # beyond the 5-cell coupling margin of 0.25 m cells
+    moved[1:, 0] += 2.5  # beyond the 7-cell coupling margin of 0.25 m cells
     moved[1:, 2] += 0.05
     batch.set_state(m1, moved, index=1)
     opts = P.SolverOptions(max_iterations=4)
