@@ -559,7 +559,7 @@ void Engine::UploadSymbolic() {
   small_tasks_.Upload(sym_.small_tasks, s);
   pack_tasks_.Upload(sym_.pack_tasks, s);
   tc_tasks_.Upload(sym_.tc_tasks, s);
-  fronts_.Alloc(static_cast<size_t>(sym_.front_doubles));
+  fronts_.AllocGrowable(static_cast<size_t>(sym_.front_doubles));
   upd_.Alloc(static_cast<size_t>(std::max<int64_t>(1, sym_.update_doubles)));
   max_front_ = 1;
   for (const SupernodeRec& r : sym_.sn) {
@@ -701,8 +701,8 @@ void Engine::RefreshView() {
 }
 
 void Engine::AllocMixed() {
-  amat_.Alloc(static_cast<size_t>(sym_.front_doubles));
-  fronts32_.Alloc(static_cast<size_t>(sym_.front_doubles));
+  amat_.AllocGrowable(static_cast<size_t>(sym_.front_doubles));
+  fronts32_.AllocGrowable(static_cast<size_t>(sym_.front_doubles));
   std::vector<int32_t> tasks;
   for (size_t s = 0; s < sym_.sn.size(); ++s) {
     const int64_t total = static_cast<int64_t>(sym_.sn[s].F) * sym_.sn[s].F;
@@ -827,9 +827,12 @@ void Engine::LaunchRows() {
 }
 
 void Engine::LaunchNormal() {
-  if (!sym_.zero_tasks.empty()) {
-    KZeroFronts<<<static_cast<unsigned>(sym_.zero_tasks.size() / 2), 32 * kZeroCols, 0, stream_>>>(
-        V_, zero_tasks_.get());
+  // the leaf fronts' trailing columns only for an in-place tensor-core
+  // Schur complement
+  const int64_t zero_count =
+      V_.tc_schur != 0 ? static_cast<int64_t>(sym_.zero_tasks.size() / 2) : sym_.zero_main;
+  if (zero_count > 0) {
+    KZeroFronts<<<static_cast<unsigned>(zero_count), 32 * kZeroCols, 0, stream_>>>(V_, zero_tasks_.get());
     CudaCheck(cudaGetLastError(), "front zeroing");
     ++times_.launches;
   }

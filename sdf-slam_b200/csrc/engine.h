@@ -77,6 +77,20 @@ class DevBuf {
     ptr_ = static_cast<T*>(CachedDeviceAlloc(bytes, &bytes_, &device_));
     count_ = bytes_ / sizeof(T);
   }
+  /// As Alloc, but a fresh block is a quarter larger than asked for from the
+  /// first allocation on (the front buffers: a re-analysis that widens a
+  /// pattern by two cells adds about a fifth more front entries, which then
+  /// fit in place instead of mapping a new multi-gigabyte block while the
+  /// solve waits).
+  void AllocGrowable(size_t count) {
+    if (count <= count_ && ptr_ != nullptr) {
+      return;
+    }
+    Free();
+    const size_t want = std::max<size_t>(1, count + count / 4);
+    ptr_ = static_cast<T*>(CachedDeviceAlloc(want * sizeof(T), &bytes_, &device_));
+    count_ = bytes_ / sizeof(T);
+  }
   template <typename A>
   void Upload(const std::vector<T, A>& v, cudaStream_t s) {
     Alloc(v.size());

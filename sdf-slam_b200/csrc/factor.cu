@@ -927,7 +927,9 @@ __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeR
     }
   }
   // the tile's current values, loaded now so that their latency hides
-  // behind the K loop (no other block touches this tile)
+  // behind the K loop (no other block touches this tile); a leaf's trailing
+  // block holds no child contribution and is taken as zero, not loaded
+  const bool fresh = panel == -1 && S.child_count == 0;
   T cur[4][4];
 #pragma unroll
   for (int b = 0; b < 4; ++b) {
@@ -935,7 +937,7 @@ __device__ __forceinline__ void UpdateBody(const DeviceView& V, const SupernodeR
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
       const int r = r0 + tx + 16 * a;
-      cur[a][b] = (c < clim && r < F && r >= c) ? Fs[static_cast<int64_t>(c) * F + r] : T(0);
+      cur[a][b] = (!fresh && c < clim && r < F && r >= c) ? Fs[static_cast<int64_t>(c) * F + r] : T(0);
     }
   }
   // K chunks of kPanel columns: the next chunk is loaded into registers
@@ -1068,6 +1070,49 @@ __device__ __forceinline__ void CpAsync8(double* dst, const double* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
 }
 
+/// The end of a KSchur tile: C - acc added into the parent front (or written
+/// in place for a front with no parent), one column group of four entries at
+/// a time, all parent reads of a group before its writes. kLoadC false: C is
+/// known to be zero and is not read.
+template <bool kLoadC>
+__device__ __forceinline__ void SchurEpilogue(const DeviceView& V, const SupernodeRec& S, const double* Fs, int r0,
+                                              int c0, const double (&acc)[4][4]) {
+  const int k = S.ncols;
+  const int F = S.F;
+  const int tx = threadIdx.x & 15;
+  const int ty = threadIdx.x >> 4;
+  const bool scatter = S.parent >= 0;
+  const SupernodeRec P = scatter ? V.sn[S.parent] : S;
+  const int32_t* rel = V.sn_rel + S.rows_off;
+  double* Fp = scatter ? V.fronts + P.front_off : V.fronts + S.front_off;
+  const int64_t PF = P.F;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int c = c0 + ty + 16 * b;
+    double cur[4];
+    int64_t pos[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int r = r0 + tx + 16 * a;
+      const bool in = c < F && r < F && r >= c;
+      cur[a] = (kLoadC && in) ? Fs[static_cast<int64_t>(c) * F + r] : 0.0;
+      pos[a] = !in ? -1
+                   : (scatter ? static_cast<int64_t>(rel[c - k]) * PF + rel[r - k] : static_cast<int64_t>(c) * F + r);
+    }
+    double old[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      old[a] = (scatter && pos[a] >= 0) ? Fp[pos[a]] : 0.0;
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      if (pos[a] >= 0) {
+        Fp[pos[a]] = scatter ? old[a] + (cur[a] - acc[a][b]) : cur[a] - acc[a][b];
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(256, kSchurBlocksPerSm)
     KSchur(DeviceView V, const int32_t* tasks, const double* dvec) {
   const int32_t* t = tasks + 4 * static_cast<int64_t>(blockIdx.x);
@@ -1163,36 +1208,11 @@ __global__ void __launch_bounds__(256, kSchurBlocksPerSm)
     }
   }
   // C - acc, added into the parent (or written in place for a front with no
-  // parent), one column group of four entries at a time
-  const bool scatter = S.parent >= 0;
-  const SupernodeRec P = scatter ? V.sn[S.parent] : S;
-  const int32_t* rel = V.sn_rel + S.rows_off;
-  double* Fp = scatter ? V.fronts + P.front_off : Fs;
-  const int64_t PF = P.F;
-#pragma unroll
-  for (int b = 0; b < 4; ++b) {
-    const int c = c0 + ty + 16 * b;
-    double cur[4];
-    int64_t pos[4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      const int r = r0 + tx + 16 * a;
-      const bool in = c < F && r < F && r >= c;
-      cur[a] = in ? Fs[static_cast<int64_t>(c) * F + r] : 0.0;
-      pos[a] = !in ? -1
-                   : (scatter ? static_cast<int64_t>(rel[c - k]) * PF + rel[r - k] : static_cast<int64_t>(c) * F + r);
-    }
-    double old[4];
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      old[a] = (scatter && pos[a] >= 0) ? Fp[pos[a]] : 0.0;
-    }
-#pragma unroll
-    for (int a = 0; a < 4; ++a) {
-      if (pos[a] >= 0) {
-        Fp[pos[a]] = scatter ? old[a] + (cur[a] - acc[a][b]) : cur[a] - acc[a][b];
-      }
-    }
+  // parent); a leaf's C is zero (no child adds into it) and is not loaded
+  if (S.child_count == 0) {
+    SchurEpilogue<false>(V, S, Fs, r0, c0, acc);
+  } else {
+    SchurEpilogue<true>(V, S, Fs, r0, c0, acc);
   }
 }
 

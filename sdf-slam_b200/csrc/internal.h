@@ -317,8 +317,13 @@ struct Symbolic {
   // the tile counters (nt x nt per front) and the diagonal-tile inverses
   // (64 x 64 doubles per tile) they use.
   // (sn, first column) pairs of kZeroCols columns: the fronts' lower
-  // triangles cleared before every assembly
+  // triangles cleared before every assembly. The first zero_main pairs are
+  // what an FP64 assembly needs; the rest are the trailing columns of the
+  // leaf fronts (no child adds into them, and their Schur update reads them
+  // as zero without loading them), cleared only for the tensor-core Schur
+  // complement of a mixed solve, which accumulates into them in place.
   std::vector<int32_t> zero_tasks;
+  int64_t zero_main{0};
   std::vector<int32_t> dense_tasks;
   std::vector<TaskRange> dense_range;
   int64_t dense_cnt_words{0};

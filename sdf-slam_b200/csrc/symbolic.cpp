@@ -721,10 +721,19 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
   }
   // front clearing tasks
   S.zero_tasks.clear();
-  for (int s = 0; s < Sn; ++s) {
-    for (int c = 0; c < S.sn[static_cast<size_t>(s)].F; c += kZeroCols) {
-      S.zero_tasks.push_back(s);
-      S.zero_tasks.push_back(c);
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int s = 0; s < Sn; ++s) {
+      const SupernodeRec& r = S.sn[static_cast<size_t>(s)];
+      const int split = r.child_count == 0 ? r.ncols : r.F;
+      for (int c = 0; c < r.F; c += kZeroCols) {
+        if ((c < split) == (pass == 0)) {
+          S.zero_tasks.push_back(s);
+          S.zero_tasks.push_back(c);
+        }
+      }
+    }
+    if (pass == 0) {
+      S.zero_main = static_cast<int64_t>(S.zero_tasks.size() / 2);
     }
   }
   // tiled dense roots: counters, inverse workspace and task lists per level
