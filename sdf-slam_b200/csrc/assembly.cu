@@ -924,10 +924,28 @@ __global__ void KCostTerms(DeviceView V, double* terms) {
     EvalPoint(V, I, c, s, pose, p.x, p.y, V.pt_exp[t], 0, false, ev);
     const int local = f - I.frame_off;
     if (ev.valid && local >= 1) {
-      const int cell = ev.h * (I.nx - 1) + ev.w;
-      const uint32_t word = V.allow_bits[I.allow_off + static_cast<int64_t>(local) * I.allow_words + (cell >> 5)];
-      if (((word >> (cell & 31)) & 1u) == 0u) {
+      const uint32_t* allow = V.allow_bits + I.allow_off + static_cast<int64_t>(local) * I.allow_words;
+      const int cw = I.nx - 1;
+      const int cell = ev.h * cw + ev.w;
+      if (((allow[cell >> 5] >> (cell & 31)) & 1u) == 0u) {
         atomicOr(V.status + i, kStatusNextOverflow);
+      } else if (I.near_cells > 0 && (V.status[i] & kStatusNearEdge) == 0) {
+        // the eight cells near_cells away (along the axes and the diagonals,
+        // those inside the grid): one outside the set marks the instance
+        const int g = I.near_cells;
+        bool near = false;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+          const int w = ev.w + g * (q % 3 - 1);
+          const int h = ev.h + g * (q / 3 - 1);
+          if (q != 4 && w >= 0 && w < cw && h >= 0 && h < I.ny - 1) {
+            const int c = h * cw + w;
+            near = near || ((allow[c >> 5] >> (c & 31)) & 1u) == 0u;
+          }
+        }
+        if (near) {
+          atomicOr(V.status + i, kStatusNearEdge);
+        }
       }
     }
     const double r = V.pt_sw[t] * ev.residual;

@@ -34,6 +34,9 @@ struct InstDev {
   int32_t pp_first;
   int32_t num_params;
   int32_t mixed;  // 1: this solve factors the grid supernodes in FP32
+  // cells probed around each point by the cost kernel for kStatusNearEdge
+  // (0: no probe)
+  int32_t near_cells;
 };
 
 /// Status bits per instance.
@@ -45,6 +48,10 @@ constexpr int kStatusNextOverflow = 4;
 /// A wait on another block's flag ran out of its limit (the results of the
 /// launch are not valid).
 constexpr int kStatusWaitTimeout = 8;
+// set by the cost kernel: at the state it evaluated, a point lies within
+// near_cells cells of its pose's analysed cell set's edge (the pattern is
+// re-centred ahead of time, in the background)
+constexpr int kStatusNearEdge = 16;
 
 /// Per point row record: 4 node Jacobian entries, 3 pose entries, residual.
 constexpr int kPointRec = 8;

@@ -134,6 +134,9 @@ void Engine::AnalyzeAndUpload(std::vector<SymPiece>* pieces, int64_t keep_rows) 
     throw;
   }
   analysis.get();
+  iters_.assign(host_.size(), 0);
+  analysed_at_.assign(host_.size(), 0);
+  near_.clear();
   UploadSymbolic();
 }
 
@@ -151,6 +154,8 @@ void Engine::Replace(HostProblem next, SymPiece* piece, int64_t keep_rows) {
     Fail(SDFGPU_ERR_INVALID_ARGUMENT, "replacement problem has another grid or other active columns");
   }
   keep_rows = std::max<int64_t>(0, std::min<int64_t>({keep_rows, host_[0].num_points(), next.num_points()}));
+  // no background analysis may still read the current problem
+  DropSpeculations(nullptr);
   // nothing enqueued may still read the current problem's buffers
   CudaCheck(cudaStreamSynchronize(stream_), "replace sync");
   DropGraph();
@@ -175,6 +180,10 @@ void Engine::DropGraph() {
 }
 
 Engine::~Engine() {
+  try {
+    DropSpeculations(nullptr);
+  } catch (...) {
+  }
   DropGraph();
   if (stream_ != nullptr) {
     cudaStreamSynchronize(stream_);
@@ -602,6 +611,7 @@ void Engine::UploadSymbolic() {
     d.pp_first = sym_.pp_first[i];
     d.num_params = host_[i].num_params();
     d.mixed = i < mixed_.size() ? mixed_[i] : 0;
+    d.near_cells = i < margin_.size() ? std::max(0, std::min(kNearCells, margin_[i] - 1)) : 0;
   }
   inst_host_ = inst;
   inst_.Upload(inst, s);
@@ -1012,6 +1022,8 @@ void Engine::LaunchStepAndCost(bool backup) {
 
 void Engine::Reanalyze(const std::vector<int>& which) {
   const auto t0 = std::chrono::steady_clock::now();
+  // a background analysis of these instances is superseded by this one
+  DropSpeculations(&which);
   std::vector<double> poses(3 * static_cast<size_t>(total_frames_));
   CudaCheck(cudaMemcpyAsync(poses.data(), poses_.get(), poses.size() * sizeof(double), cudaMemcpyDeviceToHost,
                             stream_),
@@ -1025,6 +1037,9 @@ void Engine::Reanalyze(const std::vector<int>& which) {
     margin_[static_cast<size_t>(i)] = std::min(margin_[static_cast<size_t>(i)] + kMarginStep, kMaxMargin);
   }
   AnalyzeInstances(host_, margin_, pieces_, &which);
+  for (const int i : which) {
+    analysed_at_[static_cast<size_t>(i)] = iters_[static_cast<size_t>(i)];
+  }
   sym_ = GlobalStructure();
   UploadSymbolic();
   ++times_.reanalyses;
@@ -1138,6 +1153,117 @@ void Engine::ReanalyzePending() {
   const std::vector<int> which = std::move(pending_);
   pending_.clear();
   Reanalyze(which);
+}
+
+void Engine::StartSpeculation(int i, const std::vector<double>& poses) {
+  auto sp = std::make_unique<Speculation>();
+  const InstanceLayout& L = layout_[static_cast<size_t>(i)];
+  sp->inst = i;
+  sp->margin = margin_[static_cast<size_t>(i)];
+  sp->poses.assign(poses.begin() + 3 * static_cast<int64_t>(L.frame_off),
+                   poses.begin() + 3 * static_cast<int64_t>(L.frame_off + L.num_frames));
+  sp->adopt_at = iters_[static_cast<size_t>(i)] + kSpeculationDelay;
+  sp->has_structure = host_.size() == 1;
+  sp->sched = sched_;
+  // the thread reads only this instance's problem, which stays unchanged
+  // until the speculation is installed or dropped
+  Speculation* raw = sp.get();
+  sp->done = std::async(std::launch::async, [this, raw] {
+    raw->piece = AnalyzeInstance(host_[static_cast<size_t>(raw->inst)], raw->margin, 0, &raw->poses);
+    if (raw->has_structure) {
+      raw->structure = ConcatenateOne(std::move(raw->piece), 32, 64, raw->sched);
+    }
+  });
+  specs_.push_back(std::move(sp));
+}
+
+void Engine::DropSpeculations(const std::vector<int>* which) {
+  for (auto it = specs_.begin(); it != specs_.end();) {
+    if (which != nullptr && std::find(which->begin(), which->end(), (*it)->inst) == which->end()) {
+      ++it;
+      continue;
+    }
+    if ((*it)->done.valid()) {
+      (*it)->done.wait();  // an exception it stored is discarded with it
+    }
+    it = specs_.erase(it);
+  }
+}
+
+void Engine::StepSpeculations() {
+  // instances about to be re-analysed from their current state
+  if (!pending_.empty() && !specs_.empty()) {
+    DropSpeculations(&pending_);
+  }
+  std::vector<std::unique_ptr<Speculation>> due;
+  for (auto it = specs_.begin(); it != specs_.end();) {
+    if ((*it)->adopt_at <= iters_[static_cast<size_t>((*it)->inst)]) {
+      due.push_back(std::move(*it));
+      it = specs_.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  if (!due.empty()) {
+    const auto t0 = std::chrono::steady_clock::now();
+    bool built = false;
+    for (auto& sp : due) {
+      sp->done.get();
+      const auto i = static_cast<size_t>(sp->inst);
+      host_[i].poses = std::move(sp->poses);
+      analysed_at_[i] = iters_[i];
+      if (sp->has_structure) {
+        // a single instance (never pending here: its pending state dropped
+        // the speculation); the schedule may have changed since
+        sym_ = std::move(sp->structure);
+        const Schedule& now = sched_;
+        if (now.small_pivots != sp->sched.small_pivots || now.front_rows != sp->sched.front_rows ||
+            now.panel_rows != sp->sched.panel_rows) {
+          Reschedule(sym_, sched_);
+        }
+        built = true;
+      } else {
+        pieces_[i] = std::move(sp->piece);
+      }
+    }
+    // a synchronous re-analysis (pending_) rebuilds the structure anyway
+    if (pending_.empty()) {
+      if (!built) {
+        sym_ = GlobalStructure();
+      }
+      UploadSymbolic();
+    }
+    ++times_.reanalyses;
+    times_.reanalysis_host += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+  std::vector<int> start;
+  for (const int i : near_) {
+    const auto u = static_cast<size_t>(i);
+    if (iters_[u] - analysed_at_[u] < kSpeculateAfter ||
+        std::find(pending_.begin(), pending_.end(), i) != pending_.end() ||
+        std::find(start.begin(), start.end(), i) != start.end()) {
+      continue;
+    }
+    bool busy = false;
+    for (const auto& sp : specs_) {
+      busy = busy || sp->inst == i;
+    }
+    if (!busy) {
+      start.push_back(i);
+    }
+  }
+  near_.clear();
+  if (!start.empty()) {
+    // the accepted states (a revert of other instances may still be queued)
+    std::vector<double> poses(3 * static_cast<size_t>(total_frames_));
+    CudaCheck(cudaMemcpyAsync(poses.data(), poses_.get(), poses.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                              stream_),
+              "poses");
+    CudaCheck(cudaStreamSynchronize(stream_), "speculation sync");
+    for (const int i : start) {
+      StartSpeculation(i, poses);
+    }
+  }
 }
 
 /// Rows + normal equations; re-runs the symbolic analysis (once) when a point
@@ -1622,6 +1748,10 @@ void Engine::LaunchIteration() {
     CudaCheck(cudaEventRecord(span_[0], stream_), "event");
     span_started_ = true;
   }
+  for (size_t i = 0; i < I; ++i) {
+    iters_[i] += h_active_[i] != 0 ? 1 : 0;
+  }
+  StepSpeculations();
   // a state that left its pattern is re-analysed before it is linearized
   ReanalyzePending();
   EnqueueIteration();
@@ -1802,6 +1932,9 @@ void Engine::FinishIteration() {
     if (h_active_[i] != 0 && (h_status_[i] & kStatusNextOverflow) != 0 && revert[i] == 0 &&
         (h_status_[i] & kStatusZeroPivot) == 0) {
       pending_.push_back(static_cast<int>(i));
+    } else if (h_active_[i] != 0 && (h_status_[i] & kStatusNearEdge) != 0 && revert[i] == 0 &&
+               (h_status_[i] & kStatusZeroPivot) == 0) {
+      near_.push_back(static_cast<int>(i));
     }
   }
   if (any_revert) {

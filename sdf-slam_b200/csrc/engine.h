@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <future>
 #include <memory>
 #include <string>
 #include <vector>
@@ -387,6 +388,33 @@ class Engine {
   void Reanalyze(const std::vector<int>& which);
   /// Re-analyses the instances whose state left their pattern (pending_).
   void ReanalyzePending();
+  /// A pattern re-centred ahead of time: an instance whose accepted state
+  /// brought a point within a few cells of its pattern's edge is analysed
+  /// again (same margin) on a host thread from that state, while the
+  /// iterations go on with the current pattern, and the analysis replaces
+  /// its pattern a fixed number of its own iterations later (so that no
+  /// result depends on host timing or on the other instances of a batch).
+  struct Speculation {
+    int inst{0};
+    int margin{0};
+    std::vector<double> poses;  // the state analysed
+    SymPiece piece;
+    // a single-instance engine's global structure, built on the same thread
+    // under `sched` (the piece is consumed)
+    Symbolic structure;
+    Schedule sched;
+    bool has_structure{false};
+    std::future<void> done;
+    int64_t adopt_at{0};  // iters_[inst] at which the analysis is installed
+  };
+  /// At the start of an iteration: drops the speculations of instances
+  /// that are about to be re-analysed synchronously, installs the ones that
+  /// are due, starts one for each instance near its pattern's edge.
+  void StepSpeculations();
+  void StartSpeculation(int i, const std::vector<double>& poses);
+  /// Waits for the speculations of the instances in `which` (all of them
+  /// when null) and discards them.
+  void DropSpeculations(const std::vector<int>* which);
   void EnqueueIteration();
   int AssembleWithPattern();
   [[nodiscard]] FactorPlan Plan();
@@ -397,6 +425,10 @@ class Engine {
   std::vector<SymPiece> pieces_;   // per-instance analyses (local numbering)
   std::vector<int> margin_;        // per instance: coupling margin of its piece
   std::vector<int> pending_;       // instances whose current state overflows their pattern
+  std::vector<std::unique_ptr<Speculation>> specs_;  // background re-analyses in flight
+  std::vector<int> near_;          // instances whose last accepted state nears their pattern's edge
+  std::vector<int64_t> iters_;     // per instance: iterations launched with it active, over the engine's life
+  std::vector<int64_t> analysed_at_;  // per instance: iters_ at its last analysis
   Schedule sched_;                 // factorization schedule (autotuned or default)
   Symbolic sym_;
   cudaStream_t stream_{nullptr};

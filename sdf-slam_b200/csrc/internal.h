@@ -411,10 +411,24 @@ constexpr int kDefaultMargin = 7;
 /// Growth of the dilation at each re-analysis, and its cap.
 constexpr int kMarginStep = 2;
 constexpr int kMaxMargin = 9;
+/// A point farther than margin - kNearCells cells from the cells of its
+/// pose's points at the analysed state (probed kNearCells cells around it)
+/// marks its instance near the pattern's edge.
+constexpr int kNearCells = 2;
+/// Such an instance is re-analysed in the background (same margin, from the
+/// state that marked it) once its pattern has held kSpeculateAfter
+/// iterations (the first iterations from odometry poses move points by
+/// several cells each; a pattern they leave is re-analysed at once, with a
+/// wider margin), and the analysis replaces the pattern kSpeculationDelay
+/// iterations after it started.
+constexpr int64_t kSpeculateAfter = 20;
+constexpr int64_t kSpeculationDelay = 6;
 
 /// Analyses one instance at its current state on up to `threads` host
-/// threads (0: all hardware threads).
-SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads = 0);
+/// threads (0: all hardware threads); `poses` (3 per frame), when given,
+/// replaces the problem's own poses as the state analysed.
+SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads = 0,
+                         const std::vector<double>* poses = nullptr);
 
 /// Analyses the instances listed in `which` (all when null) into
 /// pieces[i] on the host pool: one instance per thread when there are at

@@ -915,12 +915,16 @@ void OrderDenseTileTasks(std::vector<DenseTileTask>* tasks) {
   });
 }
 
-SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
+SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads, const std::vector<double>* poses) {
   if (threads <= 0) {
     threads = PoolThreads();
   }
   if (margin < 0) {
     Fail(SDFGPU_ERR_INVALID_ARGUMENT, "negative coupling margin");
+  }
+  const std::vector<double>& state = poses != nullptr ? *poses : hp.poses;
+  if (state.size() != hp.poses.size()) {
+    Fail(SDFGPU_ERR_INVALID_ARGUMENT, "analysed poses do not match the problem's frames");
   }
   // The per-pose coupling sets are derived from the current cells of every
   // point row, dilated by `margin` cells.
@@ -1031,7 +1035,7 @@ SymPiece AnalyzeInstance(const HostProblem& hp, int margin, int threads) {
       std::vector<uint64_t> tmp(static_cast<size_t>(rw));
       std::vector<uint64_t> nodes(static_cast<size_t>(rw));
       for (int f = std::max(f0, 1); f < f1; ++f) {
-        const double* pose = &hp.poses[3 * static_cast<size_t>(f)];
+        const double* pose = &state[3 * static_cast<size_t>(f)];
         const double c = std::cos(pose[2]);
         const double sn = std::sin(pose[2]);
         std::fill(occ.begin(), occ.end(), uint64_t{0});

@@ -250,6 +250,73 @@ def test_state_outside_pattern_reanalyses_only_that_instance():
     assert hg.shape == ho.shape and np.max(np.abs(hg - ho) / np.abs(ho)) <= 1e-8
 
 
+def _recentring_run(prob, index, moved, one_step, n):
+    """20 iterations, instance `index`'s poses replaced by `moved` (its map
+    kept), then n one-iteration solves; the re-analyses of each solve."""
+    P.solve(prob, [P.SolverOptions(max_iterations=20, step_tolerance=0.0)] * prob.count
+            if prob.count > 1 else P.SolverOptions(max_iterations=20, step_tolerance=0.0))
+    m, _ = prob.state(index)
+    prob.set_state(m, moved, index=index)
+    counts = []
+    for _ in range(n):
+        P.solve(prob, [one_step] * prob.count if prob.count > 1 else one_step)
+        counts.append(prob.last_profile()["reanalyses"])
+    return counts
+
+
+def test_pattern_recentred_ahead_of_time_follows_oracle():
+    # An instance whose pattern has held 20 of its iterations and whose
+    # accepted state brings points within two cells of the pattern's edge
+    # (here: poses moved by 1.5 m, six of the seven 0.25 m cells of the
+    # coupling margin) is analysed again on a host thread and the analysis
+    # replaces its pattern six of its iterations later. The results depend
+    # neither on host timing nor on the batch, and follow the oracle.
+    scs = [scenes.room_scene(seed=s, grid=g, frames=f, beams=b)
+           for s, g, f, b in [(20, 44, 9, 120), (21, 48, 11, 150)]]
+    specs = [scene_specs(sc, P.ProblemOptions(hallucination_points=3))[0] for sc in scs]
+    probe = P.Problem.from_specs(specs[1])
+    P.solve(probe, P.SolverOptions(max_iterations=20, step_tolerance=0.0))
+    _, p20 = probe.state()
+    moved = p20.copy()
+    moved[1:, 0] += 1.5
+    one = P.SolverOptions(max_iterations=1, step_tolerance=0.0)
+    n = 10
+    runs = []
+    for _ in range(2):
+        single = P.Problem.from_specs(specs[1])
+        counts = _recentring_run(single, 0, moved, one, n)
+        runs.append((counts, single.state()))
+    counts, (sm, sp) = runs[0]
+    assert sum(counts) >= 1
+    # not the re-analysis a pattern overflow forces before the next iteration
+    assert next(k for k, c in enumerate(counts) if c) >= 6
+    assert runs[1][0] == counts
+    assert np.array_equal(runs[1][1][0], sm) and np.array_equal(runs[1][1][1], sp)
+    batch = P.Problem.batch(specs)
+    bcounts = _recentring_run(batch, 1, moved, one, n)
+    assert sum(bcounts) >= 1
+    bm, bp = batch.state(1)
+    assert np.array_equal(bm, sm) and np.array_equal(bp, sp)
+    lone = P.Problem.from_specs(specs[0])
+    P.solve(lone, P.SolverOptions(max_iterations=20, step_tolerance=0.0))
+    for _ in range(n):
+        P.solve(lone, one)
+    lm, lp = lone.state()
+    bm0, bp0 = batch.state(0)
+    assert np.array_equal(bm0, lm) and np.array_equal(bp0, lp)
+    # the oracle from the moved state, one-iteration solves as well
+    orc = oracle_from_specs(specs[1])
+    orc.solve(max_iterations=20, step_tolerance=0.0, num_threads=4)
+    om, _ = orc.state()
+    orc.set_state(om, moved)
+    for _ in range(n):
+        orc.solve(max_iterations=1, step_tolerance=0.0, num_threads=4)
+    om, op = orc.state()
+    assert np.max(np.abs(sp[:, :2] - op[:, :2])) <= 1e-6
+    assert np.max(np.abs(sm - om)) <= 1e-6
+    assert rel_err(single.cost(), orc.cost()) <= 1e-8
+
+
 def test_mixed_precision_solve_follows_fp64_oracle():
     # Mixed: FP32 grid fronts, FP64 pose root, FP64 refinement. With three
     # refinement rounds the LM trajectory stays on the FP64 oracle's within
