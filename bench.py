@@ -301,7 +301,7 @@ def run_profile(args):
     specs = scene_specs(P, scene)
     gpu = P.Problem.from_specs(specs)
     opts = P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=args.precision,
-                           refine_steps=args.refine_steps)
+                           refine_steps=args.refine_steps, refine_tolerance=args.refine_tolerance)
     for it in range(args.profile):
         if it == 1:
             gpu.kernel_timing()  # every kernel class, from the second iteration on
@@ -374,7 +374,7 @@ def run_oracle_comparison(P, args, specs):
     for precision in ("fp64", "mixed"):
         g = P.Problem.from_specs(specs)
         r = P.solve(g, P.SolverOptions(max_iterations=iters, step_tolerance=0.0, precision=precision,
-                                       refine_steps=args.refine_steps))
+                                       refine_steps=args.refine_steps, refine_tolerance=args.refine_tolerance))
         out[precision] = _state_errors(r.final_cost, g.state(), ro["final_cost"], ostate)
         out[precision]["final_cost"] = r.final_cost
         g.close()
@@ -391,12 +391,15 @@ def run_mixed(P, args, specs, flusher, state0):
     the same pattern re-analyses)."""
     prob = P.Problem.from_specs(specs)
     opts1 = P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision="mixed",
-                            refine_steps=args.refine_steps)
+                            refine_steps=args.refine_steps, refine_tolerance=args.refine_tolerance)
     prob.set_state(*state0)
     for _ in range(args.warmup):
         P.solve(prob, opts1)
     if not args.no_autotune:
         prob.autotune()
+    # whether the autotuner kept the tensor-core Schur complements, with the
+    # mixed factor + solve times it measured both ways
+    tc_choice = prob.tensor_core_choice()
     prob.set_state(*state0)
     P.solve(prob, opts1)
     prob.set_state(*state0)
@@ -405,7 +408,8 @@ def run_mixed(P, args, specs, flusher, state0):
     device, launches, phases = _timed_solves(P, prob, opts1, steps, flusher, spans)
     kernels = kernel_profile(P, prob, opts1, flusher)
     prob.close()
-    out = {"value": steps / device, "unit": "LM iters/s", "refine_steps": args.refine_steps, "steps": steps,
+    out = {"value": steps / device, "unit": "LM iters/s", "refine_steps": args.refine_steps,
+           "refine_tolerance": args.refine_tolerance, "tensor_core_choice": tc_choice, "steps": steps,
            **_span_summary(spans),
            "phase_ms_per_step": {k: 1000.0 * v / steps for k, v in zip(PHASES, phases)}, "kernels": kernels}
     tc = kernels.get("KSchurTc")
@@ -500,7 +504,7 @@ def run_batch_office(P, args, flusher, plain_value):
     for precision in ("fp64", "mixed"):
         batch = P.Problem.batch(specs)
         opts1 = [P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=precision,
-                                 refine_steps=args.refine_steps)] * count
+                                 refine_steps=args.refine_steps, refine_tolerance=args.refine_tolerance)] * count
         # past the first iterations, whose large pose moves re-analyse the
         # patterns of most instances (the single office is timed as far in)
         for _ in range(args.office_batch_warmup):
@@ -525,7 +529,7 @@ def run_batch_office(P, args, flusher, plain_value):
     for precision in ("fp64", "mixed"):
         batch = P.Problem.batch(specs)
         res = P.solve(batch, [P.SolverOptions(max_iterations=iters, step_tolerance=0.0, precision=precision,
-                                              refine_steps=args.refine_steps)] * count)
+                                              refine_steps=args.refine_steps, refine_tolerance=args.refine_tolerance)] * count)
         finals[precision] = np.array([r.final_cost for r in res])
         batch.close()
     out["mixed"]["max_final_cost_rel_err_vs_fp64"] = float(
@@ -597,6 +601,7 @@ def _serve_pass(P, args, seed0, rate, check_oracle=False):
         if due > now:
             time.sleep(due - now)
         ids.append(server.submit(spec, opts))
+    last_arrival = time.perf_counter() - t0
     server.drain(600000)
     wall = time.perf_counter() - t0
     st = server.stats()
@@ -609,6 +614,9 @@ def _serve_pass(P, args, seed0, rate, check_oracle=False):
     server.close()
     out = {"requests": len(reqs), "completed_ok": ok, "rate_req_s": rate,
            "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "throughput_req_s": len(reqs) / wall,
+           # throughput counts the arrival window and the drain after it: a
+           # server that keeps up drains in about one request's latency
+           "arrival_window_s": last_arrival, "drain_after_last_arrival_s": wall - last_arrival,
            "lm_iters_s": st["iterations_per_s"]}
     if check_oracle:
         # the oracle on the smallest requests of the pass, as many as fit
@@ -845,6 +853,9 @@ def main():
     ap.add_argument("--no-incremental", action="store_true")
     ap.add_argument("--incremental-iterations", type=int, default=5)
     ap.add_argument("--refine-steps", type=int, default=3)
+    ap.add_argument("--refine-tolerance", type=float, default=1e-6,
+                    help="mixed solves: refinement stops once a round's largest correction is this fraction "
+                         "of the step's largest entry (the library's default is 1e-13)")
     ap.add_argument("--batch-count", type=int, default=64)
     ap.add_argument("--office-batch", type=int, default=8)
     ap.add_argument("--office-batch-warmup", type=int, default=8)

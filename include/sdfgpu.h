@@ -248,6 +248,12 @@ typedef struct sdfgpu_solver_options {
   int32_t num_threads; /* accepted for interface parity; unused on the GPU */
   int32_t precision;   /* SDFGPU_PRECISION_* */
   int32_t refine_steps; /* MIXED: refinement rounds per LM step (0..16) */
+  /* MIXED: a step's refinement stops once its largest correction is at
+   * most this fraction of its largest entry ([0, 1); default 1e-13, where
+   * the refined step agrees with the FP64 path's to its own rounding). The
+   * step's error after the last round is about this fraction times the
+   * error reduction of one round (cond(A) * 2^-24). */
+  double refine_tolerance;
 } sdfgpu_solver_options;
 
 typedef struct sdfgpu_solve_result {
@@ -314,7 +320,11 @@ int sdfgpu_last_profile(sdfgpu_problem* problem, double* phases);
  * int32, may be NULL) receives the chosen one, factor_ms (may be NULL) its
  * factorization time; trials (may be NULL) receives up to max_trials rows
  * of 4 doubles (small_pivots, front_rows, panel_rows, ms). Returns the
- * number of candidates timed in *num_trials when not NULL. */
+ * number of candidates timed in *num_trials when not NULL. When the
+ * handle's last solve was MIXED, the autotuner then times that solve's
+ * factorization and refined triangular solves under the chosen schedule
+ * with and without the tensor-core Schur complements of the wide FP32
+ * fronts and keeps the faster (sdfgpu_tensor_core_choice). */
 int sdfgpu_autotune(sdfgpu_problem* problem, int32_t* schedule, double* factor_ms, double* trials,
                     int32_t max_trials, int32_t* num_trials);
 
@@ -324,6 +334,19 @@ int sdfgpu_autotune(sdfgpu_problem* problem, int32_t* schedule, double* factor_m
  * by hand). small_pivots 32..128, front_rows 128..256, panel_rows 0 (whole
  * outer blocks) or 16..128; SDFGPU_ERR_INVALID_ARGUMENT otherwise. */
 int sdfgpu_set_schedule(sdfgpu_problem* problem, const int32_t* schedule);
+
+/* The autotuner's tensor-core choice for mixed solves (no counterpart in
+ * the reference): *min_rows receives the number of rows below the pivot
+ * block from which a FP32 front's Schur complement runs on the tensor cores
+ * (0: none does; 256 until an autotune of a mixed handle decides), ms_with
+ * and ms_without (may be NULL) the mixed factor + solve times the last such
+ * autotune measured (0 when it did not time that variant). */
+int sdfgpu_tensor_core_choice(sdfgpu_problem* problem, int32_t* min_rows, double* ms_with, double* ms_without);
+
+/* Installs that choice by hand (no counterpart in the reference): min_rows
+ * 0 (no tensor-core Schur complements) or 128..65536; kept across pattern
+ * re-analyses and schedule changes; SDFGPU_ERR_INVALID_ARGUMENT otherwise. */
+int sdfgpu_set_tensor_core_choice(sdfgpu_problem* problem, int32_t min_rows);
 
 /* ----------------------------------------------------------- incremental --
  * Run in incremental mode (src/pipeline/runner.cpp:226-285, without its file

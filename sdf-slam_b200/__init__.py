@@ -128,6 +128,7 @@ class SolverOptions:
     num_threads: int = 0
     precision: str = "fp64"
     refine_steps: int = 3
+    refine_tolerance: float = 1e-13
 
     def to_c(self) -> _capi.SolverOptionsC:
         if self.backend != "gpu":
@@ -138,7 +139,8 @@ class SolverOptions:
         return _capi.SolverOptionsC(int(self.max_iterations), self.step_tolerance, self.lambda_init,
                                     self.lambda_factor, int(self.reject_worse_steps),
                                     int(self.marquardt_scaling), int(self.trust_region),
-                                    int(self.num_threads), prec, int(self.refine_steps))
+                                    int(self.num_threads), prec, int(self.refine_steps),
+                                    float(self.refine_tolerance))
 
 
 @dataclass
@@ -386,6 +388,25 @@ class Problem:
         _check(lib().sdfgpu_autotune(self._h, sched, ctypes.byref(best), _d(trials), 16, ctypes.byref(n)))
         return {"schedule": tuple(int(v) for v in sched), "factor_ms": best.value,
                 "trials": [tuple(r) for r in trials[:n.value]]}
+
+    def tensor_core_choice(self) -> dict:
+        """The autotuner's tensor-core choice for mixed solves
+        (sdfgpu_tensor_core_choice): {"min_rows": rows below the pivot block
+        from which a FP32 front's Schur complement runs on the tensor cores
+        (0: none), "ms_with": ..., "ms_without": ...} (mixed factor + solve
+        times of the last autotune of a mixed handle, 0 when not timed)."""
+        rows = ctypes.c_int32()
+        w = ctypes.c_double()
+        wo = ctypes.c_double()
+        _check(lib().sdfgpu_tensor_core_choice(self._h, ctypes.byref(rows), ctypes.byref(w), ctypes.byref(wo)))
+        return {"min_rows": rows.value, "ms_with": w.value, "ms_without": wo.value}
+
+    def set_tensor_core_choice(self, min_rows: int):
+        """Installs the tensor-core choice of mixed solves by hand
+        (sdfgpu_set_tensor_core_choice): 0 for none, else the rows below the
+        pivot block from which a FP32 front's Schur complement runs on the
+        tensor cores."""
+        _check(lib().sdfgpu_set_tensor_core_choice(self._h, int(min_rows)))
 
     def set_schedule(self, small_pivots: int, front_rows: int, panel_rows: int):
         """Installs a factorization schedule for this handle's later solves

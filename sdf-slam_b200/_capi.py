@@ -64,6 +64,7 @@ class SolverOptionsC(ctypes.Structure):
         ("trust_region", ctypes.c_int32), ("num_threads", ctypes.c_int32),
         ("precision", ctypes.c_int32),
         ("refine_steps", ctypes.c_int32),
+        ("refine_tolerance", ctypes.c_double),
     ]
 
 
@@ -142,6 +143,9 @@ SIGNATURES = {
                                                 c_int_p, c_int_p, c_dbl_p, c_dbl_p, c_dbl_p]),
     "sdfgpu_last_profile": (ctypes.c_int, [vp, c_dbl_p]),
     "sdfgpu_set_schedule": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int32)]),
+    "sdfgpu_set_tensor_core_choice": (ctypes.c_int, [vp, ctypes.c_int32]),
+    "sdfgpu_tensor_core_choice": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_double),
+                                                 ctypes.POINTER(ctypes.c_double)]),
     "sdfgpu_autotune": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int32), c_dbl_p, c_dbl_p, ctypes.c_int32,
                                        ctypes.POINTER(ctypes.c_int32)]),
     "sdfgpu_run_incremental": (ctypes.c_int, [ctypes.POINTER(IncrementalDesc), ctypes.POINTER(ProblemOptionsC),

@@ -138,6 +138,7 @@ void sdfgpu_solver_options_default(sdfgpu_solver_options* o) {
   o->num_threads = 0;
   o->precision = SDFGPU_PRECISION_FP64;
   o->refine_steps = 3;
+  o->refine_tolerance = sdfgpu::kDefaultRefineTol;
 }
 
 // sdfgpu_problem_build and sdfgpu_problem_build_device (on_device: the point
@@ -385,6 +386,9 @@ static void CheckSolverOptions(const sdfgpu_solver_options& o) {
   }
   if (o.refine_steps < 0 || o.refine_steps > 16) {
     sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "refine_steps must lie in [0, 16]");
+  }
+  if (!(o.refine_tolerance >= 0.0 && o.refine_tolerance < 1.0)) {
+    sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "refine_tolerance must lie in [0, 1)");
   }
 }
 
@@ -645,7 +649,36 @@ int sdfgpu_set_schedule(sdfgpu_problem* problem, const int32_t* schedule) {
     if (schedule == nullptr) {
       sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "schedule is NULL");
     }
-    Eng(problem).SetSchedule(sdfgpu::Schedule{schedule[0], schedule[1], schedule[2]});
+    // the tensor-core choice of mixed solves stays as it is
+    sdfgpu::Schedule s = Eng(problem).schedule();
+    s.small_pivots = schedule[0];
+    s.front_rows = schedule[1];
+    s.panel_rows = schedule[2];
+    Eng(problem).SetSchedule(s);
+  });
+}
+
+int sdfgpu_tensor_core_choice(sdfgpu_problem* problem, int32_t* min_rows, double* ms_with, double* ms_without) {
+  return Guard([&] {
+    NeedHandle(min_rows, "min_rows");
+    *min_rows = Eng(problem).schedule().tc_min_rows;
+    if (ms_with != nullptr) {
+      *ms_with = Eng(problem).tc_trial_ms(true);
+    }
+    if (ms_without != nullptr) {
+      *ms_without = Eng(problem).tc_trial_ms(false);
+    }
+  });
+}
+
+int sdfgpu_set_tensor_core_choice(sdfgpu_problem* problem, int32_t min_rows) {
+  return Guard([&] {
+    if (min_rows != 0 && (min_rows < 128 || min_rows > 65536)) {
+      sdfgpu::Fail(SDFGPU_ERR_INVALID_ARGUMENT, "min_rows must be 0 or lie in [128, 65536]");
+    }
+    sdfgpu::Schedule s = Eng(problem).schedule();
+    s.tc_min_rows = min_rows;
+    Eng(problem).SetSchedule(s);
   });
 }
 

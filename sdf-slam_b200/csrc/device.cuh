@@ -34,6 +34,9 @@ struct InstDev {
   int32_t pp_first;
   int32_t num_params;
   int32_t mixed;  // 1: this solve factors the grid supernodes in FP32
+  // mixed: refinement of the step stops once its largest correction is at
+  // most this fraction of its largest entry
+  double refine_tol;
   // cells probed around each point by the cost kernel for kStatusNearEdge
   // (0: no probe)
   int32_t near_cells;

@@ -30,13 +30,13 @@ __global__ void KCostTerms(DeviceView V, double* terms);
 __global__ void KStepTerms(DeviceView V, double* sq, double* pred);
 __global__ void KSegmentPartial(const double* x, const int64_t* seg_begin, const int64_t* seg_end, double* partial);
 __global__ void KSegmentFinal(const double* partial, int num_segments, double* out);
-__global__ void KConvertFronts(DeviceView V, const int32_t* tasks, int chunk);
+__global__ void KConvertFronts(DeviceView V, const int32_t* tasks);
 __global__ void KNormalMatVecMap(DeviceView V, const double* x, double* y);
 __global__ void KNormalMatVecPose(DeviceView V, const double* x, double* y);
 __global__ void KRefineResidual(DeviceView V, const double* y, double* r);
 __global__ void KAddCorrection(DeviceView V, const double* corr);
 __global__ void KRefineReset(DeviceView V);
-__global__ void KRefineCheck(DeviceView V, double tol);
+__global__ void KRefineCheck(DeviceView V);
 void LaunchCellSort(const int32_t* pt_cell, int64_t n, int64_t num_cells, int32_t* keys_a, int32_t* vals_a,
                     int32_t* keys_b, int32_t* vals_b, int32_t* hist, cudaStream_t stream, bool* result_in_a);
 
@@ -108,6 +108,7 @@ void Engine::Init(std::vector<SymPiece>* pieces) {
   h_seg_.Alloc(5 * host_.size());
   h_status_.Alloc(host_.size());
   mixed_.assign(host_.size(), 0);  // plain FP64 until a solve asks otherwise
+  refine_tol_.assign(host_.size(), kDefaultRefineTol);
   AnalyzeAndUpload(pieces, 0);
 }
 
@@ -611,6 +612,7 @@ void Engine::UploadSymbolic() {
     d.pp_first = sym_.pp_first[i];
     d.num_params = host_[i].num_params();
     d.mixed = i < mixed_.size() ? mixed_[i] : 0;
+    d.refine_tol = i < refine_tol_.size() ? refine_tol_[i] : kDefaultRefineTol;
     d.near_cells = i < margin_.size() ? std::max(0, std::min(kNearCells, margin_[i] - 1)) : 0;
   }
   inst_host_ = inst;
@@ -713,16 +715,6 @@ void Engine::RefreshView() {
 void Engine::AllocMixed() {
   amat_.AllocGrowable(static_cast<size_t>(sym_.front_doubles));
   fronts32_.AllocGrowable(static_cast<size_t>(sym_.front_doubles));
-  std::vector<int32_t> tasks;
-  for (size_t s = 0; s < sym_.sn.size(); ++s) {
-    const int64_t total = static_cast<int64_t>(sym_.sn[s].F) * sym_.sn[s].F;
-    for (int64_t b = 0; b < total; b += kConvertChunk) {
-      tasks.push_back(static_cast<int32_t>(s));
-      tasks.push_back(static_cast<int32_t>(b));
-    }
-  }
-  conv_count_ = static_cast<int64_t>(tasks.size() / 2);
-  conv_tasks_.Upload(tasks, stream_);
   res_.Alloc(static_cast<size_t>(std::max(n_, 1)));
   ax_.Alloc(static_cast<size_t>(std::max(n_, 1)));
   corr_.Alloc(static_cast<size_t>(std::max(n_, 1)));
@@ -740,16 +732,20 @@ void Engine::AllocMixed() {
   }
 }
 
-void Engine::SetMode(const std::vector<int32_t>& mixed, int refine_steps) {
-  if (mixed == mixed_ && refine_steps == refine_steps_) {
+void Engine::SetMode(const std::vector<int32_t>& mixed, int refine_steps, const std::vector<double>& refine_tol) {
+  std::vector<double> tol = refine_tol;
+  tol.resize(mixed.size(), kDefaultRefineTol);
+  if (mixed == mixed_ && refine_steps == refine_steps_ && tol == refine_tol_) {
     return;
   }
   CudaCheck(cudaStreamSynchronize(stream_), "mode sync");
   mixed_ = mixed;
   refine_steps_ = refine_steps;
+  refine_tol_ = tol;
   any_mixed_ = std::any_of(mixed_.begin(), mixed_.end(), [](int32_t v) { return v != 0; });
   for (size_t i = 0; i < inst_host_.size(); ++i) {
     inst_host_[i].mixed = mixed_[i];
+    inst_host_[i].refine_tol = refine_tol_[i];
   }
   inst_.Upload(inst_host_, stream_);
   if (any_mixed_) {
@@ -836,11 +832,14 @@ void Engine::LaunchRows() {
                      (total_odom_ > 0 ? 1 : 0) + 1;
 }
 
-void Engine::LaunchNormal() {
+int64_t Engine::ZeroTaskCount() const {
   // the leaf fronts' trailing columns only for an in-place tensor-core
   // Schur complement
-  const int64_t zero_count =
-      V_.tc_schur != 0 ? static_cast<int64_t>(sym_.zero_tasks.size() / 2) : sym_.zero_main;
+  return V_.tc_schur != 0 ? static_cast<int64_t>(sym_.zero_tasks.size() / 2) : sym_.zero_main;
+}
+
+void Engine::LaunchNormal() {
+  const int64_t zero_count = ZeroTaskCount();
   if (zero_count > 0) {
     KZeroFronts<<<static_cast<unsigned>(zero_count), 32 * kZeroCols, 0, stream_>>>(V_, zero_tasks_.get());
     CudaCheck(cudaGetLastError(), "front zeroing");
@@ -925,9 +924,11 @@ FactorPlan Engine::Plan() {
 }
 
 void Engine::LaunchFactor() {
-  if (any_mixed_ && conv_count_ > 0) {
-    // work copies of the assembled fronts (FP32 for mixed grid supernodes)
-    KConvertFronts<<<static_cast<unsigned>(conv_count_), 256, 0, stream_>>>(V_, conv_tasks_.get(), kConvertChunk);
+  const int64_t conv_count = ZeroTaskCount();
+  if (any_mixed_ && conv_count > 0) {
+    // work copies of the assembled fronts (FP32 for mixed grid supernodes),
+    // over the region the zeroing cleared
+    KConvertFronts<<<static_cast<unsigned>(conv_count), 32 * kZeroCols, 0, stream_>>>(V_, zero_tasks_.get());
     CudaCheck(cudaGetLastError(), "convert fronts");
     ++times_.launches;
   }
@@ -942,10 +943,10 @@ void Engine::LaunchSolve() {
   // iterative refinement of the mixed instances' steps against the FP64
   // normal matrix: r = rhs - A delta, delta += (LDL^T)^-1 r
   // A round stops counting for an instance once its largest correction is
-  // below kRefineTol of its largest step entry: each round shrinks the
-  // error by about cond(A) * 2^-24, so the next one would move the step by
-  // far less than the FP64 path's own rounding differences.
-  constexpr double kRefineTol = 1e-13;
+  // below its refine_tol times its largest step entry: each round shrinks
+  // the error by about cond(A) * 2^-24, so the next one would move the step
+  // by a small fraction of that (the default, 1e-13, by far less than the
+  // FP64 path's own rounding differences).
   DeviceView Vm = V_;
   Vm.refine_done = refine_done_.get();
   Vm.refine_max = refine_max_.get();
@@ -958,13 +959,13 @@ void Engine::LaunchSolve() {
     ++times_.launches;
   }
   for (int round = 0; round < refine_steps_; ++round) {
-    KNormalMatVecMap<<<Blocks(n_, 128), 128, 0, stream_>>>(Vm, step_.get(), ax_.get());
+    KNormalMatVecMap<<<Blocks(32 * static_cast<int64_t>(n_), 256), 256, 0, stream_>>>(Vm, step_.get(), ax_.get());
     KNormalMatVecPose<<<Blocks(3 * static_cast<int64_t>(total_frames_) * 32, 256), 256, 0, stream_>>>(
         Vm, step_.get(), ax_.get());
     KRefineResidual<<<Blocks(n_, 256), 256, 0, stream_>>>(Vm, ax_.get(), res_.get());
     times_.launches += 3 + LaunchSolveLevels(sym_, Vr, Plan(), stream_);
     KAddCorrection<<<Blocks(n_, 256), 256, 0, stream_>>>(Vm, corr_.get());
-    KRefineCheck<<<1, 256, 0, stream_>>>(Vm, kRefineTol);
+    KRefineCheck<<<1, 256, 0, stream_>>>(Vm);
     times_.launches += 2;
   }
   CudaCheck(cudaGetLastError(), "refinement kernels");
@@ -1096,12 +1097,19 @@ double Engine::Autotune(std::vector<std::pair<Schedule, double>>* trials) {
   const std::vector<Schedule> candidates = {{128, 256, 128}, {128, 128, 128}, {96, 256, 128}, {64, 256, 128},
                                             {64, 128, 64},   {128, 256, 64},  {64, 128, 0},   {128, 256, 0}};
   const size_t I = host_.size();
+  // the precision of the last solve: a mixed one also decides whether the
+  // wide FP32 fronts' Schur complements run on the tensor cores
+  const std::vector<int32_t> last_mixed = mixed_;
+  const int last_refine = refine_steps_;
+  const std::vector<double> last_tol = refine_tol_;
+  const bool tune_tc = any_mixed_;
   SetMode(std::vector<int32_t>(I, 0), 0);
   SetActive(std::vector<int32_t>(I, 1));
   SetLambda(std::vector<double>(I, 1.0), std::vector<int32_t>(I, 0));
   double best = 0.0;
   Schedule best_sched = sched_;
-  for (const Schedule& c : candidates) {
+  for (Schedule c : candidates) {
+    c.tc_min_rows = sched_.tc_min_rows;
     Reschedule(sym_, c);
     UploadSchedule();
     double ms_min = 0.0;
@@ -1127,9 +1135,31 @@ double Engine::Autotune(std::vector<std::pair<Schedule, double>>* trials) {
       best_sched = c;
     }
   }
+  if (tune_tc) {
+    // factor + solve (with the refinement rounds the step needs: a less
+    // accurate factor costs rounds) of the last solve's mixed instances,
+    // with and without the tensor-core Schur complements; every front
+    // eligible for them is wide, so one threshold decides
+    SetMode(last_mixed, last_refine, last_tol);
+    double best_mixed = 0.0;
+    tc_trial_ms_[0] = tc_trial_ms_[1] = 0.0;
+    for (const int rows : {kTcMinRowsDefault, 0}) {
+      sched_ = best_sched;
+      sched_.tc_min_rows = rows;
+      InstallSchedule();
+      if (rows > 0 && sym_.tc_pack_rows == 0) {
+        continue;  // no front is wide enough
+      }
+      const double ms = TimeMixedFactorSolve();
+      tc_trial_ms_[rows > 0 ? 0 : 1] = ms;
+      if (best_mixed == 0.0 || ms < best_mixed) {
+        best_mixed = ms;
+        best_sched.tc_min_rows = rows;
+      }
+    }
+  }
   sched_ = best_sched;
-  Reschedule(sym_, sched_);
-  UploadSchedule();
+  InstallSchedule();
   return best;
 }
 
@@ -1140,8 +1170,35 @@ void Engine::SetSchedule(const Schedule& sched) {
          "schedule out of range (small_pivots 32..128, front_rows 128..256, panel_rows 0 or 16..128)");
   }
   sched_ = sched;
+  InstallSchedule();
+}
+
+void Engine::InstallSchedule() {
   Reschedule(sym_, sched_);
   UploadSchedule();
+  // the tensor-core task lists and their operand buffer follow tc_min_rows
+  if (any_mixed_) {
+    AllocMixed();
+  }
+  RefreshView();
+}
+
+double Engine::TimeMixedFactorSolve() {
+  double ms_min = 0.0;
+  for (int rep = 0; rep < 3; ++rep) {
+    ClearStatus();
+    LaunchRows();
+    LaunchNormal();
+    CudaCheck(cudaEventRecord(ev_[0], stream_), "event");
+    LaunchFactor();
+    LaunchSolve();
+    CudaCheck(cudaEventRecord(ev_[1], stream_), "event");
+    CudaCheck(cudaStreamSynchronize(stream_), "autotune");
+    float ms = 0.0f;
+    CudaCheck(cudaEventElapsedTime(&ms, ev_[0], ev_[1]), "autotune timing");
+    ms_min = rep == 0 ? ms : std::min(ms_min, static_cast<double>(ms));
+  }
+  return ms_min;
 }
 
 void Engine::ReanalyzePending() {
@@ -1218,7 +1275,7 @@ void Engine::StepSpeculations() {
         sym_ = std::move(sp->structure);
         const Schedule& now = sched_;
         if (now.small_pivots != sp->sched.small_pivots || now.front_rows != sp->sched.front_rows ||
-            now.panel_rows != sp->sched.panel_rows) {
+            now.panel_rows != sp->sched.panel_rows || now.tc_min_rows != sp->sched.tc_min_rows) {
           Reschedule(sym_, sched_);
         }
         built = true;
@@ -1653,14 +1710,16 @@ void Engine::BeginSolve(const std::vector<sdfgpu_solver_options>& options) {
   const size_t I = host_.size();
   {
     std::vector<int32_t> mixed(I, 0);
+    std::vector<double> tol(I, kDefaultRefineTol);
     int refine = 0;
     for (size_t i = 0; i < I; ++i) {
       if (options[i].precision == SDFGPU_PRECISION_MIXED) {
         mixed[i] = 1;
         refine = std::max(refine, options[i].refine_steps);
+        tol[i] = options[i].refine_tolerance;
       }
     }
-    SetMode(mixed, refine);
+    SetMode(mixed, refine, tol);
   }
   t_start_ = std::chrono::steady_clock::now();
   times_ = IterTimes{};

@@ -325,12 +325,18 @@ class Engine {
   [[nodiscard]] bool IterationReady() const;
   /// Times the factorization of the current state's normal matrix under each
   /// candidate schedule and keeps the fastest (also across re-analyses).
-  /// Returns its time in ms; trials receives every candidate's time.
+  /// When the last solve was mixed, it then times that solve's factor and
+  /// refined solve with and without the tensor-core Schur complements and
+  /// keeps the faster (Schedule::tc_min_rows). Returns the fastest FP64
+  /// factorization time in ms; trials receives every candidate's time.
   double Autotune(std::vector<std::pair<Schedule, double>>* trials);
   /// Installs a factorization schedule (checked against the ranges the
   /// kernels support) for the later solves, also across re-analyses.
   void SetSchedule(const Schedule& sched);
   [[nodiscard]] const Schedule& schedule() const { return sched_; }
+  /// Mixed factor + solve time of the last autotune with (true) or without
+  /// the tensor-core Schur complements, ms (0: not timed).
+  [[nodiscard]] double tc_trial_ms(bool with) const { return tc_trial_ms_[with ? 0 : 1]; }
   [[nodiscard]] const IterTimes& times() const { return times_; }
   [[nodiscard]] int64_t factor_flops() const { return sym_.total_flops; }
   [[nodiscard]] const Symbolic& symbolic() const { return sym_; }
@@ -357,11 +363,14 @@ class Engine {
   Symbolic GlobalStructure();
   void UploadSymbolic();
   void UploadSchedule();
+  void InstallSchedule();          // sched_ into the structure, task lists and view
+  double TimeMixedFactorSolve();   // fastest of three mixed factor + solve runs, ms
   /// The one-launch solve's task list and its scratch.
   void UploadSolveTasks(cudaStream_t s);
   /// Per-instance precision of the coming solve (1: mixed) and refinement
   /// rounds; re-uploads flags and drops the graphs when they change.
-  void SetMode(const std::vector<int32_t>& mixed, int refine_steps);
+  // refine_tol: per instance (missing entries: kDefaultRefineTol)
+  void SetMode(const std::vector<int32_t>& mixed, int refine_steps, const std::vector<double>& refine_tol = {});
   void AllocMixed();
   void RefreshView();
   void SetActive(const std::vector<int32_t>& active);
@@ -369,6 +378,7 @@ class Engine {
   void ClearStatus();
   std::vector<int32_t> DownloadStatus();
   void LaunchRows();
+  int64_t ZeroTaskCount() const;  // front-clearing (and conversion) tasks of this iteration
   void LaunchNormal();
   void LaunchFactor();
   void LaunchSolve();
@@ -430,6 +440,7 @@ class Engine {
   std::vector<int64_t> iters_;     // per instance: iterations launched with it active, over the engine's life
   std::vector<int64_t> analysed_at_;  // per instance: iters_ at its last analysis
   Schedule sched_;                 // factorization schedule (autotuned or default)
+  double tc_trial_ms_[2]{0.0, 0.0};
   Symbolic sym_;
   cudaStream_t stream_{nullptr};
   cudaEvent_t ev_[6]{};
@@ -497,13 +508,10 @@ class Engine {
   DevBuf<double> ys_, zpart_;
   DevBuf<int32_t> inv_tasks_;     // diagonal blocks of L and their inverses
   DevBuf<double> inv_;
-  // mixed precision: assembled FP64 normal matrix, FP32 work fronts, the
-  // conversion tasks and the refinement vectors
-  static constexpr int kConvertChunk = 16384;
+  // mixed precision: assembled FP64 normal matrix, FP32 work fronts and the
+  // refinement vectors (the conversion runs over zero_tasks_)
   DevBuf<double> amat_;
   DevBuf<float> fronts32_;
-  DevBuf<int32_t> conv_tasks_;
-  int64_t conv_count_{0};
   DevBuf<double> res_, ax_, corr_;
   DevBuf<int32_t> refine_done_, refine_left_;
   DevBuf<unsigned long long> refine_max_;
@@ -522,6 +530,7 @@ class Engine {
   DevBuf<int32_t> fmp_col_;
   std::vector<int32_t> mixed_;
   int refine_steps_{0};
+  std::vector<double> refine_tol_;
   bool any_mixed_{false};
   std::vector<InstDev> inst_host_;
   int32_t* cell_rows_ptr_{nullptr};

@@ -216,6 +216,10 @@ constexpr int32_t UpdateCodeInner(int panel) { return -2 - 2 * panel; }
 constexpr int32_t UpdateCodeOuter(int block) { return -3 - 2 * block; }
 /// Columns per task of the front clearing (one warp each).
 constexpr int kZeroCols = 8;
+/// Fronts with at least this many rows below the pivot block take the
+/// tensor-core Schur update in a mixed solve unless the autotuner measured
+/// the SIMT tiles faster (Schedule::tc_min_rows).
+constexpr int kTcMinRowsDefault = 256;
 /// Tile edge of the tiled dense-root factorization.
 constexpr int kDenseTileCols = 64;
 /// One task of the tiled factorization of a dense root: FACTOR (i == j ==
@@ -337,6 +341,9 @@ struct Symbolic {
   int small_pivots{128};
   int front_rows{256};
   int panel_rows{128};
+  // mixed solves: fronts with at least tc_min_rows rows below the pivot
+  // block take the tensor-core Schur update (0: none does)
+  int tc_min_rows{kTcMinRowsDefault};
   std::vector<int> height;                   // per supernode: height in the assembly tree
   // (sn, panel) of every 32-column diagonal block, in panel_base order: the
   // inverted unit triangles the solve multiplies by
@@ -408,6 +415,8 @@ struct SymPiece {
 /// for a batch, so that a problem follows the same steps alone and in a
 /// batch.
 constexpr int kDefaultMargin = 7;
+/// Default refine_tolerance of mixed solves (sdfgpu_solver_options).
+constexpr double kDefaultRefineTol = 1e-13;
 /// Growth of the dilation at each re-analysis, and its cap.
 constexpr int kMarginStep = 2;
 constexpr int kMaxMargin = 9;
@@ -449,6 +458,7 @@ struct Schedule {
   int small_pivots{128};
   int front_rows{256};
   int panel_rows{128};
+  int tc_min_rows{kTcMinRowsDefault};
 };
 
 /// Global structure (task lists, level schedule) of pieces laid out by

@@ -14,24 +14,32 @@
 namespace sdfgpu {
 
 /// Copies the assembled FP64 fronts into the factorization work fronts: FP32
-/// for a mixed solve's grid supernodes, FP64 otherwise. Task (sn, first
-/// entry) covers kConvertChunk entries of one front.
-__global__ void KConvertFronts(DeviceView V, const int32_t* tasks, int chunk) {
+/// for a mixed solve's grid supernodes, FP64 otherwise. It copies exactly
+/// the entries KZeroFronts clears before assembly, with the same tasks (sn,
+/// first of kZeroCols columns; one warp per column, rows c..F-1): the lower
+/// triangles, and the leaf fronts' trailing columns only when a tensor-core
+/// Schur complement is computed in place. No factor kernel reads a work
+/// front's entry outside that region before writing it, as on the plain
+/// path, where the work fronts are the assembled ones.
+__global__ void KConvertFronts(DeviceView V, const int32_t* tasks) {
   const int32_t* t = tasks + 2 * static_cast<int64_t>(blockIdx.x);
   const SupernodeRec S = V.sn[t[0]];
-  const int64_t total = static_cast<int64_t>(S.F) * S.F;
-  const int64_t b = t[1];
-  const int64_t e = min(total, b + chunk);
-  const double* src = V.asm_fronts + S.front_off;
+  const int c = t[1] + static_cast<int>(threadIdx.x >> 5);
+  const int lane = static_cast<int>(threadIdx.x & 31);
+  if (c >= S.F) {
+    return;
+  }
+  const int64_t col = S.front_off + static_cast<int64_t>(c) * S.F;
+  const double* src = V.asm_fronts + col;
   if (Fp32Front(V, S)) {
-    float* dst = V.fronts32 + S.front_off;
-    for (int64_t q = b + threadIdx.x; q < e; q += blockDim.x) {
-      dst[q] = static_cast<float>(src[q]);
+    float* dst = V.fronts32 + col;
+    for (int r = c + lane; r < S.F; r += 32) {
+      dst[r] = static_cast<float>(src[r]);
     }
   } else {
-    double* dst = V.fronts + S.front_off;
-    for (int64_t q = b + threadIdx.x; q < e; q += blockDim.x) {
-      dst[q] = src[q];
+    double* dst = V.fronts + col;
+    for (int r = c + lane; r < S.F; r += 32) {
+      dst[r] = src[r];
     }
   }
 }
@@ -53,11 +61,11 @@ __global__ void KRefineReset(DeviceView V) {
   }
 }
 
-/// After a round: an instance whose largest correction is at most `tol`
-/// times its largest step entry is done (the next round would change its
-/// step by a fraction of that); the maxima restart and refine_left says
-/// whether any mixed instance still refines. One block.
-__global__ void KRefineCheck(DeviceView V, double tol) {
+/// After a round: an instance whose largest correction is at most its
+/// refine_tol times its largest step entry is done (the next round would
+/// change its step by a fraction of that); the maxima restart and
+/// refine_left says whether any mixed instance still refines. One block.
+__global__ void KRefineCheck(DeviceView V) {
   __shared__ int left;
   if (threadIdx.x == 0) {
     left = 0;
@@ -66,7 +74,7 @@ __global__ void KRefineCheck(DeviceView V, double tol) {
   for (int i = threadIdx.x; i < V.num_inst; i += blockDim.x) {
     const double mc = __longlong_as_double(static_cast<long long>(V.refine_max[2 * i]));
     const double ms = __longlong_as_double(static_cast<long long>(V.refine_max[2 * i + 1]));
-    if (V.refine_done[i] == 0 && mc <= tol * ms) {
+    if (V.refine_done[i] == 0 && mc <= V.inst[i].refine_tol * ms) {
       V.refine_done[i] = 1;
     }
     V.refine_max[2 * i] = 0ull;
@@ -83,13 +91,17 @@ __global__ void KRefineCheck(DeviceView V, double tol) {
 
 /// y = A x over the map columns of mixed instances (natural order), A read
 /// in FP64 from the assembled fronts: the 9-point map stencil (mm_off) and
-/// the node's map-pose blocks (mp_*). One thread per column; every sum runs
-/// in a fixed order.
+/// the node's map-pose blocks (mp_*). One warp per column: lanes 0-8 take
+/// one stencil slot each, then the lanes stride over the column's coupled
+/// frames (a node of a revisited area couples to hundreds of frames), and a
+/// fixed butterfly sums the lanes, so every sum runs in a fixed order.
 __global__ void KNormalMatVecMap(DeviceView V, const double* x, double* y) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= V.n) {
+  const int64_t wid = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (wid >= V.n) {
     return;
   }
+  const int c = static_cast<int>(wid);
   const int node = V.col_node[c];
   if (node < 0) {
     return;
@@ -102,33 +114,37 @@ __global__ void KNormalMatVecMap(DeviceView V, const double* x, double* y) {
   const double* A = V.asm_fronts;
   const int pose0 = I.col_off + I.num_active;
   double acc = 0.0;
-  const int64_t ln = node - I.node_off;
-  const int w = static_cast<int>(ln % I.nx);
-  const int h = static_cast<int>(ln / I.nx);
-  for (int slot = 0; slot < 9; ++slot) {
-    const int dh = slot / 3 - 1;
-    const int dw = slot % 3 - 1;
-    if (w + dw < 0 || w + dw >= I.nx || h + dh < 0 || h + dh >= I.ny) {
-      continue;
-    }
-    const int c2 = V.node_col[node + static_cast<int64_t>(dh) * I.nx + dw];
-    if (c2 < 0) {
-      continue;
-    }
-    int64_t off = V.mm_off[static_cast<int64_t>(c) * 9 + slot];
-    if (off < 0) {
-      off = V.mm_off[static_cast<int64_t>(c2) * 9 + (8 - slot)];
-    }
-    if (off >= 0) {
-      acc += A[off] * x[c2];
+  if (lane < 9) {
+    const int64_t ln = node - I.node_off;
+    const int w = static_cast<int>(ln % I.nx);
+    const int h = static_cast<int>(ln / I.nx);
+    const int dh = lane / 3 - 1;
+    const int dw = lane % 3 - 1;
+    if (w + dw >= 0 && w + dw < I.nx && h + dh >= 0 && h + dh < I.ny) {
+      const int c2 = V.node_col[node + static_cast<int64_t>(dh) * I.nx + dw];
+      if (c2 >= 0) {
+        int64_t off = V.mm_off[static_cast<int64_t>(c) * 9 + lane];
+        if (off < 0) {
+          off = V.mm_off[static_cast<int64_t>(c2) * 9 + (8 - lane)];
+        }
+        if (off >= 0) {
+          acc = A[off] * x[c2];
+        }
+      }
     }
   }
-  for (int64_t e = V.mp_ptr[c]; e < V.mp_ptr[c + 1]; ++e) {
+  for (int64_t e = V.mp_ptr[c] + lane; e < V.mp_ptr[c + 1]; e += 32) {
     const int64_t off = V.mp_off[e];
     const int pc = pose0 + 3 * (V.mp_frame[e] - 1);
     acc += A[off] * x[pc] + A[off + 1] * x[pc + 1] + A[off + 2] * x[pc + 2];
   }
-  y[c] = acc;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  }
+  if (lane == 0) {
+    y[c] = acc;
+  }
 }
 
 /// y = A x over the pose columns of mixed instances: one warp per pose

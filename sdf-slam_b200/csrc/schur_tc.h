@@ -16,9 +16,6 @@ namespace sdfgpu {
 /// swizzle row) of the tensor-core Schur kernels.
 constexpr int kTcTile = 128;
 constexpr int kTcChunk = 32;
-/// Fronts with at least this many rows below the pivot block take the
-/// tensor-core Schur update in a mixed solve (narrower ones the SIMT tiles).
-constexpr int kTcMinRows = 256;
 
 /// What the tensor-core kernels read: supernodes, FP32 work fronts, D, the
 /// per-instance running / precision flags, the status words and the packed

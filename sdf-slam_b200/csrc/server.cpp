@@ -63,7 +63,8 @@ Server::~Server() {
 int64_t Server::Submit(HostProblem hp, const sdfgpu_solver_options& options) {
   if (options.max_iterations < 0 || !(options.lambda_init >= 0.0) || !(options.lambda_factor > 0.0) ||
       (options.precision != SDFGPU_PRECISION_FP64 && options.precision != SDFGPU_PRECISION_MIXED) ||
-      options.refine_steps < 0 || options.refine_steps > 16) {
+      options.refine_steps < 0 || options.refine_steps > 16 ||
+      !(options.refine_tolerance >= 0.0 && options.refine_tolerance < 1.0)) {
     Fail(SDFGPU_ERR_INVALID_ARGUMENT, "invalid solver options");
   }
   // the analysis that sizes the request is the one its engine will use

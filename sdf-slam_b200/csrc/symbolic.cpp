@@ -691,7 +691,7 @@ void Finalize(Symbolic& S, const std::vector<int>& height, int panel_width, int 
     for (int q = qb; q < qe; ++q) {
       const int s = S.level_sn[static_cast<size_t>(q)];
       SupernodeRec& r = S.sn[static_cast<size_t>(s)];
-      if (r.pose_root != 0 || r.nrows < kTcMinRows || r.ncols < 1) {
+      if (r.pose_root != 0 || S.tc_min_rows <= 0 || r.nrows < S.tc_min_rows || r.ncols < 1) {
         continue;
       }
       r.tc_pack = rows;
@@ -1369,6 +1369,7 @@ Symbolic Concatenate(const std::vector<SymPiece>& pieces, const std::vector<Inst
   S.small_pivots = sched.small_pivots;
   S.front_rows = sched.front_rows;
   S.panel_rows = sched.panel_rows;
+  S.tc_min_rows = sched.tc_min_rows;
   const size_t I = pieces.size();
   // where each instance's part starts in every global array (a prefix pass),
   // then the parts are copied and rebased in parallel
@@ -1494,6 +1495,7 @@ Symbolic ConcatenateOne(SymPiece&& piece, int panel_width, int tile, const Sched
   S.small_pivots = sched.small_pivots;
   S.front_rows = sched.front_rows;
   S.panel_rows = sched.panel_rows;
+  S.tc_min_rows = sched.tc_min_rows;
   for (SupernodeRec& r : S.sn) {
     r.instance = 0;
   }
@@ -1505,6 +1507,7 @@ void Reschedule(Symbolic& S, const Schedule& sched) {
   S.small_pivots = sched.small_pivots;
   S.front_rows = sched.front_rows;
   S.panel_rows = sched.panel_rows;
+  S.tc_min_rows = sched.tc_min_rows;
   S.ea_tasks.clear();
   S.ea_child.clear();
   S.panel_tasks.clear();

@@ -173,3 +173,79 @@ def _floorplan_oracle_three():
         om, op = orc.state()
         _ORACLE_CACHE["floorplan3"] = {"cost_history": ro["cost_history"], "poses": op, "map": om}
     return _ORACLE_CACHE["floorplan3"]
+
+
+@pytest.fixture(scope="module")
+def floorplan_oracle10():
+    specs = scene_specs(scenes.floorplan_scene(seed=1))[0]
+    orc = oracle_from_specs(specs)
+    ro = orc.solve(max_iterations=10, step_tolerance=0.0, num_threads=0)
+    return specs, np.array(ro["cost_history"]), orc.state()
+
+
+@pytest.mark.parametrize("tc_rows", [256, 0])
+def test_floorplan_mixed_follows_oracle_with_and_without_tensor_cores(tc_rows, floorplan_oracle10):
+    """Ten mixed LM iterations of the floor plan from the scene's start,
+    with the wide FP32 fronts' Schur complements on the tensor cores (256)
+    and on the SIMT tiles (0), refinement stopped once a round corrects
+    less than 1e-6 of the step: the cost history stays within 1e-8 of the
+    FP64 oracle's and the poses within 1e-4 m (the mixed path's contract)."""
+    specs, ho, (om, op) = floorplan_oracle10
+    gpu = P.Problem.from_specs(specs)
+    gpu.set_tensor_core_choice(tc_rows)
+    assert gpu.tensor_core_choice()["min_rows"] == tc_rows
+    rg = P.solve(gpu, P.SolverOptions(max_iterations=10, step_tolerance=0.0, precision="mixed",
+                                      refine_tolerance=1e-6))
+    assert rg.status == 0
+    hg = np.array(rg.cost_history)
+    assert hg.shape == ho.shape
+    assert np.max(np.abs(hg - ho) / np.abs(ho)) <= 1e-8
+    gm, gp = gpu.state()
+    print(f"floor plan mixed tc_rows={tc_rows}: cost history {np.max(np.abs(hg - ho) / np.abs(ho)):.3e}, "
+          f"poses {np.max(np.abs(gp[:, :2] - op[:, :2])):.3e} m")
+    assert np.max(np.abs(gp[:, :2] - op[:, :2])) <= 1e-4
+    assert np.max(np.abs(gm - om)) <= 1e-4
+    gpu.close()
+
+
+def test_autotune_after_mixed_solve_picks_tensor_core_choice(floorplan_oracle10):
+    """An autotune after a mixed solve times the mixed factor + refined solve
+    with and without the tensor-core Schur complements and keeps the faster;
+    the next mixed iteration from a saved state still agrees with the FP64
+    iteration from that state to 1e-9 of the step."""
+    specs = floorplan_oracle10[0]
+    gpu = P.Problem.from_specs(specs)
+    P.solve(gpu, P.SolverOptions(max_iterations=2, step_tolerance=0.0, precision="mixed"))
+    gpu.autotune()
+    choice = gpu.tensor_core_choice()
+    assert choice["min_rows"] in (0, 256)
+    assert choice["ms_with"] > 0.0 and choice["ms_without"] > 0.0
+    assert choice["min_rows"] == (256 if choice["ms_with"] <= choice["ms_without"] else 0)
+    m0, p0 = gpu.state()
+    ref = P.Problem.from_specs(specs)
+    ref.set_state(m0, p0)
+    P.solve(ref, P.SolverOptions(max_iterations=1, step_tolerance=0.0))
+    m64, p64 = ref.state()
+    step = max(np.max(np.abs(m64 - m0)), np.max(np.abs(p64 - p0)))
+    P.solve(gpu, P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision="mixed"))
+    gm, gp = gpu.state()
+    assert max(np.max(np.abs(gm - m64)), np.max(np.abs(gp - p64))) <= 1e-9 * step
+    # the choice stays when the schedule is set by hand
+    gpu.set_schedule(64, 128, 64)
+    assert gpu.tensor_core_choice()["min_rows"] == choice["min_rows"]
+    gpu.close()
+    ref.close()
+
+
+def test_mixed_option_ranges():
+    """refine_tolerance outside [0, 1) and a tensor-core row threshold
+    outside {0} and [128, 65536] are refused with the reason."""
+    specs = scene_specs(scenes.room_scene(seed=0))[0]
+    gpu = P.Problem.from_specs(specs)
+    for tol in (-1e-3, 1.0, float("nan")):
+        with pytest.raises(ValueError, match="refine_tolerance"):
+            P.solve(gpu, P.SolverOptions(max_iterations=1, precision="mixed", refine_tolerance=tol))
+    for rows in (5, 127, 70000):
+        with pytest.raises(ValueError, match="min_rows"):
+            gpu.set_tensor_core_choice(rows)
+    gpu.close()
