@@ -300,6 +300,8 @@ def run_profile(args):
     scene = make_scene(scenes, args.workload, args.seed if args.seed is not None else SEEDS[args.workload])
     specs = scene_specs(P, scene)
     gpu = P.Problem.from_specs(specs)
+    if args.tensor_core_min_rows is not None:
+        gpu.set_tensor_core_choice(args.tensor_core_min_rows)
     opts = P.SolverOptions(max_iterations=1, step_tolerance=0.0, precision=args.precision,
                            refine_steps=args.refine_steps, refine_tolerance=args.refine_tolerance)
     for it in range(args.profile):
@@ -853,6 +855,8 @@ def main():
     ap.add_argument("--no-incremental", action="store_true")
     ap.add_argument("--incremental-iterations", type=int, default=5)
     ap.add_argument("--refine-steps", type=int, default=3)
+    ap.add_argument("--tensor-core-min-rows", type=int, default=None,
+                    help="--profile runs: the tensor-core Schur choice of mixed solves (0: none)")
     ap.add_argument("--refine-tolerance", type=float, default=1e-6,
                     help="mixed solves: refinement stops once a round's largest correction is this fraction "
                          "of the step's largest entry (the library's default is 1e-13)")

@@ -1038,8 +1038,8 @@ __global__ void __launch_bounds__(256, 2) KUpdate(DeviceView V, const int32_t* t
   if (V.active[S.instance] == 0) {
     return;
   }
-  if (t[1] == -1 && (!Fp32Front(V, S) || (S.tc_pack >= 0 && V.tc_schur != 0))) {
-    return;  // FP64 Schur tiles: KSchur; wide FP32 fronts: the tensor cores
+  if (t[1] == -1) {
+    return;  // Schur tiles: KSchur, KSchurF32; wide FP32 fronts: the tensor cores
   }
   __shared__ double as_buf[kPanel * kTile];
   __shared__ double bs_buf[kPanel * kTile];
@@ -1052,22 +1052,27 @@ __global__ void __launch_bounds__(256, 2) KUpdate(DeviceView V, const int32_t* t
   }
 }
 
-/// FP64 Schur complement tiles added into the parent front (the task list
-/// of the Schur update, panel -1), built for occupancy: the K chunks are
-/// copied global -> shared with cp.async (8-byte copies: a front's columns
-/// start at any 8-byte offset), two chunks in flight, so no staging
-/// registers; each thread then scales the A entries it copied by d (the
-/// same product the register path forms); the tile's current values are
-/// read after the K loop, one column group at a time. Three blocks per SM
-/// (64 KB of shared memory each) against two for KUpdate.
+/// Schur complement tiles added into the parent front (the task list of the
+/// Schur update, panel -1), FP64 fronts and the FP32 fronts of a mixed solve
+/// that the tensor cores do not take, built for occupancy: the K chunks are
+/// copied global -> shared with cp.async (element-sized copies: a front's
+/// columns start at any element offset), two chunks in flight, so no
+/// staging registers; each thread then scales the A entries it copied by d
+/// (the same product the register path forms); the tile's current values
+/// are read after the K loop. Three blocks per SM (64 KB of shared memory
+/// each; an FP32 tile uses half) against two for KUpdate.
 constexpr int kSchurK = 32;
 constexpr int kSchurBlocksPerSm = 3;
 constexpr int kSchurPerThread = kSchurK * 64 / 256;  // entries of a chunk each thread copies
 constexpr size_t kSchurSmem = 2 * 2 * static_cast<size_t>(kSchurK) * 64 * sizeof(double);
 
-__device__ __forceinline__ void CpAsync8(double* dst, const double* src) {
+__device__ __forceinline__ void CpAsync(double* dst, const double* src) {
   const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void CpAsync(float* dst, const float* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
 }
 
 /// The end of a KSchur tile: C - acc added into the parent front (or written
@@ -1113,21 +1118,62 @@ __device__ __forceinline__ void SchurEpilogue(const DeviceView& V, const Superno
   }
 }
 
-__global__ void __launch_bounds__(256, kSchurBlocksPerSm)
-    KSchur(DeviceView V, const int32_t* tasks, const double* dvec) {
-  const int32_t* t = tasks + 4 * static_cast<int64_t>(blockIdx.x);
-  const SupernodeRec S = V.sn[t[0]];
-  if (V.active[S.instance] == 0 || Fp32Front(V, S)) {
-    return;  // FP32 fronts of a mixed solve: KUpdate or the tensor cores
+/// The end of a KSchur tile of an FP32 front (the SIMT Schur complement of
+/// a mixed solve): the tile's values (zero for a leaf, not loaded) minus
+/// acc, added into the parent front Fp (FP32, or the FP64 pose root), or
+/// written in place for a front with no parent (Fp is then the front
+/// itself); one column group of four entries at a time, all parent reads of
+/// a group before its writes; the same roundings as KUpdate's FP32 tiles.
+template <typename TP>
+__device__ __forceinline__ void SchurEpilogueF32(TP* Fp, int64_t PF, const int32_t* rel, const float* Fs, int k,
+                                                 int F, int r0, int c0, const float (&acc)[4][4]) {
+  const int tx = threadIdx.x & 15;
+  const int ty = threadIdx.x >> 4;
+  const bool scatter = rel != nullptr;
+  const bool load = k < F && Fs != nullptr;
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int c = c0 + ty + 16 * b;
+    float cur[4];
+    int64_t pos[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int r = r0 + tx + 16 * a;
+      const bool in = c < F && r < F && r >= c;
+      cur[a] = (load && in) ? Fs[static_cast<int64_t>(c) * F + r] : 0.0f;
+      pos[a] = !in ? -1
+                   : (scatter ? static_cast<int64_t>(rel[c - k]) * PF + rel[r - k] : static_cast<int64_t>(c) * F + r);
+    }
+    TP old[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      old[a] = (scatter && pos[a] >= 0) ? Fp[pos[a]] : TP(0);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      if (pos[a] >= 0) {
+        const float v = cur[a] - acc[a][b];
+        Fp[pos[a]] = scatter ? old[a] + static_cast<TP>(v) : static_cast<TP>(v);
+      }
+    }
   }
-  extern __shared__ __align__(16) double schur_sm[];
-  auto As = reinterpret_cast<double(*)[kSchurK][64]>(schur_sm);
-  auto Bs = reinterpret_cast<double(*)[kSchurK][64]>(schur_sm + 2 * kSchurK * 64);
+}
+
+/// One 64 x 64 Schur complement tile of a front held in T (double: the
+/// plain path and the pose root; float: a mixed solve's grid fronts that
+/// the tensor cores do not take): K chunks staged by cp.async, two in
+/// flight, A scaled by d in shared memory, acc accumulated in T in
+/// ascending pivot order.
+template <typename T>
+__device__ __forceinline__ void SchurTile(const DeviceView& V, const SupernodeRec& S, const int32_t* t,
+                                          const double* dvec, T* sm) {
+  auto As = reinterpret_cast<T(*)[kSchurK][64]>(sm);
+  auto Bs = reinterpret_cast<T(*)[kSchurK][64]>(sm + 2 * kSchurK * 64);
   const int k = S.ncols;
   const int F = S.F;
   const int r0 = k + t[2] * 64;
   const int c0 = k + t[3] * 64;
-  double* Fs = V.fronts + S.front_off;
+  T* Fs = WorkFront<T>(V, S);
   const double* d = dvec + S.first_col;
   const int tid = threadIdx.x;
   const int tx = tid & 15;
@@ -1141,24 +1187,24 @@ __global__ void __launch_bounds__(256, kSchurBlocksPerSm)
       const int col = kk + l;
       const int64_t base = static_cast<int64_t>(col) * F;
       if (col < k && r0 + rr < F) {
-        CpAsync8(&As[buf][l][rr], Fs + base + r0 + rr);
+        CpAsync(&As[buf][l][rr], Fs + base + r0 + rr);
       } else {
-        As[buf][l][rr] = 0.0;
+        As[buf][l][rr] = T(0);
       }
       if (col < k && c0 + rr < F) {
-        CpAsync8(&Bs[buf][l][rr], Fs + base + c0 + rr);
+        CpAsync(&Bs[buf][l][rr], Fs + base + c0 + rr);
       } else {
-        Bs[buf][l][rr] = 0.0;
+        Bs[buf][l][rr] = T(0);
       }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  double acc[4][4];
+  T acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
-      acc[a][b] = 0.0;
+      acc[a][b] = T(0);
     }
   }
   const int chunks = (k + kSchurK - 1) / kSchurK;
@@ -1181,14 +1227,14 @@ __global__ void __launch_bounds__(256, kSchurBlocksPerSm)
       const int l = e >> 6;
       const int col = ch * kSchurK + l;
       if (col < k) {
-        As[buf][l][e & 63] *= d[col];
+        As[buf][l][e & 63] *= static_cast<T>(d[col]);
       }
     }
     __syncthreads();
 #pragma unroll 8
     for (int l = 0; l < kSchurK; ++l) {
-      double av[4];
-      double bv[4];
+      T av[4];
+      T bv[4];
 #pragma unroll
       for (int a = 0; a < 4; ++a) {
         av[a] = As[buf][l][tx + 16 * a];
@@ -1207,13 +1253,55 @@ __global__ void __launch_bounds__(256, kSchurBlocksPerSm)
       issue((ch + 2) * kSchurK, buf);
     }
   }
-  // C - acc, added into the parent (or written in place for a front with no
-  // parent); a leaf's C is zero (no child adds into it) and is not loaded
-  if (S.child_count == 0) {
-    SchurEpilogue<false>(V, S, Fs, r0, c0, acc);
+  if constexpr (sizeof(T) == sizeof(double)) {
+    // C - acc, added into the parent (or written in place for a front with
+    // no parent); a leaf's C is zero (no child adds into it) and is not
+    // loaded
+    if (S.child_count == 0) {
+      SchurEpilogue<false>(V, S, Fs, r0, c0, acc);
+    } else {
+      SchurEpilogue<true>(V, S, Fs, r0, c0, acc);
+    }
   } else {
-    SchurEpilogue<true>(V, S, Fs, r0, c0, acc);
+    // a leaf's C is zero (no child adds into it) and is not loaded
+    const float* C = S.child_count > 0 ? Fs : nullptr;
+    if (S.parent < 0) {
+      SchurEpilogueF32<float>(Fs, F, nullptr, C, k, F, r0, c0, acc);
+    } else {
+      const SupernodeRec P = V.sn[S.parent];
+      const int32_t* rel = V.sn_rel + S.rows_off;
+      if (Fp32Front(V, P)) {
+        SchurEpilogueF32<float>(WorkFront<float>(V, P), P.F, rel, C, k, F, r0, c0, acc);
+      } else {
+        SchurEpilogueF32<double>(WorkFront<double>(V, P), P.F, rel, C, k, F, r0, c0, acc);
+      }
+    }
   }
+}
+
+__global__ void __launch_bounds__(256, kSchurBlocksPerSm)
+    KSchur(DeviceView V, const int32_t* tasks, const double* dvec) {
+  const int32_t* t = tasks + 4 * static_cast<int64_t>(blockIdx.x);
+  const SupernodeRec S = V.sn[t[0]];
+  if (V.active[S.instance] == 0 || Fp32Front(V, S)) {
+    return;  // FP32 fronts of a mixed solve: KSchurF32 or the tensor cores
+  }
+  extern __shared__ __align__(16) double schur_sm[];
+  SchurTile<double>(V, S, t, dvec, schur_sm);
+}
+
+/// The same tiles for the FP32 fronts of a mixed solve that the tensor
+/// cores do not take (a kernel of its own, so that neither variant's
+/// registers limit the other's).
+__global__ void __launch_bounds__(256, kSchurBlocksPerSm)
+    KSchurF32(DeviceView V, const int32_t* tasks, const double* dvec) {
+  const int32_t* t = tasks + 4 * static_cast<int64_t>(blockIdx.x);
+  const SupernodeRec S = V.sn[t[0]];
+  if (V.active[S.instance] == 0 || !Fp32Front(V, S) || (S.tc_pack >= 0 && V.tc_schur != 0)) {
+    return;
+  }
+  extern __shared__ __align__(16) double schur_sm[];
+  SchurTile<float>(V, S, t, dvec, reinterpret_cast<float*>(schur_sm));
 }
 
 template <typename T>
@@ -2644,7 +2732,8 @@ int LaunchFactorLevels(const Symbolic& S, const DeviceView& V, const FactorPlan&
       ++launches;
       if (P.fp32_fronts) {
         // the FP32 fronts of a mixed solve that the tensor cores do not take
-        KUpdate<<<static_cast<unsigned>(sr.count), 256, 0, stream>>>(V, P.update_tasks + 4 * sr.begin, P.dvec);
+        KSchurF32<<<static_cast<unsigned>(sr.count), 256, kSchurSmem / 2, stream>>>(
+            V, P.update_tasks + 4 * sr.begin, P.dvec);
         ++launches;
       }
     }
