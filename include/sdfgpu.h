@@ -36,8 +36,9 @@ extern "C" {
 /* Precision of a solve. FP64 runs every step in double precision (the plain
  * path that matches the reference). MIXED factors the grid supernodes in
  * FP32 (the dense pose-block root stays FP64) and recovers the FP64 step by
- * refine_steps rounds of iterative refinement against the FP64 normal
- * matrix; residuals, J^T J, cost, gain ratio and acceptance stay FP64. */
+ * up to refine_steps rounds of iterative refinement against the FP64 normal
+ * matrix, stopping once a round's correction falls below refine_tolerance;
+ * residuals, J^T J, cost, gain ratio and acceptance stay FP64. */
 #define SDFGPU_PRECISION_FP64 0
 #define SDFGPU_PRECISION_MIXED 1
 

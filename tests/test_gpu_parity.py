@@ -365,6 +365,32 @@ def test_mixed_and_plain_instances_in_one_batch():
     assert np.max(np.abs(bp[:, :2] - pp[:, :2])) <= 1e-4
 
 
+def test_mixed_instances_with_their_own_refinement_tolerances_in_one_batch():
+    """Each mixed instance of a batch refines to its own refine_tolerance and
+    ends bitwise where it ends alone; the looser tolerance still keeps the
+    FP64 solve's cost history within 1e-8."""
+    scs = [scenes.room_scene(seed=s, grid=g, frames=f, beams=b)
+           for s, g, f, b in [(32, 44, 9, 120), (33, 48, 11, 150)]]
+    specs = [scene_specs(sc, P.ProblemOptions(hallucination_points=3))[0] for sc in scs]
+    opts = [P.SolverOptions(max_iterations=5, precision="mixed"),
+            P.SolverOptions(max_iterations=5, precision="mixed", refine_tolerance=1e-6)]
+    batch = P.Problem.batch(specs)
+    rb = P.solve(batch, opts)
+    for i in range(2):
+        alone = P.Problem.from_specs(specs[i])
+        ra = P.solve(alone, opts[i])
+        assert rb[i].cost_history == ra.cost_history
+        assert all(np.array_equal(a, b) for a, b in zip(batch.state(i), alone.state()))
+        alone.close()
+    plain = P.Problem.from_specs(specs[1])
+    rp = P.solve(plain, P.SolverOptions(max_iterations=5))
+    hb = np.array(rb[1].cost_history)
+    hp = np.array(rp.cost_history)
+    assert hb.shape == hp.shape and np.max(np.abs(hb - hp) / np.abs(hp)) <= 1e-8
+    plain.close()
+    batch.close()
+
+
 def test_autotuned_schedule_keeps_parity():
     sc = scenes.room_scene(seed=0)
     specs, _ = scene_specs(sc, P.ProblemOptions(hallucination_points=4))
