@@ -214,6 +214,33 @@ def test_batch_matches_individual_solves():
         assert np.array_equal(bm, sm) and np.array_equal(bp, sp)
 
 
+def test_batch_instances_follow_the_oracle():
+    """Every instance of an uneven batch (grids 40-56, 7-14 poses, 90-180
+    beams, one with the active region, one with the trust region) against
+    the CPU oracle's own solve of that instance: cost history within 1e-8,
+    poses within 1e-4 m, iterations and convergence equal."""
+    scs = [scenes.room_scene(seed=s, grid=g, frames=f, beams=b, active_region=a)
+           for s, g, f, b, a in [(40, 40, 10, 180, False), (41, 56, 14, 120, True), (42, 48, 7, 90, False)]]
+    specs = [scene_specs(sc, P.ProblemOptions(hallucination_points=4, active_region=sc.options["active_region"]))[0]
+             for sc in scs]
+    kw = [dict(max_iterations=6), dict(max_iterations=4, trust_region=True), dict(max_iterations=5)]
+    batch = P.Problem.batch(specs)
+    rb = P.solve(batch, [P.SolverOptions(**k) for k in kw])
+    for i, s in enumerate(specs):
+        orc = oracle_from_specs(s)
+        ro = orc.solve(num_threads=4, **kw[i])
+        hb = np.array(rb[i].cost_history)
+        ho = np.array(ro["cost_history"])
+        assert hb.shape == ho.shape
+        assert np.max(np.abs(hb - ho) / np.abs(ho)) <= 1e-8
+        assert rb[i].iterations == ro["iterations"] and bool(rb[i].converged) == bool(ro["converged"])
+        bm, bp = batch.state(i)
+        om, op = orc.state()
+        assert np.max(np.abs(bp[:, :2] - op[:, :2])) <= 1e-4
+        assert np.max(np.abs(bm - om)) <= 1e-4
+    batch.close()
+
+
 def test_state_outside_pattern_reanalyses_only_that_instance():
     # Poses moved by set_state leave the analysed coupling pattern: the cost
     # evaluation that opens the solve sees it and that instance alone is
@@ -408,7 +435,8 @@ def test_autotuned_schedule_keeps_parity():
 
 def test_server_results_equal_alone_and_in_mix():
     """Requests merged into batched cohorts while others run give, each,
-    bitwise the result of their solve alone."""
+    bitwise the result of their solve alone, and follow the CPU oracle's
+    solve of the same request (final cost within 1e-8, poses 1e-4 m)."""
     scs = [scenes.request_scene(seed=100 + i, grid_range=(40, 70), pose_range=(8, 24), iterations=6)
            for i in range(5)]
     specs = [scene_specs(sc, P.ProblemOptions(hallucination_points=4))[0] for sc in scs]
@@ -423,6 +451,12 @@ def test_server_results_equal_alone_and_in_mix():
         assert res.status == 0
         assert res.final_cost == ra.final_cost and res.iterations == ra.iterations
         assert np.array_equal(m, am) and np.array_equal(p, ap)
+        # and the oracle's own solve of the request
+        orc = oracle_from_specs(s)
+        ro = orc.solve(max_iterations=6, num_threads=4)
+        assert rel_err(res.final_cost, ro["final_cost"]) <= 1e-8
+        _, op = orc.state()
+        assert np.max(np.abs(p[:, :2] - op[:, :2])) <= 1e-4
     st = server.stats()
     assert st["completed"] == 5 and st["p99_ms"] >= st["p50_ms"] > 0
     server.close()

@@ -148,3 +148,34 @@ def test_set_schedule_rejects_out_of_range_values():
     sched = (ctypes.c_int32 * 3)(128, 256, 128)
     assert L.sdfgpu_set_schedule(None, sched) == 1
     assert L.sdfgpu_set_schedule(None, None) == 1
+
+
+def test_tensor_core_choice_rejects_bad_arguments_without_a_device():
+    """sdfgpu_set_tensor_core_choice checks min_rows (0, or 128..65536)
+    before it touches the handle; both entry points refuse a NULL handle
+    with SDFGPU_ERR_INVALID_ARGUMENT and say why."""
+    import ctypes
+    from sdf_slam_b200 import _capi
+    L = _capi.load()
+    for rows in (5, 127, 65537, -1):
+        assert L.sdfgpu_set_tensor_core_choice(None, rows) == 1
+        assert b"min_rows" in L.sdfgpu_last_error_message()
+    assert L.sdfgpu_set_tensor_core_choice(None, 0) == 1
+    assert b"problem" in L.sdfgpu_last_error_message()
+    rows = ctypes.c_int32()
+    assert L.sdfgpu_tensor_core_choice(None, ctypes.byref(rows), None, None) == 1
+    assert L.sdfgpu_tensor_core_choice(None, None, None, None) == 1
+
+
+def test_solver_options_default_refine_tolerance():
+    """The C default of refine_tolerance is the Python mirror's (1e-13), and
+    the options struct carries it after refine_steps."""
+    from sdf_slam_b200 import _capi
+    import sdf_slam_b200 as P
+    L = _capi.load()
+    o = _capi.SolverOptionsC()
+    L.sdfgpu_solver_options_default(o)
+    assert o.refine_tolerance == 1e-13 == P.SolverOptions().refine_tolerance
+    assert o.refine_steps == 3
+    c = P.SolverOptions(precision="mixed", refine_tolerance=1e-6).to_c()
+    assert c.refine_tolerance == 1e-6 and c.precision == 1
