@@ -86,6 +86,8 @@ def _declare(L):
     L.oracle_normals.argtypes = [ctypes.c_int, c_dbl_p, c_int_p, c_dbl_p, ctypes.c_int, ctypes.c_int,
                                  c_dbl_p, ctypes.c_int, ctypes.c_int] + [ctypes.c_double] * 4 + [
                                      ctypes.c_int, ctypes.c_double, c_dbl_p]
+    L.oracle_random_map.argtypes = [ctypes.c_uint32, c_dbl_p]
+    L.oracle_random_map.restype = None
     L.oracle_selftest_jacobians.argtypes = [c_int_p]
     L.oracle_selftest_jacobians.restype = ctypes.c_int
 
@@ -405,6 +407,14 @@ def eval_point(nx, ny, mn, mx, values, pose, p, delta, smooth=False, smooth_step
                             od.ctypes.data_as(c_dbl_p), oi.ctypes.data_as(c_int_p))
     return dict(valid=bool(oi[0]), residual=od[0], d_nodes=od[1:5].copy(), node_ids=oi[1:5].copy(),
                 d_pose=od[5:8].copy())
+
+
+def random_map(seed):
+    """RandomMap(std::mt19937(seed)) of tests/test_jacobians.cpp:13-20: the
+    node values of a 6 x 5 grid over [-3, 3] x [-2, 2]."""
+    out = np.zeros(30)
+    lib().oracle_random_map(int(seed), out.ctypes.data_as(c_dbl_p))
+    return out
 
 
 def eval_odom(pi, pj, meas):

@@ -454,6 +454,17 @@ void oracle_normals(int num_frames, const double* poses, const int* scan_offsets
   }
 }
 
+// RandomMap of tests/test_jacobians.cpp:13-20: a 6 x 5 grid over
+// [-3, 3] x [-2, 2] with node values uniform in [-2, 2] drawn from
+// std::mt19937(seed), in node order. values receives 30 doubles.
+void oracle_random_map(uint32_t seed, double* values) {
+  std::mt19937 rng(seed);
+  std::uniform_real_distribution<double> dist(-2.0, 2.0);
+  for (int i = 0; i < 30; ++i) {
+    values[i] = dist(rng);
+  }
+}
+
 // Port of tests/test_jacobians.cpp:33-153 (mt19937 seeds 42, 7, 43; central
 // differences with eps 1e-6, tolerance 1e-5; frozen-cell check omitted as it
 // is Ceres-only). Returns the number of failed comparisons; `checked` gets the

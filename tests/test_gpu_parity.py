@@ -169,6 +169,31 @@ def test_e2e_corner_scan_gpu(variant):
         assert all(h[i] <= h[i - 1] + 1e-9 for i in range(1, len(h)))
 
 
+def test_ceres_parity_harness_corner_scan():
+    """The Ceres-parity comparison harness with the GPU backend, as the
+    reference compares its backends (tests/test_e2e.cpp:90-101, :155-166):
+    the GPU LM (40 iterations) and the restated Ceres backend
+    (oracle/ceres_formulation.py, 60 iterations) from the same CornerScan
+    problem both pass ExpectRecovered, and their final poses differ by at
+    most 0.1 m and 0.05 rad (the frozen cells make them different problems;
+    Ceres is absent here, so its own iterates are not compared)."""
+    from ceres_formulation import compare, observed_nodes, solve_ceres
+    s = corner_setup()
+    nx, ny, mn, mx = s["grid"]
+    prob = P.Problem(nx, ny, mn, mx, s["init"], s["scans"], [s["odo"]], s["opts"])
+    gspecs = prob.specs(min_corner=mn, max_corner=mx)
+    ospecs = O.Specs(**{k: getattr(gspecs, k) for k in O.Specs.__dataclass_fields__})
+    r = P.solve(prob, P.SolverOptions(max_iterations=40))
+    gm, gp = prob.state()
+    expect_recovered(gm, gp, s, r.initial_cost, r.final_cost, s["grid"])
+    m, poses, rc = solve_ceres(ospecs, max_iterations=60)
+    expect_recovered(m, poses, s, rc["initial_cost"], rc["final_cost"], s["grid"])
+    cmp = compare((gm, gp), {"final_cost": r.final_cost}, (m, poses), rc, observed_nodes(ospecs))
+    print("GPU LM vs Ceres formulation:", cmp)
+    assert cmp["max_pose_diff_m"] <= 0.1 and cmp["max_angle_diff_rad"] <= 0.05
+    prob.close()
+
+
 def test_zero_pivot_raises_and_keeps_state():
     """lambda = 0 leaves map nodes without residual rows with a zero pivot:
     the reference throws "sparse Cholesky factorization failed" before it
