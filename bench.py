@@ -645,7 +645,7 @@ def _serve_pass(P, args, seed0, rate, check_oracle=False):
 # (-k <kernel>, one iteration's launches; dram__bytes_read / _write)
 # summarised in profiles/launch_list_office.md
 KERNEL_TRAFFIC_BYTES = {
-    ("office", "KUpdate(schur)"): 3054.4e6 / 20,   # the 20 Schur launches of the iteration
+    ("office", "KSchur"): 3054.4e6 / 20,   # the 20 Schur launches of the iteration
     ("office", "KDenseRoot"): 33.4e6,
     ("office", "KSolveTree"): 275.2e6,
     ("office", "KFactorFront"): 137.0e6 / 10,

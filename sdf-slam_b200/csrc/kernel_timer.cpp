@@ -7,7 +7,7 @@ namespace sdfgpu {
 
 const char* KernelTimer::Name(int c) {
   static const char* const kNames[kClasses] = {"KExtendAdd",     "KFactorFront", "KPanel",
-                                               "KUpdate(panel)", "KUpdate(schur)", "KPackSchur",
+                                               "KUpdate",        "KSchur",         "KPackSchur",
                                                "KSchurTc",       "KInvertDiagonal", "KSolveTree",
                                                "KDenseRoot"};
   return c >= 0 && c < kClasses ? kNames[c] : "";

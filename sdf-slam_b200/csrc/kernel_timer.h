@@ -17,8 +17,8 @@ class KernelTimer {
     kExtendAdd,
     kFactorFront,
     kPanel,
-    kUpdatePanel,   // KUpdate of the remaining pivot columns by one panel
-    kUpdateSchur,   // KUpdate of a front's Schur complement
+    kUpdatePanel,   // KUpdate: outer-block and panel updates of the later pivot columns
+    kUpdateSchur,   // KSchur / KSchurF32: the fronts' Schur complements
     kPackSchur,
     kSchurTc,
     kInvertDiagonal,
